@@ -1,0 +1,270 @@
+"""Pins the CPU checkers against the reference's own golden vectors.
+
+The C restatement (``port``) is checked against every golden vector the
+reference's unit tests hold for this path, and -- where the reference CPU
+library could be compiled from its sources -- bit-for-bit against it on
+seeded random inputs. Tolerances are the reference tests' own.
+"""
+
+import numpy as np
+import pytest
+
+F = "test_env_mat_a.cc:TestEnvMatA:"
+
+
+def _six_atoms(fx):
+    posi = fx[F + "posi"]
+    atype = fx[F + "atype"].astype(np.int32)
+    box = np.diag([13.0, 13.0, 13.0]).reshape(9)
+    return posi, atype, box
+
+
+def _env_pipeline(lib, posi, atype, box, sec, rc=6.0, rc_smth=0.8, dtype=np.float64):
+    c, t, _ = lib.copy_coord(posi, atype, rc, box)
+    nloc = atype.size
+    ret, il, nn, rb, _ = lib.build_nlist(c.astype(dtype), nloc, rc, atype=t)
+    assert ret == 0
+    nnei = sec[-1]
+    avg = np.zeros((2, nnei * 4), dtype)
+    std = np.ones((2, nnei * 4), dtype)
+    return c, t, lib.prod_env_mat_a(c.astype(dtype), t, il, nn, rb, avg, std, nloc,
+                                    rc, rc_smth, sec)
+
+
+@pytest.mark.parametrize("cls", ["TestEnvMatA", "TestEnvMatAShortSel"])
+def test_env_mat_golden(port, ref_fixtures, cls):
+    fx = ref_fixtures
+    key = f"test_env_mat_a.cc:{cls}:"
+    posi, atype, box = fx[key + "posi"], fx[key + "atype"].astype(np.int32), np.diag([13.0] * 3).reshape(9)
+    sec = fx[key + "sec_a"].astype(np.int32)
+    _, _, (em, emd, rij, nlist) = _env_pipeline(port, posi, atype, box, sec,
+                                                float(fx[key + "rc"]), float(fx[key + "rc_smth"]))
+    np.testing.assert_allclose(em.reshape(-1), fx[key + "expected_env"], atol=1e-5, rtol=0)
+
+
+def test_env_mat_numerical_derivative(port, ref_fixtures):
+    """em_deriv is d(em)/d(r_center) (env_mat.cc:146) = -d(em)/d(r_neighbor);
+    checked against central differences (test_env_mat_a.cc:281-324)."""
+    posi, atype, box = _six_atoms(ref_fixtures)
+    sec = np.array([0, 10, 20], np.int32)
+    c, t, (em, emd, rij, nlist) = _env_pipeline(port, posi, atype, box, sec)
+    nloc, nnei, h = 6, 20, 1e-7
+    for i in range(nloc):
+        for jj in range(nnei):
+            j = nlist[i, jj]
+            if j < 0:
+                continue
+            for d in range(3):
+                out = []
+                for s in (+1, -1):
+                    cc = c.copy()
+                    cc[j, d] += s * h
+                    r = cc[j] - cc[i]
+                    r2 = r @ r
+                    nr = np.sqrt(r2)
+                    u = (nr - 0.8) / (6.0 - 0.8)
+                    sw = 1.0 if nr < 0.8 else (u**3 * (-6 * u * u + 15 * u - 10) + 1 if nr < 6 else 0)
+                    out.append(np.array([1 / nr, r[0] / r2, r[1] / r2, r[2] / r2]) * sw)
+                num = (out[0] - out[1]) / (2 * h)
+                ana = emd[i, jj * 12:(jj + 1) * 12].reshape(4, 3)[:, d]
+                np.testing.assert_allclose(ana, -num, atol=1e-5)
+
+
+def test_prod_force_golden(port, ref_fixtures):
+    fx = ref_fixtures
+    key = "test_prod_force_a.cc:TestProdForceA:"
+    posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+    box = np.diag([13.0] * 3).reshape(9)
+    sec = fx[key + "sec_a"].astype(np.int32)
+    c, t, (em, emd, rij, nlist) = _env_pipeline(port, posi, atype, box, sec)
+    nloc, nall, nnei = 6, c.shape[0], int(sec[-1])
+    nd = 10 - np.arange(nloc * nnei * 4) * 0.01
+    # the gtest doubles every array to run two identical frames
+    force = port.prod_force_a(np.tile(nd, 2), np.tile(emd.reshape(-1), 2),
+                              np.tile(nlist.reshape(-1), 2), nloc, nall, nframes=2)
+    exp = np.tile(fx[key + "expected_force"], 2)
+    np.testing.assert_allclose(force.reshape(-1), exp, atol=1e-5, rtol=0)
+
+
+def test_prod_virial_golden(port, ref_fixtures):
+    fx = ref_fixtures
+    key = "test_prod_virial_a.cc:TestProdVirialA:"
+    posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+    box = np.diag([13.0] * 3).reshape(9)
+    sec = fx[key + "sec_a"].astype(np.int32)
+    c, t, (em, emd, rij, nlist) = _env_pipeline(port, posi, atype, box, sec)
+    nloc, nall, nnei = 6, c.shape[0], int(sec[-1])
+    nd = 10 - np.arange(nloc * nnei * 4) * 0.01
+    v, av = port.prod_virial_a(nd, emd, rij, nlist, nloc, nall)
+    np.testing.assert_allclose(v, fx[key + "expected_virial"], atol=1e-5, rtol=0)
+    np.testing.assert_allclose(av.reshape(-1), fx[key + "expected_atom_virial"], atol=1e-5, rtol=0)
+
+
+def _sorted_ghosts(c, t, m, nloc):
+    rows = sorted(zip(map(tuple, c[nloc:].tolist()), t[nloc:].tolist(), m[nloc:].tolist()))
+    return rows
+
+
+@pytest.mark.parametrize("cls", ["TestCopyCoord", "TestCopyCoordMoreCell"])
+def test_copy_coord_golden(port, ref_fixtures, cls):
+    fx = ref_fixtures
+    key = f"test_coord.cc:{cls}:"
+    posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+    c, t, m = port.copy_coord(posi, atype, float(fx[key + "rc"]), fx[key + "boxt"])
+    ec = fx[key + "_expected_posi_cpy"].reshape(-1, 3)
+    et = fx[key + "_expected_atype_cpy"]
+    em = fx[key + "_expected_mapping"]
+    assert c.shape == ec.shape
+    # the gtest compares after sorting the ghost block (test_coord.cc:131-165)
+    got, exp = _sorted_ghosts(c, t, m, 6), _sorted_ghosts(ec, et, em, 6)
+    for (gc, gt, gm), (xc, xt, xm) in zip(got, exp):
+        assert gt == xt and gm == xm
+        np.testing.assert_allclose(gc, xc, atol=1e-10)
+    np.testing.assert_array_equal(c[:6], ec[:6])
+
+
+def test_normalize_golden(port, ref_fixtures):
+    fx = ref_fixtures
+    key = "test_coord.cc:TestNormCoord:"
+    for r in ("r0", "r1", "r2"):
+        out = port.normalize_coord(fx[key + r], fx[key + "boxt"])
+        np.testing.assert_allclose(out, fx[key + "posi"], atol=1e-12, rtol=0)
+
+
+def test_tabulate_golden_cc(port, ref_fixtures):
+    fx = ref_fixtures
+    key = "test_tabulate_se_a.cc:TestTabulateSeA:"
+    nloc, nnei, M = (int(fx[key + n]) for n in ("nloc", "nnei", "last_layer_size"))
+    table, info = fx[key + "table"], fx[key + "info"]
+    em_x = fx[key + "em_x"].reshape(nloc, nnei)
+    em = fx[key + "em"].reshape(nloc, nnei, 4)
+    out = port.tabulate(table, info, em_x, em, M)
+    np.testing.assert_allclose(out.reshape(-1), fx[key + "expected_xyz_scatter"], atol=1e-5)
+    dy = np.ones((nloc, 4, M))
+    dx, de = port.tabulate_grad(table, info, em_x, em, dy, M)
+    np.testing.assert_allclose(dx.reshape(-1), fx[key + "expected_dy_dem_x"], atol=1e-5)
+    np.testing.assert_allclose(de.reshape(-1), fx[key + "expected_dy_dem"], atol=1e-5)
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-10), (np.float32, 1e-5)])
+def test_tabulate_golden_py(port, ref_fixtures, dtype, tol):
+    fx = ref_fixtures
+    key = "test_tabulate_fusion_se_a.py:"
+    table = fx[key + "table_tensor"].astype(dtype).reshape(-1)
+    info = fx[key + "table_info_tensor"].astype(dtype)
+    em_x = fx[key + "em_x_tensor"].astype(dtype)
+    em = fx[key + "em_tensor"].astype(dtype)
+    M = int(fx[key + "last_layer_size"])
+    out = port.tabulate(table, info, em_x, em, M)
+    np.testing.assert_allclose(out, fx[key + "expected_descriptor_tensor"], atol=tol, rtol=tol)
+    dx, de = port.tabulate_grad(table, info, em_x, em, np.ones_like(out), M)
+    np.testing.assert_allclose(dx, fx[key + "expected_dy_dem_x"], atol=tol, rtol=tol)
+    np.testing.assert_allclose(de, fx[key + "expected_dy_dem"], atol=tol, rtol=tol)
+
+
+def test_tabulate_grad_grad_is_adjoint(port, ref_fixtures):
+    """grad is linear in dy, so grad_grad must be its adjoint:
+    <dz_dy, dy> == <dz_dem_x, dy_dem_x(dy)> + <dz_dem, dy_dem(dy)>."""
+    fx = ref_fixtures
+    key = "test_tabulate_fusion_se_a.py:"
+    table = fx[key + "table_tensor"].reshape(-1)
+    info = fx[key + "table_info_tensor"]
+    em_x, em = fx[key + "em_x_tensor"], fx[key + "em_tensor"]
+    M = 8
+    rng = np.random.default_rng(0)
+    dy = rng.normal(size=(4, 4, M))
+    zx, ze = rng.normal(size=em_x.shape), rng.normal(size=em.shape)
+    dx, de = port.tabulate_grad(table, info, em_x, em, dy, M)
+    dz = port.tabulate_grad_grad(table, info, em_x, em, zx, ze, M)
+    lhs = (dz * dy).sum()
+    rhs = (zx * dx).sum() + (ze * de).sum()
+    assert abs(lhs - rhs) < 1e-10 * max(1.0, abs(lhs))
+
+
+# ------------------------------------------------------------------ random parity
+def _random_water(rng, nmol=24, box=9.0):
+    """Loose random water-like frame: O uniform in the box, two H at ~1 A."""
+    o = rng.uniform(0, box, size=(nmol, 3))
+    h1 = o + rng.normal(size=(nmol, 3)) * 0.55
+    h2 = o + rng.normal(size=(nmol, 3)) * 0.55
+    coord = np.stack([o, h1, h2], 1).reshape(-1, 3) % box
+    atype = np.tile([0, 1, 1], nmol).astype(np.int32)
+    return coord, atype, np.diag([box] * 3).reshape(9)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_port_equals_reference_random(port, ref_lib, dtype):
+    rng = np.random.default_rng(7)
+    coord, atype, box = _random_water(rng)
+    sec = np.array([0, 12, 30], np.int32)
+    rc, rs = 4.0, 0.5
+    outs = []
+    for lib in (port, ref_lib):
+        c, t, m = lib.copy_coord(coord, atype, rc, box)
+        nloc = atype.size
+        ret, il, nn, rb, _ = lib.build_nlist(c.astype(dtype), nloc, rc, atype=t)
+        avg = rng.normal(size=(2, sec[-1] * 4)).astype(dtype) * 0 + 0.1
+        std = np.full((2, sec[-1] * 4), 0.7, dtype)
+        env = lib.prod_env_mat_a(c.astype(dtype), t, il, nn, rb, avg, std, nloc, rc, rs, sec)
+        outs.append((c, t, m, nn, rb, env))
+    (c0, t0, m0, nn0, rb0, e0), (c1, t1, m1, nn1, rb1, e1) = outs
+    np.testing.assert_array_equal(c0, c1)
+    np.testing.assert_array_equal(m0, m1)
+    np.testing.assert_array_equal(nn0, nn1)
+    for a, b in zip(e0, e1):
+        np.testing.assert_array_equal(a, b)
+    # tabulate / force / virial on these shapes
+    em, emd, rij, nlist = e1
+    nloc, nnei, M = atype.size, int(sec[-1]), 16
+    table = rng.normal(size=(40, 6 * M)).astype(dtype)
+    info = np.array([-2.0, 1.0, 2.0, 0.1, 0.2, -1], dtype)
+    emv = em.reshape(nloc, nnei, 4)
+    ex = emv[:, :, 0].copy()
+    o0 = port.tabulate(table, info, ex, emv, M)
+    o1 = ref_lib.tabulate(table, info, ex, emv, M)
+    np.testing.assert_array_equal(o0, o1)
+    dy = rng.normal(size=o0.shape).astype(dtype)
+    for a, b in zip(port.tabulate_grad(table, info, ex, emv, dy, M),
+                    ref_lib.tabulate_grad(table, info, ex, emv, dy, M)):
+        np.testing.assert_array_equal(a, b)
+    zx = rng.normal(size=ex.shape).astype(dtype)
+    ze = rng.normal(size=emv.shape).astype(dtype)
+    np.testing.assert_array_equal(port.tabulate_grad_grad(table, info, ex, emv, zx, ze, M),
+                                  ref_lib.tabulate_grad_grad(table, info, ex, emv, zx, ze, M))
+    nd = rng.normal(size=(nloc, nnei * 4)).astype(dtype)
+    nall = c1.shape[0]
+    np.testing.assert_array_equal(port.prod_force_a(nd, emd, nlist, nloc, nall),
+                                  ref_lib.prod_force_a(nd, emd, nlist, nloc, nall))
+    v0, a0 = port.prod_virial_a(nd, emd, rij, nlist, nloc, nall)
+    v1, a1 = ref_lib.prod_virial_a(nd, emd, rij, nlist, nloc, nall)
+    # the reference accumulates the virial under an OpenMP atomic in thread order
+    tol = 1e-12 if dtype == np.float64 else 1e-5
+    np.testing.assert_allclose(v0, v1, rtol=tol, atol=tol)
+    np.testing.assert_allclose(a0, a1, rtol=tol, atol=tol)
+
+
+def test_format_nlist_ties_break_by_index(port):
+    """Equal float r^2 sorts by neighbor index (fmt_nlist.cc:14-26)."""
+    posi = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [-1, 0, 0]], np.float64)
+    atype = np.zeros(5, np.int32)
+    r, fmt = port_format(port, posi, atype, [4, 3, 2, 1])
+    assert r == -1
+    np.testing.assert_array_equal(fmt, [1, 2, 3, 4, -1])
+
+
+def port_format(port, posi, atype, cand):
+    from oracle import oracle
+
+    return oracle.format_nlist_i(posi, atype, 0, np.array(cand, np.int32), 6.0,
+                                 np.array([0, 5], np.int32))
+
+
+def test_format_nlist_overflow_reports_type(port):
+    posi = np.array([[0, 0, 0], [1, 0, 0], [0, 1.1, 0], [0, 0, 1.2]], np.float64)
+    atype = np.array([0, 1, 1, 1], np.int32)
+    from oracle import oracle
+
+    r, fmt = oracle.format_nlist_i(posi, atype, 0, np.array([1, 2, 3], np.int32), 6.0,
+                                   np.array([0, 1, 3], np.int32))
+    assert r == 1  # three type-1 neighbors into two slots: farthest dropped
+    np.testing.assert_array_equal(fmt, [-1, 1, 2])
