@@ -1,0 +1,151 @@
+"""ctypes binding of the C-ABI in include/dpb200.h (libdpb200.so).
+
+The library is the only compute path: if it cannot be loaded, importing the
+package fails (no CPU fallback).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libdpb200.so")
+
+
+class DPBError(RuntimeError):
+    """deepmd::deepmd_exception counterpart ("DeePMD-kit Error: ...")."""
+
+
+class DPBCapacityError(DPBError):
+    """Return code 1 of build_nlist_gpu / copy_coord_gpu: buffers too small."""
+
+
+class DPBInvalidArgument(DPBError, ValueError):
+    """std::invalid_argument / TORCH_CHECK failures of the reference ops."""
+
+
+class DPBCudaError(DPBError):
+    """DPErrcheck failure."""
+
+
+class DPBOutOfMemory(DPBError, MemoryError):
+    """deepmd::deepmd_exception_oom."""
+
+
+class DPBNlistCapacityError(DPBError):
+    """deepmd::deepmd_exception_nlist_capacity."""
+
+
+class DPBOverflowError(DPBError):
+    """Neighbor sort-key overflow (the reference traps on the device here)."""
+
+
+_ERRORS = {
+    1: DPBCapacityError,
+    2: DPBInvalidArgument,
+    3: DPBCudaError,
+    4: DPBOutOfMemory,
+    5: DPBNlistCapacityError,
+    6: DPBOverflowError,
+}
+
+P, I, F, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_longlong
+_SPEC = {"p": P, "i": I, "f": F, "L": LL}
+
+# name -> argument kinds (p pointer, i int, f float, L long long)
+_FUNCS = {
+    "dpb_status_check": "pp",
+    "dpb_normalize_coord_f64": "pipp",
+    "dpb_normalize_coord_f32": "pipp",
+    # out_c, out_t, mapping, nall(host), scratch, scratch_bytes, in_c, in_t,
+    # nloc, mem_nall, rcut, boxt(host), stream
+    "dpb_copy_coord_f64": "pppppLppiifpp",
+    "dpb_copy_coord_f32": "pppppLppiifpp",
+    "dpb_cell_grid_build_f64": "pLpifp",
+    "dpb_cell_grid_build_f32": "pLpifp",
+    "dpb_build_nlist_f64": "pppppLpiiifipp",
+    "dpb_build_nlist_f32": "pppppLpiiifipp",
+    "dpb_prod_env_mat_a_f64": "pppppp" "ipppi" "ppiiiff" "pipp",
+    "dpb_prod_env_mat_a_f32": "pppppp" "ipppi" "ppiiiff" "pipp",
+    "dpb_env_mat_a_cells_f64": "pppppp" "p" "ppiiff" "pipp",
+    "dpb_env_mat_a_cells_f32": "pppppp" "p" "ppiiff" "pipp",
+    "dpb_env_mat_a_cells_mixed": "pppppp" "p" "ppiiff" "pipp",
+    "dpb_tabulate_fusion_se_a_f64": "pppppiiip",
+    "dpb_tabulate_fusion_se_a_f32": "pppppiiip",
+    "dpb_tabulate_fusion_se_a_grad_f64": "ppppppp" "iiip",
+    "dpb_tabulate_fusion_se_a_grad_f32": "ppppppp" "iiip",
+    "dpb_tabulate_fusion_se_a_grad_grad_f64": "ppppppp" "iiip",
+    "dpb_tabulate_fusion_se_a_grad_grad_f32": "ppppppp" "iiip",
+    "dpb_prod_force_a_f64": "ppppiiiip",
+    "dpb_prod_force_a_f32": "ppppiiiip",
+    "dpb_prod_virial_a_f64": "pppppp" "iiip",
+    "dpb_prod_virial_a_f32": "pppppp" "iiip",
+}
+_SIZE_QUERIES = {
+    "dpb_copy_coord_scratch_bytes": ("ifp", LL),
+    "dpb_cell_grid_bytes": ("i", LL),
+    "dpb_build_nlist_scratch_bytes": ("ii", LL),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libdpb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python deepmd-kit-lr-pt_b200/build.py` "
+            "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, spec in _FUNCS.items():
+        f = getattr(L, name)
+        f.argtypes = [_SPEC[c] for c in spec]
+        f.restype = I
+    for name, (spec, rt) in _SIZE_QUERIES.items():
+        f = getattr(L, name)
+        f.argtypes = [_SPEC[c] for c in spec]
+        f.restype = rt
+    L.dpb_last_error.restype = ctypes.c_char_p
+    L.dpb_abi_version.restype = I
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().dpb_last_error().decode(errors="replace")
+
+
+def check(code: int, what: str = "") -> None:
+    """Raise the exception class that mirrors the reference's error type."""
+    if code == 0:
+        return
+    cls = _ERRORS.get(code, DPBError)
+    msg = last_error()
+    raise cls(f"DeePMD-kit Error: {what + ': ' if what else ''}{msg}")
+
+
+def call(name: str, *args) -> int:
+    """Call an entry point and raise on failure."""
+    code = getattr(lib(), name)(*args)
+    check(code, name)
+    return code
+
+
+def ptr(x) -> int | None:
+    """Device/host address of a torch tensor or numpy array (None stays NULL)."""
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return x.data_ptr()
+
+
+def exported_symbols() -> list[str]:
+    return sorted(list(_FUNCS) + list(_SIZE_QUERIES) +
+                  ["dpb_last_error", "dpb_abi_version"])

@@ -1,0 +1,76 @@
+// Shared device/host helpers for the se_e2_a kernels (sm_100a).
+//
+// Error model: every C-ABI entry point returns a dpb_status code and records a
+// message readable through dpb_last_error(). Kernels never trap: conditions
+// the reference turns into a device trap or assert (sort-key overflow in
+// source/lib/src/gpu/prod_env_mat.cu:92-99, max_nbor_size assert at :640-642)
+// are written to a caller-visible device status word instead.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/dpb200.h"
+
+namespace dpb {
+
+// Device status word bits (OR-ed together by kernels; 0 = fine).
+enum : int {
+  ST_NLIST_CAPACITY = 1 << 0,  // more in-range candidates than the row buffer
+  ST_KEY_OVERFLOW = 1 << 1,    // type >= 128 or index >= 2^24 in a sort key
+  ST_SEL_OVERFLOW = 1 << 2,    // more neighbors of a type than sel (dropped)
+  ST_ROW_CAPACITY = 1 << 3,    // build_nlist row longer than mem_size
+  ST_CELL_RANGE = 1 << 4,      // ghost/cell index outside the cell grid
+};
+
+void set_error(const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* where);
+
+inline cudaStream_t as_stream(dpb_stream_t s) {
+  return reinterpret_cast<cudaStream_t>(s);
+}
+
+#define DPB_CHECK_LAUNCH(where)                                  \
+  do {                                                           \
+    cudaError_t _e = cudaGetLastError();                         \
+    if (_e != cudaSuccess) return ::dpb::cuda_status(_e, where); \
+  } while (0)
+
+#define DPB_CUDA(call, where)                                    \
+  do {                                                           \
+    cudaError_t _e = (call);                                     \
+    if (_e != cudaSuccess) return ::dpb::cuda_status(_e, where); \
+  } while (0)
+
+// ---- correctly rounded, never-contracted arithmetic -----------------------
+// The CPU oracle is compiled with -ffp-contract=off, so quantities that feed
+// integer decisions (cutoff tests, sort keys, cell indices) are computed here
+// with explicit round-to-nearest intrinsics that the compiler cannot fuse.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+
+// r0*r0 + r1*r1 + r2*r2 evaluated left to right without fusion
+// (source/lib/include/utilities.h:24-26).
+template <typename T>
+__device__ __forceinline__ T dot3_rn(T a, T b, T c) {
+  return add_rn(add_rn(mul_rn(a, a), mul_rn(b, b)), mul_rn(c, c));
+}
+
+// Warp-level inclusive sum.
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void atomic_add(double* p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add(float* p, float v) { atomicAdd(p, v); }
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace dpb

@@ -1,0 +1,644 @@
+// Coordinates: wrap into the box, periodic ghost images, and the cell grid
+// used by the neighbor search.
+//
+// copy_coord reproduces copy_coord_cpu (source/lib/src/coord.cc:29-64 ->
+// source/lib/src/neighbor_list.cc:43-148,730-849) element for element: local
+// atoms first, then for every ghost cell of the extended grid (x outer, z
+// inner, local cells skipped) the atoms of its periodic source cell in
+// ascending index, shifted by the box. The reference's own GPU version
+// (source/lib/src/gpu/coord.cu:352-414) emits a different ghost order; this
+// one matches the CPU path so that neighbor indices compare bit for bit.
+#include <math.h>
+
+#include "dpb_common.cuh"
+#include "dpb_internal.cuh"
+
+namespace dpb {
+
+// --------------------------------------------------------------- region ----
+
+void host_region(HostRegion& r, const double* b, float rcut) {
+  // |det| and cofactor inverse (source/lib/include/SimulationRegion_Impl.h:
+  // 429-480); distances between opposite faces (:364-372); cell counts
+  // (source/lib/src/neighbor_list.cc:747-772).
+  double vol = b[0] * (b[4] * b[8] - b[7] * b[5]) -
+               b[1] * (b[3] * b[8] - b[6] * b[5]) +
+               b[2] * (b[3] * b[7] - b[6] * b[4]);
+  vol = fabs(vol);
+  double vi = 1. / vol;
+  double* rc = r.rec;
+  rc[0] = (b[4] * b[8] - b[7] * b[5]) * vi;
+  rc[4] = (b[0] * b[8] - b[6] * b[2]) * vi;
+  rc[8] = (b[0] * b[4] - b[3] * b[1]) * vi;
+  rc[1] = (-b[3] * b[8] + b[6] * b[5]) * vi;
+  rc[2] = (b[3] * b[7] - b[6] * b[4]) * vi;
+  rc[3] = (-b[1] * b[8] + b[7] * b[2]) * vi;
+  rc[5] = (-b[0] * b[7] + b[6] * b[1]) * vi;
+  rc[6] = (b[1] * b[5] - b[4] * b[2]) * vi;
+  rc[7] = (-b[0] * b[5] + b[3] * b[2]) * vi;
+  for (int k = 0; k < 9; ++k) r.box[k] = b[k];
+  auto face = [&](const double* u, const double* v) {
+    double t0 = u[1] * v[2] - u[2] * v[1];
+    double t1 = u[2] * v[0] - u[0] * v[2];
+    double t2 = u[0] * v[1] - u[1] * v[0];
+    return vol * (1. / sqrt(t0 * t0 + t1 * t1 + t2 * t2));
+  };
+  double tf[3] = {face(b + 3, b + 6), face(b + 6, b + 0), face(b + 0, b + 3)};
+  double rcd = (double)rcut;
+  r.nloc_cells = 1;
+  r.next_cells = 1;
+  for (int d = 0; d < 3; ++d) {
+    int n = (int)(tf[d] / rcd);
+    if (n == 0) n = 1;
+    double cs = tf[d] / n;
+    r.nc[d] = n;
+    r.ng[d] = (int)(rcd / cs) + 1;
+    r.inv_nc[d] = 1. / n;
+    r.nloc_cells *= n;
+    r.next_cells *= n + 2 * r.ng[d];
+  }
+  r.volume = vol;
+}
+
+__device__ __forceinline__ void dev_t_dot_v(double* o, const double* t,
+                                            const double* v) {
+  // o = t . v, left-to-right, no fusion (SimulationRegion_Impl.h:388-396)
+  o[0] = add_rn(add_rn(mul_rn(v[0], t[0]), mul_rn(v[1], t[1])), mul_rn(v[2], t[2]));
+  o[1] = add_rn(add_rn(mul_rn(v[0], t[3]), mul_rn(v[1], t[4])), mul_rn(v[2], t[5]));
+  o[2] = add_rn(add_rn(mul_rn(v[0], t[6]), mul_rn(v[1], t[7])), mul_rn(v[2], t[8]));
+}
+__device__ __forceinline__ void dev_tt_dot_v(double* o, const double* t,
+                                             const double* v) {
+  // o = t^T . v (SimulationRegion_Impl.h:399-407)
+  o[0] = add_rn(add_rn(mul_rn(v[0], t[0]), mul_rn(v[1], t[3])), mul_rn(v[2], t[6]));
+  o[1] = add_rn(add_rn(mul_rn(v[0], t[1]), mul_rn(v[1], t[4])), mul_rn(v[2], t[7]));
+  o[2] = add_rn(add_rn(mul_rn(v[0], t[2]), mul_rn(v[1], t[5])), mul_rn(v[2], t[8]));
+}
+
+// ------------------------------------------------------------ normalize ----
+
+template <typename T>
+__global__ void k_normalize(T* coord, int natom, HostRegion r) {
+  // source/lib/src/coord.cc:14-27: inter = rec.p, fmod(.,1), +1 if < 0,
+  // back to physical. Region arithmetic runs in T like the reference.
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natom) return;
+  T p[3] = {coord[3 * i], coord[3 * i + 1], coord[3 * i + 2]};
+  T ri[3];
+  for (int d = 0; d < 3; ++d) {
+    ri[d] = add_rn(add_rn(mul_rn(p[0], (T)r.rec[3 * d]), mul_rn(p[1], (T)r.rec[3 * d + 1])),
+                   mul_rn(p[2], (T)r.rec[3 * d + 2]));
+    ri[d] = fmod(ri[d], (T)1.);
+    if (ri[d] < (T)0.) ri[d] = add_rn(ri[d], (T)1.);
+  }
+  for (int d = 0; d < 3; ++d) {
+    coord[3 * i + d] = add_rn(add_rn(mul_rn(ri[0], (T)r.box[d]), mul_rn(ri[1], (T)r.box[3 + d])),
+                              mul_rn(ri[2], (T)r.box[6 + d]));
+  }
+}
+
+// ------------------------------------------------------------ copy_coord ---
+
+struct CopyScratch {
+  int* cell_of;   // [nloc]
+  int* cnt;       // [nloc_cells + 1] counts, then starts
+  int* fill;      // [nloc_cells]
+  int* order;     // [nloc]
+  int* ext_off;   // [next_cells + 1]
+  int* nall;      // [1]
+};
+
+static long long copy_scratch_ints(int nloc, const HostRegion& r) {
+  return (long long)nloc * 2 + (r.nloc_cells + 1) + r.nloc_cells +
+         (r.next_cells + 1) + 1 + 64;
+}
+
+static CopyScratch carve_copy(void* p, int nloc, const HostRegion& r) {
+  int* q = (int*)p;
+  CopyScratch s;
+  s.cell_of = q; q += nloc;
+  s.cnt = q; q += r.nloc_cells + 1;
+  s.fill = q; q += r.nloc_cells;
+  s.order = q; q += nloc;
+  s.ext_off = q; q += r.next_cells + 1;
+  s.nall = q;
+  return s;
+}
+
+template <typename T>
+__global__ void k_cc_cell(CopyScratch s, T* out_c, int* out_t, int* mapping,
+                          const T* in_c, const int* in_t, int nloc,
+                          int mem_nall, HostRegion r) {
+  // cell of each local atom as build_clist computes it
+  // (source/lib/src/neighbor_list.cc:84-111, nat_stt = 0, nat_end = ncell)
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nloc) return;
+  double p[3] = {(double)in_c[3 * i], (double)in_c[3 * i + 1], (double)in_c[3 * i + 2]};
+  double inter[3];
+  dev_t_dot_v(inter, r.rec, p);
+  int idx[3];
+  for (int d = 0; d < 3; ++d) {
+    double csz = r.inv_nc[d];
+    idx[d] = (int)(__ddiv_rn(inter[d] - 0., csz));
+    if (inter[d] - 0. < 0.) idx[d]--;
+    if (idx[d] < 0) idx[d] = 0;
+    else if (idx[d] >= r.nc[d]) idx[d] = r.nc[d] - 1;
+  }
+  int c = (idx[0] * r.nc[1] + idx[1]) * r.nc[2] + idx[2];
+  s.cell_of[i] = c;
+  atomicAdd(&s.cnt[c], 1);
+  if (i < mem_nall) {
+    out_c[3 * i] = in_c[3 * i];
+    out_c[3 * i + 1] = in_c[3 * i + 1];
+    out_c[3 * i + 2] = in_c[3 * i + 2];
+    out_t[i] = in_t[i];
+    mapping[i] = i;
+  }
+}
+
+// Exclusive scan of n ints in place by one block (n may be large: chunked).
+__device__ void block_exclusive_scan(int* a, int n, int* total) {
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  for (int base = 0; base < n; base += blockDim.x) {
+    int k = base + threadIdx.x;
+    int v = k < n ? a[k] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int w = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      warp_sums[lane] = w;  // inclusive
+    }
+    __syncthreads();
+    int prefix = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + x - v;
+    if (k < n) a[k] = prefix;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = prefix + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__device__ __forceinline__ int pbc_shift(int idx, int n) {
+  // source/lib/src/neighbor_list.cc:730-745
+  int s = 0;
+  if (idx < 0) {
+    s = 1;
+    while (idx + s * n < 0) s++;
+  } else if (idx >= n) {
+    s = -1;
+    while (idx + s * n >= n) s--;
+  }
+  return s;
+}
+
+__device__ __forceinline__ void ext_cell_coords(int e, const HostRegion& r,
+                                                int* ii) {
+  int E1 = r.nc[1] + 2 * r.ng[1], E2 = r.nc[2] + 2 * r.ng[2];
+  ii[2] = e % E2 - r.ng[2];
+  int t = e / E2;
+  ii[1] = t % E1 - r.ng[1];
+  ii[0] = t / E1 - r.ng[0];
+}
+
+__global__ void k_cc_scan(CopyScratch s, int nloc, HostRegion r) {
+  // starts of the local cells, then ghost offsets in the reference's ghost
+  // loop order (source/lib/src/neighbor_list.cc:799-826)
+  __shared__ int tot;
+  block_exclusive_scan(s.cnt, r.nloc_cells + 1, &tot);
+  __syncthreads();
+  for (int e = threadIdx.x; e <= r.next_cells; e += blockDim.x) {
+    if (e == r.next_cells) {
+      s.ext_off[e] = 0;
+      continue;
+    }
+    int ii[3];
+    ext_cell_coords(e, r, ii);
+    bool local = ii[0] >= 0 && ii[0] < r.nc[0] && ii[1] >= 0 &&
+                 ii[1] < r.nc[1] && ii[2] >= 0 && ii[2] < r.nc[2];
+    int v = 0;
+    if (!local) {
+      int jj[3];
+      for (int d = 0; d < 3; ++d) jj[d] = ii[d] + pbc_shift(ii[d], r.nc[d]) * r.nc[d];
+      int c = (jj[0] * r.nc[1] + jj[1]) * r.nc[2] + jj[2];
+      v = s.cnt[c + 1] - s.cnt[c];
+    }
+    s.ext_off[e] = v;
+  }
+  __syncthreads();
+  block_exclusive_scan(s.ext_off, r.next_cells + 1, &tot);
+  __syncthreads();
+  if (threadIdx.x == 0) *s.nall = nloc + s.ext_off[r.next_cells];
+}
+
+__global__ void k_cc_fill(CopyScratch s, int nloc) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nloc) return;
+  int c = s.cell_of[i];
+  int pos = s.cnt[c] + atomicAdd(&s.fill[c], 1);
+  s.order[pos] = i;
+}
+
+__global__ void k_cc_sort(CopyScratch s, int ncells) {
+  // ascending atom index within each cell (build_clist pushes in index order)
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  int b = s.cnt[c], e = s.cnt[c + 1];
+  for (int a = b + 1; a < e; ++a) {
+    int v = s.order[a], q = a - 1;
+    while (q >= b && s.order[q] > v) {
+      s.order[q + 1] = s.order[q];
+      q--;
+    }
+    s.order[q + 1] = v;
+  }
+}
+
+template <typename T>
+__global__ void k_cc_copy(CopyScratch s, T* out_c, int* out_t, int* mapping,
+                          const T* in_c, const int* in_t, int nloc,
+                          int mem_nall, HostRegion r) {
+  // one warp per extended cell: ghost = source atom - box shift
+  // (source/lib/src/neighbor_list.cc:815-831)
+  int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (e >= r.next_cells) return;
+  int ii[3];
+  ext_cell_coords(e, r, ii);
+  if (ii[0] >= 0 && ii[0] < r.nc[0] && ii[1] >= 0 && ii[1] < r.nc[1] &&
+      ii[2] >= 0 && ii[2] < r.nc[2])
+    return;
+  int jj[3];
+  double ps[3];
+  for (int d = 0; d < 3; ++d) {
+    int sh = pbc_shift(ii[d], r.nc[d]);
+    ps[d] = (double)sh;
+    jj[d] = ii[d] + sh * r.nc[d];
+  }
+  double sv[3];
+  dev_tt_dot_v(sv, r.box, ps);
+  int c = (jj[0] * r.nc[1] + jj[1]) * r.nc[2] + jj[2];
+  int b = s.cnt[c], n = s.cnt[c + 1] - b;
+  int w0 = nloc + s.ext_off[e];
+  for (int k = lane; k < n; k += 32) {
+    int p = s.order[b + k];
+    int w = w0 + k;
+    if (w < mem_nall) {
+      out_c[3 * w + 0] = (T)sub_rn((double)in_c[3 * p + 0], sv[0]);
+      out_c[3 * w + 1] = (T)sub_rn((double)in_c[3 * p + 1], sv[1]);
+      out_c[3 * w + 2] = (T)sub_rn((double)in_c[3 * p + 2], sv[2]);
+      out_t[w] = in_t[p];
+      mapping[w] = p;
+    }
+  }
+}
+
+template <typename T>
+int copy_coord_async(T* out_c, int* out_t, int* mapping, int* nall_dev,
+                     void* scratch, long long scratch_bytes, const T* in_c,
+                     const int* in_t, int nloc, int mem_nall, float rcut,
+                     const double* boxt, cudaStream_t st) {
+  if (nloc < 0 || mem_nall < 0 || !(rcut > 0.f)) {
+    set_error("copy_coord: invalid sizes (nloc=%d mem_nall=%d rcut=%g)", nloc,
+              mem_nall, (double)rcut);
+    return DPB_ERR_INVALID;
+  }
+  HostRegion r;
+  host_region(r, boxt, rcut);
+  if (!(r.volume > 0.)) {
+    set_error("copy_coord: the box has zero volume");
+    return DPB_ERR_INVALID;
+  }
+  long long need = copy_scratch_ints(nloc, r) * (long long)sizeof(int);
+  if (scratch == nullptr || scratch_bytes < need) {
+    set_error("copy_coord: scratch too small (%lld < %lld bytes)",
+              scratch_bytes, need);
+    return DPB_ERR_INVALID;
+  }
+  CopyScratch s = carve_copy(scratch, nloc, r);
+  DPB_CUDA(cudaMemsetAsync(s.cnt, 0, sizeof(int) * (2 * r.nloc_cells + 1), st),
+           "copy_coord");
+  if (nloc > 0) {
+    k_cc_cell<T><<<ceil_div(nloc, 256), 256, 0, st>>>(s, out_c, out_t, mapping, in_c,
+                                                     in_t, nloc, mem_nall, r);
+    DPB_CHECK_LAUNCH("copy_coord/cell");
+  }
+  k_cc_scan<<<1, 1024, 0, st>>>(s, nloc, r);
+  DPB_CHECK_LAUNCH("copy_coord/scan");
+  if (nloc > 0) {
+    k_cc_fill<<<ceil_div(nloc, 256), 256, 0, st>>>(s, nloc);
+    DPB_CHECK_LAUNCH("copy_coord/fill");
+  }
+  k_cc_sort<<<ceil_div(r.nloc_cells, 128), 128, 0, st>>>(s, r.nloc_cells);
+  DPB_CHECK_LAUNCH("copy_coord/sort");
+  k_cc_copy<T><<<ceil_div((long long)r.next_cells * 32, 256), 256, 0, st>>>(
+      s, out_c, out_t, mapping, in_c, in_t, nloc, mem_nall, r);
+  DPB_CHECK_LAUNCH("copy_coord/copy");
+  if (nall_dev) {
+    DPB_CUDA(cudaMemcpyAsync(nall_dev, s.nall, sizeof(int),
+                             cudaMemcpyDeviceToDevice, st),
+             "copy_coord");
+  }
+  return DPB_OK;
+}
+
+template <typename T>
+int copy_coord_sync(T* out_c, int* out_t, int* mapping, int* nall,
+                    void* scratch, long long scratch_bytes, const T* in_c,
+                    const int* in_t, int nloc, int mem_nall, float rcut,
+                    const T* boxt, cudaStream_t st) {
+  double b[9];
+  for (int k = 0; k < 9; ++k) b[k] = (double)boxt[k];
+  int rc = copy_coord_async<T>(out_c, out_t, mapping, nullptr, scratch,
+                               scratch_bytes, in_c, in_t, nloc, mem_nall, rcut,
+                               b, st);
+  if (rc != DPB_OK) return rc;
+  HostRegion r;
+  host_region(r, b, rcut);
+  CopyScratch s = carve_copy(scratch, nloc, r);
+  int h = 0;
+  DPB_CUDA(cudaMemcpyAsync(&h, s.nall, sizeof(int), cudaMemcpyDeviceToHost, st),
+           "copy_coord");
+  DPB_CUDA(cudaStreamSynchronize(st), "copy_coord");
+  *nall = h;
+  if (h > mem_nall) {
+    set_error("copy_coord: nall=%d exceeds mem_nall=%d", h, mem_nall);
+    return DPB_ERR_CAPACITY;
+  }
+  return DPB_OK;
+}
+
+// ------------------------------------------------------------ cell grid ----
+
+__device__ __forceinline__ unsigned long long ord_key(double x) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ord_val(unsigned long long k) {
+  unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)u);
+}
+
+__global__ void k_grid_init(GridHeader* h) {
+  for (int d = 0; d < 3; ++d) {
+    h->kmin[d] = ~0ull;
+    h->kmax[d] = 0ull;
+  }
+}
+
+template <typename T>
+__global__ void k_grid_bbox(GridHeader* h, const T* coord, int nall,
+                            const int* nall_dev) {
+  int n = nall_dev ? min(*nall_dev, nall) : nall;
+  unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    for (int d = 0; d < 3; ++d) {
+      unsigned long long k = ord_key((double)coord[3 * i + d]);
+      mn[d] = k < mn[d] ? k : mn[d];
+      mx[d] = k > mx[d] ? k : mx[d];
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long a = __shfl_xor_sync(0xffffffffu, mn[d], o);
+      unsigned long long b = __shfl_xor_sync(0xffffffffu, mx[d], o);
+      mn[d] = a < mn[d] ? a : mn[d];
+      mx[d] = b > mx[d] ? b : mx[d];
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&h->kmin[d], mn[d]);
+      atomicMax(&h->kmax[d], mx[d]);
+    }
+  }
+}
+
+__global__ void k_grid_setup(GridHeader* h, float rcut, int max_cells,
+                             int nall, const int* nall_dev) {
+  // cells of edge >= rcut * (1 + 1e-4) over the bounding box, so that every
+  // pair closer than rcut lies in adjacent cells whatever the rounding
+  int n = nall_dev ? min(*nall_dev, nall) : nall;
+  double edge = (double)rcut * 1.0001;
+  int dims[3];
+  double lo[3], ext[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = n > 0 ? ord_val(h->kmin[d]) : 0.;
+    double hi = n > 0 ? ord_val(h->kmax[d]) : 0.;
+    ext[d] = hi - lo[d];
+    dims[d] = (int)(ext[d] / edge);
+    if (dims[d] < 1) dims[d] = 1;
+  }
+  while ((long long)dims[0] * dims[1] * dims[2] > max_cells) {
+    for (int d = 0; d < 3; ++d) dims[d] = dims[d] > 1 ? (dims[d] + 1) / 2 : 1;
+  }
+  for (int d = 0; d < 3; ++d) {
+    h->dims[d] = dims[d];
+    h->origin[d] = lo[d];
+    double cs = ext[d] / dims[d];
+    h->inv_cs[d] = cs > 0. ? 1. / cs : 0.;
+  }
+  h->ncells = dims[0] * dims[1] * dims[2];
+  h->natoms = n;
+}
+
+template <typename T>
+__device__ __forceinline__ int grid_cell_of(const GridHeader& h, const T* p) {
+  int c[3];
+  for (int d = 0; d < 3; ++d) {
+    int k = (int)(((double)p[d] - h.origin[d]) * h.inv_cs[d]);
+    c[d] = k < 0 ? 0 : (k >= h.dims[d] ? h.dims[d] - 1 : k);
+  }
+  return (c[0] * h.dims[1] + c[1]) * h.dims[2] + c[2];
+}
+
+template <typename T>
+__global__ void k_grid_count(GridView g, const T* coord) {
+  const GridHeader& h = *g.h;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= h.natoms) return;
+  int c = grid_cell_of(h, coord + 3 * i);
+  g.cell_of[i] = c;
+  atomicAdd(&g.cell_start[c], 1);
+}
+
+__global__ void k_grid_scan(GridView g) {
+  __shared__ int tot;
+  block_exclusive_scan(g.cell_start, g.h->ncells + 1, &tot);
+}
+
+__global__ void k_grid_fill(GridView g) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.h->natoms) return;
+  int c = g.cell_of[i];
+  int pos = g.cell_start[c] + atomicAdd(&g.fill[c], 1);
+  g.cell_atoms[pos] = i;
+}
+
+long long grid_bytes(int nall) {
+  int max_cells = nall > 64 ? nall : 64;
+  long long ints = (long long)(max_cells + 1) + max_cells + 2LL * nall + 64;
+  return (long long)sizeof(GridHeader) + 256 + ints * (long long)sizeof(int);
+}
+
+GridView carve_grid(void* p, int nall) {
+  int max_cells = nall > 64 ? nall : 64;
+  GridView g;
+  g.h = (GridHeader*)p;
+  int* q = (int*)((char*)p + ((sizeof(GridHeader) + 255) / 256) * 256);
+  g.cell_start = q; q += max_cells + 1;
+  g.fill = q; q += max_cells;
+  g.cell_of = q; q += nall;
+  g.cell_atoms = q;
+  g.max_cells = max_cells;
+  g.cap_atoms = nall;
+  return g;
+}
+
+template <typename T>
+int grid_build(void* grid, long long bytes, const T* coord, int nall,
+               const int* nall_dev, float rcut, cudaStream_t st) {
+  if (nall < 0 || !(rcut > 0.f)) {
+    set_error("cell grid: invalid arguments (nall=%d rcut=%g)", nall, (double)rcut);
+    return DPB_ERR_INVALID;
+  }
+  if (grid == nullptr || bytes < grid_bytes(nall)) {
+    set_error("cell grid: buffer too small (%lld < %lld bytes)", bytes, grid_bytes(nall));
+    return DPB_ERR_INVALID;
+  }
+  GridView g = carve_grid(grid, nall);
+  k_grid_init<<<1, 1, 0, st>>>(g.h);
+  DPB_CHECK_LAUNCH("cell grid/init");
+  int nb = nall > 0 ? ceil_div(nall, 256) : 1;
+  if (nb > 148 * 8) nb = 148 * 8;
+  k_grid_bbox<T><<<nb, 256, 0, st>>>(g.h, coord, nall, nall_dev);
+  DPB_CHECK_LAUNCH("cell grid/bbox");
+  k_grid_setup<<<1, 1, 0, st>>>(g.h, rcut, g.max_cells, nall, nall_dev);
+  DPB_CHECK_LAUNCH("cell grid/setup");
+  DPB_CUDA(cudaMemsetAsync(g.cell_start, 0, sizeof(int) * (2 * g.max_cells + 1), st),
+           "cell grid");
+  int na = nall > 0 ? ceil_div(nall, 256) : 1;
+  k_grid_count<T><<<na, 256, 0, st>>>(g, coord);
+  DPB_CHECK_LAUNCH("cell grid/count");
+  k_grid_scan<<<1, 1024, 0, st>>>(g);
+  DPB_CHECK_LAUNCH("cell grid/scan");
+  k_grid_fill<<<na, 256, 0, st>>>(g);
+  DPB_CHECK_LAUNCH("cell grid/fill");
+  return DPB_OK;
+}
+
+template int grid_build<double>(void*, long long, const double*, int, const int*, float, cudaStream_t);
+template int grid_build<float>(void*, long long, const float*, int, const int*, float, cudaStream_t);
+template int copy_coord_async<double>(double*, int*, int*, int*, void*, long long, const double*,
+                                      const int*, int, int, float, const double*, cudaStream_t);
+template int copy_coord_async<float>(float*, int*, int*, int*, void*, long long, const float*,
+                                     const int*, int, int, float, const double*, cudaStream_t);
+
+long long copy_coord_scratch_bytes(int nloc, float rcut, const double* boxt) {
+  HostRegion r;
+  host_region(r, boxt, rcut);
+  return copy_scratch_ints(nloc, r) * (long long)sizeof(int);
+}
+
+}  // namespace dpb
+
+// ------------------------------------------------------------- C-ABI -------
+using namespace dpb;
+extern "C" {
+
+int dpb_normalize_coord_f64(double* coord, int natom, const double* boxt,
+                            dpb_stream_t stream) {
+  if (natom <= 0) return DPB_OK;
+  HostRegion r;
+  host_region(r, boxt, 1.f);
+  k_normalize<double><<<ceil_div(natom, 256), 256, 0, as_stream(stream)>>>(coord, natom, r);
+  DPB_CHECK_LAUNCH("normalize_coord");
+  return DPB_OK;
+}
+
+int dpb_normalize_coord_f32(float* coord, int natom, const float* boxt,
+                            dpb_stream_t stream) {
+  if (natom <= 0) return DPB_OK;
+  // the reference keeps float boxes in float (region.cc:38-90)
+  double b[9];
+  for (int k = 0; k < 9; ++k) b[k] = boxt[k];
+  HostRegion r;
+  host_region(r, b, 1.f);
+  float bf[9], rf[9];
+  for (int k = 0; k < 9; ++k) bf[k] = boxt[k];
+  float v = bf[0] * (bf[4] * bf[8] - bf[7] * bf[5]) - bf[1] * (bf[3] * bf[8] - bf[6] * bf[5]) +
+            bf[2] * (bf[3] * bf[7] - bf[6] * bf[4]);
+  v = fabsf(v);
+  float vi = 1.f / v;
+  rf[0] = (bf[4] * bf[8] - bf[7] * bf[5]) * vi;
+  rf[4] = (bf[0] * bf[8] - bf[6] * bf[2]) * vi;
+  rf[8] = (bf[0] * bf[4] - bf[3] * bf[1]) * vi;
+  rf[1] = (-bf[3] * bf[8] + bf[6] * bf[5]) * vi;
+  rf[2] = (bf[3] * bf[7] - bf[6] * bf[4]) * vi;
+  rf[3] = (-bf[1] * bf[8] + bf[7] * bf[2]) * vi;
+  rf[5] = (-bf[0] * bf[7] + bf[6] * bf[1]) * vi;
+  rf[6] = (bf[1] * bf[5] - bf[4] * bf[2]) * vi;
+  rf[7] = (-bf[0] * bf[5] + bf[3] * bf[2]) * vi;
+  for (int k = 0; k < 9; ++k) {
+    r.rec[k] = rf[k];
+    r.box[k] = bf[k];
+  }
+  k_normalize<float><<<ceil_div(natom, 256), 256, 0, as_stream(stream)>>>(coord, natom, r);
+  DPB_CHECK_LAUNCH("normalize_coord");
+  return DPB_OK;
+}
+
+long long dpb_copy_coord_scratch_bytes(int nloc, float rcut, const double* boxt) {
+  return copy_coord_scratch_bytes(nloc, rcut, boxt);
+}
+
+int dpb_copy_coord_f64(double* out_c, int* out_t, int* mapping, int* nall,
+                       void* scratch, long long scratch_bytes,
+                       const double* in_c, const int* in_t, int nloc,
+                       int mem_nall, float rcut, const double* boxt,
+                       dpb_stream_t stream) {
+  return copy_coord_sync<double>(out_c, out_t, mapping, nall, scratch,
+                                 scratch_bytes, in_c, in_t, nloc, mem_nall,
+                                 rcut, boxt, as_stream(stream));
+}
+
+int dpb_copy_coord_f32(float* out_c, int* out_t, int* mapping, int* nall,
+                       void* scratch, long long scratch_bytes,
+                       const float* in_c, const int* in_t, int nloc,
+                       int mem_nall, float rcut, const float* boxt,
+                       dpb_stream_t stream) {
+  return copy_coord_sync<float>(out_c, out_t, mapping, nall, scratch,
+                                scratch_bytes, in_c, in_t, nloc, mem_nall,
+                                rcut, boxt, as_stream(stream));
+}
+
+long long dpb_cell_grid_bytes(int nall) { return grid_bytes(nall); }
+
+int dpb_cell_grid_build_f64(void* grid, long long grid_bytes_, const double* coord,
+                            int nall, float rcut, dpb_stream_t stream) {
+  return grid_build<double>(grid, grid_bytes_, coord, nall, nullptr, rcut,
+                            as_stream(stream));
+}
+
+int dpb_cell_grid_build_f32(void* grid, long long grid_bytes_, const float* coord,
+                            int nall, float rcut, dpb_stream_t stream) {
+  return grid_build<float>(grid, grid_bytes_, coord, nall, nullptr, rcut,
+                           as_stream(stream));
+}
+
+}  // extern "C"

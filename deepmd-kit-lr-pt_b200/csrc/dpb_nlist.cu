@@ -1,0 +1,575 @@
+// Neighbor lists and the smooth environment matrix (se_e2_a).
+//
+// One warp owns one center atom. Candidates (from the cell grid, or from an
+// input list) are filtered with the reference's exact tests, packed into
+// 64-bit keys (type, float r^2 bits, index) in shared memory and ranked in
+// place; the rank gives the sel slot. This reproduces format_nlist_i_cpu
+// (source/lib/src/fmt_nlist.cc:98-143) bit for bit: the reference GPU path
+// (source/lib/src/gpu/prod_env_mat.cu:86-219) instead sorts on a distance
+// truncated to 2^-26 A with a per-atom CUB radix sort over a global key
+// buffer and traps on key overflow; here there is no global scratch and an
+// overflow sets a status bit.
+#include "dpb_common.cuh"
+#include "dpb_internal.cuh"
+
+namespace dpb {
+
+constexpr int MAXT = 32;    // neighbor types supported (sec has <= 33 entries)
+constexpr int NMAX = 512;   // max sum(sel) per atom
+constexpr int ENV_CAP = 1024;  // max in-range candidates per atom (fused path)
+
+struct SecInfo {
+  int ntypes;
+  int nnei;
+  int sec[MAXT + 1];
+};
+
+static int make_sec(SecInfo& s, const int* sec, int nsec) {
+  if (sec == nullptr || nsec < 2 || nsec - 1 > MAXT) {
+    set_error("sec must have between 2 and %d entries (got %d)", MAXT + 1, nsec);
+    return DPB_ERR_INVALID;
+  }
+  s.ntypes = nsec - 1;
+  for (int k = 0; k < nsec; ++k) {
+    s.sec[k] = sec[k];
+    if (k > 0 && sec[k] < sec[k - 1]) {
+      set_error("sec must be non-decreasing");
+      return DPB_ERR_INVALID;
+    }
+  }
+  if (sec[0] != 0) {
+    set_error("sec[0] must be 0");
+    return DPB_ERR_INVALID;
+  }
+  s.nnei = sec[nsec - 1];
+  if (s.nnei > NMAX) {
+    set_error("sum(sel)=%d exceeds the supported maximum %d", s.nnei, NMAX);
+    return DPB_ERR_INVALID;
+  }
+  return DPB_OK;
+}
+
+// spline5_switch (source/lib/include/switcher.h:60-83), same promotion rules:
+// (xx - rmin) in T, (rmax - rmin) in float.
+template <typename T>
+__device__ __forceinline__ void spline5(T& vv, T& dd, T xx, float rmin, float rmax) {
+  if (xx < (T)rmin) {
+    dd = (T)0.;
+    vv = (T)1.;
+  } else if (xx < (T)rmax) {
+    float span = rmax - rmin;
+    T uu = (xx - (T)rmin) / (T)span;
+    T du = (T)1. / (T)span;
+    vv = uu * uu * uu * ((T)-6. * uu * uu + (T)15. * uu - (T)10.) + (T)1.;
+    dd = ((T)3. * uu * uu * ((T)-6. * uu * uu + (T)15. * uu - (T)10.) +
+          uu * uu * uu * ((T)-12. * uu + (T)15.)) * du;
+  } else {
+    dd = (T)0.;
+    vv = (T)0.;
+  }
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Candidate test + key. FUSED: build_nlist's strict FP test on c_i - c_j
+// (neighbor_list.cc:896-912) and format's float test on (float)c_j -
+// (float)c_i (fmt_nlist.cc:114-127). Otherwise only the format test.
+template <typename CT, bool FUSED>
+__device__ __forceinline__ bool accept(unsigned long long& key, int j, int i,
+                                       int ti, const CT* fc, const int* ft,
+                                       const CT xi[3], const float fxi[3],
+                                       CT rc2, float rc2f, int ntypes,
+                                       int* status) {
+  int tj = ft[j];
+  if (tj < 0) return false;
+  if (FUSED) {
+    if (j == i || ti < 0) return false;
+    CT d0 = sub_rn(xi[0], fc[3 * j + 0]);
+    CT d1 = sub_rn(xi[1], fc[3 * j + 1]);
+    CT d2 = sub_rn(xi[2], fc[3 * j + 2]);
+    if (!(dot3_rn(d0, d1, d2) < rc2)) return false;
+  }
+  float e0 = sub_rn((float)fc[3 * j + 0], fxi[0]);
+  float e1 = sub_rn((float)fc[3 * j + 1], fxi[1]);
+  float e2 = sub_rn((float)fc[3 * j + 2], fxi[2]);
+  float r2 = dot3_rn(e0, e1, e2);
+  if (!(r2 <= rc2f)) return false;
+  if (tj >= 128 || j >= (1 << 24)) {
+    atomicOr(status, ST_KEY_OVERFLOW);
+    return false;
+  }
+  if (tj >= ntypes) return false;  // no sel slot exists for this type
+  key = ((unsigned long long)tj << 56) |
+        ((unsigned long long)__float_as_uint(r2) << 24) | (unsigned long long)j;
+  return true;
+}
+
+template <typename CT, typename OT, int CAP, int WARPS, bool FROM_CELLS>
+__global__ void __launch_bounds__(WARPS * 32)
+k_env(OT* __restrict__ em, OT* __restrict__ em_deriv, OT* __restrict__ rij,
+      int* __restrict__ nlist, const CT* __restrict__ coord,
+      const int* __restrict__ type, GridView g, const int* __restrict__ ilist,
+      const int* __restrict__ numneigh, int* const* __restrict__ firstneigh,
+      const OT* __restrict__ avg, const OT* __restrict__ std_, int nloc,
+      int nall, int nrows, float rcut, float rcut_smth, SecInfo sec,
+      int* status) {
+  __shared__ unsigned long long s_keys[WARPS][CAP];
+  __shared__ int s_row[WARPS][NMAX];
+  __shared__ int s_tcnt[WARPS][MAXT];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * WARPS + w;
+  if (row >= nrows) return;
+  int f, i;
+  if (FROM_CELLS) {
+    f = 0;
+    i = row;
+  } else {
+    f = row / nloc;
+    i = ilist[row];
+  }
+  const CT* fc = coord + (size_t)f * nall * 3;
+  const int* ft = type + (size_t)f * nall;
+  const int nnei = sec.nnei, ntypes = sec.ntypes;
+  const int ti = ft[i];
+  const CT xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
+  const float fxi[3] = {(float)xi[0], (float)xi[1], (float)xi[2]};
+  const float rc2f = rcut * rcut;
+  const CT rc2 = (CT)rc2f;
+  unsigned long long* keys = s_keys[w];
+  int* srow = s_row[w];
+  int* tcnt = s_tcnt[w];
+  for (int t = lane; t < MAXT; t += 32) tcnt[t] = 0;
+  for (int jj = lane; jj < nnei; jj += 32) srow[jj] = -1;
+  __syncwarp();
+
+  // ---- gather in-range candidates into shared keys
+  int count = 0;
+  auto push = [&](bool ok, unsigned long long key) {
+    unsigned b = __ballot_sync(0xffffffffu, ok);
+    if (ok) {
+      int pos = count + __popc(b & lanemask_lt());
+      if (pos < CAP) {
+        keys[pos] = key;
+        atomicAdd(&tcnt[key >> 56], 1);
+      } else {
+        atomicOr(status, ST_NLIST_CAPACITY);
+      }
+    }
+    count += __popc(b);
+  };
+  if (FROM_CELLS) {
+    const GridHeader& h = *g.h;
+    const int ci = g.cell_of[i];
+    const int cz = ci % h.dims[2], cy = (ci / h.dims[2]) % h.dims[1],
+              cx = ci / (h.dims[2] * h.dims[1]);
+    for (int dx = -1; dx <= 1; ++dx) {
+      int x = cx + dx;
+      if (x < 0 || x >= h.dims[0]) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        int y = cy + dy;
+        if (y < 0 || y >= h.dims[1]) continue;
+        for (int dz = -1; dz <= 1; ++dz) {
+          int z = cz + dz;
+          if (z < 0 || z >= h.dims[2]) continue;
+          int c = (x * h.dims[1] + y) * h.dims[2] + z;
+          int b = g.cell_start[c], e = g.cell_start[c + 1];
+          for (int base = b; base < e; base += 32) {
+            int k = base + lane;
+            unsigned long long key = 0;
+            bool ok = false;
+            if (k < e)
+              ok = accept<CT, true>(key, g.cell_atoms[k], i, ti, fc, ft, xi, fxi,
+                                    rc2, rc2f, ntypes, status);
+            push(ok, key);
+          }
+        }
+      }
+    }
+  } else {
+    const int nn = numneigh[row];
+    const int* cand = firstneigh[row];
+    for (int base = 0; base < nn; base += 32) {
+      int k = base + lane;
+      unsigned long long key = 0;
+      bool ok = false;
+      if (k < nn)
+        ok = accept<CT, false>(key, cand[k], i, ti, fc, ft, xi, fxi, rc2, rc2f,
+                               ntypes, status);
+      push(ok, key);
+    }
+  }
+  __syncwarp();
+  const int n = count < CAP ? count : CAP;
+
+  // ---- per-type start offsets (exclusive prefix over types, lane t holds t)
+  int tstart = lane < ntypes ? tcnt[lane] : 0;
+  {
+    int x = tstart;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    tstart = x - tstart;
+  }
+  // ---- rank every key (keys are unique: they contain the index)
+  for (int q = 0; q * 32 < n; ++q) {
+    int kk = q * 32 + lane;
+    unsigned long long own = kk < n ? keys[kk] : ~0ull;
+    int r = 0;
+    for (int p = 0; p < n; ++p) r += keys[p] < own ? 1 : 0;
+    int t = (int)(own >> 56) & 31;
+    int ts = __shfl_sync(0xffffffffu, tstart, t);
+    if (kk < n) {
+      int rr = r - ts;
+      int sel = sec.sec[t + 1] - sec.sec[t];
+      if (rr < sel) srow[sec.sec[t] + rr] = (int)(own & 0xFFFFFFull);
+      else atomicOr(status, ST_SEL_OVERFLOW);
+    }
+  }
+  __syncwarp();
+
+  // ---- environment matrix, one slot per lane
+  const size_t orow = (size_t)f * nloc + i;
+  const float rmin = rcut_smth, rmax = rcut;
+  const OT* av = avg + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  const OT* sd = std_ + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  for (int jj = lane; jj < nnei; jj += 32) {
+    const int j = srow[jj];
+    nlist[orow * nnei + jj] = j;
+    OT r[3] = {(OT)0., (OT)0., (OT)0.};
+    OT v[4] = {(OT)0., (OT)0., (OT)0., (OT)0.};
+    OT gd[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) gd[k] = (OT)0.;
+    if (j >= 0) {
+      for (int d = 0; d < 3; ++d) r[d] = (OT)(fc[3 * j + d] - xi[d]);
+      OT nr2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      OT inr = (OT)1. / sqrt(nr2);
+      OT nr = nr2 * inr;
+      OT inr2 = inr * inr;
+      OT inr4 = inr2 * inr2;
+      OT inr3 = inr4 * nr;
+      OT sw, dsw;
+      spline5<OT>(sw, dsw, nr, rmin, rmax);
+      v[0] = (OT)1. / nr;
+      v[1] = r[0] / nr2;
+      v[2] = r[1] / nr2;
+      v[3] = r[2] / nr2;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) gd[d] = r[d] * inr3 * sw - v[0] * dsw * r[d] * inr;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          OT base = (OT)2. * r[a] * r[d] * inr4;
+          if (a == d) base = base - inr2;
+          gd[3 + a * 3 + d] = base * sw - v[1 + a] * dsw * r[d] * inr;
+        }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] *= sw;
+    }
+    OT* e = em + (orow * nnei + jj) * 4;
+    if (ti >= 0) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) e[k] = (v[k] - av[jj * 4 + k]) / sd[jj * 4 + k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) e[k] = (OT)0.;
+    }
+    if (em_deriv) {
+      OT* ed = em_deriv + (orow * nnei + jj) * 12;
+#pragma unroll
+      for (int k = 0; k < 12; ++k) ed[k] = ti >= 0 ? gd[k] / sd[jj * 4 + k / 3] : (OT)0.;
+    }
+    if (rij) {
+      OT* rr = rij + (orow * nnei + jj) * 3;
+      rr[0] = r[0];
+      rr[1] = r[1];
+      rr[2] = r[2];
+    }
+  }
+}
+
+template <typename CT, typename OT>
+static int env_cells(OT* em, OT* em_deriv, OT* rij, int* nlist, const CT* coord,
+                     const int* type, const void* grid, const OT* avg,
+                     const OT* std_, int nloc, int nall, float rcut,
+                     float rcut_smth, const int* sec, int nsec, int* status,
+                     dpb_stream_t stream) {
+  SecInfo s;
+  int rc = make_sec(s, sec, nsec);
+  if (rc) return rc;
+  if (nloc <= 0) return DPB_OK;
+  if (grid == nullptr || status == nullptr) {
+    set_error("env_mat_a_cells: grid and status are required");
+    return DPB_ERR_INVALID;
+  }
+  GridView g = carve_grid(const_cast<void*>(grid), nall);
+  constexpr int W = 4;
+  k_env<CT, OT, ENV_CAP, W, true><<<ceil_div(nloc, W), W * 32, 0, as_stream(stream)>>>(
+      em, em_deriv, rij, nlist, coord, type, g, nullptr, nullptr, nullptr, avg,
+      std_, nloc, nall, nloc, rcut, rcut_smth, s, status);
+  DPB_CHECK_LAUNCH("env_mat_a_cells");
+  return DPB_OK;
+}
+
+template <typename T>
+static int env_inlist(T* em, T* em_deriv, T* rij, int* nlist, const T* coord,
+                      const int* type, int inum, const int* ilist,
+                      const int* numneigh, int* const* firstneigh,
+                      int max_nbor_size, const T* avg, const T* std_, int nloc,
+                      int nall, int nframes, float rcut, float rcut_smth,
+                      const int* sec, int nsec, int* status,
+                      dpb_stream_t stream) {
+  SecInfo s;
+  int rc = make_sec(s, sec, nsec);
+  if (rc) return rc;
+  if (inum != nframes * nloc) {
+    set_error("prod_env_mat_a: inum (%d) != nframes * nloc (%d)", inum, nframes * nloc);
+    return DPB_ERR_INVALID;
+  }
+  if (status == nullptr) {
+    set_error("prod_env_mat_a: a device status word is required");
+    return DPB_ERR_INVALID;
+  }
+  if (inum <= 0) return DPB_OK;
+  cudaStream_t st = as_stream(stream);
+  GridView g{};
+  if (max_nbor_size <= 1024) {
+    constexpr int W = 4;
+    k_env<T, T, 1024, W, false><<<ceil_div(inum, W), W * 32, 0, st>>>(
+        em, em_deriv, rij, nlist, coord, type, g, ilist, numneigh, firstneigh,
+        avg, std_, nloc, nall, inum, rcut, rcut_smth, s, status);
+  } else if (max_nbor_size <= 4096) {
+    k_env<T, T, 4096, 1, false><<<inum, 32, 0, st>>>(
+        em, em_deriv, rij, nlist, coord, type, g, ilist, numneigh, firstneigh,
+        avg, std_, nloc, nall, inum, rcut, rcut_smth, s, status);
+  } else {
+    set_error("prod_env_mat_a: max_nbor_size %d exceeds 4096 (GPU_MAX_NBOR_SIZE)",
+              max_nbor_size);
+    return DPB_ERR_NLIST_CAPACITY;
+  }
+  DPB_CHECK_LAUNCH("prod_env_mat_a");
+  return DPB_OK;
+}
+
+// ------------------------------------------------------------ build_nlist --
+
+constexpr int NL_CAP = 2048;
+
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_build_nlist(int* ilist, int* numneigh, int** firstneigh, int* max_size,
+              const T* c, const int* type, GridView g, int nloc, int mem_size,
+              int row0, float rcut, int* status) {
+  // build_nlist_cpu semantics (neighbor_list.cc:875-928): j != i, both types
+  // >= 0 when type is given, strict |c_i - c_j|^2 < (T)(rcut*rcut), rows in
+  // ascending j.
+  __shared__ int s_c[4][NL_CAP];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * 4 + w;
+  if (i >= nloc) return;
+  int* cand = s_c[w];
+  const T rc2 = (T)(rcut * rcut);
+  const T xi[3] = {c[3 * i], c[3 * i + 1], c[3 * i + 2]};
+  const bool ti_ok = type == nullptr || type[i] >= 0;
+  const GridHeader& h = *g.h;
+  const int ci = g.cell_of[i];
+  const int cz = ci % h.dims[2], cy = (ci / h.dims[2]) % h.dims[1],
+            cx = ci / (h.dims[2] * h.dims[1]);
+  int count = 0;
+  for (int dx = -1; dx <= 1; ++dx) {
+    int x = cx + dx;
+    if (x < 0 || x >= h.dims[0]) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      int y = cy + dy;
+      if (y < 0 || y >= h.dims[1]) continue;
+      for (int dz = -1; dz <= 1; ++dz) {
+        int z = cz + dz;
+        if (z < 0 || z >= h.dims[2]) continue;
+        int cc = (x * h.dims[1] + y) * h.dims[2] + z;
+        int b = g.cell_start[cc], e = g.cell_start[cc + 1];
+        for (int base = b; base < e; base += 32) {
+          int k = base + lane;
+          bool ok = false;
+          int j = -1;
+          if (k < e && ti_ok) {
+            j = g.cell_atoms[k];
+            if (j != i && (type == nullptr || type[j] >= 0)) {
+              T d0 = sub_rn(xi[0], c[3 * j + 0]);
+              T d1 = sub_rn(xi[1], c[3 * j + 1]);
+              T d2 = sub_rn(xi[2], c[3 * j + 2]);
+              ok = dot3_rn(d0, d1, d2) < rc2;
+            }
+          }
+          unsigned bm = __ballot_sync(0xffffffffu, ok);
+          if (ok) {
+            int pos = count + __popc(bm & lanemask_lt());
+            if (pos < NL_CAP) cand[pos] = j;
+          }
+          count += __popc(bm);
+        }
+      }
+    }
+  }
+  __syncwarp();
+  const int row = row0 + i;
+  if (lane == 0) {
+    ilist[row] = i;
+    numneigh[row] = count < mem_size ? count : mem_size;
+    atomicMax(max_size, count);
+  }
+  if (count > mem_size) atomicOr(status, ST_ROW_CAPACITY);
+  if (count > NL_CAP) atomicOr(status, ST_NLIST_CAPACITY);
+  const int n = count < NL_CAP ? count : NL_CAP;
+  int* out = firstneigh[row];
+  for (int q = 0; q * 32 < n; ++q) {
+    int kk = q * 32 + lane;
+    int own = kk < n ? cand[kk] : 0x7fffffff;
+    int r = 0;
+    for (int p = 0; p < n; ++p) r += cand[p] < own ? 1 : 0;
+    if (kk < n && r < mem_size) out[r] = own;
+  }
+}
+
+template <typename T>
+static int build_nlist(int* ilist, int* numneigh, int** firstneigh,
+                       int* max_list_size, void* scratch,
+                       long long scratch_bytes, const T* c_cpy, int nloc,
+                       int nall, int mem_size, float rcut, int nframes,
+                       const int* type, cudaStream_t st) {
+  if (nloc < 0 || nall < nloc || mem_size < 0 || nframes < 1 || !(rcut > 0.f)) {
+    set_error("build_nlist: invalid sizes (nloc=%d nall=%d mem_size=%d nframes=%d)",
+              nloc, nall, mem_size, nframes);
+    return DPB_ERR_INVALID;
+  }
+  long long need = grid_bytes(nall) + 256;
+  if (scratch == nullptr || scratch_bytes < need) {
+    set_error("build_nlist: scratch too small (%lld < %lld bytes)", scratch_bytes, need);
+    return DPB_ERR_INVALID;
+  }
+  int* dev_words = (int*)scratch;  // [0] status, [1] max size
+  void* grid = (char*)scratch + 256;
+  DPB_CUDA(cudaMemsetAsync(dev_words, 0, 2 * sizeof(int), st), "build_nlist");
+  for (int f = 0; f < nframes; ++f) {
+    const T* cf = c_cpy + (size_t)f * nall * 3;
+    const int* tf = type ? type + (size_t)f * nall : nullptr;
+    int rc = grid_build<T>(grid, scratch_bytes - 256, cf, nall, nullptr, rcut, st);
+    if (rc) return rc;
+    if (nloc > 0) {
+      GridView g = carve_grid(grid, nall);
+      k_build_nlist<T><<<ceil_div(nloc, 4), 128, 0, st>>>(
+          ilist, numneigh, firstneigh, dev_words + 1, cf, tf, g, nloc, mem_size,
+          f * nloc, rcut, dev_words);
+      DPB_CHECK_LAUNCH("build_nlist");
+    }
+  }
+  int h[2] = {0, 0};
+  DPB_CUDA(cudaMemcpyAsync(h, dev_words, 2 * sizeof(int), cudaMemcpyDeviceToHost, st),
+           "build_nlist");
+  DPB_CUDA(cudaStreamSynchronize(st), "build_nlist");
+  *max_list_size = h[1];
+  if (h[0] & (ST_ROW_CAPACITY | ST_NLIST_CAPACITY)) {
+    set_error("build_nlist: a row holds %d neighbors, more than mem_size=%d", h[1], mem_size);
+    return DPB_ERR_CAPACITY;
+  }
+  return DPB_OK;
+}
+
+}  // namespace dpb
+
+using namespace dpb;
+extern "C" {
+
+long long dpb_build_nlist_scratch_bytes(int nloc, int nall) {
+  (void)nloc;
+  return grid_bytes(nall) + 256;
+}
+
+int dpb_build_nlist_f64(int* ilist, int* numneigh, int** firstneigh,
+                        int* max_list_size, void* scratch,
+                        long long scratch_bytes, const double* c_cpy, int nloc,
+                        int nall, int mem_size, float rcut, int nframes,
+                        const int* type, dpb_stream_t stream) {
+  return build_nlist<double>(ilist, numneigh, firstneigh, max_list_size, scratch,
+                             scratch_bytes, c_cpy, nloc, nall, mem_size, rcut,
+                             nframes, type, as_stream(stream));
+}
+
+int dpb_build_nlist_f32(int* ilist, int* numneigh, int** firstneigh,
+                        int* max_list_size, void* scratch,
+                        long long scratch_bytes, const float* c_cpy, int nloc,
+                        int nall, int mem_size, float rcut, int nframes,
+                        const int* type, dpb_stream_t stream) {
+  return build_nlist<float>(ilist, numneigh, firstneigh, max_list_size, scratch,
+                            scratch_bytes, c_cpy, nloc, nall, mem_size, rcut,
+                            nframes, type, as_stream(stream));
+}
+
+int dpb_prod_env_mat_a_f64(double* em, double* em_deriv, double* rij,
+                           int* nlist, const double* coord, const int* type,
+                           int inum, const int* ilist, const int* numneigh,
+                           int* const* firstneigh, int max_nbor_size,
+                           const double* avg, const double* std_, int nloc,
+                           int nall, int nframes, float rcut, float rcut_smth,
+                           const int* sec, int nsec, int* status,
+                           dpb_stream_t stream) {
+  return env_inlist<double>(em, em_deriv, rij, nlist, coord, type, inum, ilist,
+                            numneigh, firstneigh, max_nbor_size, avg, std_,
+                            nloc, nall, nframes, rcut, rcut_smth, sec, nsec,
+                            status, stream);
+}
+
+int dpb_prod_env_mat_a_f32(float* em, float* em_deriv, float* rij, int* nlist,
+                           const float* coord, const int* type, int inum,
+                           const int* ilist, const int* numneigh,
+                           int* const* firstneigh, int max_nbor_size,
+                           const float* avg, const float* std_, int nloc,
+                           int nall, int nframes, float rcut, float rcut_smth,
+                           const int* sec, int nsec, int* status,
+                           dpb_stream_t stream) {
+  return env_inlist<float>(em, em_deriv, rij, nlist, coord, type, inum, ilist,
+                           numneigh, firstneigh, max_nbor_size, avg, std_,
+                           nloc, nall, nframes, rcut, rcut_smth, sec, nsec,
+                           status, stream);
+}
+
+int dpb_env_mat_a_cells_f64(double* em, double* em_deriv, double* rij,
+                            int* nlist, const double* coord, const int* type,
+                            const void* grid, const double* avg,
+                            const double* std_, int nloc, int nall, float rcut,
+                            float rcut_smth, const int* sec, int nsec,
+                            int* status, dpb_stream_t stream) {
+  return env_cells<double, double>(em, em_deriv, rij, nlist, coord, type, grid,
+                                   avg, std_, nloc, nall, rcut, rcut_smth, sec,
+                                   nsec, status, stream);
+}
+
+int dpb_env_mat_a_cells_f32(float* em, float* em_deriv, float* rij, int* nlist,
+                            const float* coord, const int* type,
+                            const void* grid, const float* avg,
+                            const float* std_, int nloc, int nall, float rcut,
+                            float rcut_smth, const int* sec, int nsec,
+                            int* status, dpb_stream_t stream) {
+  return env_cells<float, float>(em, em_deriv, rij, nlist, coord, type, grid,
+                                 avg, std_, nloc, nall, rcut, rcut_smth, sec,
+                                 nsec, status, stream);
+}
+
+int dpb_env_mat_a_cells_mixed(float* em, float* em_deriv, float* rij,
+                              int* nlist, const double* coord, const int* type,
+                              const void* grid, const float* avg,
+                              const float* std_, int nloc, int nall,
+                              float rcut, float rcut_smth, const int* sec,
+                              int nsec, int* status, dpb_stream_t stream) {
+  return env_cells<double, float>(em, em_deriv, rij, nlist, coord, type, grid,
+                                  avg, std_, nloc, nall, rcut, rcut_smth, sec,
+                                  nsec, status, stream);
+}
+
+}  // extern "C"

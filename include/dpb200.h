@@ -1,0 +1,246 @@
+/* dpb200: C-ABI of the B200 (sm_100a) se_e2_a energy/force/virial kernels.
+ *
+ * Plain pointers and sizes only. All array arguments are DEVICE pointers
+ * unless marked "host". Every call is asynchronous on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream) and returns a dpb_status;
+ * dpb_last_error() gives the message of the last failure on this thread.
+ * Nothing here allocates device memory: the caller passes every output and
+ * scratch buffer (sizes from the *_scratch_bytes queries), as the reference's
+ * callers do (source/lib/tests/test_env_mat_a.cc:960-964).
+ *
+ * Device-side conditions that the reference turns into a device trap
+ * (source/lib/src/gpu/prod_env_mat.cu:92-99) are written to a caller-owned
+ * device status word instead; dpb_status_check() reads it back.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * the reference project). Layouts and argument meaning follow the reference.
+ */
+#ifndef DPB200_H
+#define DPB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPB_API __attribute__((visibility("default")))
+
+typedef void* dpb_stream_t;
+
+typedef enum {
+  DPB_OK = 0,
+  /* capacity return code 1 of build_nlist_gpu / copy_coord_gpu
+   * (source/lib/include/neighbor_list.h:255-258, coord.h:44-47) */
+  DPB_ERR_CAPACITY = 1,
+  DPB_ERR_INVALID = 2,        /* std::invalid_argument / deepmd_exception */
+  DPB_ERR_CUDA = 3,           /* DPErrcheck failure (gpu_cuda.h:21-57) */
+  DPB_ERR_OOM = 4,            /* deepmd_exception_oom (errors.h:20-25) */
+  DPB_ERR_NLIST_CAPACITY = 5, /* deepmd_exception_nlist_capacity (errors.h:27-33) */
+  DPB_ERR_OVERFLOW = 6        /* sort-key overflow: the reference traps here */
+} dpb_status;
+
+DPB_API const char* dpb_last_error(void);
+DPB_API int dpb_abi_version(void);
+
+/* Reads the device status word written by the kernels of earlier calls on
+ * `stream` (synchronises the stream) and maps it to a dpb_status. */
+DPB_API int dpb_status_check(const int* status, dpb_stream_t stream);
+
+/* ---------------------------------------------------------- coordinates -- */
+
+/* normalize_coord_gpu (source/lib/include/coord.h:56-59; coord.cu:263-282).
+ * boxt: host, 9 values, rows are the box vectors. */
+DPB_API int dpb_normalize_coord_f64(double* coord, int natom,
+                                    const double* boxt, dpb_stream_t stream);
+DPB_API int dpb_normalize_coord_f32(float* coord, int natom, const float* boxt,
+                                    dpb_stream_t stream);
+
+/* copy_coord_gpu (source/lib/include/coord.h:72-85; coord.cu:352-414),
+ * producing the same extended array as copy_coord_cpu (coord.cc:29-64):
+ * locals first, then ghost images cell by cell, ascending atom index within a
+ * cell. *nall is host. Returns DPB_ERR_CAPACITY when nall > mem_nall (nall is
+ * still reported). Synchronises `stream` to read nall. */
+DPB_API long long dpb_copy_coord_scratch_bytes(int nloc, float rcut,
+                                               const double* boxt);
+DPB_API int dpb_copy_coord_f64(double* out_c, int* out_t, int* mapping,
+                               int* nall, void* scratch,
+                               long long scratch_bytes, const double* in_c,
+                               const int* in_t, int nloc, int mem_nall,
+                               float rcut, const double* boxt,
+                               dpb_stream_t stream);
+DPB_API int dpb_copy_coord_f32(float* out_c, int* out_t, int* mapping,
+                               int* nall, void* scratch,
+                               long long scratch_bytes, const float* in_c,
+                               const int* in_t, int nloc, int mem_nall,
+                               float rcut, const float* boxt,
+                               dpb_stream_t stream);
+
+/* ---------------------------------------------------------- cell grid ---- */
+
+/* Spatial hash of nall points into cells of edge >= rcut over their bounding
+ * box, built on the device (no host round trip). Used by the neighbor search
+ * below; it replaces the O(nloc*nall) pair test of build_nlist_gpu
+ * (source/lib/src/gpu/neighbor_list.cu:77-113). */
+DPB_API long long dpb_cell_grid_bytes(int nall);
+DPB_API int dpb_cell_grid_build_f64(void* grid, long long grid_bytes,
+                                    const double* coord, int nall, float rcut,
+                                    dpb_stream_t stream);
+DPB_API int dpb_cell_grid_build_f32(void* grid, long long grid_bytes,
+                                    const float* coord, int nall, float rcut,
+                                    dpb_stream_t stream);
+
+/* ------------------------------------------------------- neighbor list -- */
+
+/* build_nlist_gpu (source/lib/include/neighbor_list.h:260-270;
+ * gpu/neighbor_list.cu:197-250): every j != i with |r_i - r_j|^2 < rc^2
+ * (strict), types < 0 excluded, rows in ascending j, exactly as
+ * build_nlist_cpu (neighbor_list.cc:875-928). ilist/numneigh: device [nloc*
+ * nframes]; firstneigh: device array of device row pointers, each row holding
+ * mem_size ints. *max_list_size is host. Returns DPB_ERR_CAPACITY when a row
+ * exceeds mem_size. Synchronises `stream`. */
+DPB_API long long dpb_build_nlist_scratch_bytes(int nloc, int nall);
+DPB_API int dpb_build_nlist_f64(int* ilist, int* numneigh, int** firstneigh,
+                                int* max_list_size, void* scratch,
+                                long long scratch_bytes, const double* c_cpy,
+                                int nloc, int nall, int mem_size, float rcut,
+                                int nframes, const int* type,
+                                dpb_stream_t stream);
+DPB_API int dpb_build_nlist_f32(int* ilist, int* numneigh, int** firstneigh,
+                                int* max_list_size, void* scratch,
+                                long long scratch_bytes, const float* c_cpy,
+                                int nloc, int nall, int mem_size, float rcut,
+                                int nframes, const int* type,
+                                dpb_stream_t stream);
+
+/* ----------------------------------------------------- environment matrix -- */
+
+/* prod_env_mat_a_gpu (source/lib/include/prod_env_mat.h:97-116;
+ * gpu/prod_env_mat.cu:681-726) from an input list (ilist, numneigh,
+ * firstneigh as in build_nlist). The formatted nlist equals
+ * format_nlist_i_cpu's (source/lib/src/fmt_nlist.cc:98-143): per-type sel
+ * slots sorted by (type, float r^2, index), padding -1. em/em_deriv/rij
+ * follow env_mat_a_cpu (source/lib/src/env_mat.cc:123-209) with the
+ * per-center-type avg/std normalisation of prod_env_mat.cc:104-124.
+ * sec: host, nsec = ntypes + 1 (cumulative sel). status: device int. */
+DPB_API int dpb_prod_env_mat_a_f64(double* em, double* em_deriv, double* rij,
+                                   int* nlist, const double* coord,
+                                   const int* type, int inum, const int* ilist,
+                                   const int* numneigh, int* const* firstneigh,
+                                   int max_nbor_size, const double* avg,
+                                   const double* std_, int nloc, int nall,
+                                   int nframes, float rcut, float rcut_smth,
+                                   const int* sec, int nsec, int* status,
+                                   dpb_stream_t stream);
+DPB_API int dpb_prod_env_mat_a_f32(float* em, float* em_deriv, float* rij,
+                                   int* nlist, const float* coord,
+                                   const int* type, int inum, const int* ilist,
+                                   const int* numneigh, int* const* firstneigh,
+                                   int max_nbor_size, const float* avg,
+                                   const float* std_, int nloc, int nall,
+                                   int nframes, float rcut, float rcut_smth,
+                                   const int* sec, int nsec, int* status,
+                                   dpb_stream_t stream);
+
+/* Fused neighbor search + format + environment matrix over a cell grid (one
+ * frame): the composition build_nlist_gpu -> prod_env_mat_a_gpu in a single
+ * pass, with no intermediate list in HBM. Same outputs as
+ * dpb_prod_env_mat_a_*. The _mixed variant takes FP64 coordinates (the
+ * coordinate differences stay FP64) and writes FP32 em/em_deriv/rij.
+ * em_deriv and rij may be NULL (not written). */
+DPB_API int dpb_env_mat_a_cells_f64(double* em, double* em_deriv, double* rij,
+                                    int* nlist, const double* coord,
+                                    const int* type, const void* grid,
+                                    const double* avg, const double* std_,
+                                    int nloc, int nall, float rcut,
+                                    float rcut_smth, const int* sec, int nsec,
+                                    int* status, dpb_stream_t stream);
+DPB_API int dpb_env_mat_a_cells_f32(float* em, float* em_deriv, float* rij,
+                                    int* nlist, const float* coord,
+                                    const int* type, const void* grid,
+                                    const float* avg, const float* std_,
+                                    int nloc, int nall, float rcut,
+                                    float rcut_smth, const int* sec, int nsec,
+                                    int* status, dpb_stream_t stream);
+DPB_API int dpb_env_mat_a_cells_mixed(float* em, float* em_deriv, float* rij,
+                                      int* nlist, const double* coord,
+                                      const int* type, const void* grid,
+                                      const float* avg, const float* std_,
+                                      int nloc, int nall, float rcut,
+                                      float rcut_smth, const int* sec,
+                                      int nsec, int* status,
+                                      dpb_stream_t stream);
+
+/* ------------------------------------------------- compressed embedding -- */
+
+/* tabulate_fusion_se_a_gpu (source/lib/include/tabulate.h:175-186;
+ * gpu/tabulate.cu:1219-1264), ndescrpt = 4, se_a (two_embed = NULL), sorted
+ * padding fold on. out: [nloc, 4, M]. table: [nspline, 6*M] in the reference
+ * layout; table_info: host, 6 values. M = last_layer_size in [1, 1024]. */
+DPB_API int dpb_tabulate_fusion_se_a_f64(double* out, const double* table,
+                                         const double* table_info,
+                                         const double* em_x, const double* em,
+                                         int nloc, int nnei,
+                                         int last_layer_size,
+                                         dpb_stream_t stream);
+DPB_API int dpb_tabulate_fusion_se_a_f32(float* out, const float* table,
+                                         const float* table_info,
+                                         const float* em_x, const float* em,
+                                         int nloc, int nnei,
+                                         int last_layer_size,
+                                         dpb_stream_t stream);
+
+/* tabulate_fusion_se_a_grad_gpu (tabulate.h:188-201; tabulate.cu:1266-1315):
+ * dy_dem_x [nloc, nnei], dy_dem [nloc, nnei, 4] from dy [nloc, 4, M]. */
+DPB_API int dpb_tabulate_fusion_se_a_grad_f64(
+    double* dy_dem_x, double* dy_dem, const double* table,
+    const double* table_info, const double* em_x, const double* em,
+    const double* dy, int nloc, int nnei, int last_layer_size,
+    dpb_stream_t stream);
+DPB_API int dpb_tabulate_fusion_se_a_grad_f32(
+    float* dy_dem_x, float* dy_dem, const float* table,
+    const float* table_info, const float* em_x, const float* em,
+    const float* dy, int nloc, int nnei, int last_layer_size,
+    dpb_stream_t stream);
+
+/* tabulate_fusion_se_a_grad_grad_gpu (tabulate.h:203-217;
+ * tabulate.cu:1317-1367): dz_dy [nloc, 4, M]. */
+DPB_API int dpb_tabulate_fusion_se_a_grad_grad_f64(
+    double* dz_dy, const double* table, const double* table_info,
+    const double* em_x, const double* em, const double* dz_dy_dem_x,
+    const double* dz_dy_dem, int nloc, int nnei, int last_layer_size,
+    dpb_stream_t stream);
+DPB_API int dpb_tabulate_fusion_se_a_grad_grad_f32(
+    float* dz_dy, const float* table, const float* table_info,
+    const float* em_x, const float* em, const float* dz_dy_dem_x,
+    const float* dz_dy_dem, int nloc, int nnei, int last_layer_size,
+    dpb_stream_t stream);
+
+/* ------------------------------------------------------ force and virial -- */
+
+/* prod_force_a_gpu (source/lib/include/prod_force.h:71-79;
+ * gpu/prod_force.cu:104-138): force [nframes, nall, 3] (zeroed here). */
+DPB_API int dpb_prod_force_a_f64(double* force, const double* net_deriv,
+                                 const double* in_deriv, const int* nlist,
+                                 int nloc, int nall, int nnei, int nframes,
+                                 dpb_stream_t stream);
+DPB_API int dpb_prod_force_a_f32(float* force, const float* net_deriv,
+                                 const float* in_deriv, const int* nlist,
+                                 int nloc, int nall, int nnei, int nframes,
+                                 dpb_stream_t stream);
+
+/* prod_virial_a_gpu (source/lib/include/prod_virial.h:29-38;
+ * gpu/prod_virial.cu:106-139): virial [9], atom_virial [nall, 9]. */
+DPB_API int dpb_prod_virial_a_f64(double* virial, double* atom_virial,
+                                  const double* net_deriv,
+                                  const double* env_deriv, const double* rij,
+                                  const int* nlist, int nloc, int nall,
+                                  int nnei, dpb_stream_t stream);
+DPB_API int dpb_prod_virial_a_f32(float* virial, float* atom_virial,
+                                  const float* net_deriv,
+                                  const float* env_deriv, const float* rij,
+                                  const int* nlist, int nloc, int nall,
+                                  int nnei, dpb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DPB200_H */

@@ -1,0 +1,73 @@
+"""CPU-side checks of the C-ABI library: it loads without a GPU, exports every
+entry point include/dpb200.h declares, the ctypes argument specs agree with
+the header, and the product refuses CPU tensors instead of falling back."""
+
+import os
+import re
+import subprocess
+
+import pytest
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "dpb200.h")
+
+
+def _declared():
+    text = open(HEADER).read()
+    decls = {}
+    for m in re.finditer(r"DPB_API\s+[\w\s\*]+?\b(dpb_\w+)\s*\(([^;]*?)\)\s*;", text, re.S):
+        args = [a.strip() for a in m.group(2).split(",") if a.strip() and a.strip() != "void"]
+        decls[m.group(1)] = args
+    return decls
+
+
+def test_header_declares_entry_points():
+    d = _declared()
+    assert "dpb_tabulate_fusion_se_a_f32" in d and "dpb_prod_force_a_f64" in d
+    assert len(d) >= 29
+
+
+def test_library_exports_every_declared_symbol(dpb):
+    lib = dpb._capi.LIB_PATH
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
+    missing = sorted(set(_declared()) - exported)
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_ctypes_specs_match_header(dpb):
+    d = _declared()
+    from deepmd_kit_lr_pt_b200 import _capi
+
+    for name, spec in _capi._FUNCS.items():
+        assert name in d, name
+        assert len(spec) == len(d[name]), f"{name}: spec {len(spec)} args, header {len(d[name])}"
+        for kind, arg in zip(spec, d[name]):
+            if kind == "p":
+                assert "*" in arg or "dpb_stream_t" in arg, (name, arg)
+            elif kind == "i":
+                assert arg.startswith("int ") and "*" not in arg, (name, arg)
+            elif kind == "f":
+                assert arg.startswith("float ") and "*" not in arg, (name, arg)
+            elif kind == "L":
+                assert arg.startswith("long long"), (name, arg)
+
+
+def test_library_loads_and_reports_version(dpb):
+    lib = dpb._capi.lib()
+    assert lib.dpb_abi_version() == 1
+    # size queries run on the host without a device
+    assert dpb._capi.lib().dpb_cell_grid_bytes(1000) > 1000 * 8
+
+
+def test_cpu_tensors_are_refused(dpb):
+    table = torch.zeros((4, 48), dtype=torch.float64)
+    info = torch.tensor([0, 0.2, 0.4, 0.01, 0.1, -1], dtype=torch.float64)
+    with pytest.raises(Exception, match="CPU"):
+        torch.ops.deepmd.tabulate_fusion_se_a(table, info, torch.zeros((4, 4), dtype=torch.float64),
+                                              torch.zeros((4, 4, 4), dtype=torch.float64), 8)
+    with pytest.raises(dpb._capi.DPBInvalidArgument):
+        dpb.ops.prod_force_a(torch.zeros((1, 4)), torch.zeros((1, 12)),
+                             torch.zeros((1, 1), dtype=torch.int32), 1, 1)
