@@ -21,6 +21,7 @@ enum : int {
   ST_SEL_OVERFLOW = 1 << 2,    // more neighbors of a type than sel (dropped)
   ST_ROW_CAPACITY = 1 << 3,    // build_nlist row longer than mem_size
   ST_CELL_RANGE = 1 << 4,      // ghost/cell index outside the cell grid
+  ST_TYPE_RANGE = 1 << 5,      // center type >= ntypes (no avg/std row)
 };
 
 void set_error(const char* fmt, ...);

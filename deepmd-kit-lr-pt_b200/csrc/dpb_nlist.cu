@@ -134,7 +134,11 @@ k_env(OT* __restrict__ em, OT* __restrict__ em_deriv, OT* __restrict__ rij,
   const CT* fc = coord + (size_t)f * nall * 3;
   const int* ft = type + (size_t)f * nall;
   const int nnei = sec.nnei, ntypes = sec.ntypes;
-  const int ti = ft[i];
+  int ti = ft[i];
+  if (ti >= ntypes) {  // no avg/std row exists for this center type
+    atomicOr(status, ST_TYPE_RANGE);
+    ti = -1;
+  }
   const CT xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
   const float fxi[3] = {(float)xi[0], (float)xi[1], (float)xi[2]};
   const float rc2f = rcut * rcut;

@@ -290,6 +290,26 @@ def _info_host(table_info: torch.Tensor, dtype) -> np.ndarray:
     return np.ascontiguousarray(a.astype(np.float64 if dtype == torch.float64 else np.float32))
 
 
+def table_rows_needed(info: np.ndarray) -> int:
+    """Rows locate_xx can address (tabulate.cc:21-30,45-73): the kernels read up
+    to row first + int((nextafter(max, lower) - upper) / stride1)."""
+    lower, upper, mx, s0, s1 = (info[k] for k in range(5))
+    first = int((upper - lower) / s0)
+    if info.dtype == np.float32:
+        bxx = np.nextafter(np.float32(mx), np.float32(lower))
+    else:
+        bxx = np.nextafter(mx, lower)
+    return first + int((bxx - upper) / s1) + 1
+
+
+def _check_table_size(table: torch.Tensor, info: np.ndarray, M: int) -> None:
+    need = table_rows_needed(info) * 6 * M
+    if table.numel() < need:
+        raise _capi.DPBInvalidArgument(
+            f"DeePMD-kit Error: the table holds {table.numel()} values but table_info "
+            f"addresses {need} (= rows x 6 x last_layer_size)")
+
+
 def _tab_fwd_impl(table, table_info, em_x, em, last_layer_size):
     _check_tab(table, table_info, [("em_x", em_x), ("em", em)], "tabulate_fusion_se_a")
     if table.dim() != 2:
@@ -309,6 +329,8 @@ def _tab_fwd_impl(table, table_info, em_x, em, last_layer_size):
     nloc, nnei = em.size(0), em.size(1)
     out = torch.empty((nloc, 4, M), dtype=table.dtype, device=table.device)
     info = _info_host(table_info, table.dtype)
+    if nnei > 0:
+        _check_table_size(table, info, M)
     call(f"dpb_tabulate_fusion_se_a_{sfx}", ptr(out), ptr(table.contiguous()), info.ctypes.data,
          ptr(em_x.contiguous()), ptr(em.contiguous()), nloc, nnei, M, _stream())
     return [out]
@@ -323,6 +345,8 @@ def _tab_grad_impl(table, table_info, em_x, em, dy, descriptor):
     dx = torch.zeros_like(em_x)
     de = torch.zeros_like(em)
     info = _info_host(table_info, table.dtype)
+    if nnei > 0:
+        _check_table_size(table, info, M)
     call(f"dpb_tabulate_fusion_se_a_grad_{sfx}", ptr(dx), ptr(de), ptr(table.contiguous()),
          info.ctypes.data, ptr(em_x.contiguous()), ptr(em.contiguous()), ptr(dy.contiguous()),
          nloc, nnei, M, _stream())
@@ -338,6 +362,8 @@ def _tab_grad_grad_impl(table, table_info, em_x, em, dz_dy_dem_x, dz_dy_dem, des
     M = descriptor.size(-1)
     out = torch.empty_like(descriptor)
     info = _info_host(table_info, table.dtype)
+    if nnei > 0:
+        _check_table_size(table, info, M)
     call(f"dpb_tabulate_fusion_se_a_grad_grad_{sfx}", ptr(out), ptr(table.contiguous()),
          info.ctypes.data, ptr(em_x.contiguous()), ptr(em.contiguous()),
          ptr(dz_dy_dem_x.contiguous()), ptr(dz_dy_dem.contiguous()), nloc, nnei, M, _stream())

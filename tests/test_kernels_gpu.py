@@ -262,9 +262,10 @@ def test_tabulate_golden_cc(dpb, ref_fixtures):
 
 def _rand_tab_case(rng, nloc, nnei, M, pad, dtype):
     """Random table/em with sorted padding tails and some extrapolated x."""
-    nspline = 60
+    info = np.array([-1.0, 2.0, 4.0, 0.05, 0.2, -1.0])
+    first = int((info[1] - info[0]) / info[3])
+    nspline = first + int((np.nextafter(info[2], info[0]) - info[1]) / info[4]) + 1
     table = rng.normal(size=(nspline, 6 * M)) * 0.3
-    info = np.array([-1.0, 2.0, 4.0, 0.05, 0.2, -1.0])  # 60 rows, high idx 59
     em = rng.normal(size=(nloc, nnei, 4))
     em_x = rng.uniform(-1.5, 5.0, size=(nloc, nnei))  # below lower / above max too
     for i in range(nloc):
