@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""se_e2_a energy/force/virial throughput on B200: microseconds per step per atom.
+
+Workload: 12,288-atom water (4096 H2O in a 49.67 A box, 16^3 molecules on a
+3.104 A grid with +-0.3 A jitter and random rigid rotations), seeded synthetic
+data; model rcut 6.0 / rcut_smth 0.5, sel [46, 92], embedding [25, 50, 100],
+axis 16, fitting [240, 240, 240], seeded random weights, statistics from the
+frame, the FP64 quintic table (stride 0.01 / 0.1, 5x extrapolation).
+
+One step = one full evaluation from coordinates: wrap, ghost copy, cell grid,
+neighbor search + format + env matrix, compressed embedding + descriptor,
+fitting net forward and backward, descriptor backward, force and virial.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours:      the compressed FP32 path (FP64 coordinate differences and sums),
+           replayed as a CUDA graph; device time per step with the L2 flushed
+           between steps; e2e through SeAEvaluator.compute() with pinned host
+           buffers (H2D coordinates, D2H energy/force/virial) in the timed
+           region. The FP64 plain path, per-stage times and errors are
+           reported beside it.
+reference: the reference's own CPU implementation (deepmd:: *_cpu functions
+           compiled from the reference sources, FP64, OpenMP where the
+           reference has it, the fitting net in FP64 torch on all host cores)
+           on bounded samples of the same workload (a subset of center atoms
+           per step; per-atom cost does not depend on which atoms).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "us/step/atom, se_e2_a water: mixed-precision vs FP64 plain on same B200"
+UNIT = "us/step/atom"
+N_SIDE = 16          # 16^3 molecules = 12,288 atoms
+PARAM_SEED = 1
+CPU_SAMPLE_ATOMS = 1024
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _load():
+    import importlib
+
+    import __graft_entry__
+
+    __graft_entry__.load_package()
+    return (importlib.import_module("deepmd_kit_lr_pt_b200.model"),
+            importlib.import_module("deepmd_kit_lr_pt_b200.workload"),
+            importlib.import_module("deepmd_kit_lr_pt_b200.table"))
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------- CPU reference --
+class CpuReference:
+    """The reference CPU path (oracle/_ref: deepmd:: *_cpu compiled from the
+    reference sources; the restatement where that library is absent)."""
+
+    def __init__(self, params, coord, atype, box):
+        import torch
+
+        from oracle import oracle
+
+        self.lib = oracle.ref()
+        self.kind = "reference"
+        if self.lib is None:
+            self.lib, self.kind = oracle.port(), "port"
+        self.p, self.coord, self.atype, self.box = params, coord, atype, box
+        self.threads = os.cpu_count() or 1
+        torch.set_num_threads(self.threads)
+        self.fit = []
+        for f in params.fit:
+            self.fit.append(([(torch.tensor(W), torch.tensor(b),
+                               None if d is None else torch.tensor(d)) for W, b, d in f["layers"]],
+                             (torch.tensor(f["out"][0]), torch.tensor(f["out"][1]))))
+
+    def step(self, sample: int):
+        """One FP64 evaluation of the first `sample` atoms as centers (all
+        geometry of the full frame); returns the wall time in seconds."""
+        import torch
+
+        p, lib, cfg = self.p, self.lib, self.p.cfg
+        M = cfg.neuron[-1]
+        t0 = time.perf_counter()
+        cn = lib.normalize_coord(self.coord.reshape(-1), self.box).reshape(-1, 3)
+        c, t, mapping = lib.copy_coord(cn, self.atype, cfg.rcut, self.box)
+        nall = c.shape[0]
+        S = sample
+        ret, il, nn, rb, _ = lib.build_nlist(c, S, cfg.rcut, atype=t, mem_size=512)
+        em, emd, rij, nlist = lib.prod_env_mat_a(c, t, il, nn, rb, p.davg, p.dstd, S,
+                                                 cfg.rcut, cfg.rcut_smth, cfg.sec)
+        nnei = cfg.nnei
+        emv = em.reshape(S, nnei, 4)
+        xyz = np.zeros((S, 4, M))
+        blocks = []
+        for ty in range(cfg.ntypes):
+            a, b = int(cfg.sec[ty]), int(cfg.sec[ty + 1])
+            e = np.ascontiguousarray(emv[:, a:b, :])
+            ex = np.ascontiguousarray(e[:, :, 0])
+            table, info = p.tables[ty]
+            xyz += lib.tabulate(table, info, ex, e, M)
+            blocks.append((a, b, e, ex, table, info))
+        xt = torch.from_numpy(xyz / nnei).requires_grad_(True)
+        D = (xt.transpose(1, 2) @ xt[:, :, :cfg.axis_neuron]).reshape(S, -1)
+        at = self.atype[:S]
+        E = torch.zeros((), dtype=torch.float64)
+        for ty in range(cfg.ntypes):
+            idx = torch.from_numpy(np.nonzero(at == ty)[0])
+            if idx.numel() == 0:
+                continue
+            layers, (Wo, bo) = self.fit[ty]
+            h = D[idx]
+            for W, b, d in layers:
+                y = torch.tanh(torch.addmm(b, h, W))
+                h = h + d * y if d is not None else y
+            E = E + torch.addmm(bo, h, Wo).sum()
+        (dxyz,) = torch.autograd.grad(E, xt)
+        dy = np.ascontiguousarray(dxyz.numpy() / nnei)
+        nd = np.zeros((S, nnei, 4))
+        for a, b, e, ex, table, info in blocks:
+            dx, de = lib.tabulate_grad(table, info, ex, e, dy, M)
+            nd[:, a:b, :] = de
+            nd[:, a:b, 0] += dx
+        nd = nd.reshape(S, nnei * 4)
+        force = lib.prod_force_a(nd, emd, nlist, S, nall)
+        virial, _ = lib.prod_virial_a(nd, emd, rij, nlist, S, nall)
+        del force, virial
+        return time.perf_counter() - t0
+
+
+def _setup_frame(mdl, wl, tab, rank: int, device):
+    cfg = mdl.SeAConfig()
+    coord, atype, box = wl.water_frame(N_SIDE, seed=100 + rank)
+    params = mdl.init_params(cfg, seed=PARAM_SEED)
+    mdl.prepare(params, coord, atype, box, device=device)
+    return cfg, params, coord, atype, box
+
+
+# ---------------------------------------------------------------- arms -------
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    mdl, wl, tab = _load()
+    cfg = mdl.SeAConfig()
+    coord, atype, box = wl.water_frame(N_SIDE, seed=100)
+    params = mdl.init_params(cfg, seed=PARAM_SEED)
+    # statistics and tables on the CPU with the reference library
+    from oracle import model_ref, oracle
+
+    lib = oracle.ref() or oracle.port()
+    params.davg, params.dstd, mind = model_ref.env_stats(lib, cfg, coord, atype, box)
+    params.tables = tab.build_tables(params.emb, params.davg, params.dstd, cfg.sel, mind,
+                                     cfg.rcut_smth, cfg.rcut)
+    ref = CpuReference(params, coord, atype, box)
+    S = CPU_SAMPLE_ATOMS
+    for _ in range(args.warmup):
+        ref.step(S)
+    ts = [ref.step(S) for _ in range(args.steps)]
+    us = float(np.mean(ts)) * 1e6 / S
+    line = {
+        "impl": "reference", "metric": METRIC, "value": us, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": us * atype.size / 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"water {atype.size} atoms ({atype.size // 3} H2O, "
+                               f"{box[0]:.2f} A box), se_e2_a compressed E/F/V, reference CPU path",
+                   "nloc": int(atype.size), "sel": list(cfg.sel)},
+        "cpu_baseline": {"value": us, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
+                         "sample": f"{S} of {atype.size} center atoms per step, full-frame "
+                                   "geometry; deepmd:: CPU lib compiled from the reference "
+                                   "sources + FP64 torch fitting"},
+        "e2e": {"value": us, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    import torch.distributed as dist
+
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    mdl, wl, tab = _load()
+    cfg, params, coord, atype, box = _setup_frame(mdl, wl, tab, rank, device)
+    nloc = atype.size
+    ev = mdl.SeAEvaluator(params, atype, box, mode="compressed", device=device)
+    ev.compute(coord)
+    nall = ev.check()
+    ev.capture()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed_steps(evl, k):
+        ts = []
+        for _ in range(k):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            evl.replay()
+            b.record()
+            ts.append((a, b))
+        torch.cuda.synchronize()
+        return [x.elapsed_time(y) for x, y in ts]
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timed region (CUDA graph replay, L2 flushed between)
+    for _ in range(args.warmup):
+        ev.replay()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ms = timed_steps(ev, args.steps)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms_step = max_over_ranks(float(np.sum(ms)) / args.steps)
+    value = ms_step * 1e3 / (nloc * world)
+
+    # ---- end to end through the public call: pinned host in, pinned host out
+    host_c = torch.tensor(coord, dtype=torch.float64).pin_memory()
+    host_out = torch.empty(1 + 3 * nloc + 9, dtype=torch.float64).pin_memory()
+    for _ in range(args.warmup):
+        ev.compute(host_c, out=host_out)
+    barrier()
+    e2e = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev.compute(host_c, out=host_out)
+        e2e.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks(float(np.mean(e2e)) * 1e3)
+    ev.check()
+
+    # ---- per-stage device times (eager step, same inputs) for the roofline
+    stages = {}
+    for _ in range(max(3, min(args.steps, 10))):
+        flush.zero_()
+        ev.step(timers=stages)
+    torch.cuda.synchronize()
+    stage_ms = {k: float(np.mean([a.elapsed_time(b) for a, b in v[1:]])) for k, v in stages.items()}
+
+    # kernel launches per step (CUPTI, one eager step)
+    launches_per_step = None
+    try:
+        from torch.profiler import ProfilerActivity, profile
+
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            ev.step()
+            torch.cuda.synchronize()
+        names = [e.name for e in prof.events() if e.device_type.name == "CUDA"]
+        launches_per_step = sum(1 for n in names if "dpb" in n)
+    except Exception:  # profiler unavailable: count stays unknown
+        launches_per_step = None
+
+    # ---- FP64 plain path on the same frame, and the accuracy of both
+    plain = mdl.SeAEvaluator(params, atype, box, mode="plain", device=device)
+    Ep, Fp, Vp = plain.compute(coord)
+    plain.check()
+    plain.capture()
+    for _ in range(2):
+        plain.replay()
+    kp = max(3, min(args.steps, 10))
+    ms_plain = max_over_ranks(float(np.mean(timed_steps(plain, kp))))
+    Ec, Fc, Vc = ev.compute(coord)
+    acc = {"vs": "FP64 plain GPU path (matches the reference PyTorch model to 1e-10 in tests)",
+           "energy_err_ev_per_atom": abs(Ec - Ep) / nloc,
+           "force_rmse_ev_per_a": float(np.sqrt(np.mean((Fc - Fp) ** 2))),
+           "force_max_abs_err": float(np.abs(Fc - Fp).max()),
+           "virial_max_abs_err": float(np.abs(Vc - Vp).max()),
+           "energy": Ep, "force_rms": float(np.sqrt(np.mean(Fp ** 2)))}
+
+    # ---- roofline of the dominant kernel stage
+    per_atom_bytes = {  # algorithmic HBM bytes per atom (FP32, nnei=138, M=100)
+        "env_mat": 138 * (4 + 12 + 3) * 4 + 138 * 4,
+        "descriptor_fwd": 138 * 4 * 4 + 4 * 100 * 4 + 1600 * 4,
+        "descriptor_bwd": 1600 * 4 + 4 * 100 * 4 + 2 * 138 * 4 * 4,
+        "force_virial": 138 * (4 + 12 + 3) * 4 + 138 * 4,
+    }
+    ours = {k: v for k, v in stage_ms.items() if k in per_atom_bytes}
+    dom = max(ours, key=ours.get)
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        with open(pk_path) as f:
+            peaks = json.load(f)
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = per_atom_bytes[dom] * nloc / (ours[dom] * 1e-3) / 1e9
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "algorithmic_bytes_per_atom": per_atom_bytes[dom],
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    # ---- CPU baseline: the reference CPU path on a bounded sample (rank 0, N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref = CpuReference(params, coord, atype, box)
+        ref.step(CPU_SAMPLE_ATOMS)
+        ts = [ref.step(CPU_SAMPLE_ATOMS) for _ in range(3)]
+        us_cpu = float(np.mean(ts)) * 1e6 / CPU_SAMPLE_ATOMS
+        cpu = {"value": us_cpu, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
+               "sample": f"{CPU_SAMPLE_ATOMS} of {nloc} center atoms, 3 steps, full-frame "
+                         "geometry; FP64"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"water {nloc} atoms per GPU ({nloc // 3} H2O, "
+                                   f"{box[0]:.2f} A box), se_e2_a compressed E/F/V",
+                       "nloc": nloc, "nall": nall, "sel": list(cfg.sel),
+                       "embedding": list(cfg.neuron), "fitting": list(cfg.fitting),
+                       "precision": "FP32 table/contraction/fitting, FP64 coordinate "
+                                    "differences and energy/force/virial sums",
+                       "l2": "256 MiB buffer written between timed steps",
+                       "graph": "one CUDA graph per step"},
+            "e2e": {"value": e2e_ms * 1e3 / (nloc * world), "unit": UNIT,
+                    "h2d_bytes_per_step": nloc * 3 * 8,
+                    "d2h_bytes_per_step": (1 + 3 * nloc + 9) * 8},
+            "gpu_launches": None if launches_per_step is None else launches_per_step * args.steps,
+            "clocks": clk,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "plain_fp64": {"ms_per_step": ms_plain, "value": ms_plain * 1e3 / nloc,
+                           "unit": UNIT, "speedup_of_compressed": ms_plain / ms_step},
+            "stages_ms": stage_ms,
+            "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    del plain, ev
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

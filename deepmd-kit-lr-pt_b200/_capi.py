@@ -83,6 +83,12 @@ _FUNCS = {
     "dpb_prod_force_a_f32": "ppppiiiip",
     "dpb_prod_virial_a_f64": "pppppp" "iiip",
     "dpb_prod_virial_a_f32": "pppppp" "iiip",
+    "dpb_copy_coord_async_f64": "ppppp" "L" "ppiifpp",
+    "dpb_cell_grid_build_async_f64": "pLpipfp",
+    "dpb_se_a_descriptor_fwd_f32": "pppp" "pp" "pi" "iiip",
+    "dpb_se_a_descriptor_bwd_f32": "ppppp" "pp" "pi" "iiip",
+    "dpb_force_virial_a_f32": "pppppp" "pp" "iiiip",
+    "dpb_force_virial_a_f64": "pppppp" "pp" "iiiip",
 }
 _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),

@@ -1,0 +1,455 @@
+"""se_e2_a energy model: parameters and the GPU energy/force/virial step.
+
+Model (deepmd/pt/model/descriptor/se_a.py, deepmd/pt/model/task/ener.py):
+  embedding  per neighbor type t (type_one_side): 1 -> n1 -> n2 -> M tanh,
+             residual when a layer doubles its width (no timestep);
+  descriptor xyz = sum_t R_t^T G_t(R_t[:, 0]) / nnei, D = xyz^T xyz[:, :axis];
+  fitting    per center type: D -> f1 -> f2 -> f3 tanh with timestep residual
+             (y = x + idt * tanh(xW + b) when widths match), then a linear
+             output plus the per-type energy bias;
+  E = sum_i e_i, F = -dE/dr (ghost contributions folded onto owners),
+  virial = sum over pairs of f_ij (x) r_ij (prod_virial.cc:55-63).
+
+Two evaluation paths share the geometry kernels:
+  compressed (FP32): FP64 coordinate differences, FP32 env matrix, the FP32
+     quintic table fused with the contraction and D, FP32 fitting, FP64
+     energy/force/virial accumulation;
+  plain (FP64): FP64 env matrix, the embedding MLP and fitting in FP64.
+Both are stream-ordered without host synchronisation inside a step, so a step
+is captured once into a CUDA graph and replayed.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _capi, ops, table as table_mod
+from ._capi import call, ptr
+
+
+@dataclass
+class SeAConfig:
+    rcut: float = 6.0
+    rcut_smth: float = 0.5
+    sel: tuple = (46, 92)
+    neuron: tuple = (25, 50, 100)
+    axis_neuron: int = 16
+    fitting: tuple = (240, 240, 240)
+
+    @property
+    def ntypes(self) -> int:
+        return len(self.sel)
+
+    @property
+    def nnei(self) -> int:
+        return int(sum(self.sel))
+
+    @property
+    def sec(self) -> np.ndarray:
+        return np.concatenate([[0], np.cumsum(self.sel)]).astype(np.int32)
+
+
+@dataclass
+class SeAParams:
+    cfg: SeAConfig
+    emb: list                 # per neighbor type: [(W, b), ...]
+    fit: list                 # per center type: [(W, b, idt|None), ...] + out (W, b)
+    bias_atom_e: np.ndarray
+    davg: np.ndarray = None   # [ntypes, nnei * 4]
+    dstd: np.ndarray = None
+    tables: list = field(default_factory=list)  # [(table f64, info f64)] per neighbor type
+
+
+def init_params(cfg: SeAConfig, seed: int = 0) -> SeAParams:
+    """Seeded random weights: W ~ N(0, 1/fan_in), b ~ N(0, 1); timestep
+    vectors ~ N(0.1, 0.001) as the reference initialises them
+    (deepmd/dpmodel/utils/network.py:135-146)."""
+    rng = np.random.default_rng(seed)
+
+    def layer(n_in, n_out, idt=False):
+        W = rng.normal(0.0, np.sqrt(1.0 / n_in), size=(n_in, n_out))
+        b = rng.normal(0.0, 1.0, size=n_out)
+        d = rng.normal(0.1, 0.001, size=n_out) if idt else None
+        return W, b, d
+
+    emb = []
+    for _ in range(cfg.ntypes):
+        widths = [1, *cfg.neuron]
+        emb.append([layer(widths[k], widths[k + 1])[:2] for k in range(len(cfg.neuron))])
+    fit = []
+    din = cfg.neuron[-1] * cfg.axis_neuron
+    for _ in range(cfg.ntypes):
+        widths = [din, *cfg.fitting]
+        layers = []
+        for k in range(len(cfg.fitting)):
+            W, b, d = layer(widths[k], widths[k + 1], idt=True)
+            layers.append((W, b, d if widths[k] == widths[k + 1] else None))
+        Wo, bo, _ = layer(cfg.fitting[-1], 1)
+        fit.append({"layers": layers, "out": (Wo, bo)})
+    return SeAParams(cfg=cfg, emb=emb, fit=fit, bias_atom_e=np.zeros(cfg.ntypes))
+
+
+# ------------------------------------------------------------ statistics --
+
+def env_stats(params: SeAParams, coord: np.ndarray, atype: np.ndarray, box: np.ndarray,
+              device="cuda:0", protection: float = 1e-2):
+    """davg/dstd from the frame's own raw environment matrix
+    (deepmd/dpmodel/utils/env_mat_stat.py:296-425, utils/env_mat_stat.py:24-101):
+    per center type, the radial column's mean and std and the angular columns'
+    std over all slots including padding; davg = [r_avg, 0, 0, 0],
+    dstd = [r_std, a_std, a_std, a_std], tiled over the slots.
+    Also returns the minimum neighbor distance of the frame."""
+    cfg = params.cfg
+    dev = torch.device(device)
+    ce, te, _ = ops.copy_coord(torch.tensor(coord, device=dev), torch.tensor(atype, device=dev),
+                               cfg.rcut, box)
+    nloc = atype.size
+    zeros = torch.zeros((cfg.ntypes, cfg.nnei * 4), dtype=torch.float64, device=dev)
+    ones = torch.ones_like(zeros)
+    em, _, rij, nlist = ops.env_mat_a_cells(ce, te, nloc, zeros, ones, cfg.rcut, cfg.rcut_smth,
+                                            cfg.sec)
+    em = em.view(nloc, cfg.nnei, 4).cpu().numpy()
+    davg = np.zeros((cfg.ntypes, cfg.nnei, 4))
+    dstd = np.ones((cfg.ntypes, cfg.nnei, 4))
+    for t in range(cfg.ntypes):
+        sel = em[atype == t]
+        if sel.size == 0:
+            dstd[t] *= 0.1
+            continue
+        r = sel[:, :, 0].reshape(-1)
+        a = sel[:, :, 1:].reshape(-1)
+
+        def std(v):
+            s = np.sqrt(max(np.mean(v * v) - np.mean(v) ** 2, 0.0))
+            return protection if abs(s) < protection else s
+
+        davg[t, :, 0] = np.mean(r)
+        dstd[t, :, 0] = std(r)
+        dstd[t, :, 1:] = std(a)
+    rr = rij.view(nloc, cfg.nnei, 3).cpu().numpy()
+    valid = nlist.cpu().numpy() >= 0
+    dist = np.linalg.norm(rr, axis=-1)[valid]
+    min_dist = float(dist.min()) if dist.size else cfg.rcut
+    return davg.reshape(cfg.ntypes, -1), dstd.reshape(cfg.ntypes, -1), min_dist
+
+
+def prepare(params: SeAParams, coord, atype, box, device="cuda:0", with_tables=True):
+    """Statistics from the frame and (optionally) the FP64 compression tables."""
+    davg, dstd, min_dist = env_stats(params, coord, atype, box, device)
+    params.davg, params.dstd = davg, dstd
+    if with_tables:
+        params.tables = table_mod.build_tables(params.emb, davg, dstd, params.cfg.sel, min_dist,
+                                               params.cfg.rcut_smth, params.cfg.rcut)
+    return params
+
+
+# --------------------------------------------------------------- fitting --
+
+class _Fitting:
+    """Per-type fitting networks on the device in one precision."""
+
+    def __init__(self, params: SeAParams, dtype, device):
+        self.layers = []
+        self.out = []
+        for f in params.fit:
+            ls = []
+            for W, b, d in f["layers"]:
+                ls.append((torch.tensor(W, dtype=dtype, device=device),
+                           torch.tensor(b, dtype=dtype, device=device),
+                           None if d is None else torch.tensor(d, dtype=dtype, device=device)))
+            self.layers.append(ls)
+            Wo, bo = f["out"]
+            self.out.append((torch.tensor(Wo, dtype=dtype, device=device),
+                             torch.tensor(bo, dtype=dtype, device=device)))
+        self.bias = torch.tensor(params.bias_atom_e, dtype=dtype, device=device)
+
+    def forward_backward(self, t: int, x: torch.Tensor):
+        """Atomic energies of type-t rows and their gradient w.r.t. the rows."""
+        acts = []
+        h = x
+        for W, b, d in self.layers[t]:
+            y = torch.tanh(torch.addmm(b, h, W))
+            acts.append((h, y, W, d))
+            h = h + d * y if d is not None else y
+        Wo, bo = self.out[t]
+        e = torch.addmm(bo, h, Wo).view(-1) + self.bias[t]
+        g = Wo.view(1, -1).expand(h.shape[0], -1)
+        for hin, y, W, d in reversed(acts):
+            gz = g * (1.0 - y * y)
+            if d is not None:
+                gz = gz * d
+                g = g + gz @ W.t()
+            else:
+                g = gz @ W.t()
+        return e, g
+
+    def forward(self, t: int, x: torch.Tensor):
+        h = x
+        for W, b, d in self.layers[t]:
+            y = torch.tanh(torch.addmm(b, h, W))
+            h = h + d * y if d is not None else y
+        Wo, bo = self.out[t]
+        return torch.addmm(bo, h, Wo).view(-1) + self.bias[t]
+
+
+# ------------------------------------------------------------ evaluators --
+
+class _Stages:
+    """Context manager factory recording CUDA events around named stages."""
+
+    def __init__(self, timers):
+        self.timers = timers
+
+    def __call__(self, name):
+        return _Stage(self.timers, name)
+
+
+class _Stage:
+    def __init__(self, timers, name):
+        self.timers, self.name = timers, name
+
+    def __enter__(self):
+        if self.timers is not None:
+            self.a = torch.cuda.Event(enable_timing=True)
+            self.a.record()
+
+    def __exit__(self, *exc):
+        if self.timers is not None:
+            b = torch.cuda.Event(enable_timing=True)
+            b.record()
+            self.timers.setdefault(self.name, []).append((self.a, b))
+        return False
+
+
+class SeAEvaluator:
+    """Energy/force/virial of one frame of fixed size, types and box.
+
+    mode "compressed": FP32 table path (needs params.tables);
+    mode "plain": FP64 embedding-MLP path.
+    Device buffers are allocated once; ``step()`` runs one evaluation on the
+    current coordinates in ``self.coord``; ``capture()`` records the step into
+    a CUDA graph that ``replay()`` re-runs."""
+
+    def __init__(self, params: SeAParams, atype: np.ndarray, box: np.ndarray,
+                 mode: str = "compressed", device="cuda:0", nall_capacity: int | None = None):
+        cfg = params.cfg
+        self.cfg, self.params, self.mode = cfg, params, mode
+        self.dev = torch.device(device)
+        self.nloc = int(atype.size)
+        self.box = np.ascontiguousarray(np.asarray(box, np.float64).reshape(9))
+        self.atype = torch.tensor(atype, dtype=torch.int32, device=self.dev)
+        self.sec = cfg.sec
+        nloc, nnei = self.nloc, cfg.nnei
+        lib = _capi.lib()
+        self.copy_bytes = int(lib.dpb_copy_coord_scratch_bytes(nloc, ctypes.c_float(cfg.rcut),
+                                                               self.box.ctypes.data))
+        if nall_capacity is None:
+            # ghosts are at most the ghost cells' share of the atoms; +25% slack
+            nall_capacity = int(self._estimate_nall() * 1.25) + 64
+        self.mem_nall = nall_capacity
+        self.grid_bytes = int(lib.dpb_cell_grid_bytes(self.mem_nall))
+        dev = self.dev
+        fdt = torch.float32 if mode == "compressed" else torch.float64
+        self.fdt = fdt
+        self.coord = torch.zeros((nloc, 3), dtype=torch.float64, device=dev)
+        self.coord_n = torch.zeros_like(self.coord)
+        self.cext = torch.zeros((self.mem_nall, 3), dtype=torch.float64, device=dev)
+        self.text = torch.zeros(self.mem_nall, dtype=torch.int32, device=dev)
+        self.mapping = torch.zeros(self.mem_nall, dtype=torch.int32, device=dev)
+        self.nall_dev = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.copy_scratch = torch.empty(self.copy_bytes, dtype=torch.uint8, device=dev)
+        self.grid = torch.empty(self.grid_bytes, dtype=torch.uint8, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.avg = torch.tensor(params.davg, dtype=fdt, device=dev)
+        self.std = torch.tensor(params.dstd, dtype=fdt, device=dev)
+        self.em = torch.empty((nloc, nnei * 4), dtype=fdt, device=dev)
+        self.emd = torch.empty((nloc, nnei * 12), dtype=fdt, device=dev)
+        self.rij = torch.empty((nloc, nnei * 3), dtype=fdt, device=dev)
+        self.nlist = torch.empty((nloc, nnei), dtype=torch.int32, device=dev)
+        self.net_deriv = torch.empty((nloc, nnei * 4), dtype=fdt, device=dev)
+        self.force = torch.zeros((nloc, 3), dtype=torch.float64, device=dev)
+        self.virial = torch.zeros(9, dtype=torch.float64, device=dev)
+        self.energy = torch.zeros(1, dtype=torch.float64, device=dev)
+        M, ax = cfg.neuron[-1], cfg.axis_neuron
+        # atoms grouped by type for the per-type fitting networks
+        order = np.argsort(atype, kind="stable")
+        row = np.empty(nloc, np.int32)
+        row[order] = np.arange(nloc, dtype=np.int32)
+        self.drow = torch.tensor(row, device=dev)
+        self.order = torch.tensor(order.astype(np.int64), device=dev)
+        counts = np.bincount(atype, minlength=cfg.ntypes)
+        self.type_ranges = [(int(s), int(s + c)) for s, c in
+                            zip(np.concatenate([[0], np.cumsum(counts)[:-1]]), counts)]
+        # the FP32 fitting must not silently drop to TF32 tensor-core math
+        torch.backends.cuda.matmul.allow_tf32 = False
+        self.fitting = _Fitting(params, fdt, dev)
+        if mode == "compressed":
+            self.xyz = torch.empty((nloc, 4, M), dtype=torch.float32, device=dev)
+            self.D = torch.empty((nloc, M * ax), dtype=torch.float32, device=dev)
+            self.dD = torch.empty_like(self.D)
+            self.tab = [torch.tensor(t, dtype=torch.float32, device=dev) for t, _ in params.tables]
+            self.tab_ptrs = (ctypes.c_void_p * len(self.tab))(*[t.data_ptr() for t in self.tab])
+            self.tab_info = np.ascontiguousarray(
+                np.concatenate([i for _, i in params.tables]).astype(np.float32))
+            for (t, info), dt in zip(params.tables, self.tab):
+                need = ops.table_rows_needed(info.astype(np.float32)) * 6 * M
+                if dt.numel() < need:
+                    raise _capi.DPBInvalidArgument("table smaller than its table_info addresses")
+        else:
+            self.emb = [[(torch.tensor(W, dtype=torch.float64, device=dev),
+                          torch.tensor(b, dtype=torch.float64, device=dev)) for W, b in net]
+                        for net in params.emb]
+        self.graph = None
+
+    def _estimate_nall(self) -> int:
+        # extended cells over local cells, times nloc (the reference's own
+        # estimate in neighbor_list.cc:774-778)
+        b = self.box
+        L = np.array([np.linalg.norm(b[0:3]), np.linalg.norm(b[3:6]), np.linalg.norm(b[6:9])])
+        nc = np.maximum(1, np.floor(L / self.cfg.rcut))
+        ng = np.floor(self.cfg.rcut / (L / nc)) + 1
+        return int(np.prod(nc + 2 * ng) / np.prod(nc) * self.nloc)
+
+    # ---- one step, no host synchronisation
+    def step(self, timers: dict | None = None):
+        """One evaluation. ``timers`` (eager runs only) collects a pair of CUDA
+        events around every stage, keyed by stage name."""
+        cfg, s = self.cfg, torch.cuda.current_stream().cuda_stream
+        nloc, nnei = self.nloc, cfg.nnei
+        tm = _Stages(timers)
+        with tm("coord"):
+            self.coord_n.copy_(self.coord)
+            call("dpb_normalize_coord_f64", ptr(self.coord_n), nloc, self.box.ctypes.data, s)
+            call("dpb_copy_coord_async_f64", ptr(self.cext), ptr(self.text), ptr(self.mapping),
+                 ptr(self.nall_dev), ptr(self.copy_scratch), self.copy_bytes, ptr(self.coord_n),
+                 ptr(self.atype), nloc, self.mem_nall, ctypes.c_float(cfg.rcut),
+                 self.box.ctypes.data, s)
+        with tm("cell_grid"):
+            call("dpb_cell_grid_build_async_f64", ptr(self.grid), self.grid_bytes,
+                 ptr(self.cext), self.mem_nall, ptr(self.nall_dev), ctypes.c_float(cfg.rcut), s)
+        env = "dpb_env_mat_a_cells_mixed" if self.mode == "compressed" else \
+            "dpb_env_mat_a_cells_f64"
+        with tm("env_mat"):
+            call(env, ptr(self.em), ptr(self.emd), ptr(self.rij), ptr(self.nlist),
+                 ptr(self.cext), ptr(self.text), ptr(self.grid), ptr(self.avg), ptr(self.std),
+                 nloc, self.mem_nall, ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth),
+                 self.sec.ctypes.data, self.sec.size, ptr(self.status), s)
+        if self.mode == "compressed":
+            self._descriptor_compressed(s, tm)
+        else:
+            with tm("descriptor_fitting_fp64"):
+                self._descriptor_plain()
+        fv = "dpb_force_virial_a_f32" if self.mode == "compressed" else "dpb_force_virial_a_f64"
+        with tm("force_virial"):
+            call(fv, ptr(self.force), ptr(self.virial), None, ptr(self.net_deriv),
+                 ptr(self.emd), ptr(self.rij), ptr(self.nlist), ptr(self.mapping), nloc, nloc,
+                 self.mem_nall, nnei, s)
+
+    def _descriptor_compressed(self, s, tm):
+        cfg = self.cfg
+        M, ax = cfg.neuron[-1], cfg.axis_neuron
+        with tm("descriptor_fwd"):
+            call("dpb_se_a_descriptor_fwd_f32", ptr(self.xyz), ptr(self.D), ptr(self.drow),
+                 ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data, self.sec.ctypes.data,
+                 self.sec.size, self.nloc, M, ax, s)
+        with tm("fitting"):
+            etot = torch.zeros((), dtype=torch.float64, device=self.dev)
+            for t, (a, b) in enumerate(self.type_ranges):
+                if b == a:
+                    continue
+                e, g = self.fitting.forward_backward(t, self.D[a:b])
+                self.dD[a:b].copy_(g)
+                etot = etot + e.to(torch.float64).sum()
+            self.energy.copy_(etot.view(1))
+        with tm("descriptor_bwd"):
+            call("dpb_se_a_descriptor_bwd_f32", ptr(self.net_deriv), ptr(self.dD),
+                 ptr(self.drow), ptr(self.xyz), ptr(self.em), self.tab_ptrs,
+                 self.tab_info.ctypes.data, self.sec.ctypes.data, self.sec.size, self.nloc, M,
+                 ax, s)
+
+    def _descriptor_plain(self):
+        cfg = self.cfg
+        nloc, nnei = self.nloc, cfg.nnei
+        with torch.enable_grad():
+            em = self.em.view(nloc, nnei, 4).detach().requires_grad_(True)
+            xyz = None
+            for t in range(cfg.ntypes):
+                a, b = int(self.sec[t]), int(self.sec[t + 1])
+                if b == a:
+                    continue
+                rr = em[:, a:b, :]
+                h = rr[:, :, :1]
+                for W, bb in self.emb[t]:
+                    y = torch.tanh(h @ W + bb)
+                    if W.shape[1] == W.shape[0]:
+                        y = y + h
+                    elif W.shape[1] == 2 * W.shape[0]:
+                        y = y + torch.cat([h, h], -1)
+                    h = y
+                gr = rr.transpose(1, 2) @ h
+                xyz = gr if xyz is None else xyz + gr
+            xyz = xyz / nnei
+            D = (xyz.transpose(1, 2) @ xyz[:, :, :cfg.axis_neuron]).reshape(nloc, -1)
+            Dp = D[self.order]  # rows grouped by type
+            etot = torch.zeros((), dtype=torch.float64, device=self.dev)
+            for t, (a, b) in enumerate(self.type_ranges):
+                if b > a:
+                    etot = etot + self.fitting.forward(t, Dp[a:b]).sum()
+            (g,) = torch.autograd.grad(etot, em)
+        self.energy.copy_(etot.detach().view(1))
+        self.net_deriv.copy_(g.reshape(nloc, nnei * 4))
+
+    # ---- graph capture / replay
+    def capture(self, warmup: int = 2):
+        s = torch.cuda.Stream(device=self.dev)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(warmup):
+                self.step()
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.step()
+        torch.cuda.synchronize()
+        return self
+
+    def replay(self):
+        if self.graph is None:
+            self.step()
+        else:
+            self.graph.replay()
+
+    def check(self):
+        """Raise if the last step overflowed a capacity (reads device words)."""
+        h = torch.stack([self.nall_dev[0], self.status[0]]).cpu().numpy()
+        if h[0] > self.mem_nall:
+            raise _capi.DPBCapacityError(
+                f"DeePMD-kit Error: nall={h[0]} exceeds the capacity {self.mem_nall}")
+        call("dpb_status_check", ptr(self.status), torch.cuda.current_stream().cuda_stream)
+        return int(h[0])
+
+    # ---- public call: host in, host out
+    def compute(self, coord, out: torch.Tensor | None = None):
+        """Energy (float), force [nloc, 3] and virial [9] of host coordinates.
+
+        ``coord`` is a host array/tensor (pinned for an asynchronous copy);
+        ``out`` an optional pinned host buffer of 1 + 3 nloc + 9 doubles."""
+        if isinstance(coord, torch.Tensor):
+            self.coord.copy_(coord.view(-1, 3), non_blocking=True)
+        else:
+            self.coord.copy_(torch.as_tensor(np.asarray(coord, np.float64).reshape(-1, 3)))
+        self.replay()
+        n = self.nloc
+        if out is None:
+            out = torch.empty(1 + 3 * n + 9, dtype=torch.float64, pin_memory=True)
+        out[0:1].copy_(self.energy, non_blocking=True)
+        out[1:1 + 3 * n].copy_(self.force.view(-1), non_blocking=True)
+        out[1 + 3 * n:].copy_(self.virial, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        o = out.numpy()
+        return float(o[0]), o[1:1 + 3 * n].reshape(-1, 3).copy(), o[1 + 3 * n:].copy()

@@ -240,6 +240,67 @@ DPB_API int dpb_prod_virial_a_f32(float* virial, float* atom_virial,
                                   const int* nlist, int nloc, int nall,
                                   int nnei, dpb_stream_t stream);
 
+/* ------------------------------------------ fused evaluation pipeline -- */
+/* These entry points have no one-to-one counterpart in the reference: they
+ * fuse the calls the reference makes in sequence for one se_e2_a energy /
+ * force / virial evaluation (source/op/tf/prod_env_mat_multi_device.cc:
+ * 2400-2600 for the geometry, deepmd/pt/model/descriptor/se_a.py:742-859 for
+ * the descriptor) and are stream-ordered with no host synchronisation, so a
+ * whole step can be captured in a CUDA graph. */
+
+/* copy_coord without the host read-back: the extended size is written to the
+ * device int *nall_dev; arrays are sized for mem_nall (ghosts beyond it are
+ * not written, and *nall_dev > mem_nall tells the caller to grow them). */
+DPB_API int dpb_copy_coord_async_f64(double* out_c, int* out_t, int* mapping,
+                                     int* nall_dev, void* scratch,
+                                     long long scratch_bytes,
+                                     const double* in_c, const int* in_t,
+                                     int nloc, int mem_nall, float rcut,
+                                     const double* boxt, dpb_stream_t stream);
+/* cell grid over the first *nall_dev of mem_nall points (grid sized by
+ * dpb_cell_grid_bytes(mem_nall); pass mem_nall as nall to the env kernels). */
+DPB_API int dpb_cell_grid_build_async_f64(void* grid, long long grid_bytes,
+                                          const double* coord, int mem_nall,
+                                          const int* nall_dev, float rcut,
+                                          dpb_stream_t stream);
+
+/* Compressed descriptor forward over all neighbor types: tables[t] (a HOST
+ * array of device pointers, one [nspline_t, 6*M] FP32 table per neighbor
+ * type), table_info: host [ntypes * 6]. em: [nloc, nnei, 4] FP32 from the env
+ * kernels. Writes xyz [nloc, 4, M] (= sum_t G_t^T R_t / nnei) and the
+ * descriptor row of atom i at descrpt + descrpt_row[i] * M * axis_neuron.
+ * M <= 128, axis_neuron <= 16, ntypes <= 8. */
+DPB_API int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt,
+                                        const int* descrpt_row, const float* em,
+                                        const float* const* tables,
+                                        const float* table_info, const int* sec,
+                                        int nsec, int nloc, int last_layer_size,
+                                        int axis_neuron, dpb_stream_t stream);
+/* Adjoint of the above: net_deriv [nloc, nnei * 4] = dE/d(em) from the
+ * descriptor gradient d_descrpt (rows at descrpt_row[i]) and xyz. */
+DPB_API int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
+                                        const int* descrpt_row, const float* xyz,
+                                        const float* em,
+                                        const float* const* tables,
+                                        const float* table_info, const int* sec,
+                                        int nsec, int nloc, int last_layer_size,
+                                        int axis_neuron, dpb_stream_t stream);
+/* prod_force_a + prod_virial_a in one pass with FP64 accumulation; ghost
+ * forces are added to their owner mapping[j] (force: [nforce, 3], nforce =
+ * nloc with a mapping, nall without). atom_virial [nall, 9] may be NULL. */
+DPB_API int dpb_force_virial_a_f32(double* force, double* virial,
+                                   double* atom_virial, const float* net_deriv,
+                                   const float* env_deriv, const float* rij,
+                                   const int* nlist, const int* mapping,
+                                   int nloc, int nforce, int nall, int nnei,
+                                   dpb_stream_t stream);
+DPB_API int dpb_force_virial_a_f64(double* force, double* virial,
+                                   double* atom_virial, const double* net_deriv,
+                                   const double* env_deriv, const double* rij,
+                                   const int* nlist, const int* mapping,
+                                   int nloc, int nforce, int nall, int nnei,
+                                   dpb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,101 @@
+"""Pins the FP64 energy/force/virial oracle (oracle/model_ref.py) against the
+reference's own PyTorch model (tests/golden/model_golden.npz), and checks the
+product's host-side model pieces that run without a GPU (seeded weights, FP64
+table builder)."""
+
+import importlib
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "model_golden.npz")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    with np.load(GOLD) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.fixture(scope="module")
+def mdl(dpb):
+    return importlib.import_module("deepmd_kit_lr_pt_b200.model")
+
+
+@pytest.fixture(scope="module")
+def tab(dpb):
+    return importlib.import_module("deepmd_kit_lr_pt_b200.table")
+
+
+def _params(mdl, tab, gold, case):
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_model_golden import weight_checksum
+
+    cfg = mdl.SeAConfig()
+    p = mdl.init_params(cfg, seed=int(gold["param_seed"]))
+    assert abs(weight_checksum(p) - float(gold["weight_checksum"])) < 1e-9
+    p.davg, p.dstd = gold[f"{case}:davg"], gold[f"{case}:dstd"]
+    p.tables = tab.build_tables(p.emb, p.davg, p.dstd, cfg.sel, float(gold[f"{case}:min_nbor_dist"]),
+                                cfg.rcut_smth, cfg.rcut)
+    return p
+
+
+@pytest.mark.parametrize("case", ["w24", "w192"])
+def test_oracle_matches_reference_model(port, mdl, tab, gold, case):
+    from oracle import model_ref
+
+    p = _params(mdl, tab, gold, case)
+    coord, atype, box = gold[f"{case}:coord"], gold[f"{case}:atype"], gold[f"{case}:box"]
+    E, F, V = model_ref.evaluate(port, p, coord, atype, box, mode="plain")
+    assert abs(E - float(gold[f"{case}:energy"])) < 1e-10
+    np.testing.assert_allclose(F, gold[f"{case}:force"], atol=1e-10)
+    np.testing.assert_allclose(V, gold[f"{case}:virial"], atol=1e-9)
+
+
+def test_oracle_stats_match_golden(port, mdl, gold):
+    from oracle import model_ref
+
+    cfg = mdl.SeAConfig()
+    davg, dstd, mind = model_ref.env_stats(port, cfg, gold["w192:coord"], gold["w192:atype"],
+                                           gold["w192:box"])
+    np.testing.assert_allclose(davg, gold["w192:davg"], atol=1e-12)
+    np.testing.assert_allclose(dstd, gold["w192:dstd"], atol=1e-12)
+    assert abs(mind - float(gold["w192:min_nbor_dist"])) < 1e-12
+
+
+def test_compressed_fp64_close_to_plain(port, mdl, tab, gold):
+    """The FP64 quintic table reproduces the MLP to ~1e-12 on this model."""
+    from oracle import model_ref
+
+    p = _params(mdl, tab, gold, "w24")
+    coord, atype, box = gold["w24:coord"], gold["w24:atype"], gold["w24:box"]
+    E, F, V = model_ref.evaluate(port, p, coord, atype, box, mode="compressed")
+    assert abs(E - float(gold["w24:energy"])) < 1e-9
+    np.testing.assert_allclose(F, gold["w24:force"], atol=1e-9)
+
+
+def test_table_reproduces_embedding(mdl, tab):
+    """Table value at random x vs the FP64 MLP (Hermite quintic interpolation)."""
+    cfg = mdl.SeAConfig()
+    p = mdl.init_params(cfg, seed=3)
+    davg = np.zeros((2, cfg.nnei * 4))
+    dstd = np.ones((2, cfg.nnei * 4))
+    davg[:, 0::4] = 0.1
+    dstd[:, 0::4] = 0.3
+    (t0, info), _ = tab.build_tables(p.emb, davg, dstd, cfg.sel, 0.95, cfg.rcut_smth, cfg.rcut)
+    x = np.random.default_rng(0).uniform(info[0], info[2] * 0.999, size=200)
+    ref, _, _ = tab.embedding_derivatives(p.emb[0], x)
+    first = int((info[1] - info[0]) / info[3])
+    for k, xv in enumerate(x):
+        if xv < info[1]:
+            idx = int((xv - info[0]) / info[3])
+            tt = xv - (idx * info[3] + info[0])
+        else:
+            idx = first + int((xv - info[1]) / info[4])
+            tt = xv - ((idx - first) * info[4] + info[1])
+        c = t0[idx].reshape(-1, 6)
+        val = c[:, 0] + (c[:, 1] + (c[:, 2] + (c[:, 3] + (c[:, 4] + c[:, 5] * tt) * tt) * tt) * tt) * tt
+        np.testing.assert_allclose(val, ref[k], atol=1e-7)
