@@ -1,0 +1,236 @@
+// deepmd:: C++ drop-in over the C-ABI (see include/deepmd_b200/deepmd_api.h).
+//
+// Same function templates and explicit float/double instantiations as the
+// reference (source/lib/src/gpu/{neighbor_list,prod_env_mat,tabulate,
+// prod_force,prod_virial}.cu), hence the same mangled symbols. Calls run on
+// the legacy default stream and end with a device synchronisation, as the
+// reference's do; failures throw the reference's exception types.
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/dpb200.h"
+#include "../../include/deepmd_b200/deepmd_api.h"
+
+namespace {
+
+void raise(int code, const char* what) {
+  if (code == DPB_OK) return;
+  std::string msg = std::string(what) + ": " + dpb_last_error();
+  if (code == DPB_ERR_OOM) throw deepmd::deepmd_exception_oom(msg);
+  if (code == DPB_ERR_NLIST_CAPACITY) throw deepmd::deepmd_exception_nlist_capacity(msg);
+  throw deepmd::deepmd_exception(msg);
+}
+
+void sync(const char* what) {
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess)
+    throw deepmd::deepmd_exception(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void se_a_only(const void* two_embed, bool is_sorted, int ndescrpt, const char* what) {
+  if (two_embed != nullptr)
+    throw deepmd::deepmd_exception(std::string(what) +
+                                   ": two_embed (se_atten) is not supported by this library");
+  if (!is_sorted)
+    throw deepmd::deepmd_exception(std::string(what) + ": only the sorted-padding mode is supported");
+  if (ndescrpt != 4)
+    throw deepmd::deepmd_exception(std::string(what) +
+                                   ": the environment basis dimension must be 4 for se_a, got " +
+                                   std::to_string(ndescrpt));
+}
+
+// overloads selecting the C-ABI precision
+int c_tab(float* o, const float* t, const float* i, const float* x, const float* e, int a, int b, int m) {
+  return dpb_tabulate_fusion_se_a_f32(o, t, i, x, e, a, b, m, nullptr);
+}
+int c_tab(double* o, const double* t, const double* i, const double* x, const double* e, int a, int b, int m) {
+  return dpb_tabulate_fusion_se_a_f64(o, t, i, x, e, a, b, m, nullptr);
+}
+int c_tab_g(float* dx, float* de, const float* t, const float* i, const float* x, const float* e,
+            const float* dy, int a, int b, int m) {
+  return dpb_tabulate_fusion_se_a_grad_f32(dx, de, t, i, x, e, dy, a, b, m, nullptr);
+}
+int c_tab_g(double* dx, double* de, const double* t, const double* i, const double* x,
+            const double* e, const double* dy, int a, int b, int m) {
+  return dpb_tabulate_fusion_se_a_grad_f64(dx, de, t, i, x, e, dy, a, b, m, nullptr);
+}
+int c_tab_gg(float* o, const float* t, const float* i, const float* x, const float* e,
+             const float* zx, const float* ze, int a, int b, int m) {
+  return dpb_tabulate_fusion_se_a_grad_grad_f32(o, t, i, x, e, zx, ze, a, b, m, nullptr);
+}
+int c_tab_gg(double* o, const double* t, const double* i, const double* x, const double* e,
+             const double* zx, const double* ze, int a, int b, int m) {
+  return dpb_tabulate_fusion_se_a_grad_grad_f64(o, t, i, x, e, zx, ze, a, b, m, nullptr);
+}
+int c_force(float* f, const float* nd, const float* ed, const int* nl, int a, int b, int c, int d) {
+  return dpb_prod_force_a_f32(f, nd, ed, nl, a, b, c, d, nullptr);
+}
+int c_force(double* f, const double* nd, const double* ed, const int* nl, int a, int b, int c, int d) {
+  return dpb_prod_force_a_f64(f, nd, ed, nl, a, b, c, d, nullptr);
+}
+int c_virial(float* v, float* av, const float* nd, const float* ed, const float* r, const int* nl,
+             int a, int b, int c) {
+  return dpb_prod_virial_a_f32(v, av, nd, ed, r, nl, a, b, c, nullptr);
+}
+int c_virial(double* v, double* av, const double* nd, const double* ed, const double* r,
+             const int* nl, int a, int b, int c) {
+  return dpb_prod_virial_a_f64(v, av, nd, ed, r, nl, a, b, c, nullptr);
+}
+int c_env(float* em, float* ed, float* r, int* nl, const float* c, const int* t, int inum,
+          const int* il, const int* nn, int* const* fn, int mx, const float* av, const float* sd,
+          int nloc, int nall, int nf, float rc, float rs, const int* sec, int nsec, int* st) {
+  return dpb_prod_env_mat_a_f32(em, ed, r, nl, c, t, inum, il, nn, fn, mx, av, sd, nloc, nall, nf,
+                                rc, rs, sec, nsec, st, nullptr);
+}
+int c_env(double* em, double* ed, double* r, int* nl, const double* c, const int* t, int inum,
+          const int* il, const int* nn, int* const* fn, int mx, const double* av,
+          const double* sd, int nloc, int nall, int nf, float rc, float rs, const int* sec,
+          int nsec, int* st) {
+  return dpb_prod_env_mat_a_f64(em, ed, r, nl, c, t, inum, il, nn, fn, mx, av, sd, nloc, nall,
+                                nf, rc, rs, sec, nsec, st, nullptr);
+}
+int c_nlist(int* il, int* nn, int** fn, int* mx, void* s, long long sb, const float* c, int nloc,
+            int nall, int mem, float rc, int nf, const int* t) {
+  return dpb_build_nlist_f32(il, nn, fn, mx, s, sb, c, nloc, nall, mem, rc, nf, t, nullptr);
+}
+int c_nlist(int* il, int* nn, int** fn, int* mx, void* s, long long sb, const double* c, int nloc,
+            int nall, int mem, float rc, int nf, const int* t) {
+  return dpb_build_nlist_f64(il, nn, fn, mx, s, sb, c, nloc, nall, mem, rc, nf, t, nullptr);
+}
+
+}  // namespace
+
+namespace deepmd {
+
+template <typename FPTYPE>
+int build_nlist_gpu(InputNlist& nlist, int* max_list_size, int* nlist_data,
+                    const FPTYPE* c_cpy, const int& nloc, const int& nall,
+                    const int& mem_size, const float& rcut, const int& nframes,
+                    const int* type) {
+  // neighbor_list.cu:207-210: the row buffers must be able to hold nall
+  if (mem_size < nall) return 1;
+  // nlist_data: >= 2 * nframes * nloc * mem_size ints of caller scratch
+  // (neighbor_list.h:236-238); the cell grid needs far less.
+  long long have = 2LL * nframes * nloc * mem_size * (long long)sizeof(int);
+  long long need = dpb_build_nlist_scratch_bytes(nloc, nall);
+  if (have < need)
+    throw deepmd_exception("build_nlist_gpu: nlist_data is smaller than " +
+                           std::to_string(need) + " bytes");
+  nlist.inum = nframes * nloc;
+  int code = c_nlist(nlist.ilist, nlist.numneigh, nlist.firstneigh, max_list_size, nlist_data,
+                     have, c_cpy, nloc, nall, mem_size, rcut, nframes, type);
+  if (code == DPB_ERR_CAPACITY) return 1;
+  raise(code, "build_nlist_gpu");
+  sync("build_nlist_gpu");
+  return 0;
+}
+
+template <typename FPTYPE>
+void prod_env_mat_a_gpu(FPTYPE* em, FPTYPE* em_deriv, FPTYPE* rij, int* nlist,
+                        const FPTYPE* coord, const int* type,
+                        const InputNlist& gpu_inlist, int* array_int,
+                        unsigned long long* array_longlong, const int max_nbor_size,
+                        const FPTYPE* avg, const FPTYPE* std, const int nloc,
+                        const int nall, const int nframes, const float rcut,
+                        const float rcut_smth, const std::vector<int> sec,
+                        const int* f_type) {
+  (void)array_longlong;
+  if (f_type != nullptr && f_type != type)
+    throw deepmd_exception("prod_env_mat_a_gpu: a separate f_type is not supported");
+  if (cudaMemsetAsync(array_int, 0, sizeof(int), nullptr) != cudaSuccess)
+    throw deepmd_exception("prod_env_mat_a_gpu: cannot reset the status word");
+  raise(c_env(em, em_deriv, rij, nlist, coord, type, gpu_inlist.inum, gpu_inlist.ilist,
+              gpu_inlist.numneigh, gpu_inlist.firstneigh, max_nbor_size, avg, std, nloc, nall,
+              nframes, rcut, rcut_smth, sec.data(), (int)sec.size(), array_int),
+        "prod_env_mat_a_gpu");
+  raise(dpb_status_check(array_int, nullptr), "prod_env_mat_a_gpu");
+  sync("prod_env_mat_a_gpu");
+}
+
+template <typename FPTYPE>
+void tabulate_fusion_se_a_gpu(FPTYPE* out, const FPTYPE* table, const FPTYPE* table_info,
+                              const FPTYPE* em_x, const FPTYPE* em, const FPTYPE* two_embed,
+                              const int nloc, const int nnei, const int last_layer_size,
+                              const bool is_sorted, const int ndescrpt) {
+  se_a_only(two_embed, is_sorted, ndescrpt, "tabulate_fusion_se_a_gpu");
+  raise(c_tab(out, table, table_info, em_x, em, nloc, nnei, last_layer_size),
+        "tabulate_fusion_se_a_gpu");
+  sync("tabulate_fusion_se_a_gpu");
+}
+
+template <typename FPTYPE>
+void tabulate_fusion_se_a_grad_gpu(FPTYPE* dy_dem_x, FPTYPE* dy_dem, FPTYPE* dy_dtwo,
+                                   const FPTYPE* table, const FPTYPE* table_info,
+                                   const FPTYPE* em_x, const FPTYPE* em,
+                                   const FPTYPE* two_embed, const FPTYPE* dy, const int nloc,
+                                   const int nnei, const int last_layer_size,
+                                   const bool is_sorted, const int ndescrpt) {
+  (void)dy_dtwo;
+  se_a_only(two_embed, is_sorted, ndescrpt, "tabulate_fusion_se_a_grad_gpu");
+  raise(c_tab_g(dy_dem_x, dy_dem, table, table_info, em_x, em, dy, nloc, nnei, last_layer_size),
+        "tabulate_fusion_se_a_grad_gpu");
+  sync("tabulate_fusion_se_a_grad_gpu");
+}
+
+template <typename FPTYPE>
+void tabulate_fusion_se_a_grad_grad_gpu(FPTYPE* dz_dy, const FPTYPE* table,
+                                        const FPTYPE* table_info, const FPTYPE* em_x,
+                                        const FPTYPE* em, const FPTYPE* two_embed,
+                                        const FPTYPE* dz_dy_dem_x, const FPTYPE* dz_dy_dem,
+                                        const FPTYPE* dz_dy_dtwo, const int nloc,
+                                        const int nnei, const int last_layer_size,
+                                        const bool is_sorted, const int ndescrpt) {
+  (void)dz_dy_dtwo;
+  se_a_only(two_embed, is_sorted, ndescrpt, "tabulate_fusion_se_a_grad_grad_gpu");
+  raise(c_tab_gg(dz_dy, table, table_info, em_x, em, dz_dy_dem_x, dz_dy_dem, nloc, nnei,
+                 last_layer_size),
+        "tabulate_fusion_se_a_grad_grad_gpu");
+  sync("tabulate_fusion_se_a_grad_grad_gpu");
+}
+
+template <typename FPTYPE>
+void prod_force_a_gpu(FPTYPE* force, const FPTYPE* net_deriv, const FPTYPE* in_deriv,
+                      const int* nlist, const int nloc, const int nall, const int nnei,
+                      const int nframes) {
+  raise(c_force(force, net_deriv, in_deriv, nlist, nloc, nall, nnei, nframes), "prod_force_a_gpu");
+  sync("prod_force_a_gpu");
+}
+
+template <typename FPTYPE>
+void prod_virial_a_gpu(FPTYPE* virial, FPTYPE* atom_virial, const FPTYPE* net_deriv,
+                       const FPTYPE* env_deriv, const FPTYPE* rij, const int* nlist,
+                       const int nloc, const int nall, const int nnei) {
+  raise(c_virial(virial, atom_virial, net_deriv, env_deriv, rij, nlist, nloc, nall, nnei),
+        "prod_virial_a_gpu");
+  sync("prod_virial_a_gpu");
+}
+
+#define DPB_INSTANTIATE(T)                                                                   \
+  template int build_nlist_gpu<T>(InputNlist&, int*, int*, const T*, const int&, const int&, \
+                                  const int&, const float&, const int&, const int*);         \
+  template void prod_env_mat_a_gpu<T>(T*, T*, T*, int*, const T*, const int*,                \
+                                      const InputNlist&, int*, unsigned long long*, const int, \
+                                      const T*, const T*, const int, const int, const int,    \
+                                      const float, const float, const std::vector<int>,       \
+                                      const int*);                                            \
+  template void tabulate_fusion_se_a_gpu<T>(T*, const T*, const T*, const T*, const T*,      \
+                                            const T*, const int, const int, const int,       \
+                                            const bool, const int);                          \
+  template void tabulate_fusion_se_a_grad_gpu<T>(T*, T*, T*, const T*, const T*, const T*,   \
+                                                 const T*, const T*, const T*, const int,    \
+                                                 const int, const int, const bool,           \
+                                                 const int);                                 \
+  template void tabulate_fusion_se_a_grad_grad_gpu<T>(                                       \
+      T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*, const T*,    \
+      const int, const int, const int, const bool, const int);                               \
+  template void prod_force_a_gpu<T>(T*, const T*, const T*, const int*, const int,           \
+                                    const int, const int, const int);                        \
+  template void prod_virial_a_gpu<T>(T*, T*, const T*, const T*, const T*, const int*,       \
+                                     const int, const int, const int);
+
+DPB_INSTANTIATE(float)
+DPB_INSTANTIATE(double)
+
+}  // namespace deepmd

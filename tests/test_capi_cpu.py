@@ -71,3 +71,14 @@ def test_cpu_tensors_are_refused(dpb):
     with pytest.raises(dpb._capi.DPBInvalidArgument):
         dpb.ops.prod_force_a(torch.zeros((1, 4)), torch.zeros((1, 12)),
                              torch.zeros((1, 1), dtype=torch.int32), 1, 1)
+
+
+def test_cxx_dropin_exports_reference_symbols(dpb):
+    """libdpb200.so defines every deepmd:: GPU function on this path under the
+    mangled name the reference headers produce (tests/golden/ref_abi_symbols.txt)."""
+    want = open(os.path.join(ROOT, "tests", "golden", "ref_abi_symbols.txt")).read().split()
+    out = subprocess.run(["nm", "-D", "--defined-only", dpb._capi.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    have = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
+    missing = [s for s in want if s not in have]
+    assert len(want) == 14 and not missing, missing
