@@ -336,7 +336,7 @@ def test_tabulate_second_order_fd(dpb, ref_fixtures):
             d2 = flat.clone()
             d2[k] += s * eps
             a, b = first(d2.view_as(dy))
-            vals.append(float((a * zx).sum() + (b * ze).sum()))
+            vals.append(float(((a * zx).sum() + (b * ze).sum()).detach()))
         num.view(-1)[k] = (vals[0] - vals[1]) / (2 * eps)
     np.testing.assert_allclose(ana.cpu().numpy(), num.cpu().numpy(), atol=1e-6, rtol=1e-6)
 
