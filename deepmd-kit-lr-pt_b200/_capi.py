@@ -89,11 +89,13 @@ _FUNCS = {
     "dpb_se_a_descriptor_bwd_f32": "ppppp" "pp" "pi" "iiip",
     "dpb_force_virial_a_f32": "pppppp" "pp" "iiiip",
     "dpb_force_virial_a_f64": "pppppp" "pp" "iiiip",
+    "dpb_build_nlist_noalloc_f64": "ppppp" "iiif" "i" "pp",
 }
 _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),
     "dpb_cell_grid_bytes": ("i", LL),
     "dpb_build_nlist_scratch_bytes": ("ii", LL),
+    "dpb_build_nlist_noalloc_max_bytes": ("", LL),
 }
 
 _lib = None

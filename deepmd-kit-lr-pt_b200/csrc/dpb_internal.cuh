@@ -51,5 +51,10 @@ int copy_coord_async(T* out_c, int* out_t, int* mapping, int* nall_dev,
                      const int* in_t, int nloc, int mem_nall, float rcut,
                      const double* boxt, cudaStream_t st);
 long long copy_coord_scratch_bytes(int nloc, float rcut, const double* boxt);
+template <typename T>
+int build_nlist(int* ilist, int* numneigh, int** firstneigh, int* max_list_size,
+                void* scratch, long long scratch_bytes, const T* c_cpy, int nloc,
+                int nall, int mem_size, float rcut, int nframes, const int* type,
+                cudaStream_t st);
 
 }  // namespace dpb

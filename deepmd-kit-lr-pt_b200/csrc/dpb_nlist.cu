@@ -442,7 +442,7 @@ k_build_nlist(int* ilist, int* numneigh, int** firstneigh, int* max_size,
 }
 
 template <typename T>
-static int build_nlist(int* ilist, int* numneigh, int** firstneigh,
+int build_nlist(int* ilist, int* numneigh, int** firstneigh,
                        int* max_list_size, void* scratch,
                        long long scratch_bytes, const T* c_cpy, int nloc,
                        int nall, int mem_size, float rcut, int nframes,
@@ -484,6 +484,11 @@ static int build_nlist(int* ilist, int* numneigh, int** firstneigh,
   }
   return DPB_OK;
 }
+
+template int build_nlist<double>(int*, int*, int**, int*, void*, long long, const double*, int,
+                                 int, int, float, int, const int*, cudaStream_t);
+template int build_nlist<float>(int*, int*, int**, int*, void*, long long, const float*, int,
+                                int, int, float, int, const int*, cudaStream_t);
 
 }  // namespace dpb
 

@@ -301,6 +301,24 @@ DPB_API int dpb_force_virial_a_f64(double* force, double* virial,
                                    int nloc, int nforce, int nall, int nnei,
                                    dpb_stream_t stream);
 
+/* ------------------------------------------- allocation-free variant ---- */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc,
+ * e.g. an MD engine's force callback that runs inside the engine's own
+ * device-memory pool and may not allocate during a step: the same neighbor
+ * list as dpb_build_nlist_f64 (same arguments and results) without the
+ * caller scratch. Its working memory is a 4 MiB file-scope device array in
+ * the library (held by every GPU that loads it until exit), which limits nall
+ * to what fits (dpb_cell_grid_bytes(nall) + 256 <= 4 MiB, about 260k atoms);
+ * larger sizes are rejected with DPB_ERR_INVALID. The first call on a device
+ * looks up the array's device address (call it before any stream capture).
+ * All calls share the array: calls that overlap on the same GPU race. */
+DPB_API long long dpb_build_nlist_noalloc_max_bytes(void);
+DPB_API int dpb_build_nlist_noalloc_f64(int* ilist, int* numneigh,
+                                        int** firstneigh, int* max_list_size,
+                                        const double* c_cpy, int nloc, int nall,
+                                        int mem_size, float rcut, int nframes,
+                                        const int* type, dpb_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
