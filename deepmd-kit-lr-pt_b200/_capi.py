@@ -90,6 +90,8 @@ _FUNCS = {
     "dpb_force_virial_a_f32": "pppppp" "pp" "iiiip",
     "dpb_force_virial_a_f64": "pppppp" "pp" "iiiip",
     "dpb_build_nlist_noalloc_f64": "ppppp" "iiif" "i" "pp",
+    "dpb_force_virial_a_env_mixed": "pppppppp" "iiii" "ff" "p",
+    "dpb_force_virial_a_env_f64": "pppppppp" "iiii" "ff" "p",
 }
 _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),

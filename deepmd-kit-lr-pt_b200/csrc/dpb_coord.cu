@@ -254,18 +254,40 @@ __global__ void k_cc_fill(CopyScratch s, int nloc) {
   s.order[pos] = i;
 }
 
+constexpr int SORT_CAP = 256;
+
 __global__ void k_cc_sort(CopyScratch s, int ncells) {
-  // ascending atom index within each cell (build_clist pushes in index order)
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  // ascending atom index within each cell (build_clist pushes in index
+  // order): one warp per cell ranks the cell's entries in shared memory;
+  // cells larger than SORT_CAP (none at cell edges near rcut) fall back to a
+  // serial insertion sort by lane 0.
+  __shared__ int buf[4][SORT_CAP];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * 4 + w;
   if (c >= ncells) return;
-  int b = s.cnt[c], e = s.cnt[c + 1];
-  for (int a = b + 1; a < e; ++a) {
-    int v = s.order[a], q = a - 1;
-    while (q >= b && s.order[q] > v) {
-      s.order[q + 1] = s.order[q];
-      q--;
+  const int b = s.cnt[c], e = s.cnt[c + 1], n = e - b;
+  if (n <= 1) return;
+  if (n <= SORT_CAP) {
+    int* v = buf[w];
+    for (int k = lane; k < n; k += 32) v[k] = s.order[b + k];
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) {
+      const int x = v[k];
+      int r = 0;
+      for (int q = 0; q < n; ++q) r += v[q] < x ? 1 : 0;
+      s.order[b + r] = x;  // indices are distinct: ranks are a permutation
     }
-    s.order[q + 1] = v;
+    return;
+  }
+  if (lane == 0) {
+    for (int a = b + 1; a < e; ++a) {
+      int v = s.order[a], q = a - 1;
+      while (q >= b && s.order[q] > v) {
+        s.order[q + 1] = s.order[q];
+        q--;
+      }
+      s.order[q + 1] = v;
+    }
   }
 }
 
@@ -344,7 +366,7 @@ int copy_coord_async(T* out_c, int* out_t, int* mapping, int* nall_dev,
     k_cc_fill<<<ceil_div(nloc, 256), 256, 0, st>>>(s, nloc);
     DPB_CHECK_LAUNCH("copy_coord/fill");
   }
-  k_cc_sort<<<ceil_div(r.nloc_cells, 128), 128, 0, st>>>(s, r.nloc_cells);
+  k_cc_sort<<<ceil_div(r.nloc_cells, 4), 128, 0, st>>>(s, r.nloc_cells);
   DPB_CHECK_LAUNCH("copy_coord/sort");
   k_cc_copy<T><<<ceil_div((long long)r.next_cells * 32, 256), 256, 0, st>>>(
       s, out_c, out_t, mapping, in_c, in_t, nloc, mem_nall, r);
@@ -492,7 +514,7 @@ __global__ void k_grid_fill(GridView g) {
 
 long long grid_bytes(int nall) {
   int max_cells = nall > 64 ? nall : 64;
-  long long ints = (long long)(max_cells + 1) + max_cells + 2LL * nall + 64;
+  long long ints = (long long)(max_cells + 1) + max_cells + 3LL * nall + 1 + 64;
   return (long long)sizeof(GridHeader) + 256 + ints * (long long)sizeof(int);
 }
 
@@ -504,7 +526,8 @@ GridView carve_grid(void* p, int nall) {
   g.cell_start = q; q += max_cells + 1;
   g.fill = q; q += max_cells;
   g.cell_of = q; q += nall;
-  g.cell_atoms = q;
+  g.cell_atoms = q; q += nall;
+  g.redo = q;
   g.max_cells = max_cells;
   g.cap_atoms = nall;
   return g;

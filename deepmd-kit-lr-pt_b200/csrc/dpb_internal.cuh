@@ -36,6 +36,7 @@ struct GridView {
   int* fill;        // [ncells]
   int* cell_of;     // [natoms]
   int* cell_atoms;  // [natoms], atoms sorted by cell
+  int* redo;        // [natoms + 1]: count, then atoms deferred to a larger buffer
   int max_cells;
   int cap_atoms;
 };

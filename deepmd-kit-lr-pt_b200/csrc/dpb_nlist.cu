@@ -10,13 +10,13 @@
 // buffer and traps on key overflow; here there is no global scratch and an
 // overflow sets a status bit.
 #include "dpb_common.cuh"
+#include "dpb_envmath.cuh"
 #include "dpb_internal.cuh"
 
 namespace dpb {
 
 constexpr int MAXT = 32;    // neighbor types supported (sec has <= 33 entries)
 constexpr int NMAX = 512;   // max sum(sel) per atom
-constexpr int ENV_CAP = 1024;  // max in-range candidates per atom (fused path)
 
 struct SecInfo {
   int ntypes;
@@ -47,26 +47,6 @@ static int make_sec(SecInfo& s, const int* sec, int nsec) {
     return DPB_ERR_INVALID;
   }
   return DPB_OK;
-}
-
-// spline5_switch (source/lib/include/switcher.h:60-83), same promotion rules:
-// (xx - rmin) in T, (rmax - rmin) in float.
-template <typename T>
-__device__ __forceinline__ void spline5(T& vv, T& dd, T xx, float rmin, float rmax) {
-  if (xx < (T)rmin) {
-    dd = (T)0.;
-    vv = (T)1.;
-  } else if (xx < (T)rmax) {
-    float span = rmax - rmin;
-    T uu = (xx - (T)rmin) / (T)span;
-    T du = (T)1. / (T)span;
-    vv = uu * uu * uu * ((T)-6. * uu * uu + (T)15. * uu - (T)10.) + (T)1.;
-    dd = ((T)3. * uu * uu * ((T)-6. * uu * uu + (T)15. * uu - (T)10.) +
-          uu * uu * uu * ((T)-12. * uu + (T)15.)) * du;
-  } else {
-    dd = (T)0.;
-    vv = (T)0.;
-  }
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -108,44 +88,63 @@ __device__ __forceinline__ bool accept(unsigned long long& key, int j, int i,
   return true;
 }
 
-template <typename CT, typename OT, int CAP, int WARPS, bool FROM_CELLS>
-__global__ void __launch_bounds__(WARPS * 32)
-k_env(OT* __restrict__ em, OT* __restrict__ em_deriv, OT* __restrict__ rij,
-      int* __restrict__ nlist, const CT* __restrict__ coord,
-      const int* __restrict__ type, GridView g, const int* __restrict__ ilist,
-      const int* __restrict__ numneigh, int* const* __restrict__ firstneigh,
-      const OT* __restrict__ avg, const OT* __restrict__ std_, int nloc,
-      int nall, int nrows, float rcut, float rcut_smth, SecInfo sec,
-      int* status) {
-  __shared__ unsigned long long s_keys[WARPS][CAP];
-  __shared__ int s_row[WARPS][NMAX];
-  __shared__ int s_tcnt[WARPS][MAXT];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = blockIdx.x * WARPS + w;
-  if (row >= nrows) return;
+// Shared-memory workspace of one warp (one center atom).
+template <int CAP>
+struct EnvSmem {
+  unsigned long long keys[CAP];
+  int row[NMAX];
+  int tcnt[MAXT];
+};
+
+template <typename CT, typename OT>
+struct EnvIO {
+  OT* em;
+  OT* em_deriv;  // may be null
+  OT* rij;       // may be null
+  int* nlist;
+  const CT* coord;
+  const int* type;
+  GridView g;
+  const int* ilist;
+  const int* numneigh;
+  int* const* firstneigh;
+  const OT* avg;
+  const OT* std_;
+  int nloc, nall;
+  float rcut, rcut_smth;
+  int* status;
+};
+
+// One center atom. With `defer`, an atom with more in-range candidates than
+// CAP writes nothing and returns false (the caller queues it for the
+// large-buffer pass); otherwise the overflow is reported in the status word.
+template <typename CT, typename OT, int CAP, bool FROM_CELLS>
+__device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
+                        EnvSmem<CAP>& sm, bool defer) {
+  const int lane = threadIdx.x & 31;
   int f, i;
   if (FROM_CELLS) {
     f = 0;
     i = row;
   } else {
-    f = row / nloc;
-    i = ilist[row];
+    f = row / io.nloc;
+    i = io.ilist[row];
   }
-  const CT* fc = coord + (size_t)f * nall * 3;
-  const int* ft = type + (size_t)f * nall;
+  const CT* fc = io.coord + (size_t)f * io.nall * 3;
+  const int* ft = io.type + (size_t)f * io.nall;
   const int nnei = sec.nnei, ntypes = sec.ntypes;
   int ti = ft[i];
   if (ti >= ntypes) {  // no avg/std row exists for this center type
-    atomicOr(status, ST_TYPE_RANGE);
+    atomicOr(io.status, ST_TYPE_RANGE);
     ti = -1;
   }
   const CT xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
   const float fxi[3] = {(float)xi[0], (float)xi[1], (float)xi[2]};
-  const float rc2f = rcut * rcut;
+  const float rc2f = io.rcut * io.rcut;
   const CT rc2 = (CT)rc2f;
-  unsigned long long* keys = s_keys[w];
-  int* srow = s_row[w];
-  int* tcnt = s_tcnt[w];
+  unsigned long long* keys = sm.keys;
+  int* srow = sm.row;
+  int* tcnt = sm.tcnt;
   for (int t = lane; t < MAXT; t += 32) tcnt[t] = 0;
   for (int jj = lane; jj < nnei; jj += 32) srow[jj] = -1;
   __syncwarp();
@@ -159,15 +158,13 @@ k_env(OT* __restrict__ em, OT* __restrict__ em_deriv, OT* __restrict__ rij,
       if (pos < CAP) {
         keys[pos] = key;
         atomicAdd(&tcnt[key >> 56], 1);
-      } else {
-        atomicOr(status, ST_NLIST_CAPACITY);
       }
     }
     count += __popc(b);
   };
   if (FROM_CELLS) {
-    const GridHeader& h = *g.h;
-    const int ci = g.cell_of[i];
+    const GridHeader& h = *io.g.h;
+    const int ci = io.g.cell_of[i];
     const int cz = ci % h.dims[2], cy = (ci / h.dims[2]) % h.dims[1],
               cx = ci / (h.dims[2] * h.dims[1]);
     for (int dx = -1; dx <= 1; ++dx) {
@@ -180,33 +177,37 @@ k_env(OT* __restrict__ em, OT* __restrict__ em_deriv, OT* __restrict__ rij,
           int z = cz + dz;
           if (z < 0 || z >= h.dims[2]) continue;
           int c = (x * h.dims[1] + y) * h.dims[2] + z;
-          int b = g.cell_start[c], e = g.cell_start[c + 1];
+          int b = io.g.cell_start[c], e = io.g.cell_start[c + 1];
           for (int base = b; base < e; base += 32) {
             int k = base + lane;
             unsigned long long key = 0;
             bool ok = false;
             if (k < e)
-              ok = accept<CT, true>(key, g.cell_atoms[k], i, ti, fc, ft, xi, fxi,
-                                    rc2, rc2f, ntypes, status);
+              ok = accept<CT, true>(key, io.g.cell_atoms[k], i, ti, fc, ft, xi, fxi, rc2,
+                                    rc2f, ntypes, io.status);
             push(ok, key);
           }
         }
       }
     }
   } else {
-    const int nn = numneigh[row];
-    const int* cand = firstneigh[row];
+    const int nn = io.numneigh[row];
+    const int* cand = io.firstneigh[row];
     for (int base = 0; base < nn; base += 32) {
       int k = base + lane;
       unsigned long long key = 0;
       bool ok = false;
       if (k < nn)
-        ok = accept<CT, false>(key, cand[k], i, ti, fc, ft, xi, fxi, rc2, rc2f,
-                               ntypes, status);
+        ok = accept<CT, false>(key, cand[k], i, ti, fc, ft, xi, fxi, rc2, rc2f, ntypes,
+                               io.status);
       push(ok, key);
     }
   }
   __syncwarp();
+  if (count > CAP) {
+    if (defer) return false;
+    if (lane == 0) atomicOr(io.status, ST_NLIST_CAPACITY);
+  }
   const int n = count < CAP ? count : CAP;
 
   // ---- per-type start offsets (exclusive prefix over types, lane t holds t)
@@ -230,21 +231,22 @@ k_env(OT* __restrict__ em, OT* __restrict__ em_deriv, OT* __restrict__ rij,
     int ts = __shfl_sync(0xffffffffu, tstart, t);
     if (kk < n) {
       int rr = r - ts;
-      int sel = sec.sec[t + 1] - sec.sec[t];
-      if (rr < sel) srow[sec.sec[t] + rr] = (int)(own & 0xFFFFFFull);
-      else atomicOr(status, ST_SEL_OVERFLOW);
+      int selt = sec.sec[t + 1] - sec.sec[t];
+      if (rr < selt) srow[sec.sec[t] + rr] = (int)(own & 0xFFFFFFull);
+      else atomicOr(io.status, ST_SEL_OVERFLOW);
     }
   }
   __syncwarp();
 
   // ---- environment matrix, one slot per lane
-  const size_t orow = (size_t)f * nloc + i;
-  const float rmin = rcut_smth, rmax = rcut;
-  const OT* av = avg + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
-  const OT* sd = std_ + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  const size_t orow = (size_t)f * io.nloc + i;
+  const float rmin = io.rcut_smth, rmax = io.rcut;
+  const OT* av = io.avg + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  const OT* sd = io.std_ + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  const bool want_d = io.em_deriv != nullptr;
   for (int jj = lane; jj < nnei; jj += 32) {
     const int j = srow[jj];
-    nlist[orow * nnei + jj] = j;
+    io.nlist[orow * nnei + jj] = j;
     OT r[3] = {(OT)0., (OT)0., (OT)0.};
     OT v[4] = {(OT)0., (OT)0., (OT)0., (OT)0.};
     OT gd[12];
@@ -252,32 +254,9 @@ k_env(OT* __restrict__ em, OT* __restrict__ em_deriv, OT* __restrict__ rij,
     for (int k = 0; k < 12; ++k) gd[k] = (OT)0.;
     if (j >= 0) {
       for (int d = 0; d < 3; ++d) r[d] = (OT)(fc[3 * j + d] - xi[d]);
-      OT nr2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-      OT inr = (OT)1. / sqrt(nr2);
-      OT nr = nr2 * inr;
-      OT inr2 = inr * inr;
-      OT inr4 = inr2 * inr2;
-      OT inr3 = inr4 * nr;
-      OT sw, dsw;
-      spline5<OT>(sw, dsw, nr, rmin, rmax);
-      v[0] = (OT)1. / nr;
-      v[1] = r[0] / nr2;
-      v[2] = r[1] / nr2;
-      v[3] = r[2] / nr2;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) gd[d] = r[d] * inr3 * sw - v[0] * dsw * r[d] * inr;
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          OT base = (OT)2. * r[a] * r[d] * inr4;
-          if (a == d) base = base - inr2;
-          gd[3 + a * 3 + d] = base * sw - v[1 + a] * dsw * r[d] * inr;
-        }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) v[k] *= sw;
+      env_row<OT>(r, rmin, rmax, v, want_d ? gd : nullptr);
     }
-    OT* e = em + (orow * nnei + jj) * 4;
+    OT* e = io.em + (orow * nnei + jj) * 4;
     if (ti >= 0) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) e[k] = (v[k] - av[jj * 4 + k]) / sd[jj * 4 + k];
@@ -285,19 +264,50 @@ k_env(OT* __restrict__ em, OT* __restrict__ em_deriv, OT* __restrict__ rij,
 #pragma unroll
       for (int k = 0; k < 4; ++k) e[k] = (OT)0.;
     }
-    if (em_deriv) {
-      OT* ed = em_deriv + (orow * nnei + jj) * 12;
+    if (want_d) {
+      OT* ed = io.em_deriv + (orow * nnei + jj) * 12;
 #pragma unroll
       for (int k = 0; k < 12; ++k) ed[k] = ti >= 0 ? gd[k] / sd[jj * 4 + k / 3] : (OT)0.;
     }
-    if (rij) {
-      OT* rr = rij + (orow * nnei + jj) * 3;
+    if (io.rij) {
+      OT* rr = io.rij + (orow * nnei + jj) * 3;
       rr[0] = r[0];
       rr[1] = r[1];
       rr[2] = r[2];
     }
   }
+  return true;
 }
+
+template <typename CT, typename OT, int CAP, int WARPS, bool FROM_CELLS>
+__global__ void __launch_bounds__(WARPS * 32)
+k_env(EnvIO<CT, OT> io, SecInfo sec, int nrows, int* redo) {
+  __shared__ EnvSmem<CAP> sm[WARPS];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * WARPS + w;
+  if (row >= nrows) return;
+  const bool ok = env_one<CT, OT, CAP, FROM_CELLS>(io, sec, row, sm[w], redo != nullptr);
+  if (!ok && lane == 0) {
+    int p = atomicAdd(&redo[0], 1);
+    redo[1 + p] = row;
+  }
+}
+
+// Atoms deferred by k_env: one warp each with the large key buffer. Launched
+// unconditionally with a fixed grid; it reads the queue length on the device.
+template <typename CT, typename OT, int CAP>
+__global__ void __launch_bounds__(32) k_env_redo(EnvIO<CT, OT> io, SecInfo sec,
+                                                 const int* redo) {
+  __shared__ EnvSmem<CAP> sm;
+  const int n = redo[0];
+  for (int r = blockIdx.x; r < n; r += gridDim.x) {
+    env_one<CT, OT, CAP, true>(io, sec, redo[1 + r], sm, false);
+    __syncwarp();
+  }
+}
+
+constexpr int ENV_SMALL_CAP = 256;
+constexpr int ENV_LARGE_CAP = 4096;
 
 template <typename CT, typename OT>
 static int env_cells(OT* em, OT* em_deriv, OT* rij, int* nlist, const CT* coord,
@@ -313,12 +323,21 @@ static int env_cells(OT* em, OT* em_deriv, OT* rij, int* nlist, const CT* coord,
     set_error("env_mat_a_cells: grid and status are required");
     return DPB_ERR_INVALID;
   }
+  if ((em_deriv == nullptr) != (rij == nullptr)) {
+    set_error("env_mat_a_cells: em_deriv and rij are either both given or both null");
+    return DPB_ERR_INVALID;
+  }
   GridView g = carve_grid(const_cast<void*>(grid), nall);
+  EnvIO<CT, OT> io{em, em_deriv, rij, nlist, coord, type, g, nullptr, nullptr, nullptr,
+                   avg, std_, nloc, nall, rcut, rcut_smth, status};
+  cudaStream_t st = as_stream(stream);
+  DPB_CUDA(cudaMemsetAsync(g.redo, 0, sizeof(int), st), "env_mat_a_cells");
   constexpr int W = 4;
-  k_env<CT, OT, ENV_CAP, W, true><<<ceil_div(nloc, W), W * 32, 0, as_stream(stream)>>>(
-      em, em_deriv, rij, nlist, coord, type, g, nullptr, nullptr, nullptr, avg,
-      std_, nloc, nall, nloc, rcut, rcut_smth, s, status);
+  k_env<CT, OT, ENV_SMALL_CAP, W, true><<<ceil_div(nloc, W), W * 32, 0, st>>>(io, s, nloc,
+                                                                             g.redo);
   DPB_CHECK_LAUNCH("env_mat_a_cells");
+  k_env_redo<CT, OT, ENV_LARGE_CAP><<<64, 32, 0, st>>>(io, s, g.redo);
+  DPB_CHECK_LAUNCH("env_mat_a_cells/large");
   return DPB_OK;
 }
 
@@ -342,21 +361,20 @@ static int env_inlist(T* em, T* em_deriv, T* rij, int* nlist, const T* coord,
     return DPB_ERR_INVALID;
   }
   if (inum <= 0) return DPB_OK;
-  cudaStream_t st = as_stream(stream);
-  GridView g{};
-  if (max_nbor_size <= 1024) {
-    constexpr int W = 4;
-    k_env<T, T, 1024, W, false><<<ceil_div(inum, W), W * 32, 0, st>>>(
-        em, em_deriv, rij, nlist, coord, type, g, ilist, numneigh, firstneigh,
-        avg, std_, nloc, nall, inum, rcut, rcut_smth, s, status);
-  } else if (max_nbor_size <= 4096) {
-    k_env<T, T, 4096, 1, false><<<inum, 32, 0, st>>>(
-        em, em_deriv, rij, nlist, coord, type, g, ilist, numneigh, firstneigh,
-        avg, std_, nloc, nall, inum, rcut, rcut_smth, s, status);
-  } else {
+  if (max_nbor_size > ENV_LARGE_CAP) {
     set_error("prod_env_mat_a: max_nbor_size %d exceeds 4096 (GPU_MAX_NBOR_SIZE)",
               max_nbor_size);
     return DPB_ERR_NLIST_CAPACITY;
+  }
+  cudaStream_t st = as_stream(stream);
+  GridView g{};
+  EnvIO<T, T> io{em, em_deriv, rij, nlist, coord, type, g, ilist, numneigh, firstneigh,
+                 avg, std_, nloc, nall, rcut, rcut_smth, status};
+  if (max_nbor_size <= 1024) {
+    constexpr int W = 4;
+    k_env<T, T, 1024, W, false><<<ceil_div(inum, W), W * 32, 0, st>>>(io, s, inum, nullptr);
+  } else {
+    k_env<T, T, ENV_LARGE_CAP, 1, false><<<inum, 32, 0, st>>>(io, s, inum, nullptr);
   }
   DPB_CHECK_LAUNCH("prod_env_mat_a");
   return DPB_OK;

@@ -20,6 +20,7 @@
 #include <math.h>
 
 #include "dpb_common.cuh"
+#include "dpb_envmath.cuh"
 #include "dpb_internal.cuh"
 
 namespace dpb {
@@ -63,15 +64,6 @@ __device__ __forceinline__ void flocate(const FTab& t, float x, int& idx, float&
   }
 }
 
-__device__ __forceinline__ void fpoly(const float* p, float xx, float delta, float& v,
-                                      float& g) {
-  const float2* q = reinterpret_cast<const float2*>(p);
-  float2 A = __ldg(q), B = __ldg(q + 1), C = __ldg(q + 2);
-  g = A.y + (2.f * B.x + (3.f * B.y + (4.f * C.x + 5.f * C.y * xx) * xx) * xx) * xx;
-  v = A.x + (A.y + (B.x + (B.y + (C.x + C.y * xx) * xx) * xx) * xx) * xx;
-  v = v + g * delta;
-}
-
 // first slot q in [0, n) of a type block whose em_x equals the block's last
 // and whose em[1..3] are zero; n when there is none
 __device__ __forceinline__ int block_fold(const float4* e4, int n, int lane) {
@@ -90,7 +82,55 @@ __device__ __forceinline__ int block_fold(const float4* e4, int n, int lane) {
   return n;
 }
 
-template <int MC>
+// Coefficients of 4 consecutive channels m0..m0+3 of one table row: 24 floats
+// = 6 x 16-byte loads (the row offset (idx*M + m0)*6 floats is a multiple of 4
+// floats when M % 4 == 0).
+struct Coef4 {
+  float4 q[6];
+};
+
+__device__ __forceinline__ Coef4 load_coef4(const float* row, int m0) {
+  const float4* p = reinterpret_cast<const float4*>(row + (size_t)m0 * 6);
+  Coef4 c;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) c.q[k] = __ldg(p + k);
+  return c;
+}
+
+// coefficient a_k of channel c (0..3) in the 24-float group
+__device__ __forceinline__ float cf(const Coef4& c, int ch, int k) {
+  const int f = ch * 6 + k;
+  const float4& v = c.q[f >> 2];
+  switch (f & 3) {
+    case 0: return v.x;
+    case 1: return v.y;
+    case 2: return v.z;
+    default: return v.w;
+  }
+}
+
+// value only: a0 + (a1 + (a2 + (a3 + (a4 + a5 x) x) x) x) x  (tabulate.cc:123-130)
+__device__ __forceinline__ float hval(const Coef4& c, int ch, float x) {
+  return cf(c, ch, 0) +
+         (cf(c, ch, 1) +
+          (cf(c, ch, 2) + (cf(c, ch, 3) + (cf(c, ch, 4) + cf(c, ch, 5) * x) * x) * x) * x) * x;
+}
+
+// value and derivative by the joint Horner recurrence (9 FMA)
+__device__ __forceinline__ void hvalgrad(const Coef4& c, int ch, float x, float& v, float& g) {
+  float p = cf(c, ch, 5), d = p;
+  p = p * x + cf(c, ch, 4);
+  d = d * x + p;
+  p = p * x + cf(c, ch, 3);
+  d = d * x + p;
+  p = p * x + cf(c, ch, 2);
+  d = d * x + p;
+  p = p * x + cf(c, ch, 1);
+  d = d * x + p;
+  v = p * x + cf(c, ch, 0);
+  g = d;
+}
+
 __global__ void __launch_bounds__(SW * 32)
 k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
            const int* __restrict__ drow, const float* __restrict__ em,
@@ -100,9 +140,11 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
   const int i = blockIdx.x * SW + w;
   if (i >= nloc) return;
   const int nnei = tt.nnei;
-  float acc[MC][4];
+  const int m0 = 4 * lane;
+  const bool act = m0 < M;
+  float acc[4][4];
 #pragma unroll
-  for (int c = 0; c < MC; ++c)
+  for (int c = 0; c < 4; ++c)
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[c][k] = 0.f;
   const float4* erow = reinterpret_cast<const float4*>(em + (size_t)i * nnei * 4);
@@ -118,35 +160,44 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
       int idx;
       float xx, delta;
       flocate(inf, e.x, idx, xx, delta);
-      const float rep = q == brk ? (float)(nt - q) : 1.f;
-      const float* row = tab + (size_t)idx * M * 6;
+      if (act) {
+        const Coef4 c = load_coef4(tab + (size_t)idx * M * 6, m0);
+        float v[4];
+        if (delta == 0.f) {
 #pragma unroll
-      for (int c = 0; c < MC; ++c) {
-        const int m = c * 32 + lane;
-        if (m < M) {
-          float v, g;
-          fpoly(row + m * 6, xx, delta, v, g);
-          const float sc = rep * v;
-          acc[c][0] += sc * e.x;
-          acc[c][1] += sc * e.y;
-          acc[c][2] += sc * e.z;
-          acc[c][3] += sc * e.w;
+          for (int ch = 0; ch < 4; ++ch) v[ch] = hval(c, ch, xx);
+        } else {  // linear extrapolation outside the table (tabulate.cc:133-144)
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch) {
+            float g;
+            hvalgrad(c, ch, xx, v[ch], g);
+            v[ch] = v[ch] + g * delta;
+          }
+        }
+        if (q == brk) {
+          const float rep = (float)(nt - q);
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch) v[ch] *= rep;
+        }
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) {
+          acc[ch][0] += v[ch] * e.x;
+          acc[ch][1] += v[ch] * e.y;
+          acc[ch][2] += v[ch] * e.z;
+          acc[ch][3] += v[ch] * e.w;
         }
       }
       if (q == brk) break;
     }
   }
   float* xo = xyz_out + (size_t)i * 4 * M;
+  if (act) {
 #pragma unroll
-  for (int c = 0; c < MC; ++c) {
-    const int m = c * 32 + lane;
-    if (m < M) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float v = acc[c][k] * inv_nnei;
-        s_x[w][k][m] = v;
-        xo[k * M + m] = v;
-      }
+    for (int k = 0; k < 4; ++k) {
+      float4 o = make_float4(acc[0][k] * inv_nnei, acc[1][k] * inv_nnei, acc[2][k] * inv_nnei,
+                             acc[3][k] * inv_nnei);
+      *reinterpret_cast<float4*>(xo + k * M + m0) = o;
+      *reinterpret_cast<float4*>(&s_x[w][k][m0]) = o;
     }
   }
   __syncwarp();
@@ -159,7 +210,8 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
   }
 }
 
-template <int MC>
+constexpr int GRP = 8;  // neighbors reduced together in the backward
+
 __global__ void __launch_bounds__(SW * 32)
 k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
            const int* __restrict__ drow, const float* __restrict__ xyz,
@@ -167,6 +219,7 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
            float inv_nnei) {
   __shared__ float s_x[SW][4][MAXM];
   __shared__ float s_d[SW][MAXM * (MAXAX + 1)];
+  __shared__ float s_t[SW][4 * MAXAX];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * SW + w;
   if (i >= nloc) return;
@@ -180,37 +233,40 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
     s_d[w][m * ldd + a] = dr[q];
   }
   __syncwarp();
-  // dxyz[k, m] = sum_a dD[m, a] x[k, a] + [m < naxis] sum_m' dD[m', m] x[k, m']
-  float dyr[MC][4];
+  // second term of dxyz for the first naxis channels, spread over the warp:
+  // T[k, a] = sum_m' dD[m', a] x[k, m']
+  for (int o = lane; o < 4 * naxis; o += 32) {
+    const int k = o / naxis, a = o - k * naxis;
+    float acc = 0.f;
+    for (int mp = 0; mp < M; ++mp) acc += s_d[w][mp * ldd + a] * s_x[w][k][mp];
+    s_t[w][o] = acc;
+  }
+  __syncwarp();
+  // dxyz[k, m] = sum_a dD[m, a] x[k, a] + [m < naxis] T[k, m]
+  const int m0 = 4 * lane;
+  const bool act = m0 < M;
+  float dyr[4][4];
 #pragma unroll
-  for (int c = 0; c < MC; ++c) {
-    const int m = c * 32 + lane;
-    float d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
-    if (m < M) {
+  for (int ch = 0; ch < 4; ++ch) {
+    const int m = m0 + ch;
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    if (act) {
       for (int a = 0; a < naxis; ++a) {
         const float g = s_d[w][m * ldd + a];
-        d0 += g * s_x[w][0][a];
-        d1 += g * s_x[w][1][a];
-        d2 += g * s_x[w][2][a];
-        d3 += g * s_x[w][3][a];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) d[k] += g * s_x[w][k][a];
       }
       if (m < naxis) {
-        for (int mp = 0; mp < M; ++mp) {
-          const float g = s_d[w][mp * ldd + m];
-          d0 += g * s_x[w][0][mp];
-          d1 += g * s_x[w][1][mp];
-          d2 += g * s_x[w][2][mp];
-          d3 += g * s_x[w][3][mp];
-        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) d[k] += s_t[w][k * naxis + m];
       }
     }
-    dyr[c][0] = d0 * inv_nnei;
-    dyr[c][1] = d1 * inv_nnei;
-    dyr[c][2] = d2 * inv_nnei;
-    dyr[c][3] = d3 * inv_nnei;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dyr[ch][k] = d[k] * inv_nnei;
   }
   const float4* erow = reinterpret_cast<const float4*>(em + (size_t)i * nnei * 4);
   float4* nrow = reinterpret_cast<float4*>(net_deriv + (size_t)i * nnei * 4);
+  const int b4 = (lane >> 4) & 1, b3 = (lane >> 3) & 1, b2 = (lane >> 2) & 1;
   for (int t = 0; t < tt.ntypes; ++t) {
     const int s0 = tt.sec[t], nt = tt.sec[t + 1] - s0;
     if (nt <= 0) continue;
@@ -219,42 +275,74 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
     const int last = brk < nt ? brk : nt - 1;
     const float* tab = tt.table[t];
     const FTab inf = tt.info[t];
-    for (int base = 0; base < nt; base += 32) {
-      float4 keep = make_float4(0.f, 0.f, 0.f, 0.f);
-      const int cnt = (last + 1 - base) < 32 ? (last + 1 - base) : 32;
-      for (int q = 0; q < cnt; ++q) {
-        const int qq = base + q;
-        const float4 e = e4[qq];
-        int idx;
-        float xx, delta;
-        flocate(inf, e.x, idx, xx, delta);
-        const float* row = tab + (size_t)idx * M * 6;
-        float px = 0.f, p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+    for (int g0 = 0; g0 < nt; g0 += GRP) {
+      float P[GRP][5];
 #pragma unroll
-        for (int c = 0; c < MC; ++c) {
-          const int m = c * 32 + lane;
-          if (m < M) {
-            float v, g;
-            fpoly(row + m * 6, xx, delta, v, g);
-            const float dot = e.x * dyr[c][0] + e.y * dyr[c][1] + e.z * dyr[c][2] +
-                              e.w * dyr[c][3];
-            px += g * dot;
-            p0 += v * dyr[c][0];
-            p1 += v * dyr[c][1];
-            p2 += v * dyr[c][2];
-            p3 += v * dyr[c][3];
+      for (int q = 0; q < GRP; ++q) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) P[q][k] = 0.f;
+        const int qq = g0 + q;
+        if (qq <= last) {  // warp-uniform
+          const float4 e = e4[qq];
+          int idx;
+          float xx, delta;
+          flocate(inf, e.x, idx, xx, delta);
+          if (act) {
+            const Coef4 c = load_coef4(tab + (size_t)idx * M * 6, m0);
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch) {
+              float v, g;
+              hvalgrad(c, ch, xx, v, g);
+              v = v + g * delta;
+              const float dot =
+                  e.x * dyr[ch][0] + e.y * dyr[ch][1] + e.z * dyr[ch][2] + e.w * dyr[ch][3];
+              P[q][0] += g * dot;
+              P[q][1] += v * dyr[ch][0];
+              P[q][2] += v * dyr[ch][1];
+              P[q][3] += v * dyr[ch][2];
+              P[q][4] += v * dyr[ch][3];
+            }
+          }
+          if (qq == brk) {
+            const float rep = (float)(nt - qq);
+#pragma unroll
+            for (int k = 0; k < 5; ++k) P[q][k] *= rep;
           }
         }
-        px = warp_sum(px);
-        p0 = warp_sum(p0);
-        p1 = warp_sum(p1);
-        p2 = warp_sum(p2);
-        p3 = warp_sum(p3);
-        const float rep = qq == brk ? (float)(nt - qq) : 1.f;
-        if (lane == q) keep = make_float4((p0 + px) * rep, p1 * rep, p2 * rep, p3 * rep);
       }
-      const int qq = base + lane;
-      if (qq < nt) nrow[s0 + qq] = keep;  // zero beyond the fold point
+      // reduce-scatter of the 8 x 5 partials over the warp: after the xor-16,
+      // -8 and -4 steps lane L holds neighbor q = 4*b4 + 2*b3 + b2 summed over
+      // 8 lanes; xor-2 and xor-1 finish the sum in every lane of the quad.
+      float R1[4][5];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const float mine = b4 ? P[4 + q][k] : P[q][k];
+          const float other = b4 ? P[q][k] : P[4 + q][k];
+          R1[q][k] = mine + __shfl_xor_sync(0xffffffffu, other, 16);
+        }
+      float R2[2][5];
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const float mine = b3 ? R1[2 + q][k] : R1[q][k];
+          const float other = b3 ? R1[q][k] : R1[2 + q][k];
+          R2[q][k] = mine + __shfl_xor_sync(0xffffffffu, other, 8);
+        }
+      float R3[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const float mine = b2 ? R2[1][k] : R2[0][k];
+        const float other = b2 ? R2[0][k] : R2[1][k];
+        R3[k] = mine + __shfl_xor_sync(0xffffffffu, other, 4);
+        R3[k] += __shfl_xor_sync(0xffffffffu, R3[k], 2);
+        R3[k] += __shfl_xor_sync(0xffffffffu, R3[k], 1);
+      }
+      const int qq = g0 + 4 * b4 + 2 * b3 + b2;
+      if ((lane & 3) == 0 && qq < nt)  // zero beyond the fold point
+        nrow[s0 + qq] = make_float4(R3[1] + R3[0], R3[2], R3[3], R3[4]);
     }
   }
 }
@@ -322,14 +410,99 @@ k_force_virial(double* __restrict__ force, double* __restrict__ virial,
   }
 }
 
+// Force and virial with em_deriv and rij recomputed from the coordinates and
+// the neighbor list instead of being read back (same formulas and precision
+// as the env kernels, dpb_envmath.cuh): the forward pass then stores only em.
+template <typename CT, typename OT>
+__global__ void __launch_bounds__(SW * 32)
+k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
+                  const OT* __restrict__ nd, const CT* __restrict__ coord,
+                  const int* __restrict__ type, const OT* __restrict__ std_,
+                  const int* __restrict__ nlist, const int* __restrict__ mapping, int nloc,
+                  int nnei, int ntypes, float rcut, float rcut_smth) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * SW + w;
+  if (i >= nloc) return;
+  const int ti = type[i];
+  if (ti < 0 || ti >= ntypes) return;  // em_deriv rows are zero (prod_env_mat.cc:117-123)
+  const CT xi[3] = {coord[3 * i], coord[3 * i + 1], coord[3 * i + 2]};
+  const OT* sd = std_ + (size_t)ti * nnei * 4;
+  const OT* ndr = nd + (size_t)i * nnei * 4;
+  double c0 = 0., c1 = 0., c2 = 0.;
+  double vs[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) vs[k] = 0.;
+  for (int jj = lane; jj < nnei; jj += 32) {
+    const int j = nlist[(size_t)i * nnei + jj];
+    if (j < 0) continue;  // padding: em_deriv = 0
+    OT r[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[d] = (OT)(coord[3 * j + d] - xi[d]);
+    OT v[4], gd[12];
+    env_row<OT>(r, rcut_smth, rcut, v, gd);
+    OT p[3] = {(OT)0., (OT)0., (OT)0.};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const OT n = ndr[jj * 4 + a];
+      const OT s = sd[jj * 4 + a];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) p[d] += n * (gd[a * 3 + d] / s);
+    }
+    const double q[3] = {(double)p[0], (double)p[1], (double)p[2]};
+    c0 += q[0];
+    c1 += q[1];
+    c2 += q[2];
+    const int o = mapping ? mapping[j] : j;
+    atomicAdd(&force[(size_t)o * 3 + 0], q[0]);
+    atomicAdd(&force[(size_t)o * 3 + 1], q[1]);
+    atomicAdd(&force[(size_t)o * 3 + 2], q[2]);
+#pragma unroll
+    for (int d0 = 0; d0 < 3; ++d0)
+#pragma unroll
+      for (int d1 = 0; d1 < 3; ++d1) vs[d0 * 3 + d1] += q[d0] * (double)r[d1];
+  }
+  c0 = warp_sum(c0);
+  c1 = warp_sum(c1);
+  c2 = warp_sum(c2);
+  if (lane == 0) {
+    atomicAdd(&force[(size_t)i * 3 + 0], -c0);
+    atomicAdd(&force[(size_t)i * 3 + 1], -c1);
+    atomicAdd(&force[(size_t)i * 3 + 2], -c2);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const double s = warp_sum(vs[k]);
+    if (lane == 0) atomicAdd(&virial[k], s);
+  }
+}
+
+template <typename CT, typename OT>
+static int force_virial_rc(double* force, double* virial, const OT* nd, const CT* coord,
+                           const int* type, const OT* std_, const int* nlist,
+                           const int* mapping, int nloc, int nforce, int nnei, int ntypes,
+                           float rcut, float rcut_smth, cudaStream_t st) {
+  if (nloc < 0 || nforce < 0 || nnei < 0 || ntypes <= 0) {
+    set_error("force_virial_env: invalid sizes");
+    return DPB_ERR_INVALID;
+  }
+  DPB_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * 3 * (size_t)nforce, st), "force_virial");
+  DPB_CUDA(cudaMemsetAsync(virial, 0, sizeof(double) * 9, st), "force_virial");
+  if (nloc == 0 || nnei == 0) return DPB_OK;
+  k_force_virial_rc<CT, OT><<<ceil_div(nloc, SW), SW * 32, 0, st>>>(
+      force, virial, nd, coord, type, std_, nlist, mapping, nloc, nnei, ntypes, rcut, rcut_smth);
+  DPB_CHECK_LAUNCH("force_virial_env");
+  return DPB_OK;
+}
+
 static int make_tables(TypeTables& tt, const float* const* tables, const float* info,
                        const int* sec, int nsec, int M) {
   if (nsec < 2 || nsec - 1 > PMAXT || tables == nullptr || info == nullptr || sec == nullptr) {
     set_error("se_a pipeline: need 1..%d neighbor types with tables, info and sec", PMAXT);
     return DPB_ERR_INVALID;
   }
-  if (M <= 0 || M > MAXM) {
-    set_error("se_a pipeline: last_layer_size must be in [1, %d], got %d", MAXM, M);
+  if (M <= 0 || M > MAXM || M % 4 != 0) {
+    set_error("se_a pipeline: last_layer_size must be a multiple of 4 in [4, %d], got %d",
+              MAXM, M);
     return DPB_ERR_INVALID;
   }
   tt.ntypes = nsec - 1;
@@ -395,10 +568,7 @@ int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_r
   const float inv = tt.nnei > 0 ? 1.f / (float)tt.nnei : 0.f;
   cudaStream_t st = as_stream(stream);
   dim3 g(ceil_div(nloc, SW));
-  if (M <= 32) k_desc_fwd<1><<<g, SW * 32, 0, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M, axis_neuron, inv);
-  else if (M <= 64) k_desc_fwd<2><<<g, SW * 32, 0, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M, axis_neuron, inv);
-  else if (M <= 96) k_desc_fwd<3><<<g, SW * 32, 0, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M, axis_neuron, inv);
-  else k_desc_fwd<4><<<g, SW * 32, 0, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M, axis_neuron, inv);
+  k_desc_fwd<<<g, SW * 32, 0, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M, axis_neuron, inv);
   DPB_CHECK_LAUNCH("se_a_descriptor_fwd");
   return DPB_OK;
 }
@@ -420,12 +590,29 @@ int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
   const float inv = tt.nnei > 0 ? 1.f / (float)tt.nnei : 0.f;
   cudaStream_t st = as_stream(stream);
   dim3 g(ceil_div(nloc, SW));
-  if (M <= 32) k_desc_bwd<1><<<g, SW * 32, 0, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em, tt, nloc, M, axis_neuron, inv);
-  else if (M <= 64) k_desc_bwd<2><<<g, SW * 32, 0, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em, tt, nloc, M, axis_neuron, inv);
-  else if (M <= 96) k_desc_bwd<3><<<g, SW * 32, 0, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em, tt, nloc, M, axis_neuron, inv);
-  else k_desc_bwd<4><<<g, SW * 32, 0, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em, tt, nloc, M, axis_neuron, inv);
+  k_desc_bwd<<<g, SW * 32, 0, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em, tt, nloc, M, axis_neuron, inv);
   DPB_CHECK_LAUNCH("se_a_descriptor_bwd");
   return DPB_OK;
+}
+
+int dpb_force_virial_a_env_mixed(double* force, double* virial, const float* net_deriv,
+                                 const double* coord, const int* type, const float* std_,
+                                 const int* nlist, const int* mapping, int nloc, int nforce,
+                                 int nnei, int ntypes, float rcut, float rcut_smth,
+                                 dpb_stream_t stream) {
+  return force_virial_rc<double, float>(force, virial, net_deriv, coord, type, std_, nlist,
+                                        mapping, nloc, nforce, nnei, ntypes, rcut, rcut_smth,
+                                        as_stream(stream));
+}
+
+int dpb_force_virial_a_env_f64(double* force, double* virial, const double* net_deriv,
+                               const double* coord, const int* type, const double* std_,
+                               const int* nlist, const int* mapping, int nloc, int nforce,
+                               int nnei, int ntypes, float rcut, float rcut_smth,
+                               dpb_stream_t stream) {
+  return force_virial_rc<double, double>(force, virial, net_deriv, coord, type, std_, nlist,
+                                         mapping, nloc, nforce, nnei, ntypes, rcut, rcut_smth,
+                                         as_stream(stream));
 }
 
 int dpb_force_virial_a_f32(double* force, double* virial, double* atom_virial,

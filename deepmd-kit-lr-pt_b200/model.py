@@ -267,8 +267,6 @@ class SeAEvaluator:
         self.avg = torch.tensor(params.davg, dtype=fdt, device=dev)
         self.std = torch.tensor(params.dstd, dtype=fdt, device=dev)
         self.em = torch.empty((nloc, nnei * 4), dtype=fdt, device=dev)
-        self.emd = torch.empty((nloc, nnei * 12), dtype=fdt, device=dev)
-        self.rij = torch.empty((nloc, nnei * 3), dtype=fdt, device=dev)
         self.nlist = torch.empty((nloc, nnei), dtype=torch.int32, device=dev)
         self.net_deriv = torch.empty((nloc, nnei * 4), dtype=fdt, device=dev)
         self.force = torch.zeros((nloc, 3), dtype=torch.float64, device=dev)
@@ -334,7 +332,9 @@ class SeAEvaluator:
         env = "dpb_env_mat_a_cells_mixed" if self.mode == "compressed" else \
             "dpb_env_mat_a_cells_f64"
         with tm("env_mat"):
-            call(env, ptr(self.em), ptr(self.emd), ptr(self.rij), ptr(self.nlist),
+            # only em and nlist are stored: em_deriv and rij are recomputed by
+            # the force/virial kernel
+            call(env, ptr(self.em), None, None, ptr(self.nlist),
                  ptr(self.cext), ptr(self.text), ptr(self.grid), ptr(self.avg), ptr(self.std),
                  nloc, self.mem_nall, ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth),
                  self.sec.ctypes.data, self.sec.size, ptr(self.status), s)
@@ -343,11 +343,12 @@ class SeAEvaluator:
         else:
             with tm("descriptor_fitting_fp64"):
                 self._descriptor_plain()
-        fv = "dpb_force_virial_a_f32" if self.mode == "compressed" else "dpb_force_virial_a_f64"
+        fv = "dpb_force_virial_a_env_mixed" if self.mode == "compressed" else \
+            "dpb_force_virial_a_env_f64"
         with tm("force_virial"):
-            call(fv, ptr(self.force), ptr(self.virial), None, ptr(self.net_deriv),
-                 ptr(self.emd), ptr(self.rij), ptr(self.nlist), ptr(self.mapping), nloc, nloc,
-                 self.mem_nall, nnei, s)
+            call(fv, ptr(self.force), ptr(self.virial), ptr(self.net_deriv), ptr(self.cext),
+                 ptr(self.text), ptr(self.std), ptr(self.nlist), ptr(self.mapping), nloc, nloc,
+                 nnei, cfg.ntypes, ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth), s)
 
     def _descriptor_compressed(self, s, tm):
         cfg = self.cfg

@@ -301,6 +301,26 @@ DPB_API int dpb_force_virial_a_f64(double* force, double* virial,
                                    int nloc, int nforce, int nall, int nnei,
                                    dpb_stream_t stream);
 
+/* The same force and virial with em_deriv and rij recomputed from the
+ * extended coordinates and the neighbor list (so the forward pass need not
+ * store them): coord [nall, 3] FP64, type [nall], std_ the env-mat
+ * normalisation [ntypes, nnei * 4] used in the forward. _mixed: FP32
+ * net_deriv/std with the env-mat derivative in FP32 from FP64 differences. */
+DPB_API int dpb_force_virial_a_env_mixed(double* force, double* virial,
+                                         const float* net_deriv,
+                                         const double* coord, const int* type,
+                                         const float* std_, const int* nlist,
+                                         const int* mapping, int nloc, int nforce,
+                                         int nnei, int ntypes, float rcut,
+                                         float rcut_smth, dpb_stream_t stream);
+DPB_API int dpb_force_virial_a_env_f64(double* force, double* virial,
+                                       const double* net_deriv,
+                                       const double* coord, const int* type,
+                                       const double* std_, const int* nlist,
+                                       const int* mapping, int nloc, int nforce,
+                                       int nnei, int ntypes, float rcut,
+                                       float rcut_smth, dpb_stream_t stream);
+
 /* ------------------------------------------- allocation-free variant ---- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc,
  * e.g. an MD engine's force callback that runs inside the engine's own
