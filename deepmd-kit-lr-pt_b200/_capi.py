@@ -91,6 +91,7 @@ _FUNCS = {
     "dpb_force_virial_a_f64": "pppppp" "pp" "iiiip",
     "dpb_build_nlist_noalloc_f64": "ppppp" "iiif" "i" "pp",
     "dpb_force_virial_a_env_mixed": "pppppppp" "iiii" "ff" "p",
+    "dpb_gemm_tf32x3_f32": "pii" "pp" "i" "pi" "i" "pppp" "ppp" "pp" "p",
     "dpb_force_virial_a_env_f64": "pppppppp" "iiii" "ff" "p",
 }
 _SIZE_QUERIES = {

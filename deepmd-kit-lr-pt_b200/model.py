@@ -196,6 +196,103 @@ class _Fitting:
         return torch.addmm(bo, h, Wo).view(-1) + self.bias[t]
 
 
+def tf32_split(w: np.ndarray):
+    """(hi, lo) FP32 arrays with hi the round-to-nearest (ties away) TF32 value
+    of w, as cvt.rna.tf32.f32 computes it, and lo = w - hi."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    u = w.view(np.uint32).astype(np.uint64)
+    hi = ((u + 0x1000) & 0xFFFFE000).astype(np.uint32).view(np.float32)
+    lo = (w - hi).astype(np.float32)
+    return hi, lo
+
+
+class _FittingTC:
+    """Per-type fitting networks, forward and input-gradient, as six fused
+    3xTF32 tensor-core GEMMs (dpb_gemm_tf32x3_f32). Rows of the descriptor are
+    grouped by center type; ``type_rows`` gives the group sizes."""
+
+    EPI_STORE, EPI_TANH, EPI_RES_DT, EPI_LAST, EPI_BWD_DT, EPI_BWD_RES = range(6)
+
+    def __init__(self, params: SeAParams, type_rows, device):
+        dev = torch.device(device)
+        self.dev = dev
+        cfg = params.cfg
+        if len(cfg.fitting) != 3 or len(set(cfg.fitting)) != 1:
+            raise _capi.DPBInvalidArgument(
+                "the tensor-core fitting path handles three equal-width hidden layers")
+        self.type_rows = np.ascontiguousarray(type_rows, dtype=np.int32)
+        self.n = int(self.type_rows.sum())
+        self.ntypes = cfg.ntypes
+        self.width = cfg.fitting[0]
+        self.din = cfg.neuron[-1] * cfg.axis_neuron
+        f32 = lambda a: torch.tensor(np.asarray(a, np.float32), device=dev)  # noqa: E731
+        keep = []
+
+        def split(mats):
+            hs, ls = [], []
+            for m in mats:
+                h, l = tf32_split(m)
+                hs.append(f32(h))
+                ls.append(f32(l))
+            keep.extend(hs + ls)
+            return ((ctypes.c_void_p * len(hs))(*[t.data_ptr() for t in hs]),
+                    (ctypes.c_void_p * len(ls))(*[t.data_ptr() for t in ls]))
+
+        def vecs(vs):
+            ts = [f32(v) for v in vs]
+            keep.extend(ts)
+            return (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+        L = [f["layers"] for f in params.fit]
+        # B operands are [N, K] row-major: forward uses W^T, backward uses W
+        self.B1f = split([l[0][0].T for l in L])
+        self.B2f = split([l[1][0].T for l in L])
+        self.B3f = split([l[2][0].T for l in L])
+        self.B3b = split([l[2][0] for l in L])
+        self.B2b = split([l[1][0] for l in L])
+        self.B1b = split([l[0][0] for l in L])
+        self.b1 = vecs([l[0][1] for l in L])
+        self.b2 = vecs([l[1][1] for l in L])
+        self.b3 = vecs([l[2][1] for l in L])
+        self.d2 = vecs([l[1][2] for l in L])
+        self.d3 = vecs([l[2][2] for l in L])
+        self.w4 = vecs([f["out"][0][:, 0] for f in params.fit])
+        self._keep = keep
+        # per-type constant of the energy: output bias + atomic energy bias
+        self.e_const = float(sum(int(self.type_rows[t]) * (float(params.fit[t]["out"][1][0])
+                                                           + float(params.bias_atom_e[t]))
+                                 for t in range(self.ntypes)))
+        n, w = self.n, self.width
+        z = lambda *shape: torch.zeros(shape, dtype=torch.float32, device=dev)  # noqa: E731
+        self.H1, self.Y2, self.H2, self.G3 = z(n, w), z(n, w), z(n, w), z(n, w)
+        self.g2, self.G2, self.G1 = z(n, w), z(n, w), z(n, w)
+        self.e = z(n)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def _gemm(self, A, K, B, N, mode, out0, out1=None, aux0=None, aux1=None, bias=None,
+              idt=None, w=None, s=None):
+        call("dpb_gemm_tf32x3_f32", ptr(A), self.n, K, B[0], B[1], N, self.type_rows.ctypes.data,
+             self.ntypes, mode, ptr(out0), ptr(out1), ptr(aux0), ptr(aux1), bias, idt, w,
+             ptr(self.e), ptr(self.status), s)
+
+    def forward_backward(self, D: torch.Tensor, dD: torch.Tensor, energy: torch.Tensor):
+        """energy[0] = sum of atomic energies (FP64); dD = dE/dD (FP32)."""
+        s = torch.cuda.current_stream().cuda_stream
+        w, din = self.width, self.din
+        self.e.zero_()
+        self._gemm(D, din, self.B1f, w, self.EPI_TANH, self.H1, bias=self.b1, s=s)
+        self._gemm(self.H1, w, self.B2f, w, self.EPI_RES_DT, self.Y2, self.H2, aux0=self.H1,
+                   bias=self.b2, idt=self.d2, s=s)
+        self._gemm(self.H2, w, self.B3f, w, self.EPI_LAST, self.G3, aux0=self.H2, bias=self.b3,
+                   idt=self.d3, w=self.w4, s=s)
+        self._gemm(self.G3, w, self.B3b, w, self.EPI_BWD_DT, self.G2, self.g2, aux0=self.Y2,
+                   idt=self.d2, w=self.w4, s=s)
+        self._gemm(self.G2, w, self.B2b, w, self.EPI_BWD_RES, self.G1, aux0=self.H1,
+                   aux1=self.g2, s=s)
+        self._gemm(self.G1, w, self.B1b, din, self.EPI_STORE, dD, s=s)
+        energy.copy_((self.e.to(torch.float64).sum() + self.e_const).view(1))
+
+
 # ------------------------------------------------------------ evaluators --
 
 class _Stages:
@@ -235,7 +332,8 @@ class SeAEvaluator:
     a CUDA graph that ``replay()`` re-runs."""
 
     def __init__(self, params: SeAParams, atype: np.ndarray, box: np.ndarray,
-                 mode: str = "compressed", device="cuda:0", nall_capacity: int | None = None):
+                 mode: str = "compressed", device="cuda:0", nall_capacity: int | None = None,
+                 tensor_core_fitting: bool = True):
         cfg = params.cfg
         self.cfg, self.params, self.mode = cfg, params, mode
         self.dev = torch.device(device)
@@ -289,6 +387,7 @@ class SeAEvaluator:
             self.xyz = torch.empty((nloc, 4, M), dtype=torch.float32, device=dev)
             self.D = torch.empty((nloc, M * ax), dtype=torch.float32, device=dev)
             self.dD = torch.empty_like(self.D)
+            self.fit_tc = _FittingTC(params, counts, dev) if tensor_core_fitting else None
             self.tab = [torch.tensor(t, dtype=torch.float32, device=dev) for t, _ in params.tables]
             self.tab_ptrs = (ctypes.c_void_p * len(self.tab))(*[t.data_ptr() for t in self.tab])
             self.tab_info = np.ascontiguousarray(
@@ -358,14 +457,17 @@ class SeAEvaluator:
                  ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data, self.sec.ctypes.data,
                  self.sec.size, self.nloc, M, ax, s)
         with tm("fitting"):
-            etot = torch.zeros((), dtype=torch.float64, device=self.dev)
-            for t, (a, b) in enumerate(self.type_ranges):
-                if b == a:
-                    continue
-                e, g = self.fitting.forward_backward(t, self.D[a:b])
-                self.dD[a:b].copy_(g)
-                etot = etot + e.to(torch.float64).sum()
-            self.energy.copy_(etot.view(1))
+            if self.fit_tc is not None:
+                self.fit_tc.forward_backward(self.D, self.dD, self.energy)
+            else:
+                etot = torch.zeros((), dtype=torch.float64, device=self.dev)
+                for t, (a, b) in enumerate(self.type_ranges):
+                    if b == a:
+                        continue
+                    e, g = self.fitting.forward_backward(t, self.D[a:b])
+                    self.dD[a:b].copy_(g)
+                    etot = etot + e.to(torch.float64).sum()
+                self.energy.copy_(etot.view(1))
         with tm("descriptor_bwd"):
             call("dpb_se_a_descriptor_bwd_f32", ptr(self.net_deriv), ptr(self.dD),
                  ptr(self.drow), ptr(self.xyz), ptr(self.em), self.tab_ptrs,
@@ -432,6 +534,9 @@ class SeAEvaluator:
             raise _capi.DPBCapacityError(
                 f"DeePMD-kit Error: nall={h[0]} exceeds the capacity {self.mem_nall}")
         call("dpb_status_check", ptr(self.status), torch.cuda.current_stream().cuda_stream)
+        if getattr(self, "fit_tc", None) is not None:
+            call("dpb_status_check", ptr(self.fit_tc.status),
+                 torch.cuda.current_stream().cuda_stream)
         return int(h[0])
 
     # ---- public call: host in, host out

@@ -321,6 +321,25 @@ DPB_API int dpb_force_virial_a_env_f64(double* force, double* virial,
                                        int nnei, int ntypes, float rcut,
                                        float rcut_smth, dpb_stream_t stream);
 
+/* FP32-accurate (3xTF32) GEMM on the sm_100a tensor cores for the per-type
+ * fitting networks (deepmd/pt/model/task/ener.py; layer math of
+ * deepmd/dpmodel/utils/network.py:282-330): C = A B^T with A [M, K] FP32
+ * row-major (rows grouped by type, type_rows[t] rows of type t) and, per
+ * type, B [N, K] given pre-split into TF32 hi/lo parts (b_hi/b_lo: HOST
+ * arrays of device pointers). mode selects the fused epilogue (0 store,
+ * 1 tanh(acc+bias), 2 tanh+timestep residual, 3 last layer + energy and its
+ * first gradient, 4/5 backward of the residual layers); bias/idt/w are HOST
+ * arrays of per-type device vectors [N]. N must be a multiple of 80 (<= 240)
+ * or of 160; K*4 and the row pitch must be multiples of 16 bytes. */
+DPB_API int dpb_gemm_tf32x3_f32(const float* A, int M, int K,
+                                const float* const* b_hi,
+                                const float* const* b_lo, int N,
+                                const int* type_rows, int ntypes, int mode,
+                                float* out0, float* out1, const float* aux0,
+                                const float* aux1, const float* const* bias,
+                                const float* const* idt, const float* const* w,
+                                float* e, int* status, dpb_stream_t stream);
+
 /* ------------------------------------------- allocation-free variant ---- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc,
  * e.g. an MD engine's force callback that runs inside the engine's own

@@ -1,0 +1,133 @@
+"""3xTF32 tensor-core GEMM (dpb_gemm_tf32x3_f32) and the fitting networks built
+on it, against FP64 references. 3xTF32 keeps FP32-level accuracy: relative
+errors of a few 1e-6 on these sizes; the bar is 2e-5 relative to the output
+scale (the FP32 bar of the reference tests is 1e-5 absolute on O(1) values)."""
+
+import ctypes
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+
+@pytest.fixture(scope="module")
+def mdl(dpb):
+    return importlib.import_module("deepmd_kit_lr_pt_b200.model")
+
+
+def _ptrs(ts):
+    return (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+
+def _run(dpb, mdl, A, Bs, type_rows, mode, aux0=None, aux1=None, bias=None, idt=None, w=None):
+    M, K = A.shape
+    N = Bs[0].shape[0]
+    hi, lo = zip(*[mdl.tf32_split(b) for b in Bs])
+    th = [torch.tensor(h, device=DEV) for h in hi]
+    tl = [torch.tensor(l, device=DEV) for l in lo]
+    out0 = torch.zeros((M, N), dtype=torch.float32, device=DEV)
+    out1 = torch.zeros((M, N), dtype=torch.float32, device=DEV)
+    e = torch.zeros(M, dtype=torch.float32, device=DEV)
+    st = torch.zeros(1, dtype=torch.int32, device=DEV)
+    tr = np.asarray(type_rows, np.int32)
+    keep = []
+
+    def vec(vs):
+        if vs is None:
+            return None
+        ts = [torch.tensor(np.asarray(v, np.float32), device=DEV) for v in vs]
+        keep.extend(ts)
+        return _ptrs(ts)
+
+    cap = dpb._capi
+    ta = torch.tensor(A, device=DEV)
+    x0 = None if aux0 is None else torch.tensor(aux0, device=DEV)
+    x1 = None if aux1 is None else torch.tensor(aux1, device=DEV)
+    cap.call("dpb_gemm_tf32x3_f32", cap.ptr(ta), M, K, _ptrs(th), _ptrs(tl), N, tr.ctypes.data,
+             len(Bs), mode, cap.ptr(out0), cap.ptr(out1), cap.ptr(x0), cap.ptr(x1), vec(bias),
+             vec(idt), vec(w), cap.ptr(e), cap.ptr(st), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    cap.call("dpb_status_check", cap.ptr(st), torch.cuda.current_stream().cuda_stream)
+    return out0.cpu().numpy(), out1.cpu().numpy(), e.cpu().numpy()
+
+
+def _ref(A, Bs, type_rows):
+    out, r = [], 0
+    for B, n in zip(Bs, type_rows):
+        out.append(A[r:r + n].astype(np.float64) @ B.astype(np.float64).T)
+        r += n
+    return np.concatenate(out)
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(1e-30, np.abs(b).max()))
+
+
+@pytest.mark.parametrize("M,K,N,rows", [(256, 64, 80, [128, 128]), (300, 240, 240, [100, 200]),
+                                        (777, 1600, 240, [259, 518]), (640, 240, 1600, [640])])
+def test_gemm_store(dpb, mdl, M, K, N, rows):
+    rng = np.random.default_rng(M + K + N)
+    A = rng.normal(size=(M, K)).astype(np.float32)
+    Bs = [rng.normal(size=(N, K)).astype(np.float32) / np.sqrt(K) for _ in rows]
+    out0, _, _ = _run(dpb, mdl, A, Bs, rows, 0)
+    ref = _ref(A, Bs, rows)
+    err = _rel(out0, ref)
+    print(f"M={M} K={K} N={N}: rel err {err:.2e}")
+    assert err < 2e-5
+
+
+def test_gemm_epilogues(dpb, mdl):
+    rng = np.random.default_rng(3)
+    rows, M, K, N = [96, 160], 256, 240, 240
+    A = rng.normal(size=(M, K)).astype(np.float32) * 0.5
+    Bs = [rng.normal(size=(N, K)).astype(np.float32) / np.sqrt(K) for _ in rows]
+    acc = _ref(A, Bs, rows)
+    tid = np.repeat(np.arange(2), rows)
+    bias = [rng.normal(size=N) for _ in rows]
+    idt = [rng.normal(0.1, 0.01, size=N) for _ in rows]
+    w = [rng.normal(size=N) for _ in rows]
+    b = np.stack(bias)[tid]
+    d = np.stack(idt)[tid]
+    wv = np.stack(w)[tid]
+    x0 = rng.normal(size=(M, N)).astype(np.float32) * 0.5
+    x1 = rng.normal(size=(M, N)).astype(np.float32)
+    tol = 2e-5
+    o0, _, _ = _run(dpb, mdl, A, Bs, rows, 1, bias=bias)
+    assert _rel(o0, np.tanh(acc + b)) < tol
+    o0, o1, _ = _run(dpb, mdl, A, Bs, rows, 2, aux0=x0, bias=bias, idt=idt)
+    y = np.tanh(acc + b)
+    assert _rel(o0, y) < tol and _rel(o1, x0 + d * y) < tol
+    o0, _, e = _run(dpb, mdl, A, Bs, rows, 3, aux0=x0, bias=bias, idt=idt, w=w)
+    h = x0 + d * y
+    assert _rel(e, (h * wv).sum(1)) < tol and _rel(o0, wv * d * (1 - y * y)) < tol
+    o0, o1, _ = _run(dpb, mdl, A, Bs, rows, 4, aux0=x0, idt=idt, w=w)
+    g = wv + acc
+    assert _rel(o1, g) < tol and _rel(o0, g * d * (1 - x0 * x0)) < tol
+    o0, _, _ = _run(dpb, mdl, A, Bs, rows, 5, aux0=x0, aux1=x1)
+    assert _rel(o0, (x1 + acc) * (1 - x0 * x0)) < tol
+
+
+def test_fitting_tc_matches_fp64(dpb, mdl):
+    cfg = mdl.SeAConfig()
+    p = mdl.init_params(cfg, seed=2)
+    rows = [64, 200]
+    n = sum(rows)
+    rng = np.random.default_rng(0)
+    D = (rng.normal(size=(n, 1600)) * 0.05).astype(np.float32)
+    fit = mdl._FittingTC(p, rows, DEV)
+    dD = torch.zeros((n, 1600), dtype=torch.float32, device=DEV)
+    E = torch.zeros(1, dtype=torch.float64, device=DEV)
+    fit.forward_backward(torch.tensor(D, device=DEV), dD, E)
+    ref = mdl._Fitting(p, torch.float64, DEV)
+    Dt = torch.tensor(D, dtype=torch.float64, device=DEV)
+    e0, g0 = ref.forward_backward(0, Dt[:rows[0]])
+    e1, g1 = ref.forward_backward(1, Dt[rows[0]:])
+    Eref = float(e0.sum() + e1.sum())
+    gref = torch.cat([g0, g1]).cpu().numpy()
+    print(f"E {float(E):.8f} ref {Eref:.8f}; dD rel {_rel(dD.cpu().numpy(), gref):.2e}")
+    assert abs(float(E) - Eref) / n < 1e-6
+    assert _rel(dD.cpu().numpy(), gref) < 2e-5
