@@ -296,56 +296,76 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
     have = __shfl_sync(0xffffffffu, have ? 1 : 0, 0) != 0;  // tcgen05.ld is warp-wide
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (have) {
-      const int lane_base = 32 * (warp & 3);
-      const int row = row0 + lane_base + lane;
-      const bool valid = row < row_end;
+      // TMEM -> registers (one row per thread) -> a 32 x 16 staging tile in
+      // the now idle pipeline shared memory -> coalesced row segments: each
+      // half-warp handles one row, 16 consecutive columns per instruction.
+      const int wq = warp & 3;
+      const int lane_base = 32 * wq;
+      float* stg = reinterpret_cast<float*>(smem) + wq * (32 * 17 + 32);
+      float* erow = stg + 32 * 17;
+      erow[lane] = 0.f;
       const float* bias = epi.bias[ty];
       const float* idt = epi.idt[ty];
       const float* wv = epi.w[ty];
-      float epart = 0.f;
+      const int half = lane >> 4, cl = lane & 15;
       for (int c0 = 0; c0 < BN; c0 += 16) {
         float v[16];
         tmem_ld16(tmem + ((uint32_t)lane_base << 16) + (uint32_t)c0, v);
-        if (!valid) continue;
-        const size_t base = (size_t)row * epi.ld + n0 + c0;
+        __syncwarp();
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c0 + j;
-          if (col >= shp.N) break;
-          float a = v[j];
+        for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = v[j];
+        __syncwarp();
+        const int col = n0 + c0 + cl;
+        float bcol = 0.f, dcol = 0.f, wcol = 0.f;
+        if (bias) bcol = bias[col];
+        if (idt) dcol = idt[col];
+        if (wv) wcol = wv[col];
+        for (int rr = 0; rr < 32; rr += 2) {
+          const int r = rr + half;
+          const int row = row0 + lane_base + r;
+          const float a = stg[r * 17 + cl];
+          if (row >= row_end) continue;
+          const size_t at = (size_t)row * epi.ld + col;
           switch (epi.mode) {
             case EPI_STORE:
-              epi.out0[base + j] = a;
+              epi.out0[at] = a;
               break;
             case EPI_TANH:
-              epi.out0[base + j] = tanhf(a + bias[col]);
+              epi.out0[at] = tanhf(a + bcol);
               break;
             case EPI_RES_DT: {
-              const float y = tanhf(a + bias[col]);
-              epi.out0[base + j] = y;
-              epi.out1[base + j] = epi.aux0[base + j] + idt[col] * y;
+              const float y = tanhf(a + bcol);
+              epi.out0[at] = y;
+              epi.out1[at] = epi.aux0[at] + dcol * y;
             } break;
             case EPI_LAST: {
-              const float y = tanhf(a + bias[col]);
-              const float h = epi.aux0[base + j] + idt[col] * y;
-              epart += h * wv[col];
-              epi.out0[base + j] = wv[col] * idt[col] * (1.f - y * y);
+              const float y = tanhf(a + bcol);
+              const float h = epi.aux0[at] + dcol * y;
+              epi.out0[at] = wcol * dcol * (1.f - y * y);
+              float pe = h * wcol;  // this row's energy share over 16 columns
+              pe += __shfl_xor_sync(0x0000ffffu << (16 * half), pe, 8);
+              pe += __shfl_xor_sync(0x0000ffffu << (16 * half), pe, 4);
+              pe += __shfl_xor_sync(0x0000ffffu << (16 * half), pe, 2);
+              pe += __shfl_xor_sync(0x0000ffffu << (16 * half), pe, 1);
+              if (cl == 0) erow[r] += pe;
             } break;
             case EPI_BWD_DT: {
-              const float g = wv[col] + a;
-              const float y = epi.aux0[base + j];
-              epi.out1[base + j] = g;
-              epi.out0[base + j] = g * idt[col] * (1.f - y * y);
+              const float g = wcol + a;
+              const float y = epi.aux0[at];
+              epi.out1[at] = g;
+              epi.out0[at] = g * dcol * (1.f - y * y);
             } break;
             default: {  // EPI_BWD_RES
-              const float g = epi.aux1[base + j] + a;
-              const float h = epi.aux0[base + j];
-              epi.out0[base + j] = g * (1.f - h * h);
+              const float g = epi.aux1[at] + a;
+              const float h = epi.aux0[at];
+              epi.out0[at] = g * (1.f - h * h);
             } break;
           }
         }
       }
-      if (epi.mode == EPI_LAST && valid) atomicAdd(&epi.e[row], epart);
+      __syncwarp();
+      if (epi.mode == EPI_LAST && row0 + lane_base + lane < row_end)
+        atomicAdd(&epi.e[row0 + lane_base + lane], erow[lane]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
