@@ -167,7 +167,7 @@ __device__ __forceinline__ float tf32_hi(float x) {
 }
 
 template <int BN, int STAGES>
-__global__ void __launch_bounds__(GT_THREADS, 1)
+__global__ void __launch_bounds__(GT_THREADS, STAGES <= 2 ? 2 : 1)
 k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi, int* status) {
   constexpr int A_BYTES = GT_BM * GT_BK * 4;  // 16 KB
   constexpr int B_BYTES = BN * GT_BK * 4;
@@ -320,45 +320,61 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
         if (bias) bcol = bias[col];
         if (idt) dcol = idt[col];
         if (wv) wcol = wv[col];
-        for (int rr = 0; rr < 32; rr += 2) {
-          const int r = rr + half;
+        // gather the chunk's 16 rows per half-warp first (independent loads in
+        // flight), then compute and store
+        const int mode = epi.mode;
+        const bool need0 = mode >= EPI_RES_DT, need1 = mode == EPI_BWD_RES;
+        float x0[16], x1[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int row = row0 + lane_base + 2 * q + half;
+          const size_t at = (size_t)row * epi.ld + col;
+          const bool ok = row < row_end;
+          x0[q] = (need0 && ok) ? epi.aux0[at] : 0.f;
+          x1[q] = (need1 && ok) ? epi.aux1[at] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int r = 2 * q + half;
           const int row = row0 + lane_base + r;
           const float a = stg[r * 17 + cl];
-          if (row >= row_end) continue;
+          const bool ok = row < row_end;
           const size_t at = (size_t)row * epi.ld + col;
-          switch (epi.mode) {
+          switch (mode) {
             case EPI_STORE:
-              epi.out0[at] = a;
+              if (ok) epi.out0[at] = a;
               break;
             case EPI_TANH:
-              epi.out0[at] = tanhf(a + bcol);
+              if (ok) epi.out0[at] = tanhf(a + bcol);
               break;
             case EPI_RES_DT: {
               const float y = tanhf(a + bcol);
-              epi.out0[at] = y;
-              epi.out1[at] = epi.aux0[at] + dcol * y;
+              if (ok) {
+                epi.out0[at] = y;
+                epi.out1[at] = x0[q] + dcol * y;
+              }
             } break;
             case EPI_LAST: {
               const float y = tanhf(a + bcol);
-              const float h = epi.aux0[at] + dcol * y;
-              epi.out0[at] = wcol * dcol * (1.f - y * y);
-              float pe = h * wcol;  // this row's energy share over 16 columns
-              pe += __shfl_xor_sync(0x0000ffffu << (16 * half), pe, 8);
-              pe += __shfl_xor_sync(0x0000ffffu << (16 * half), pe, 4);
-              pe += __shfl_xor_sync(0x0000ffffu << (16 * half), pe, 2);
-              pe += __shfl_xor_sync(0x0000ffffu << (16 * half), pe, 1);
+              const float h = x0[q] + dcol * y;
+              if (ok) epi.out0[at] = wcol * dcol * (1.f - y * y);
+              float pe = ok ? h * wcol : 0.f;  // this row's energy share, 16 columns
+              pe += __shfl_xor_sync(0xffffffffu, pe, 8);
+              pe += __shfl_xor_sync(0xffffffffu, pe, 4);
+              pe += __shfl_xor_sync(0xffffffffu, pe, 2);
+              pe += __shfl_xor_sync(0xffffffffu, pe, 1);
               if (cl == 0) erow[r] += pe;
             } break;
             case EPI_BWD_DT: {
               const float g = wcol + a;
-              const float y = epi.aux0[at];
-              epi.out1[at] = g;
-              epi.out0[at] = g * dcol * (1.f - y * y);
+              if (ok) {
+                epi.out1[at] = g;
+                epi.out0[at] = g * dcol * (1.f - x0[q] * x0[q]);
+              }
             } break;
             default: {  // EPI_BWD_RES
-              const float g = epi.aux1[at] + a;
-              const float h = epi.aux0[at];
-              epi.out0[at] = g * (1.f - h * h);
+              const float g = x1[q] + a;
+              if (ok) epi.out0[at] = g * (1.f - x0[q] * x0[q]);
             } break;
           }
         }
@@ -448,11 +464,11 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
   }
   int rc = get_encoder();
   if (rc) return rc;
-  const int BN = (N % 80 == 0 && N <= 240) ? 80 : 160;
-  if (N % BN != 0 && BN == 160 && N % 160 != 0) {
-    set_error("gemm_tf32x3: N=%d must be a multiple of 80 (N <= 240) or 160", N);
+  if (N % 80 != 0) {
+    set_error("gemm_tf32x3: N=%d must be a multiple of 80", N);
     return DPB_ERR_INVALID;
   }
+  const int BN = 80;
   GemmMaps maps;
   GemmShape shp;
   shp.ntypes = ntypes;
@@ -490,8 +506,10 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
     ep.w[t] = w ? w[t] : nullptr;
   }
   cudaStream_t st = as_stream(stream);
-  if (BN == 80) return launch<80, 4>(maps, shp, ep, status, st);
-  return launch<160, 3>(maps, shp, ep, status, st);
+  // short reductions: two CTAs per SM (2 stages each) so one CTA's epilogue
+  // overlaps the other's main loop; long reductions: a deep 4-stage ring
+  if (K <= 256) return launch<BN, 2>(maps, shp, ep, status, st);
+  return launch<BN, 4>(maps, shp, ep, status, st);
 }
 
 }  // extern "C"

@@ -329,8 +329,8 @@ DPB_API int dpb_force_virial_a_env_f64(double* force, double* virial,
  * arrays of device pointers). mode selects the fused epilogue (0 store,
  * 1 tanh(acc+bias), 2 tanh+timestep residual, 3 last layer + energy and its
  * first gradient, 4/5 backward of the residual layers); bias/idt/w are HOST
- * arrays of per-type device vectors [N]. N must be a multiple of 80 (<= 240)
- * or of 160; K*4 and the row pitch must be multiples of 16 bytes. */
+ * arrays of per-type device vectors [N]. N must be a multiple of 80
+ *; K*4 and the row pitch must be multiples of 16 bytes. */
 DPB_API int dpb_gemm_tf32x3_f32(const float* A, int M, int K,
                                 const float* const* b_hi,
                                 const float* const* b_lo, int N,
