@@ -85,6 +85,7 @@ _FUNCS = {
     "dpb_prod_virial_a_f32": "pppppp" "iiip",
     "dpb_copy_coord_async_f64": "ppppp" "L" "ppiifpp",
     "dpb_cell_grid_build_async_f64": "pLpipfp",
+    "dpb_se_a_pack_table_f32": "ppiip",
     "dpb_se_a_descriptor_fwd_f32": "pppp" "pp" "pi" "iiip",
     "dpb_se_a_descriptor_bwd_f32": "ppppp" "pp" "pi" "iiip",
     "dpb_force_virial_a_f32": "pppppp" "pp" "iiiip",

@@ -65,7 +65,8 @@ __device__ __forceinline__ void flocate(const FTab& t, float x, int& idx, float&
 }
 
 // first slot q in [0, n) of a type block whose em_x equals the block's last
-// and whose em[1..3] are zero; n when there is none
+// and whose em[1..3] are zero; n when there is none (rows staged in shared
+// memory)
 __device__ __forceinline__ int block_fold(const float4* e4, int n, int lane) {
   if (n <= 0) return 0;
   const float last = e4[n - 1].x;
@@ -82,26 +83,26 @@ __device__ __forceinline__ int block_fold(const float4* e4, int n, int lane) {
   return n;
 }
 
-// Coefficients of 4 consecutive channels m0..m0+3 of one table row: 24 floats
-// = 6 x 16-byte loads (the row offset (idx*M + m0)*6 floats is a multiple of 4
-// floats when M % 4 == 0).
+// Coefficients of 4 consecutive channels m0..m0+3 of one table row in the
+// pipeline layout [row][6][M] (coefficient-major, dpb_se_a_pack_table_f32):
+// q[k] holds a_k of the 4 channels, so each of the 6 loads of a warp reads one
+// contiguous 4M-byte segment of the row (M % 4 == 0 keeps them 16-byte
+// aligned).
 struct Coef4 {
   float4 q[6];
 };
 
-__device__ __forceinline__ Coef4 load_coef4(const float* row, int m0) {
-  const float4* p = reinterpret_cast<const float4*>(row + (size_t)m0 * 6);
+__device__ __forceinline__ Coef4 load_coef4(const float* row, int M) {
   Coef4 c;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) c.q[k] = __ldg(p + k);
+  for (int k = 0; k < 6; ++k) c.q[k] = __ldg(reinterpret_cast<const float4*>(row + k * M));
   return c;
 }
 
-// coefficient a_k of channel c (0..3) in the 24-float group
+// coefficient a_k of channel ch (0..3)
 __device__ __forceinline__ float cf(const Coef4& c, int ch, int k) {
-  const int f = ch * 6 + k;
-  const float4& v = c.q[f >> 2];
-  switch (f & 3) {
+  const float4& v = c.q[k];
+  switch (ch) {
     case 0: return v.x;
     case 1: return v.y;
     case 2: return v.z;
@@ -131,15 +132,50 @@ __device__ __forceinline__ void hvalgrad(const Coef4& c, int ch, float x, float&
   g = d;
 }
 
+// Per-warp staging of one center atom's neighbor slots in shared memory:
+// se[s] = em row s, sl[s] = (table row as int bits, offset in the row,
+// extrapolation distance, 0). The table coordinates are computed once per
+// slot, lane-parallel, so the channel loops only wait on coefficient loads.
+__device__ __forceinline__ void stage_slots(float4* se, float4* sl, const float4* erow,
+                                            const TypeTables& tt, int lane) {
+  for (int t = 0; t < tt.ntypes; ++t) {
+    const FTab inf = tt.info[t];
+    for (int s = tt.sec[t] + lane; s < tt.sec[t + 1]; s += 32) {
+      const float4 e = erow[s];
+      int idx;
+      float xx, delta;
+      flocate(inf, e.x, idx, xx, delta);
+      se[s] = e;
+      sl[s] = make_float4(__int_as_float(idx), xx, delta, 0.f);
+    }
+  }
+}
+
+// shared memory of the descriptor kernels: per warp, 2 * nnei float4 of slot
+// staging, or (backward) the dD / x tiles of the prologue when larger
+static size_t fwd_smem_floats(int M, int nnei) {
+  const size_t slots = (size_t)nnei * 8, xs = (size_t)4 * M;
+  return slots > xs ? slots : xs;
+}
+static size_t bwd_smem_floats(int M, int nnei, int naxis) {
+  const size_t slots = (size_t)nnei * 8, dd = (size_t)M * (naxis + 1);
+  return (size_t)4 * M + 4 * MAXAX + (slots > dd ? slots : dd);
+}
+
 __global__ void __launch_bounds__(SW * 32)
 k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
            const int* __restrict__ drow, const float* __restrict__ em,
-           TypeTables tt, int nloc, int M, int naxis, float inv_nnei) {
-  __shared__ float s_x[SW][4][MAXM];
+           TypeTables tt, int nloc, int M, int naxis, float inv_nnei, int warp_floats) {
+  extern __shared__ float4 dsm4[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * SW + w;
   if (i >= nloc) return;
   const int nnei = tt.nnei;
+  float* wsm = reinterpret_cast<float*>(dsm4) + (size_t)w * warp_floats;
+  float4* se = reinterpret_cast<float4*>(wsm);
+  float4* sl = se + nnei;
+  stage_slots(se, sl, reinterpret_cast<const float4*>(em + (size_t)i * nnei * 4), tt, lane);
+  __syncwarp();
   const int m0 = 4 * lane;
   const bool act = m0 < M;
   float acc[4][4];
@@ -147,31 +183,38 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
   for (int c = 0; c < 4; ++c)
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[c][k] = 0.f;
-  const float4* erow = reinterpret_cast<const float4*>(em + (size_t)i * nnei * 4);
   for (int t = 0; t < tt.ntypes; ++t) {
     const int s0 = tt.sec[t], nt = tt.sec[t + 1] - s0;
     if (nt <= 0) continue;
-    const float4* e4 = erow + s0;
-    const int brk = block_fold(e4, nt, lane);
-    const float* tab = tt.table[t];
-    const FTab inf = tt.info[t];
-    for (int q = 0; q < nt; ++q) {
-      const float4 e = e4[q];
-      int idx;
-      float xx, delta;
-      flocate(inf, e.x, idx, xx, delta);
+    const int brk = block_fold(se + s0, nt, lane);
+    const int last = brk < nt ? brk : nt - 1;
+    const float* tab = tt.table[t] + m0;
+    const size_t rs = (size_t)M * 6;
+    int ci = __float_as_int(sl[s0].x);
+    Coef4 cc;
+    if (act) cc = load_coef4(tab + (size_t)ci * rs, M);
+    for (int q = 0; q <= last; ++q) {
+      // next row in flight while this one is evaluated; consecutive slots of
+      // a distance-sorted block often share a row, which is then reused
+      int ni = ci;
+      Coef4 cn = cc;
+      if (q < last) {
+        ni = __float_as_int(sl[s0 + q + 1].x);
+        if (ni != ci && act) cn = load_coef4(tab + (size_t)ni * rs, M);
+      }
       if (act) {
-        const Coef4 c = load_coef4(tab + (size_t)idx * M * 6, m0);
+        const float4 e = se[s0 + q];
+        const float4 L = sl[s0 + q];
         float v[4];
-        if (delta == 0.f) {
+        if (L.z == 0.f) {
 #pragma unroll
-          for (int ch = 0; ch < 4; ++ch) v[ch] = hval(c, ch, xx);
+          for (int ch = 0; ch < 4; ++ch) v[ch] = hval(cc, ch, L.y);
         } else {  // linear extrapolation outside the table (tabulate.cc:133-144)
 #pragma unroll
           for (int ch = 0; ch < 4; ++ch) {
             float g;
-            hvalgrad(c, ch, xx, v[ch], g);
-            v[ch] = v[ch] + g * delta;
+            hvalgrad(cc, ch, L.y, v[ch], g);
+            v[ch] = v[ch] + g * L.z;
           }
         }
         if (q == brk) {
@@ -187,9 +230,12 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
           acc[ch][3] += v[ch] * e.w;
         }
       }
-      if (q == brk) break;
+      cc = cn;
+      ci = ni;
     }
   }
+  __syncwarp();  // the slot staging is reused for x below
+  float* sx = wsm;  // [4][M]
   float* xo = xyz_out + (size_t)i * 4 * M;
   if (act) {
 #pragma unroll
@@ -197,7 +243,7 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
       float4 o = make_float4(acc[0][k] * inv_nnei, acc[1][k] * inv_nnei, acc[2][k] * inv_nnei,
                              acc[3][k] * inv_nnei);
       *reinterpret_cast<float4*>(xo + k * M + m0) = o;
-      *reinterpret_cast<float4*>(&s_x[w][k][m0]) = o;
+      *reinterpret_cast<float4*>(sx + k * M + m0) = o;
     }
   }
   __syncwarp();
@@ -205,8 +251,8 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
   const int nd = M * naxis;
   for (int q = lane; q < nd; q += 32) {
     const int m = q / naxis, a = q - m * naxis;
-    Dr[q] = s_x[w][0][m] * s_x[w][0][a] + s_x[w][1][m] * s_x[w][1][a] +
-            s_x[w][2][m] * s_x[w][2][a] + s_x[w][3][m] * s_x[w][3][a];
+    Dr[q] = sx[m] * sx[a] + sx[M + m] * sx[M + a] + sx[2 * M + m] * sx[2 * M + a] +
+            sx[3 * M + m] * sx[3 * M + a];
   }
 }
 
@@ -216,21 +262,23 @@ __global__ void __launch_bounds__(SW * 32)
 k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
            const int* __restrict__ drow, const float* __restrict__ xyz,
            const float* __restrict__ em, TypeTables tt, int nloc, int M, int naxis,
-           float inv_nnei) {
-  __shared__ float s_x[SW][4][MAXM];
-  __shared__ float s_d[SW][MAXM * (MAXAX + 1)];
-  __shared__ float s_t[SW][4 * MAXAX];
+           float inv_nnei, int warp_floats) {
+  extern __shared__ float4 dsm4[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * SW + w;
   if (i >= nloc) return;
   const int nnei = tt.nnei;
+  float* wsm = reinterpret_cast<float*>(dsm4) + (size_t)w * warp_floats;
+  float* s_x = wsm;                // [4][M]
+  float* s_t = s_x + 4 * M;        // [4][naxis]
+  float* s_d = s_t + 4 * MAXAX;    // [M][naxis + 1], later the slot staging
   const float* xi = xyz + (size_t)i * 4 * M;
-  for (int q = lane; q < 4 * M; q += 32) s_x[w][q / M][q % M] = xi[q];
+  for (int q = lane; q < 4 * M; q += 32) s_x[q] = xi[q];
   const float* dr = dD + (size_t)drow[i] * M * naxis;
   const int ldd = naxis + 1;  // padded row: conflict-free column reads
   for (int q = lane; q < M * naxis; q += 32) {
     const int m = q / naxis, a = q - m * naxis;
-    s_d[w][m * ldd + a] = dr[q];
+    s_d[m * ldd + a] = dr[q];
   }
   __syncwarp();
   // second term of dxyz for the first naxis channels, spread over the warp:
@@ -238,8 +286,8 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
   for (int o = lane; o < 4 * naxis; o += 32) {
     const int k = o / naxis, a = o - k * naxis;
     float acc = 0.f;
-    for (int mp = 0; mp < M; ++mp) acc += s_d[w][mp * ldd + a] * s_x[w][k][mp];
-    s_t[w][o] = acc;
+    for (int mp = 0; mp < M; ++mp) acc += s_d[mp * ldd + a] * s_x[k * M + mp];
+    s_t[o] = acc;
   }
   __syncwarp();
   // dxyz[k, m] = sum_a dD[m, a] x[k, a] + [m < naxis] T[k, m]
@@ -252,29 +300,35 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
     float d[4] = {0.f, 0.f, 0.f, 0.f};
     if (act) {
       for (int a = 0; a < naxis; ++a) {
-        const float g = s_d[w][m * ldd + a];
+        const float g = s_d[m * ldd + a];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) d[k] += g * s_x[w][k][a];
+        for (int k = 0; k < 4; ++k) d[k] += g * s_x[k * M + a];
       }
       if (m < naxis) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) d[k] += s_t[w][k * naxis + m];
+        for (int k = 0; k < 4; ++k) d[k] += s_t[k * naxis + m];
       }
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) dyr[ch][k] = d[k] * inv_nnei;
   }
-  const float4* erow = reinterpret_cast<const float4*>(em + (size_t)i * nnei * 4);
+  __syncwarp();  // dD tile dead: stage the slots in its place
+  float4* se = reinterpret_cast<float4*>(s_d);
+  float4* sl = se + nnei;
+  stage_slots(se, sl, reinterpret_cast<const float4*>(em + (size_t)i * nnei * 4), tt, lane);
+  __syncwarp();
   float4* nrow = reinterpret_cast<float4*>(net_deriv + (size_t)i * nnei * 4);
   const int b4 = (lane >> 4) & 1, b3 = (lane >> 3) & 1, b2 = (lane >> 2) & 1;
   for (int t = 0; t < tt.ntypes; ++t) {
     const int s0 = tt.sec[t], nt = tt.sec[t + 1] - s0;
     if (nt <= 0) continue;
-    const float4* e4 = erow + s0;
-    const int brk = block_fold(e4, nt, lane);
+    const int brk = block_fold(se + s0, nt, lane);
     const int last = brk < nt ? brk : nt - 1;
-    const float* tab = tt.table[t];
-    const FTab inf = tt.info[t];
+    const float* tab = tt.table[t] + m0;
+    const size_t rs = (size_t)M * 6;
+    int ci = __float_as_int(sl[s0].x);
+    Coef4 cc;
+    if (act) cc = load_coef4(tab + (size_t)ci * rs, M);
     for (int g0 = 0; g0 < nt; g0 += GRP) {
       float P[GRP][5];
 #pragma unroll
@@ -283,17 +337,20 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
         for (int k = 0; k < 5; ++k) P[q][k] = 0.f;
         const int qq = g0 + q;
         if (qq <= last) {  // warp-uniform
-          const float4 e = e4[qq];
-          int idx;
-          float xx, delta;
-          flocate(inf, e.x, idx, xx, delta);
+          int ni = ci;
+          Coef4 cn = cc;
+          if (qq < last) {
+            ni = __float_as_int(sl[s0 + qq + 1].x);
+            if (ni != ci && act) cn = load_coef4(tab + (size_t)ni * rs, M);
+          }
           if (act) {
-            const Coef4 c = load_coef4(tab + (size_t)idx * M * 6, m0);
+            const float4 e = se[s0 + qq];
+            const float4 L = sl[s0 + qq];
 #pragma unroll
             for (int ch = 0; ch < 4; ++ch) {
               float v, g;
-              hvalgrad(c, ch, xx, v, g);
-              v = v + g * delta;
+              hvalgrad(cc, ch, L.y, v, g);
+              v = v + g * L.z;
               const float dot =
                   e.x * dyr[ch][0] + e.y * dyr[ch][1] + e.z * dyr[ch][2] + e.w * dyr[ch][3];
               P[q][0] += g * dot;
@@ -308,6 +365,8 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
 #pragma unroll
             for (int k = 0; k < 5; ++k) P[q][k] *= rep;
           }
+          cc = cn;
+          ci = ni;
         }
       }
       // reduce-scatter of the 8 x 5 partials over the warp: after the xor-16,
@@ -494,6 +553,18 @@ static int force_virial_rc(double* force, double* virial, const OT* nd, const CT
   return DPB_OK;
 }
 
+// [nrow][M][6] (reference layout) -> [nrow][6][M] (pipeline layout)
+__global__ void k_pack_table(float* __restrict__ out, const float* __restrict__ in, long long n,
+                             int M) {
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n;
+       o += (long long)gridDim.x * blockDim.x) {
+    const long long r = o / (6LL * M);
+    const int rem = (int)(o - r * 6LL * M);
+    const int k = rem / M, m = rem - k * M;
+    out[o] = in[r * 6LL * M + (long long)m * 6 + k];
+  }
+}
+
 static int make_tables(TypeTables& tt, const float* const* tables, const float* info,
                        const int* sec, int nsec, int M) {
   if (nsec < 2 || nsec - 1 > PMAXT || tables == nullptr || info == nullptr || sec == nullptr) {
@@ -551,6 +622,21 @@ int dpb_cell_grid_build_async_f64(void* grid, long long grid_bytes_, const doubl
                             as_stream(stream));
 }
 
+int dpb_se_a_pack_table_f32(float* out, const float* table, int nrow, int M,
+                             dpb_stream_t stream) {
+  if (nrow < 0 || M <= 0 || (nrow > 0 && (out == nullptr || table == nullptr || out == table))) {
+    set_error("se_a_pack_table: invalid arguments (nrow=%d M=%d, out must not alias table)",
+              nrow, M);
+    return DPB_ERR_INVALID;
+  }
+  const long long n = 6LL * M * nrow;
+  if (n == 0) return DPB_OK;
+  const int blocks = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+  k_pack_table<<<blocks, 256, 0, as_stream(stream)>>>(out, table, n, M);
+  DPB_CHECK_LAUNCH("se_a_pack_table");
+  return DPB_OK;
+}
+
 int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_row,
                                 const float* em, const float* const* tables,
                                 const float* table_info, const int* sec, int nsec,
@@ -568,7 +654,13 @@ int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_r
   const float inv = tt.nnei > 0 ? 1.f / (float)tt.nnei : 0.f;
   cudaStream_t st = as_stream(stream);
   dim3 g(ceil_div(nloc, SW));
-  k_desc_fwd<<<g, SW * 32, 0, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M, axis_neuron, inv);
+  const int wf = (int)fwd_smem_floats(M, tt.nnei);
+  const size_t smem = sizeof(float) * SW * (size_t)wf;
+  DPB_CUDA(cudaFuncSetAttribute(k_desc_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem),
+           "se_a_descriptor_fwd");
+  k_desc_fwd<<<g, SW * 32, smem, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M, axis_neuron,
+                                       inv, wf);
   DPB_CHECK_LAUNCH("se_a_descriptor_fwd");
   return DPB_OK;
 }
@@ -590,7 +682,13 @@ int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
   const float inv = tt.nnei > 0 ? 1.f / (float)tt.nnei : 0.f;
   cudaStream_t st = as_stream(stream);
   dim3 g(ceil_div(nloc, SW));
-  k_desc_bwd<<<g, SW * 32, 0, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em, tt, nloc, M, axis_neuron, inv);
+  const int wf = (int)bwd_smem_floats(M, tt.nnei, axis_neuron);
+  const size_t smem = sizeof(float) * SW * (size_t)wf;
+  DPB_CUDA(cudaFuncSetAttribute(k_desc_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem),
+           "se_a_descriptor_bwd");
+  k_desc_bwd<<<g, SW * 32, smem, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em, tt, nloc, M,
+                                       axis_neuron, inv, wf);
   DPB_CHECK_LAUNCH("se_a_descriptor_bwd");
   return DPB_OK;
 }

@@ -388,7 +388,14 @@ class SeAEvaluator:
             self.D = torch.empty((nloc, M * ax), dtype=torch.float32, device=dev)
             self.dD = torch.empty_like(self.D)
             self.fit_tc = _FittingTC(params, counts, dev) if tensor_core_fitting else None
-            self.tab = [torch.tensor(t, dtype=torch.float32, device=dev) for t, _ in params.tables]
+            self.tab = []
+            for t, _ in params.tables:
+                ref_layout = torch.tensor(t, dtype=torch.float32, device=dev)
+                packed = torch.empty_like(ref_layout)
+                call("dpb_se_a_pack_table_f32", ptr(packed), ptr(ref_layout), t.shape[0], M,
+                     torch.cuda.current_stream(dev).cuda_stream)
+                self.tab.append(packed)
+            torch.cuda.synchronize(dev)
             self.tab_ptrs = (ctypes.c_void_p * len(self.tab))(*[t.data_ptr() for t in self.tab])
             self.tab_info = np.ascontiguousarray(
                 np.concatenate([i for _, i in params.tables]).astype(np.float32))

@@ -264,9 +264,17 @@ DPB_API int dpb_cell_grid_build_async_f64(void* grid, long long grid_bytes,
                                           const int* nall_dev, float rcut,
                                           dpb_stream_t stream);
 
+/* Repacks one compression table from the tabulate layout [nrow][M][6]
+ * (source/lib/src/tabulate.cc:190-197) into the layout the fused descriptor
+ * kernels below read, [nrow][6][M] (coefficient-major: a warp's loads of one
+ * coefficient of a row are contiguous). out and table must not overlap.
+ * No counterpart in the reference (its pipeline calls the tabulate op). */
+DPB_API int dpb_se_a_pack_table_f32(float* out, const float* table, int nrow, int M,
+                                    dpb_stream_t stream);
+
 /* Compressed descriptor forward over all neighbor types: tables[t] (a HOST
- * array of device pointers, one [nspline_t, 6*M] FP32 table per neighbor
- * type), table_info: host [ntypes * 6]. em: [nloc, nnei, 4] FP32 from the env
+ * array of device pointers, one [nspline_t, 6, M] FP32 table per neighbor
+ * type in the dpb_se_a_pack_table_f32 layout), table_info: host [ntypes * 6]. em: [nloc, nnei, 4] FP32 from the env
  * kernels. Writes xyz [nloc, 4, M] (= sum_t G_t^T R_t / nnei) and the
  * descriptor row of atom i at descrpt + descrpt_row[i] * M * axis_neuron.
  * M <= 128, axis_neuron <= 16, ntypes <= 8. */
