@@ -162,7 +162,50 @@ static size_t bwd_smem_floats(int M, int nnei, int naxis) {
   return (size_t)4 * M + 4 * MAXAX + (slots > dd ? slots : dd);
 }
 
-__global__ void __launch_bounds__(SW * 32)
+// one neighbor slot of the forward: G row of 4 channels (fold multiplier at
+// the fold slot) times the env row, accumulated into acc[channel][k]
+__device__ __forceinline__ void fwd_slot(float (&acc)[4][4], const Coef4& c, const float4 e,
+                                         const float4 L, float rep) {
+  float v[4];
+  if (L.z == 0.f) {
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) v[ch] = hval(c, ch, L.y);
+  } else {  // linear extrapolation outside the table (tabulate.cc:133-144)
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      float g;
+      hvalgrad(c, ch, L.y, v[ch], g);
+      v[ch] = v[ch] + g * L.z;
+    }
+  }
+#pragma unroll
+  for (int ch = 0; ch < 4; ++ch) {
+    const float u = v[ch] * rep;
+    acc[ch][0] += u * e.x;
+    acc[ch][1] += u * e.y;
+    acc[ch][2] += u * e.z;
+    acc[ch][3] += u * e.w;
+  }
+}
+
+// D[m, a] = sum_k x[k, m] x[k, a] of one atom from x [4][M] in shared memory
+__device__ __forceinline__ void write_descriptor(float* __restrict__ Dr, const float* sx, int M,
+                                                 int naxis, int lane) {
+  if (32 % naxis == 0) {  // fixed column a per lane, 32 / naxis rows per pass
+    const int per = 32 / naxis, a = lane % naxis;
+    const float x0 = sx[a], x1 = sx[M + a], x2 = sx[2 * M + a], x3 = sx[3 * M + a];
+    for (int m = lane / naxis; m < M; m += per)
+      Dr[m * naxis + a] = sx[m] * x0 + sx[M + m] * x1 + sx[2 * M + m] * x2 + sx[3 * M + m] * x3;
+  } else {
+    for (int q = lane; q < M * naxis; q += 32) {
+      const int m = q / naxis, a = q - m * naxis;
+      Dr[q] = sx[m] * sx[a] + sx[M + m] * sx[M + a] + sx[2 * M + m] * sx[2 * M + a] +
+              sx[3 * M + m] * sx[3 * M + a];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SW * 32, 5)
 k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
            const int* __restrict__ drow, const float* __restrict__ em,
            TypeTables tt, int nloc, int M, int naxis, float inv_nnei, int warp_floats) {
@@ -188,51 +231,24 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
     if (nt <= 0) continue;
     const int brk = block_fold(se + s0, nt, lane);
     const int last = brk < nt ? brk : nt - 1;
+    if (!act) continue;
     const float* tab = tt.table[t] + m0;
     const size_t rs = (size_t)M * 6;
-    int ci = __float_as_int(sl[s0].x);
-    Coef4 cc;
-    if (act) cc = load_coef4(tab + (size_t)ci * rs, M);
-    for (int q = 0; q <= last; ++q) {
-      // next row in flight while this one is evaluated; consecutive slots of
-      // a distance-sorted block often share a row, which is then reused
-      int ni = ci;
-      Coef4 cn = cc;
-      if (q < last) {
-        ni = __float_as_int(sl[s0 + q + 1].x);
-        if (ni != ci && act) cn = load_coef4(tab + (size_t)ni * rs, M);
-      }
-      if (act) {
-        const float4 e = se[s0 + q];
-        const float4 L = sl[s0 + q];
-        float v[4];
-        if (L.z == 0.f) {
-#pragma unroll
-          for (int ch = 0; ch < 4; ++ch) v[ch] = hval(cc, ch, L.y);
-        } else {  // linear extrapolation outside the table (tabulate.cc:133-144)
-#pragma unroll
-          for (int ch = 0; ch < 4; ++ch) {
-            float g;
-            hvalgrad(cc, ch, L.y, v[ch], g);
-            v[ch] = v[ch] + g * L.z;
-          }
-        }
-        if (q == brk) {
-          const float rep = (float)(nt - q);
-#pragma unroll
-          for (int ch = 0; ch < 4; ++ch) v[ch] *= rep;
-        }
-#pragma unroll
-        for (int ch = 0; ch < 4; ++ch) {
-          acc[ch][0] += v[ch] * e.x;
-          acc[ch][1] += v[ch] * e.y;
-          acc[ch][2] += v[ch] * e.z;
-          acc[ch][3] += v[ch] * e.w;
-        }
-      }
-      cc = cn;
-      ci = ni;
+    const float4* E = se + s0;
+    const float4* Ls = sl + s0;
+    auto rep = [&](int q) { return q == brk ? (float)(nt - q) : 1.f; };
+    auto row = [&](int q) { return tab + (size_t)__float_as_int(Ls[q].x) * rs; };
+    // two coefficient buffers in turn: the next slot's row is in flight while
+    // the current one is evaluated
+    Coef4 ca = load_coef4(row(0), M), cb;
+    int q = 0;
+    for (; q + 1 <= last; q += 2) {
+      cb = load_coef4(row(q + 1), M);
+      fwd_slot(acc, ca, E[q], Ls[q], rep(q));
+      if (q + 2 <= last) ca = load_coef4(row(q + 2), M);
+      fwd_slot(acc, cb, E[q + 1], Ls[q + 1], rep(q + 1));
     }
+    if (q <= last) fwd_slot(acc, ca, E[q], Ls[q], rep(q));
   }
   __syncwarp();  // the slot staging is reused for x below
   float* sx = wsm;  // [4][M]
@@ -247,16 +263,31 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
     }
   }
   __syncwarp();
-  float* Dr = D + (size_t)drow[i] * M * naxis;
-  const int nd = M * naxis;
-  for (int q = lane; q < nd; q += 32) {
-    const int m = q / naxis, a = q - m * naxis;
-    Dr[q] = sx[m] * sx[a] + sx[M + m] * sx[M + a] + sx[2 * M + m] * sx[2 * M + a] +
-            sx[3 * M + m] * sx[3 * M + a];
-  }
+  write_descriptor(D + (size_t)drow[i] * M * naxis, sx, M, naxis, lane);
 }
 
-constexpr int GRP = 8;  // neighbors reduced together in the backward
+constexpr int GRP = 8;  // neighbors reduced together in the backward (even)
+
+// one neighbor slot of the backward: P[0] = sum_c G'_c (e . dyr_c), P[1 + d] =
+// sum_c G_c dyr_c[d] over this lane's 4 channels (times the fold multiplier)
+__device__ __forceinline__ void bwd_slot(float (&P)[5], const Coef4& c, const float4 e,
+                                         const float4 L, float rep,
+                                         const float (&dyr)[4][4]) {
+#pragma unroll
+  for (int ch = 0; ch < 4; ++ch) {
+    float v, g;
+    hvalgrad(c, ch, L.y, v, g);
+    v = v + g * L.z;
+    const float dot = e.x * dyr[ch][0] + e.y * dyr[ch][1] + e.z * dyr[ch][2] + e.w * dyr[ch][3];
+    P[0] += g * dot;
+    P[1] += v * dyr[ch][0];
+    P[2] += v * dyr[ch][1];
+    P[3] += v * dyr[ch][2];
+    P[4] += v * dyr[ch][3];
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) P[k] *= rep;
+}
 
 __global__ void __launch_bounds__(SW * 32)
 k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
@@ -276,9 +307,14 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
   for (int q = lane; q < 4 * M; q += 32) s_x[q] = xi[q];
   const float* dr = dD + (size_t)drow[i] * M * naxis;
   const int ldd = naxis + 1;  // padded row: conflict-free column reads
-  for (int q = lane; q < M * naxis; q += 32) {
-    const int m = q / naxis, a = q - m * naxis;
-    s_d[m * ldd + a] = dr[q];
+  if (32 % naxis == 0) {
+    const int per = 32 / naxis, a = lane % naxis;
+    for (int m = lane / naxis; m < M; m += per) s_d[m * ldd + a] = dr[m * naxis + a];
+  } else {
+    for (int q = lane; q < M * naxis; q += 32) {
+      const int m = q / naxis, a = q - m * naxis;
+      s_d[m * ldd + a] = dr[q];
+    }
   }
   __syncwarp();
   // second term of dxyz for the first naxis channels, spread over the warp:
@@ -295,22 +331,30 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
   const bool act = m0 < M;
   float dyr[4][4];
 #pragma unroll
-  for (int ch = 0; ch < 4; ++ch) {
-    const int m = m0 + ch;
-    float d[4] = {0.f, 0.f, 0.f, 0.f};
-    if (act) {
-      for (int a = 0; a < naxis; ++a) {
-        const float g = s_d[m * ldd + a];
+  for (int ch = 0; ch < 4; ++ch)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) d[k] += g * s_x[k * M + a];
-      }
-      if (m < naxis) {
+    for (int k = 0; k < 4; ++k) dyr[ch][k] = 0.f;
+  if (act) {
+    for (int a = 0; a < naxis; ++a) {
+      const float x0 = s_x[a], x1 = s_x[M + a], x2 = s_x[2 * M + a], x3 = s_x[3 * M + a];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) d[k] += s_t[k * naxis + m];
+      for (int ch = 0; ch < 4; ++ch) {
+        const float g = s_d[(m0 + ch) * ldd + a];
+        dyr[ch][0] += g * x0;
+        dyr[ch][1] += g * x1;
+        dyr[ch][2] += g * x2;
+        dyr[ch][3] += g * x3;
       }
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) dyr[ch][k] = d[k] * inv_nnei;
+    for (int ch = 0; ch < 4; ++ch) {
+      const int m = m0 + ch;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (m < naxis) dyr[ch][k] += s_t[k * naxis + m];
+        dyr[ch][k] *= inv_nnei;
+      }
+    }
   }
   __syncwarp();  // dD tile dead: stage the slots in its place
   float4* se = reinterpret_cast<float4*>(s_d);
@@ -326,9 +370,14 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
     const int last = brk < nt ? brk : nt - 1;
     const float* tab = tt.table[t] + m0;
     const size_t rs = (size_t)M * 6;
-    int ci = __float_as_int(sl[s0].x);
-    Coef4 cc;
-    if (act) cc = load_coef4(tab + (size_t)ci * rs, M);
+    const float4* E = se + s0;
+    const float4* Ls = sl + s0;
+    auto rep = [&](int q) { return q == brk ? (float)(nt - q) : 1.f; };
+    auto row = [&](int q) { return tab + (size_t)__float_as_int(Ls[q].x) * rs; };
+    // two coefficient buffers in turn (GRP is even, so slot parity fixes the
+    // buffer): the next slot's row is in flight while the current one is used
+    Coef4 ca, cb;
+    if (act) ca = load_coef4(row(0), M);
     for (int g0 = 0; g0 < nt; g0 += GRP) {
       float P[GRP][5];
 #pragma unroll
@@ -336,37 +385,14 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
 #pragma unroll
         for (int k = 0; k < 5; ++k) P[q][k] = 0.f;
         const int qq = g0 + q;
-        if (qq <= last) {  // warp-uniform
-          int ni = ci;
-          Coef4 cn = cc;
-          if (qq < last) {
-            ni = __float_as_int(sl[s0 + qq + 1].x);
-            if (ni != ci && act) cn = load_coef4(tab + (size_t)ni * rs, M);
+        if (qq <= last && act) {  // warp-uniform apart from the idle lanes
+          if ((q & 1) == 0) {
+            if (qq + 1 <= last) cb = load_coef4(row(qq + 1), M);
+            bwd_slot(P[q], ca, E[qq], Ls[qq], rep(qq), dyr);
+          } else {
+            if (qq + 1 <= last) ca = load_coef4(row(qq + 1), M);
+            bwd_slot(P[q], cb, E[qq], Ls[qq], rep(qq), dyr);
           }
-          if (act) {
-            const float4 e = se[s0 + qq];
-            const float4 L = sl[s0 + qq];
-#pragma unroll
-            for (int ch = 0; ch < 4; ++ch) {
-              float v, g;
-              hvalgrad(cc, ch, L.y, v, g);
-              v = v + g * L.z;
-              const float dot =
-                  e.x * dyr[ch][0] + e.y * dyr[ch][1] + e.z * dyr[ch][2] + e.w * dyr[ch][3];
-              P[q][0] += g * dot;
-              P[q][1] += v * dyr[ch][0];
-              P[q][2] += v * dyr[ch][1];
-              P[q][3] += v * dyr[ch][2];
-              P[q][4] += v * dyr[ch][3];
-            }
-          }
-          if (qq == brk) {
-            const float rep = (float)(nt - qq);
-#pragma unroll
-            for (int k = 0; k < 5; ++k) P[q][k] *= rep;
-          }
-          cc = cn;
-          ci = ni;
         }
       }
       // reduce-scatter of the 8 x 5 partials over the warp: after the xor-16,
