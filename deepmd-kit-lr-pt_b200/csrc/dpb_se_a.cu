@@ -89,46 +89,47 @@ __device__ __forceinline__ int block_fold(const float4* e4, int n, int lane) {
 // contiguous 4M-byte segment of the row (M % 4 == 0 keeps them 16-byte
 // aligned).
 struct Coef4 {
-  float4 q[6];
+  float2 lo[6];  // a_k of channels (0, 1)
+  float2 hi[6];  // a_k of channels (2, 3)
 };
 
 __device__ __forceinline__ Coef4 load_coef4(const float* row, int M) {
   Coef4 c;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) c.q[k] = __ldg(reinterpret_cast<const float4*>(row + k * M));
+  for (int k = 0; k < 6; ++k) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(row + k * M));
+    c.lo[k] = make_float2(v.x, v.y);
+    c.hi[k] = make_float2(v.z, v.w);
+  }
   return c;
 }
 
-// coefficient a_k of channel ch (0..3)
-__device__ __forceinline__ float cf(const Coef4& c, int ch, int k) {
-  const float4& v = c.q[k];
-  switch (ch) {
-    case 0: return v.x;
-    case 1: return v.y;
-    case 2: return v.z;
-    default: return v.w;
-  }
-}
+// Two channels per instruction with the sm_100 packed FP32 operations
+// (__ffma2_rn and friends: per component exactly __fmaf_rn / __fmul_rn /
+// __fadd_rn).
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
 // value only: a0 + (a1 + (a2 + (a3 + (a4 + a5 x) x) x) x) x  (tabulate.cc:123-130)
-__device__ __forceinline__ float hval(const Coef4& c, int ch, float x) {
-  return cf(c, ch, 0) +
-         (cf(c, ch, 1) +
-          (cf(c, ch, 2) + (cf(c, ch, 3) + (cf(c, ch, 4) + cf(c, ch, 5) * x) * x) * x) * x) * x;
+__device__ __forceinline__ float2 hval2(const float2 (&c)[6], float2 x) {
+  float2 p = __ffma2_rn(c[5], x, c[4]);
+  p = __ffma2_rn(p, x, c[3]);
+  p = __ffma2_rn(p, x, c[2]);
+  p = __ffma2_rn(p, x, c[1]);
+  return __ffma2_rn(p, x, c[0]);
 }
 
 // value and derivative by the joint Horner recurrence (9 FMA)
-__device__ __forceinline__ void hvalgrad(const Coef4& c, int ch, float x, float& v, float& g) {
-  float p = cf(c, ch, 5), d = p;
-  p = p * x + cf(c, ch, 4);
-  d = d * x + p;
-  p = p * x + cf(c, ch, 3);
-  d = d * x + p;
-  p = p * x + cf(c, ch, 2);
-  d = d * x + p;
-  p = p * x + cf(c, ch, 1);
-  d = d * x + p;
-  v = p * x + cf(c, ch, 0);
+__device__ __forceinline__ void hvalgrad2(const float2 (&c)[6], float2 x, float2& v, float2& g) {
+  float2 p = c[5], d = c[5];
+  p = __ffma2_rn(p, x, c[4]);
+  d = __ffma2_rn(d, x, p);
+  p = __ffma2_rn(p, x, c[3]);
+  d = __ffma2_rn(d, x, p);
+  p = __ffma2_rn(p, x, c[2]);
+  d = __ffma2_rn(d, x, p);
+  p = __ffma2_rn(p, x, c[1]);
+  d = __ffma2_rn(d, x, p);
+  v = __ffma2_rn(p, x, c[0]);
   g = d;
 }
 
@@ -163,28 +164,31 @@ static size_t bwd_smem_floats(int M, int nnei, int naxis) {
 }
 
 // one neighbor slot of the forward: G row of 4 channels (fold multiplier at
-// the fold slot) times the env row, accumulated into acc[channel][k]
-__device__ __forceinline__ void fwd_slot(float (&acc)[4][4], const Coef4& c, const float4 e,
-                                         const float4 L, float rep) {
-  float v[4];
+// the fold slot) times the env row, accumulated into acc01[k] / acc23[k]
+// (channel pairs (0, 1) and (2, 3) of env column k)
+__device__ __forceinline__ void fwd_slot(float2 (&acc01)[4], float2 (&acc23)[4], const Coef4& c,
+                                         const float4 e, const float4 L, float rep) {
+  const float2 x = f2(L.y);
+  float2 v01, v23;
   if (L.z == 0.f) {
-#pragma unroll
-    for (int ch = 0; ch < 4; ++ch) v[ch] = hval(c, ch, L.y);
+    v01 = hval2(c.lo, x);
+    v23 = hval2(c.hi, x);
   } else {  // linear extrapolation outside the table (tabulate.cc:133-144)
-#pragma unroll
-    for (int ch = 0; ch < 4; ++ch) {
-      float g;
-      hvalgrad(c, ch, L.y, v[ch], g);
-      v[ch] = v[ch] + g * L.z;
-    }
+    float2 g01, g23;
+    hvalgrad2(c.lo, x, v01, g01);
+    hvalgrad2(c.hi, x, v23, g23);
+    v01 = __ffma2_rn(g01, f2(L.z), v01);
+    v23 = __ffma2_rn(g23, f2(L.z), v23);
   }
+  if (rep != 1.f) {
+    v01 = __fmul2_rn(v01, f2(rep));
+    v23 = __fmul2_rn(v23, f2(rep));
+  }
+  const float ek[4] = {e.x, e.y, e.z, e.w};
 #pragma unroll
-  for (int ch = 0; ch < 4; ++ch) {
-    const float u = v[ch] * rep;
-    acc[ch][0] += u * e.x;
-    acc[ch][1] += u * e.y;
-    acc[ch][2] += u * e.z;
-    acc[ch][3] += u * e.w;
+  for (int k = 0; k < 4; ++k) {
+    acc01[k] = __ffma2_rn(v01, f2(ek[k]), acc01[k]);
+    acc23[k] = __ffma2_rn(v23, f2(ek[k]), acc23[k]);
   }
 }
 
@@ -221,11 +225,9 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
   __syncwarp();
   const int m0 = 4 * lane;
   const bool act = m0 < M;
-  float acc[4][4];
+  float2 acc01[4], acc23[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc[c][k] = 0.f;
+  for (int k = 0; k < 4; ++k) acc01[k] = acc23[k] = make_float2(0.f, 0.f);
   for (int t = 0; t < tt.ntypes; ++t) {
     const int s0 = tt.sec[t], nt = tt.sec[t + 1] - s0;
     if (nt <= 0) continue;
@@ -239,16 +241,18 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
     auto rep = [&](int q) { return q == brk ? (float)(nt - q) : 1.f; };
     auto row = [&](int q) { return tab + (size_t)__float_as_int(Ls[q].x) * rs; };
     // two coefficient buffers in turn: the next slot's row is in flight while
-    // the current one is evaluated
+    // the current one is evaluated (reusing a row shared by consecutive slots
+    // saves L1 traffic but costs the prefetch distance, a net loss measured
+    // on 12k-atom water)
     Coef4 ca = load_coef4(row(0), M), cb;
     int q = 0;
     for (; q + 1 <= last; q += 2) {
       cb = load_coef4(row(q + 1), M);
-      fwd_slot(acc, ca, E[q], Ls[q], rep(q));
+      fwd_slot(acc01, acc23, ca, E[q], Ls[q], rep(q));
       if (q + 2 <= last) ca = load_coef4(row(q + 2), M);
-      fwd_slot(acc, cb, E[q + 1], Ls[q + 1], rep(q + 1));
+      fwd_slot(acc01, acc23, cb, E[q + 1], Ls[q + 1], rep(q + 1));
     }
-    if (q <= last) fwd_slot(acc, ca, E[q], Ls[q], rep(q));
+    if (q <= last) fwd_slot(acc01, acc23, ca, E[q], Ls[q], rep(q));
   }
   __syncwarp();  // the slot staging is reused for x below
   float* sx = wsm;  // [4][M]
@@ -256,8 +260,8 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
   if (act) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      float4 o = make_float4(acc[0][k] * inv_nnei, acc[1][k] * inv_nnei, acc[2][k] * inv_nnei,
-                             acc[3][k] * inv_nnei);
+      float4 o = make_float4(acc01[k].x * inv_nnei, acc01[k].y * inv_nnei,
+                             acc23[k].x * inv_nnei, acc23[k].y * inv_nnei);
       *reinterpret_cast<float4*>(xo + k * M + m0) = o;
       *reinterpret_cast<float4*>(sx + k * M + m0) = o;
     }
@@ -266,30 +270,42 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
   write_descriptor(D + (size_t)drow[i] * M * naxis, sx, M, naxis, lane);
 }
 
-constexpr int GRP = 8;  // neighbors reduced together in the backward (even)
+constexpr int GRP = 4;  // neighbors reduced together in the backward (even)
 
 // one neighbor slot of the backward: P[0] = sum_c G'_c (e . dyr_c), P[1 + d] =
-// sum_c G_c dyr_c[d] over this lane's 4 channels (times the fold multiplier)
+// sum_c G_c dyr_c[d] over this lane's 4 channels (times the fold multiplier);
+// dyr01[d] / dyr23[d] hold dyr of channel pairs (0, 1) / (2, 3)
 __device__ __forceinline__ void bwd_slot(float (&P)[5], const Coef4& c, const float4 e,
-                                         const float4 L, float rep,
-                                         const float (&dyr)[4][4]) {
+                                         const float4 L, float rep, const float2 (&dyr01)[4],
+                                         const float2 (&dyr23)[4]) {
+  const float2 x = f2(L.y), dl = f2(L.z);
+  float2 v01, g01, v23, g23;
+  hvalgrad2(c.lo, x, v01, g01);
+  hvalgrad2(c.hi, x, v23, g23);
+  v01 = __ffma2_rn(g01, dl, v01);
+  v23 = __ffma2_rn(g23, dl, v23);
+  float2 d01 = __fmul2_rn(dyr01[0], f2(e.x));
+  float2 d23 = __fmul2_rn(dyr23[0], f2(e.x));
+  d01 = __ffma2_rn(dyr01[1], f2(e.y), d01);
+  d23 = __ffma2_rn(dyr23[1], f2(e.y), d23);
+  d01 = __ffma2_rn(dyr01[2], f2(e.z), d01);
+  d23 = __ffma2_rn(dyr23[2], f2(e.z), d23);
+  d01 = __ffma2_rn(dyr01[3], f2(e.w), d01);
+  d23 = __ffma2_rn(dyr23[3], f2(e.w), d23);
+  const float2 p0 = __ffma2_rn(g23, d23, __fmul2_rn(g01, d01));
+  P[0] = p0.x + p0.y;
 #pragma unroll
-  for (int ch = 0; ch < 4; ++ch) {
-    float v, g;
-    hvalgrad(c, ch, L.y, v, g);
-    v = v + g * L.z;
-    const float dot = e.x * dyr[ch][0] + e.y * dyr[ch][1] + e.z * dyr[ch][2] + e.w * dyr[ch][3];
-    P[0] += g * dot;
-    P[1] += v * dyr[ch][0];
-    P[2] += v * dyr[ch][1];
-    P[3] += v * dyr[ch][2];
-    P[4] += v * dyr[ch][3];
+  for (int d = 0; d < 4; ++d) {
+    const float2 pd = __ffma2_rn(v23, dyr23[d], __fmul2_rn(v01, dyr01[d]));
+    P[1 + d] = pd.x + pd.y;
   }
+  if (rep != 1.f) {
 #pragma unroll
-  for (int k = 0; k < 5; ++k) P[k] *= rep;
+    for (int k = 0; k < 5; ++k) P[k] *= rep;
+  }
 }
 
-__global__ void __launch_bounds__(SW * 32)
+__global__ void __launch_bounds__(SW * 32, 5)
 k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
            const int* __restrict__ drow, const float* __restrict__ xyz,
            const float* __restrict__ em, TypeTables tt, int nloc, int M, int naxis,
@@ -356,13 +372,19 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
       }
     }
   }
+  float2 dyr01[4], dyr23[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    dyr01[k] = make_float2(dyr[0][k], dyr[1][k]);
+    dyr23[k] = make_float2(dyr[2][k], dyr[3][k]);
+  }
   __syncwarp();  // dD tile dead: stage the slots in its place
   float4* se = reinterpret_cast<float4*>(s_d);
   float4* sl = se + nnei;
   stage_slots(se, sl, reinterpret_cast<const float4*>(em + (size_t)i * nnei * 4), tt, lane);
   __syncwarp();
   float4* nrow = reinterpret_cast<float4*>(net_deriv + (size_t)i * nnei * 4);
-  const int b4 = (lane >> 4) & 1, b3 = (lane >> 3) & 1, b2 = (lane >> 2) & 1;
+  const int b4 = (lane >> 4) & 1, b3 = (lane >> 3) & 1;
   for (int t = 0; t < tt.ntypes; ++t) {
     const int s0 = tt.sec[t], nt = tt.sec[t + 1] - s0;
     if (nt <= 0) continue;
@@ -379,6 +401,11 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
     Coef4 ca, cb;
     if (act) ca = load_coef4(row(0), M);
     for (int g0 = 0; g0 < nt; g0 += GRP) {
+      if (g0 > last) {  // beyond the fold point: zero rows
+        for (int qq = g0 + lane; qq < nt && qq < g0 + GRP; qq += 32)
+          nrow[s0 + qq] = make_float4(0.f, 0.f, 0.f, 0.f);
+        continue;
+      }
       float P[GRP][5];
 #pragma unroll
       for (int q = 0; q < GRP; ++q) {
@@ -388,46 +415,38 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
         if (qq <= last && act) {  // warp-uniform apart from the idle lanes
           if ((q & 1) == 0) {
             if (qq + 1 <= last) cb = load_coef4(row(qq + 1), M);
-            bwd_slot(P[q], ca, E[qq], Ls[qq], rep(qq), dyr);
+            bwd_slot(P[q], ca, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
           } else {
             if (qq + 1 <= last) ca = load_coef4(row(qq + 1), M);
-            bwd_slot(P[q], cb, E[qq], Ls[qq], rep(qq), dyr);
+            bwd_slot(P[q], cb, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
           }
         }
       }
-      // reduce-scatter of the 8 x 5 partials over the warp: after the xor-16,
-      // -8 and -4 steps lane L holds neighbor q = 4*b4 + 2*b3 + b2 summed over
-      // 8 lanes; xor-2 and xor-1 finish the sum in every lane of the quad.
-      float R1[4][5];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          const float mine = b4 ? P[4 + q][k] : P[q][k];
-          const float other = b4 ? P[q][k] : P[4 + q][k];
-          R1[q][k] = mine + __shfl_xor_sync(0xffffffffu, other, 16);
-        }
-      float R2[2][5];
+      // reduce-scatter of the 4 x 5 partials over the warp: after the xor-16
+      // and -8 steps lane L holds neighbor q = 2*b4 + b3 summed over 8 lanes;
+      // xor-4, -2 and -1 finish the sum in every lane of the group of 8.
+      float R1[2][5];
 #pragma unroll
       for (int q = 0; q < 2; ++q)
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-          const float mine = b3 ? R1[2 + q][k] : R1[q][k];
-          const float other = b3 ? R1[q][k] : R1[2 + q][k];
-          R2[q][k] = mine + __shfl_xor_sync(0xffffffffu, other, 8);
+          const float mine = b4 ? P[2 + q][k] : P[q][k];
+          const float other = b4 ? P[q][k] : P[2 + q][k];
+          R1[q][k] = mine + __shfl_xor_sync(0xffffffffu, other, 16);
         }
-      float R3[5];
+      float R2[5];
 #pragma unroll
       for (int k = 0; k < 5; ++k) {
-        const float mine = b2 ? R2[1][k] : R2[0][k];
-        const float other = b2 ? R2[0][k] : R2[1][k];
-        R3[k] = mine + __shfl_xor_sync(0xffffffffu, other, 4);
-        R3[k] += __shfl_xor_sync(0xffffffffu, R3[k], 2);
-        R3[k] += __shfl_xor_sync(0xffffffffu, R3[k], 1);
+        const float mine = b3 ? R1[1][k] : R1[0][k];
+        const float other = b3 ? R1[0][k] : R1[1][k];
+        R2[k] = mine + __shfl_xor_sync(0xffffffffu, other, 8);
+        R2[k] += __shfl_xor_sync(0xffffffffu, R2[k], 4);
+        R2[k] += __shfl_xor_sync(0xffffffffu, R2[k], 2);
+        R2[k] += __shfl_xor_sync(0xffffffffu, R2[k], 1);
       }
-      const int qq = g0 + 4 * b4 + 2 * b3 + b2;
-      if ((lane & 3) == 0 && qq < nt)  // zero beyond the fold point
-        nrow[s0 + qq] = make_float4(R3[1] + R3[0], R3[2], R3[3], R3[4]);
+      const int qq = g0 + 2 * b4 + b3;
+      if ((lane & 7) == 0 && qq < nt)  // zero beyond the fold point
+        nrow[s0 + qq] = make_float4(R2[1] + R2[0], R2[2], R2[3], R2[4]);
     }
   }
 }
