@@ -166,7 +166,7 @@ __device__ __forceinline__ float tf32_hi(float x) {
   return __uint_as_float(r);
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int MODE>
 __global__ void __launch_bounds__(GT_THREADS, STAGES <= 2 ? 2 : 1)
 k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi, int* status) {
   constexpr int A_BYTES = GT_BM * GT_BK * 4;  // 16 KB
@@ -291,97 +291,83 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&conv_bar[s]);
     }
-    // epilogue: warp (warp % 4) owns TMEM lanes 32 * (warp % 4) ...
+    // epilogue: warp (warp % 4) owns TMEM lanes 32 * (warp % 4) ..., one row
+    // per thread; each 16-column chunk moves as 4 x 16-byte loads / stores
+    // per operand (64 contiguous bytes per thread and row)
     bool have = mbar_wait(&acc_bar, 0, abort) && !*abort;
     have = __shfl_sync(0xffffffffu, have ? 1 : 0, 0) != 0;  // tcgen05.ld is warp-wide
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (have) {
-      // TMEM -> registers (one row per thread) -> a 32 x 16 staging tile in
-      // the now idle pipeline shared memory -> coalesced row segments: each
-      // half-warp handles one row, 16 consecutive columns per instruction.
-      const int wq = warp & 3;
-      const int lane_base = 32 * wq;
-      float* stg = reinterpret_cast<float*>(smem) + wq * (32 * 17 + 32);
-      float* erow = stg + 32 * 17;
-      erow[lane] = 0.f;
+      const int lane_base = 32 * (warp & 3);
+      const int row = row0 + lane_base + lane;
+      const bool ok = row < row_end;
+      const size_t at = (size_t)(ok ? row : row0) * epi.ld + n0;
       const float* bias = epi.bias[ty];
       const float* idt = epi.idt[ty];
       const float* wv = epi.w[ty];
-      const int half = lane >> 4, cl = lane & 15;
+      constexpr bool NEED0 = MODE >= EPI_RES_DT, NEED1 = MODE == EPI_BWD_RES;
+      float esum = 0.f;
+#pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 16) {
+        float4 x0[4], x1[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {  // in flight during the TMEM load
+          x0[j] = x1[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (NEED0 && ok) x0[j] = __ldg(reinterpret_cast<const float4*>(epi.aux0 + at + c0) + j);
+          if (NEED1 && ok) x1[j] = __ldg(reinterpret_cast<const float4*>(epi.aux1 + at + c0) + j);
+        }
         float v[16];
         tmem_ld16(tmem + ((uint32_t)lane_base << 16) + (uint32_t)c0, v);
-        __syncwarp();
 #pragma unroll
-        for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = v[j];
-        __syncwarp();
-        const int col = n0 + c0 + cl;
-        float bcol = 0.f, dcol = 0.f, wcol = 0.f;
-        if (bias) bcol = bias[col];
-        if (idt) dcol = idt[col];
-        if (wv) wcol = wv[col];
-        // gather the chunk's 16 rows per half-warp first (independent loads in
-        // flight), then compute and store
-        const int mode = epi.mode;
-        const bool need0 = mode >= EPI_RES_DT, need1 = mode == EPI_BWD_RES;
-        float x0[16], x1[16];
+        for (int j = 0; j < 4; ++j) {
+          const int cj = n0 + c0 + 4 * j;
+          float4 bb = make_float4(0.f, 0.f, 0.f, 0.f), dd = bb, ww = bb;
+          if (MODE == EPI_TANH || MODE == EPI_RES_DT || MODE == EPI_LAST)
+            bb = __ldg(reinterpret_cast<const float4*>(bias + cj));
+          if (MODE == EPI_RES_DT || MODE == EPI_LAST || MODE == EPI_BWD_DT)
+            dd = __ldg(reinterpret_cast<const float4*>(idt + cj));
+          if (MODE == EPI_LAST || MODE == EPI_BWD_DT)
+            ww = __ldg(reinterpret_cast<const float4*>(wv + cj));
+          const float a[4] = {v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]};
+          const float b4[4] = {bb.x, bb.y, bb.z, bb.w}, d4[4] = {dd.x, dd.y, dd.z, dd.w};
+          const float w4[4] = {ww.x, ww.y, ww.z, ww.w};
+          const float p0[4] = {x0[j].x, x0[j].y, x0[j].z, x0[j].w};
+          const float p1[4] = {x1[j].x, x1[j].y, x1[j].z, x1[j].w};
+          float o0[4], o1[4];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int row = row0 + lane_base + 2 * q + half;
-          const size_t at = (size_t)row * epi.ld + col;
-          const bool ok = row < row_end;
-          x0[q] = (need0 && ok) ? epi.aux0[at] : 0.f;
-          x1[q] = (need1 && ok) ? epi.aux1[at] : 0.f;
-        }
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int r = 2 * q + half;
-          const int row = row0 + lane_base + r;
-          const float a = stg[r * 17 + cl];
-          const bool ok = row < row_end;
-          const size_t at = (size_t)row * epi.ld + col;
-          switch (mode) {
-            case EPI_STORE:
-              if (ok) epi.out0[at] = a;
-              break;
-            case EPI_TANH:
-              if (ok) epi.out0[at] = tanhf(a + bcol);
-              break;
-            case EPI_RES_DT: {
-              const float y = tanhf(a + bcol);
-              if (ok) {
-                epi.out0[at] = y;
-                epi.out1[at] = x0[q] + dcol * y;
-              }
-            } break;
-            case EPI_LAST: {
-              const float y = tanhf(a + bcol);
-              const float h = x0[q] + dcol * y;
-              if (ok) epi.out0[at] = wcol * dcol * (1.f - y * y);
-              float pe = ok ? h * wcol : 0.f;  // this row's energy share, 16 columns
-              pe += __shfl_xor_sync(0xffffffffu, pe, 8);
-              pe += __shfl_xor_sync(0xffffffffu, pe, 4);
-              pe += __shfl_xor_sync(0xffffffffu, pe, 2);
-              pe += __shfl_xor_sync(0xffffffffu, pe, 1);
-              if (cl == 0) erow[r] += pe;
-            } break;
-            case EPI_BWD_DT: {
-              const float g = wcol + a;
-              if (ok) {
-                epi.out1[at] = g;
-                epi.out0[at] = g * dcol * (1.f - x0[q] * x0[q]);
-              }
-            } break;
-            default: {  // EPI_BWD_RES
-              const float g = x1[q] + a;
-              if (ok) epi.out0[at] = g * (1.f - x0[q] * x0[q]);
-            } break;
+          for (int u = 0; u < 4; ++u) {
+            if (MODE == EPI_STORE) {
+              o0[u] = a[u];
+            } else if (MODE == EPI_TANH) {
+              o0[u] = tanhf(a[u] + b4[u]);
+            } else if (MODE == EPI_RES_DT) {
+              const float y = tanhf(a[u] + b4[u]);
+              o0[u] = y;
+              o1[u] = p0[u] + d4[u] * y;
+            } else if (MODE == EPI_LAST) {
+              const float y = tanhf(a[u] + b4[u]);
+              const float h = p0[u] + d4[u] * y;
+              esum += h * w4[u];
+              o0[u] = w4[u] * d4[u] * (1.f - y * y);
+            } else if (MODE == EPI_BWD_DT) {
+              const float g = w4[u] + a[u];
+              o1[u] = g;
+              o0[u] = g * d4[u] * (1.f - p0[u] * p0[u]);
+            } else {  // EPI_BWD_RES
+              const float g = p1[u] + a[u];
+              o0[u] = g * (1.f - p0[u] * p0[u]);
+            }
+          }
+          if (ok) {
+            reinterpret_cast<float4*>(epi.out0 + at + c0)[j] =
+                make_float4(o0[0], o0[1], o0[2], o0[3]);
+            if (MODE == EPI_RES_DT || MODE == EPI_BWD_DT)
+              reinterpret_cast<float4*>(epi.out1 + at + c0)[j] =
+                  make_float4(o1[0], o1[1], o1[2], o1[3]);
           }
         }
       }
-      __syncwarp();
-      if (epi.mode == EPI_LAST && row0 + lane_base + lane < row_end)
-        atomicAdd(&epi.e[row0 + lane_base + lane], erow[lane]);
+      if (MODE == EPI_LAST && ok) atomicAdd(&epi.e[row], esum);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -395,6 +381,22 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
 }
 
 // ---------------------------------------------------------------- host -----
+template <int BN, int STAGES, int MODE>
+static int launch_mode(const struct GemmMaps& maps, const struct GemmShape& shp,
+                       const struct GemmEpi& epi, int* status, cudaStream_t st);
+
+template <int BN, int STAGES>
+static int launch(const GemmMaps& maps, const GemmShape& shp, const GemmEpi& epi, int* status,
+                  cudaStream_t st) {
+  switch (epi.mode) {
+    case EPI_STORE: return launch_mode<BN, STAGES, EPI_STORE>(maps, shp, epi, status, st);
+    case EPI_TANH: return launch_mode<BN, STAGES, EPI_TANH>(maps, shp, epi, status, st);
+    case EPI_RES_DT: return launch_mode<BN, STAGES, EPI_RES_DT>(maps, shp, epi, status, st);
+    case EPI_LAST: return launch_mode<BN, STAGES, EPI_LAST>(maps, shp, epi, status, st);
+    case EPI_BWD_DT: return launch_mode<BN, STAGES, EPI_BWD_DT>(maps, shp, epi, status, st);
+    default: return launch_mode<BN, STAGES, EPI_BWD_RES>(maps, shp, epi, status, st);
+  }
+}
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
@@ -432,16 +434,16 @@ static int make_map(CUtensorMap* m, const float* base, int rows, int cols, int b
   return DPB_OK;
 }
 
-template <int BN, int STAGES>
-static int launch(const GemmMaps& maps, const GemmShape& shp, const GemmEpi& epi, int* status,
-                  cudaStream_t st) {
+template <int BN, int STAGES, int MODE>
+static int launch_mode(const GemmMaps& maps, const GemmShape& shp, const GemmEpi& epi,
+                       int* status, cudaStream_t st) {
   constexpr int SMEM = STAGES * (2 * GT_BM * GT_BK * 4 + 2 * BN * GT_BK * 4) + 1024;
-  DPB_CUDA(cudaFuncSetAttribute(k_gemm_tf32x3<BN, STAGES>,
+  DPB_CUDA(cudaFuncSetAttribute(k_gemm_tf32x3<BN, STAGES, MODE>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM),
            "gemm");
   const int tiles = shp.tile_start[shp.ntypes] * shp.n_tiles;
   if (tiles == 0) return DPB_OK;
-  k_gemm_tf32x3<BN, STAGES><<<tiles, GT_THREADS, SMEM, st>>>(maps, shp, epi, status);
+  k_gemm_tf32x3<BN, STAGES, MODE><<<tiles, GT_THREADS, SMEM, st>>>(maps, shp, epi, status);
   DPB_CHECK_LAUNCH("gemm_tf32x3");
   return DPB_OK;
 }
@@ -491,6 +493,15 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
   for (int t = 0; t < ntypes; ++t) {
     if ((rc = make_map(&maps.bh[t], b_hi[t], N, K, BN))) return rc;
     if ((rc = make_map(&maps.bl[t], b_lo[t], N, K, BN))) return rc;
+  }
+  auto misaligned = [](const void* q) { return ((uintptr_t)q & 15) != 0; };
+  bool bad = misaligned(out0) || misaligned(out1) || misaligned(aux0) || misaligned(aux1);
+  for (int t = 0; t < ntypes; ++t)
+    bad = bad || (bias && misaligned(bias[t])) || (idt && misaligned(idt[t])) ||
+          (w && misaligned(w[t]));
+  if (bad) {
+    set_error("gemm_tf32x3: outputs, aux operands and per-type vectors must be 16-byte aligned");
+    return DPB_ERR_INVALID;
   }
   GemmEpi ep{};
   ep.mode = mode;
