@@ -72,6 +72,43 @@ __device__ __forceinline__ T warp_sum(T v) {
 __device__ __forceinline__ void atomic_add(double* p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add(float* p, float v) { atomicAdd(p, v); }
 
+// Adds the nine per-lane partial sums vs of every warp of the block to
+// out[0..8] with one atomic per component and block: a warp butterfly, then
+// the NW warps' sums through shared memory. Every thread of the block must
+// call it (it synchronises the block).
+template <int NW, typename T>
+__device__ __forceinline__ void block_add9(const T (&vs)[9], T* out) {
+  __shared__ T s9[NW][9];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const T s = warp_sum(vs[k]);
+    if (lane == 0) s9[w][k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    T t = (T)0.;
+#pragma unroll
+    for (int q = 0; q < NW; ++q) t += s9[q][threadIdx.x];
+    atomic_add(&out[threadIdx.x], t);
+  }
+}
+
+// Blocks for a grid-stride kernel of `per_block` items per block pass: the
+// item count, capped at 8 blocks per SM.
+inline int grid_stride_blocks(long long items, int per_block) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms <= 0)
+      sms = 148;
+  }
+  const long long need = (items + per_block - 1) / per_block;
+  return (int)(need < (long long)sms * 8 ? need : (long long)sms * 8);
+}
+
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 }  // namespace dpb

@@ -5,8 +5,8 @@
 // slot's 4 net_deriv values with its 4x3 em_deriv block into the pair force
 // f_jj = sum_a nd[a] * ed[a, :]. The center force is -sum_jj f_jj (a warp
 // butterfly, no atomics), the neighbor gets +f_jj (one atomic per component),
-// and the pair virial f_jj (x) rij is reduced per warp before one atomic per
-// component. References: source/lib/src/prod_force.cc:23-72 and
+// and the pair virial f_jj (x) rij is reduced per block (warps stride over
+// the center atoms) before one atomic per component. References: source/lib/src/prod_force.cc:23-72 and
 // source/lib/src/prod_virial.cc:22-69 (sign conventions included).
 #include "dpb_common.cuh"
 
@@ -61,14 +61,13 @@ k_prod_virial(T* __restrict__ virial, T* __restrict__ atom_virial,
               const T* __restrict__ rij, const int* __restrict__ nlist,
               int nloc, int nnei) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * FW + w;
-  if (i >= nloc) return;
-  const T* ndr = nd + (size_t)i * nnei * 4;
-  const T* edr = ed + (size_t)i * nnei * 12;
-  const T* rr = rij + (size_t)i * nnei * 3;
   T vs[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) vs[k] = (T)0.;
+  for (int i = blockIdx.x * FW + w; i < nloc; i += gridDim.x * FW) {
+  const T* ndr = nd + (size_t)i * nnei * 4;
+  const T* edr = ed + (size_t)i * nnei * 12;
+  const T* rr = rij + (size_t)i * nnei * 3;
   for (int jj = lane; jj < nnei; jj += 32) {
     const int j = nlist[(size_t)i * nnei + jj];
     if (j < 0) continue;
@@ -89,11 +88,8 @@ k_prod_virial(T* __restrict__ virial, T* __restrict__ atom_virial,
         atomic_add(&atom_virial[(size_t)j * 9 + d0 * 3 + d1], v);
       }
   }
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    T s = warp_sum(vs[k]);
-    if (lane == 0) atomic_add(&virial[k], s);
   }
+  block_add9<FW>(vs, virial);
 }
 
 template <typename T>
@@ -128,7 +124,7 @@ static int prod_virial(T* virial, T* atom_virial, const T* nd, const T* ed,
     DPB_CUDA(cudaMemsetAsync(atom_virial, 0, sizeof(T) * 9 * (size_t)nall, st),
              "prod_virial_a");
   if (nloc == 0 || nnei == 0) return DPB_OK;
-  k_prod_virial<T><<<ceil_div(nloc, FW), FW * 32, 0, st>>>(virial, atom_virial, nd, ed,
+  k_prod_virial<T><<<grid_stride_blocks(nloc, FW), FW * 32, 0, st>>>(virial, atom_virial, nd, ed,
                                                            rij, nlist, nloc, nnei);
   DPB_CHECK_LAUNCH("prod_virial_a");
   return DPB_OK;

@@ -459,15 +459,14 @@ k_force_virial(double* __restrict__ force, double* __restrict__ virial,
                const int* __restrict__ nlist, const int* __restrict__ mapping,
                int nloc, int nnei) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * SW + w;
-  if (i >= nloc) return;
+  double vs[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) vs[k] = 0.;
+  for (int i = blockIdx.x * SW + w; i < nloc; i += gridDim.x * SW) {
   const T* ndr = nd + (size_t)i * nnei * 4;
   const T* edr = ed + (size_t)i * nnei * 12;
   const T* rr = rij + (size_t)i * nnei * 3;
   double c0 = 0., c1 = 0., c2 = 0.;
-  double vs[9];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) vs[k] = 0.;
   for (int jj = lane; jj < nnei; jj += 32) {
     T p[3] = {(T)0., (T)0., (T)0.};
 #pragma unroll
@@ -507,11 +506,8 @@ k_force_virial(double* __restrict__ force, double* __restrict__ virial,
     atomicAdd(&force[(size_t)i * 3 + 1], -c1);
     atomicAdd(&force[(size_t)i * 3 + 2], -c2);
   }
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    const double s = warp_sum(vs[k]);
-    if (lane == 0) atomicAdd(&virial[k], s);
   }
+  block_add9<SW>(vs, virial);
 }
 
 // Force and virial with em_deriv and rij recomputed from the coordinates and
@@ -524,7 +520,6 @@ k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
                   const int* __restrict__ type, const OT* __restrict__ std_,
                   const int* __restrict__ nlist, const int* __restrict__ mapping, int nloc,
                   int nnei, int ntypes, float rcut, float rcut_smth) {
-  __shared__ double s_v[SW][9];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // grid-stride over center atoms (one warp each); the virial stays in
   // registers across atoms and is reduced once per block, so the nine
@@ -577,32 +572,7 @@ k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
     atomicAdd(&force[(size_t)i * 3 + 2], -c2);
   }
   }
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    const double s = warp_sum(vs[k]);
-    if (lane == 0) s_v[w][k] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x < 9) {
-    double t = 0.;
-#pragma unroll
-    for (int q = 0; q < SW; ++q) t += s_v[q][threadIdx.x];
-    atomicAdd(&virial[threadIdx.x], t);
-  }
-}
-
-// blocks for the grid-stride force kernels: enough to fill every SM
-static int force_grid(int nloc) {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        sms <= 0)
-      sms = 148;
-  }
-  const int need = ceil_div(nloc, SW);
-  return need < sms * 8 ? need : sms * 8;
+  block_add9<SW>(vs, virial);
 }
 
 template <typename CT, typename OT>
@@ -617,7 +587,7 @@ static int force_virial_rc(double* force, double* virial, const OT* nd, const CT
   DPB_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * 3 * (size_t)nforce, st), "force_virial");
   DPB_CUDA(cudaMemsetAsync(virial, 0, sizeof(double) * 9, st), "force_virial");
   if (nloc == 0 || nnei == 0) return DPB_OK;
-  k_force_virial_rc<CT, OT><<<force_grid(nloc), SW * 32, 0, st>>>(
+  k_force_virial_rc<CT, OT><<<grid_stride_blocks(nloc, SW), SW * 32, 0, st>>>(
       force, virial, nd, coord, type, std_, nlist, mapping, nloc, nnei, ntypes, rcut, rcut_smth);
   DPB_CHECK_LAUNCH("force_virial_env");
   return DPB_OK;
@@ -794,7 +764,7 @@ int dpb_force_virial_a_f32(double* force, double* virial, double* atom_virial,
     DPB_CUDA(cudaMemsetAsync(atom_virial, 0, sizeof(double) * 9 * (size_t)nall, st),
              "force_virial");
   if (nloc <= 0 || nnei <= 0) return DPB_OK;
-  k_force_virial<float><<<ceil_div(nloc, SW), SW * 32, 0, st>>>(
+  k_force_virial<float><<<grid_stride_blocks(nloc, SW), SW * 32, 0, st>>>(
       force, virial, atom_virial, net_deriv, env_deriv, rij, nlist, mapping, nloc, nnei);
   DPB_CHECK_LAUNCH("force_virial");
   return DPB_OK;
@@ -811,7 +781,7 @@ int dpb_force_virial_a_f64(double* force, double* virial, double* atom_virial,
     DPB_CUDA(cudaMemsetAsync(atom_virial, 0, sizeof(double) * 9 * (size_t)nall, st),
              "force_virial");
   if (nloc <= 0 || nnei <= 0) return DPB_OK;
-  k_force_virial<double><<<ceil_div(nloc, SW), SW * 32, 0, st>>>(
+  k_force_virial<double><<<grid_stride_blocks(nloc, SW), SW * 32, 0, st>>>(
       force, virial, atom_virial, net_deriv, env_deriv, rij, nlist, mapping, nloc, nnei);
   DPB_CHECK_LAUNCH("force_virial");
   return DPB_OK;
