@@ -94,17 +94,23 @@ __device__ __forceinline__ void block_add9(const T (&vs)[9], T* out) {
   }
 }
 
+// SM count of the current device (looked up once per process)
+inline int sm_count() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+    sms = n;
+  }
+  return sms;
+}
+
 // Blocks for a grid-stride kernel of `per_block` items per block pass: the
 // item count, capped at 8 blocks per SM.
 inline int grid_stride_blocks(long long items, int per_block) {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        sms <= 0)
-      sms = 148;
-  }
+  const int sms = sm_count();
   const long long need = (items + per_block - 1) / per_block;
   return (int)(need < (long long)sms * 8 ? need : (long long)sms * 8);
 }

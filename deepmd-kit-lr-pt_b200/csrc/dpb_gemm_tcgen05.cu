@@ -9,14 +9,24 @@
 // product is Ah Bh + Al Bh + Ah Bl (the Al Bl term, ~2^-22 relative, is
 // dropped), accumulated in FP32 in tensor memory.
 //
-// CTA (192 threads, one per SM): warp 0 issues the TMA loads of a 4-stage ring
-// (A tile 128 x 32, B hi/lo tiles BN x 32, 128-byte swizzle); warps 2-5 split
-// the A tile into hi/lo in shared memory (an elementwise operation, so the
-// swizzled layout is preserved) and later run the epilogue from TMEM; one
-// elected lane of warp 1 issues tcgen05.mma (M=128, N=BN, K=8) and commits to
-// the ring's mbarriers. Every mbarrier wait is bounded: on time-out the CTA
-// raises an error bit in the caller's status word, stops issuing work and
-// frees its tensor memory before returning.
+// Persistent, warp-specialised CTA (one per SM, 320 threads) walking output
+// tiles of 128 rows x 80 columns:
+//   warp 0      TMA producer: A tile 128 x 32 and B hi/lo tiles 80 x 32 per
+//               k-block into a 4-stage shared-memory ring (128-byte swizzle);
+//   warps 2-5   split each A tile row by row (one row per thread) into TF32
+//               hi / lo and store both straight into tensor memory, so the
+//               MMAs read A from TMEM and only B from shared memory;
+//   warp 1      one elected lane issues tcgen05.mma (M=128, N=80, K=8) into
+//               one of two TMEM accumulators and commits to the ring's and
+//               the accumulator's mbarriers;
+//   warps 6-9   epilogue of the previous tile from the other accumulator
+//               (one row per thread, 16-byte loads / stores), overlapping the
+//               current tile's MMAs.
+// Tensor memory (512 columns): accumulators at columns 0 and 128, A stage s
+// hi / lo at 256 + 64 s and 256 + 64 s + 32. Every mbarrier wait is bounded:
+// on time-out the CTA raises an error bit in the caller's status word, stops
+// issuing work, waits (bounded) for its copies and MMAs in flight and frees
+// its tensor memory before returning.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <stdint.h>
@@ -25,11 +35,16 @@
 
 namespace dpb {
 
-constexpr int GT_THREADS = 192;
+constexpr int GT_THREADS = 320;
 constexpr int GT_BM = 128;
+constexpr int GT_BN = 80;
 constexpr int GT_BK = 32;  // 32 FP32 = one 128-byte swizzle row
+constexpr int GT_STAGES = 4;
 constexpr int GT_MAXT = 4;
 constexpr unsigned GT_WAIT_LIMIT = 1u << 24;
+constexpr uint32_t TM_COLS = 512;
+constexpr uint32_t TM_ACC = 128;  // column distance of the two accumulators
+constexpr uint32_t TM_A0 = 256;   // first A stage column
 
 enum : int {
   ST_MMA_TIMEOUT = 1 << 8,
@@ -62,7 +77,7 @@ struct GemmShape {
   int ntypes;
   int row_start[GT_MAXT + 1];
   int tile_start[GT_MAXT + 1];
-  int n_tiles;
+  int n_tiles;  // column tiles per row tile
   int N, K;
 };
 
@@ -129,14 +144,15 @@ __device__ __forceinline__ uint64_t smem_desc(const void* p) {
   return d;
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
-                                         uint32_t accumulate) {
+// D (TMEM) += A (TMEM, lanes = rows, one TF32 per column) x B (shared memory)
+__device__ __forceinline__ void mma_tf32_ta(uint32_t tmem_d, uint32_t tmem_a, uint64_t b,
+                                            uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-      ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u),
-      "r"(0u));
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u),
+      "r"(0u), "r"(0u));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
@@ -160,39 +176,62 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
 
+// 16 consecutive columns of this warp's 32 lanes, one row per thread
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15])
+      : "memory");
+}
+
 __device__ __forceinline__ float tf32_hi(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
 }
 
-template <int BN, int STAGES, int MODE>
-__global__ void __launch_bounds__(GT_THREADS, STAGES <= 2 ? 2 : 1)
+// tile t -> (type, first row, end of the type's rows, first column)
+struct TileCoord {
+  int ty, row0, row_end, n0;
+};
+__device__ __forceinline__ TileCoord tile_coord(const GemmShape& shp, int t) {
+  TileCoord c;
+  const int nt = t % shp.n_tiles, rt = t / shp.n_tiles;
+  int ty = 0;
+  while (ty + 1 < shp.ntypes && rt >= shp.tile_start[ty + 1]) ++ty;
+  c.ty = ty;
+  c.row0 = shp.row_start[ty] + (rt - shp.tile_start[ty]) * GT_BM;
+  c.row_end = shp.row_start[ty + 1];
+  c.n0 = nt * GT_BN;
+  return c;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(GT_THREADS, 1)
 k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi, int* status) {
+  constexpr int BN = GT_BN;
+  constexpr int STAGES = GT_STAGES;
   constexpr int A_BYTES = GT_BM * GT_BK * 4;  // 16 KB
-  constexpr int B_BYTES = BN * GT_BK * 4;
-  constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-  constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  constexpr int B_BYTES = BN * GT_BK * 4;     // 10 KB
+  constexpr int STAGE_BYTES = A_BYTES + 2 * B_BYTES;
   constexpr uint32_t IDESC = (1u << 4)            // D: FP32
                              | (2u << 7)          // A: TF32
                              | (2u << 10)         // B: TF32
                              | ((uint32_t)(BN >> 3) << 17)  // N
                              | ((uint32_t)(GT_BM >> 4) << 24);  // M = 128
+  static_assert(BN % 16 == 0 && BN <= (int)TM_ACC, "accumulator width");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t full_bar[STAGES], conv_bar[STAGES], empty_bar[STAGES];
-  __shared__ __align__(8) uint64_t acc_bar;
+  __shared__ __align__(8) uint64_t tfull_bar[2], tempty_bar[2], drain_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // tile of this CTA
-  const int nt = blockIdx.x % shp.n_tiles, rt = blockIdx.x / shp.n_tiles;
-  int ty = 0;
-  while (ty + 1 < shp.ntypes && rt >= shp.tile_start[ty + 1]) ++ty;
-  const int row0 = shp.row_start[ty] + (rt - shp.tile_start[ty]) * GT_BM;
-  const int row_end = shp.row_start[ty + 1];
-  const int n0 = nt * BN;
+  const int n_total = shp.tile_start[shp.ntypes] * shp.n_tiles;
   const int nk = (shp.K + GT_BK - 1) / GT_BK;
 
   if (threadIdx.x == 0) {
@@ -202,13 +241,17 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
       mbar_init(&conv_bar[s], 128);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(&acc_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], 128);
+    }
+    mbar_init(&drain_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      su32(&tmem_slot)),
-                 "r"(TMEM_COLS));
+                 "r"(TM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -220,92 +263,143 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
   if (warp == 0) {
     // ---------------------------------------------------------------- TMA
     if (lane == 0) {
-      int issued = 0;
-      for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % STAGES;
-        const uint32_t ph = (kb / STAGES) & 1;
-        if (!mbar_wait(&empty_bar[s], ph ^ 1, abort)) break;
-        unsigned char* st = smem + s * STAGE_BYTES;
-        mbar_expect_tx(&full_bar[s], A_BYTES + 2 * B_BYTES);
-        tma_load_2d(st, &maps.a, &full_bar[s], kb * GT_BK, row0);
-        tma_load_2d(st + 2 * A_BYTES, &maps.bh[ty], &full_bar[s], kb * GT_BK, n0);
-        tma_load_2d(st + 2 * A_BYTES + B_BYTES, &maps.bl[ty], &full_bar[s], kb * GT_BK, n0);
-        issued = kb + 1;
+      int g = 0;  // k-blocks issued over all tiles
+      bool ok = true;
+      for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x) {
+        const TileCoord tc = tile_coord(shp, t);
+        for (int kb = 0; kb < nk; ++kb, ++g) {
+          const int s = g % STAGES;
+          const uint32_t ph = (g / STAGES) & 1;
+          if (!mbar_wait(&empty_bar[s], ph ^ 1, abort)) {
+            ok = false;
+            break;
+          }
+          unsigned char* st = smem + s * STAGE_BYTES;
+          mbar_expect_tx(&full_bar[s], A_BYTES + 2 * B_BYTES);
+          tma_load_2d(st, &maps.a, &full_bar[s], kb * GT_BK, tc.row0);
+          tma_load_2d(st + A_BYTES, &maps.bh[tc.ty], &full_bar[s], kb * GT_BK, tc.n0);
+          tma_load_2d(st + A_BYTES + B_BYTES, &maps.bl[tc.ty], &full_bar[s], kb * GT_BK, tc.n0);
+        }
       }
-      if (*abort) {
-        // let the copies already in flight land before the CTA's shared memory
-        // is released (bounded, like every other wait here)
-        for (int kb = issued - STAGES < 0 ? 0 : issued - STAGES; kb < issued; ++kb) {
-          const int s = kb % STAGES;
+      if (!ok) {
+        // let the copies already in flight land before the CTA's shared
+        // memory is released (bounded, like every other wait here)
+        for (int q = g - STAGES < 0 ? 0 : g - STAGES; q < g; ++q) {
+          const int s = q % STAGES;
           for (unsigned it = 0; it < GT_WAIT_LIMIT; ++it)
-            if (mbar_try(&full_bar[s], (kb / STAGES) & 1)) break;
+            if (mbar_try(&full_bar[s], (q / STAGES) & 1)) break;
         }
       }
     }
+    __syncwarp();
   } else if (warp == 1) {
     // ---------------------------------------------------------------- MMA
     if (lane == 0) {
+      int g = 0, lt = 0;
       bool ok = true;
-      for (int kb = 0; kb < nk && ok; ++kb) {
-        const int s = kb % STAGES;
-        const uint32_t ph = (kb / STAGES) & 1;
-        if (!mbar_wait(&conv_bar[s], ph, abort)) {
+      for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x, ++lt) {
+        const int b = lt & 1;
+        if (!mbar_wait(&tempty_bar[b], ((lt >> 1) & 1) ^ 1, abort)) {
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        unsigned char* st = smem + s * STAGE_BYTES;
-        const uint64_t ah = smem_desc(st), al = smem_desc(st + A_BYTES);
-        const uint64_t bh = smem_desc(st + 2 * A_BYTES);
-        const uint64_t bl = smem_desc(st + 2 * A_BYTES + B_BYTES);
+        const uint32_t d = tmem + (uint32_t)b * TM_ACC;
+        for (int kb = 0; kb < nk; ++kb, ++g) {
+          const int s = g % STAGES;
+          const uint32_t ph = (g / STAGES) & 1;
+          if (!mbar_wait(&conv_bar[s], ph, abort)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          unsigned char* st = smem + s * STAGE_BYTES;
+          const uint32_t ah = tmem + TM_A0 + 64u * (uint32_t)s, al = ah + 32u;
+          const uint64_t bh = smem_desc(st + A_BYTES);
+          const uint64_t bl = smem_desc(st + A_BYTES + B_BYTES);
 #pragma unroll
-        for (int j = 0; j < GT_BK / 8; ++j) {  // K = 8 per instruction: +32 B
-          const uint64_t o = (uint64_t)(j * 32) >> 4;
-          const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
-          mma_tf32(tmem, ah + o, bh + o, IDESC, acc);
-          mma_tf32(tmem, al + o, bh + o, IDESC, 1u);
-          mma_tf32(tmem, ah + o, bl + o, IDESC, 1u);
+          for (int j = 0; j < GT_BK / 8; ++j) {  // K = 8 per instruction
+            const uint32_t ca = 8u * (uint32_t)j;           // TMEM columns
+            const uint64_t ob = (uint64_t)(j * 32) >> 4;    // +32 B in the swizzled row
+            const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
+            mma_tf32_ta(d, ah + ca, bh + ob, IDESC, acc);
+            mma_tf32_ta(d, al + ca, bh + ob, IDESC, 1u);
+            mma_tf32_ta(d, ah + ca, bl + ob, IDESC, 1u);
+          }
+          mma_commit(&empty_bar[s]);  // frees the stage (smem and TMEM A) once read
         }
-        mma_commit(&empty_bar[s]);  // frees the stage once these MMAs have read it
+        if (!ok) break;
+        mma_commit(&tfull_bar[b]);  // accumulator b complete
       }
-      mma_commit(&acc_bar);  // accumulator complete (or all issued work drained)
       if (!ok) *abort = 1;
+      // every MMA issued by this thread has completed before teardown
+      mma_commit(&drain_bar);
+      for (unsigned it = 0; it < GT_WAIT_LIMIT; ++it)
+        if (mbar_try(&drain_bar, 0)) break;
+    }
+    __syncwarp();
+  } else if (warp < 6) {
+    // ------------------------------------------- split A into TMEM hi / lo
+    const uint32_t lane_base = 32u * (uint32_t)(warp & 3);
+    const int r = (int)lane_base + lane;  // tile row of this thread
+    int g = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x) {
+      for (int kb = 0; kb < nk; ++kb, ++g) {
+        const int s = g % STAGES;
+        const uint32_t ph = (g / STAGES) & 1;
+        const bool got = mbar_wait(&full_bar[s], ph, abort);
+        if (!__all_sync(0xffffffffu, got)) {  // tcgen05.st below is warp-wide
+          ok = false;
+          break;
+        }
+        // row r of the 128-byte-swizzled tile: 16-byte chunk c at c ^ (r & 7)
+        const unsigned char* rowp = smem + s * STAGE_BYTES + r * 128;
+        uint32_t hi[32], lo[32];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const float4 x = *reinterpret_cast<const float4*>(rowp + ((c ^ (r & 7)) << 4));
+          const float xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float h = tf32_hi(xs[u]);
+            hi[4 * c + u] = __float_as_uint(h);
+            lo[4 * c + u] = __float_as_uint(xs[u] - h);
+          }
+        }
+        const uint32_t ta = tmem + (lane_base << 16) + TM_A0 + 64u * (uint32_t)s;
+        tmem_st16(ta, hi);
+        tmem_st16(ta + 16u, hi + 16);
+        tmem_st16(ta + 32u, lo);
+        tmem_st16(ta + 48u, lo + 16);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive(&conv_bar[s]);
+      }
     }
   } else {
-    // ------------------------------------------- split A, then epilogue
-    const int ct = threadIdx.x - 64;  // 0..127
-    for (int kb = 0; kb < nk; ++kb) {
-      const int s = kb % STAGES;
-      const uint32_t ph = (kb / STAGES) & 1;
-      if (!mbar_wait(&full_bar[s], ph, abort)) break;
-      float4* ah = reinterpret_cast<float4*>(smem + s * STAGE_BYTES);
-      float4* al = reinterpret_cast<float4*>(smem + s * STAGE_BYTES + A_BYTES);
-#pragma unroll
-      for (int q = 0; q < A_BYTES / 16 / 128; ++q) {
-        const int idx = q * 128 + ct;
-        float4 x = ah[idx];
-        float4 h = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
-        ah[idx] = h;
-        al[idx] = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(&conv_bar[s]);
-    }
-    // epilogue: warp (warp % 4) owns TMEM lanes 32 * (warp % 4) ..., one row
-    // per thread; each 16-column chunk moves as 4 x 16-byte loads / stores
-    // per operand (64 contiguous bytes per thread and row)
-    bool have = mbar_wait(&acc_bar, 0, abort) && !*abort;
-    have = __shfl_sync(0xffffffffu, have ? 1 : 0, 0) != 0;  // tcgen05.ld is warp-wide
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (have) {
-      const int lane_base = 32 * (warp & 3);
-      const int row = row0 + lane_base + lane;
-      const bool ok = row < row_end;
-      const size_t at = (size_t)(ok ? row : row0) * epi.ld + n0;
-      const float* bias = epi.bias[ty];
-      const float* idt = epi.idt[ty];
-      const float* wv = epi.w[ty];
+    // ---------------------------------------------------------------- epilogue
+    // warp (warp % 4) owns TMEM lanes 32 * (warp % 4) ..., one row per
+    // thread; each 16-column chunk moves as 4 x 16-byte loads / stores per
+    // operand (64 contiguous bytes per thread and row)
+    const int lane_base = 32 * (warp & 3);
+    int lt = 0;
+    for (int t = blockIdx.x; t < n_total; t += gridDim.x, ++lt) {
+      const int b = lt & 1;
+      bool have = mbar_wait(&tfull_bar[b], (lt >> 1) & 1, abort) && !*abort;
+      have = __shfl_sync(0xffffffffu, have ? 1 : 0, 0) != 0;  // tcgen05.ld is warp-wide
+      if (!have) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const TileCoord tc = tile_coord(shp, t);
+      const int row = tc.row0 + lane_base + lane;
+      const bool ok = row < tc.row_end;
+      const int n0 = tc.n0;
+      const size_t at = (size_t)(ok ? row : tc.row0) * epi.ld + n0;
+      const float* bias = epi.bias[tc.ty];
+      const float* idt = epi.idt[tc.ty];
+      const float* wv = epi.w[tc.ty];
       constexpr bool NEED0 = MODE >= EPI_RES_DT, NEED1 = MODE == EPI_BWD_RES;
+      const uint32_t acc_base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)b * TM_ACC;
       float esum = 0.f;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 16) {
@@ -317,7 +411,7 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
           if (NEED1 && ok) x1[j] = __ldg(reinterpret_cast<const float4*>(epi.aux1 + at + c0) + j);
         }
         float v[16];
-        tmem_ld16(tmem + ((uint32_t)lane_base << 16) + (uint32_t)c0, v);
+        tmem_ld16(acc_base + (uint32_t)c0, v);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const int cj = n0 + c0 + 4 * j;
@@ -367,6 +461,9 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
           }
         }
       }
+      // accumulator b may be overwritten by the tile after next
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&tempty_bar[b]);
       if (MODE == EPI_LAST && ok) atomicAdd(&epi.e[row], esum);
     }
   }
@@ -376,25 +473,36 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(TMEM_COLS));
+                 "r"(TM_COLS));
   }
 }
 
 // ---------------------------------------------------------------- host -----
-template <int BN, int STAGES, int MODE>
-static int launch_mode(const struct GemmMaps& maps, const struct GemmShape& shp,
-                       const struct GemmEpi& epi, int* status, cudaStream_t st);
+template <int MODE>
+static int launch_mode(const GemmMaps& maps, const GemmShape& shp, const GemmEpi& epi,
+                       int* status, cudaStream_t st) {
+  constexpr int SMEM = GT_STAGES * (GT_BM * GT_BK * 4 + 2 * GT_BN * GT_BK * 4) + 1024;
+  DPB_CUDA(cudaFuncSetAttribute(k_gemm_tf32x3<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SMEM),
+           "gemm");
+  const int tiles = shp.tile_start[shp.ntypes] * shp.n_tiles;
+  if (tiles == 0) return DPB_OK;
+  const int sms = sm_count();
+  const int grid = tiles < sms ? tiles : sms;
+  k_gemm_tf32x3<MODE><<<grid, GT_THREADS, SMEM, st>>>(maps, shp, epi, status);
+  DPB_CHECK_LAUNCH("gemm_tf32x3");
+  return DPB_OK;
+}
 
-template <int BN, int STAGES>
 static int launch(const GemmMaps& maps, const GemmShape& shp, const GemmEpi& epi, int* status,
                   cudaStream_t st) {
   switch (epi.mode) {
-    case EPI_STORE: return launch_mode<BN, STAGES, EPI_STORE>(maps, shp, epi, status, st);
-    case EPI_TANH: return launch_mode<BN, STAGES, EPI_TANH>(maps, shp, epi, status, st);
-    case EPI_RES_DT: return launch_mode<BN, STAGES, EPI_RES_DT>(maps, shp, epi, status, st);
-    case EPI_LAST: return launch_mode<BN, STAGES, EPI_LAST>(maps, shp, epi, status, st);
-    case EPI_BWD_DT: return launch_mode<BN, STAGES, EPI_BWD_DT>(maps, shp, epi, status, st);
-    default: return launch_mode<BN, STAGES, EPI_BWD_RES>(maps, shp, epi, status, st);
+    case EPI_STORE: return launch_mode<EPI_STORE>(maps, shp, epi, status, st);
+    case EPI_TANH: return launch_mode<EPI_TANH>(maps, shp, epi, status, st);
+    case EPI_RES_DT: return launch_mode<EPI_RES_DT>(maps, shp, epi, status, st);
+    case EPI_LAST: return launch_mode<EPI_LAST>(maps, shp, epi, status, st);
+    case EPI_BWD_DT: return launch_mode<EPI_BWD_DT>(maps, shp, epi, status, st);
+    default: return launch_mode<EPI_BWD_RES>(maps, shp, epi, status, st);
   }
 }
 
@@ -434,20 +542,6 @@ static int make_map(CUtensorMap* m, const float* base, int rows, int cols, int b
   return DPB_OK;
 }
 
-template <int BN, int STAGES, int MODE>
-static int launch_mode(const GemmMaps& maps, const GemmShape& shp, const GemmEpi& epi,
-                       int* status, cudaStream_t st) {
-  constexpr int SMEM = STAGES * (2 * GT_BM * GT_BK * 4 + 2 * BN * GT_BK * 4) + 1024;
-  DPB_CUDA(cudaFuncSetAttribute(k_gemm_tf32x3<BN, STAGES, MODE>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM),
-           "gemm");
-  const int tiles = shp.tile_start[shp.ntypes] * shp.n_tiles;
-  if (tiles == 0) return DPB_OK;
-  k_gemm_tf32x3<BN, STAGES, MODE><<<tiles, GT_THREADS, SMEM, st>>>(maps, shp, epi, status);
-  DPB_CHECK_LAUNCH("gemm_tf32x3");
-  return DPB_OK;
-}
-
 }  // namespace dpb
 
 using namespace dpb;
@@ -470,7 +564,7 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
     set_error("gemm_tf32x3: N=%d must be a multiple of 80", N);
     return DPB_ERR_INVALID;
   }
-  const int BN = 80;
+  const int BN = GT_BN;
   GemmMaps maps;
   GemmShape shp;
   shp.ntypes = ntypes;
@@ -517,10 +611,7 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
     ep.w[t] = w ? w[t] : nullptr;
   }
   cudaStream_t st = as_stream(stream);
-  // short reductions: two CTAs per SM (2 stages each) so one CTA's epilogue
-  // overlaps the other's main loop; long reductions: a deep 4-stage ring
-  if (K <= 256) return launch<BN, 2>(maps, shp, ep, status, st);
-  return launch<BN, 4>(maps, shp, ep, status, st);
+  return launch(maps, shp, ep, status, st);
 }
 
 }  // extern "C"
