@@ -9,6 +9,11 @@ Two libraries sit behind the same Python functions:
   ``oracle/ref_shim.cc``; present only where the reference tree was available
   at build time.
 
+``ref_gpu()`` loads ``oracle/_ref/libdpref_gpu.so``, the reference's own CUDA
+kernels (``source/lib/src/gpu/*.cu``, built for sm_100a) behind
+``oracle/ref_gpu_shim.cu``, for the GPU tests that compare them with this
+package's drop-ins.
+
 Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` import this module; the product never does.
 """
@@ -24,6 +29,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "libdporacle.so")
 REF_SO = os.path.join(HERE, "_ref", "libdpref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libdpref_gpu.so")
 REF_TREE = "/root/reference"
 
 _i = ctypes.c_int
@@ -31,14 +37,19 @@ _f = ctypes.c_float
 _p = ctypes.c_void_p
 
 
-def build(ref: bool | None = None) -> None:
-    """Compile the checkers with ``make -C oracle`` (the reference library only
-    when its sources exist)."""
+def build(ref: bool | None = None, ref_gpu: bool | None = None) -> None:
+    """Compile the checkers with ``make -C oracle`` (the reference libraries
+    only when its sources exist; the GPU one also needs nvcc)."""
     targets = ["port"]
+    have_tree = os.path.isdir(os.path.join(REF_TREE, "source", "lib"))
     if ref is None:
-        ref = os.path.isdir(os.path.join(REF_TREE, "source", "lib"))
+        ref = have_tree
+    if ref_gpu is None:
+        ref_gpu = have_tree and os.path.exists("/usr/local/cuda/bin/nvcc")
     if ref:
         targets.append("ref")
+    if ref_gpu:
+        targets.append("refgpu")
     subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
 
 
@@ -230,6 +241,23 @@ def ref() -> _Lib | None:
                 return None
         _cache["ref"] = _Lib(REF_SO, "dpref")
     return _cache["ref"]
+
+
+def ref_gpu():
+    """ctypes handle of the reference CUDA kernels (refgpu_* entry points, each
+    returning 0 or 1 when the reference raised), or None where not built."""
+    if "ref_gpu" not in _cache:
+        if not os.path.exists(REF_GPU_SO):
+            return None
+        lib = ctypes.CDLL(REF_GPU_SO)
+        for name in ("build_nlist_f64", "prod_env_mat_a_f64", "prod_env_mat_a_f32",
+                     "tabulate_fusion_se_a_f64", "tabulate_fusion_se_a_f32",
+                     "tabulate_fusion_se_a_grad_f64", "tabulate_fusion_se_a_grad_f32",
+                     "prod_force_a_f64", "prod_force_a_f32", "prod_virial_a_f64",
+                     "prod_virial_a_f32"):
+            getattr(lib, "refgpu_" + name).restype = _i
+        _cache["ref_gpu"] = lib
+    return _cache["ref_gpu"]
 
 
 def best() -> _Lib:
