@@ -9,24 +9,27 @@
 // product is Ah Bh + Al Bh + Ah Bl (the Al Bl term, ~2^-22 relative, is
 // dropped), accumulated in FP32 in tensor memory.
 //
-// Persistent, warp-specialised CTA (one per SM, 320 threads) walking output
-// tiles of 128 rows x 80 columns:
-//   warp 0      TMA producer: A tile 128 x 32 and B hi/lo tiles 80 x 32 per
-//               k-block into a 4-stage shared-memory ring (128-byte swizzle);
+// Persistent, warp-specialised CTA (one per SM) walking output tiles of 128
+// rows x BN columns (BN = 160 when it divides N, else 80):
+//   warp 0      TMA producer: A tile 128 x 32 and B hi/lo tiles BN x 32 per
+//               k-block into a STAGES-deep shared-memory ring (128-byte
+//               swizzle);
 //   warps 2-5   split each A tile row by row (one row per thread) into TF32
-//               hi / lo and store both straight into tensor memory, so the
-//               MMAs read A from TMEM and only B from shared memory;
-//   warp 1      one elected lane issues tcgen05.mma (M=128, N=80, K=8) into
-//               one of two TMEM accumulators and commits to the ring's and
-//               the accumulator's mbarriers;
-//   warps 6-9   epilogue of the previous tile from the other accumulator
-//               (one row per thread, 16-byte loads / stores), overlapping the
-//               current tile's MMAs.
-// Tensor memory (512 columns): accumulators at columns 0 and 128, A stage s
-// hi / lo at 256 + 64 s and 256 + 64 s + 32. Every mbarrier wait is bounded:
-// on time-out the CTA raises an error bit in the caller's status word, stops
-// issuing work, waits (bounded) for its copies and MMAs in flight and frees
-// its tensor memory before returning.
+//               hi / lo and store both straight into one of ASLOTS tensor-
+//               memory slots, so the MMAs read A from TMEM and only B from
+//               shared memory;
+//   warp 1      one elected lane issues tcgen05.mma (M=128, N=BN, K=8) into
+//               one of ACCBUF TMEM accumulators and commits to the ring's,
+//               the A slots' and the accumulator's mbarriers;
+//   warps 6..   EPIW epilogue warps (two per TMEM lane quadrant when EPIW = 8,
+//               splitting the columns): one row per thread, 16-byte loads /
+//               stores; with two accumulators the epilogue of one tile
+//               overlaps the next tile's MMAs.
+// Tensor memory (512 columns): accumulators from column 0, A slot s hi / lo at
+// A0 + 64 s and A0 + 64 s + 32. Every mbarrier wait is bounded: on time-out
+// the CTA raises an error bit in the caller's status word, stops issuing
+// work, waits (bounded) for its copies and MMAs in flight and frees its
+// tensor memory before returning.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <stdint.h>
@@ -35,16 +38,37 @@
 
 namespace dpb {
 
-constexpr int GT_THREADS = 320;
 constexpr int GT_BM = 128;
-constexpr int GT_BN = 80;
 constexpr int GT_BK = 32;  // 32 FP32 = one 128-byte swizzle row
-constexpr int GT_STAGES = 4;
 constexpr int GT_MAXT = 4;
 constexpr unsigned GT_WAIT_LIMIT = 1u << 24;
 constexpr uint32_t TM_COLS = 512;
-constexpr uint32_t TM_ACC = 128;  // column distance of the two accumulators
-constexpr uint32_t TM_A0 = 256;   // first A stage column
+
+// one kernel configuration: tile width, ring depth, TMEM A slots,
+// accumulator buffers and epilogue warps
+template <int BN_, int STAGES_, int ASLOTS_, int ACCBUF_, int EPIW_>
+struct GemmCfg {
+  static constexpr int BN = BN_, STAGES = STAGES_, ASLOTS = ASLOTS_, ACCBUF = ACCBUF_,
+                       EPIW = EPIW_;
+  static constexpr int THREADS = 64 + 128 + 32 * EPIW;
+  static constexpr uint32_t ACC_STRIDE = BN <= 128 ? 128u : (uint32_t)((BN + 31) / 32 * 32);
+  static constexpr uint32_t A0 = ACCBUF * ACC_STRIDE;
+  static constexpr int A_BYTES = GT_BM * GT_BK * 4;  // 16 KB
+  static constexpr int B_BYTES = BN * GT_BK * 4;
+  static constexpr int STAGE_BYTES = A_BYTES + 2 * B_BYTES;
+  static constexpr int SMEM = STAGES * STAGE_BYTES + 1024;
+  static_assert(BN % 16 == 0 && BN <= 256, "MMA N");
+  static_assert(A0 + 64u * ASLOTS <= TM_COLS, "tensor memory columns");
+  static_assert(STAGE_BYTES % 1024 == 0, "stage alignment for the 128-byte swizzle");
+  static_assert(SMEM <= 232448, "shared memory per CTA");
+  static_assert(EPIW == 4 || EPIW == 8, "epilogue warps");
+};
+// Measured on the fitting layers of 12,288-atom water: 80-column tiles are
+// fastest for N = 240 (288 tiles keep every SM busy; a single 240-column tile
+// per row block leaves 52 SMs idle), 160-column tiles for N = 1600 (half the
+// A re-reads).
+using CfgN80 = GemmCfg<80, 4, 4, 2, 4>;
+using CfgN160 = GemmCfg<160, 4, 2, 2, 8>;
 
 enum : int {
   ST_MMA_TIMEOUT = 1 << 8,
@@ -197,7 +221,7 @@ __device__ __forceinline__ float tf32_hi(float x) {
 struct TileCoord {
   int ty, row0, row_end, n0;
 };
-__device__ __forceinline__ TileCoord tile_coord(const GemmShape& shp, int t) {
+__device__ __forceinline__ TileCoord tile_coord(const GemmShape& shp, int t, int BN) {
   TileCoord c;
   const int nt = t % shp.n_tiles, rt = t / shp.n_tiles;
   int ty = 0;
@@ -205,28 +229,33 @@ __device__ __forceinline__ TileCoord tile_coord(const GemmShape& shp, int t) {
   c.ty = ty;
   c.row0 = shp.row_start[ty] + (rt - shp.tile_start[ty]) * GT_BM;
   c.row_end = shp.row_start[ty + 1];
-  c.n0 = nt * GT_BN;
+  c.n0 = nt * BN;
   return c;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(GT_THREADS, 1)
+template <class CFG, int MODE>
+__global__ void __launch_bounds__(CFG::THREADS, 1)
 k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi, int* status) {
-  constexpr int BN = GT_BN;
-  constexpr int STAGES = GT_STAGES;
-  constexpr int A_BYTES = GT_BM * GT_BK * 4;  // 16 KB
-  constexpr int B_BYTES = BN * GT_BK * 4;     // 10 KB
-  constexpr int STAGE_BYTES = A_BYTES + 2 * B_BYTES;
+  constexpr int BN = CFG::BN;
+  constexpr int STAGES = CFG::STAGES;
+  constexpr int ASLOTS = CFG::ASLOTS;
+  constexpr int ACCBUF = CFG::ACCBUF;
+  constexpr int EPIW = CFG::EPIW;
+  constexpr uint32_t TM_ACC = CFG::ACC_STRIDE;
+  constexpr uint32_t TM_A0 = CFG::A0;
+  constexpr int A_BYTES = CFG::A_BYTES;
+  constexpr int B_BYTES = CFG::B_BYTES;
+  constexpr int STAGE_BYTES = CFG::STAGE_BYTES;
   constexpr uint32_t IDESC = (1u << 4)            // D: FP32
                              | (2u << 7)          // A: TF32
                              | (2u << 10)         // B: TF32
                              | ((uint32_t)(BN >> 3) << 17)  // N
                              | ((uint32_t)(GT_BM >> 4) << 24);  // M = 128
-  static_assert(BN % 16 == 0 && BN <= (int)TM_ACC, "accumulator width");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t full_bar[STAGES], conv_bar[STAGES], empty_bar[STAGES];
-  __shared__ __align__(8) uint64_t tfull_bar[2], tempty_bar[2], drain_bar;
+  __shared__ __align__(8) uint64_t afree_bar[ASLOTS];
+  __shared__ __align__(8) uint64_t tfull_bar[ACCBUF], tempty_bar[ACCBUF], drain_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
 
@@ -241,9 +270,10 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
       mbar_init(&conv_bar[s], 128);
       mbar_init(&empty_bar[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int a = 0; a < ASLOTS; ++a) mbar_init(&afree_bar[a], 1);
+    for (int b = 0; b < ACCBUF; ++b) {
       mbar_init(&tfull_bar[b], 1);
-      mbar_init(&tempty_bar[b], 128);
+      mbar_init(&tempty_bar[b], 32 * EPIW);
     }
     mbar_init(&drain_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -266,7 +296,7 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
       int g = 0;  // k-blocks issued over all tiles
       bool ok = true;
       for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x) {
-        const TileCoord tc = tile_coord(shp, t);
+        const TileCoord tc = tile_coord(shp, t, BN);
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const int s = g % STAGES;
           const uint32_t ph = (g / STAGES) & 1;
@@ -298,8 +328,8 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
       int g = 0, lt = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x, ++lt) {
-        const int b = lt & 1;
-        if (!mbar_wait(&tempty_bar[b], ((lt >> 1) & 1) ^ 1, abort)) {
+        const int b = lt % ACCBUF;
+        if (!mbar_wait(&tempty_bar[b], ((lt / ACCBUF) & 1) ^ 1, abort)) {
           ok = false;
           break;
         }
@@ -314,7 +344,8 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           unsigned char* st = smem + s * STAGE_BYTES;
-          const uint32_t ah = tmem + TM_A0 + 64u * (uint32_t)s, al = ah + 32u;
+          const int as = g % ASLOTS;
+          const uint32_t ah = tmem + TM_A0 + 64u * (uint32_t)as, al = ah + 32u;
           const uint64_t bh = smem_desc(st + A_BYTES);
           const uint64_t bl = smem_desc(st + A_BYTES + B_BYTES);
 #pragma unroll
@@ -326,7 +357,8 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
             mma_tf32_ta(d, al + ca, bh + ob, IDESC, 1u);
             mma_tf32_ta(d, ah + ca, bl + ob, IDESC, 1u);
           }
-          mma_commit(&empty_bar[s]);  // frees the stage (smem and TMEM A) once read
+          mma_commit(&empty_bar[s]);    // frees the shared-memory stage once read
+          mma_commit(&afree_bar[as]);   // and the TMEM A slot
         }
         if (!ok) break;
         mma_commit(&tfull_bar[b]);  // accumulator b complete
@@ -348,11 +380,15 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % STAGES;
         const uint32_t ph = (g / STAGES) & 1;
-        const bool got = mbar_wait(&full_bar[s], ph, abort);
+        const int as = g % ASLOTS;
+        // the stage has landed and the TMEM slot's previous MMAs are done
+        const bool got = mbar_wait(&full_bar[s], ph, abort) &&
+                         mbar_wait(&afree_bar[as], ((g / ASLOTS) & 1) ^ 1, abort);
         if (!__all_sync(0xffffffffu, got)) {  // tcgen05.st below is warp-wide
           ok = false;
           break;
         }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         // row r of the 128-byte-swizzled tile: 16-byte chunk c at c ^ (r & 7)
         const unsigned char* rowp = smem + s * STAGE_BYTES + r * 128;
         uint32_t hi[32], lo[32];
@@ -367,7 +403,7 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
             lo[4 * c + u] = __float_as_uint(xs[u] - h);
           }
         }
-        const uint32_t ta = tmem + (lane_base << 16) + TM_A0 + 64u * (uint32_t)s;
+        const uint32_t ta = tmem + (lane_base << 16) + TM_A0 + 64u * (uint32_t)as;
         tmem_st16(ta, hi);
         tmem_st16(ta + 16u, hi + 16);
         tmem_st16(ta + 32u, lo);
@@ -383,14 +419,15 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
     // thread; each 16-column chunk moves as 4 x 16-byte loads / stores per
     // operand (64 contiguous bytes per thread and row)
     const int lane_base = 32 * (warp & 3);
+    const int ehalf = EPIW == 8 ? (warp - 6) >> 2 : 0;  // column share of this warp
     int lt = 0;
     for (int t = blockIdx.x; t < n_total; t += gridDim.x, ++lt) {
-      const int b = lt & 1;
-      bool have = mbar_wait(&tfull_bar[b], (lt >> 1) & 1, abort) && !*abort;
+      const int b = lt % ACCBUF;
+      bool have = mbar_wait(&tfull_bar[b], (lt / ACCBUF) & 1, abort) && !*abort;
       have = __shfl_sync(0xffffffffu, have ? 1 : 0, 0) != 0;  // tcgen05.ld is warp-wide
       if (!have) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const TileCoord tc = tile_coord(shp, t);
+      const TileCoord tc = tile_coord(shp, t, BN);
       const int row = tc.row0 + lane_base + lane;
       const bool ok = row < tc.row_end;
       const int n0 = tc.n0;
@@ -402,7 +439,7 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
       const uint32_t acc_base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)b * TM_ACC;
       float esum = 0.f;
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 16) {
+      for (int c0 = 16 * ehalf; c0 < BN; c0 += 16 * (EPIW / 4)) {
         float4 x0[4], x1[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {  // in flight during the TMEM load
@@ -464,7 +501,7 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
       // accumulator b may be overwritten by the tile after next
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&tempty_bar[b]);
-      if (MODE == EPI_LAST && ok) atomicAdd(&epi.e[row], esum);
+      if (MODE == EPI_LAST && ok) atomicAdd(&epi.e[row], esum);  // per warp's columns
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -478,31 +515,31 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
 }
 
 // ---------------------------------------------------------------- host -----
-template <int MODE>
+template <class CFG, int MODE>
 static int launch_mode(const GemmMaps& maps, const GemmShape& shp, const GemmEpi& epi,
                        int* status, cudaStream_t st) {
-  constexpr int SMEM = GT_STAGES * (GT_BM * GT_BK * 4 + 2 * GT_BN * GT_BK * 4) + 1024;
-  DPB_CUDA(cudaFuncSetAttribute(k_gemm_tf32x3<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                SMEM),
+  DPB_CUDA(cudaFuncSetAttribute(k_gemm_tf32x3<CFG, MODE>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, CFG::SMEM),
            "gemm");
   const int tiles = shp.tile_start[shp.ntypes] * shp.n_tiles;
   if (tiles == 0) return DPB_OK;
   const int sms = sm_count();
   const int grid = tiles < sms ? tiles : sms;
-  k_gemm_tf32x3<MODE><<<grid, GT_THREADS, SMEM, st>>>(maps, shp, epi, status);
+  k_gemm_tf32x3<CFG, MODE><<<grid, CFG::THREADS, CFG::SMEM, st>>>(maps, shp, epi, status);
   DPB_CHECK_LAUNCH("gemm_tf32x3");
   return DPB_OK;
 }
 
+template <class CFG>
 static int launch(const GemmMaps& maps, const GemmShape& shp, const GemmEpi& epi, int* status,
                   cudaStream_t st) {
   switch (epi.mode) {
-    case EPI_STORE: return launch_mode<EPI_STORE>(maps, shp, epi, status, st);
-    case EPI_TANH: return launch_mode<EPI_TANH>(maps, shp, epi, status, st);
-    case EPI_RES_DT: return launch_mode<EPI_RES_DT>(maps, shp, epi, status, st);
-    case EPI_LAST: return launch_mode<EPI_LAST>(maps, shp, epi, status, st);
-    case EPI_BWD_DT: return launch_mode<EPI_BWD_DT>(maps, shp, epi, status, st);
-    default: return launch_mode<EPI_BWD_RES>(maps, shp, epi, status, st);
+    case EPI_STORE: return launch_mode<CFG, EPI_STORE>(maps, shp, epi, status, st);
+    case EPI_TANH: return launch_mode<CFG, EPI_TANH>(maps, shp, epi, status, st);
+    case EPI_RES_DT: return launch_mode<CFG, EPI_RES_DT>(maps, shp, epi, status, st);
+    case EPI_LAST: return launch_mode<CFG, EPI_LAST>(maps, shp, epi, status, st);
+    case EPI_BWD_DT: return launch_mode<CFG, EPI_BWD_DT>(maps, shp, epi, status, st);
+    default: return launch_mode<CFG, EPI_BWD_RES>(maps, shp, epi, status, st);
   }
 }
 
@@ -564,7 +601,7 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
     set_error("gemm_tf32x3: N=%d must be a multiple of 80", N);
     return DPB_ERR_INVALID;
   }
-  const int BN = GT_BN;
+  const int BN = N % CfgN160::BN == 0 ? CfgN160::BN : CfgN80::BN;
   GemmMaps maps;
   GemmShape shp;
   shp.ntypes = ntypes;
@@ -611,7 +648,8 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
     ep.w[t] = w ? w[t] : nullptr;
   }
   cudaStream_t st = as_stream(stream);
-  return launch(maps, shp, ep, status, st);
+  if (BN == CfgN160::BN) return launch<CfgN160>(maps, shp, ep, status, st);
+  return launch<CfgN80>(maps, shp, ep, status, st);
 }
 
 }  // extern "C"

@@ -80,9 +80,10 @@ def test_gemm_store(dpb, mdl, M, K, N, rows):
     assert err < 2e-5
 
 
-def test_gemm_epilogues(dpb, mdl):
-    rng = np.random.default_rng(3)
-    rows, M, K, N = [96, 160], 256, 240, 240
+@pytest.mark.parametrize("N", [240, 320, 400])  # tiles of 80, 160 and 80 columns
+def test_gemm_epilogues(dpb, mdl, N):
+    rng = np.random.default_rng(3 + N)
+    rows, M, K = [96, 290], 386, 240
     A = rng.normal(size=(M, K)).astype(np.float32) * 0.5
     Bs = [rng.normal(size=(N, K)).astype(np.float32) / np.sqrt(K) for _ in rows]
     acc = _ref(A, Bs, rows)
