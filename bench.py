@@ -377,10 +377,40 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             peaks = json.load(f)
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = per_atom_bytes[dom] * nloc / (ours[dom] * 1e-3) / 1e9
+    # DRAM bytes per launch of the stage's kernel from the committed ncu capture
+    # of this workload (profiles/ncu_dram_water12288.json)
+    kernel_of = {"env_mat": "dpb::k_env<double, float, 256, 4, 1>",
+                 "descriptor_fwd": "dpb::k_desc_fwd", "descriptor_bwd": "dpb::k_desc_bwd",
+                 "force_virial": "dpb::k_force_virial_rc<double, float>"}
+    traffic = None
+    dram_path = os.path.join(ROOT, "profiles", "ncu_dram_water12288.json")
+    if nloc == 12288 and os.path.exists(dram_path):
+        with open(dram_path) as f:
+            kd = json.load(f)["kernels"].get(kernel_of[dom])
+        if kd:
+            traffic = kd["dram_read_bytes"] + kd["dram_write_bytes"]
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
+                "traffic_source": "profiles/ncu_dram_water12288.json" if traffic else None,
+                "algorithmic_bytes_per_launch": per_atom_bytes[dom] * nloc,
                 "algorithmic_bytes_per_atom": per_atom_bytes[dom],
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    # every stage against its own roof: HBM bytes for the memory stages, the
+    # tensor pipe for the fitting GEMMs (3xTF32: three TF32 products per FP32
+    # multiply-add; TF32 dense peak taken as half the measured BF16 GEMM rate)
+    fit = cfg.fitting
+    din = cfg.neuron[-1] * cfg.axis_neuron
+    mac_fit = 2 * (din * fit[0] + sum(fit[k] * fit[k + 1] for k in range(len(fit) - 1)))
+    tf32_peak = float(peaks.get("bf16_tflops", 1590.0)) / 2
+    stage_roofs = {}
+    for k, v in stage_ms.items():
+        if k in per_atom_bytes:
+            gbs = per_atom_bytes[k] * nloc / (v * 1e-3) / 1e9
+            stage_roofs[k] = {"bound": "hbm", "achieved_gbs": gbs, "frac": gbs / hbm_peak}
+        elif k == "fitting":
+            tf = 3 * 2 * mac_fit * nloc / (v * 1e-3) / 1e12
+            stage_roofs[k] = {"bound": "tensor", "achieved_tflops_tf32": tf,
+                              "peak_tflops_tf32": tf32_peak, "frac": tf / tf32_peak}
 
     # ---- CPU baseline: the reference CPU path on a bounded sample (rank 0, N=1)
     cpu = None
@@ -416,6 +446,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             "cpu_baseline": cpu,
             "plain_fp64": plain_line,
             "stages_ms": stage_ms,
+            "stage_rooflines": stage_roofs,
             "accuracy": acc,
         }
         print(json.dumps(line), flush=True)
