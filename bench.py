@@ -29,6 +29,7 @@ reference: the reference's own CPU implementation (deepmd:: *_cpu functions
 from __future__ import annotations
 
 import argparse
+import importlib
 import json
 import os
 import subprocess
@@ -198,6 +199,50 @@ def _setup_frame(mdl, wl, tab, rank: int, device):
     params = mdl.init_params(cfg, seed=PARAM_SEED)
     mdl.prepare(params, coord, atype, box, device=device)
     return cfg, params, coord, atype, box
+
+
+# ------------------------------------------------- repeated evaluation (c4) --
+def run_repeated(args) -> None:
+    """A large frame evaluated many times with small moves, an rcut + skin
+    list rebuilt every --rebuild-every steps, FP64 plain-path checks every
+    --check-every steps. One GPU; prints its own JSON line."""
+    import torch
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    mdl, wl, tab = _load()
+    rep = importlib.import_module("deepmd_kit_lr_pt_b200.repeated")
+    cfg = mdl.SeAConfig()
+    coord, atype, box = wl.water_frame(args.n_side, seed=100)
+    params = mdl.init_params(cfg, seed=PARAM_SEED)
+    mdl.prepare(params, coord, atype, box, device=device)
+    nloc = atype.size
+    ev = mdl.SeAEvaluator(params, atype, box, mode="compressed", device=device, skin=args.skin)
+    plain = mdl.SeAEvaluator(params, atype, box, mode="plain", device=device)
+    clocks = ClockSampler(0)
+    clocks.start()
+    out = rep.repeated_evaluation(ev, coord, steps=args.steps, rebuild_every=args.rebuild_every,
+                                  sigma=args.sigma, seed=7, check=plain.compute,
+                                  check_every=args.check_every)
+    clk = clocks.stop()
+    us = out["wall_s"] * 1e6 / (args.steps * nloc)
+    line = {"metric": "us/step/atom, se_e2_a water repeated evaluation, skin list "
+                      "(compressed, mixed precision)",
+            "value": us, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": 0,
+            "ms_per_step": out["wall_s"] * 1e3 / args.steps, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"water {nloc} atoms ({nloc // 3} H2O, {box[0]:.2f} A box), "
+                                   f"coordinates + N(0, {args.sigma}^2) A per step, list "
+                                   f"rcut + {args.skin} A rebuilt every "
+                                   f"{args.rebuild_every} steps",
+                       "nloc": nloc, "sel": list(cfg.sel), "embedding": list(cfg.neuron),
+                       "fitting": list(cfg.fitting)},
+            "rebuilds": out["rebuilds"],
+            "step_device_ms": {"mean": out["step_device_ms_mean"],
+                               "max": out["step_device_ms_max"]},
+            "clocks": clk,
+            "checks_vs_fp64_plain": out["checks"]}
+    print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------- arms -------
@@ -462,6 +507,14 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the FP64 plain path (smaller device footprint for profiling)")
+    ap.add_argument("--workload", choices=["step", "repeated"], default="step",
+                    help="repeated: many evaluations of one large frame with a skin list")
+    ap.add_argument("--n-side", type=int, default=48,
+                    help="repeated workload: oxygen grid per box side (48: 331,776 atoms)")
+    ap.add_argument("--skin", type=float, default=2.0)
+    ap.add_argument("--rebuild-every", type=int, default=10)
+    ap.add_argument("--sigma", type=float, default=0.002)
+    ap.add_argument("--check-every", type=int, default=100)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -469,6 +522,10 @@ def main() -> None:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "repeated":
+        if rank == 0:
+            run_repeated(args)
         return
     if world > 1:
         import datetime

@@ -70,6 +70,9 @@ _FUNCS = {
     "dpb_build_nlist_f32": "pppppLpiiifipp",
     "dpb_prod_env_mat_a_f64": "pppppp" "ipppi" "ppiiiff" "pipp",
     "dpb_prod_env_mat_a_f32": "pppppp" "ipppi" "ppiiiff" "pipp",
+    "dpb_prod_env_mat_a_mixed": "pppppp" "ipppi" "ppiiiff" "pipp",
+    "dpb_ghost_shift_f64": "pppppip",
+    "dpb_ghost_refresh_f64": "pppppip",
     "dpb_env_mat_a_cells_f64": "pppppp" "p" "ppiiff" "pipp",
     "dpb_env_mat_a_cells_f32": "pppppp" "p" "ppiiff" "pipp",
     "dpb_env_mat_a_cells_mixed": "pppppp" "p" "ppiiff" "pipp",

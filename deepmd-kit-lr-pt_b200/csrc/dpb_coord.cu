@@ -582,7 +582,59 @@ long long copy_coord_scratch_bytes(int nloc, float rcut, const double* boxt) {
 
 // ------------------------------------------------------------- C-ABI -------
 using namespace dpb;
+// ghost j keeps its periodic image between list rebuilds: shift_j =
+// c_ext_j - c_{mapping_j} at the rebuild, c_ext_j = c_{mapping_j} + shift_j
+// at every later step (the positions are not re-wrapped between rebuilds)
+__global__ void k_ghost_shift(double* shift, const double* cext, const double* coord,
+                              const int* mapping, const int* nall_dev, int mem_nall) {
+  const int n = nall_dev ? min(*nall_dev, mem_nall) : mem_nall;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int o = mapping[j];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) shift[3 * j + d] = cext[3 * j + d] - coord[3 * o + d];
+  }
+}
+
+__global__ void k_ghost_refresh(double* cext, const double* shift, const double* coord,
+                                const int* mapping, const int* nall_dev, int mem_nall) {
+  const int n = nall_dev ? min(*nall_dev, mem_nall) : mem_nall;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int o = mapping[j];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) cext[3 * j + d] = coord[3 * o + d] + shift[3 * j + d];
+  }
+}
+
 extern "C" {
+
+int dpb_ghost_shift_f64(double* shift, const double* cext, const double* coord,
+                        const int* mapping, const int* nall_dev, int mem_nall,
+                        dpb_stream_t stream) {
+  if (mem_nall < 0 || (mem_nall > 0 && (!shift || !cext || !coord || !mapping))) {
+    set_error("ghost_shift: invalid arguments");
+    return DPB_ERR_INVALID;
+  }
+  if (mem_nall == 0) return DPB_OK;
+  k_ghost_shift<<<grid_stride_blocks(mem_nall, 256), 256, 0, as_stream(stream)>>>(
+      shift, cext, coord, mapping, nall_dev, mem_nall);
+  DPB_CHECK_LAUNCH("ghost_shift");
+  return DPB_OK;
+}
+
+int dpb_ghost_refresh_f64(double* cext, const double* shift, const double* coord,
+                          const int* mapping, const int* nall_dev, int mem_nall,
+                          dpb_stream_t stream) {
+  if (mem_nall < 0 || (mem_nall > 0 && (!shift || !cext || !coord || !mapping))) {
+    set_error("ghost_refresh: invalid arguments");
+    return DPB_ERR_INVALID;
+  }
+  if (mem_nall == 0) return DPB_OK;
+  k_ghost_refresh<<<grid_stride_blocks(mem_nall, 256), 256, 0, as_stream(stream)>>>(
+      cext, shift, coord, mapping, nall_dev, mem_nall);
+  DPB_CHECK_LAUNCH("ghost_refresh");
+  return DPB_OK;
+}
+
 
 int dpb_normalize_coord_f64(double* coord, int natom, const double* boxt,
                             dpb_stream_t stream) {

@@ -341,11 +341,11 @@ static int env_cells(OT* em, OT* em_deriv, OT* rij, int* nlist, const CT* coord,
   return DPB_OK;
 }
 
-template <typename T>
-static int env_inlist(T* em, T* em_deriv, T* rij, int* nlist, const T* coord,
+template <typename CT, typename OT = CT>
+static int env_inlist(OT* em, OT* em_deriv, OT* rij, int* nlist, const CT* coord,
                       const int* type, int inum, const int* ilist,
                       const int* numneigh, int* const* firstneigh,
-                      int max_nbor_size, const T* avg, const T* std_, int nloc,
+                      int max_nbor_size, const OT* avg, const OT* std_, int nloc,
                       int nall, int nframes, float rcut, float rcut_smth,
                       const int* sec, int nsec, int* status,
                       dpb_stream_t stream) {
@@ -368,13 +368,13 @@ static int env_inlist(T* em, T* em_deriv, T* rij, int* nlist, const T* coord,
   }
   cudaStream_t st = as_stream(stream);
   GridView g{};
-  EnvIO<T, T> io{em, em_deriv, rij, nlist, coord, type, g, ilist, numneigh, firstneigh,
-                 avg, std_, nloc, nall, rcut, rcut_smth, status};
+  EnvIO<CT, OT> io{em, em_deriv, rij, nlist, coord, type, g, ilist, numneigh, firstneigh,
+                   avg, std_, nloc, nall, rcut, rcut_smth, status};
   if (max_nbor_size <= 1024) {
     constexpr int W = 4;
-    k_env<T, T, 1024, W, false><<<ceil_div(inum, W), W * 32, 0, st>>>(io, s, inum, nullptr);
+    k_env<CT, OT, 1024, W, false><<<ceil_div(inum, W), W * 32, 0, st>>>(io, s, inum, nullptr);
   } else {
-    k_env<T, T, ENV_LARGE_CAP, 1, false><<<inum, 32, 0, st>>>(io, s, inum, nullptr);
+    k_env<CT, OT, ENV_LARGE_CAP, 1, false><<<inum, 32, 0, st>>>(io, s, inum, nullptr);
   }
   DPB_CHECK_LAUNCH("prod_env_mat_a");
   return DPB_OK;
@@ -564,6 +564,19 @@ int dpb_prod_env_mat_a_f32(float* em, float* em_deriv, float* rij, int* nlist,
                            numneigh, firstneigh, max_nbor_size, avg, std_,
                            nloc, nall, nframes, rcut, rcut_smth, sec, nsec,
                            status, stream);
+}
+
+int dpb_prod_env_mat_a_mixed(float* em, float* em_deriv, float* rij, int* nlist,
+                             const double* coord, const int* type, int inum,
+                             const int* ilist, const int* numneigh,
+                             int* const* firstneigh, int max_nbor_size,
+                             const float* avg, const float* std_, int nloc, int nall,
+                             int nframes, float rcut, float rcut_smth, const int* sec,
+                             int nsec, int* status, dpb_stream_t stream) {
+  return env_inlist<double, float>(em, em_deriv, rij, nlist, coord, type, inum, ilist,
+                                   numneigh, firstneigh, max_nbor_size, avg, std_, nloc,
+                                   nall, nframes, rcut, rcut_smth, sec, nsec, status,
+                                   stream);
 }
 
 int dpb_env_mat_a_cells_f64(double* em, double* em_deriv, double* rij,

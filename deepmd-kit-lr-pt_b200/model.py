@@ -326,16 +326,28 @@ class SeAEvaluator:
     """Energy/force/virial of one frame of fixed size, types and box.
 
     mode "compressed": FP32 table path (needs params.tables);
-    mode "plain": FP64 embedding-MLP path.
+    mode "plain": FP64 embedding-MLP path (centers in chunks of
+    ``plain_chunk`` atoms, so large frames fit).
     Device buffers are allocated once; ``step()`` runs one evaluation on the
     current coordinates in ``self.coord``; ``capture()`` records the step into
-    a CUDA graph that ``replay()`` re-runs."""
+    a CUDA graph that ``replay()`` re-runs.
+
+    ``skin > 0`` switches to an MD engine's pattern: ``rebuild()`` makes the
+    ghosts and a neighbor list within rcut + skin (host synchronisation
+    allowed there); each step only moves the ghosts with their owners
+    (``dpb_ghost_refresh_f64``) and formats the kept list against rcut
+    (``dpb_prod_env_mat_a_mixed``), as prod_env_mat_a_gpu does with the list
+    LAMMPS passes."""
 
     def __init__(self, params: SeAParams, atype: np.ndarray, box: np.ndarray,
                  mode: str = "compressed", device="cuda:0", nall_capacity: int | None = None,
-                 tensor_core_fitting: bool = True):
+                 tensor_core_fitting: bool = True, skin: float = 0.0,
+                 plain_chunk: int = 16384):
         cfg = params.cfg
         self.cfg, self.params, self.mode = cfg, params, mode
+        self.skin = float(skin)
+        self.rc_list = float(cfg.rcut) + self.skin
+        self.plain_chunk = int(plain_chunk)
         self.dev = torch.device(device)
         self.nloc = int(atype.size)
         self.box = np.ascontiguousarray(np.asarray(box, np.float64).reshape(9))
@@ -343,8 +355,8 @@ class SeAEvaluator:
         self.sec = cfg.sec
         nloc, nnei = self.nloc, cfg.nnei
         lib = _capi.lib()
-        self.copy_bytes = int(lib.dpb_copy_coord_scratch_bytes(nloc, ctypes.c_float(cfg.rcut),
-                                                               self.box.ctypes.data))
+        self.copy_bytes = int(lib.dpb_copy_coord_scratch_bytes(
+            nloc, ctypes.c_float(self.rc_list), self.box.ctypes.data))
         if nall_capacity is None:
             # ghosts are at most the ghost cells' share of the atoms; +25% slack
             nall_capacity = int(self._estimate_nall() * 1.25) + 64
@@ -407,16 +419,90 @@ class SeAEvaluator:
             self.emb = [[(torch.tensor(W, dtype=torch.float64, device=dev),
                           torch.tensor(b, dtype=torch.float64, device=dev)) for W, b in net]
                         for net in params.emb]
+        if mode != "compressed":
+            self._plain_index(atype)
+        if self.skin > 0:
+            self.shift = torch.zeros_like(self.cext)
+            self.ilist = torch.arange(nloc, dtype=torch.int32, device=dev)
+            self.numneigh = torch.zeros(nloc, dtype=torch.int32, device=dev)
+            self.nl_width = 0
+            self.rows = None
+            self.firstneigh = None
+            self.nl_bytes = int(lib.dpb_build_nlist_scratch_bytes(nloc, self.mem_nall))
+            self.nl_scratch = torch.empty(self.nl_bytes, dtype=torch.uint8, device=dev)
+            self.built = False
         self.graph = None
 
     def _estimate_nall(self) -> int:
         # extended cells over local cells, times nloc (the reference's own
-        # estimate in neighbor_list.cc:774-778)
+        # estimate in neighbor_list.cc:774-778), for the ghost cutoff in use
         b = self.box
+        rc = self.rc_list
         L = np.array([np.linalg.norm(b[0:3]), np.linalg.norm(b[3:6]), np.linalg.norm(b[6:9])])
-        nc = np.maximum(1, np.floor(L / self.cfg.rcut))
-        ng = np.floor(self.cfg.rcut / (L / nc)) + 1
+        nc = np.maximum(1, np.floor(L / rc))
+        ng = np.floor(rc / (L / nc)) + 1
         return int(np.prod(nc + 2 * ng) / np.prod(nc) * self.nloc)
+
+    def _plain_index(self, atype: np.ndarray):
+        """Per chunk of centers and per type: the rows of that type (device
+        index tensors built once, so the plain step stays capturable)."""
+        n, ch = self.nloc, self.plain_chunk
+        self.plain_chunks = []
+        for a in range(0, n, ch):
+            b = min(n, a + ch)
+            per_type = []
+            for t in range(self.cfg.ntypes):
+                idx = np.nonzero(atype[a:b] == t)[0]
+                per_type.append(None if idx.size == 0 else
+                                torch.tensor(idx, dtype=torch.int64, device=self.dev))
+            self.plain_chunks.append((a, b, per_type))
+
+    # ---- neighbor list with a skin, rebuilt on request (host syncs allowed)
+    def rebuild(self):
+        """Ghosts and the rcut + skin neighbor list from the current
+        ``self.coord``; later steps reuse them until the next rebuild."""
+        if self.skin <= 0:
+            raise _capi.DPBInvalidArgument("rebuild() needs an evaluator made with skin > 0")
+        cfg, nloc = self.cfg, self.nloc
+        s = torch.cuda.current_stream().cuda_stream
+        self.coord_n.copy_(self.coord)
+        call("dpb_normalize_coord_f64", ptr(self.coord_n), nloc, self.box.ctypes.data, s)
+        call("dpb_copy_coord_async_f64", ptr(self.cext), ptr(self.text), ptr(self.mapping),
+             ptr(self.nall_dev), ptr(self.copy_scratch), self.copy_bytes, ptr(self.coord_n),
+             ptr(self.atype), nloc, self.mem_nall, ctypes.c_float(self.rc_list),
+             self.box.ctypes.data, s)
+        nall = int(self.nall_dev.item())
+        if nall > self.mem_nall:
+            raise _capi.DPBCapacityError(
+                f"DeePMD-kit Error: nall={nall} exceeds the capacity {self.mem_nall}")
+        # ghost images relative to the raw (unwrapped) coordinates the steps move
+        call("dpb_ghost_shift_f64", ptr(self.shift), ptr(self.cext), ptr(self.coord),
+             ptr(self.mapping), ptr(self.nall_dev), self.mem_nall, s)
+        width = max(self.nl_width, 256)
+        while True:
+            if self.rows is None or width != self.nl_width:
+                self.rows = torch.full((nloc, width), -1, dtype=torch.int32, device=self.dev)
+                fn = ops._row_pointers(self.rows)
+                if self.firstneigh is None:
+                    self.firstneigh = fn
+                else:
+                    self.firstneigh.copy_(fn)
+                if width != self.nl_width and self.graph is not None:
+                    self.graph = None  # the list width is a launch argument
+                    self._recapture = True
+                self.nl_width = width
+            mx = ctypes.c_int(0)
+            code = _capi.lib().dpb_build_nlist_f64(
+                ptr(self.ilist), ptr(self.numneigh), ptr(self.firstneigh),
+                ctypes.addressof(mx), ptr(self.nl_scratch), self.nl_bytes, ptr(self.cext),
+                nloc, nall, width, ctypes.c_float(self.rc_list), 1, ptr(self.text), s)
+            if code == 1 and mx.value > width:
+                width = (mx.value * 5 // 4 + 31) // 32 * 32
+                continue
+            _capi.check(code, "build_nlist")
+            break
+        self.built = True
+        return nall
 
     # ---- one step, no host synchronisation
     def step(self, timers: dict | None = None):
@@ -425,25 +511,43 @@ class SeAEvaluator:
         cfg, s = self.cfg, torch.cuda.current_stream().cuda_stream
         nloc, nnei = self.nloc, cfg.nnei
         tm = _Stages(timers)
-        with tm("coord"):
-            self.coord_n.copy_(self.coord)
-            call("dpb_normalize_coord_f64", ptr(self.coord_n), nloc, self.box.ctypes.data, s)
-            call("dpb_copy_coord_async_f64", ptr(self.cext), ptr(self.text), ptr(self.mapping),
-                 ptr(self.nall_dev), ptr(self.copy_scratch), self.copy_bytes, ptr(self.coord_n),
-                 ptr(self.atype), nloc, self.mem_nall, ctypes.c_float(cfg.rcut),
-                 self.box.ctypes.data, s)
-        with tm("cell_grid"):
-            call("dpb_cell_grid_build_async_f64", ptr(self.grid), self.grid_bytes,
-                 ptr(self.cext), self.mem_nall, ptr(self.nall_dev), ctypes.c_float(cfg.rcut), s)
-        env = "dpb_env_mat_a_cells_mixed" if self.mode == "compressed" else \
-            "dpb_env_mat_a_cells_f64"
-        with tm("env_mat"):
-            # only em and nlist are stored: em_deriv and rij are recomputed by
-            # the force/virial kernel
-            call(env, ptr(self.em), None, None, ptr(self.nlist),
-                 ptr(self.cext), ptr(self.text), ptr(self.grid), ptr(self.avg), ptr(self.std),
-                 nloc, self.mem_nall, ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth),
-                 self.sec.ctypes.data, self.sec.size, ptr(self.status), s)
+        if self.skin > 0:
+            if not self.built:
+                raise _capi.DPBInvalidArgument("call rebuild() before the first step")
+            with tm("coord"):
+                call("dpb_ghost_refresh_f64", ptr(self.cext), ptr(self.shift), ptr(self.coord),
+                     ptr(self.mapping), ptr(self.nall_dev), self.mem_nall, s)
+            env = "dpb_prod_env_mat_a_mixed" if self.mode == "compressed" else \
+                "dpb_prod_env_mat_a_f64"
+            with tm("env_mat"):
+                call(env, ptr(self.em), None, None, ptr(self.nlist), ptr(self.cext),
+                     ptr(self.text), nloc, ptr(self.ilist), ptr(self.numneigh),
+                     ptr(self.firstneigh), self.nl_width, ptr(self.avg), ptr(self.std), nloc,
+                     self.mem_nall, 1, ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth),
+                     self.sec.ctypes.data, self.sec.size, ptr(self.status), s)
+        else:
+            with tm("coord"):
+                self.coord_n.copy_(self.coord)
+                call("dpb_normalize_coord_f64", ptr(self.coord_n), nloc, self.box.ctypes.data,
+                     s)
+                call("dpb_copy_coord_async_f64", ptr(self.cext), ptr(self.text),
+                     ptr(self.mapping), ptr(self.nall_dev), ptr(self.copy_scratch),
+                     self.copy_bytes, ptr(self.coord_n), ptr(self.atype), nloc, self.mem_nall,
+                     ctypes.c_float(cfg.rcut), self.box.ctypes.data, s)
+            with tm("cell_grid"):
+                call("dpb_cell_grid_build_async_f64", ptr(self.grid), self.grid_bytes,
+                     ptr(self.cext), self.mem_nall, ptr(self.nall_dev),
+                     ctypes.c_float(cfg.rcut), s)
+            env = "dpb_env_mat_a_cells_mixed" if self.mode == "compressed" else \
+                "dpb_env_mat_a_cells_f64"
+            with tm("env_mat"):
+                # only em and nlist are stored: em_deriv and rij are recomputed
+                # by the force/virial kernel
+                call(env, ptr(self.em), None, None, ptr(self.nlist),
+                     ptr(self.cext), ptr(self.text), ptr(self.grid), ptr(self.avg),
+                     ptr(self.std), nloc, self.mem_nall, ctypes.c_float(cfg.rcut),
+                     ctypes.c_float(cfg.rcut_smth), self.sec.ctypes.data, self.sec.size,
+                     ptr(self.status), s)
         if self.mode == "compressed":
             self._descriptor_compressed(s, tm)
         else:
@@ -483,38 +587,43 @@ class SeAEvaluator:
 
     def _descriptor_plain(self):
         cfg = self.cfg
-        nloc, nnei = self.nloc, cfg.nnei
-        with torch.enable_grad():
-            em = self.em.view(nloc, nnei, 4).detach().requires_grad_(True)
-            xyz = None
-            for t in range(cfg.ntypes):
-                a, b = int(self.sec[t]), int(self.sec[t + 1])
-                if b == a:
-                    continue
-                rr = em[:, a:b, :]
-                h = rr[:, :, :1]
-                for W, bb in self.emb[t]:
-                    y = torch.tanh(h @ W + bb)
-                    if W.shape[1] == W.shape[0]:
-                        y = y + h
-                    elif W.shape[1] == 2 * W.shape[0]:
-                        y = y + torch.cat([h, h], -1)
-                    h = y
-                gr = rr.transpose(1, 2) @ h
-                xyz = gr if xyz is None else xyz + gr
-            xyz = xyz / nnei
-            D = (xyz.transpose(1, 2) @ xyz[:, :, :cfg.axis_neuron]).reshape(nloc, -1)
-            Dp = D[self.order]  # rows grouped by type
-            etot = torch.zeros((), dtype=torch.float64, device=self.dev)
-            for t, (a, b) in enumerate(self.type_ranges):
-                if b > a:
-                    etot = etot + self.fitting.forward(t, Dp[a:b]).sum()
-            (g,) = torch.autograd.grad(etot, em)
-        self.energy.copy_(etot.detach().view(1))
-        self.net_deriv.copy_(g.reshape(nloc, nnei * 4))
+        nnei = cfg.nnei
+        etot = torch.zeros((), dtype=torch.float64, device=self.dev)
+        for a, b, per_type in self.plain_chunks:
+            with torch.enable_grad():
+                n = b - a
+                em = self.em[a:b].view(n, nnei, 4).detach().requires_grad_(True)
+                xyz = None
+                for t in range(cfg.ntypes):
+                    s0, s1 = int(self.sec[t]), int(self.sec[t + 1])
+                    if s1 == s0:
+                        continue
+                    rr = em[:, s0:s1, :]
+                    h = rr[:, :, :1]
+                    for W, bb in self.emb[t]:
+                        y = torch.tanh(h @ W + bb)
+                        if W.shape[1] == W.shape[0]:
+                            y = y + h
+                        elif W.shape[1] == 2 * W.shape[0]:
+                            y = y + torch.cat([h, h], -1)
+                        h = y
+                    gr = rr.transpose(1, 2) @ h
+                    xyz = gr if xyz is None else xyz + gr
+                xyz = xyz / nnei
+                D = (xyz.transpose(1, 2) @ xyz[:, :, :cfg.axis_neuron]).reshape(n, -1)
+                e = torch.zeros((), dtype=torch.float64, device=self.dev)
+                for t, idx in enumerate(per_type):
+                    if idx is not None:
+                        e = e + self.fitting.forward(t, D.index_select(0, idx)).sum()
+                (g,) = torch.autograd.grad(e, em)
+            etot = etot + e.detach()
+            self.net_deriv[a:b].copy_(g.reshape(n, nnei * 4))
+        self.energy.copy_(etot.view(1))
 
     # ---- graph capture / replay
     def capture(self, warmup: int = 2):
+        if self.skin > 0 and not self.built:
+            self.rebuild()
         s = torch.cuda.Stream(device=self.dev)
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
@@ -529,6 +638,9 @@ class SeAEvaluator:
         return self
 
     def replay(self):
+        if getattr(self, "_recapture", False):
+            self._recapture = False
+            self.capture()
         if self.graph is None:
             self.step()
         else:
@@ -547,15 +659,19 @@ class SeAEvaluator:
         return int(h[0])
 
     # ---- public call: host in, host out
-    def compute(self, coord, out: torch.Tensor | None = None):
+    def compute(self, coord, out: torch.Tensor | None = None, rebuild: bool = False):
         """Energy (float), force [nloc, 3] and virial [9] of host coordinates.
 
         ``coord`` is a host array/tensor (pinned for an asynchronous copy);
-        ``out`` an optional pinned host buffer of 1 + 3 nloc + 9 doubles."""
+        ``out`` an optional pinned host buffer of 1 + 3 nloc + 9 doubles;
+        ``rebuild`` (skin > 0 only) remakes the ghosts and the list first (it
+        is also done on the first call)."""
         if isinstance(coord, torch.Tensor):
             self.coord.copy_(coord.view(-1, 3), non_blocking=True)
         else:
             self.coord.copy_(torch.as_tensor(np.asarray(coord, np.float64).reshape(-1, 3)))
+        if self.skin > 0 and (rebuild or not self.built):
+            self.rebuild()
         self.replay()
         n = self.nloc
         if out is None:

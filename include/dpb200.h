@@ -140,6 +140,21 @@ DPB_API int dpb_prod_env_mat_a_f32(float* em, float* em_deriv, float* rij,
                                    const int* sec, int nsec, int* status,
                                    dpb_stream_t stream);
 
+/* Mixed precision of the above (no counterpart in the reference): FP64
+ * coordinates (the coordinate differences stay FP64), FP32 em / em_deriv /
+ * rij; em_deriv and rij may be NULL (not written). For an input list built
+ * with a skin (rcut + skin) that is reused over several steps, as an MD
+ * engine passes it; the format keeps r <= rcut. */
+DPB_API int dpb_prod_env_mat_a_mixed(float* em, float* em_deriv, float* rij,
+                                     int* nlist, const double* coord,
+                                     const int* type, int inum, const int* ilist,
+                                     const int* numneigh, int* const* firstneigh,
+                                     int max_nbor_size, const float* avg,
+                                     const float* std_, int nloc, int nall,
+                                     int nframes, float rcut, float rcut_smth,
+                                     const int* sec, int nsec, int* status,
+                                     dpb_stream_t stream);
+
 /* Fused neighbor search + format + environment matrix over a cell grid (one
  * frame): the composition build_nlist_gpu -> prod_env_mat_a_gpu in a single
  * pass, with no intermediate list in HBM. Same outputs as
@@ -257,6 +272,18 @@ DPB_API int dpb_copy_coord_async_f64(double* out_c, int* out_t, int* mapping,
                                      const double* in_c, const int* in_t,
                                      int nloc, int mem_nall, float rcut,
                                      const double* boxt, dpb_stream_t stream);
+/* Ghost positions between neighbor-list rebuilds (no counterpart in the
+ * reference, whose MD engines exchange ghosts themselves): at a rebuild,
+ * shift[j] = cext[j] - coord[mapping[j]] for the first *nall_dev (or mem_nall
+ * when nall_dev is NULL) extended atoms; at later steps
+ * cext[j] = coord[mapping[j]] + shift[j], so every ghost keeps its periodic
+ * image while the atoms move. All arrays FP64 [n, 3] on the device. */
+DPB_API int dpb_ghost_shift_f64(double* shift, const double* cext, const double* coord,
+                                const int* mapping, const int* nall_dev, int mem_nall,
+                                dpb_stream_t stream);
+DPB_API int dpb_ghost_refresh_f64(double* cext, const double* shift, const double* coord,
+                                  const int* mapping, const int* nall_dev, int mem_nall,
+                                  dpb_stream_t stream);
 /* cell grid over the first *nall_dev of mem_nall points (grid sized by
  * dpb_cell_grid_bytes(mem_nall); pass mem_nall as nall to the env kernels). */
 DPB_API int dpb_cell_grid_build_async_f64(void* grid, long long grid_bytes,
