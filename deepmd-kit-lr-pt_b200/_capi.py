@@ -83,6 +83,10 @@ _FUNCS = {
     "dpb_tabulate_fusion_se_a_grad_grad_f64": "ppppppp" "iiip",
     "dpb_tabulate_fusion_se_a_grad_grad_f32": "ppppppp" "iiip",
     "dpb_prod_force_a_f64": "ppppiiiip",
+    "dpb_prod_force_grad_a_f64": "ppppiiip",
+    "dpb_prod_force_grad_a_f32": "ppppiiip",
+    "dpb_prod_virial_grad_a_f64": "pppppiip",
+    "dpb_prod_virial_grad_a_f32": "pppppiip",
     "dpb_prod_force_a_f32": "ppppiiiip",
     "dpb_prod_virial_a_f64": "pppppp" "iiip",
     "dpb_prod_virial_a_f32": "pppppp" "iiip",

@@ -78,6 +78,22 @@ int c_virial(double* v, double* av, const double* nd, const double* ed, const do
              const int* nl, int a, int b, int c) {
   return dpb_prod_virial_a_f64(v, av, nd, ed, r, nl, a, b, c, nullptr);
 }
+int c_force_grad(float* g, const float* gr, const float* ed, const int* nl, int a, int b,
+                 int c) {
+  return dpb_prod_force_grad_a_f32(g, gr, ed, nl, a, b, c, nullptr);
+}
+int c_force_grad(double* g, const double* gr, const double* ed, const int* nl, int a, int b,
+                 int c) {
+  return dpb_prod_force_grad_a_f64(g, gr, ed, nl, a, b, c, nullptr);
+}
+int c_virial_grad(float* g, const float* gr, const float* ed, const float* r, const int* nl,
+                  int a, int b) {
+  return dpb_prod_virial_grad_a_f32(g, gr, ed, r, nl, a, b, nullptr);
+}
+int c_virial_grad(double* g, const double* gr, const double* ed, const double* r,
+                  const int* nl, int a, int b) {
+  return dpb_prod_virial_grad_a_f64(g, gr, ed, r, nl, a, b, nullptr);
+}
 int c_env(float* em, float* ed, float* r, int* nl, const float* c, const int* t, int inum,
           const int* il, const int* nn, int* const* fn, int mx, const float* av, const float* sd,
           int nloc, int nall, int nf, float rc, float rs, const int* sec, int nsec, int* st) {
@@ -207,6 +223,24 @@ void prod_virial_a_gpu(FPTYPE* virial, FPTYPE* atom_virial, const FPTYPE* net_de
   sync("prod_virial_a_gpu");
 }
 
+template <typename FPTYPE>
+void prod_force_grad_a_gpu(FPTYPE* grad_net, const FPTYPE* grad, const FPTYPE* env_deriv,
+                           const int* nlist, const int nloc, const int nnei,
+                           const int nframes) {
+  raise(c_force_grad(grad_net, grad, env_deriv, nlist, nloc, nnei, nframes),
+        "prod_force_grad_a_gpu");
+  sync("prod_force_grad_a_gpu");
+}
+
+template <typename FPTYPE>
+void prod_virial_grad_a_gpu(FPTYPE* grad_net, const FPTYPE* grad, const FPTYPE* env_deriv,
+                            const FPTYPE* rij, const int* nlist, const int nloc,
+                            const int nnei) {
+  raise(c_virial_grad(grad_net, grad, env_deriv, rij, nlist, nloc, nnei),
+        "prod_virial_grad_a_gpu");
+  sync("prod_virial_grad_a_gpu");
+}
+
 #define DPB_INSTANTIATE(T)                                                                   \
   template int build_nlist_gpu<T>(InputNlist&, int*, int*, const T*, const int&, const int&, \
                                   const int&, const float&, const int&, const int*);         \
@@ -228,7 +262,11 @@ void prod_virial_a_gpu(FPTYPE* virial, FPTYPE* atom_virial, const FPTYPE* net_de
   template void prod_force_a_gpu<T>(T*, const T*, const T*, const int*, const int,           \
                                     const int, const int, const int);                        \
   template void prod_virial_a_gpu<T>(T*, T*, const T*, const T*, const T*, const int*,       \
-                                     const int, const int, const int);
+                                     const int, const int, const int);                       \
+  template void prod_force_grad_a_gpu<T>(T*, const T*, const T*, const int*, const int,      \
+                                         const int, const int);                              \
+  template void prod_virial_grad_a_gpu<T>(T*, const T*, const T*, const T*, const int*,      \
+                                          const int, const int);
 
 DPB_INSTANTIATE(float)
 DPB_INSTANTIATE(double)

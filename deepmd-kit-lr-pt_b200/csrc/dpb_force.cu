@@ -92,6 +92,97 @@ k_prod_virial(T* __restrict__ virial, T* __restrict__ atom_virial,
   block_add9<FW>(vs, virial);
 }
 
+// Adjoints of prod_force_a / prod_virial_a with respect to net_deriv (the TF
+// path's second derivatives), one thread per (row, descriptor element):
+//   force:  g[i,a] = -sum_d grad[i,d] ed[i,a,d]
+//                    + sum_d grad[f, j mod nloc, d] ed[i,a,d]   (slot a/4 -> j >= 0)
+//   virial: g[i,a] = sum_{d0,d1} grad[d0,d1] rij[i,a/4,d1] ed[i,a,d0]   (j >= 0)
+// with the reference's operation order (prod_force_grad.cc:22-70,
+// prod_virial_grad.cc:21-62).
+template <typename T>
+__global__ void k_prod_force_grad(T* __restrict__ gnet, const T* __restrict__ grad,
+                                  const T* __restrict__ ed, const int* __restrict__ nlist,
+                                  int nloc, int nnei, long long n) {
+  const int ndescrpt = nnei * 4;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n;
+       o += (long long)gridDim.x * blockDim.x) {
+    const long long row = o / ndescrpt;
+    const int a = (int)(o - row * ndescrpt);
+    const T* e = ed + o * 3;
+    T g = (T)0.;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) g -= grad[row * 3 + d] * e[d];
+    int j = nlist[row * nnei + a / 4];
+    if (j >= nloc) j = j % nloc;
+    if (j >= 0) {
+      const long long f = row / nloc;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) g += grad[(f * nloc + j) * 3 + d] * e[d];
+    }
+    gnet[o] = g;
+  }
+}
+
+template <typename T>
+__global__ void k_prod_virial_grad(T* __restrict__ gnet, const T* __restrict__ grad,
+                                   const T* __restrict__ ed, const T* __restrict__ rij,
+                                   const int* __restrict__ nlist, int nnei, long long n) {
+  const int ndescrpt = nnei * 4;
+  T gv[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) gv[k] = grad[k];
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n;
+       o += (long long)gridDim.x * blockDim.x) {
+    const long long row = o / ndescrpt;
+    const int a = (int)(o - row * ndescrpt);
+    const int jj = a / 4;
+    T g = (T)0.;
+    if (nlist[row * nnei + jj] >= 0) {
+      const T* e = ed + o * 3;
+      const T* r = rij + (row * nnei + jj) * 3;
+      // the reference's literal -1.0 is a double: in the FP32 build the
+      // product and the subtraction are done in double, then rounded
+#pragma unroll
+      for (int d0 = 0; d0 < 3; ++d0)
+#pragma unroll
+        for (int d1 = 0; d1 < 3; ++d1)
+          g = (T)((double)g - -1.0 * (double)gv[d0 * 3 + d1] * (double)r[d1] * (double)e[d0]);
+    }
+    gnet[o] = g;
+  }
+}
+
+template <typename T>
+static int prod_force_grad(T* gnet, const T* grad, const T* ed, const int* nlist, int nloc,
+                           int nnei, int nframes, cudaStream_t st) {
+  if (nloc < 0 || nnei < 0 || nframes < 1) {
+    set_error("prod_force_grad_a: invalid sizes (nloc=%d nnei=%d nframes=%d)", nloc, nnei,
+              nframes);
+    return DPB_ERR_INVALID;
+  }
+  const long long n = (long long)nframes * nloc * nnei * 4;
+  if (n == 0) return DPB_OK;
+  k_prod_force_grad<T><<<grid_stride_blocks(n, 256), 256, 0, st>>>(gnet, grad, ed, nlist,
+                                                                   nloc, nnei, n);
+  DPB_CHECK_LAUNCH("prod_force_grad_a");
+  return DPB_OK;
+}
+
+template <typename T>
+static int prod_virial_grad(T* gnet, const T* grad, const T* ed, const T* rij,
+                            const int* nlist, int nloc, int nnei, cudaStream_t st) {
+  if (nloc < 0 || nnei < 0) {
+    set_error("prod_virial_grad_a: invalid sizes (nloc=%d nnei=%d)", nloc, nnei);
+    return DPB_ERR_INVALID;
+  }
+  const long long n = (long long)nloc * nnei * 4;
+  if (n == 0) return DPB_OK;
+  k_prod_virial_grad<T><<<grid_stride_blocks(n, 256), 256, 0, st>>>(gnet, grad, ed, rij,
+                                                                    nlist, nnei, n);
+  DPB_CHECK_LAUNCH("prod_virial_grad_a");
+  return DPB_OK;
+}
+
 template <typename T>
 static int prod_force(T* force, const T* nd, const T* ed, const int* nlist,
                       int nloc, int nall, int nnei, int nframes, cudaStream_t st) {
@@ -163,6 +254,34 @@ int dpb_prod_virial_a_f32(float* virial, float* atom_virial,
                           int nall, int nnei, dpb_stream_t stream) {
   return prod_virial<float>(virial, atom_virial, net_deriv, env_deriv, rij,
                             nlist, nloc, nall, nnei, as_stream(stream));
+}
+
+int dpb_prod_force_grad_a_f64(double* grad_net, const double* grad, const double* env_deriv,
+                              const int* nlist, int nloc, int nnei, int nframes,
+                              dpb_stream_t stream) {
+  return prod_force_grad<double>(grad_net, grad, env_deriv, nlist, nloc, nnei, nframes,
+                                 as_stream(stream));
+}
+
+int dpb_prod_force_grad_a_f32(float* grad_net, const float* grad, const float* env_deriv,
+                              const int* nlist, int nloc, int nnei, int nframes,
+                              dpb_stream_t stream) {
+  return prod_force_grad<float>(grad_net, grad, env_deriv, nlist, nloc, nnei, nframes,
+                                as_stream(stream));
+}
+
+int dpb_prod_virial_grad_a_f64(double* grad_net, const double* grad, const double* env_deriv,
+                               const double* rij, const int* nlist, int nloc, int nnei,
+                               dpb_stream_t stream) {
+  return prod_virial_grad<double>(grad_net, grad, env_deriv, rij, nlist, nloc, nnei,
+                                  as_stream(stream));
+}
+
+int dpb_prod_virial_grad_a_f32(float* grad_net, const float* grad, const float* env_deriv,
+                               const float* rij, const int* nlist, int nloc, int nnei,
+                               dpb_stream_t stream) {
+  return prod_virial_grad<float>(grad_net, grad, env_deriv, rij, nlist, nloc, nnei,
+                                 as_stream(stream));
 }
 
 }  // extern "C"

@@ -271,6 +271,35 @@ def prod_virial_a(net_deriv: torch.Tensor, env_deriv: torch.Tensor, rij: torch.T
     return virial, av
 
 
+def prod_force_grad_a(grad: torch.Tensor, env_deriv: torch.Tensor, nlist: torch.Tensor,
+                      nloc: int, nframes: int = 1) -> torch.Tensor:
+    """prod_force_grad_a_gpu (prod_force_grad.h:26-32): d(force . grad)/d(net_deriv),
+    [nframes * nloc, nnei * 4]."""
+    _need_cuda(grad, env_deriv, nlist, what="prod_force_grad_a")
+    ed = env_deriv.contiguous()
+    sfx = _suffix(ed.dtype)
+    nnei = nlist.numel() // (nframes * nloc) if nloc > 0 else 0
+    out = torch.empty((nframes * nloc, nnei * 4), dtype=ed.dtype, device=ed.device)
+    call(f"dpb_prod_force_grad_a_{sfx}", ptr(out), ptr(grad.to(ed.dtype).contiguous()), ptr(ed),
+         ptr(nlist.to(torch.int32).contiguous()), nloc, nnei, nframes, _stream())
+    return out
+
+
+def prod_virial_grad_a(grad: torch.Tensor, env_deriv: torch.Tensor, rij: torch.Tensor,
+                       nlist: torch.Tensor, nloc: int) -> torch.Tensor:
+    """prod_virial_grad_a_gpu (prod_virial_grad.h:26-32): d(virial . grad)/d(net_deriv),
+    [nloc, nnei * 4]."""
+    _need_cuda(grad, env_deriv, rij, nlist, what="prod_virial_grad_a")
+    ed = env_deriv.contiguous()
+    sfx = _suffix(ed.dtype)
+    nnei = nlist.numel() // nloc if nloc > 0 else 0
+    out = torch.empty((nloc, nnei * 4), dtype=ed.dtype, device=ed.device)
+    call(f"dpb_prod_virial_grad_a_{sfx}", ptr(out), ptr(grad.to(ed.dtype).contiguous()),
+         ptr(ed), ptr(rij.to(ed.dtype).contiguous()), ptr(nlist.to(torch.int32).contiguous()),
+         nloc, nnei, _stream())
+    return out
+
+
 # ------------------------------------------------- torch.ops.deepmd.* ops --
 
 def _check_tab(table, table_info, tensors, what):

@@ -128,4 +128,18 @@ DPB_CXX_API void prod_virial_a_gpu(FPTYPE* virial, FPTYPE* atom_virial,
                                    const int* nlist, const int nloc,
                                    const int nall, const int nnei);
 
+// source/lib/include/prod_force_grad.h:26-32
+template <typename FPTYPE>
+DPB_CXX_API void prod_force_grad_a_gpu(FPTYPE* grad_net, const FPTYPE* grad,
+                                       const FPTYPE* env_deriv, const int* nlist,
+                                       const int nloc, const int nnei,
+                                       const int nframes);
+
+// source/lib/include/prod_virial_grad.h:26-32
+template <typename FPTYPE>
+DPB_CXX_API void prod_virial_grad_a_gpu(FPTYPE* grad_net, const FPTYPE* grad,
+                                        const FPTYPE* env_deriv, const FPTYPE* rij,
+                                        const int* nlist, const int nloc,
+                                        const int nnei);
+
 }  // namespace deepmd

@@ -155,6 +155,26 @@ DPB_API int dpb_prod_env_mat_a_mixed(float* em, float* em_deriv, float* rij,
                                      const int* sec, int nsec, int* status,
                                      dpb_stream_t stream);
 
+/* prod_force_grad_a_gpu / prod_virial_grad_a_gpu (prod_force_grad.h:26-32,
+ * prod_virial_grad.h:26-32): gradients of the force and the virial with
+ * respect to net_deriv. grad_net [nframes * nloc, nnei * 4] is fully written
+ * (no memset needed); grad is [nframes, nloc, 3] (force) or [9] (virial);
+ * neighbor indices >= nloc are taken modulo nloc, as in the reference. */
+DPB_API int dpb_prod_force_grad_a_f64(double* grad_net, const double* grad,
+                                      const double* env_deriv, const int* nlist, int nloc,
+                                      int nnei, int nframes, dpb_stream_t stream);
+DPB_API int dpb_prod_force_grad_a_f32(float* grad_net, const float* grad,
+                                      const float* env_deriv, const int* nlist, int nloc,
+                                      int nnei, int nframes, dpb_stream_t stream);
+DPB_API int dpb_prod_virial_grad_a_f64(double* grad_net, const double* grad,
+                                       const double* env_deriv, const double* rij,
+                                       const int* nlist, int nloc, int nnei,
+                                       dpb_stream_t stream);
+DPB_API int dpb_prod_virial_grad_a_f32(float* grad_net, const float* grad,
+                                       const float* env_deriv, const float* rij,
+                                       const int* nlist, int nloc, int nnei,
+                                       dpb_stream_t stream);
+
 /* Fused neighbor search + format + environment matrix over a cell grid (one
  * frame): the composition build_nlist_gpu -> prod_env_mat_a_gpu in a single
  * pass, with no intermediate list in HBM. Same outputs as

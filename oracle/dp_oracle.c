@@ -592,6 +592,53 @@ int orc_copy_coord(double* out_c, int* out_t, int* mapping, int* nall,
         }                                                                      \
       }                                                                        \
     return 0;                                                                  \
+  }                                                                            \
+                                                                               \
+  int orc_prod_force_grad_a_##SUF(T* gnet, const T* grad, const T* ed,         \
+                                  const int* nlist, int nloc, int nnei,        \
+                                  int nframes) {                               \
+    /* source/lib/src/prod_force_grad.cc:22-70: minus the center term, plus  \
+       the term of the slot's neighbor (index taken modulo nloc) */           \
+    int ndes = 4 * nnei;                                                       \
+    for (int i = 0; i < nframes * nloc; ++i) {                                 \
+      int f = i / nloc;                                                        \
+      for (int aa = 0; aa < ndes; ++aa) {                                      \
+        const T* e = ed + ((size_t)i * ndes + aa) * 3;                         \
+        T g = (T)0.;                                                           \
+        for (int d = 0; d < 3; ++d) g -= grad[(size_t)i * 3 + d] * e[d];       \
+        int j = nlist[(size_t)i * nnei + aa / 4];                              \
+        if (j >= nloc) j = j % nloc;                                           \
+        if (j >= 0)                                                            \
+          for (int d = 0; d < 3; ++d)                                          \
+            g += grad[((size_t)f * nloc + j) * 3 + d] * e[d];                  \
+        gnet[(size_t)i * ndes + aa] = g;                                       \
+      }                                                                        \
+    }                                                                          \
+    return 0;                                                                  \
+  }                                                                            \
+                                                                               \
+  int orc_prod_virial_grad_a_##SUF(T* gnet, const T* grad, const T* ed,        \
+                                   const T* rij, const int* nlist, int nloc,   \
+                                   int nnei) {                                 \
+    /* source/lib/src/prod_virial_grad.cc:21-62 */                            \
+    int ndes = 4 * nnei;                                                       \
+    for (int i = 0; i < nloc; ++i)                                             \
+      for (int aa = 0; aa < ndes; ++aa) {                                      \
+        int jj = aa / 4;                                                       \
+        T g = (T)0.;                                                           \
+        if (nlist[(size_t)i * nnei + jj] >= 0) {                               \
+          const T* e = ed + ((size_t)i * ndes + aa) * 3;                       \
+          const T* r = rij + ((size_t)i * nnei + jj) * 3;                      \
+          /* the reference's literal -1.0 is a double: in the FP32 build the  \
+             product and the subtraction are done in double, then rounded */  \
+          for (int d0 = 0; d0 < 3; ++d0)                                       \
+            for (int d1 = 0; d1 < 3; ++d1)                                     \
+              g = (T)((double)g - -1.0 * (double)grad[d0 * 3 + d1] *           \
+                                      (double)r[d1] * (double)e[d0]);          \
+        }                                                                      \
+        gnet[(size_t)i * ndes + aa] = g;                                       \
+      }                                                                        \
+    return 0;                                                                  \
   }
 
 ORC_DEFINE(double, f64)

@@ -122,6 +122,21 @@ int orc_prod_virial_a_f32(float* virial, float* atom_virial,
                           const float* rij, const int* nlist, int nloc,
                           int nall, int nnei);
 
+/* prod_force_grad_a (source/lib/src/prod_force_grad.cc:22-70) and
+ * prod_virial_grad_a (source/lib/src/prod_virial_grad.cc:21-62). */
+int orc_prod_force_grad_a_f64(double* grad_net, const double* grad,
+                              const double* env_deriv, const int* nlist,
+                              int nloc, int nnei, int nframes);
+int orc_prod_force_grad_a_f32(float* grad_net, const float* grad,
+                              const float* env_deriv, const int* nlist,
+                              int nloc, int nnei, int nframes);
+int orc_prod_virial_grad_a_f64(double* grad_net, const double* grad,
+                               const double* env_deriv, const double* rij,
+                               const int* nlist, int nloc, int nnei);
+int orc_prod_virial_grad_a_f32(float* grad_net, const float* grad,
+                               const float* env_deriv, const float* rij,
+                               const int* nlist, int nloc, int nnei);
+
 #ifdef __cplusplus
 }
 #endif

@@ -218,6 +218,28 @@ class _Lib:
             _ptr(np.ascontiguousarray(nlist, np.int32)), _i(nloc), _i(nall), _i(nnei))
         return virial, av.reshape(nall, 9)
 
+    def prod_force_grad_a(self, grad, env_deriv, nlist, nloc, nframes=1):
+        dt = env_deriv.dtype
+        suf = "f64" if dt == np.float64 else "f32"
+        nnei = nlist.size // (nframes * nloc)
+        out = np.zeros(nframes * nloc * nnei * 4, dt)
+        self.fn(f"prod_force_grad_a_{suf}")(
+            _ptr(out), _ptr(np.ascontiguousarray(grad, dt)),
+            _ptr(np.ascontiguousarray(env_deriv)),
+            _ptr(np.ascontiguousarray(nlist, np.int32)), _i(nloc), _i(nnei), _i(nframes))
+        return out.reshape(nframes * nloc, nnei * 4)
+
+    def prod_virial_grad_a(self, grad, env_deriv, rij, nlist, nloc):
+        dt = env_deriv.dtype
+        suf = "f64" if dt == np.float64 else "f32"
+        nnei = nlist.size // nloc
+        out = np.zeros(nloc * nnei * 4, dt)
+        self.fn(f"prod_virial_grad_a_{suf}")(
+            _ptr(out), _ptr(np.ascontiguousarray(grad, dt)),
+            _ptr(np.ascontiguousarray(env_deriv)), _ptr(np.ascontiguousarray(rij, dt)),
+            _ptr(np.ascontiguousarray(nlist, np.int32)), _i(nloc), _i(nnei))
+        return out.reshape(nloc, nnei * 4)
+
 
 _cache: dict[str, _Lib] = {}
 

@@ -17,7 +17,9 @@
 #include "neighbor_list.h"
 #include "prod_env_mat.h"
 #include "prod_force.h"
+#include "prod_force_grad.h"
 #include "prod_virial.h"
+#include "prod_virial_grad.h"
 #include "region.h"
 #include "tabulate.h"
 
@@ -194,6 +196,28 @@ int dpref_format_nlist_f64(int* nlist, const double* coord, const int* type,
     try {                                                                     \
       deepmd::prod_virial_a_cpu<T>(virial, atom_virial, net_deriv, env_deriv, \
                                    rij, nlist, nloc, nall, nnei);             \
+    } catch (const std::exception&) {                                         \
+      return 2;                                                               \
+    }                                                                         \
+    return 0;                                                                 \
+  }                                                                           \
+  int dpref_prod_force_grad_a_##SUF(T* grad_net, const T* grad,               \
+                                    const T* env_deriv, const int* nlist,     \
+                                    int nloc, int nnei, int nframes) {        \
+    try {                                                                     \
+      deepmd::prod_force_grad_a_cpu<T>(grad_net, grad, env_deriv, nlist,      \
+                                       nloc, nnei, nframes);                  \
+    } catch (const std::exception&) {                                         \
+      return 2;                                                               \
+    }                                                                         \
+    return 0;                                                                 \
+  }                                                                           \
+  int dpref_prod_virial_grad_a_##SUF(T* grad_net, const T* grad,              \
+                                     const T* env_deriv, const T* rij,        \
+                                     const int* nlist, int nloc, int nnei) {  \
+    try {                                                                     \
+      deepmd::prod_virial_grad_a_cpu<T>(grad_net, grad, env_deriv, rij,       \
+                                        nlist, nloc, nnei);                   \
     } catch (const std::exception&) {                                         \
       return 2;                                                               \
     }                                                                         \

@@ -19,13 +19,16 @@ OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_abi_symbols.
 
 FUNCS = ["build_nlist_gpu", "prod_env_mat_a_gpu", "tabulate_fusion_se_a_gpu",
          "tabulate_fusion_se_a_grad_gpu", "tabulate_fusion_se_a_grad_grad_gpu",
-         "prod_force_a_gpu", "prod_virial_a_gpu"]
+         "prod_force_a_gpu", "prod_virial_a_gpu", "prod_force_grad_a_gpu",
+         "prod_virial_grad_a_gpu"]
 
 SRC = """#include "neighbor_list.h"
 #include "prod_env_mat.h"
 #include "tabulate.h"
 #include "prod_force.h"
 #include "prod_virial.h"
+#include "prod_force_grad.h"
+#include "prod_virial_grad.h"
 #include <vector>
 """ + "".join(
     f"void* p_{f}_{t} = (void*)static_cast<decltype(&deepmd::{f}<{t}>)>(&deepmd::{f}<{t}>);\n"

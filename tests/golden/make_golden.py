@@ -9,6 +9,7 @@ hold for the se_e2_a path and stores them as numpy arrays, keyed
 * source/lib/tests/test_prod_virial_a.cc   (expected_virial, expected_atom_virial)
 * source/lib/tests/test_coord.cc           (normalize / copy_coord fixtures)
 * source/lib/tests/test_tabulate_se_a.cc   (table, em_x, em, expected outputs)
+* source/lib/tests/test_prod_{force,virial}_grad_a.cc (expected_grad_net)
 * source/tests/pt/test_tabulate_fusion_se_a.py (op goldens, set up in setUp)
 
 Run in a container that holds the reference tree:
@@ -36,6 +37,8 @@ CC_FILES = [
     "source/lib/tests/test_prod_virial_a.cc",
     "source/lib/tests/test_coord.cc",
     "source/lib/tests/test_tabulate_se_a.cc",
+    "source/lib/tests/test_prod_force_grad_a.cc",
+    "source/lib/tests/test_prod_virial_grad_a.cc",
 ]
 PY_FILE = "source/tests/pt/test_tabulate_fusion_se_a.py"
 

@@ -398,3 +398,48 @@ def test_prod_force_virial_golden(ops, port, ref_fixtures):
     np.testing.assert_allclose(v.cpu().numpy(), ref_fixtures[kv + "expected_virial"], atol=1e-5)
     np.testing.assert_allclose(av.cpu().numpy().reshape(-1),
                                ref_fixtures[kv + "expected_atom_virial"], atol=1e-5)
+
+
+# ------------------------------------------ force / virial second derivatives
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_prod_force_virial_grad(ops, port, wl, dtype):
+    coord, atype, box = wl.water_frame(4, seed=37)
+    rc, rs, sec = 6.0, 0.5, np.array([0, 46, 138])
+    c0, t0, _ = port.copy_coord(coord, atype, rc, box)
+    nloc, nnei = atype.size, 138
+    avg, std = _stats(np.random.default_rng(5), nnei)
+    (e0, ed0, r0, n0), _ = _oracle_env(port, c0, t0, nloc, avg, std, rc, rs, sec, dtype)
+    rng = np.random.default_rng(6)
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    for nframes in (1, 2):
+        gf = rng.normal(size=(nframes * nloc, 3)).astype(dtype)
+        edn = np.tile(ed0.reshape(-1), nframes)
+        nln = np.tile(n0.reshape(-1), nframes)
+        g = ops.prod_force_grad_a(_t(gf, tdt), _t(edn, tdt), _t(nln), nloc, nframes)
+        _close(g.cpu().numpy(), port.prod_force_grad_a(gf, edn, nln, nloc, nframes), dtype,
+               "force_grad")
+    gv = rng.normal(size=9).astype(dtype)
+    g = ops.prod_virial_grad_a(_t(gv, tdt), _t(ed0, tdt), _t(r0, tdt), _t(n0), nloc)
+    _close(g.cpu().numpy(), port.prod_virial_grad_a(gv, ed0, r0, n0, nloc), dtype, "virial_grad")
+
+
+def test_prod_force_virial_grad_golden(ops, port, ref_fixtures):
+    fx = ref_fixtures
+    for key, kind in (("test_prod_force_grad_a.cc:TestProdForceGradA:", "force"),
+                      ("test_prod_virial_grad_a.cc:TestProdVirialGradA:", "virial")):
+        posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+        box = np.diag([13.0] * 3).reshape(9)
+        sec = fx[key + "sec_a"].astype(np.int32)
+        c0, t0, _ = port.copy_coord(posi, atype, 6.0, box)
+        nnei = int(sec[-1])
+        avg = np.zeros((2, nnei * 4))
+        std = np.ones((2, nnei * 4))
+        (e0, ed0, r0, n0), _ = _oracle_env(port, c0, t0, 6, avg, std, 6.0, 0.8, sec, np.float64)
+        if kind == "force":
+            grad = 10 - np.arange(18) * 0.1
+            g = ops.prod_force_grad_a(_t(grad), _t(ed0), _t(n0), 6)
+        else:
+            grad = 10 - np.arange(9) * 1.0
+            g = ops.prod_virial_grad_a(_t(grad), _t(ed0), _t(r0), _t(n0), 6)
+        np.testing.assert_allclose(g.cpu().numpy().reshape(-1), fx[key + "expected_grad_net"],
+                                   atol=1e-5, rtol=0)

@@ -100,6 +100,35 @@ def test_prod_virial_golden(port, ref_fixtures):
     np.testing.assert_allclose(av.reshape(-1), fx[key + "expected_atom_virial"], atol=1e-5, rtol=0)
 
 
+def test_prod_force_grad_golden(port, ref_fixtures):
+    """test_prod_force_grad_a.cc: grad[i] = 10 - 0.1 i, two identical frames."""
+    fx = ref_fixtures
+    key = "test_prod_force_grad_a.cc:TestProdForceGradA:"
+    posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+    box = np.diag([13.0] * 3).reshape(9)
+    sec = fx[key + "sec_a"].astype(np.int32)
+    c, t, (em, emd, rij, nlist) = _env_pipeline(port, posi, atype, box, sec)
+    nloc = 6
+    grad = 10 - np.arange(nloc * 3) * 0.1
+    g = port.prod_force_grad_a(np.tile(grad, 2), np.tile(emd.reshape(-1), 2),
+                               np.tile(nlist.reshape(-1), 2), nloc, nframes=2)
+    exp = np.tile(fx[key + "expected_grad_net"], 2)
+    np.testing.assert_allclose(g.reshape(-1), exp, atol=1e-5, rtol=0)
+
+
+def test_prod_virial_grad_golden(port, ref_fixtures):
+    """test_prod_virial_grad_a.cc: grad[k] = 10 - k."""
+    fx = ref_fixtures
+    key = "test_prod_virial_grad_a.cc:TestProdVirialGradA:"
+    posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+    box = np.diag([13.0] * 3).reshape(9)
+    sec = fx[key + "sec_a"].astype(np.int32)
+    c, t, (em, emd, rij, nlist) = _env_pipeline(port, posi, atype, box, sec)
+    grad = 10 - np.arange(9) * 1.0
+    g = port.prod_virial_grad_a(grad, emd, rij, nlist, 6)
+    np.testing.assert_allclose(g.reshape(-1), fx[key + "expected_grad_net"], atol=1e-5, rtol=0)
+
+
 def _sorted_ghosts(c, t, m, nloc):
     rows = sorted(zip(map(tuple, c[nloc:].tolist()), t[nloc:].tolist(), m[nloc:].tolist()))
     return rows
@@ -237,10 +266,20 @@ def test_port_equals_reference_random(port, ref_lib, dtype):
                                   ref_lib.prod_force_a(nd, emd, nlist, nloc, nall))
     v0, a0 = port.prod_virial_a(nd, emd, rij, nlist, nloc, nall)
     v1, a1 = ref_lib.prod_virial_a(nd, emd, rij, nlist, nloc, nall)
-    # the reference accumulates the virial under an OpenMP atomic in thread order
-    tol = 1e-12 if dtype == np.float64 else 1e-5
+    # the reference accumulates the virial under an OpenMP atomic in thread
+    # order, so FP32 sums of a few hundred terms differ run to run in the
+    # last digits
+    tol = 1e-12 if dtype == np.float64 else 1e-4
     np.testing.assert_allclose(v0, v1, rtol=tol, atol=tol)
     np.testing.assert_allclose(a0, a1, rtol=tol, atol=tol)
+    # second derivatives (prod_force_grad_a / prod_virial_grad_a), neighbor
+    # indices of ghosts folded modulo nloc as the reference does
+    gf = rng.normal(size=(nloc, 3)).astype(dtype)
+    np.testing.assert_array_equal(port.prod_force_grad_a(gf, emd, nlist, nloc),
+                                  ref_lib.prod_force_grad_a(gf, emd, nlist, nloc))
+    gv = rng.normal(size=9).astype(dtype)
+    np.testing.assert_array_equal(port.prod_virial_grad_a(gv, emd, rij, nlist, nloc),
+                                  ref_lib.prod_virial_grad_a(gv, emd, rij, nlist, nloc))
 
 
 def test_format_nlist_ties_break_by_index(port):
