@@ -93,6 +93,7 @@ _FUNCS = {
     "dpb_copy_coord_async_f64": "ppppp" "L" "ppiifpp",
     "dpb_cell_grid_build_async_f64": "pLpipfp",
     "dpb_se_a_pack_table_f32": "ppiip",
+    "dpb_se_a_build_table_f64": "pppiipppipLp",
     "dpb_se_a_descriptor_fwd_f32": "pppp" "pp" "pi" "iiip",
     "dpb_se_a_descriptor_bwd_f32": "ppppp" "pp" "pi" "iiip",
     "dpb_force_virial_a_f32": "pppppp" "pp" "iiiip",
@@ -107,6 +108,7 @@ _SIZE_QUERIES = {
     "dpb_cell_grid_bytes": ("i", LL),
     "dpb_build_nlist_scratch_bytes": ("ii", LL),
     "dpb_build_nlist_noalloc_max_bytes": ("", LL),
+    "dpb_se_a_build_table_scratch_bytes": ("ii", LL),
 }
 
 _lib = None

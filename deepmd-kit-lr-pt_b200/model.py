@@ -138,12 +138,17 @@ def env_stats(params: SeAParams, coord: np.ndarray, atype: np.ndarray, box: np.n
 
 
 def prepare(params: SeAParams, coord, atype, box, device="cuda:0", with_tables=True):
-    """Statistics from the frame and (optionally) the FP64 compression tables."""
+    """Statistics from the frame and (optionally) the FP64 compression tables
+    (built on the device, dpb_se_a_build_table_f64)."""
     davg, dstd, min_dist = env_stats(params, coord, atype, box, device)
     params.davg, params.dstd = davg, dstd
     if with_tables:
-        params.tables = table_mod.build_tables(params.emb, davg, dstd, params.cfg.sel, min_dist,
-                                               params.cfg.rcut_smth, params.cfg.rcut)
+        # FP64 tables built on the device, kept on the host as the model's
+        # compressed data (the evaluators upload them in their own layout)
+        dev_tables = table_mod.build_tables_device(params.emb, davg, dstd, params.cfg.sel,
+                                                   min_dist, params.cfg.rcut_smth,
+                                                   params.cfg.rcut, device=device)
+        params.tables = [(t.cpu().numpy(), info) for t, info in dev_tables]
     return params
 
 

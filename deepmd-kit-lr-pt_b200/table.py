@@ -9,9 +9,10 @@ coefficients (ascending powers of t = x - x_r) at columns 6m..6m+5: the layout
 the tabulate kernels read (source/lib/src/tabulate.cc:190-197).
 
 Grid and bounds follow the reference compressor (deepmd/utils/tabulate.py:
-67-152, 468-486): lower = floor(min_t(-davg_t / dstd_t)), upper =
-ceil(max_t((s(r_min)/r_min - davg_t) / dstd_t)) over the radial column, stride0
-on [lower, upper), stride1 on [upper, extrapolate * upper), and
+67-152, 468-486): lower / upper from the four normalised columns of the
+first slot (floor of -davg/dstd, ceil of (s(r_min)/r_min - davg)/dstd, min /
+max over columns and types), stride0 on [lower, upper), stride1 on
+[upper, extrapolate * upper), and
 table_info = [lower, upper, extrapolate * upper, stride0, stride1, -1]
 (deepmd/pt/model/descriptor/se_a.py:725-734).
 """
@@ -82,12 +83,19 @@ def hermite_quintic(xx: np.ndarray, vv, dd, d2, nspline: int, steps: np.ndarray)
 
 def env_range(davg: np.ndarray, dstd: np.ndarray, min_nbor_dist: float, rcut_smth: float,
               rcut: float):
-    """Per center type (lower, upper) of the normalized radial input."""
+    """Per center type (lower, upper) of the normalized table input.
+
+    As the reference compressor does for se_a (deepmd/utils/tabulate.py:
+    468-486 with the descriptor's statistics shaped [ntypes, nnei, 4], then
+    :94-96): the bounds are taken over the four columns of the first slot,
+    (0 - davg) / dstd and (s(r_min)/r_min - davg) / dstd, floored / ceiled
+    per column, then the minimum / maximum over the columns; the angular
+    columns (davg 0, their own dstd) usually set the upper bound."""
     sw = spline5_switch(min_nbor_dist, rcut_smth, rcut)
-    a0 = davg.reshape(davg.shape[0], -1, 4)[:, 0, 0]
-    s0 = dstd.reshape(dstd.shape[0], -1, 4)[:, 0, 0]
-    lower = np.floor(-a0 / s0)
-    upper = np.ceil(((1.0 / min_nbor_dist) * sw - a0) / s0)
+    a0 = davg.reshape(davg.shape[0], -1, 4)[:, 0, :]
+    s0 = dstd.reshape(dstd.shape[0], -1, 4)[:, 0, :]
+    lower = np.floor(-a0 / s0).min(axis=1)
+    upper = np.ceil(((1.0 / min_nbor_dist) * sw - a0) / s0).max(axis=1)
     return lower, upper
 
 
@@ -104,14 +112,63 @@ def build_tables(emb_layers, davg, dstd, sel, min_nbor_dist: float, rcut_smth: f
     for net in range(len(emb_layers)):
         uu = float(np.max(upper[valid]))
         ll = float(np.min(lower[valid]))
-        xx = np.arange(ll, uu, stride0, dtype=np.float64)
-        xx = np.append(xx, np.arange(uu, extrapolate * uu, stride1, dtype=np.float64))
-        xx = np.append(xx, np.array([extrapolate * uu]))
-        nspline = int((uu - ll) / stride0 + (extrapolate * uu - uu) / stride1)
+        xx, steps, nspline = _grid(ll, uu, extrapolate, stride0, stride1)
         vv, dd, d2 = embedding_derivatives(emb_layers[net], xx)
-        steps = np.full(nspline, stride1)
-        steps[: int((uu - ll) / stride0)] = stride0
         table = hermite_quintic(xx, vv, dd, d2, nspline, steps)
         info = np.array([int(ll), int(uu), int(uu) * extrapolate, stride0, stride1, -1.0])
         out.append((table, info))
     return out
+
+
+def _grid(ll: float, uu: float, extrapolate: float, stride0: float, stride1: float):
+    """The compressor's x grid, interval widths and row count
+    (deepmd/utils/tabulate.py:135-147)."""
+    xx = np.arange(ll, uu, stride0, dtype=np.float64)
+    xx = np.append(xx, np.arange(uu, extrapolate * uu, stride1, dtype=np.float64))
+    xx = np.append(xx, np.array([extrapolate * uu]))
+    nspline = int((uu - ll) / stride0 + (extrapolate * uu - uu) / stride1)
+    steps = np.full(nspline, stride1)
+    steps[: int((uu - ll) / stride0)] = stride0
+    return xx, steps, nspline
+
+
+def build_tables_device(emb_layers, davg, dstd, sel, min_nbor_dist: float, rcut_smth: float,
+                        rcut: float, device="cuda:0", extrapolate: float = 5.0,
+                        stride0: float = 0.01, stride1: float = 0.1):
+    """build_tables on the GPU (dpb_se_a_build_table_f64): the same grid and
+    table_info, the embedding-net derivatives and the Hermite coefficients in
+    FP64 on the device. Returns a list of (table [nspline, 6M] FP64 device
+    tensor, info [6] numpy) per neighbor type."""
+    import ctypes
+
+    import torch
+
+    from . import _capi
+
+    dev = torch.device(device)
+    lower, upper = env_range(davg, dstd, min_nbor_dist, rcut_smth, rcut)
+    valid = [t for t in range(len(sel)) if sel[t] > 0]
+    uu = float(np.max(upper[valid]))
+    ll = float(np.min(lower[valid]))
+    xx, steps, nspline = _grid(ll, uu, extrapolate, stride0, stride1)
+    x_d = torch.tensor(xx, dtype=torch.float64, device=dev)
+    s_d = torch.tensor(steps, dtype=torch.float64, device=dev)
+    info = np.array([int(ll), int(uu), int(uu) * extrapolate, stride0, stride1, -1.0])
+    out = []
+    for net in emb_layers:
+        Ws = [torch.tensor(np.asarray(W, np.float64), device=dev).contiguous() for W, _ in net]
+        bs = [torch.tensor(np.asarray(b, np.float64), device=dev).contiguous() for _, b in net]
+        widths = np.array([1] + [int(W.shape[1]) for W, _ in net], np.int32)
+        M = int(widths[-1])
+        sbytes = int(_capi.lib().dpb_se_a_build_table_scratch_bytes(xx.size, M))
+        scratch = torch.empty(sbytes, dtype=torch.uint8, device=dev)
+        table = torch.empty((nspline, 6 * M), dtype=torch.float64, device=dev)
+        wp = (ctypes.c_void_p * len(Ws))(*[w.data_ptr() for w in Ws])
+        bp = (ctypes.c_void_p * len(bs))(*[b.data_ptr() for b in bs])
+        _capi.call("dpb_se_a_build_table_f64", _capi.ptr(table), _capi.ptr(x_d), _capi.ptr(s_d),
+                   xx.size, nspline, wp, bp, widths.ctypes.data, len(net), _capi.ptr(scratch),
+                   sbytes, torch.cuda.current_stream(dev).cuda_stream)
+        torch.cuda.synchronize(dev)
+        out.append((table, info.copy()))
+    return out
+

@@ -311,6 +311,21 @@ DPB_API int dpb_cell_grid_build_async_f64(void* grid, long long grid_bytes,
                                           const int* nall_dev, float rcut,
                                           dpb_stream_t stream);
 
+/* FP64 compression table of one se_a embedding net, built on the device
+ * (the reference builds it on the host: deepmd/utils/tabulate.py:275-371).
+ * xx: device [npoints] grid, steps: device [nspline] interval widths
+ * (npoints >= nspline + 1); W[l] / b[l]: host arrays of device pointers to the
+ * FP64 layer weights [widths[l], widths[l+1]] (row-major) and biases, widths:
+ * host [nlayers + 1] with widths[0] = 1, each width <= 512, nlayers <= 8.
+ * table: device [nspline, 6 * M] in the tabulate layout (M = widths[nlayers]).
+ * scratch: device, dpb_se_a_build_table_scratch_bytes(npoints, M) bytes. */
+DPB_API long long dpb_se_a_build_table_scratch_bytes(int npoints, int M);
+DPB_API int dpb_se_a_build_table_f64(double* table, const double* xx, const double* steps,
+                                     int npoints, int nspline, const double* const* W,
+                                     const double* const* b, const int* widths, int nlayers,
+                                     void* scratch, long long scratch_bytes,
+                                     dpb_stream_t stream);
+
 /* Repacks one compression table from the tabulate layout [nrow][M][6]
  * (source/lib/src/tabulate.cc:190-197) into the layout the fused descriptor
  * kernels below read, [nrow][6][M] (coefficient-major: a warp's loads of one

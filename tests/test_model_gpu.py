@@ -100,3 +100,40 @@ def test_graph_replay_equals_eager(mdl, gold, mode):
     np.testing.assert_allclose(F2, F3, atol=tol * max(1.0, np.abs(F3).max()))
     # order of atomic adds differs between runs: results agree to rounding only
     np.testing.assert_allclose(V1, V0, rtol=1e-9 if mode == "plain" else 1e-5, atol=1e-9)
+
+
+def _quintic_close(a, b, rows, info, M):
+    """a0..a2 to 1e-12 and the quintic to 1e-12 across each interval (a3..a5
+    carry the cancellation of their formulas, divided by up to h^5)."""
+    a, b = a.reshape(-1, M, 6), b.reshape(-1, M, 6)
+    assert np.abs(a[:, :, :3] - b[:, :, :3]).max() <= 1e-12
+    first = int((info[1] - info[0]) / info[3])
+    h = np.where(rows < first, info[3], info[4])[:, None]
+    for frac in (0.0, 0.37, 0.999):
+        pw = np.stack([(h * frac) ** k for k in range(6)], -1)
+        assert np.abs(((a - b) * pw).sum(-1)).max() <= 1e-12, frac
+
+
+def test_device_tables_match_host_builder_and_reference(dpb):
+    """dpb_se_a_build_table_f64 against the FP64 host builder (every row) and
+    the reference compressor's rows (tests/golden/table_golden.npz)."""
+    mdl = importlib.import_module("deepmd_kit_lr_pt_b200.model")
+    tab = importlib.import_module("deepmd_kit_lr_pt_b200.table")
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    with np.load(os.path.join(here, "table_golden.npz")) as z:
+        g = {k: z[k] for k in z.files}
+    cfg = mdl.SeAConfig()
+    p = mdl.init_params(cfg, seed=1)
+    args = (p.emb, g["davg"], g["dstd"], cfg.sel, float(g["min_nbor_dist"]), cfg.rcut_smth,
+            cfg.rcut)
+    host = tab.build_tables(*args)
+    dev = tab.build_tables_device(*args)
+    M = cfg.neuron[-1]
+    for t in range(cfg.ntypes):
+        td, info = dev[t][0].cpu().numpy(), dev[t][1]
+        np.testing.assert_array_equal(info, host[t][1])
+        np.testing.assert_array_equal(info, g[f"net{t}:info"])
+        assert td.shape == host[t][0].shape == tuple(g[f"net{t}:shape"])
+        _quintic_close(td, host[t][0], np.arange(td.shape[0]), info, M)
+        rows = g[f"net{t}:rows"]
+        _quintic_close(td[rows], g[f"net{t}:table_rows"], rows, info, M)

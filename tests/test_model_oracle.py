@@ -99,3 +99,40 @@ def test_table_reproduces_embedding(mdl, tab):
         c = t0[idx].reshape(-1, 6)
         val = c[:, 0] + (c[:, 1] + (c[:, 2] + (c[:, 3] + (c[:, 4] + c[:, 5] * tt) * tt) * tt) * tt) * tt
         np.testing.assert_allclose(val, ref[k], atol=1e-7)
+
+
+def test_tables_match_reference_compressor(mdl, tab):
+    """The FP64 table builder against the reference's own compressor
+    (tests/golden/table_golden.npz, made by enable_compression of the
+    reference se_a descriptor on the same weights and statistics): identical
+    table_info and shape, coefficients a0..a2 to 1e-12, a3..a5 within the
+    cancellation their formulas amplify (differences of values divided by up to
+    h^5 = 1e-10), and the polynomial itself to 1e-12 across each interval."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_model_golden import weight_checksum
+
+    with np.load(os.path.join(os.path.dirname(GOLD), "table_golden.npz")) as z:
+        g = {k: z[k] for k in z.files}
+    cfg = mdl.SeAConfig()
+    p = mdl.init_params(cfg, seed=1)
+    assert abs(weight_checksum(p) - float(g["weight_checksum"])) < 1e-9
+    tables = tab.build_tables(p.emb, g["davg"], g["dstd"], cfg.sel, float(g["min_nbor_dist"]),
+                              cfg.rcut_smth, cfg.rcut)
+    M = cfg.neuron[-1]
+    tol = [1e-12, 1e-12, 1e-12, 1e-6, 1e-4, 2e-3]
+    for t, (table, info) in enumerate(tables):
+        np.testing.assert_array_equal(info, g[f"net{t}:info"])
+        assert tuple(table.shape) == tuple(g[f"net{t}:shape"])
+        rows = g[f"net{t}:rows"]
+        mine, ref = table[rows].reshape(-1, M, 6), g[f"net{t}:table_rows"].reshape(-1, M, 6)
+        for k in range(6):
+            err = np.abs(mine[:, :, k] - ref[:, :, k]).max()
+            assert err <= tol[k], (t, k, err)
+        first = int((info[1] - info[0]) / info[3])
+        h = np.where(rows < first, info[3], info[4])[:, None]  # [rows, 1]
+        for frac in (0.0, 0.37, 0.999):
+            x = h * frac
+            pw = np.stack([x ** k for k in range(6)], -1)
+            assert np.abs(((mine - ref) * pw).sum(-1)).max() <= 1e-12, (t, frac)
