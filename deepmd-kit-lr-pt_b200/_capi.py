@@ -94,6 +94,9 @@ _FUNCS = {
     "dpb_cell_grid_build_async_f64": "pLpipfp",
     "dpb_se_a_pack_table_f32": "ppiip",
     "dpb_se_a_build_table_f64": "pppiipppipLp",
+    "dpb_batch_env_mat_a_f32": "pppppppppp" "ppppp" "iiff" "pipp",
+    "dpb_batch_force_virial_a": "ppppppp" "ppppp" "iiiiff" "p",
+    "dpb_batch_energy": "pppppip",
     "dpb_se_a_descriptor_fwd_f32": "pppp" "pp" "pi" "iiip",
     "dpb_se_a_descriptor_bwd_f32": "ppppp" "pp" "pi" "iiip",
     "dpb_force_virial_a_f32": "pppppp" "pp" "iiiip",

@@ -1,0 +1,179 @@
+"""Many frames of uneven size and species mix evaluated together: every stage
+is one launch over all frames (geometry through per-frame cell lists with
+periodic images, dpb_batch_env_mat_a_f32; the descriptor and the tensor-core
+fitting over the concatenated rows; dpb_batch_force_virial_a and
+dpb_batch_energy per frame), captured as one CUDA graph.
+
+Frames must have orthorhombic boxes whose edges are all at least rcut.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _capi
+from ._capi import call, ptr
+from .model import SeAParams, _FittingTC
+
+CELL_MARGIN = 1.0001  # cell edge >= rcut * margin, as the single-frame grid
+
+
+class BatchEvaluator:
+    """Energy [F], force [N, 3] and virial [F, 9] of F frames whose atoms are
+    concatenated in frame order (compressed FP32 path, FP64 sums)."""
+
+    def __init__(self, params: SeAParams, frames, device="cuda:0"):
+        cfg = params.cfg
+        self.cfg, self.params = cfg, params
+        self.dev = dev = torch.device(device)
+        self.nframes = F = len(frames)
+        if F == 0:
+            raise _capi.DPBInvalidArgument("no frames")
+        counts, boxes, ncell, types = [], [], [], []
+        for f, (coord, atype, box) in enumerate(frames):
+            b = np.asarray(box, np.float64).reshape(3, 3)
+            if np.any(b - np.diag(np.diag(b))):
+                raise _capi.DPBInvalidArgument(f"frame {f}: the batched path needs an "
+                                               "orthorhombic box")
+            L = np.diag(b)
+            nc = np.floor(L / (cfg.rcut * CELL_MARGIN)).astype(np.int64)
+            if np.any(nc < 1):
+                raise _capi.DPBInvalidArgument(
+                    f"frame {f}: box edges {L} must be at least rcut ({cfg.rcut})")
+            if int(np.prod(nc)) > 4096 or atype.size > 600000:
+                raise _capi.DPBInvalidArgument(f"frame {f}: more than 4096 cells or 600,000 "
+                                               "atoms")
+            counts.append(int(atype.size))
+            boxes.append(L)
+            ncell.append(nc)
+            types.append(np.asarray(atype, np.int32))
+        self.counts = np.array(counts)
+        self.N = N = int(self.counts.sum())
+        atom_off = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int32)
+        cells = np.array([int(np.prod(c)) + 1 for c in ncell])
+        cell_off = np.concatenate([[0], np.cumsum(cells)]).astype(np.int32)
+        row_frame = np.repeat(np.arange(F, dtype=np.int32), self.counts)
+        atype_all = np.concatenate(types)
+        i32 = lambda a: torch.tensor(np.ascontiguousarray(a, np.int32), device=dev)  # noqa: E731
+        self.atom_off_h = atom_off
+        self.atom_off, self.cell_off = i32(atom_off), i32(cell_off)
+        self.box = torch.tensor(np.array(boxes), dtype=torch.float64, device=dev)
+        self.ncell = i32(np.array(ncell))
+        self.row_frame = i32(row_frame)
+        self.type = i32(atype_all)
+        nnei, M, ax = cfg.nnei, cfg.neuron[-1], cfg.axis_neuron
+        f64, f32 = torch.float64, torch.float32
+        z = lambda shape, dt: torch.zeros(shape, dtype=dt, device=dev)  # noqa: E731
+        self.coord = z((N, 3), f64)
+        self.cw = z((N, 3), f64)
+        self.cell_of = z(N, torch.int32)
+        self.cell_atoms = z(N, torch.int32)
+        self.cell_start = z(int(cell_off[-1]), torch.int32)
+        self.em = z((N, nnei * 4), f32)
+        self.nlist = z((N, nnei), torch.int32)
+        self.xyz = z((N, 4, M), f32)
+        self.D = z((N, M * ax), f32)
+        self.dD = z((N, M * ax), f32)
+        self.net_deriv = z((N, nnei * 4), f32)
+        self.force = z((N, 3), f64)
+        self.virial = z((F, 9), f64)
+        self.energy = z(F, f64)
+        self.status = z(1, torch.int32)
+        self.avg = torch.tensor(params.davg, dtype=f32, device=dev)
+        self.std = torch.tensor(params.dstd, dtype=f32, device=dev)
+        # fitting rows grouped by type over all frames
+        order = np.argsort(atype_all, kind="stable")
+        drow = np.empty(N, np.int32)
+        drow[order] = np.arange(N, dtype=np.int32)
+        self.drow = i32(drow)
+        tcount = np.bincount(atype_all, minlength=cfg.ntypes)
+        self.fit = _FittingTC(params, tcount, dev)
+        const_t = np.array([float(params.fit[t]["out"][1][0]) + float(params.bias_atom_e[t])
+                            for t in range(cfg.ntypes)])
+        per_frame = np.array([np.bincount(t, minlength=cfg.ntypes) @ const_t for t in types])
+        self.e_const = torch.tensor(per_frame, dtype=f64, device=dev)
+        self.tab = []
+        s = torch.cuda.current_stream(dev).cuda_stream
+        for t, _ in params.tables:
+            ref_layout = torch.tensor(t, dtype=f32, device=dev)
+            packed = torch.empty_like(ref_layout)
+            call("dpb_se_a_pack_table_f32", ptr(packed), ptr(ref_layout), t.shape[0], M, s)
+            self.tab.append(packed)
+        torch.cuda.synchronize(dev)
+        self.tab_ptrs = (ctypes.c_void_p * len(self.tab))(*[t.data_ptr() for t in self.tab])
+        self.tab_info = np.ascontiguousarray(
+            np.concatenate([i for _, i in params.tables]).astype(np.float32))
+        self.graph = None
+        self.set_coords([fr[0] for fr in frames])
+
+    def set_coords(self, coords):
+        """Host coordinates of every frame (a list, or one [N, 3] array)."""
+        c = np.concatenate([np.asarray(x, np.float64).reshape(-1, 3) for x in coords]) \
+            if isinstance(coords, (list, tuple)) else np.asarray(coords, np.float64)
+        self.coord.copy_(torch.as_tensor(c.reshape(self.N, 3)))
+
+    # ---- one step over all frames, no host synchronisation
+    def step(self):
+        cfg, s = self.cfg, torch.cuda.current_stream().cuda_stream
+        M, ax, F, N = cfg.neuron[-1], cfg.axis_neuron, self.nframes, self.N
+        call("dpb_batch_env_mat_a_f32", ptr(self.em), ptr(self.nlist), ptr(self.cw),
+             ptr(self.cell_of), ptr(self.cell_start), ptr(self.cell_atoms), ptr(self.coord),
+             ptr(self.type), ptr(self.avg), ptr(self.std), ptr(self.atom_off),
+             ptr(self.cell_off), ptr(self.box), ptr(self.ncell), ptr(self.row_frame), F, N,
+             ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth), cfg.sec.ctypes.data,
+             cfg.sec.size, ptr(self.status), s)
+        call("dpb_se_a_descriptor_fwd_f32", ptr(self.xyz), ptr(self.D), ptr(self.drow),
+             ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data, cfg.sec.ctypes.data,
+             cfg.sec.size, N, M, ax, s)
+        self.fit.layers(self.D, self.dD)
+        call("dpb_se_a_descriptor_bwd_f32", ptr(self.net_deriv), ptr(self.dD), ptr(self.drow),
+             ptr(self.xyz), ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data,
+             cfg.sec.ctypes.data, cfg.sec.size, N, M, ax, s)
+        call("dpb_batch_force_virial_a", ptr(self.force), ptr(self.virial),
+             ptr(self.net_deriv), ptr(self.cw), ptr(self.type), ptr(self.std),
+             ptr(self.nlist), ptr(self.atom_off), ptr(self.cell_off), ptr(self.box),
+             ptr(self.ncell), ptr(self.row_frame), F, N, cfg.nnei, cfg.ntypes,
+             ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth), s)
+        call("dpb_batch_energy", ptr(self.energy), ptr(self.fit.e), ptr(self.drow),
+             ptr(self.e_const), ptr(self.atom_off), F, s)
+
+    def capture(self, warmup: int = 2):
+        s = torch.cuda.Stream(device=self.dev)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(warmup):
+                self.step()
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.step()
+        torch.cuda.synchronize()
+        return self
+
+    def replay(self):
+        if self.graph is None:
+            self.step()
+        else:
+            self.graph.replay()
+
+    def check(self):
+        """Raise if a step overflowed a capacity (reads the status words)."""
+        s = torch.cuda.current_stream().cuda_stream
+        call("dpb_status_check", ptr(self.status), s)
+        call("dpb_status_check", ptr(self.fit.status), s)
+
+    def compute(self, coords=None):
+        """(energy [F], force [N, 3], virial [F, 9]) as host arrays."""
+        if coords is not None:
+            self.set_coords(coords)
+        self.replay()
+        torch.cuda.synchronize()
+        return (self.energy.cpu().numpy(), self.force.cpu().numpy(),
+                self.virial.cpu().numpy())
+
+    def frame_slice(self, f: int) -> slice:
+        return slice(int(self.atom_off_h[f]), int(self.atom_off_h[f + 1]))

@@ -1,0 +1,418 @@
+// Many frames of uneven size in one pass per stage (batched workload): the
+// geometry of every frame is handled by the same launch instead of one launch
+// sequence per frame.
+//
+//  k_bt_cells  : one CTA per frame: positions wrapped into the frame's
+//                orthorhombic box, atoms binned into cells of edge >= rcut
+//                (counting sort in shared memory).
+//  k_bt_env    : one warp per center atom of any frame: the 27 lattice cells
+//                around the center, each mapped to (cell, periodic image), so
+//                ghosts are never materialised; the candidate tests, keys
+//                (type, float r^2, index) and slot filling of the single-frame
+//                env pass (format_nlist_i_cpu order, fmt_nlist.cc:98-143), the
+//                index being (local atom * 27 + image code); env rows in FP32
+//                from FP64 differences (env_mat.cc:146-205).
+//  k_bt_force  : one warp per center: the env derivative recomputed from the
+//                packed (atom, image) index, pair forces added to the owners
+//                directly (no ghost fold), the virial reduced per warp into
+//                its frame's 9 components (prod_force.cc:23-72,
+//                prod_virial.cc:22-69).
+//  k_bt_energy : one CTA per frame: the atomic energies of its rows plus the
+//                per-type constants, summed in FP64.
+// Requirements checked on the host: orthorhombic boxes whose edges are all
+// at least rcut (every neighbor then lies in the 27 lattice cells), at most
+// 4096 cells and 600,000 atoms per frame.
+#include "dpb_common.cuh"
+#include "dpb_envmath.cuh"
+
+namespace dpb {
+
+constexpr int BT_MAXCELLS = 4096;
+constexpr int BT_CAP = 256;     // in-range candidates per center
+constexpr int BT_MAXT = 8;      // neighbor types
+constexpr int BT_NMAX = 512;    // sum(sel)
+constexpr int BT_WARPS = 4;
+
+struct BtFrames {
+  const int* atom_off;   // [F + 1]
+  const int* cell_off;   // [F + 1] (each frame: ncell + 1 entries)
+  const double* box;     // [F, 3] orthorhombic edge lengths
+  const int* ncell;      // [F, 3] cells per edge (>= 1)
+  const int* row_frame;  // [N]
+  int nframes;
+};
+
+struct BtSec {
+  int ntypes, nnei;
+  int sec[BT_MAXT + 1];
+};
+
+__device__ __forceinline__ int bt_wrap_cell(double x, double L, int n) {
+  int c = (int)(x / L * n);
+  return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
+__global__ void __launch_bounds__(256)
+k_bt_cells(double* __restrict__ cw, int* __restrict__ cell_of, int* __restrict__ cell_start,
+           int* __restrict__ cell_atoms, const double* __restrict__ coord, BtFrames fr) {
+  __shared__ int cnt[BT_MAXCELLS + 1];
+  const int f = blockIdx.x;
+  const int a0 = fr.atom_off[f], na = fr.atom_off[f + 1] - a0;
+  const int nx = fr.ncell[3 * f], ny = fr.ncell[3 * f + 1], nz = fr.ncell[3 * f + 2];
+  const int nc = nx * ny * nz;
+  const double L[3] = {fr.box[3 * f], fr.box[3 * f + 1], fr.box[3 * f + 2]};
+  for (int c = threadIdx.x; c <= nc; c += blockDim.x) cnt[c] = 0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < na; k += blockDim.x) {
+    double w[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double x = coord[3 * (size_t)(a0 + k) + d];
+      w[d] = x - floor(x / L[d]) * L[d];
+      if (w[d] >= L[d]) w[d] -= L[d];  // rounding at the upper edge
+      if (w[d] < 0.0) w[d] += L[d];    // and at the lower one
+      cw[3 * (size_t)(a0 + k) + d] = w[d];
+    }
+    const int c = (bt_wrap_cell(w[0], L[0], nx) * ny + bt_wrap_cell(w[1], L[1], ny)) * nz +
+                  bt_wrap_cell(w[2], L[2], nz);
+    cell_of[a0 + k] = c;
+    atomicAdd(&cnt[c + 1], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)  // exclusive offsets over at most 4096 cells
+    for (int c = 0; c < nc; ++c) cnt[c + 1] += cnt[c];
+  __syncthreads();
+  int* cs = cell_start + fr.cell_off[f];
+  for (int c = threadIdx.x; c <= nc; c += blockDim.x) cs[c] = cnt[c];
+  __syncthreads();
+  for (int k = threadIdx.x; k < na; k += blockDim.x) {
+    const int pos = atomicAdd(&cnt[cell_of[a0 + k]], 1);
+    cell_atoms[a0 + pos] = k;
+  }
+}
+
+__device__ __forceinline__ unsigned bt_lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// image code (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1) of shifts in {-1, 0, 1}
+__device__ __forceinline__ void bt_unpack(int packed, int& j, double s[3]) {
+  j = packed / 27;
+  const int code = packed - j * 27;
+  s[0] = (double)(code / 9 - 1);
+  s[1] = (double)((code / 3) % 3 - 1);
+  s[2] = (double)(code % 3 - 1);
+}
+
+struct BtEnvSmem {
+  unsigned long long keys[BT_CAP];
+  int row[BT_NMAX];
+  int tcnt[32];
+};
+
+__global__ void __launch_bounds__(BT_WARPS * 32)
+k_bt_env(float* __restrict__ em, int* __restrict__ nlist, const double* __restrict__ cw,
+         const int* __restrict__ type, const int* __restrict__ cell_of,
+         const int* __restrict__ cell_start, const int* __restrict__ cell_atoms,
+         const float* __restrict__ avg, const float* __restrict__ std_, BtFrames fr, BtSec sec,
+         int nrows, float rcut, float rcut_smth, int* status) {
+  __shared__ BtEnvSmem smem[BT_WARPS];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * BT_WARPS + w;
+  if (row >= nrows) return;
+  BtEnvSmem& sm = smem[w];
+  const int f = fr.row_frame[row];
+  const int a0 = fr.atom_off[f];
+  const int i = row - a0;
+  const int nx = fr.ncell[3 * f], ny = fr.ncell[3 * f + 1], nz = fr.ncell[3 * f + 2];
+  const double L[3] = {fr.box[3 * f], fr.box[3 * f + 1], fr.box[3 * f + 2]};
+  const double* fc = cw + 3 * (size_t)a0;
+  const int* ft = type + a0;
+  const int* cs = cell_start + fr.cell_off[f];
+  const int* ca = cell_atoms + a0;
+  const int nnei = sec.nnei, ntypes = sec.ntypes;
+  int ti = ft[i];
+  if (ti < 0 || ti >= ntypes) {
+    if (lane == 0) atomicOr(status, ST_TYPE_RANGE);
+    ti = -1;
+  }
+  const double xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
+  const float fxi[3] = {(float)xi[0], (float)xi[1], (float)xi[2]};
+  const float rc2f = rcut * rcut;
+  const double rc2 = (double)rc2f;
+  for (int t = lane; t < 32; t += 32) sm.tcnt[t] = 0;
+  for (int jj = lane; jj < nnei; jj += 32) sm.row[jj] = -1;
+  __syncwarp();
+  int count = 0;
+  const int ci = cell_of[row];
+  const int cz = ci % nz, cy = (ci / nz) % ny, cx = ci / (nz * ny);
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dz = -1; dz <= 1; ++dz) {
+        // lattice cell (cx+dx, cy+dy, cz+dz) = stored cell (wrapped) + image
+        int X = cx + dx, Y = cy + dy, Z = cz + dz;
+        const int sx = X < 0 ? -1 : (X >= nx ? 1 : 0);
+        const int sy = Y < 0 ? -1 : (Y >= ny ? 1 : 0);
+        const int sz = Z < 0 ? -1 : (Z >= nz ? 1 : 0);
+        X -= sx * nx;
+        Y -= sy * ny;
+        Z -= sz * nz;
+        const int code = (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1);
+        const double sh[3] = {sx * L[0], sy * L[1], sz * L[2]};
+        const int c = (X * ny + Y) * nz + Z;
+        const int b = cs[c], e = cs[c + 1];
+        for (int base = b; base < e; base += 32) {
+          const int k = base + lane;
+          bool ok = false;
+          unsigned long long key = 0;
+          if (k < e) {
+            const int j = ca[k];
+            const int tj = ft[j];
+            if (tj >= 0 && tj < ntypes && ti >= 0 && !(j == i && code == 13)) {
+              // the image's position, then the single-frame path's two tests
+              const double g0 = fc[3 * j] + sh[0], g1 = fc[3 * j + 1] + sh[1],
+                           g2 = fc[3 * j + 2] + sh[2];
+              const double d0 = sub_rn(xi[0], g0), d1 = sub_rn(xi[1], g1),
+                           d2 = sub_rn(xi[2], g2);
+              if (dot3_rn(d0, d1, d2) < rc2) {
+                const float e0 = sub_rn((float)g0, fxi[0]), e1 = sub_rn((float)g1, fxi[1]),
+                            e2 = sub_rn((float)g2, fxi[2]);
+                const float r2 = dot3_rn(e0, e1, e2);
+                if (r2 <= rc2f) {
+                  ok = true;
+                  key = ((unsigned long long)tj << 56) |
+                        ((unsigned long long)__float_as_uint(r2) << 24) |
+                        (unsigned long long)(j * 27 + code);
+                }
+              }
+            }
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, ok);
+          if (ok) {
+            const int pos = count + __popc(bal & bt_lanemask_lt());
+            if (pos < BT_CAP) {
+              sm.keys[pos] = key;
+              atomicAdd(&sm.tcnt[key >> 56], 1);
+            }
+          }
+          count += __popc(bal);
+        }
+      }
+  __syncwarp();
+  if (count > BT_CAP && lane == 0) atomicOr(status, ST_NLIST_CAPACITY);
+  const int n = count < BT_CAP ? count : BT_CAP;
+  int tstart = lane < ntypes ? sm.tcnt[lane] : 0;
+  {
+    int x = tstart;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    tstart = x - tstart;
+  }
+  for (int q = 0; q * 32 < n; ++q) {
+    const int kk = q * 32 + lane;
+    const unsigned long long own = kk < n ? sm.keys[kk] : ~0ull;
+    int r = 0;
+    for (int p = 0; p < n; ++p) r += sm.keys[p] < own ? 1 : 0;
+    const int t = (int)(own >> 56) & 31;
+    const int ts = __shfl_sync(0xffffffffu, tstart, t);
+    if (kk < n) {
+      const int rr = r - ts;
+      if (rr < sec.sec[t + 1] - sec.sec[t]) sm.row[sec.sec[t] + rr] = (int)(own & 0xFFFFFFull);
+      else atomicOr(status, ST_SEL_OVERFLOW);
+    }
+  }
+  __syncwarp();
+  const float* av = avg + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  const float* sd = std_ + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  for (int jj = lane; jj < nnei; jj += 32) {
+    const int packed = sm.row[jj];
+    nlist[(size_t)row * nnei + jj] = packed;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (packed >= 0) {
+      int j;
+      double s[3];
+      bt_unpack(packed, j, s);
+      float r[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) r[d] = (float)((fc[3 * j + d] + s[d] * L[d]) - xi[d]);
+      env_row<float>(r, rcut_smth, rcut, v, nullptr);
+    }
+    float* e = em + ((size_t)row * nnei + jj) * 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) e[k] = ti >= 0 ? (v[k] - av[jj * 4 + k]) / sd[jj * 4 + k] : 0.f;
+  }
+}
+
+__global__ void __launch_bounds__(BT_WARPS * 32)
+k_bt_force(double* __restrict__ force, double* __restrict__ virial,
+           const float* __restrict__ nd, const double* __restrict__ cw,
+           const int* __restrict__ type, const float* __restrict__ std_,
+           const int* __restrict__ nlist, BtFrames fr, int ntypes, int nnei, int nrows,
+           float rcut, float rcut_smth) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * BT_WARPS + w;
+  if (row >= nrows) return;
+  const int f = fr.row_frame[row];
+  const int a0 = fr.atom_off[f];
+  const int i = row - a0;
+  const int ti = type[row];
+  if (ti < 0 || ti >= ntypes) return;  // env derivative rows are zero
+  const double L[3] = {fr.box[3 * f], fr.box[3 * f + 1], fr.box[3 * f + 2]};
+  const double* fc = cw + 3 * (size_t)a0;
+  const double xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
+  const float* sd = std_ + (size_t)ti * nnei * 4;
+  const float* ndr = nd + (size_t)row * nnei * 4;
+  double c0 = 0., c1 = 0., c2 = 0.;
+  double vs[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) vs[k] = 0.;
+  for (int jj = lane; jj < nnei; jj += 32) {
+    const int packed = nlist[(size_t)row * nnei + jj];
+    if (packed < 0) continue;
+    int j;
+    double s[3];
+    bt_unpack(packed, j, s);
+    float r[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[d] = (float)((fc[3 * j + d] + s[d] * L[d]) - xi[d]);
+    float v[4], gd[12];
+    env_row<float>(r, rcut_smth, rcut, v, gd);
+    float p[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const float n = ndr[jj * 4 + a];
+      const float sa = sd[jj * 4 + a];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) p[d] += n * (gd[a * 3 + d] / sa);
+    }
+    const double q[3] = {(double)p[0], (double)p[1], (double)p[2]};
+    c0 += q[0];
+    c1 += q[1];
+    c2 += q[2];
+    atomicAdd(&force[3 * (size_t)(a0 + j) + 0], q[0]);
+    atomicAdd(&force[3 * (size_t)(a0 + j) + 1], q[1]);
+    atomicAdd(&force[3 * (size_t)(a0 + j) + 2], q[2]);
+#pragma unroll
+    for (int d0 = 0; d0 < 3; ++d0)
+#pragma unroll
+      for (int d1 = 0; d1 < 3; ++d1) vs[d0 * 3 + d1] += q[d0] * (double)r[d1];
+  }
+  c0 = warp_sum(c0);
+  c1 = warp_sum(c1);
+  c2 = warp_sum(c2);
+  if (lane == 0) {
+    atomicAdd(&force[3 * (size_t)row + 0], -c0);
+    atomicAdd(&force[3 * (size_t)row + 1], -c1);
+    atomicAdd(&force[3 * (size_t)row + 2], -c2);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const double t = warp_sum(vs[k]);
+    if (lane == 0) atomicAdd(&virial[9 * (size_t)f + k], t);
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_bt_energy(double* __restrict__ energy, const float* __restrict__ e_rows,
+            const int* __restrict__ drow, const double* __restrict__ e_const, BtFrames fr) {
+  __shared__ double part[8];
+  const int f = blockIdx.x;
+  double s = 0.;
+  for (int r = fr.atom_off[f] + threadIdx.x; r < fr.atom_off[f + 1]; r += blockDim.x)
+    s += (double)e_rows[drow[r]];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = e_const[f];
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
+    energy[f] = t;
+  }
+}
+
+static int bt_frames(BtFrames& fr, const int* atom_off, const int* cell_off, const double* box,
+                     const int* ncell, const int* row_frame, int nframes) {
+  if (nframes <= 0 || !atom_off || !cell_off || !box || !ncell || !row_frame) {
+    set_error("batched frames: invalid frame table (nframes=%d)", nframes);
+    return DPB_ERR_INVALID;
+  }
+  fr = BtFrames{atom_off, cell_off, box, ncell, row_frame, nframes};
+  return DPB_OK;
+}
+
+}  // namespace dpb
+
+using namespace dpb;
+extern "C" {
+
+int dpb_batch_env_mat_a_f32(float* em, int* nlist, double* cw, int* cell_of, int* cell_start,
+                            int* cell_atoms, const double* coord, const int* type,
+                            const float* avg, const float* std_, const int* atom_off,
+                            const int* cell_off, const double* box, const int* ncell,
+                            const int* row_frame, int nframes, int nrows, float rcut,
+                            float rcut_smth, const int* sec, int nsec, int* status,
+                            dpb_stream_t stream) {
+  BtFrames fr;
+  int rc = bt_frames(fr, atom_off, cell_off, box, ncell, row_frame, nframes);
+  if (rc) return rc;
+  if (sec == nullptr || nsec < 2 || nsec - 1 > BT_MAXT || sec[0] != 0 ||
+      sec[nsec - 1] > BT_NMAX || status == nullptr) {
+    set_error("batch_env_mat_a: need 1..%d types, sum(sel) <= %d and a status word", BT_MAXT,
+              BT_NMAX);
+    return DPB_ERR_INVALID;
+  }
+  BtSec s{};
+  s.ntypes = nsec - 1;
+  s.nnei = sec[nsec - 1];
+  for (int k = 0; k < nsec; ++k) s.sec[k] = sec[k];
+  if (nrows <= 0) return DPB_OK;
+  cudaStream_t st = as_stream(stream);
+  k_bt_cells<<<nframes, 256, 0, st>>>(cw, cell_of, cell_start, cell_atoms, coord, fr);
+  DPB_CHECK_LAUNCH("batch_env_mat_a/cells");
+  k_bt_env<<<ceil_div(nrows, BT_WARPS), BT_WARPS * 32, 0, st>>>(
+      em, nlist, cw, type, cell_of, cell_start, cell_atoms, avg, std_, fr, s, nrows, rcut,
+      rcut_smth, status);
+  DPB_CHECK_LAUNCH("batch_env_mat_a/env");
+  return DPB_OK;
+}
+
+int dpb_batch_force_virial_a(double* force, double* virial, const float* net_deriv,
+                             const double* cw, const int* type, const float* std_,
+                             const int* nlist, const int* atom_off, const int* cell_off,
+                             const double* box, const int* ncell, const int* row_frame,
+                             int nframes, int nrows, int nnei, int ntypes, float rcut,
+                             float rcut_smth, dpb_stream_t stream) {
+  BtFrames fr;
+  int rc = bt_frames(fr, atom_off, cell_off, box, ncell, row_frame, nframes);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  DPB_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * 3 * (size_t)nrows, st), "batch_force");
+  DPB_CUDA(cudaMemsetAsync(virial, 0, sizeof(double) * 9 * (size_t)nframes, st),
+           "batch_force");
+  if (nrows <= 0 || nnei <= 0) return DPB_OK;
+  k_bt_force<<<ceil_div(nrows, BT_WARPS), BT_WARPS * 32, 0, st>>>(
+      force, virial, net_deriv, cw, type, std_, nlist, fr, ntypes, nnei, nrows, rcut,
+      rcut_smth);
+  DPB_CHECK_LAUNCH("batch_force_virial_a");
+  return DPB_OK;
+}
+
+int dpb_batch_energy(double* energy, const float* e_rows, const int* drow,
+                     const double* e_const, const int* atom_off, int nframes,
+                     dpb_stream_t stream) {
+  if (nframes <= 0 || !energy || !e_rows || !drow || !e_const || !atom_off) {
+    set_error("batch_energy: invalid arguments");
+    return DPB_ERR_INVALID;
+  }
+  BtFrames fr{atom_off, nullptr, nullptr, nullptr, nullptr, nframes};
+  k_bt_energy<<<nframes, 256, 0, as_stream(stream)>>>(energy, e_rows, drow, e_const, fr);
+  DPB_CHECK_LAUNCH("batch_energy");
+  return DPB_OK;
+}
+
+}  // extern "C"

@@ -137,6 +137,68 @@ def env_stats(params: SeAParams, coord: np.ndarray, atype: np.ndarray, box: np.n
     return davg.reshape(cfg.ntypes, -1), dstd.reshape(cfg.ntypes, -1), min_dist
 
 
+def env_stats_frames(params: SeAParams, frames, device="cuda:0", protection: float = 1e-2):
+    """env_stats over several frames: the per-center-type moments of the raw
+    environment matrix summed over all frames (a type absent from every frame
+    keeps davg 0, dstd 1)."""
+    cfg = params.cfg
+    dev = torch.device(device)
+    nt = cfg.ntypes
+    s_r, s_r2, n_r = np.zeros(nt), np.zeros(nt), np.zeros(nt)
+    s_a, s_a2, n_a = np.zeros(nt), np.zeros(nt), np.zeros(nt)
+    min_dist = cfg.rcut
+    zeros = torch.zeros((nt, cfg.nnei * 4), dtype=torch.float64, device=dev)
+    ones = torch.ones_like(zeros)
+    for coord, atype, box in frames:
+        ce, te, _ = ops.copy_coord(torch.tensor(coord, device=dev),
+                                   torch.tensor(atype, device=dev), cfg.rcut, box)
+        nloc = atype.size
+        em, _, rij, nlist = ops.env_mat_a_cells(ce, te, nloc, zeros, ones, cfg.rcut,
+                                                cfg.rcut_smth, cfg.sec)
+        em = em.view(nloc, cfg.nnei, 4).cpu().numpy()
+        for t in range(nt):
+            sel = em[atype == t]
+            if sel.size == 0:
+                continue
+            r, a = sel[:, :, 0], sel[:, :, 1:]
+            s_r[t] += r.sum()
+            s_r2[t] += (r * r).sum()
+            n_r[t] += r.size
+            s_a[t] += a.sum()
+            s_a2[t] += (a * a).sum()
+            n_a[t] += a.size
+        rr = rij.view(nloc, cfg.nnei, 3).cpu().numpy()
+        valid = nlist.cpu().numpy() >= 0
+        d = np.linalg.norm(rr, axis=-1)[valid]
+        if d.size:
+            min_dist = min(min_dist, float(d.min()))
+
+    def std(s1, s2, n):
+        v = np.sqrt(max(s2 / n - (s1 / n) ** 2, 0.0))
+        return protection if abs(v) < protection else v
+
+    davg = np.zeros((nt, cfg.nnei, 4))
+    dstd = np.ones((nt, cfg.nnei, 4))
+    for t in range(nt):
+        if n_r[t] == 0:
+            continue
+        davg[t, :, 0] = s_r[t] / n_r[t]
+        dstd[t, :, 0] = std(s_r[t], s_r2[t], n_r[t])
+        dstd[t, :, 1:] = std(s_a[t], s_a2[t], n_a[t])
+    return davg.reshape(nt, -1), dstd.reshape(nt, -1), min_dist
+
+
+def prepare_frames(params: SeAParams, frames, device="cuda:0"):
+    """prepare() for a set of frames (statistics over all of them)."""
+    davg, dstd, min_dist = env_stats_frames(params, frames, device)
+    params.davg, params.dstd = davg, dstd
+    dev_tables = table_mod.build_tables_device(params.emb, davg, dstd, params.cfg.sel, min_dist,
+                                               params.cfg.rcut_smth, params.cfg.rcut,
+                                               device=device)
+    params.tables = [(t.cpu().numpy(), info) for t, info in dev_tables]
+    return params
+
+
 def prepare(params: SeAParams, coord, atype, box, device="cuda:0", with_tables=True):
     """Statistics from the frame and (optionally) the FP64 compression tables
     (built on the device, dpb_se_a_build_table_f64)."""
@@ -282,6 +344,12 @@ class _FittingTC:
 
     def forward_backward(self, D: torch.Tensor, dD: torch.Tensor, energy: torch.Tensor):
         """energy[0] = sum of atomic energies (FP64); dD = dE/dD (FP32)."""
+        self.layers(D, dD)
+        energy.copy_((self.e.to(torch.float64).sum() + self.e_const).view(1))
+
+    def layers(self, D: torch.Tensor, dD: torch.Tensor):
+        """The six GEMMs: self.e[r] = atomic energy of fitting row r without
+        its constant (output bias + atomic energy bias); dD = dE/dD."""
         s = torch.cuda.current_stream().cuda_stream
         w, din = self.width, self.din
         self.e.zero_()
@@ -295,7 +363,6 @@ class _FittingTC:
         self._gemm(self.G2, w, self.B2b, w, self.EPI_BWD_RES, self.G1, aux0=self.H1,
                    aux1=self.g2, s=s)
         self._gemm(self.G1, w, self.B1b, din, self.EPI_STORE, dD, s=s)
-        energy.copy_((self.e.to(torch.float64).sum() + self.e_const).view(1))
 
 
 # ------------------------------------------------------------ evaluators --

@@ -52,3 +52,56 @@ def water_frame(n_side: int = 4, seed: int = 0):
     atype = np.tile(np.array([0, 1, 1], np.int32), nm)
     box = np.diag([L, L, L]).reshape(9)
     return coord, atype, box
+
+
+# ------------------------------------------------ batched uneven frames ---
+WATER_VOLUME_PER_MOLECULE = 18.015 / 0.60221408  # A^3 per molecule at 1.0 g/cm^3
+CU_A = 3.615                                      # FCC lattice constant (A)
+FCC_BASIS = np.array([[0.0, 0.0, 0.0], [0.0, 0.5, 0.5], [0.5, 0.0, 0.5], [0.5, 0.5, 0.0]])
+
+
+def water_frame_density(n_atoms: int, rng: np.random.Generator):
+    """Water of about n_atoms atoms (round(n/3) molecules) in a cubic box at
+    1.0 g/cm^3: O on the sites of an n_side^3 grid over the box (a random
+    subset when the molecule count is not a cube), +-0.3 A jitter, H placed as
+    in water_frame. Types O=0, H=1."""
+    nm = max(1, int(round(n_atoms / 3)))
+    L = (nm * WATER_VOLUME_PER_MOLECULE) ** (1.0 / 3.0)
+    n_side = int(np.ceil(nm ** (1.0 / 3.0) - 1e-9))
+    g = (np.arange(n_side) + 0.5) * (L / n_side)
+    sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    o = sites[np.sort(rng.choice(sites.shape[0], nm, replace=False))]
+    o = o + rng.uniform(-0.3, 0.3, size=o.shape)
+    half = HOH / 2
+    h_local = np.array([[OH * np.sin(half), OH * np.cos(half), 0.0],
+                        [-OH * np.sin(half), OH * np.cos(half), 0.0]])
+    R = random_rotations(rng, nm)
+    h = np.einsum("mij,kj->mki", R, h_local) + o[:, None, :]
+    coord = np.mod(np.concatenate([o[:, None, :], h], axis=1).reshape(-1, 3), L)
+    atype = np.tile(np.array([0, 1, 1], np.int32), nm)
+    return coord, atype, np.diag([L, L, L]).reshape(9)
+
+
+def cu_frame(n_atoms: int, rng: np.random.Generator, sigma: float = 0.05):
+    """FCC copper (a = 3.615 A) of exactly n_atoms atoms: the smallest cubic
+    supercell of k^3 unit cells (k >= 2, so every box edge exceeds the 6 A
+    cutoff) that holds them, Gaussian jitter sigma, then random atoms deleted
+    down to n_atoms (vacancies; the periodic box is kept). Type Cu=2."""
+    k = max(2, int(np.ceil((n_atoms / 4.0) ** (1.0 / 3.0) - 1e-9)))
+    g = np.arange(k)
+    cells = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 1, 3)
+    pos = ((cells + FCC_BASIS[None]) * CU_A).reshape(-1, 3)
+    pos = pos + rng.normal(0.0, sigma, size=pos.shape)
+    keep = np.sort(rng.choice(pos.shape[0], n_atoms, replace=False))
+    L = k * CU_A
+    return np.mod(pos[keep], L), np.full(n_atoms, 2, np.int32), np.diag([L, L, L]).reshape(9)
+
+
+def batched_frames(n_frames: int = 512, seed: int = 0, n_min: int = 24, n_max: int = 3000):
+    """Frames of log-uniform atom counts in [n_min, n_max]: even frames water
+    at 1.0 g/cm^3, odd frames FCC Cu with vacancies. Returns a list of
+    (coord [n, 3], atype [n], box [9])."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(n_min), np.log(n_max), size=n_frames)).astype(int)
+    return [water_frame_density(int(n), rng) if f % 2 == 0 else cu_frame(int(n), rng)
+            for f, n in enumerate(counts)]

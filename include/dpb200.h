@@ -311,6 +311,43 @@ DPB_API int dpb_cell_grid_build_async_f64(void* grid, long long grid_bytes,
                                           const int* nall_dev, float rcut,
                                           dpb_stream_t stream);
 
+/* Batched frames (no counterpart in the reference, which evaluates frames of
+ * different sizes one call at a time): many frames of uneven atom counts in
+ * one launch per stage. Rows (atoms) of all frames are concatenated; the
+ * frame table is on the device: atom_off [F + 1], cell_off [F + 1] (frame f
+ * owns ncell_f + 1 cell_start entries from cell_off[f]), box [F, 3]
+ * (orthorhombic edges, each >= rcut), ncell [F, 3] (cells per edge, each >= 1
+ * with box / ncell >= rcut; at most 4096 cells and 600,000 atoms per frame),
+ * row_frame [N]. Neighbors are periodic images found through the frame's own
+ * cell list; nlist holds (frame-local atom * 27 + image code) per slot, with
+ * the image code (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1) for shifts in
+ * {-1, 0, 1} box edges. Scratch: cw [N, 3] FP64 (wrapped positions),
+ * cell_of [N], cell_atoms [N], cell_start [cell_off[F]]. em is FP32 from FP64
+ * differences (as dpb_env_mat_a_cells_mixed); sec: host, status: device. */
+DPB_API int dpb_batch_env_mat_a_f32(float* em, int* nlist, double* cw, int* cell_of,
+                                    int* cell_start, int* cell_atoms, const double* coord,
+                                    const int* type, const float* avg, const float* std_,
+                                    const int* atom_off, const int* cell_off,
+                                    const double* box, const int* ncell, const int* row_frame,
+                                    int nframes, int nrows, float rcut, float rcut_smth,
+                                    const int* sec, int nsec, int* status,
+                                    dpb_stream_t stream);
+/* Force [N, 3] and per-frame virial [F, 9] (FP64) of the batched frames from
+ * net_deriv [N, nnei * 4] (FP32), the wrapped positions cw and the packed
+ * nlist of dpb_batch_env_mat_a_f32; the env derivative is recomputed. */
+DPB_API int dpb_batch_force_virial_a(double* force, double* virial, const float* net_deriv,
+                                     const double* cw, const int* type, const float* std_,
+                                     const int* nlist, const int* atom_off,
+                                     const int* cell_off, const double* box,
+                                     const int* ncell, const int* row_frame, int nframes,
+                                     int nrows, int nnei, int ntypes, float rcut,
+                                     float rcut_smth, dpb_stream_t stream);
+/* Per-frame energy [F] (FP64): e_const[f] + sum over the frame's rows r of
+ * e_rows[drow[r]] (the atomic energies of the fitting, in fitting-row order). */
+DPB_API int dpb_batch_energy(double* energy, const float* e_rows, const int* drow,
+                             const double* e_const, const int* atom_off, int nframes,
+                             dpb_stream_t stream);
+
 /* FP64 compression table of one se_a embedding net, built on the device
  * (the reference builds it on the host: deepmd/utils/tabulate.py:275-371).
  * xx: device [npoints] grid, steps: device [nspline] interval widths
