@@ -245,6 +245,79 @@ def run_repeated(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------- batched frames (c2) --
+def run_batched(args) -> None:
+    """Uneven frames (log-uniform 24..3000 atoms, half water at 1.0 g/cm^3, half
+    FCC Cu with vacancies; 3-species model) in one graph per step over all
+    frames; FP64 plain-path checks on a few frames. One GPU."""
+    import torch
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    mdl, wl, tab = _load()
+    bt = importlib.import_module("deepmd_kit_lr_pt_b200.batch")
+    frames = wl.batched_frames(args.frames, seed=0)
+    cfg = mdl.SeAConfig(sel=(46, 92, 60))
+    params = mdl.init_params(cfg, seed=PARAM_SEED)
+    # statistics from a subset of the frames (every 16th)
+    mdl.prepare_frames(params, frames[::16], device=device)
+    ev = bt.BatchEvaluator(params, frames, device=device)
+    ev.compute()
+    ev.check()
+    ev.capture()
+    N = ev.N
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    clocks = ClockSampler(0)
+    clocks.start()
+    t_end, nw = time.time() + 0.6, 0
+    while nw < args.warmup or time.time() < t_end:
+        ev.replay()
+        nw += 1
+        if nw % 16 == 0:
+            torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        ev.replay()
+        b.record()
+        ts.append((a, b))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in ts]))
+    ev.check()
+    E, F, V = ev.compute()
+    checks = []
+    half = len(frames) // 2 - (len(frames) // 2) % 2
+    for f in sorted({0, min(1, len(frames) - 1), half, min(half + 1, len(frames) - 1)}):
+        coord, atype, box = frames[f]
+        plain = mdl.SeAEvaluator(params, atype, box, mode="plain", device=device)
+        e0, f0, v0 = plain.compute(coord)
+        n = atype.size
+        checks.append({"frame": f, "atoms": int(n), "species": "water" if f % 2 == 0 else "Cu",
+                       "energy_err_ev_per_atom": abs(E[f] - e0) / n,
+                       "force_rmse_ev_per_a": float(np.sqrt(np.mean(
+                           (F[ev.frame_slice(f)] - f0) ** 2))),
+                       "virial_max_abs_err": float(np.abs(V[f] - v0).max())})
+        del plain
+    line = {"metric": "us/step/atom, se_e2_a batched uneven frames (compressed, mixed "
+                      "precision)",
+            "value": ms * 1e3 / N, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(frames)} frames, {N} atoms (log-uniform 24..3000 "
+                                   "atoms per frame; even frames water at 1.0 g/cm^3, odd "
+                                   "frames FCC Cu a=3.615 A with vacancies)",
+                       "sel": list(cfg.sel), "embedding": list(cfg.neuron),
+                       "fitting": list(cfg.fitting), "graph": "one CUDA graph per step",
+                       "l2": "256 MiB buffer written between timed steps"},
+            "clocks": clk, "checks_vs_fp64_plain": checks}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- arms -------
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
@@ -507,8 +580,10 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the FP64 plain path (smaller device footprint for profiling)")
-    ap.add_argument("--workload", choices=["step", "repeated"], default="step",
-                    help="repeated: many evaluations of one large frame with a skin list")
+    ap.add_argument("--workload", choices=["step", "repeated", "batched"], default="step",
+                    help="repeated: many evaluations of one large frame with a skin list; "
+                         "batched: many uneven water / Cu frames per step")
+    ap.add_argument("--frames", type=int, default=512, help="batched workload: frame count")
     ap.add_argument("--n-side", type=int, default=48,
                     help="repeated workload: oxygen grid per box side (48: 331,776 atoms)")
     ap.add_argument("--skin", type=float, default=2.0)
@@ -526,6 +601,10 @@ def main() -> None:
     if args.workload == "repeated":
         if rank == 0:
             run_repeated(args)
+        return
+    if args.workload == "batched":
+        if rank == 0:
+            run_batched(args)
         return
     if world > 1:
         import datetime
