@@ -52,10 +52,10 @@ _ERRORS = {
     6: DPBOverflowError,
 }
 
-P, I, F, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_longlong
-_SPEC = {"p": P, "i": I, "f": F, "L": LL}
+P, I, F, LL, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_longlong, ctypes.c_double
+_SPEC = {"p": P, "i": I, "f": F, "L": LL, "d": D}
 
-# name -> argument kinds (p pointer, i int, f float, L long long)
+# name -> argument kinds (p pointer, i int, f float, L long long, d double)
 _FUNCS = {
     "dpb_status_check": "pp",
     "dpb_normalize_coord_f64": "pipp",
@@ -97,6 +97,9 @@ _FUNCS = {
     "dpb_batch_env_mat_a_f32": "pppppppppp" "ppppp" "iiff" "pipp",
     "dpb_batch_force_virial_a": "ppppppp" "ppppp" "iiiiff" "p",
     "dpb_batch_energy": "pppppip",
+    "dpb_batch_env_mat_a_f64": "pppppppppp" "ppppp" "iiff" "pipp",
+    "dpb_batch_force_virial_a_f64": "ppppppp" "ppppp" "iiiiff" "p",
+    "dpb_batch_energy_f64": "pppppip",
     "dpb_se_a_descriptor_fwd_f32": "pppp" "pp" "pi" "iiip",
     "dpb_se_a_descriptor_bwd_f32": "ppppp" "pp" "pi" "iiip",
     "dpb_force_virial_a_f32": "pppppp" "pp" "iiiip",
@@ -106,6 +109,24 @@ _FUNCS = {
     "dpb_gemm_tf32x3_f32": "pii" "pp" "i" "pi" "i" "pppp" "ppp" "pp" "p",
     "dpb_force_virial_a_env_f64": "pppppppp" "iiii" "ff" "p",
 }
+_TRAIN = {
+    "dpb_se_a_train_fwd": "pppppppppp" "iii" "pp",
+    "dpb_se_a_train_bwd": "ppppppppppp" "iii" "p",
+    "dpb_se_a_train_tan": "pppppppppppppp" "i" "pppp" "iii" "ff" "p",
+    "dpb_se_a_train_rev": "ppppppppppppppppp" "i" "pppp" "iii" "p" "ff" "p",
+    "dpb_fit_act": "pppp" "iii" "p",
+    "dpb_fit_tan": "ppppp" "iii" "p",
+    "dpb_fit_bwd": "pppp" "ii" "p",
+    "dpb_fit_rev": "ppppppppp" "ii" "p",
+    "dpb_fit_res_adj": "pp" "iii" "p",
+    "dpb_fit_out": "pppp" "d" "ii" "p",
+    "dpb_fit_out_adj": "pppppppp" "ii" "p",
+    "dpb_train_lam": "pppp" "i" "p",
+    "dpb_adam": "pppp" "L" "p" "ddd" "p",
+}
+for _name, _spec in _TRAIN.items():
+    for _suf in ("f32", "f64"):
+        _FUNCS[f"{_name}_{_suf}"] = _spec
 _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),
     "dpb_cell_grid_bytes": ("i", LL),

@@ -21,19 +21,20 @@ from .model import SeAParams, _FittingTC
 CELL_MARGIN = 1.0001  # cell edge >= rcut * margin, as the single-frame grid
 
 
-class BatchEvaluator:
-    """Energy [F], force [N, 3] and virial [F, 9] of F frames whose atoms are
-    concatenated in frame order (compressed FP32 path, FP64 sums)."""
+class FrameTable:
+    """Device frame table of F frames whose atoms are concatenated in frame
+    order: atom_off [F + 1], cell_off [F + 1], box [F, 3], ncell [F, 3],
+    row_frame [N], type [N], drow [N] (the atom's row when rows are grouped
+    by type, stable) and the geometry scratch (cw, cell_of, cell_atoms,
+    cell_start). Frames need orthorhombic boxes with every edge >= rcut."""
 
-    def __init__(self, params: SeAParams, frames, device="cuda:0"):
-        cfg = params.cfg
-        self.cfg, self.params = cfg, params
+    def __init__(self, cfg, frames, device):
         self.dev = dev = torch.device(device)
         self.nframes = F = len(frames)
         if F == 0:
             raise _capi.DPBInvalidArgument("no frames")
         counts, boxes, ncell, types = [], [], [], []
-        for f, (coord, atype, box) in enumerate(frames):
+        for f, (_, atype, box) in enumerate(frames):
             b = np.asarray(box, np.float64).reshape(3, 3)
             if np.any(b - np.diag(np.diag(b))):
                 raise _capi.DPBInvalidArgument(f"frame {f}: the batched path needs an "
@@ -46,6 +47,9 @@ class BatchEvaluator:
             if int(np.prod(nc)) > 4096 or atype.size > 600000:
                 raise _capi.DPBInvalidArgument(f"frame {f}: more than 4096 cells or 600,000 "
                                                "atoms")
+            if atype.size and (atype.min() < 0 or atype.max() >= cfg.ntypes):
+                raise _capi.DPBInvalidArgument(f"frame {f}: atom types outside "
+                                               f"[0, {cfg.ntypes})")
             counts.append(int(atype.size))
             boxes.append(L)
             ncell.append(nc)
@@ -56,22 +60,52 @@ class BatchEvaluator:
         cells = np.array([int(np.prod(c)) + 1 for c in ncell])
         cell_off = np.concatenate([[0], np.cumsum(cells)]).astype(np.int32)
         row_frame = np.repeat(np.arange(F, dtype=np.int32), self.counts)
-        atype_all = np.concatenate(types)
+        self.atype = atype_all = np.concatenate(types)
+        self.types = types
         i32 = lambda a: torch.tensor(np.ascontiguousarray(a, np.int32), device=dev)  # noqa: E731
         self.atom_off_h = atom_off
         self.atom_off, self.cell_off = i32(atom_off), i32(cell_off)
         self.box = torch.tensor(np.array(boxes), dtype=torch.float64, device=dev)
         self.ncell = i32(np.array(ncell))
+        self.row_frame_h = row_frame
         self.row_frame = i32(row_frame)
         self.type = i32(atype_all)
+        self.cw = torch.zeros((N, 3), dtype=torch.float64, device=dev)
+        self.cell_of = torch.zeros(N, dtype=torch.int32, device=dev)
+        self.cell_atoms = torch.zeros(N, dtype=torch.int32, device=dev)
+        self.cell_start = torch.zeros(int(cell_off[-1]), dtype=torch.int32, device=dev)
+        order = np.argsort(atype_all, kind="stable")
+        drow = np.empty(N, np.int32)
+        drow[order] = np.arange(N, dtype=np.int32)
+        self.drow_h = drow
+        self.drow = i32(drow)
+        self.tcount = np.bincount(atype_all, minlength=cfg.ntypes)
+
+    def frame_slice(self, f: int) -> slice:
+        return slice(int(self.atom_off_h[f]), int(self.atom_off_h[f + 1]))
+
+
+class BatchEvaluator:
+    """Energy [F], force [N, 3] and virial [F, 9] of F frames whose atoms are
+    concatenated in frame order (compressed FP32 path, FP64 sums)."""
+
+    def __init__(self, params: SeAParams, frames, device="cuda:0"):
+        cfg = params.cfg
+        self.cfg, self.params = cfg, params
+        self.dev = dev = torch.device(device)
+        self.ft = ft = FrameTable(cfg, frames, dev)
+        self.nframes = F = ft.nframes
+        self.counts, self.N, N = ft.counts, ft.N, ft.N
+        self.atom_off_h = ft.atom_off_h
+        self.atom_off, self.cell_off, self.box, self.ncell = (ft.atom_off, ft.cell_off, ft.box,
+                                                              ft.ncell)
+        self.row_frame, self.type, self.drow = ft.row_frame, ft.type, ft.drow
+        self.cw, self.cell_of, self.cell_atoms, self.cell_start = (ft.cw, ft.cell_of,
+                                                                   ft.cell_atoms, ft.cell_start)
         nnei, M, ax = cfg.nnei, cfg.neuron[-1], cfg.axis_neuron
         f64, f32 = torch.float64, torch.float32
         z = lambda shape, dt: torch.zeros(shape, dtype=dt, device=dev)  # noqa: E731
         self.coord = z((N, 3), f64)
-        self.cw = z((N, 3), f64)
-        self.cell_of = z(N, torch.int32)
-        self.cell_atoms = z(N, torch.int32)
-        self.cell_start = z(int(cell_off[-1]), torch.int32)
         self.em = z((N, nnei * 4), f32)
         self.nlist = z((N, nnei), torch.int32)
         self.xyz = z((N, 4, M), f32)
@@ -84,16 +118,10 @@ class BatchEvaluator:
         self.status = z(1, torch.int32)
         self.avg = torch.tensor(params.davg, dtype=f32, device=dev)
         self.std = torch.tensor(params.dstd, dtype=f32, device=dev)
-        # fitting rows grouped by type over all frames
-        order = np.argsort(atype_all, kind="stable")
-        drow = np.empty(N, np.int32)
-        drow[order] = np.arange(N, dtype=np.int32)
-        self.drow = i32(drow)
-        tcount = np.bincount(atype_all, minlength=cfg.ntypes)
-        self.fit = _FittingTC(params, tcount, dev)
+        self.fit = _FittingTC(params, ft.tcount, dev)
         const_t = np.array([float(params.fit[t]["out"][1][0]) + float(params.bias_atom_e[t])
                             for t in range(cfg.ntypes)])
-        per_frame = np.array([np.bincount(t, minlength=cfg.ntypes) @ const_t for t in types])
+        per_frame = np.array([np.bincount(t, minlength=cfg.ntypes) @ const_t for t in ft.types])
         self.e_const = torch.tensor(per_frame, dtype=f64, device=dev)
         self.tab = []
         s = torch.cuda.current_stream(dev).cuda_stream

@@ -22,35 +22,10 @@
 // Requirements checked on the host: orthorhombic boxes whose edges are all
 // at least rcut (every neighbor then lies in the 27 lattice cells), at most
 // 4096 cells and 600,000 atoms per frame.
-#include "dpb_common.cuh"
+#include "dpb_batch.cuh"
 #include "dpb_envmath.cuh"
 
 namespace dpb {
-
-constexpr int BT_MAXCELLS = 4096;
-constexpr int BT_CAP = 256;     // in-range candidates per center
-constexpr int BT_MAXT = 8;      // neighbor types
-constexpr int BT_NMAX = 512;    // sum(sel)
-constexpr int BT_WARPS = 4;
-
-struct BtFrames {
-  const int* atom_off;   // [F + 1]
-  const int* cell_off;   // [F + 1] (each frame: ncell + 1 entries)
-  const double* box;     // [F, 3] orthorhombic edge lengths
-  const int* ncell;      // [F, 3] cells per edge (>= 1)
-  const int* row_frame;  // [N]
-  int nframes;
-};
-
-struct BtSec {
-  int ntypes, nnei;
-  int sec[BT_MAXT + 1];
-};
-
-__device__ __forceinline__ int bt_wrap_cell(double x, double L, int n) {
-  int c = (int)(x / L * n);
-  return c < 0 ? 0 : (c >= n ? n - 1 : c);
-}
 
 __global__ void __launch_bounds__(256)
 k_bt_cells(double* __restrict__ cw, int* __restrict__ cell_of, int* __restrict__ cell_start,
@@ -91,32 +66,18 @@ k_bt_cells(double* __restrict__ cw, int* __restrict__ cell_of, int* __restrict__
   }
 }
 
-__device__ __forceinline__ unsigned bt_lanemask_lt() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-// image code (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1) of shifts in {-1, 0, 1}
-__device__ __forceinline__ void bt_unpack(int packed, int& j, double s[3]) {
-  j = packed / 27;
-  const int code = packed - j * 27;
-  s[0] = (double)(code / 9 - 1);
-  s[1] = (double)((code / 3) % 3 - 1);
-  s[2] = (double)(code % 3 - 1);
-}
-
 struct BtEnvSmem {
   unsigned long long keys[BT_CAP];
   int row[BT_NMAX];
   int tcnt[32];
 };
 
+template <typename ET>
 __global__ void __launch_bounds__(BT_WARPS * 32)
-k_bt_env(float* __restrict__ em, int* __restrict__ nlist, const double* __restrict__ cw,
+k_bt_env(ET* __restrict__ em, int* __restrict__ nlist, const double* __restrict__ cw,
          const int* __restrict__ type, const int* __restrict__ cell_of,
          const int* __restrict__ cell_start, const int* __restrict__ cell_atoms,
-         const float* __restrict__ avg, const float* __restrict__ std_, BtFrames fr, BtSec sec,
+         const ET* __restrict__ avg, const ET* __restrict__ std_, BtFrames fr, BtSec sec,
          int nrows, float rcut, float rcut_smth, int* status) {
   __shared__ BtEnvSmem smem[BT_WARPS];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -227,31 +188,29 @@ k_bt_env(float* __restrict__ em, int* __restrict__ nlist, const double* __restri
     }
   }
   __syncwarp();
-  const float* av = avg + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
-  const float* sd = std_ + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  const ET* av = avg + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
+  const ET* sd = std_ + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
   for (int jj = lane; jj < nnei; jj += 32) {
     const int packed = sm.row[jj];
     nlist[(size_t)row * nnei + jj] = packed;
-    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    ET v[4] = {(ET)0, (ET)0, (ET)0, (ET)0};
     if (packed >= 0) {
-      int j;
-      double s[3];
-      bt_unpack(packed, j, s);
-      float r[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) r[d] = (float)((fc[3 * j + d] + s[d] * L[d]) - xi[d]);
-      env_row<float>(r, rcut_smth, rcut, v, nullptr);
+      ET r[3];
+      bt_rij<ET>(r, fc, packed, xi, L);
+      env_row<ET>(r, rcut_smth, rcut, v, nullptr);
     }
-    float* e = em + ((size_t)row * nnei + jj) * 4;
+    ET* e = em + ((size_t)row * nnei + jj) * 4;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) e[k] = ti >= 0 ? (v[k] - av[jj * 4 + k]) / sd[jj * 4 + k] : 0.f;
+    for (int k = 0; k < 4; ++k)
+      e[k] = ti >= 0 ? (v[k] - av[jj * 4 + k]) / sd[jj * 4 + k] : (ET)0;
   }
 }
 
+template <typename ET>
 __global__ void __launch_bounds__(BT_WARPS * 32)
 k_bt_force(double* __restrict__ force, double* __restrict__ virial,
-           const float* __restrict__ nd, const double* __restrict__ cw,
-           const int* __restrict__ type, const float* __restrict__ std_,
+           const ET* __restrict__ nd, const double* __restrict__ cw,
+           const int* __restrict__ type, const ET* __restrict__ std_,
            const int* __restrict__ nlist, BtFrames fr, int ntypes, int nnei, int nrows,
            float rcut, float rcut_smth) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -265,8 +224,8 @@ k_bt_force(double* __restrict__ force, double* __restrict__ virial,
   const double L[3] = {fr.box[3 * f], fr.box[3 * f + 1], fr.box[3 * f + 2]};
   const double* fc = cw + 3 * (size_t)a0;
   const double xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
-  const float* sd = std_ + (size_t)ti * nnei * 4;
-  const float* ndr = nd + (size_t)row * nnei * 4;
+  const ET* sd = std_ + (size_t)ti * nnei * 4;
+  const ET* ndr = nd + (size_t)row * nnei * 4;
   double c0 = 0., c1 = 0., c2 = 0.;
   double vs[9];
 #pragma unroll
@@ -274,19 +233,16 @@ k_bt_force(double* __restrict__ force, double* __restrict__ virial,
   for (int jj = lane; jj < nnei; jj += 32) {
     const int packed = nlist[(size_t)row * nnei + jj];
     if (packed < 0) continue;
-    int j;
-    double s[3];
-    bt_unpack(packed, j, s);
-    float r[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) r[d] = (float)((fc[3 * j + d] + s[d] * L[d]) - xi[d]);
-    float v[4], gd[12];
-    env_row<float>(r, rcut_smth, rcut, v, gd);
-    float p[3] = {0.f, 0.f, 0.f};
+    const int j = packed / 27;
+    ET r[3];
+    bt_rij<ET>(r, fc, packed, xi, L);
+    ET v[4], gd[12];
+    env_row<ET>(r, rcut_smth, rcut, v, gd);
+    ET p[3] = {(ET)0, (ET)0, (ET)0};
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-      const float n = ndr[jj * 4 + a];
-      const float sa = sd[jj * 4 + a];
+      const ET n = ndr[jj * 4 + a];
+      const ET sa = sd[jj * 4 + a];
 #pragma unroll
       for (int d = 0; d < 3; ++d) p[d] += n * (gd[a * 3 + d] / sa);
     }
@@ -317,8 +273,9 @@ k_bt_force(double* __restrict__ force, double* __restrict__ virial,
   }
 }
 
+template <typename ET>
 __global__ void __launch_bounds__(256)
-k_bt_energy(double* __restrict__ energy, const float* __restrict__ e_rows,
+k_bt_energy(double* __restrict__ energy, const ET* __restrict__ e_rows,
             const int* __restrict__ drow, const double* __restrict__ e_const, BtFrames fr) {
   __shared__ double part[8];
   const int f = blockIdx.x;
@@ -335,28 +292,16 @@ k_bt_energy(double* __restrict__ energy, const float* __restrict__ e_rows,
   }
 }
 
-static int bt_frames(BtFrames& fr, const int* atom_off, const int* cell_off, const double* box,
-                     const int* ncell, const int* row_frame, int nframes) {
-  if (nframes <= 0 || !atom_off || !cell_off || !box || !ncell || !row_frame) {
-    set_error("batched frames: invalid frame table (nframes=%d)", nframes);
-    return DPB_ERR_INVALID;
-  }
-  fr = BtFrames{atom_off, cell_off, box, ncell, row_frame, nframes};
-  return DPB_OK;
-}
-
 }  // namespace dpb
 
-using namespace dpb;
-extern "C" {
+namespace dpb {
 
-int dpb_batch_env_mat_a_f32(float* em, int* nlist, double* cw, int* cell_of, int* cell_start,
-                            int* cell_atoms, const double* coord, const int* type,
-                            const float* avg, const float* std_, const int* atom_off,
-                            const int* cell_off, const double* box, const int* ncell,
-                            const int* row_frame, int nframes, int nrows, float rcut,
-                            float rcut_smth, const int* sec, int nsec, int* status,
-                            dpb_stream_t stream) {
+template <typename ET>
+static int batch_env(ET* em, int* nlist, double* cw, int* cell_of, int* cell_start,
+                     int* cell_atoms, const double* coord, const int* type, const ET* avg,
+                     const ET* std_, const int* atom_off, const int* cell_off, const double* box,
+                     const int* ncell, const int* row_frame, int nframes, int nrows, float rcut,
+                     float rcut_smth, const int* sec, int nsec, int* status, dpb_stream_t stream) {
   BtFrames fr;
   int rc = bt_frames(fr, atom_off, cell_off, box, ncell, row_frame, nframes);
   if (rc) return rc;
@@ -374,19 +319,19 @@ int dpb_batch_env_mat_a_f32(float* em, int* nlist, double* cw, int* cell_of, int
   cudaStream_t st = as_stream(stream);
   k_bt_cells<<<nframes, 256, 0, st>>>(cw, cell_of, cell_start, cell_atoms, coord, fr);
   DPB_CHECK_LAUNCH("batch_env_mat_a/cells");
-  k_bt_env<<<ceil_div(nrows, BT_WARPS), BT_WARPS * 32, 0, st>>>(
+  k_bt_env<ET><<<ceil_div(nrows, BT_WARPS), BT_WARPS * 32, 0, st>>>(
       em, nlist, cw, type, cell_of, cell_start, cell_atoms, avg, std_, fr, s, nrows, rcut,
       rcut_smth, status);
   DPB_CHECK_LAUNCH("batch_env_mat_a/env");
   return DPB_OK;
 }
 
-int dpb_batch_force_virial_a(double* force, double* virial, const float* net_deriv,
-                             const double* cw, const int* type, const float* std_,
-                             const int* nlist, const int* atom_off, const int* cell_off,
-                             const double* box, const int* ncell, const int* row_frame,
-                             int nframes, int nrows, int nnei, int ntypes, float rcut,
-                             float rcut_smth, dpb_stream_t stream) {
+template <typename ET>
+static int batch_force(double* force, double* virial, const ET* net_deriv, const double* cw,
+                       const int* type, const ET* std_, const int* nlist, const int* atom_off,
+                       const int* cell_off, const double* box, const int* ncell,
+                       const int* row_frame, int nframes, int nrows, int nnei, int ntypes,
+                       float rcut, float rcut_smth, dpb_stream_t stream) {
   BtFrames fr;
   int rc = bt_frames(fr, atom_off, cell_off, box, ncell, row_frame, nframes);
   if (rc) return rc;
@@ -395,24 +340,79 @@ int dpb_batch_force_virial_a(double* force, double* virial, const float* net_der
   DPB_CUDA(cudaMemsetAsync(virial, 0, sizeof(double) * 9 * (size_t)nframes, st),
            "batch_force");
   if (nrows <= 0 || nnei <= 0) return DPB_OK;
-  k_bt_force<<<ceil_div(nrows, BT_WARPS), BT_WARPS * 32, 0, st>>>(
+  k_bt_force<ET><<<ceil_div(nrows, BT_WARPS), BT_WARPS * 32, 0, st>>>(
       force, virial, net_deriv, cw, type, std_, nlist, fr, ntypes, nnei, nrows, rcut,
       rcut_smth);
   DPB_CHECK_LAUNCH("batch_force_virial_a");
   return DPB_OK;
 }
 
-int dpb_batch_energy(double* energy, const float* e_rows, const int* drow,
-                     const double* e_const, const int* atom_off, int nframes,
-                     dpb_stream_t stream) {
+template <typename ET>
+static int batch_energy(double* energy, const ET* e_rows, const int* drow, const double* e_const,
+                        const int* atom_off, int nframes, dpb_stream_t stream) {
   if (nframes <= 0 || !energy || !e_rows || !drow || !e_const || !atom_off) {
     set_error("batch_energy: invalid arguments");
     return DPB_ERR_INVALID;
   }
   BtFrames fr{atom_off, nullptr, nullptr, nullptr, nullptr, nframes};
-  k_bt_energy<<<nframes, 256, 0, as_stream(stream)>>>(energy, e_rows, drow, e_const, fr);
+  k_bt_energy<ET><<<nframes, 256, 0, as_stream(stream)>>>(energy, e_rows, drow, e_const, fr);
   DPB_CHECK_LAUNCH("batch_energy");
   return DPB_OK;
+}
+
+}  // namespace dpb
+
+using namespace dpb;
+extern "C" {
+
+#define DPB_BATCH_ENTRIES(SUF, ET)                                                              \
+  int dpb_batch_env_mat_a_##SUF(ET* em, int* nlist, double* cw, int* cell_of, int* cell_start,  \
+                                int* cell_atoms, const double* coord, const int* type,         \
+                                const ET* avg, const ET* std_, const int* atom_off,            \
+                                const int* cell_off, const double* box, const int* ncell,      \
+                                const int* row_frame, int nframes, int nrows, float rcut,      \
+                                float rcut_smth, const int* sec, int nsec, int* status,        \
+                                dpb_stream_t stream) {                                         \
+    return batch_env<ET>(em, nlist, cw, cell_of, cell_start, cell_atoms, coord, type, avg,     \
+                         std_, atom_off, cell_off, box, ncell, row_frame, nframes, nrows, rcut, \
+                         rcut_smth, sec, nsec, status, stream);                                \
+  }
+
+DPB_BATCH_ENTRIES(f32, float)
+DPB_BATCH_ENTRIES(f64, double)
+
+int dpb_batch_force_virial_a(double* force, double* virial, const float* net_deriv,
+                             const double* cw, const int* type, const float* std_,
+                             const int* nlist, const int* atom_off, const int* cell_off,
+                             const double* box, const int* ncell, const int* row_frame,
+                             int nframes, int nrows, int nnei, int ntypes, float rcut,
+                             float rcut_smth, dpb_stream_t stream) {
+  return batch_force<float>(force, virial, net_deriv, cw, type, std_, nlist, atom_off, cell_off,
+                            box, ncell, row_frame, nframes, nrows, nnei, ntypes, rcut, rcut_smth,
+                            stream);
+}
+
+int dpb_batch_force_virial_a_f64(double* force, double* virial, const double* net_deriv,
+                                 const double* cw, const int* type, const double* std_,
+                                 const int* nlist, const int* atom_off, const int* cell_off,
+                                 const double* box, const int* ncell, const int* row_frame,
+                                 int nframes, int nrows, int nnei, int ntypes, float rcut,
+                                 float rcut_smth, dpb_stream_t stream) {
+  return batch_force<double>(force, virial, net_deriv, cw, type, std_, nlist, atom_off, cell_off,
+                             box, ncell, row_frame, nframes, nrows, nnei, ntypes, rcut, rcut_smth,
+                             stream);
+}
+
+int dpb_batch_energy(double* energy, const float* e_rows, const int* drow,
+                     const double* e_const, const int* atom_off, int nframes,
+                     dpb_stream_t stream) {
+  return batch_energy<float>(energy, e_rows, drow, e_const, atom_off, nframes, stream);
+}
+
+int dpb_batch_energy_f64(double* energy, const double* e_rows, const int* drow,
+                         const double* e_const, const int* atom_off, int nframes,
+                         dpb_stream_t stream) {
+  return batch_energy<double>(energy, e_rows, drow, e_const, atom_off, nframes, stream);
 }
 
 }  // extern "C"

@@ -332,6 +332,15 @@ DPB_API int dpb_batch_env_mat_a_f32(float* em, int* nlist, double* cw, int* cell
                                     int nframes, int nrows, float rcut, float rcut_smth,
                                     const int* sec, int nsec, int* status,
                                     dpb_stream_t stream);
+/* The same in FP64 throughout (env rows from FP64 differences, FP64 avg/std). */
+DPB_API int dpb_batch_env_mat_a_f64(double* em, int* nlist, double* cw, int* cell_of,
+                                    int* cell_start, int* cell_atoms, const double* coord,
+                                    const int* type, const double* avg, const double* std_,
+                                    const int* atom_off, const int* cell_off,
+                                    const double* box, const int* ncell, const int* row_frame,
+                                    int nframes, int nrows, float rcut, float rcut_smth,
+                                    const int* sec, int nsec, int* status,
+                                    dpb_stream_t stream);
 /* Force [N, 3] and per-frame virial [F, 9] (FP64) of the batched frames from
  * net_deriv [N, nnei * 4] (FP32), the wrapped positions cw and the packed
  * nlist of dpb_batch_env_mat_a_f32; the env derivative is recomputed. */
@@ -342,11 +351,22 @@ DPB_API int dpb_batch_force_virial_a(double* force, double* virial, const float*
                                      const int* ncell, const int* row_frame, int nframes,
                                      int nrows, int nnei, int ntypes, float rcut,
                                      float rcut_smth, dpb_stream_t stream);
+DPB_API int dpb_batch_force_virial_a_f64(double* force, double* virial,
+                                         const double* net_deriv, const double* cw,
+                                         const int* type, const double* std_,
+                                         const int* nlist, const int* atom_off,
+                                         const int* cell_off, const double* box,
+                                         const int* ncell, const int* row_frame, int nframes,
+                                         int nrows, int nnei, int ntypes, float rcut,
+                                         float rcut_smth, dpb_stream_t stream);
 /* Per-frame energy [F] (FP64): e_const[f] + sum over the frame's rows r of
  * e_rows[drow[r]] (the atomic energies of the fitting, in fitting-row order). */
 DPB_API int dpb_batch_energy(double* energy, const float* e_rows, const int* drow,
                              const double* e_const, const int* atom_off, int nframes,
                              dpb_stream_t stream);
+DPB_API int dpb_batch_energy_f64(double* energy, const double* e_rows, const int* drow,
+                                 const double* e_const, const int* atom_off, int nframes,
+                                 dpb_stream_t stream);
 
 /* FP64 compression table of one se_a embedding net, built on the device
  * (the reference builds it on the host: deepmd/utils/tabulate.py:275-371).
@@ -446,6 +466,154 @@ DPB_API int dpb_gemm_tf32x3_f32(const float* A, int M, int K,
                                 const float* aux1, const float* const* bias,
                                 const float* const* idt, const float* const* w,
                                 float* e, int* status, dpb_stream_t stream);
+
+/* ------------------------------------------------- training step ----- */
+/* Energy, force and virial of the uncompressed se_e2_a model together with
+ * the gradient of a loss L(E, F, V) w.r.t. every embedding and fitting
+ * weight. The reference gets this gradient from torch autograd with
+ * create_graph=True through its PyTorch model (deepmd/pt/model/model/
+ * transform_output.py:70-101, deepmd/pt/model/descriptor/se_a.py:742-859,
+ * loss deepmd/pt/loss/ener.py:219-340); here it is hand-written: since the
+ * force depends on the weights only through g = dE/d(em), dL/dtheta is the
+ * energy term plus d/dtheta <u, g> with u = dL/dg, a tangent pass of the
+ * network along u followed by one reverse pass over primal and tangent.
+ *
+ * Shared arguments: nlist / type / drow / geometry as dpb_batch_env_mat_a_*
+ * (packed (atom * 27 + image) neighbors, -1 padding; drow [N] = the atom's
+ * row in the type-grouped descriptor); W / b: host arrays [ntypes * 3] of
+ * device pointers to the embedding layers of neighbor type t, layer l at
+ * index t * 3 + l (W row-major [n_in, n_out]); widths: host [1, n1, n2, n3]
+ * with 3 <= n1 <= 32, n2 <= 64, n3 <= 128 (a layer that keeps or doubles its
+ * width adds the residual); axis <= 32; sec: host section offsets; fold:
+ * host [ntypes * ntypes] flags, fold[ti * ntypes + t] = 1 when every padded
+ * slot of section t of a type-ti center has the same avg/std (padded slots
+ * are then evaluated once with their multiplicity), or NULL.
+ *
+ * fwd: xyz [N, 4, n3] (atom order), descrpt [N, n3 * axis] (drow order) from
+ *      em [N, nnei, 4].
+ * bwd: net_deriv = dE/d(em) [N, nnei, 4] (zero on padded slots) from
+ *      d_descrpt = dE/dD (drow order).
+ * tan: tangent of xyz and D along u, u recomputed from the coordinates (cw,
+ *      FP64), avg/std [ntypes, nnei * 4], force_bar = dL/dF [N, 3] and
+ *      virial_bar = dL/dV [F, 9] (FP64): u = (d em / d r_i) . (Fbar_j -
+ *      Fbar_i + Vbar r_ij) per slot.
+ * rev: adds to gW / gb (host arrays of device pointers laid out as W / b)
+ *      the embedding gradient of J = <Dbar_J, D> + <Ddbar, D'> continued
+ *      through xyz, xyz' and the embedding: d_descrpt / d_descrpt_t are the
+ *      adjoints of D and D' from the fitting's reverse pass. */
+/* float */
+DPB_API int dpb_se_a_train_fwd_f32(float* xyz, float* descrpt, const float* em, const int* nlist,
+                                   const int* type, const int* drow, const float* const* W,
+                                   const float* const* b, const int* widths, const int* sec,
+                                   int nsec, int nrows, int axis, const unsigned char* fold,
+                                   dpb_stream_t stream);
+DPB_API int dpb_se_a_train_bwd_f32(float* net_deriv, const float* em, const float* xyz,
+                                   const float* d_descrpt, const int* nlist, const int* type,
+                                   const int* drow, const float* const* W, const float* const* b,
+                                   const int* widths, const int* sec, int nsec, int nrows, int axis,
+                                   dpb_stream_t stream);
+DPB_API int dpb_se_a_train_tan_f32(float* xyz_t, float* descrpt_t, const float* xyz,
+                                   const float* avg, const float* std_, const double* force_bar,
+                                   const double* virial_bar, const double* cw, const int* nlist,
+                                   const int* type, const int* drow, const int* atom_off,
+                                   const double* box, const int* row_frame, int nframes,
+                                   const float* const* W, const float* const* b, const int* widths,
+                                   const int* sec, int nsec, int nrows, int axis, float rcut,
+                                   float rcut_smth, dpb_stream_t stream);
+DPB_API int dpb_se_a_train_rev_f32(float* const* gW, float* const* gb, const float* xyz,
+                                   const float* xyz_t, const float* d_descrpt,
+                                   const float* d_descrpt_t, const float* avg, const float* std_,
+                                   const double* force_bar, const double* virial_bar,
+                                   const double* cw, const int* nlist, const int* type,
+                                   const int* drow, const int* atom_off, const double* box,
+                                   const int* row_frame, int nframes, const float* const* W,
+                                   const float* const* b, const int* widths, const int* sec,
+                                   int nsec, int nrows, int axis, const unsigned char* fold,
+                                   float rcut, float rcut_smth, dpb_stream_t stream);
+/* fitting layer (deepmd/dpmodel/utils/network.py:282-330) around a library GEMM:
+ * act: Y holds Z = H_in W + b on entry; Y = tanh(Z), H = res(H_in) + d * Y (d may be
+ * NULL); tan: Hd = res(Hd_in) + d (1 - Y^2) Zd; bwd: Zb = G d (1 - Y^2); rev: reverse
+ * over tangent, Zbd = d Ad q, Zb = (d A - 2 Y Zd d Ad) q with q = 1 - Y^2, gb +=
+ * column sums of Zb, gd += column sums of A Y + Ad q Zd (gd may be NULL); res_adj:
+ * out += adjoint of the residual; out: e = H . Wo + bo + ebias; out_adj: A = lam Wo,
+ * Ad = Wo, gWo += sum lam H + Hd, gbo += sum lam (lam NULL = 1; Ad, Hd, gWo/gbo may be
+ * NULL); lam: lam[drow[r]] = gE[row_frame[r]]. */
+DPB_API int dpb_fit_act_f32(float* Y, float* H, const float* Hin, const float* d, int n, int w_out,
+                            int w_in, dpb_stream_t stream);
+DPB_API int dpb_fit_tan_f32(float* Hd, const float* Zd, const float* Hdin, const float* Y,
+                            const float* d, int n, int w_out, int w_in, dpb_stream_t stream);
+DPB_API int dpb_fit_bwd_f32(float* Zb, const float* G, const float* Y, const float* d, int n, int w,
+                            dpb_stream_t stream);
+DPB_API int dpb_fit_rev_f32(float* Zb, float* Zbd, float* gb, float* gd, const float* A,
+                            const float* Ad, const float* Y, const float* Zd, const float* d, int n,
+                            int w, dpb_stream_t stream);
+DPB_API int dpb_fit_res_adj_f32(float* out, const float* G, int n, int w_out, int w_in,
+                                dpb_stream_t stream);
+DPB_API int dpb_fit_out_f32(float* e, const float* H, const float* Wo, const float* bo,
+                            double ebias, int n, int w, dpb_stream_t stream);
+DPB_API int dpb_fit_out_adj_f32(float* A, float* Ad, float* gWo, float* gbo, const float* H,
+                                const float* Hd, const float* Wo, const float* lam, int n, int w,
+                                dpb_stream_t stream);
+DPB_API int dpb_train_lam_f32(float* lam, const double* gE, const int* drow, const int* row_frame,
+                              int n, dpb_stream_t stream);
+/* Adam step as torch.optim.Adam (no weight decay, no amsgrad); hp: device
+ * {lr, 1 - beta1^step, sqrt(1 - beta2^step)} (read at run time, so a captured step
+ * follows the schedule). */
+DPB_API int dpb_adam_f32(float* p, const float* g, float* m, float* v, long long n,
+                         const double* hp, double beta1, double beta2, double eps,
+                         dpb_stream_t stream);
+
+/* double */
+DPB_API int dpb_se_a_train_fwd_f64(double* xyz, double* descrpt, const double* em, const int* nlist,
+                                   const int* type, const int* drow, const double* const* W,
+                                   const double* const* b, const int* widths, const int* sec,
+                                   int nsec, int nrows, int axis, const unsigned char* fold,
+                                   dpb_stream_t stream);
+DPB_API int dpb_se_a_train_bwd_f64(double* net_deriv, const double* em, const double* xyz,
+                                   const double* d_descrpt, const int* nlist, const int* type,
+                                   const int* drow, const double* const* W, const double* const* b,
+                                   const int* widths, const int* sec, int nsec, int nrows, int axis,
+                                   dpb_stream_t stream);
+DPB_API int dpb_se_a_train_tan_f64(double* xyz_t, double* descrpt_t, const double* xyz,
+                                   const double* avg, const double* std_, const double* force_bar,
+                                   const double* virial_bar, const double* cw, const int* nlist,
+                                   const int* type, const int* drow, const int* atom_off,
+                                   const double* box, const int* row_frame, int nframes,
+                                   const double* const* W, const double* const* b,
+                                   const int* widths, const int* sec, int nsec, int nrows, int axis,
+                                   float rcut, float rcut_smth, dpb_stream_t stream);
+DPB_API int dpb_se_a_train_rev_f64(double* const* gW, double* const* gb, const double* xyz,
+                                   const double* xyz_t, const double* d_descrpt,
+                                   const double* d_descrpt_t, const double* avg, const double* std_,
+                                   const double* force_bar, const double* virial_bar,
+                                   const double* cw, const int* nlist, const int* type,
+                                   const int* drow, const int* atom_off, const double* box,
+                                   const int* row_frame, int nframes, const double* const* W,
+                                   const double* const* b, const int* widths, const int* sec,
+                                   int nsec, int nrows, int axis, const unsigned char* fold,
+                                   float rcut, float rcut_smth, dpb_stream_t stream);
+DPB_API int dpb_fit_act_f64(double* Y, double* H, const double* Hin, const double* d, int n,
+                            int w_out, int w_in, dpb_stream_t stream);
+DPB_API int dpb_fit_tan_f64(double* Hd, const double* Zd, const double* Hdin, const double* Y,
+                            const double* d, int n, int w_out, int w_in, dpb_stream_t stream);
+DPB_API int dpb_fit_bwd_f64(double* Zb, const double* G, const double* Y, const double* d, int n,
+                            int w, dpb_stream_t stream);
+DPB_API int dpb_fit_rev_f64(double* Zb, double* Zbd, double* gb, double* gd, const double* A,
+                            const double* Ad, const double* Y, const double* Zd, const double* d,
+                            int n, int w, dpb_stream_t stream);
+DPB_API int dpb_fit_res_adj_f64(double* out, const double* G, int n, int w_out, int w_in,
+                                dpb_stream_t stream);
+DPB_API int dpb_fit_out_f64(double* e, const double* H, const double* Wo, const double* bo,
+                            double ebias, int n, int w, dpb_stream_t stream);
+DPB_API int dpb_fit_out_adj_f64(double* A, double* Ad, double* gWo, double* gbo, const double* H,
+                                const double* Hd, const double* Wo, const double* lam, int n, int w,
+                                dpb_stream_t stream);
+DPB_API int dpb_train_lam_f64(double* lam, const double* gE, const int* drow, const int* row_frame,
+                              int n, dpb_stream_t stream);
+DPB_API int dpb_adam_f64(double* p, const double* g, double* m, double* v, long long n,
+                         const double* hp, double beta1, double beta2, double eps,
+                         dpb_stream_t stream);
+
 
 /* ------------------------------------------- allocation-free variant ---- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc,

@@ -141,3 +141,132 @@ def evaluate(lib, params, coord, atype, box, mode="plain"):
     np.add.at(force, mapping, fext)
     virial, _ = lib.prod_virial_a(nd, emd, rij, nlist, nloc, nall)
     return float(E.detach()), force, virial
+
+
+# ----------------------------------------------------------------- training --
+
+EMB_PREFIX = "atomic_model.descriptor.sea.filter_layers.networks"
+FIT_PREFIX = "atomic_model.fitting_net.filter_layers.networks"
+
+
+def trainable(params):
+    """{reference state_dict name: FP64 leaf tensor} of every trainable weight
+    (embedding matrix/bias, fitting matrix/bias/idt, output layer)."""
+    out = {}
+    for t, net in enumerate(params.emb):
+        for l, (W, b) in enumerate(net):
+            out[f"{EMB_PREFIX}.{t}.layers.{l}.matrix"] = np.asarray(W)
+            out[f"{EMB_PREFIX}.{t}.layers.{l}.bias"] = np.asarray(b)
+    for t, f in enumerate(params.fit):
+        for l, (W, b, d) in enumerate(f["layers"]):
+            out[f"{FIT_PREFIX}.{t}.layers.{l}.matrix"] = np.asarray(W)
+            out[f"{FIT_PREFIX}.{t}.layers.{l}.bias"] = np.asarray(b)
+            if d is not None:
+                out[f"{FIT_PREFIX}.{t}.layers.{l}.idt"] = np.asarray(d)
+        L = len(f["layers"])
+        out[f"{FIT_PREFIX}.{t}.layers.{L}.matrix"] = np.asarray(f["out"][0]).reshape(-1, 1)
+        out[f"{FIT_PREFIX}.{t}.layers.{L}.bias"] = np.asarray(f["out"][1]).reshape(1)
+    return {k: torch.tensor(v, dtype=torch.float64, requires_grad=True) for k, v in out.items()}
+
+
+def _geometry(lib, params, coord, atype, box):
+    cfg = params.cfg
+    nloc = atype.size
+    cn = lib.normalize_coord(np.asarray(coord, np.float64).reshape(-1), box).reshape(-1, 3)
+    c, t, mapping = lib.copy_coord(cn, atype, cfg.rcut, box)
+    nall = c.shape[0]
+    ret, il, nn, rb, _ = lib.build_nlist(c, nloc, cfg.rcut, atype=t, mem_size=nall)
+    assert ret == 0
+    em, emd, rij, nlist = lib.prod_env_mat_a(c, t, il, nn, rb, params.davg, params.dstd, nloc,
+                                             cfg.rcut, cfg.rcut_smth, cfg.sec)
+    return em, emd, rij, nlist, mapping, nall
+
+
+def _energy_force_virial(params, P, geo, atype, create_graph):
+    """FP64 torch E, force [nloc, 3], virial [9] of one frame as functions of
+    the weights P (create_graph keeps the force differentiable)."""
+    cfg = params.cfg
+    em, emd, rij, nlist, mapping, nall = geo
+    nloc, nnei = atype.size, cfg.nnei
+    emt = torch.from_numpy(em.reshape(nloc, nnei, 4).copy()).requires_grad_(True)
+    xyz = torch.zeros((nloc, 4, cfg.neuron[-1]), dtype=torch.float64)
+    sec = cfg.sec
+    for ty in range(cfg.ntypes):
+        a, b = int(sec[ty]), int(sec[ty + 1])
+        if b == a:
+            continue
+        rr = emt[:, a:b, :]
+        h = rr[:, :, :1]
+        for l in range(len(cfg.neuron)):
+            W = P[f"{EMB_PREFIX}.{ty}.layers.{l}.matrix"]
+            y = torch.tanh(h @ W + P[f"{EMB_PREFIX}.{ty}.layers.{l}.bias"])
+            if W.shape[1] == W.shape[0]:
+                y = y + h
+            elif W.shape[1] == 2 * W.shape[0]:
+                y = y + torch.cat([h, h], -1)
+            h = y
+        xyz = xyz + rr.transpose(1, 2) @ h
+    xyz = xyz / nnei
+    D = (xyz.transpose(1, 2) @ xyz[:, :, :cfg.axis_neuron]).reshape(nloc, -1)
+    E = torch.zeros((), dtype=torch.float64)
+    for ty in range(cfg.ntypes):
+        idx = np.nonzero(atype == ty)[0]
+        if idx.size == 0:
+            continue
+        h = D[torch.from_numpy(idx)]
+        L = len(params.fit[ty]["layers"])
+        for l in range(L):
+            key = f"{FIT_PREFIX}.{ty}.layers.{l}"
+            W = P[key + ".matrix"]
+            y = torch.tanh(h @ W + P[key + ".bias"])
+            if key + ".idt" in P:
+                y = y * P[key + ".idt"]
+            h = h + y if W.shape[0] == W.shape[1] else y
+        key = f"{FIT_PREFIX}.{ty}.layers.{L}"
+        e = (h @ P[key + ".matrix"] + P[key + ".bias"]).view(-1) + float(params.bias_atom_e[ty])
+        E = E + e.sum()
+    (g,) = torch.autograd.grad(E, emt, create_graph=create_graph)
+    # prod_force / prod_virial (prod_force.cc:23-72, prod_virial.cc:22-69) in torch
+    ed = torch.from_numpy(emd.reshape(nloc, nnei, 4, 3).copy())
+    q = torch.einsum("ina,inad->ind", g, ed)  # per slot
+    nl = torch.from_numpy(nlist.reshape(nloc, nnei).astype(np.int64))
+    mask = (nl >= 0).to(torch.float64).unsqueeze(-1)
+    q = q * mask
+    fext = torch.zeros((nall, 3), dtype=torch.float64)
+    fext = fext.index_add(0, nl.clamp(min=0).reshape(-1), q.reshape(-1, 3))
+    fext = fext.index_add(0, torch.arange(nloc), -q.sum(1))
+    force = torch.zeros((nloc, 3), dtype=torch.float64).index_add(
+        0, torch.from_numpy(np.asarray(mapping, np.int64)), fext)
+    r = torch.from_numpy(rij.reshape(nloc, nnei, 3).copy())
+    virial = torch.einsum("ind,ine->de", q, r).reshape(9)
+    return E, force, virial
+
+
+def train_loss_grads(lib, params, frames, labels, prefs, P=None):
+    """EnergyStdLoss of a batch of frames and its gradient w.r.t. every
+    trainable weight, by FP64 torch autograd through the force
+    (create_graph), the way the reference trains (transform_output.py:70-101,
+    ener.py:219-340). frames: [(coord, atype, box)]; labels: (E [F], F [N, 3],
+    V [F, 9]); prefs: (p_e, p_f, p_v). Returns (loss, E, F, V, {name: grad})."""
+    P = trainable(params) if P is None else P
+    Es, Fs, Vs, nat = [], [], [], []
+    for coord, atype, box in frames:
+        geo = _geometry(lib, params, coord, atype, box)
+        E, F, V = _energy_force_virial(params, P, geo, atype, create_graph=True)
+        Es.append(E)
+        Fs.append(F)
+        Vs.append(V)
+        nat.append(atype.size)
+    E = torch.stack(Es)
+    F = torch.cat(Fs)
+    V = torch.stack(Vs)
+    Eh, Fh, Vh = (torch.as_tensor(np.asarray(x, np.float64)) for x in labels)
+    inv = 1.0 / torch.tensor(nat, dtype=torch.float64)
+    pe, pf, pv = prefs
+    loss = (pe * torch.mean((E - Eh.reshape(-1)) ** 2 * inv) +
+            pf * torch.sum((Fh.reshape(-1, 3) - F) ** 2) / F.numel() +
+            pv * torch.mean(torch.mean((Vh.reshape(-1, 9) - V) ** 2, -1) * inv))
+    names = list(P)
+    grads = torch.autograd.grad(loss, [P[k] for k in names])
+    return (float(loss.detach()), E.detach().numpy(), F.detach().numpy(), V.detach().numpy(),
+            {k: g.numpy() for k, g in zip(names, grads)})

@@ -53,6 +53,8 @@ def test_ctypes_specs_match_header(dpb):
                 assert arg.startswith("float ") and "*" not in arg, (name, arg)
             elif kind == "L":
                 assert arg.startswith("long long"), (name, arg)
+            elif kind == "d":
+                assert arg.startswith("double ") and "*" not in arg, (name, arg)
 
 
 def test_library_loads_and_reports_version(dpb):
