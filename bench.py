@@ -318,6 +318,176 @@ def run_batched(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_train(args) -> None:
+    """Training step of the uncompressed model: 16 frames of 192-atom water,
+    FP32, EnergyStdLoss (prefactors e 0.02, f 1000, v 0.02) with its gradient
+    through the force (hand-written double backward) and an Adam update, one
+    CUDA graph per step. The FP64 step and the oracle's FP64 torch-autograd
+    step on the host cores are reported beside it. One GPU."""
+    import torch
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    mdl, wl, tab = _load()
+    tr = importlib.import_module("deepmd_kit_lr_pt_b200.train")
+    cfg = mdl.SeAConfig()
+    frames = [wl.water_frame(4, seed=100 + s) for s in range(args.frames)]
+    params = mdl.init_params(cfg, seed=PARAM_SEED)
+    params.davg, params.dstd, _ = mdl.env_stats_frames(params, frames[:1], device)
+    prefs = (0.02, 1000.0, 0.02)
+    lr = 1e-5
+
+    def make(dtype):
+        loss = tr.EnergyStdLoss(starter_learning_rate=lr, start_pref_e=prefs[0],
+                                limit_pref_e=prefs[0], start_pref_f=prefs[1],
+                                limit_pref_f=prefs[1], start_pref_v=prefs[2],
+                                limit_pref_v=prefs[2])
+        return tr.SeATrainer(params, frames, dtype=dtype, device=device, loss=loss)
+
+    t32 = make(torch.float32)
+    E, F, V = t32.compute()
+    rng = np.random.default_rng(3)
+    labels = (E + rng.normal(0, 1.0, E.shape), 0.5 * F, V + rng.normal(0, 1.0, V.shape))
+    t32.set_labels(*labels)
+    t64 = make(torch.float64)
+    t64.set_labels(*labels)
+    N = t32.ft.N
+    # gradient accuracy of the FP32 step against the FP64 one (same weights)
+    g = {}
+    for name, t in (("f32", t32), ("f64", t64)):
+        with torch.no_grad():
+            E_, F_, V_ = t._forward()
+            Eh, Fh, Vh = t.labels
+            t._pref.copy_(torch.tensor(t.loss.prefactors(lr), dtype=torch.float64))
+            _, gE, gF, gV = tr.loss_grads(E_, F_, V_, Eh, Fh, Vh, t._natoms_inv, t._pref)
+            g[name] = t._backward(gE, gF, gV).double().clone()
+    grad_rel = float(torch.linalg.norm(g["f32"] - g["f64"]) / torch.linalg.norm(g["f64"]))
+    # launches of the product's kernels in one step (C-ABI calls; the batched
+    # env call launches two kernels)
+    calls = {"n": 0, "names": []}
+    orig = tr.call
+
+    def counting(name, *a):
+        calls["n"] += 2 if name.startswith("dpb_batch_env_mat_a") else 1
+        calls["names"].append(name)
+        return orig(name, *a)
+
+    tr.call = counting
+    torch.cuda.nvtx.range_push("train_step")  # one eager step, for ncu --nvtx-include
+    with torch.no_grad():
+        t32._set_step_scalars(lr, 0.9, 0.999)
+        t32._step_body(0.9, 0.999, 1e-8)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    tr.call = orig
+    torch.cuda.synchronize()
+    # stage times (eager, events on the launching stream)
+    st = {"forward": [], "backward": [], "step": []}
+    for _ in range(3 + args.warmup):
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        with torch.no_grad():
+            a.record()
+            E_, F_, V_ = t32._forward()
+            Eh, Fh, Vh = t32.labels
+            _, gE, gF, gV = tr.loss_grads(E_, F_, V_, Eh, Fh, Vh, t32._natoms_inv, t32._pref)
+            b.record()
+            t32._backward(gE, gF, gV)
+            c.record()
+        st["forward"].append((a, b))
+        st["backward"].append((b, c))
+    torch.cuda.synchronize()
+    stages = {k: float(np.median([x.elapsed_time(y) for x, y in v[args.warmup:]]))
+              for k, v in st.items() if v}
+
+    def timed(trainer, k, flush):
+        trainer.capture()
+        for _ in range(args.warmup):
+            trainer.train_step(lr)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(k):
+            flush.zero_()
+            trainer._set_step_scalars(lr, 0.9, 0.999)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            trainer.graph.replay()
+            b.record()
+            ts.append((a, b))
+        torch.cuda.synchronize()
+        trainer.check()
+        return float(np.mean([a.elapsed_time(b) for a, b in ts]))
+
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = timed(t32, args.steps, flush)
+    clk = clocks.stop()
+    ms64 = timed(t64, max(3, args.steps // 4), flush)
+    # end to end: host coordinates and labels in, loss out, every step
+    pin = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64)).pin_memory()  # noqa: E731
+    h_coord = pin(np.concatenate([c for c, _, _ in frames]).reshape(-1, 3))
+    h_lab = [pin(x) for x in labels]
+    h_loss = torch.empty(1, dtype=torch.float64).pin_memory()
+    ts = []
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        t32._set_step_scalars(lr, 0.9, 0.999)  # 48 bytes: lr, bias corrections, prefactors
+        t32.coord.copy_(h_coord, non_blocking=True)
+        for dst, src in zip(t32.labels, h_lab):
+            dst.copy_(src.view(dst.shape), non_blocking=True)
+        t32.graph.replay()
+        h_loss.copy_(t32._loss.double(), non_blocking=True)
+        b.record()
+        ts.append((a, b))
+    torch.cuda.synchronize()
+    e2e_ms = float(np.mean([a.elapsed_time(b) for a, b in ts]))
+    h2d = h_coord.numel() * 8 + sum(x.numel() * 8 for x in h_lab) + 48
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import model_ref, oracle
+
+        lib = oracle.ref() or oracle.port()
+        torch.set_num_threads(os.cpu_count() or 1)
+        sample = frames[:2]
+        lab_s = (labels[0][:2], labels[1][:2 * frames[0][1].size], labels[2][:2])
+        model_ref.train_loss_grads(lib, params, sample, lab_s, prefs)  # warm-up
+        t0 = time.perf_counter()
+        reps = 0
+        while reps < 3 or time.perf_counter() - t0 < 10.0:
+            model_ref.train_loss_grads(lib, params, sample, lab_s, prefs)
+            reps += 1
+        el = (time.perf_counter() - t0) / reps
+        na = sum(a.size for _, a, _ in sample)
+        cpu = {"value": el * 1e6 / na, "unit": UNIT, "cores": torch.get_num_threads(),
+               "kind": "port",
+               "sample": f"loss + gradient of 2 frames ({na} atoms) per step, FP64 torch autograd "
+                         f"through the force on the host cores, geometry from "
+                         f"{'the compiled reference library' if oracle.ref() else 'the restatement'}"
+                         f", {reps} repetitions"}
+    line = {"metric": "us/step/atom, se_e2_a training step (energy + force + virial loss, "
+                      "double backward, Adam)",
+            "value": ms * 1e3 / N, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(frames)} frames x 192 atoms water ({N} atoms), "
+                                   "uncompressed se_e2_a [25, 50, 100] / fitting [240, 240, 240]"
+                                   ", EnergyStdLoss prefactors (0.02, 1000, 0.02), Adam",
+                       "graph": "one CUDA graph per step (forward, loss gradient, backward, "
+                                "Adam)",
+                       "l2": "256 MiB buffer written between timed steps"},
+            "e2e": {"value": e2e_ms * 1e3 / N, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 8},
+            "gpu_launches": calls["n"],
+            "fp64_step": {"value": ms64 * 1e3 / N, "ms_per_step": ms64,
+                          "speedup_of_f32": ms64 / ms},
+            "grad_rel_err_f32_vs_f64": grad_rel,
+            "stages_ms": stages, "clocks": clk, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- arms -------
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
@@ -580,10 +750,13 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the FP64 plain path (smaller device footprint for profiling)")
-    ap.add_argument("--workload", choices=["step", "repeated", "batched"], default="step",
+    ap.add_argument("--workload", choices=["step", "repeated", "batched", "train"],
+                    default="step",
                     help="repeated: many evaluations of one large frame with a skin list; "
-                         "batched: many uneven water / Cu frames per step")
-    ap.add_argument("--frames", type=int, default=512, help="batched workload: frame count")
+                         "batched: many uneven water / Cu frames per step; train: training "
+                         "step with the force/virial loss on 16 water frames")
+    ap.add_argument("--frames", type=int, default=None,
+                    help="frame count (batched: 512, train: 16)")
     ap.add_argument("--n-side", type=int, default=48,
                     help="repeated workload: oxygen grid per box side (48: 331,776 atoms)")
     ap.add_argument("--skin", type=float, default=2.0)
@@ -602,9 +775,15 @@ def main() -> None:
         if rank == 0:
             run_repeated(args)
         return
+    if args.frames is None:
+        args.frames = 16 if args.workload == "train" else 512
     if args.workload == "batched":
         if rank == 0:
             run_batched(args)
+        return
+    if args.workload == "train":
+        if rank == 0:
+            run_train(args)
         return
     if world > 1:
         import datetime
