@@ -111,9 +111,9 @@ _FUNCS = {
 }
 _TRAIN = {
     "dpb_se_a_train_fwd": "pppppppppp" "iii" "pp",
-    "dpb_se_a_train_bwd": "ppppppppppp" "iii" "p",
+    "dpb_se_a_train_bwd": "pppppppppppp" "iii" "p",
     "dpb_se_a_train_tan": "pppppppppppppp" "i" "pppp" "iii" "ff" "p",
-    "dpb_se_a_train_rev": "ppppppppppppppppp" "i" "pppp" "iii" "p" "ff" "p",
+    "dpb_se_a_train_rev": "pppppppppppppppppp" "i" "pppp" "iii" "p" "ff" "p",
     "dpb_fit_act": "pppp" "iii" "p",
     "dpb_fit_tan": "ppppp" "iii" "p",
     "dpb_fit_bwd": "pppp" "ii" "p",

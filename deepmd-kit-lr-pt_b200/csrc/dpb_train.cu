@@ -138,11 +138,12 @@ __device__ void tr_stage_weights(T* sw, const TrNet<T>& net, const TrLayout& lay
 }
 
 // entry list of one center: (slot | multiplicity << 16) per row to evaluate,
-// grouped by neighbor type; secn[t] = first entry of section t
+// grouped by neighbor type over the sections [t0, t1); secn[t] = first entry
+// of section t, secn[t1] = the end
 __device__ __forceinline__ void tr_entries(int* ent, int* secn, const int* nl, const TrGeom& g,
-                                           int ti, bool with_pad, int lane) {
+                                           int ti, bool with_pad, int lane, int t0, int t1) {
   int total = 0;
-  for (int t = 0; t < g.ntypes; ++t) {
+  for (int t = t0; t < t1; ++t) {
     secn[t] = total;
     const int s0 = g.sec[t], s1 = g.sec[t + 1];
     const bool fold = with_pad && ((g.fold >> (ti * 8 + t)) & 1ull);
@@ -165,9 +166,13 @@ __device__ __forceinline__ void tr_entries(int* ent, int* secn, const int* nl, c
       total += 1;
     }
   }
-  if (lane == 0) secn[g.ntypes] = total;
+  if (lane == 0) secn[t1] = total;
   __syncwarp();
 }
+
+// Staged per-row vectors are [channel][row] with the odd row stride R + 1:
+// a lane-owned channel touches its R rows without bank conflicts and the
+// next layer reads one channel of all rows as a broadcast.
 
 template <typename T, int R>
 __device__ __forceinline__ void tr_load_col(T (&a)[R], const T* p) {
@@ -183,9 +188,10 @@ __device__ __forceinline__ void tr_gemv(T (&acc)[CP][R], const T* in, int n_in, 
   for (int j = 0; j < CP; ++j)
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[j][r] = (T)0;
+#pragma unroll 2
   for (int i = 0; i < n_in; ++i) {
     T a[R];
-    tr_load_col<T, R>(a, in + i * R);
+    tr_load_col<T, R>(a, in + i * (R + 1));
 #pragma unroll
     for (int j = 0; j < CP; ++j) {
       const int c = lane + 32 * j;
@@ -207,8 +213,8 @@ __device__ __forceinline__ void tr_gemv2(T (&acc)[CP][R], T (&acd)[CP][R], const
     for (int r = 0; r < R; ++r) acc[j][r] = acd[j][r] = (T)0;
   for (int i = 0; i < n_in; ++i) {
     T a[R], ad[R];
-    tr_load_col<T, R>(a, in + i * R);
-    tr_load_col<T, R>(ad, ind + i * R);
+    tr_load_col<T, R>(a, in + i * (R + 1));
+    tr_load_col<T, R>(ad, ind + i * (R + 1));
 #pragma unroll
     for (int j = 0; j < CP; ++j) {
       const int c = lane + 32 * j;
@@ -231,9 +237,10 @@ __device__ __forceinline__ void tr_gemvT(T (&acc)[CP][R], const T* zb, int n_out
   for (int j = 0; j < CP; ++j)
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[j][r] = (T)0;
+#pragma unroll 2
   for (int c = 0; c < n_out; ++c) {
     T z[R];
-    tr_load_col<T, R>(z, zb + c * R);
+    tr_load_col<T, R>(z, zb + c * (R + 1));
 #pragma unroll
     for (int j = 0; j < CP; ++j) {
       const int i = lane + 32 * j;
@@ -254,8 +261,8 @@ __device__ __forceinline__ void tr_gemvT2(T (&acc)[CP][R], T (&acd)[CP][R], cons
     for (int r = 0; r < R; ++r) acc[j][r] = acd[j][r] = (T)0;
   for (int c = 0; c < n_out; ++c) {
     T z[R], zd[R];
-    tr_load_col<T, R>(z, zb + c * R);
-    tr_load_col<T, R>(zd, zbd + c * R);
+    tr_load_col<T, R>(z, zb + c * (R + 1));
+    tr_load_col<T, R>(zd, zbd + c * (R + 1));
 #pragma unroll
     for (int j = 0; j < CP; ++j) {
       const int i = lane + 32 * j;
@@ -269,20 +276,20 @@ __device__ __forceinline__ void tr_gemvT2(T (&acc)[CP][R], T (&acd)[CP][R], cons
   }
 }
 
-// residual term of output channel c (< n_out) from the staged input [n_in][R]
+// residual term of output channel c (< n_out) from the staged input
 template <typename T, int R>
 __device__ __forceinline__ T tr_res(const T* in, int res, int c, int n_in, int r) {
-  if (res == TR_RES_IDENT) return in[c * R + r];
-  if (res == TR_RES_DUP) return in[(c < n_in ? c : c - n_in) * R + r];
+  if (res == TR_RES_IDENT) return in[c * (R + 1) + r];
+  if (res == TR_RES_DUP) return in[(c < n_in ? c : c - n_in) * (R + 1) + r];
   return (T)0;
 }
 
 // adjoint of the residual for input channel i (< n_in) from the staged
-// output adjoint [n_out][R]
+// output adjoint
 template <typename T, int R>
 __device__ __forceinline__ T tr_res_adj(const T* gb, int res, int i, int n_in, int r) {
-  if (res == TR_RES_IDENT) return gb[i * R + r];
-  if (res == TR_RES_DUP) return gb[i * R + r] + gb[(i + n_in) * R + r];
+  if (res == TR_RES_IDENT) return gb[i * (R + 1) + r];
+  if (res == TR_RES_DUP) return gb[i * (R + 1) + r] + gb[(i + n_in) * (R + 1) + r];
   return (T)0;
 }
 
@@ -367,8 +374,8 @@ __device__ __forceinline__ void tr_env_tangent(T Rv[4], T Rd[4], const TrGeom& g
   }
 }
 
-// xb[a][j] (lane channels c_j) = sum_k Db[c][k] X[a][k] + [c < ax] sum_m Db[m][c] X[a][m]
-// with Db staged as [n3][sax] and X as [4][n3]; accumulates into xb
+// xb[a][j] (lane channels c_j) += sum_k Db[c][k] X[a][k] + [c < ax] sum_m Db[m][c] X[a][m]
+// with Db staged as [n3][sax] and X as [4][n3]
 template <typename T>
 __device__ __forceinline__ void tr_dbar_to_xbar(T (&xb)[4][TR_C3], const T* Db, const T* X,
                                                 int n3, int ax, int sax, int lane) {
@@ -397,16 +404,78 @@ __device__ __forceinline__ void tr_stage_row(T* dst, const T* src, int n3, int a
 }
 
 template <typename T>
-__device__ __forceinline__ T* tr_warp_base(unsigned char* smem_raw, const TrLayout& lay, int w,
-                                           int*& ints) {
-  ints = reinterpret_cast<int*>(smem_raw) + (size_t)w * lay.ints_warp;
-  T* tbase = reinterpret_cast<T*>(smem_raw + (((size_t)lay.nw * lay.ints_warp * 4 + 15) & ~15));
-  return tbase + lay.warp_off + (size_t)w * lay.warp_sz;
+__device__ __forceinline__ T* tr_tbase(unsigned char* smem_raw, const TrLayout& lay) {
+  return reinterpret_cast<T*>(smem_raw + (((size_t)lay.nw * lay.ints_warp * 4 + 15) & ~15));
 }
 
 template <typename T>
-__device__ __forceinline__ T* tr_tbase(unsigned char* smem_raw, const TrLayout& lay) {
-  return reinterpret_cast<T*>(smem_raw + (((size_t)lay.nw * lay.ints_warp * 4 + 15) & ~15));
+__device__ __forceinline__ T* tr_warp_base(unsigned char* smem_raw, const TrLayout& lay, int w,
+                                           int*& ints) {
+  ints = reinterpret_cast<int*>(smem_raw) + (size_t)w * lay.ints_warp;
+  return tr_tbase<T>(smem_raw, lay) + lay.warp_off + (size_t)w * lay.warp_sz;
+}
+
+// lane channels of a per-atom [4][n3] vector from global memory
+template <typename T>
+__device__ __forceinline__ void tr_read_x4(T (&x)[4][TR_C3], const T* src, int n3, int lane) {
+#pragma unroll
+  for (int j = 0; j < TR_C3; ++j) {
+    const int c = lane + 32 * j;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) x[a][j] = c < n3 ? src[a * n3 + c] : (T)0;
+  }
+}
+
+// ------------------------------------------------- per-atom adjoints of xyz --
+// xb = (dJ/dxyz) / nnei and xbd = (dJ/dxyz') / nnei from the descriptor
+// adjoints (D = xyz^T xyz[:, :ax], D' = xyz'^T xyz[:, :ax] + xyz^T xyz'[:, :ax]):
+//   without Dd: xb from Dj only (force backward);
+//   with Dd:    xbd from Dd and xyz; xb from Dj and xyz plus Dd and xyz'.
+// One warp per atom, rows staged with the odd stride sax.
+template <typename T>
+__global__ void __launch_bounds__(64)
+k_tr_xbar(T* __restrict__ xb_out, T* __restrict__ xbd_out, const T* __restrict__ xyz,
+          const T* __restrict__ xyzd, const T* __restrict__ Dj, const T* __restrict__ Dd,
+          const int* __restrict__ drow, int nrows, int n3, int ax, int nnei, int sax) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* base = reinterpret_cast<T*>(smem_raw) + (size_t)w * (8 * n3 + 2 * n3 * sax);
+  T* X = base;
+  T* Xd = base + 4 * n3;
+  T* Sj = base + 8 * n3;
+  T* Sd = Sj + n3 * sax;
+  const T nn = (T)nnei;
+  for (int row = blockIdx.x * 2 + w; row < nrows; row += gridDim.x * 2) {
+    const size_t dr = (size_t)drow[row] * n3 * ax;
+    for (int e = lane; e < 4 * n3; e += 32) {
+      X[e] = xyz[(size_t)row * 4 * n3 + e];
+      if (Dd) Xd[e] = xyzd[(size_t)row * 4 * n3 + e];
+    }
+    tr_stage_row(Sj, Dj + dr, n3, ax, sax, lane);
+    if (Dd) tr_stage_row(Sd, Dd + dr, n3, ax, sax, lane);
+    __syncwarp();
+    T xb[4][TR_C3], xbd[4][TR_C3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int j = 0; j < TR_C3; ++j) xb[a][j] = xbd[a][j] = (T)0;
+    tr_dbar_to_xbar(xb, Sj, X, n3, ax, sax, lane);
+    if (Dd) {
+      tr_dbar_to_xbar(xb, Sd, Xd, n3, ax, sax, lane);
+      tr_dbar_to_xbar(xbd, Sd, X, n3, ax, sax, lane);
+    }
+#pragma unroll
+    for (int j = 0; j < TR_C3; ++j) {
+      const int c = lane + 32 * j;
+      if (c < n3)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          xb_out[((size_t)row * 4 + a) * n3 + c] = xb[a][j] / nn;
+          if (Dd) xbd_out[((size_t)row * 4 + a) * n3 + c] = xbd[a][j] / nn;
+        }
+    }
+    __syncwarp();
+  }
 }
 
 // ---------------------------------------------------------------- forward --
@@ -415,6 +484,7 @@ template <typename T, int R>
 __global__ void __launch_bounds__(256, 1)
 k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ em,
          TrNet<T> net, TrGeom g, TrLayout lay) {
+  constexpr int RS = R + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -431,7 +501,7 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
   for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
     const int ti = g.type[row];
     const int* nl = g.nlist + (size_t)row * g.nnei;
-    tr_entries(ent, secn, nl, g, ti, true, lane);
+    tr_entries(ent, secn, nl, g, ti, true, lane, 0, g.ntypes);
     T xyz[4][TR_C3];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -461,7 +531,7 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
         if (lane < n1) {
           const T w1 = W.W1[lane], b1 = W.b1[lane];
 #pragma unroll
-          for (int r = 0; r < R; ++r) A1[lane * R + r] = tr_tanh(fma(ss[r], w1, b1));
+          for (int r = 0; r < R; ++r) A1[lane * RS + r] = tr_tanh(fma(ss[r], w1, b1));
         }
         __syncwarp();
         {
@@ -474,7 +544,7 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
               const T bb = W.b2[c];
 #pragma unroll
               for (int r = 0; r < R; ++r)
-                A2[c * R + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, net.res2, c, n1, r);
+                A2[c * RS + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, net.res2, c, n1, r);
             }
           }
         }
@@ -535,8 +605,9 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
 
 template <typename T, int R>
 __global__ void __launch_bounds__(256, 1)
-k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xyz,
-         const T* __restrict__ Dbar, TrNet<T> net, TrGeom g, TrLayout lay) {
+k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xbar,
+         TrNet<T> net, TrGeom g, TrLayout lay) {
+  constexpr int RS = R + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -548,34 +619,16 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xy
   int* secn = ints + g.nnei;
   T *rr = ws + lay.o_rr, *ss = ws + lay.o_s;
   T *A1 = ws + lay.o_A1, *A2 = ws + lay.o_A2, *big = ws + lay.o_big;
-  const int n1 = net.n1, n2 = net.n2, n3 = net.n3, ax = g.ax;
+  const int n1 = net.n1, n2 = net.n2, n3 = net.n3;
   const int gw = gridDim.x * lay.nw;
   for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
     const int ti = g.type[row];
     const int* nl = g.nlist + (size_t)row * g.nnei;
-    // xbar = dE/dxyz / nnei from Dbar (lane channels)
-    T xb[4][TR_C3];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int j = 0; j < TR_C3; ++j) xb[a][j] = (T)0;
-    {
-      T* X = big;
-      T* Db = big + 4 * n3;
-      for (int e = lane; e < 4 * n3; e += 32) X[e] = xyz[(size_t)row * 4 * n3 + e];
-      tr_stage_row(Db, Dbar + (size_t)g.drow[row] * n3 * ax, n3, ax, lay.sax, lane);
-      __syncwarp();
-      tr_dbar_to_xbar(xb, Db, X, n3, ax, lay.sax, lane);
-      const T nn = (T)g.nnei;
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int j = 0; j < TR_C3; ++j) xb[a][j] = xb[a][j] / nn;
-      __syncwarp();
-    }
-    tr_entries(ent, secn, nl, g, ti, false, lane);
+    T xb[4][TR_C3];  // (dE/dxyz) / nnei, lane channels
+    tr_read_x4(xb, xbar + (size_t)row * 4 * n3, n3, lane);
+    tr_entries(ent, secn, nl, g, ti, false, lane, 0, g.ntypes);
     T* Zb3 = big;
-    T* Gb = big + n3 * R;
+    T* Gb = big + n3 * RS;
     for (int t = 0; t < g.ntypes; ++t) {
       const WV<T> W = tr_wview(net, lay, sw, t);
       for (int e0 = secn[t]; e0 < secn[t + 1]; e0 += R) {
@@ -597,7 +650,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xy
         if (lane < n1) {
           const T w1 = W.W1[lane], b1 = W.b1[lane];
 #pragma unroll
-          for (int r = 0; r < R; ++r) A1[lane * R + r] = tr_tanh(fma(ss[r], w1, b1));
+          for (int r = 0; r < R; ++r) A1[lane * RS + r] = tr_tanh(fma(ss[r], w1, b1));
         }
         __syncwarp();
         {
@@ -610,7 +663,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xy
               const T bb = W.b2[c];
 #pragma unroll
               for (int r = 0; r < R; ++r)
-                A2[c * R + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, net.res2, c, n1, r);
+                A2[c * RS + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, net.res2, c, n1, r);
             }
           }
         }
@@ -636,8 +689,8 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xy
                   part[r * 4 + a] = fma(G, xb[a][j], part[r * 4 + a]);
                   gbar = fma(rr[r * 4 + a], xb[a][j], gbar);
                 }
-                Zb3[c * R + r] = gbar * ((T)1 - y * y);
-                Gb[c * R + r] = gbar;
+                Zb3[c * RS + r] = gbar * ((T)1 - y * y);
+                Gb[c * RS + r] = gbar;
               }
             }
           }
@@ -654,7 +707,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xy
             for (int r = 0; r < R; ++r) {
               if (i < n2) {
                 hb2[j][r] += tr_res_adj<T, R>(Gb, net.res3, i, n2, r);
-                const T y2 = A2[i * R + r] - tr_res<T, R>(A1, net.res2, i, n1, r);
+                const T y2 = A2[i * RS + r] - tr_res<T, R>(A1, net.res2, i, n1, r);
                 zb2[j][r] = hb2[j][r] * ((T)1 - y2 * y2);
               } else {
                 zb2[j][r] = hb2[j][r] = (T)0;
@@ -664,15 +717,15 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xy
         }
         __syncwarp();
         T* Zb2 = big;
-        T* Hb2 = big + n2 * R;
+        T* Hb2 = big + n2 * RS;
 #pragma unroll
         for (int j = 0; j < TR_C2; ++j) {
           const int i = lane + 32 * j;
           if (i < n2)
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-              Zb2[i * R + r] = zb2[j][r];
-              Hb2[i * R + r] = hb2[j][r];
+              Zb2[i * RS + r] = zb2[j][r];
+              Hb2[i * RS + r] = hb2[j][r];
             }
         }
         __syncwarp();
@@ -684,7 +737,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xy
 #pragma unroll
             for (int r = 0; r < R; ++r) {
               const T h = hb1[0][r] + tr_res_adj<T, R>(Hb2, net.res2, lane, n1, r);
-              const T y1 = A1[lane * R + r];
+              const T y1 = A1[lane * RS + r];
               part[r * 4] = fma(h * ((T)1 - y1 * y1), w1, part[r * 4]);
             }
           }
@@ -708,6 +761,7 @@ __global__ void __launch_bounds__(256, 1)
 k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__ xyz,
          const T* __restrict__ avg, const T* __restrict__ std_, const double* __restrict__ fbar,
          const double* __restrict__ vbar, TrNet<T> net, TrGeom g, TrLayout lay) {
+  constexpr int RS = R + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -726,7 +780,7 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
     const TrAtom A = tr_atom(g, row);
     const T* av = avg + (size_t)A.ti * g.nnei * 4;
     const T* sdv = std_ + (size_t)A.ti * g.nnei * 4;
-    tr_entries(ent, secn, g.nlist + (size_t)row * g.nnei, g, A.ti, false, lane);
+    tr_entries(ent, secn, g.nlist + (size_t)row * g.nnei, g, A.ti, false, lane, 0, g.ntypes);
     T xd[4][TR_C3];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -754,8 +808,8 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const T y = tr_tanh(fma(ss[r], w1, b1));
-            A1[lane * R + r] = y;
-            At1[lane * R + r] = ((T)1 - y * y) * (sd[r] * w1);
+            A1[lane * RS + r] = y;
+            At1[lane * RS + r] = ((T)1 - y * y) * (sd[r] * w1);
           }
         }
         __syncwarp();
@@ -770,8 +824,9 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                A2[c * R + r] = y + tr_res<T, R>(A1, net.res2, c, n1, r);
-                At2[c * R + r] = ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, net.res2, c, n1, r);
+                A2[c * RS + r] = y + tr_res<T, R>(A1, net.res2, c, n1, r);
+                At2[c * RS + r] =
+                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, net.res2, c, n1, r);
               }
             }
           }
@@ -789,7 +844,8 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
                 const T G = y + tr_res<T, R>(A2, net.res3, c, n2, r);
-                const T Gd = ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At2, net.res3, c, n2, r);
+                const T Gd =
+                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At2, net.res3, c, n2, r);
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
                   xd[a][j] = fma(rd[r * 4 + a], G, fma(rr[r * 4 + a], Gd, xd[a][j]));
@@ -828,7 +884,8 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
         for (int k = 0; k < g.ax; ++k) {
           T d = (T)0;
 #pragma unroll
-          for (int a = 0; a < 4; ++a) d = fma(xd[a][j], X[a * n3 + k], fma(xc[a], Xd[a * n3 + k], d));
+          for (int a = 0; a < 4; ++a)
+            d = fma(xd[a][j], X[a * n3 + k], fma(xc[a], Xd[a * n3 + k], d));
           Drow[c * g.ax + k] = d;
         }
       }
@@ -838,21 +895,21 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
 }
 
 // ------------------------------------------------- reverse over tangent --
+// Neighbor types one after another: the block stages the weights of type t
+// and every warp accumulates that net's gradient in a private shared-memory
+// copy (plain adds, no atomics); the block sums its warps' copies into the
+// global gradient after each type.
 
 template <typename T, int R>
 __global__ void __launch_bounds__(256, 1)
-k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
-         const T* __restrict__ DbarJ, const T* __restrict__ Ddbar, const T* __restrict__ avg,
-         const T* __restrict__ std_, const double* __restrict__ fbar,
+k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard,
+         const T* __restrict__ avg, const T* __restrict__ std_, const double* __restrict__ fbar,
          const double* __restrict__ vbar, TrNet<T> net, TrGeom g, TrLayout lay) {
+  constexpr int RS = R + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* tb = tr_tbase<T>(smem_raw, lay);
-  T* sw = tb + lay.w_off;
-  T* sacc = tb + lay.acc_off;
-  if (lay.wsmem) tr_stage_weights(sw, net, lay, g.ntypes);
-  for (int e = threadIdx.x; e < g.ntypes * lay.pw; e += blockDim.x) sacc[e] = (T)0;
-  __syncthreads();
+  T* sw = tb + lay.w_off;  // weights of the current type (at type 0 of the view)
   int* ints;
   T* ws = tr_warp_base<T>(smem_raw, lay, w, ints);
   int* ent = ints;
@@ -861,55 +918,41 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
     *sd = ws + lay.o_sd;
   T *A1 = ws + lay.o_A1, *At1 = ws + lay.o_At1, *A2 = ws + lay.o_A2, *At2 = ws + lay.o_At2,
     *Zt2 = ws + lay.o_Zt2, *big = ws + lay.o_big;
-  const int n1 = net.n1, n2 = net.n2, n3 = net.n3, ax = g.ax;
+  const int n1 = net.n1, n2 = net.n2, n3 = net.n3;
+  const int s2 = lay.s2, s3 = lay.s3;
+  T* gacc = tb + lay.acc_off + (size_t)w * lay.pw;  // this warp's gradient copy
+  T* gW1 = gacc;
+  T* gb1 = gW1 + n1;
+  T* gW2 = gb1 + n1;
+  T* gb2 = gW2 + n1 * s2;
+  T* gW3 = gb2 + n2;
+  T* gb3 = gW3 + n2 * s3;
   const int gw = gridDim.x * lay.nw;
-  for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
-    const TrAtom A = tr_atom(g, row);
-    const T* av = avg + (size_t)A.ti * g.nnei * 4;
-    const T* sdv = std_ + (size_t)A.ti * g.nnei * 4;
-    // adjoints of xyz and xyz' (lane channels), divided by nnei
-    T xb[4][TR_C3], xbd[4][TR_C3];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int j = 0; j < TR_C3; ++j) xb[a][j] = xbd[a][j] = (T)0;
-    {
-      T* X = big;
-      T* Xd = big + 4 * n3;
-      T* Dj = big + 8 * n3;
-      T* Dd = Dj + n3 * lay.sax;
-      for (int e = lane; e < 4 * n3; e += 32) {
-        X[e] = xyz[(size_t)row * 4 * n3 + e];
-        Xd[e] = xyzd[(size_t)row * 4 * n3 + e];
-      }
-      const size_t dr = (size_t)g.drow[row] * n3 * ax;
-      tr_stage_row(Dj, DbarJ + dr, n3, ax, lay.sax, lane);
-      tr_stage_row(Dd, Ddbar + dr, n3, ax, lay.sax, lane);
-      __syncwarp();
-      tr_dbar_to_xbar(xbd, Dd, X, n3, ax, lay.sax, lane);
-      tr_dbar_to_xbar(xb, Dj, X, n3, ax, lay.sax, lane);
-      tr_dbar_to_xbar(xb, Dd, Xd, n3, ax, lay.sax, lane);
-      const T nn = (T)g.nnei;
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int j = 0; j < TR_C3; ++j) {
-          xb[a][j] = xb[a][j] / nn;
-          xbd[a][j] = xbd[a][j] / nn;
-        }
-      __syncwarp();
+  for (int t = 0; t < g.ntypes; ++t) {
+    __syncthreads();
+    if (lay.wsmem) {
+      TrNet<T> one = net;
+      one.W[0][0] = net.W[t][0];
+      one.W[0][1] = net.W[t][1];
+      one.W[0][2] = net.W[t][2];
+      one.b[0][0] = net.b[t][0];
+      one.b[0][1] = net.b[t][1];
+      one.b[0][2] = net.b[t][2];
+      tr_stage_weights(sw, one, lay, 1);
     }
-    tr_entries(ent, secn, g.nlist + (size_t)row * g.nnei, g, A.ti, true, lane);
-    for (int t = 0; t < g.ntypes; ++t) {
-      const WV<T> W = tr_wview(net, lay, sw, t);
-      T* gacc = sacc + (size_t)t * lay.pw;  // same layout as the staged weights
-      T* gW1 = gacc;
-      T* gb1 = gW1 + n1;
-      T* gW2 = gb1 + n1;
-      T* gb2 = gW2 + n1 * lay.s2;
-      T* gW3 = gb2 + n2;
-      T* gb3 = gW3 + n2 * lay.s3;
-      for (int e0 = secn[t]; e0 < secn[t + 1]; e0 += R) {
+    for (int e = lane; e < lay.pw; e += 32) gacc[e] = (T)0;
+    __syncthreads();
+    WV<T> W = tr_wview(net, lay, sw, lay.wsmem ? 0 : t);
+    for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
+      const TrAtom A = tr_atom(g, row);
+      const T* av = avg + (size_t)A.ti * g.nnei * 4;
+      const T* sdv = std_ + (size_t)A.ti * g.nnei * 4;
+      tr_entries(ent, secn, g.nlist + (size_t)row * g.nnei, g, A.ti, true, lane, t, t + 1);
+      if (secn[t + 1] == 0) continue;
+      T xb[4][TR_C3], xbd[4][TR_C3];
+      tr_read_x4(xb, xbar + (size_t)row * 4 * n3, n3, lane);
+      tr_read_x4(xbd, xbard + (size_t)row * 4 * n3, n3, lane);
+      for (int e0 = 0; e0 < secn[t + 1]; e0 += R) {
         const int ne = min(R, secn[t + 1] - e0);
         if (lane < R) {
           T Rv[4] = {(T)0, (T)0, (T)0, (T)0}, Rd[4] = {(T)0, (T)0, (T)0, (T)0};
@@ -935,8 +978,8 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const T y = tr_tanh(fma(ss[r], w1, b1));
-            A1[lane * R + r] = y;
-            At1[lane * R + r] = ((T)1 - y * y) * (sd[r] * w1);
+            A1[lane * RS + r] = y;
+            At1[lane * RS + r] = ((T)1 - y * y) * (sd[r] * w1);
           }
         }
         __syncwarp();
@@ -951,9 +994,10 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                A2[c * R + r] = y + tr_res<T, R>(A1, net.res2, c, n1, r);
-                At2[c * R + r] = ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, net.res2, c, n1, r);
-                Zt2[c * R + r] = acd[j][r];
+                A2[c * RS + r] = y + tr_res<T, R>(A1, net.res2, c, n1, r);
+                At2[c * RS + r] =
+                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, net.res2, c, n1, r);
+                Zt2[c * RS + r] = acd[j][r];
               }
             }
           }
@@ -961,18 +1005,18 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
         __syncwarp();
         // layer 3: forward, tangent and its adjoints
         T* Zb3 = big;
-        T* Zbt3 = big + n3 * R;
-        T* Gb = big + 2 * n3 * R;
-        T* Gbt = big + 3 * n3 * R;
+        T* Zbt3 = big + n3 * RS;
+        T* Gb = big + 2 * n3 * RS;
+        T* Gbt = big + 3 * n3 * RS;
         {
           T acc[TR_C3][R], acd[TR_C3][R];
           tr_gemv2<T, R, TR_C3>(acc, acd, A2, At2, n2, W.W3, W.s3, n3, lane);
 #pragma unroll
           for (int j = 0; j < TR_C3; ++j) {
             const int c = lane + 32 * j;
-            T zsum = (T)0;
             if (c < n3) {
               const T bb = W.b3[c];
+              T zsum = (T)0;
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
@@ -987,22 +1031,22 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
                 gbard *= mus[r];
                 const T zbd = gbard * q;
                 const T zb = (gbar - (T)2 * y * acd[j][r] * gbard) * q;
-                Zb3[c * R + r] = zb;
-                Zbt3[c * R + r] = zbd;
-                Gb[c * R + r] = gbar;
-                Gbt[c * R + r] = gbard;
+                Zb3[c * RS + r] = zb;
+                Zbt3[c * RS + r] = zbd;
+                Gb[c * RS + r] = gbar;
+                Gbt[c * RS + r] = gbard;
                 zsum += zb;
                 acc[j][r] = zb;   // reuse as z-bar
                 acd[j][r] = zbd;  // and z-bar of the tangent
               }
-              atomicAdd(&gb3[c], zsum);
+              gb3[c] += zsum;
             }
           }
           // W3 gradient: sum_r A2[i][r] zb[c][r] + At2[i][r] zbd[c][r]
           for (int i = 0; i < n2; ++i) {
             T a[R], ad[R];
-            tr_load_col<T, R>(a, A2 + i * R);
-            tr_load_col<T, R>(ad, At2 + i * R);
+            tr_load_col<T, R>(a, A2 + i * RS);
+            tr_load_col<T, R>(ad, At2 + i * RS);
 #pragma unroll
             for (int j = 0; j < TR_C3; ++j) {
               const int c = lane + 32 * j;
@@ -1010,7 +1054,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
                 T s = (T)0;
 #pragma unroll
                 for (int r = 0; r < R; ++r) s = fma(a[r], acc[j][r], fma(ad[r], acd[j][r], s));
-                atomicAdd(&gW3[i * lay.s3 + c], s);
+                gW3[i * s3 + c] += s;
               }
             }
           }
@@ -1028,21 +1072,21 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
             if (i < n2) {
               hb2[j][r] += tr_res_adj<T, R>(Gb, net.res3, i, n2, r);
               hbd2[j][r] += tr_res_adj<T, R>(Gbt, net.res3, i, n2, r);
-              const T y = A2[i * R + r] - tr_res<T, R>(A1, net.res2, i, n1, r);
+              const T y = A2[i * RS + r] - tr_res<T, R>(A1, net.res2, i, n1, r);
               const T q = (T)1 - y * y;
               zbd2[j][r] = hbd2[j][r] * q;
-              zb2[j][r] = (hb2[j][r] - (T)2 * y * Zt2[i * R + r] * hbd2[j][r]) * q;
+              zb2[j][r] = (hb2[j][r] - (T)2 * y * Zt2[i * RS + r] * hbd2[j][r]) * q;
               zsum += zb2[j][r];
             } else {
               zb2[j][r] = zbd2[j][r] = hb2[j][r] = hbd2[j][r] = (T)0;
             }
           }
-          if (i < n2) atomicAdd(&gb2[i], zsum);
+          if (i < n2) gb2[i] += zsum;
         }
         for (int k = 0; k < n1; ++k) {
           T a[R], ad[R];
-          tr_load_col<T, R>(a, A1 + k * R);
-          tr_load_col<T, R>(ad, At1 + k * R);
+          tr_load_col<T, R>(a, A1 + k * RS);
+          tr_load_col<T, R>(ad, At1 + k * RS);
 #pragma unroll
           for (int j = 0; j < TR_C2; ++j) {
             const int i = lane + 32 * j;
@@ -1050,25 +1094,25 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
               T s = (T)0;
 #pragma unroll
               for (int r = 0; r < R; ++r) s = fma(a[r], zb2[j][r], fma(ad[r], zbd2[j][r], s));
-              atomicAdd(&gW2[k * lay.s2 + i], s);
+              gW2[k * s2 + i] += s;
             }
           }
         }
         __syncwarp();
         T* Zb2 = big;
-        T* Zbd2 = big + n2 * R;
-        T* Hb2 = big + 2 * n2 * R;
-        T* Hbd2 = big + 3 * n2 * R;
+        T* Zbd2 = big + n2 * RS;
+        T* Hb2 = big + 2 * n2 * RS;
+        T* Hbd2 = big + 3 * n2 * RS;
 #pragma unroll
         for (int j = 0; j < TR_C2; ++j) {
           const int i = lane + 32 * j;
           if (i < n2)
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-              Zb2[i * R + r] = zb2[j][r];
-              Zbd2[i * R + r] = zbd2[j][r];
-              Hb2[i * R + r] = hb2[j][r];
-              Hbd2[i * R + r] = hbd2[j][r];
+              Zb2[i * RS + r] = zb2[j][r];
+              Zbd2[i * RS + r] = zbd2[j][r];
+              Hb2[i * RS + r] = hb2[j][r];
+              Hbd2[i * RS + r] = hbd2[j][r];
             }
         }
         __syncwarp();
@@ -1078,47 +1122,46 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xyz, const T* __restrict__ xyzd,
           tr_gemvT2<T, R, TR_C1>(hb1, hbd1, Zb2, Zbd2, n2, W.W2, W.s2, n1, lane);
           if (lane < n1) {
             const T w1 = W.W1[lane];
-            T gw = (T)0, gbs = (T)0;
+            T gws = (T)0, gbs = (T)0;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
               const T h = hb1[0][r] + tr_res_adj<T, R>(Hb2, net.res2, lane, n1, r);
               const T hd = hbd1[0][r] + tr_res_adj<T, R>(Hbd2, net.res2, lane, n1, r);
-              const T y = A1[lane * R + r];
+              const T y = A1[lane * RS + r];
               const T q = (T)1 - y * y;
               const T zd = sd[r] * w1;
               const T zbd = hd * q;
               const T zb = (h - (T)2 * y * zd * hd) * q;
-              gw = fma(ss[r], zb, fma(sd[r], zbd, gw));
+              gws = fma(ss[r], zb, fma(sd[r], zbd, gws));
               gbs += zb;
             }
-            atomicAdd(&gW1[lane], gw);
-            atomicAdd(&gb1[lane], gbs);
+            gW1[lane] += gws;
+            gb1[lane] += gbs;
           }
         }
         __syncwarp();
       }
     }
-  }
-  __syncthreads();
-  // block partials -> global gradients (unpadded layouts)
-  for (int t = 0; t < g.ntypes; ++t) {
-    const T* gacc = sacc + (size_t)t * lay.pw;
-    const T* gW1 = gacc;
-    const T* gb1 = gW1 + n1;
-    const T* gW2 = gb1 + n1;
-    const T* gb2 = gW2 + n1 * lay.s2;
-    const T* gW3 = gb2 + n2;
-    const T* gb3 = gW3 + n2 * lay.s3;
+    __syncthreads();
+    // the block's warps' copies -> the global gradient of net t (unpadded)
+    const T* accb = tb + lay.acc_off;
+    auto sumw = [&](int e) {
+      T s = (T)0;
+      for (int k = 0; k < lay.nw; ++k) s += accb[(size_t)k * lay.pw + e];
+      return s;
+    };
     for (int k = threadIdx.x; k < n1; k += blockDim.x) {
-      atomicAdd(&grad.W[t][0][k], gW1[k]);
-      atomicAdd(&grad.b[t][0][k], gb1[k]);
+      atomicAdd(&grad.W[t][0][k], sumw(k));
+      atomicAdd(&grad.b[t][0][k], sumw(n1 + k));
     }
     for (int e = threadIdx.x; e < n1 * n2; e += blockDim.x)
-      atomicAdd(&grad.W[t][1][e], gW2[(e / n2) * lay.s2 + e % n2]);
-    for (int k = threadIdx.x; k < n2; k += blockDim.x) atomicAdd(&grad.b[t][1][k], gb2[k]);
+      atomicAdd(&grad.W[t][1][e], sumw(2 * n1 + (e / n2) * s2 + e % n2));
+    for (int k = threadIdx.x; k < n2; k += blockDim.x)
+      atomicAdd(&grad.b[t][1][k], sumw(2 * n1 + n1 * s2 + k));
     for (int e = threadIdx.x; e < n2 * n3; e += blockDim.x)
-      atomicAdd(&grad.W[t][2][e], gW3[(e / n3) * lay.s3 + e % n3]);
-    for (int k = threadIdx.x; k < n3; k += blockDim.x) atomicAdd(&grad.b[t][2][k], gb3[k]);
+      atomicAdd(&grad.W[t][2][e], sumw(2 * n1 + n1 * s2 + n2 + (e / n3) * s3 + e % n3));
+    for (int k = threadIdx.x; k < n3; k += blockDim.x)
+      atomicAdd(&grad.b[t][2][k], sumw(2 * n1 + n1 * s2 + n2 + n2 * s3 + k));
   }
 }
 
@@ -1324,6 +1367,7 @@ enum TrKind { TR_FWD, TR_BWD, TR_TAN, TR_REV };
 
 template <typename T>
 static TrLayout tr_layout(TrKind kind, int R, const TrDims& d, bool wsmem, int nw) {
+  const int RS = R + 1;
   TrLayout L{};
   L.nw = nw;
   L.ints_warp = (d.nnei + TR_MAXT + 1 + 3) & ~3;
@@ -1333,8 +1377,14 @@ static TrLayout tr_layout(TrKind kind, int R, const TrDims& d, bool wsmem, int n
   L.pw = (2 * d.n1 + d.n1 * L.s2 + d.n2 + d.n2 * L.s3 + d.n3 + 3) & ~3;
   L.wsmem = wsmem ? 1 : 0;
   L.w_off = 0;
-  L.acc_off = wsmem ? d.ntypes * L.pw : 0;
-  L.warp_off = L.acc_off + (kind == TR_REV ? d.ntypes * L.pw : 0);
+  if (kind == TR_REV) {  // one type's weights, then a gradient copy per warp
+    L.acc_off = wsmem ? L.pw : 0;
+    L.warp_off = L.acc_off + nw * L.pw;
+  } else {
+    L.acc_off = wsmem ? d.ntypes * L.pw : 0;
+    L.warp_off = L.acc_off;
+  }
+  const bool tan = kind == TR_TAN || kind == TR_REV;
   int o = 0;
   L.o_rr = o;
   o += 4 * R;
@@ -1348,28 +1398,21 @@ static TrLayout tr_layout(TrKind kind, int R, const TrDims& d, bool wsmem, int n
   o += R;
   o = (o + 3) & ~3;
   L.o_A1 = o;
-  o += d.n1 * R;
+  o += d.n1 * RS;
   L.o_At1 = o;
-  if (kind == TR_TAN || kind == TR_REV) o += d.n1 * R;
+  if (tan) o += d.n1 * RS;
   L.o_A2 = o;
-  o += d.n2 * R;
+  o += d.n2 * RS;
   L.o_At2 = o;
-  if (kind == TR_TAN || kind == TR_REV) o += d.n2 * R;
+  if (tan) o += d.n2 * RS;
   L.o_Zt2 = o;
-  if (kind == TR_REV) o += d.n2 * R;
+  if (kind == TR_REV) o += d.n2 * RS;
   o = (o + 3) & ~3;
   L.o_big = o;
   int big = 4 * d.n3;
-  if (kind == TR_BWD) {
-    big = std::max(big, 4 * d.n3 + d.n3 * L.sax);
-    big = std::max(big, 2 * d.n3 * R);
-    big = std::max(big, 2 * d.n2 * R);
-  } else if (kind == TR_TAN) {
-    big = 8 * d.n3;
-  } else if (kind == TR_REV) {
-    big = std::max(8 * d.n3 + 2 * d.n3 * L.sax, 4 * d.n3 * R);
-    big = std::max(big, 4 * d.n2 * R);
-  }
+  if (kind == TR_BWD) big = std::max(2 * d.n3 * RS, 2 * d.n2 * RS);
+  else if (kind == TR_TAN) big = 8 * d.n3;
+  else if (kind == TR_REV) big = std::max(4 * d.n3 * RS, 4 * d.n2 * RS);
   o += big;
   L.warp_sz = (o + 3) & ~3;
   return L;
@@ -1512,6 +1555,23 @@ static int tr_prepare(TrKind kind, TrNet<T>& net, TrGeom& g, TrLayout& L, const 
 
 static int fit_grid(long long items) { return grid_stride_blocks(items, 256); }
 
+template <typename T>
+static int tr_xbar(T* xb, T* xbd, const T* xyz, const T* xyzd, const T* Dj, const T* Dd,
+                   const int* drow, int nrows, int n3, int ax, int nnei, cudaStream_t st) {
+  const int sax = ax | 1;
+  const size_t smem = 2 * (size_t)(8 * n3 + 2 * n3 * sax) * sizeof(T);
+  if (cudaFuncSetAttribute(k_tr_xbar<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess) {
+    set_error("se_a_train: cannot reserve %zu bytes of shared memory", smem);
+    return DPB_ERR_CUDA;
+  }
+  const int grid = std::max(1, std::min(ceil_div(nrows, 2), sm_count() * 8));
+  k_tr_xbar<T><<<grid, 64, smem, st>>>(xb, xbd, xyz, xyzd, Dj, Dd, drow, nrows, n3, ax, nnei,
+                                       sax);
+  DPB_CHECK_LAUNCH("se_a_train/xbar");
+  return DPB_OK;
+}
+
 }  // namespace dpb
 
 using namespace dpb;
@@ -1542,10 +1602,10 @@ using namespace dpb;
     DPB_CHECK_LAUNCH("se_a_train_fwd");                                                         \
     return DPB_OK;                                                                              \
   }                                                                                             \
-  int dpb_se_a_train_bwd_##SUF(T* net_deriv, const T* em, const T* xyz, const T* d_descrpt,    \
-                               const int* nlist, const int* type, const int* drow,              \
-                               const T* const* W, const T* const* b, const int* widths,         \
-                               const int* sec, int nsec, int nrows, int axis,                   \
+  int dpb_se_a_train_bwd_##SUF(T* net_deriv, T* scratch, const T* em, const T* xyz,          \
+                               const T* d_descrpt, const int* nlist, const int* type,           \
+                               const int* drow, const T* const* W, const T* const* b,           \
+                               const int* widths, const int* sec, int nsec, int nrows, int axis,\
                                dpb_stream_t stream) {                                           \
     TrNet<T> net;                                                                               \
     TrGeom g;                                                                                   \
@@ -1555,19 +1615,22 @@ using namespace dpb;
                            0.f);                                                                \
     if (rc) return rc;                                                                          \
     if (nrows == 0) return DPB_OK;                                                              \
-    if (!net_deriv || !em || !xyz || !d_descrpt) {                                              \
+    if (!net_deriv || !scratch || !em || !xyz || !d_descrpt) {                                  \
       set_error("se_a_train_bwd: null buffer");                                                 \
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
     cudaStream_t st = as_stream(stream);                                                        \
     DPB_CUDA(cudaMemsetAsync(net_deriv, 0, sizeof(T) * (size_t)nrows * g.nnei * 4, st),         \
              "se_a_train_bwd");                                                                 \
+    rc = tr_xbar<T>(scratch, nullptr, xyz, nullptr, d_descrpt, nullptr, drow, nrows, net.n3,    \
+                    axis, g.nnei, st);                                                          \
+    if (rc) return rc;                                                                          \
     auto kern = k_tr_bwd<T, TrTraits<T>::R>;                                                    \
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
     if (rc) return rc;                                                                          \
-    kern<<<grid, L.nw * 32, smem, st>>>(net_deriv, em, xyz, d_descrpt, net, g, L);              \
+    kern<<<grid, L.nw * 32, smem, st>>>(net_deriv, em, scratch, net, g, L);                     \
     DPB_CHECK_LAUNCH("se_a_train_bwd");                                                         \
     return DPB_OK;                                                                              \
   }                                                                                             \
@@ -1602,9 +1665,9 @@ using namespace dpb;
     DPB_CHECK_LAUNCH("se_a_train_tan");                                                         \
     return DPB_OK;                                                                              \
   }                                                                                             \
-  int dpb_se_a_train_rev_##SUF(T* const* gW, T* const* gb, const T* xyz, const T* xyz_t,       \
-                               const T* d_descrpt, const T* d_descrpt_t, const T* avg,          \
-                               const T* std_, const double* force_bar,                          \
+  int dpb_se_a_train_rev_##SUF(T* const* gW, T* const* gb, T* scratch, const T* xyz,         \
+                               const T* xyz_t, const T* d_descrpt, const T* d_descrpt_t,        \
+                               const T* avg, const T* std_, const double* force_bar,            \
                                const double* virial_bar, const double* cw, const int* nlist,    \
                                const int* type, const int* drow, const int* atom_off,           \
                                const double* box, const int* row_frame, int nframes,            \
@@ -1620,8 +1683,8 @@ using namespace dpb;
                            rcut_smth);                                                          \
     if (rc) return rc;                                                                          \
     if (nrows == 0) return DPB_OK;                                                              \
-    if (!gW || !gb || !xyz || !xyz_t || !d_descrpt || !d_descrpt_t || !avg || !std_ ||          \
-        !force_bar || !virial_bar || !cw || !atom_off || !box || !row_frame) {                  \
+    if (!gW || !gb || !scratch || !xyz || !xyz_t || !d_descrpt || !d_descrpt_t || !avg ||       \
+        !std_ || !force_bar || !virial_bar || !cw || !atom_off || !box || !row_frame) {         \
       set_error("se_a_train_rev: null buffer");                                                 \
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
@@ -1635,14 +1698,19 @@ using namespace dpb;
           return DPB_ERR_INVALID;                                                               \
         }                                                                                       \
       }                                                                                         \
+    cudaStream_t st = as_stream(stream);                                                        \
+    T* xb = scratch;                                                                            \
+    T* xbd = scratch + (size_t)nrows * 4 * net.n3;                                              \
+    rc = tr_xbar<T>(xb, xbd, xyz, xyz_t, d_descrpt, d_descrpt_t, drow, nrows, net.n3, axis,     \
+                    g.nnei, st);                                                                \
+    if (rc) return rc;                                                                          \
     auto kern = k_tr_rev<T, TrTraits<T>::R>;                                                    \
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
     if (rc) return rc;                                                                          \
-    kern<<<grid, L.nw * 32, smem, as_stream(stream)>>>(gr, xyz, xyz_t, d_descrpt, d_descrpt_t, \
-                                                       avg, std_, force_bar, virial_bar, net,   \
-                                                       g, L);                                   \
+    kern<<<grid, L.nw * 32, smem, st>>>(gr, xb, xbd, avg, std_, force_bar, virial_bar, net, g,  \
+                                        L);                                                     \
     DPB_CHECK_LAUNCH("se_a_train_rev");                                                         \
     return DPB_OK;                                                                              \
   }                                                                                             \

@@ -241,6 +241,7 @@ class SeATrainer:
         self.Dbar = z((N, M * ax))
         self.net_deriv = z((N, nnei * 4))
         self.xyz_t = z((N, 4, M))
+        self.xbar = z((2, N, 4, M))  # adjoints of xyz and xyz' (kernel scratch)
         self.Dt = z((N, M * ax))
         self.DbarJ = z((N, M * ax))
         self.Ddbar = z((N, M * ax))
@@ -374,7 +375,8 @@ class SeATrainer:
         e_fn = "dpb_batch_energy" if suf == "f32" else "dpb_batch_energy_f64"
         call(e_fn, ptr(self.energy), ptr(self.e_rows), ptr(ft.drow), ptr(self.e_const),
              ptr(ft.atom_off), F, s)
-        call(f"dpb_se_a_train_bwd_{suf}", ptr(self.net_deriv), ptr(self.em), ptr(self.xyz),
+        call(f"dpb_se_a_train_bwd_{suf}", ptr(self.net_deriv), ptr(self.xbar), ptr(self.em),
+             ptr(self.xyz),
              ptr(self.Dbar), ptr(self.nlist), ptr(ft.type), ptr(ft.drow), self.Wp, self.bp,
              self.widths.ctypes.data, sec.ctypes.data, sec.size, N, self.ax, s)
         f_fn = "dpb_batch_force_virial_a" if suf == "f32" else "dpb_batch_force_virial_a_f64"
@@ -430,7 +432,8 @@ class SeATrainer:
                 dAd = self.Ddbar[o:o + n] if l == 0 else bufs[l - 1]["Ad"]
                 self._adj_in(dA, bf["Zb"], ly["W"], bf["A"], ly["w_out"], ly["w_in"], s)
                 self._adj_in(dAd, bf["Zbd"], ly["W"], bf["Ad"], ly["w_out"], ly["w_in"], s)
-        call(f"dpb_se_a_train_rev_{suf}", self.gWp, self.gbp, ptr(self.xyz), ptr(self.xyz_t),
+        call(f"dpb_se_a_train_rev_{suf}", self.gWp, self.gbp, ptr(self.xbar), ptr(self.xyz),
+             ptr(self.xyz_t),
              ptr(self.DbarJ), ptr(self.Ddbar), ptr(self.avg), ptr(self.std), ptr(gF), ptr(gV),
              ptr(ft.cw), ptr(self.nlist), ptr(ft.type), ptr(ft.drow), ptr(ft.atom_off),
              ptr(ft.box), ptr(ft.row_frame), F, self.Wp, self.bp, self.widths.ctypes.data,

@@ -492,7 +492,7 @@ DPB_API int dpb_gemm_tf32x3_f32(const float* A, int M, int K,
  * fwd: xyz [N, 4, n3] (atom order), descrpt [N, n3 * axis] (drow order) from
  *      em [N, nnei, 4].
  * bwd: net_deriv = dE/d(em) [N, nnei, 4] (zero on padded slots) from
- *      d_descrpt = dE/dD (drow order).
+ *      d_descrpt = dE/dD (drow order); scratch: device [N, 4, n3].
  * tan: tangent of xyz and D along u, u recomputed from the coordinates (cw,
  *      FP64), avg/std [ntypes, nnei * 4], force_bar = dL/dF [N, 3] and
  *      virial_bar = dL/dV [F, 9] (FP64): u = (d em / d r_i) . (Fbar_j -
@@ -500,18 +500,19 @@ DPB_API int dpb_gemm_tf32x3_f32(const float* A, int M, int K,
  * rev: adds to gW / gb (host arrays of device pointers laid out as W / b)
  *      the embedding gradient of J = <Dbar_J, D> + <Ddbar, D'> continued
  *      through xyz, xyz' and the embedding: d_descrpt / d_descrpt_t are the
- *      adjoints of D and D' from the fitting's reverse pass. */
+ *      adjoints of D and D' from the fitting's reverse pass; scratch: device
+ *      [2, N, 4, n3]. */
 /* float */
 DPB_API int dpb_se_a_train_fwd_f32(float* xyz, float* descrpt, const float* em, const int* nlist,
                                    const int* type, const int* drow, const float* const* W,
                                    const float* const* b, const int* widths, const int* sec,
                                    int nsec, int nrows, int axis, const unsigned char* fold,
                                    dpb_stream_t stream);
-DPB_API int dpb_se_a_train_bwd_f32(float* net_deriv, const float* em, const float* xyz,
-                                   const float* d_descrpt, const int* nlist, const int* type,
-                                   const int* drow, const float* const* W, const float* const* b,
-                                   const int* widths, const int* sec, int nsec, int nrows, int axis,
-                                   dpb_stream_t stream);
+DPB_API int dpb_se_a_train_bwd_f32(float* net_deriv, float* scratch, const float* em,
+                                   const float* xyz, const float* d_descrpt, const int* nlist,
+                                   const int* type, const int* drow, const float* const* W,
+                                   const float* const* b, const int* widths, const int* sec,
+                                   int nsec, int nrows, int axis, dpb_stream_t stream);
 DPB_API int dpb_se_a_train_tan_f32(float* xyz_t, float* descrpt_t, const float* xyz,
                                    const float* avg, const float* std_, const double* force_bar,
                                    const double* virial_bar, const double* cw, const int* nlist,
@@ -520,8 +521,8 @@ DPB_API int dpb_se_a_train_tan_f32(float* xyz_t, float* descrpt_t, const float* 
                                    const float* const* W, const float* const* b, const int* widths,
                                    const int* sec, int nsec, int nrows, int axis, float rcut,
                                    float rcut_smth, dpb_stream_t stream);
-DPB_API int dpb_se_a_train_rev_f32(float* const* gW, float* const* gb, const float* xyz,
-                                   const float* xyz_t, const float* d_descrpt,
+DPB_API int dpb_se_a_train_rev_f32(float* const* gW, float* const* gb, float* scratch,
+                                   const float* xyz, const float* xyz_t, const float* d_descrpt,
                                    const float* d_descrpt_t, const float* avg, const float* std_,
                                    const double* force_bar, const double* virial_bar,
                                    const double* cw, const int* nlist, const int* type,
@@ -569,11 +570,11 @@ DPB_API int dpb_se_a_train_fwd_f64(double* xyz, double* descrpt, const double* e
                                    const double* const* b, const int* widths, const int* sec,
                                    int nsec, int nrows, int axis, const unsigned char* fold,
                                    dpb_stream_t stream);
-DPB_API int dpb_se_a_train_bwd_f64(double* net_deriv, const double* em, const double* xyz,
-                                   const double* d_descrpt, const int* nlist, const int* type,
-                                   const int* drow, const double* const* W, const double* const* b,
-                                   const int* widths, const int* sec, int nsec, int nrows, int axis,
-                                   dpb_stream_t stream);
+DPB_API int dpb_se_a_train_bwd_f64(double* net_deriv, double* scratch, const double* em,
+                                   const double* xyz, const double* d_descrpt, const int* nlist,
+                                   const int* type, const int* drow, const double* const* W,
+                                   const double* const* b, const int* widths, const int* sec,
+                                   int nsec, int nrows, int axis, dpb_stream_t stream);
 DPB_API int dpb_se_a_train_tan_f64(double* xyz_t, double* descrpt_t, const double* xyz,
                                    const double* avg, const double* std_, const double* force_bar,
                                    const double* virial_bar, const double* cw, const int* nlist,
@@ -582,8 +583,8 @@ DPB_API int dpb_se_a_train_tan_f64(double* xyz_t, double* descrpt_t, const doubl
                                    const double* const* W, const double* const* b,
                                    const int* widths, const int* sec, int nsec, int nrows, int axis,
                                    float rcut, float rcut_smth, dpb_stream_t stream);
-DPB_API int dpb_se_a_train_rev_f64(double* const* gW, double* const* gb, const double* xyz,
-                                   const double* xyz_t, const double* d_descrpt,
+DPB_API int dpb_se_a_train_rev_f64(double* const* gW, double* const* gb, double* scratch,
+                                   const double* xyz, const double* xyz_t, const double* d_descrpt,
                                    const double* d_descrpt_t, const double* avg, const double* std_,
                                    const double* force_bar, const double* virial_bar,
                                    const double* cw, const int* nlist, const int* type,
