@@ -39,6 +39,24 @@ constexpr int TR_C1 = 1, TR_C2 = 2, TR_C3 = 4;  // channels per lane: n1 <= 32, 
 constexpr int TR_MAXAX = 32;
 enum { TR_RES_NONE = 0, TR_RES_IDENT = 1, TR_RES_DUP = 2 };
 
+// rows per group and where the weights live, per precision
+template <typename T>
+struct TrTraits;
+template <>
+struct TrTraits<float> {
+  static constexpr int R = 8;
+  static constexpr bool WSMEM = true;
+};
+template <>
+struct TrTraits<double> {
+  static constexpr int R = 4;
+  static constexpr bool WSMEM = false;
+};
+
+__host__ __device__ constexpr int tr_res_kind(int n_out, int n_in) {
+  return n_out == n_in ? TR_RES_IDENT : (n_out == 2 * n_in ? TR_RES_DUP : TR_RES_NONE);
+}
+
 __device__ __forceinline__ float tr_tanh(float x) { return tanhf(x); }
 __device__ __forceinline__ double tr_tanh(double x) { return tanh(x); }
 
@@ -84,20 +102,20 @@ struct WV {
   int s2, s3;
 };
 
-template <typename T>
-__device__ __forceinline__ WV<T> tr_wview(const TrNet<T>& net, const TrLayout& lay,
-                                          const T* sw, int t) {
+// layer pointers of net t: staged in shared memory (odd strides sw2 = n2 | 1,
+// sw3 = n3 | 1, type blocks of pw elements) or read from global memory
+template <typename T, bool WS>
+__device__ __forceinline__ WV<T> tr_wview(const TrNet<T>& net, const T* sw, int t, int pw,
+                                          int n1, int n2, int sw2, int sw3) {
   WV<T> v;
-  if (lay.wsmem) {
-    const T* base = sw + (size_t)t * lay.pw;
+  if (WS) {
+    const T* base = sw + (size_t)t * pw;
     v.W1 = base;
-    v.b1 = v.W1 + net.n1;
-    v.W2 = v.b1 + net.n1;
-    v.b2 = v.W2 + net.n1 * lay.s2;
-    v.W3 = v.b2 + net.n2;
-    v.b3 = v.W3 + net.n2 * lay.s3;
-    v.s2 = lay.s2;
-    v.s3 = lay.s3;
+    v.b1 = v.W1 + n1;
+    v.W2 = v.b1 + n1;
+    v.b2 = v.W2 + n1 * sw2;
+    v.W3 = v.b2 + n2;
+    v.b3 = v.W3 + n2 * sw3;
   } else {
     v.W1 = net.W[t][0];
     v.b1 = net.b[t][0];
@@ -105,9 +123,9 @@ __device__ __forceinline__ WV<T> tr_wview(const TrNet<T>& net, const TrLayout& l
     v.b2 = net.b[t][1];
     v.W3 = net.W[t][2];
     v.b3 = net.b[t][2];
-    v.s2 = net.n2;
-    v.s3 = net.n3;
   }
+  v.s2 = sw2;
+  v.s3 = sw3;
   return v;
 }
 
@@ -188,7 +206,7 @@ __device__ __forceinline__ void tr_gemv(T (&acc)[CP][R], const T* in, int n_in, 
   for (int j = 0; j < CP; ++j)
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[j][r] = (T)0;
-#pragma unroll 2
+#pragma unroll 5
   for (int i = 0; i < n_in; ++i) {
     T a[R];
     tr_load_col<T, R>(a, in + i * (R + 1));
@@ -211,6 +229,7 @@ __device__ __forceinline__ void tr_gemv2(T (&acc)[CP][R], T (&acd)[CP][R], const
   for (int j = 0; j < CP; ++j)
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[j][r] = acd[j][r] = (T)0;
+#pragma unroll 5
   for (int i = 0; i < n_in; ++i) {
     T a[R], ad[R];
     tr_load_col<T, R>(a, in + i * (R + 1));
@@ -237,7 +256,7 @@ __device__ __forceinline__ void tr_gemvT(T (&acc)[CP][R], const T* zb, int n_out
   for (int j = 0; j < CP; ++j)
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[j][r] = (T)0;
-#pragma unroll 2
+#pragma unroll 5
   for (int c = 0; c < n_out; ++c) {
     T z[R];
     tr_load_col<T, R>(z, zb + c * (R + 1));
@@ -259,6 +278,7 @@ __device__ __forceinline__ void tr_gemvT2(T (&acc)[CP][R], T (&acd)[CP][R], cons
   for (int j = 0; j < CP; ++j)
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[j][r] = acd[j][r] = (T)0;
+#pragma unroll 5
   for (int c = 0; c < n_out; ++c) {
     T z[R], zd[R];
     tr_load_col<T, R>(z, zb + c * (R + 1));
@@ -480,7 +500,7 @@ k_tr_xbar(T* __restrict__ xb_out, T* __restrict__ xbd_out, const T* __restrict__
 
 // ---------------------------------------------------------------- forward --
 
-template <typename T, int R>
+template <typename T, int R, int N1, int N2, int N3>
 __global__ void __launch_bounds__(256, 1)
 k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ em,
          TrNet<T> net, TrGeom g, TrLayout lay) {
@@ -488,7 +508,7 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
-  if (lay.wsmem) tr_stage_weights(sw, net, lay, g.ntypes);
+  if (TrTraits<T>::WSMEM) tr_stage_weights(sw, net, lay, g.ntypes);
   __syncthreads();
   int* ints;
   T* ws = tr_warp_base<T>(smem_raw, lay, w, ints);
@@ -496,7 +516,12 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
   int* secn = ints + g.nnei;
   T *rr = ws + lay.o_rr, *mus = ws + lay.o_mu, *ss = ws + lay.o_s;
   T *A1 = ws + lay.o_A1, *A2 = ws + lay.o_A2, *big = ws + lay.o_big;
-  const int n1 = net.n1, n2 = net.n2, n3 = net.n3;
+  // compile-time widths when N1 > 0 (the standard [25, 50, 100] net), else runtime
+  constexpr bool WS = TrTraits<T>::WSMEM;
+  const int n1 = N1 > 0 ? N1 : net.n1, n2 = N1 > 0 ? N2 : net.n2, n3 = N1 > 0 ? N3 : net.n3;
+  const int res2 = N1 > 0 ? tr_res_kind(N2, N1) : net.res2;
+  const int res3 = N1 > 0 ? tr_res_kind(N3, N2) : net.res3;
+  const int sw2 = WS ? (n2 | 1) : n2, sw3 = WS ? (n3 | 1) : n3;
   const int gw = gridDim.x * lay.nw;
   for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
     const int ti = g.type[row];
@@ -508,7 +533,7 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
 #pragma unroll
       for (int j = 0; j < TR_C3; ++j) xyz[a][j] = (T)0;
     for (int t = 0; t < g.ntypes; ++t) {
-      const WV<T> W = tr_wview(net, lay, sw, t);
+      const WV<T> W = tr_wview<T, WS>(net, sw, t, lay.pw, n1, n2, sw2, sw3);
       for (int e0 = secn[t]; e0 < secn[t + 1]; e0 += R) {
         const int ne = min(R, secn[t + 1] - e0);
         if (lane < R) {
@@ -536,7 +561,7 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
         __syncwarp();
         {
           T acc[TR_C2][R];
-          tr_gemv<T, R, TR_C2>(acc, A1, n1, W.W2, W.s2, n2, lane);
+          tr_gemv<T, R, TR_C2>(acc, A1, n1, W.W2, sw2, n2, lane);
 #pragma unroll
           for (int j = 0; j < TR_C2; ++j) {
             const int c = lane + 32 * j;
@@ -544,14 +569,14 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
               const T bb = W.b2[c];
 #pragma unroll
               for (int r = 0; r < R; ++r)
-                A2[c * RS + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, net.res2, c, n1, r);
+                A2[c * RS + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, res2, c, n1, r);
             }
           }
         }
         __syncwarp();
         {
           T acc[TR_C3][R];
-          tr_gemv<T, R, TR_C3>(acc, A2, n2, W.W3, W.s3, n3, lane);
+          tr_gemv<T, R, TR_C3>(acc, A2, n2, W.W3, sw3, n3, lane);
 #pragma unroll
           for (int j = 0; j < TR_C3; ++j) {
             const int c = lane + 32 * j;
@@ -559,7 +584,7 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
               const T bb = W.b3[c];
 #pragma unroll
               for (int r = 0; r < R; ++r) {
-                const T G = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A2, net.res3, c, n2, r);
+                const T G = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A2, res3, c, n2, r);
                 const T mg = mus[r] * G;
 #pragma unroll
                 for (int a = 0; a < 4; ++a) xyz[a][j] = fma(rr[r * 4 + a], mg, xyz[a][j]);
@@ -603,7 +628,7 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
 
 // ------------------------------------------------------- force backward --
 
-template <typename T, int R>
+template <typename T, int R, int N1, int N2, int N3>
 __global__ void __launch_bounds__(256, 1)
 k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xbar,
          TrNet<T> net, TrGeom g, TrLayout lay) {
@@ -611,7 +636,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
-  if (lay.wsmem) tr_stage_weights(sw, net, lay, g.ntypes);
+  if (TrTraits<T>::WSMEM) tr_stage_weights(sw, net, lay, g.ntypes);
   __syncthreads();
   int* ints;
   T* ws = tr_warp_base<T>(smem_raw, lay, w, ints);
@@ -619,7 +644,12 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
   int* secn = ints + g.nnei;
   T *rr = ws + lay.o_rr, *ss = ws + lay.o_s;
   T *A1 = ws + lay.o_A1, *A2 = ws + lay.o_A2, *big = ws + lay.o_big;
-  const int n1 = net.n1, n2 = net.n2, n3 = net.n3;
+  // compile-time widths when N1 > 0 (the standard [25, 50, 100] net), else runtime
+  constexpr bool WS = TrTraits<T>::WSMEM;
+  const int n1 = N1 > 0 ? N1 : net.n1, n2 = N1 > 0 ? N2 : net.n2, n3 = N1 > 0 ? N3 : net.n3;
+  const int res2 = N1 > 0 ? tr_res_kind(N2, N1) : net.res2;
+  const int res3 = N1 > 0 ? tr_res_kind(N3, N2) : net.res3;
+  const int sw2 = WS ? (n2 | 1) : n2, sw3 = WS ? (n3 | 1) : n3;
   const int gw = gridDim.x * lay.nw;
   for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
     const int ti = g.type[row];
@@ -630,7 +660,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
     T* Zb3 = big;
     T* Gb = big + n3 * RS;
     for (int t = 0; t < g.ntypes; ++t) {
-      const WV<T> W = tr_wview(net, lay, sw, t);
+      const WV<T> W = tr_wview<T, WS>(net, sw, t, lay.pw, n1, n2, sw2, sw3);
       for (int e0 = secn[t]; e0 < secn[t + 1]; e0 += R) {
         const int ne = min(R, secn[t + 1] - e0);
         if (lane < R) {
@@ -655,7 +685,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
         __syncwarp();
         {
           T acc[TR_C2][R];
-          tr_gemv<T, R, TR_C2>(acc, A1, n1, W.W2, W.s2, n2, lane);
+          tr_gemv<T, R, TR_C2>(acc, A1, n1, W.W2, sw2, n2, lane);
 #pragma unroll
           for (int j = 0; j < TR_C2; ++j) {
             const int c = lane + 32 * j;
@@ -663,7 +693,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
               const T bb = W.b2[c];
 #pragma unroll
               for (int r = 0; r < R; ++r)
-                A2[c * RS + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, net.res2, c, n1, r);
+                A2[c * RS + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, res2, c, n1, r);
             }
           }
         }
@@ -673,7 +703,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
         for (int k = 0; k < 4 * R; ++k) part[k] = (T)0;
         {
           T acc[TR_C3][R];
-          tr_gemv<T, R, TR_C3>(acc, A2, n2, W.W3, W.s3, n3, lane);
+          tr_gemv<T, R, TR_C3>(acc, A2, n2, W.W3, sw3, n3, lane);
 #pragma unroll
           for (int j = 0; j < TR_C3; ++j) {
             const int c = lane + 32 * j;
@@ -682,7 +712,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                const T G = y + tr_res<T, R>(A2, net.res3, c, n2, r);
+                const T G = y + tr_res<T, R>(A2, res3, c, n2, r);
                 T gbar = (T)0;
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
@@ -699,15 +729,15 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
         // layer 2 adjoint, lanes over layer-2 channels
         T zb2[TR_C2][R], hb2[TR_C2][R];
         {
-          tr_gemvT<T, R, TR_C2>(hb2, Zb3, n3, W.W3, W.s3, n2, lane);
+          tr_gemvT<T, R, TR_C2>(hb2, Zb3, n3, W.W3, sw3, n2, lane);
 #pragma unroll
           for (int j = 0; j < TR_C2; ++j) {
             const int i = lane + 32 * j;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
               if (i < n2) {
-                hb2[j][r] += tr_res_adj<T, R>(Gb, net.res3, i, n2, r);
-                const T y2 = A2[i * RS + r] - tr_res<T, R>(A1, net.res2, i, n1, r);
+                hb2[j][r] += tr_res_adj<T, R>(Gb, res3, i, n2, r);
+                const T y2 = A2[i * RS + r] - tr_res<T, R>(A1, res2, i, n1, r);
                 zb2[j][r] = hb2[j][r] * ((T)1 - y2 * y2);
               } else {
                 zb2[j][r] = hb2[j][r] = (T)0;
@@ -731,12 +761,12 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
         __syncwarp();
         {
           T hb1[TR_C1][R];
-          tr_gemvT<T, R, TR_C1>(hb1, Zb2, n2, W.W2, W.s2, n1, lane);
+          tr_gemvT<T, R, TR_C1>(hb1, Zb2, n2, W.W2, sw2, n1, lane);
           if (lane < n1) {
             const T w1 = W.W1[lane];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-              const T h = hb1[0][r] + tr_res_adj<T, R>(Hb2, net.res2, lane, n1, r);
+              const T h = hb1[0][r] + tr_res_adj<T, R>(Hb2, res2, lane, n1, r);
               const T y1 = A1[lane * RS + r];
               part[r * 4] = fma(h * ((T)1 - y1 * y1), w1, part[r * 4]);
             }
@@ -756,7 +786,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
 
 // --------------------------------------------------------------- tangent --
 
-template <typename T, int R>
+template <typename T, int R, int N1, int N2, int N3>
 __global__ void __launch_bounds__(256, 1)
 k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__ xyz,
          const T* __restrict__ avg, const T* __restrict__ std_, const double* __restrict__ fbar,
@@ -765,7 +795,7 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
-  if (lay.wsmem) tr_stage_weights(sw, net, lay, g.ntypes);
+  if (TrTraits<T>::WSMEM) tr_stage_weights(sw, net, lay, g.ntypes);
   __syncthreads();
   int* ints;
   T* ws = tr_warp_base<T>(smem_raw, lay, w, ints);
@@ -774,7 +804,12 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
   T *rr = ws + lay.o_rr, *rd = ws + lay.o_rd, *ss = ws + lay.o_s, *sd = ws + lay.o_sd;
   T *A1 = ws + lay.o_A1, *At1 = ws + lay.o_At1, *A2 = ws + lay.o_A2, *At2 = ws + lay.o_At2;
   T* big = ws + lay.o_big;
-  const int n1 = net.n1, n2 = net.n2, n3 = net.n3;
+  // compile-time widths when N1 > 0 (the standard [25, 50, 100] net), else runtime
+  constexpr bool WS = TrTraits<T>::WSMEM;
+  const int n1 = N1 > 0 ? N1 : net.n1, n2 = N1 > 0 ? N2 : net.n2, n3 = N1 > 0 ? N3 : net.n3;
+  const int res2 = N1 > 0 ? tr_res_kind(N2, N1) : net.res2;
+  const int res3 = N1 > 0 ? tr_res_kind(N3, N2) : net.res3;
+  const int sw2 = WS ? (n2 | 1) : n2, sw3 = WS ? (n3 | 1) : n3;
   const int gw = gridDim.x * lay.nw;
   for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
     const TrAtom A = tr_atom(g, row);
@@ -787,7 +822,7 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
 #pragma unroll
       for (int j = 0; j < TR_C3; ++j) xd[a][j] = (T)0;
     for (int t = 0; t < g.ntypes; ++t) {
-      const WV<T> W = tr_wview(net, lay, sw, t);
+      const WV<T> W = tr_wview<T, WS>(net, sw, t, lay.pw, n1, n2, sw2, sw3);
       for (int e0 = secn[t]; e0 < secn[t + 1]; e0 += R) {
         const int ne = min(R, secn[t + 1] - e0);
         if (lane < R) {
@@ -815,7 +850,7 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
         __syncwarp();
         {
           T acc[TR_C2][R], acd[TR_C2][R];
-          tr_gemv2<T, R, TR_C2>(acc, acd, A1, At1, n1, W.W2, W.s2, n2, lane);
+          tr_gemv2<T, R, TR_C2>(acc, acd, A1, At1, n1, W.W2, sw2, n2, lane);
 #pragma unroll
           for (int j = 0; j < TR_C2; ++j) {
             const int c = lane + 32 * j;
@@ -824,9 +859,9 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                A2[c * RS + r] = y + tr_res<T, R>(A1, net.res2, c, n1, r);
+                A2[c * RS + r] = y + tr_res<T, R>(A1, res2, c, n1, r);
                 At2[c * RS + r] =
-                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, net.res2, c, n1, r);
+                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, res2, c, n1, r);
               }
             }
           }
@@ -834,7 +869,7 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
         __syncwarp();
         {
           T acc[TR_C3][R], acd[TR_C3][R];
-          tr_gemv2<T, R, TR_C3>(acc, acd, A2, At2, n2, W.W3, W.s3, n3, lane);
+          tr_gemv2<T, R, TR_C3>(acc, acd, A2, At2, n2, W.W3, sw3, n3, lane);
 #pragma unroll
           for (int j = 0; j < TR_C3; ++j) {
             const int c = lane + 32 * j;
@@ -843,9 +878,9 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                const T G = y + tr_res<T, R>(A2, net.res3, c, n2, r);
+                const T G = y + tr_res<T, R>(A2, res3, c, n2, r);
                 const T Gd =
-                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At2, net.res3, c, n2, r);
+                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At2, res3, c, n2, r);
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
                   xd[a][j] = fma(rd[r * 4 + a], G, fma(rr[r * 4 + a], Gd, xd[a][j]));
@@ -900,7 +935,7 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
 // copy (plain adds, no atomics); the block sums its warps' copies into the
 // global gradient after each type.
 
-template <typename T, int R>
+template <typename T, int R, int N1, int N2, int N3>
 __global__ void __launch_bounds__(256, 1)
 k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard,
          const T* __restrict__ avg, const T* __restrict__ std_, const double* __restrict__ fbar,
@@ -918,8 +953,13 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
     *sd = ws + lay.o_sd;
   T *A1 = ws + lay.o_A1, *At1 = ws + lay.o_At1, *A2 = ws + lay.o_A2, *At2 = ws + lay.o_At2,
     *Zt2 = ws + lay.o_Zt2, *big = ws + lay.o_big;
-  const int n1 = net.n1, n2 = net.n2, n3 = net.n3;
-  const int s2 = lay.s2, s3 = lay.s3;
+  // compile-time widths when N1 > 0 (the standard [25, 50, 100] net), else runtime
+  constexpr bool WS = TrTraits<T>::WSMEM;
+  const int n1 = N1 > 0 ? N1 : net.n1, n2 = N1 > 0 ? N2 : net.n2, n3 = N1 > 0 ? N3 : net.n3;
+  const int res2 = N1 > 0 ? tr_res_kind(N2, N1) : net.res2;
+  const int res3 = N1 > 0 ? tr_res_kind(N3, N2) : net.res3;
+  const int sw2 = WS ? (n2 | 1) : n2, sw3 = WS ? (n3 | 1) : n3;
+  const int s2 = n2 | 1, s3 = n3 | 1;  // gradient copies: the staged layout
   T* gacc = tb + lay.acc_off + (size_t)w * lay.pw;  // this warp's gradient copy
   T* gW1 = gacc;
   T* gb1 = gW1 + n1;
@@ -930,7 +970,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
   const int gw = gridDim.x * lay.nw;
   for (int t = 0; t < g.ntypes; ++t) {
     __syncthreads();
-    if (lay.wsmem) {
+    if (WS) {
       TrNet<T> one = net;
       one.W[0][0] = net.W[t][0];
       one.W[0][1] = net.W[t][1];
@@ -942,7 +982,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
     }
     for (int e = lane; e < lay.pw; e += 32) gacc[e] = (T)0;
     __syncthreads();
-    WV<T> W = tr_wview(net, lay, sw, lay.wsmem ? 0 : t);
+    const WV<T> W = tr_wview<T, WS>(net, sw, WS ? 0 : t, lay.pw, n1, n2, sw2, sw3);
     for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
       const TrAtom A = tr_atom(g, row);
       const T* av = avg + (size_t)A.ti * g.nnei * 4;
@@ -985,7 +1025,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
         __syncwarp();
         {
           T acc[TR_C2][R], acd[TR_C2][R];
-          tr_gemv2<T, R, TR_C2>(acc, acd, A1, At1, n1, W.W2, W.s2, n2, lane);
+          tr_gemv2<T, R, TR_C2>(acc, acd, A1, At1, n1, W.W2, sw2, n2, lane);
 #pragma unroll
           for (int j = 0; j < TR_C2; ++j) {
             const int c = lane + 32 * j;
@@ -994,9 +1034,9 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                A2[c * RS + r] = y + tr_res<T, R>(A1, net.res2, c, n1, r);
+                A2[c * RS + r] = y + tr_res<T, R>(A1, res2, c, n1, r);
                 At2[c * RS + r] =
-                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, net.res2, c, n1, r);
+                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, res2, c, n1, r);
                 Zt2[c * RS + r] = acd[j][r];
               }
             }
@@ -1010,7 +1050,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
         T* Gbt = big + 3 * n3 * RS;
         {
           T acc[TR_C3][R], acd[TR_C3][R];
-          tr_gemv2<T, R, TR_C3>(acc, acd, A2, At2, n2, W.W3, W.s3, n3, lane);
+          tr_gemv2<T, R, TR_C3>(acc, acd, A2, At2, n2, W.W3, sw3, n3, lane);
 #pragma unroll
           for (int j = 0; j < TR_C3; ++j) {
             const int c = lane + 32 * j;
@@ -1062,7 +1102,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
         __syncwarp();
         // layer 2 adjoints, lanes over layer-2 channels
         T zb2[TR_C2][R], zbd2[TR_C2][R], hb2[TR_C2][R], hbd2[TR_C2][R];
-        tr_gemvT2<T, R, TR_C2>(hb2, hbd2, Zb3, Zbt3, n3, W.W3, W.s3, n2, lane);
+        tr_gemvT2<T, R, TR_C2>(hb2, hbd2, Zb3, Zbt3, n3, W.W3, sw3, n2, lane);
 #pragma unroll
         for (int j = 0; j < TR_C2; ++j) {
           const int i = lane + 32 * j;
@@ -1070,9 +1110,9 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             if (i < n2) {
-              hb2[j][r] += tr_res_adj<T, R>(Gb, net.res3, i, n2, r);
-              hbd2[j][r] += tr_res_adj<T, R>(Gbt, net.res3, i, n2, r);
-              const T y = A2[i * RS + r] - tr_res<T, R>(A1, net.res2, i, n1, r);
+              hb2[j][r] += tr_res_adj<T, R>(Gb, res3, i, n2, r);
+              hbd2[j][r] += tr_res_adj<T, R>(Gbt, res3, i, n2, r);
+              const T y = A2[i * RS + r] - tr_res<T, R>(A1, res2, i, n1, r);
               const T q = (T)1 - y * y;
               zbd2[j][r] = hbd2[j][r] * q;
               zb2[j][r] = (hb2[j][r] - (T)2 * y * Zt2[i * RS + r] * hbd2[j][r]) * q;
@@ -1119,14 +1159,14 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
         // layer 1, lanes over its channels
         {
           T hb1[TR_C1][R], hbd1[TR_C1][R];
-          tr_gemvT2<T, R, TR_C1>(hb1, hbd1, Zb2, Zbd2, n2, W.W2, W.s2, n1, lane);
+          tr_gemvT2<T, R, TR_C1>(hb1, hbd1, Zb2, Zbd2, n2, W.W2, sw2, n1, lane);
           if (lane < n1) {
             const T w1 = W.W1[lane];
             T gws = (T)0, gbs = (T)0;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-              const T h = hb1[0][r] + tr_res_adj<T, R>(Hb2, net.res2, lane, n1, r);
-              const T hd = hbd1[0][r] + tr_res_adj<T, R>(Hbd2, net.res2, lane, n1, r);
+              const T h = hb1[0][r] + tr_res_adj<T, R>(Hb2, res2, lane, n1, r);
+              const T hd = hbd1[0][r] + tr_res_adj<T, R>(Hbd2, res2, lane, n1, r);
               const T y = A1[lane * RS + r];
               const T q = (T)1 - y * y;
               const T zd = sd[r] * w1;
@@ -1423,18 +1463,12 @@ static size_t tr_smem_bytes(const TrLayout& L, size_t tsize) {
   return ib + ((size_t)L.warp_off + (size_t)L.nw * L.warp_sz) * tsize;
 }
 
+// the standard embedding (1 -> 25 -> 50 -> 100, deepmd/dpmodel/descriptor/se_e2_a.py
+// defaults) runs a build with compile-time widths; other widths the generic one
 template <typename T>
-struct TrTraits;
-template <>
-struct TrTraits<float> {
-  static constexpr int R = 8;
-  static constexpr bool WSMEM = true;
-};
-template <>
-struct TrTraits<double> {
-  static constexpr int R = 4;
-  static constexpr bool WSMEM = false;
-};
+static bool tr_std_net(const TrNet<T>& net) {
+  return net.n1 == 25 && net.n2 == 50 && net.n3 == 100;
+}
 
 template <typename T>
 static int tr_net(TrNet<T>& net, const T* const* W, const T* const* b, const int* widths,
@@ -1593,7 +1627,8 @@ using namespace dpb;
       set_error("se_a_train_fwd: null buffer");                                                 \
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
-    auto kern = k_tr_fwd<T, TrTraits<T>::R>;                                                    \
+    auto kern = tr_std_net(net) ? k_tr_fwd<T, TrTraits<T>::R, 25, 50, 100>              \
+                                : k_tr_fwd<T, TrTraits<T>::R, 0, 0, 0>;                         \
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1625,7 +1660,8 @@ using namespace dpb;
     rc = tr_xbar<T>(scratch, nullptr, xyz, nullptr, d_descrpt, nullptr, drow, nrows, net.n3,    \
                     axis, g.nnei, st);                                                          \
     if (rc) return rc;                                                                          \
-    auto kern = k_tr_bwd<T, TrTraits<T>::R>;                                                    \
+    auto kern = tr_std_net(net) ? k_tr_bwd<T, TrTraits<T>::R, 25, 50, 100>              \
+                                : k_tr_bwd<T, TrTraits<T>::R, 0, 0, 0>;                         \
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1655,7 +1691,8 @@ using namespace dpb;
       set_error("se_a_train_tan: null buffer");                                                 \
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
-    auto kern = k_tr_tan<T, TrTraits<T>::R>;                                                    \
+    auto kern = tr_std_net(net) ? k_tr_tan<T, TrTraits<T>::R, 25, 50, 100>              \
+                                : k_tr_tan<T, TrTraits<T>::R, 0, 0, 0>;                         \
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1704,7 +1741,8 @@ using namespace dpb;
     rc = tr_xbar<T>(xb, xbd, xyz, xyz_t, d_descrpt, d_descrpt_t, drow, nrows, net.n3, axis,     \
                     g.nnei, st);                                                                \
     if (rc) return rc;                                                                          \
-    auto kern = k_tr_rev<T, TrTraits<T>::R>;                                                    \
+    auto kern = tr_std_net(net) ? k_tr_rev<T, TrTraits<T>::R, 25, 50, 100>              \
+                                : k_tr_rev<T, TrTraits<T>::R, 0, 0, 0>;                         \
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
