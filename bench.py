@@ -264,7 +264,11 @@ def run_batched(args) -> None:
     ev = bt.BatchEvaluator(params, frames, device=device)
     ev.compute()
     ev.check()
-    ev.capture()
+    # tile shapes (atoms per CTA of the env / force and descriptor kernels,
+    # fitting GEMM N tile) timed on this workload; leaves the step captured
+    tuned = ev.tune(reps=5, use_cache=False) if not args.no_tune else None
+    if tuned is None:
+        ev.capture()
     N = ev.N
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
     clocks = ClockSampler(0)
@@ -314,7 +318,10 @@ def run_batched(args) -> None:
                        "sel": list(cfg.sel), "embedding": list(cfg.neuron),
                        "fitting": list(cfg.fitting), "graph": "one CUDA graph per step",
                        "l2": "256 MiB buffer written between timed steps"},
-            "clocks": clk, "checks_vs_fp64_plain": checks}
+            "clocks": clk, "checks_vs_fp64_plain": checks,
+            "autotune": None if tuned is None else {
+                "knobs": tuned["knobs"], "tuned_ms": tuned["ms"],
+                "default_shapes_ms": tuned["baseline_ms"], "trials": len(tuned["history"])}}
     print(json.dumps(line), flush=True)
 
 
@@ -421,6 +428,10 @@ def run_train(args) -> None:
         return float(np.mean([a.elapsed_time(b) for a, b in ts]))
 
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    tuned = None
+    if not args.no_tune:
+        t32._set_step_scalars(lr, 0.9, 0.999)
+        tuned = t32.tune(reps=5, use_cache=False)
     clocks = ClockSampler(0)
     clocks.start()
     ms = timed(t32, args.steps, flush)
@@ -486,7 +497,10 @@ def run_train(args) -> None:
             "fp64_step": {"value": ms64 * 1e3 / N, "ms_per_step": ms64,
                           "speedup_of_f32": ms64 / ms},
             "grad_rel_err_f32_vs_f64": grad_rel,
-            "stages_ms": stages, "clocks": clk, "cpu_baseline": cpu}
+            "stages_ms": stages, "clocks": clk, "cpu_baseline": cpu,
+            "autotune": None if tuned is None else {
+                "knobs": tuned["knobs"], "tuned_ms": tuned["ms"],
+                "default_shapes_ms": tuned["baseline_ms"], "trials": len(tuned["history"])}}
     print(json.dumps(line), flush=True)
 
 
@@ -750,6 +764,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the tile-shape autotuner (batched and train workloads)")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the FP64 plain path (smaller device footprint for profiling)")
     ap.add_argument("--workload", choices=["step", "repeated", "batched", "train"],

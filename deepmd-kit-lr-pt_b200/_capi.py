@@ -127,6 +127,8 @@ _TRAIN = {
 for _name, _spec in _TRAIN.items():
     for _suf in ("f32", "f64"):
         _FUNCS[f"{_name}_{_suf}"] = _spec
+_FUNCS.update({"dpb_tune_count": "", "dpb_tune_get": "p", "dpb_tune_options": "ppi",
+               "dpb_tune_set": "pi"})
 _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),
     "dpb_cell_grid_bytes": ("i", LL),
@@ -157,6 +159,8 @@ def lib() -> ctypes.CDLL:
         f.argtypes = [_SPEC[c] for c in spec]
         f.restype = rt
     L.dpb_last_error.restype = ctypes.c_char_p
+    L.dpb_tune_name.argtypes = [I]
+    L.dpb_tune_name.restype = ctypes.c_char_p
     L.dpb_abi_version.restype = I
     _lib = L
     return L
@@ -193,4 +197,4 @@ def ptr(x) -> int | None:
 
 def exported_symbols() -> list[str]:
     return sorted(list(_FUNCS) + list(_SIZE_QUERIES) +
-                  ["dpb_last_error", "dpb_abi_version"])
+                  ["dpb_last_error", "dpb_abi_version", "dpb_tune_name"])

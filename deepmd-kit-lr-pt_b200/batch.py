@@ -205,3 +205,16 @@ class BatchEvaluator:
 
     def frame_slice(self, f: int) -> slice:
         return slice(int(self.atom_off_h[f]), int(self.atom_off_h[f + 1]))
+
+    def tune(self, reps: int = 10, use_cache: bool = True) -> dict:
+        """Autotune the tile shapes of this step (atoms per CTA of the env /
+        force and descriptor kernels, fitting GEMM N tile) on its own frames;
+        leaves the step captured with the fastest shapes."""
+        from . import autotune
+
+        cfg = self.cfg
+        sig = (f"batch:{self.nframes}f:{self.N}a:sel{'-'.join(map(str, cfg.sel))}:"
+               f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
+        return autotune.tune(self.replay, lambda: self.capture(),
+                             ["batch_atoms_per_cta", "desc_atoms_per_cta", "fit_n_tile"],
+                             signature=sig, reps=reps, device=self.dev, use_cache=use_cache)

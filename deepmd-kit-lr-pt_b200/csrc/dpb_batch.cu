@@ -72,16 +72,16 @@ struct BtEnvSmem {
   int tcnt[32];
 };
 
-template <typename ET>
-__global__ void __launch_bounds__(BT_WARPS * 32)
+template <typename ET, int WP>
+__global__ void __launch_bounds__(WP * 32)
 k_bt_env(ET* __restrict__ em, int* __restrict__ nlist, const double* __restrict__ cw,
          const int* __restrict__ type, const int* __restrict__ cell_of,
          const int* __restrict__ cell_start, const int* __restrict__ cell_atoms,
          const ET* __restrict__ avg, const ET* __restrict__ std_, BtFrames fr, BtSec sec,
          int nrows, float rcut, float rcut_smth, int* status) {
-  __shared__ BtEnvSmem smem[BT_WARPS];
+  __shared__ BtEnvSmem smem[WP];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = blockIdx.x * BT_WARPS + w;
+  const int row = blockIdx.x * WP + w;
   if (row >= nrows) return;
   BtEnvSmem& sm = smem[w];
   const int f = fr.row_frame[row];
@@ -206,15 +206,15 @@ k_bt_env(ET* __restrict__ em, int* __restrict__ nlist, const double* __restrict_
   }
 }
 
-template <typename ET>
-__global__ void __launch_bounds__(BT_WARPS * 32)
+template <typename ET, int WP>
+__global__ void __launch_bounds__(WP * 32)
 k_bt_force(double* __restrict__ force, double* __restrict__ virial,
            const ET* __restrict__ nd, const double* __restrict__ cw,
            const int* __restrict__ type, const ET* __restrict__ std_,
            const int* __restrict__ nlist, BtFrames fr, int ntypes, int nnei, int nrows,
            float rcut, float rcut_smth) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = blockIdx.x * BT_WARPS + w;
+  const int row = blockIdx.x * WP + w;
   if (row >= nrows) return;
   const int f = fr.row_frame[row];
   const int a0 = fr.atom_off[f];
@@ -319,11 +319,18 @@ static int batch_env(ET* em, int* nlist, double* cw, int* cell_of, int* cell_sta
   cudaStream_t st = as_stream(stream);
   k_bt_cells<<<nframes, 256, 0, st>>>(cw, cell_of, cell_start, cell_atoms, coord, fr);
   DPB_CHECK_LAUNCH("batch_env_mat_a/cells");
-  k_bt_env<ET><<<ceil_div(nrows, BT_WARPS), BT_WARPS * 32, 0, st>>>(
-      em, nlist, cw, type, cell_of, cell_start, cell_atoms, avg, std_, fr, s, nrows, rcut,
-      rcut_smth, status);
-  DPB_CHECK_LAUNCH("batch_env_mat_a/env");
-  return DPB_OK;
+  auto run = [&](auto kern, int wp) -> int {
+    kern<<<ceil_div(nrows, wp), wp * 32, 0, st>>>(em, nlist, cw, type, cell_of, cell_start,
+                                                 cell_atoms, avg, std_, fr, s, nrows, rcut,
+                                                 rcut_smth, status);
+    DPB_CHECK_LAUNCH("batch_env_mat_a/env");
+    return DPB_OK;
+  };
+  switch (tune_value("batch_atoms_per_cta", BT_WARPS)) {
+    case 2: return run(k_bt_env<ET, 2>, 2);
+    case 8: return run(k_bt_env<ET, 8>, 8);
+    default: return run(k_bt_env<ET, 4>, 4);
+  }
 }
 
 template <typename ET>
@@ -340,11 +347,18 @@ static int batch_force(double* force, double* virial, const ET* net_deriv, const
   DPB_CUDA(cudaMemsetAsync(virial, 0, sizeof(double) * 9 * (size_t)nframes, st),
            "batch_force");
   if (nrows <= 0 || nnei <= 0) return DPB_OK;
-  k_bt_force<ET><<<ceil_div(nrows, BT_WARPS), BT_WARPS * 32, 0, st>>>(
-      force, virial, net_deriv, cw, type, std_, nlist, fr, ntypes, nnei, nrows, rcut,
-      rcut_smth);
-  DPB_CHECK_LAUNCH("batch_force_virial_a");
-  return DPB_OK;
+  auto run = [&](auto kern, int wp) -> int {
+    kern<<<ceil_div(nrows, wp), wp * 32, 0, st>>>(force, virial, net_deriv, cw, type, std_,
+                                                 nlist, fr, ntypes, nnei, nrows, rcut,
+                                                 rcut_smth);
+    DPB_CHECK_LAUNCH("batch_force_virial_a");
+    return DPB_OK;
+  };
+  switch (tune_value("batch_atoms_per_cta", BT_WARPS)) {
+    case 2: return run(k_bt_force<ET, 2>, 2);
+    case 8: return run(k_bt_force<ET, 8>, 8);
+    default: return run(k_bt_force<ET, 4>, 4);
+  }
 }
 
 template <typename ET>

@@ -25,6 +25,8 @@ enum : int {
 };
 
 void set_error(const char* fmt, ...);
+// current value of a tile-shape knob (csrc/dpb_tune.cc), fallback if unknown
+int tune_value(const char* name, int fallback);
 int cuda_status(cudaError_t e, const char* where);
 
 inline cudaStream_t as_stream(dpb_stream_t s) {

@@ -10,7 +10,8 @@
 // dropped), accumulated in FP32 in tensor memory.
 //
 // Persistent, warp-specialised CTA (one per SM) walking output tiles of 128
-// rows x BN columns (BN = 160 when it divides N, else 80):
+// rows x BN columns (BN = 160 when it divides N and the fit_n_tile knob allows it,
+// else 80):
 //   warp 0      TMA producer: A tile 128 x 32 and B hi/lo tiles BN x 32 per
 //               k-block into a STAGES-deep shared-memory ring (128-byte
 //               swizzle);
@@ -601,7 +602,9 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
     set_error("gemm_tf32x3: N=%d must be a multiple of 80", N);
     return DPB_ERR_INVALID;
   }
-  const int BN = N % CfgN160::BN == 0 ? CfgN160::BN : CfgN80::BN;
+  const int BN = (N % CfgN160::BN == 0 && tune_value("fit_n_tile", CfgN160::BN) == CfgN160::BN)
+                     ? CfgN160::BN
+                     : CfgN80::BN;
   GemmMaps maps;
   GemmShape shp;
   shp.ntypes = ntypes;

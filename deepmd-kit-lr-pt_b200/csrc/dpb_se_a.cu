@@ -209,13 +209,15 @@ __device__ __forceinline__ void write_descriptor(float* __restrict__ Dr, const f
   }
 }
 
-__global__ void __launch_bounds__(SW * 32, 5)
+// SWT warps (one center atom each) per CTA, about 20 warps per SM
+template <int SWT>
+__global__ void __launch_bounds__(SWT * 32, 20 / SWT)
 k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
            const int* __restrict__ drow, const float* __restrict__ em,
            TypeTables tt, int nloc, int M, int naxis, float inv_nnei, int warp_floats) {
   extern __shared__ float4 dsm4[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * SW + w;
+  const int i = blockIdx.x * SWT + w;
   if (i >= nloc) return;
   const int nnei = tt.nnei;
   float* wsm = reinterpret_cast<float*>(dsm4) + (size_t)w * warp_floats;
@@ -305,14 +307,15 @@ __device__ __forceinline__ void bwd_slot(float (&P)[5], const Coef4& c, const fl
   }
 }
 
-__global__ void __launch_bounds__(SW * 32, 5)
+template <int SWT>
+__global__ void __launch_bounds__(SWT * 32, 20 / SWT)
 k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
            const int* __restrict__ drow, const float* __restrict__ xyz,
            const float* __restrict__ em, TypeTables tt, int nloc, int M, int naxis,
            float inv_nnei, int warp_floats) {
   extern __shared__ float4 dsm4[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * SW + w;
+  const int i = blockIdx.x * SWT + w;
   if (i >= nloc) return;
   const int nnei = tt.nnei;
   float* wsm = reinterpret_cast<float*>(dsm4) + (size_t)w * warp_floats;
@@ -693,16 +696,21 @@ int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_r
   const int M = last_layer_size;
   const float inv = tt.nnei > 0 ? 1.f / (float)tt.nnei : 0.f;
   cudaStream_t st = as_stream(stream);
-  dim3 g(ceil_div(nloc, SW));
   const int wf = (int)fwd_smem_floats(M, tt.nnei);
-  const size_t smem = sizeof(float) * SW * (size_t)wf;
-  DPB_CUDA(cudaFuncSetAttribute(k_desc_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem),
-           "se_a_descriptor_fwd");
-  k_desc_fwd<<<g, SW * 32, smem, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M, axis_neuron,
-                                       inv, wf);
-  DPB_CHECK_LAUNCH("se_a_descriptor_fwd");
-  return DPB_OK;
+  auto run = [&](auto kern, int sw) -> int {
+    const size_t smem = sizeof(float) * sw * (size_t)wf;
+    DPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "se_a_descriptor_fwd");
+    kern<<<ceil_div(nloc, sw), sw * 32, smem, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M,
+                                                   axis_neuron, inv, wf);
+    DPB_CHECK_LAUNCH("se_a_descriptor_fwd");
+    return DPB_OK;
+  };
+  switch (tune_value("desc_atoms_per_cta", SW)) {
+    case 2: return run(k_desc_fwd<2>, 2);
+    case 8: return run(k_desc_fwd<8>, 8);
+    default: return run(k_desc_fwd<4>, 4);
+  }
 }
 
 int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
@@ -721,16 +729,21 @@ int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
   const int M = last_layer_size;
   const float inv = tt.nnei > 0 ? 1.f / (float)tt.nnei : 0.f;
   cudaStream_t st = as_stream(stream);
-  dim3 g(ceil_div(nloc, SW));
   const int wf = (int)bwd_smem_floats(M, tt.nnei, axis_neuron);
-  const size_t smem = sizeof(float) * SW * (size_t)wf;
-  DPB_CUDA(cudaFuncSetAttribute(k_desc_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem),
-           "se_a_descriptor_bwd");
-  k_desc_bwd<<<g, SW * 32, smem, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em, tt, nloc, M,
-                                       axis_neuron, inv, wf);
-  DPB_CHECK_LAUNCH("se_a_descriptor_bwd");
-  return DPB_OK;
+  auto run = [&](auto kern, int sw) -> int {
+    const size_t smem = sizeof(float) * sw * (size_t)wf;
+    DPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "se_a_descriptor_bwd");
+    kern<<<ceil_div(nloc, sw), sw * 32, smem, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em,
+                                                   tt, nloc, M, axis_neuron, inv, wf);
+    DPB_CHECK_LAUNCH("se_a_descriptor_bwd");
+    return DPB_OK;
+  };
+  switch (tune_value("desc_atoms_per_cta", SW)) {
+    case 2: return run(k_desc_bwd<2>, 2);
+    case 8: return run(k_desc_bwd<8>, 8);
+    default: return run(k_desc_bwd<4>, 4);
+  }
 }
 
 int dpb_force_virial_a_env_mixed(double* force, double* virial, const float* net_deriv,

@@ -1554,16 +1554,26 @@ static int tr_launch_cfg(K kernel, const TrLayout& L, size_t tsize, int nrows, i
 }
 
 template <typename T>
-static int tr_pick_warps(TrKind kind, const TrDims& d, int maxw) {
+static int tr_pick_warps(TrKind kind, const TrDims& d, int maxw, int R) {
   for (int nw = maxw; nw >= 1; --nw) {
-    const TrLayout L = tr_layout<T>(kind, TrTraits<T>::R, d, TrTraits<T>::WSMEM, nw);
+    const TrLayout L = tr_layout<T>(kind, R, d, TrTraits<T>::WSMEM, nw);
     if (tr_smem_bytes(L, sizeof(T)) <= 227 * 1024) return nw;
   }
   return 0;
 }
 
+// rows per group: the train_rows_per_group knob for the FP32 standard net,
+// else the precision's default
 template <typename T>
-static int tr_prepare(TrKind kind, TrNet<T>& net, TrGeom& g, TrLayout& L, const T* const* W,
+static int tr_rows(const TrNet<T>& net) {
+  if (sizeof(T) == 4 && tr_std_net(net))
+    return tune_value("train_rows_per_group", TrTraits<T>::R) == 4 ? 4 : 8;
+  return TrTraits<T>::R;
+}
+
+template <typename T>
+static int tr_prepare(TrKind kind, TrNet<T>& net, TrGeom& g, TrLayout& L, int& R,
+                      const T* const* W,
                       const T* const* b, const int* widths, const double* cw, const int* type,
                       const int* nlist, const int* drow, const int* atom_off, const double* box,
                       const int* row_frame, int nframes, int nrows, const int* sec, int nsec,
@@ -1578,12 +1588,14 @@ static int tr_prepare(TrKind kind, TrNet<T>& net, TrGeom& g, TrLayout& L, const 
     return DPB_ERR_INVALID;
   }
   const TrDims d{net.n1, net.n2, net.n3, ax, g.nnei, g.ntypes};
-  const int nw = tr_pick_warps<T>(kind, d, kind == TR_REV ? 4 : 8);
+  R = tr_rows(net);
+  const int maxw = std::min(tune_value("train_warps_per_cta", 8), kind == TR_REV ? 4 : 8);
+  const int nw = tr_pick_warps<T>(kind, d, maxw, R);
   if (nw < 1) {
     set_error("se_a_train: the network does not fit in shared memory");
     return DPB_ERR_INVALID;
   }
-  L = tr_layout<T>(kind, TrTraits<T>::R, d, TrTraits<T>::WSMEM, nw);
+  L = tr_layout<T>(kind, R, d, TrTraits<T>::WSMEM, nw);
   return DPB_OK;
 }
 
@@ -1619,7 +1631,8 @@ using namespace dpb;
     TrNet<T> net;                                                                               \
     TrGeom g;                                                                                   \
     TrLayout L;                                                                                 \
-    int rc = tr_prepare<T>(TR_FWD, net, g, L, W, b, widths, nullptr, type, nlist, drow,         \
+    int R;                                                                                      \
+    int rc = tr_prepare<T>(TR_FWD, net, g, L, R, W, b, widths, nullptr, type, nlist, drow,         \
                            nullptr, nullptr, nullptr, 0, nrows, sec, nsec, axis, fold, 0.f, 0.f); \
     if (rc) return rc;                                                                          \
     if (nrows == 0) return DPB_OK;                                                              \
@@ -1627,8 +1640,8 @@ using namespace dpb;
       set_error("se_a_train_fwd: null buffer");                                                 \
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
-    auto kern = tr_std_net(net) ? k_tr_fwd<T, TrTraits<T>::R, 25, 50, 100>              \
-                                : k_tr_fwd<T, TrTraits<T>::R, 0, 0, 0>;                         \
+    auto kern = !tr_std_net(net) ? k_tr_fwd<T, TrTraits<T>::R, 0, 0, 0>                         \
+                : (R == 4 ? k_tr_fwd<T, 4, 25, 50, 100> : k_tr_fwd<T, TrTraits<T>::R, 25, 50, 100>);\
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1645,7 +1658,8 @@ using namespace dpb;
     TrNet<T> net;                                                                               \
     TrGeom g;                                                                                   \
     TrLayout L;                                                                                 \
-    int rc = tr_prepare<T>(TR_BWD, net, g, L, W, b, widths, nullptr, type, nlist, drow,         \
+    int R;                                                                                      \
+    int rc = tr_prepare<T>(TR_BWD, net, g, L, R, W, b, widths, nullptr, type, nlist, drow,         \
                            nullptr, nullptr, nullptr, 0, nrows, sec, nsec, axis, nullptr, 0.f,  \
                            0.f);                                                                \
     if (rc) return rc;                                                                          \
@@ -1660,8 +1674,8 @@ using namespace dpb;
     rc = tr_xbar<T>(scratch, nullptr, xyz, nullptr, d_descrpt, nullptr, drow, nrows, net.n3,    \
                     axis, g.nnei, st);                                                          \
     if (rc) return rc;                                                                          \
-    auto kern = tr_std_net(net) ? k_tr_bwd<T, TrTraits<T>::R, 25, 50, 100>              \
-                                : k_tr_bwd<T, TrTraits<T>::R, 0, 0, 0>;                         \
+    auto kern = !tr_std_net(net) ? k_tr_bwd<T, TrTraits<T>::R, 0, 0, 0>                         \
+                : (R == 4 ? k_tr_bwd<T, 4, 25, 50, 100> : k_tr_bwd<T, TrTraits<T>::R, 25, 50, 100>);\
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1681,7 +1695,8 @@ using namespace dpb;
     TrNet<T> net;                                                                               \
     TrGeom g;                                                                                   \
     TrLayout L;                                                                                 \
-    int rc = tr_prepare<T>(TR_TAN, net, g, L, W, b, widths, cw, type, nlist, drow, atom_off,    \
+    int R;                                                                                      \
+    int rc = tr_prepare<T>(TR_TAN, net, g, L, R, W, b, widths, cw, type, nlist, drow, atom_off,    \
                            box, row_frame, nframes, nrows, sec, nsec, axis, nullptr, rcut,      \
                            rcut_smth);                                                          \
     if (rc) return rc;                                                                          \
@@ -1691,8 +1706,8 @@ using namespace dpb;
       set_error("se_a_train_tan: null buffer");                                                 \
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
-    auto kern = tr_std_net(net) ? k_tr_tan<T, TrTraits<T>::R, 25, 50, 100>              \
-                                : k_tr_tan<T, TrTraits<T>::R, 0, 0, 0>;                         \
+    auto kern = !tr_std_net(net) ? k_tr_tan<T, TrTraits<T>::R, 0, 0, 0>                         \
+                : (R == 4 ? k_tr_tan<T, 4, 25, 50, 100> : k_tr_tan<T, TrTraits<T>::R, 25, 50, 100>);\
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1715,7 +1730,8 @@ using namespace dpb;
     TrNet<T> net;                                                                               \
     TrGeom g;                                                                                   \
     TrLayout L;                                                                                 \
-    int rc = tr_prepare<T>(TR_REV, net, g, L, W, b, widths, cw, type, nlist, drow, atom_off,    \
+    int R;                                                                                      \
+    int rc = tr_prepare<T>(TR_REV, net, g, L, R, W, b, widths, cw, type, nlist, drow, atom_off,    \
                            box, row_frame, nframes, nrows, sec, nsec, axis, fold, rcut,         \
                            rcut_smth);                                                          \
     if (rc) return rc;                                                                          \
@@ -1741,8 +1757,8 @@ using namespace dpb;
     rc = tr_xbar<T>(xb, xbd, xyz, xyz_t, d_descrpt, d_descrpt_t, drow, nrows, net.n3, axis,     \
                     g.nnei, st);                                                                \
     if (rc) return rc;                                                                          \
-    auto kern = tr_std_net(net) ? k_tr_rev<T, TrTraits<T>::R, 25, 50, 100>              \
-                                : k_tr_rev<T, TrTraits<T>::R, 0, 0, 0>;                         \
+    auto kern = !tr_std_net(net) ? k_tr_rev<T, TrTraits<T>::R, 0, 0, 0>                         \
+                : (R == 4 ? k_tr_rev<T, 4, 25, 50, 100> : k_tr_rev<T, TrTraits<T>::R, 25, 50, 100>);\
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \

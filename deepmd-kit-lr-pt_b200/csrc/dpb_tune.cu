@@ -1,0 +1,84 @@
+// Tile-shape knobs read by the launchers (atoms per CTA, rows per group,
+// GEMM N tile). Process-wide values, set by the autotuner (autotune.py) or
+// the caller before a step is launched or captured; a captured CUDA graph
+// keeps the shapes it was captured with.
+#include <cstring>
+
+#include "dpb_common.cuh"
+
+namespace dpb {
+
+struct Knob {
+  const char* name;
+  int value;
+  int nopt;
+  int options[4];
+};
+
+static Knob g_knobs[] = {
+    // warps (one center atom each) per CTA of the fused descriptor kernels
+    {"desc_atoms_per_cta", 4, 3, {2, 4, 8, 0}},
+    // columns per tensor-core tile of the fitting GEMMs (160 only where it
+    // divides N)
+    {"fit_n_tile", 160, 2, {80, 160, 0, 0}},
+    // warps (one center atom each) per CTA of the batched env / force kernels
+    {"batch_atoms_per_cta", 4, 3, {2, 4, 8, 0}},
+    // neighbor rows per group in the FP32 training kernels
+    {"train_rows_per_group", 8, 2, {4, 8, 0, 0}},
+    // most warps per CTA of the training kernels (fewer when shared memory
+    // does not allow them)
+    {"train_warps_per_cta", 8, 4, {1, 2, 4, 8}},
+};
+
+static Knob* find_knob(const char* name) {
+  if (name == nullptr) return nullptr;
+  for (auto& k : g_knobs)
+    if (std::strcmp(k.name, name) == 0) return &k;
+  return nullptr;
+}
+
+int tune_value(const char* name, int fallback) {
+  const Knob* k = find_knob(name);
+  return k ? k->value : fallback;
+}
+
+}  // namespace dpb
+
+using namespace dpb;
+extern "C" {
+
+int dpb_tune_count(void) { return (int)(sizeof(g_knobs) / sizeof(g_knobs[0])); }
+
+const char* dpb_tune_name(int index) {
+  if (index < 0 || index >= dpb_tune_count()) return nullptr;
+  return g_knobs[index].name;
+}
+
+int dpb_tune_get(const char* name) {
+  const Knob* k = find_knob(name);
+  return k ? k->value : -1;
+}
+
+int dpb_tune_options(const char* name, int* out, int capacity) {
+  const Knob* k = find_knob(name);
+  if (k == nullptr) return -1;
+  for (int i = 0; i < k->nopt && i < capacity && out; ++i) out[i] = k->options[i];
+  return k->nopt;
+}
+
+int dpb_tune_set(const char* name, int value) {
+  Knob* k = find_knob(name);
+  if (k == nullptr) {
+    set_error("tune: unknown knob '%s'", name ? name : "(null)");
+    return DPB_ERR_INVALID;
+  }
+  for (int i = 0; i < k->nopt; ++i)
+    if (k->options[i] == value) {
+      k->value = value;
+      return DPB_OK;
+    }
+  set_error("tune: %d is not an option of %s", value, k->name);
+  return DPB_ERR_INVALID;
+}
+
+}  // extern "C"

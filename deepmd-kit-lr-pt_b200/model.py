@@ -709,6 +709,19 @@ class SeAEvaluator:
         torch.cuda.synchronize()
         return self
 
+    def tune(self, reps: int = 10, use_cache: bool = True) -> dict:
+        """Autotune the tile shapes of this step (atoms per CTA of the fused
+        descriptor kernels, fitting GEMM N tile); leaves it captured with the
+        fastest shapes."""
+        from . import autotune
+
+        cfg = self.cfg
+        sig = (f"frame:{self.nloc}a:{self.mode}:sel{'-'.join(map(str, cfg.sel))}:"
+               f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
+        return autotune.tune(self.replay, lambda: self.capture(),
+                             ["desc_atoms_per_cta", "fit_n_tile"], signature=sig, reps=reps,
+                             device=self.dev, use_cache=use_cache)
+
     def replay(self):
         if getattr(self, "_recapture", False):
             self._recapture = False

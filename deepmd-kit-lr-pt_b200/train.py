@@ -522,3 +522,33 @@ class SeATrainer:
         torch.cuda.synchronize(self.dev)
         self._graph_adam = (beta1, beta2, eps)
         return self
+
+    def tune(self, reps: int = 10, use_cache: bool = True) -> dict:
+        """Autotune the training kernels' tile shapes (rows per group, warps
+        per CTA, atoms per CTA of the batched geometry) on this batch with
+        the learning rate held at zero; parameters and Adam moments are
+        restored afterwards and the step is left captured."""
+        from . import autotune
+
+        if self.loss is None or self.labels is None:
+            raise _capi.DPBInvalidArgument("tune needs a loss and labels")
+        saved = (self.flat.detach().clone(), self.adam_m.clone(), self.adam_v.clone(),
+                 self.adam_step)
+        zero = torch.tensor([0.0, 1.0, 1.0], dtype=torch.float64)
+
+        def step():
+            self._hp.copy_(zero)
+            self.graph.replay()
+
+        cfg = self.cfg
+        sig = (f"train:{self.ft.nframes}f:{self.ft.N}a:{self.suf}:"
+               f"sel{'-'.join(map(str, cfg.sel))}:emb{'-'.join(map(str, cfg.neuron))}")
+        res = autotune.tune(step, lambda: self.capture(),
+                            ["train_rows_per_group", "train_warps_per_cta",
+                             "batch_atoms_per_cta"],
+                            signature=sig, reps=reps, device=self.dev, use_cache=use_cache)
+        self.flat.detach().copy_(saved[0])
+        self.adam_m.copy_(saved[1])
+        self.adam_v.copy_(saved[2])
+        self.adam_step = saved[3]
+        return res

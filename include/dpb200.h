@@ -616,6 +616,21 @@ DPB_API int dpb_adam_f64(double* p, const double* g, double* m, double* v, long 
                          dpb_stream_t stream);
 
 
+/* ------------------------------------------------- tile-shape knobs ---- */
+/* No counterpart in the reference (its kernels have fixed launch shapes).
+ * Process-wide knobs read when a launcher runs (a captured CUDA graph keeps
+ * the shapes it was captured with): desc_atoms_per_cta {2, 4, 8} (fused
+ * descriptor kernels), fit_n_tile {80, 160} (fitting GEMM N tile, 160 only
+ * where it divides N), batch_atoms_per_cta {2, 4, 8} (batched env / force),
+ * train_rows_per_group {4, 8} (FP32 training kernels, standard net),
+ * train_warps_per_cta {1, 2, 4, 8}. The autotuner (autotune.py) times the
+ * options on the caller's own step and sets the fastest. */
+DPB_API int dpb_tune_count(void);
+DPB_API const char* dpb_tune_name(int index);
+DPB_API int dpb_tune_get(const char* name);
+DPB_API int dpb_tune_options(const char* name, int* out, int capacity);
+DPB_API int dpb_tune_set(const char* name, int value);
+
 /* ------------------------------------------- allocation-free variant ---- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc,
  * e.g. an MD engine's force callback that runs inside the engine's own

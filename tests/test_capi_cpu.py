@@ -84,3 +84,24 @@ def test_cxx_dropin_exports_reference_symbols(dpb):
     have = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
     missing = [s for s in want if s not in have]
     assert len(want) == 18 and not missing, missing
+
+
+def test_tile_knob_registry(dpb):
+    """The tile-shape knobs list their options, accept only those, and read
+    back what was set (no device needed)."""
+    from deepmd_kit_lr_pt_b200 import autotune
+
+    names = autotune.names()
+    assert {"desc_atoms_per_cta", "fit_n_tile", "batch_atoms_per_cta",
+            "train_rows_per_group", "train_warps_per_cta"} <= set(names)
+    for n in names:
+        opts = autotune.options(n)
+        old = autotune.get(n)
+        assert old in opts and len(opts) >= 2
+        autotune.set_knob(n, opts[0])
+        assert autotune.get(n) == opts[0]
+        autotune.set_knob(n, old)
+    with pytest.raises(dpb._capi.DPBInvalidArgument):
+        autotune.set_knob("desc_atoms_per_cta", 3)
+    with pytest.raises(dpb._capi.DPBInvalidArgument):
+        autotune.get("no_such_knob")
