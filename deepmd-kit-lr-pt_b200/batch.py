@@ -216,5 +216,6 @@ class BatchEvaluator:
         sig = (f"batch:{self.nframes}f:{self.N}a:sel{'-'.join(map(str, cfg.sel))}:"
                f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
         return autotune.tune(self.replay, lambda: self.capture(),
-                             ["batch_atoms_per_cta", "desc_atoms_per_cta", "fit_n_tile"],
+                             ["batch_atoms_per_cta", "desc_atoms_per_cta", "desc_coef_l1",
+                              "fit_n_tile"],
                              signature=sig, reps=reps, device=self.dev, use_cache=use_cache)

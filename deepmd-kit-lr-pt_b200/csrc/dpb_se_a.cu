@@ -19,6 +19,8 @@
 // for the per-type fitting networks without a gather.
 #include <math.h>
 
+#include <type_traits>
+
 #include "dpb_common.cuh"
 #include "dpb_envmath.cuh"
 #include "dpb_internal.cuh"
@@ -93,11 +95,31 @@ struct Coef4 {
   float2 hi[6];  // a_k of channels (2, 3)
 };
 
+// 16-byte read-only load of table coefficients with the L1 policy CH:
+// 0 default, 1 L1::no_allocate, 2 L1::evict_first, 3 L1::evict_last
+template <int CH>
+__device__ __forceinline__ float4 ld_coef(const float* p) {
+  float4 v;
+  if (CH == 1)
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  else if (CH == 2)
+    asm("ld.global.nc.L1::evict_first.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  else if (CH == 3)
+    asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  else
+    v = __ldg(reinterpret_cast<const float4*>(p));
+  return v;
+}
+
+template <int CH = 0>
 __device__ __forceinline__ Coef4 load_coef4(const float* row, int M) {
   Coef4 c;
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(row + k * M));
+    const float4 v = ld_coef<CH>(row + k * M);
     c.lo[k] = make_float2(v.x, v.y);
     c.hi[k] = make_float2(v.z, v.w);
   }
@@ -210,7 +232,7 @@ __device__ __forceinline__ void write_descriptor(float* __restrict__ Dr, const f
 }
 
 // SWT warps (one center atom each) per CTA, about 20 warps per SM
-template <int SWT>
+template <int SWT, int CH>
 __global__ void __launch_bounds__(SWT * 32, 20 / SWT)
 k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
            const int* __restrict__ drow, const float* __restrict__ em,
@@ -246,12 +268,12 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
     // the current one is evaluated (reusing a row shared by consecutive slots
     // saves L1 traffic but costs the prefetch distance, a net loss measured
     // on 12k-atom water)
-    Coef4 ca = load_coef4(row(0), M), cb;
+    Coef4 ca = load_coef4<CH>(row(0), M), cb;
     int q = 0;
     for (; q + 1 <= last; q += 2) {
-      cb = load_coef4(row(q + 1), M);
+      cb = load_coef4<CH>(row(q + 1), M);
       fwd_slot(acc01, acc23, ca, E[q], Ls[q], rep(q));
-      if (q + 2 <= last) ca = load_coef4(row(q + 2), M);
+      if (q + 2 <= last) ca = load_coef4<CH>(row(q + 2), M);
       fwd_slot(acc01, acc23, cb, E[q + 1], Ls[q + 1], rep(q + 1));
     }
     if (q <= last) fwd_slot(acc01, acc23, ca, E[q], Ls[q], rep(q));
@@ -307,7 +329,7 @@ __device__ __forceinline__ void bwd_slot(float (&P)[5], const Coef4& c, const fl
   }
 }
 
-template <int SWT>
+template <int SWT, int CH>
 __global__ void __launch_bounds__(SWT * 32, 20 / SWT)
 k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
            const int* __restrict__ drow, const float* __restrict__ xyz,
@@ -402,7 +424,7 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
     // two coefficient buffers in turn (GRP is even, so slot parity fixes the
     // buffer): the next slot's row is in flight while the current one is used
     Coef4 ca, cb;
-    if (act) ca = load_coef4(row(0), M);
+    if (act) ca = load_coef4<CH>(row(0), M);
     for (int g0 = 0; g0 < nt; g0 += GRP) {
       if (g0 > last) {  // beyond the fold point: zero rows
         for (int qq = g0 + lane; qq < nt && qq < g0 + GRP; qq += 32)
@@ -417,10 +439,10 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
         const int qq = g0 + q;
         if (qq <= last && act) {  // warp-uniform apart from the idle lanes
           if ((q & 1) == 0) {
-            if (qq + 1 <= last) cb = load_coef4(row(qq + 1), M);
+            if (qq + 1 <= last) cb = load_coef4<CH>(row(qq + 1), M);
             bwd_slot(P[q], ca, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
           } else {
-            if (qq + 1 <= last) ca = load_coef4(row(qq + 1), M);
+            if (qq + 1 <= last) ca = load_coef4<CH>(row(qq + 1), M);
             bwd_slot(P[q], cb, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
           }
         }
@@ -706,10 +728,20 @@ int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_r
     DPB_CHECK_LAUNCH("se_a_descriptor_fwd");
     return DPB_OK;
   };
+  const int ch = tune_value("desc_coef_l1", 3);
+  auto pick = [&](auto sw_tag) -> int {
+    constexpr int SWV = decltype(sw_tag)::value;
+    switch (ch) {
+      case 1: return run(k_desc_fwd<SWV, 1>, SWV);
+      case 2: return run(k_desc_fwd<SWV, 2>, SWV);
+      case 3: return run(k_desc_fwd<SWV, 3>, SWV);
+      default: return run(k_desc_fwd<SWV, 0>, SWV);
+    }
+  };
   switch (tune_value("desc_atoms_per_cta", SW)) {
-    case 2: return run(k_desc_fwd<2>, 2);
-    case 8: return run(k_desc_fwd<8>, 8);
-    default: return run(k_desc_fwd<4>, 4);
+    case 2: return pick(std::integral_constant<int, 2>{});
+    case 8: return pick(std::integral_constant<int, 8>{});
+    default: return pick(std::integral_constant<int, 4>{});
   }
 }
 
@@ -739,10 +771,20 @@ int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
     DPB_CHECK_LAUNCH("se_a_descriptor_bwd");
     return DPB_OK;
   };
+  const int ch = tune_value("desc_coef_l1", 3);
+  auto pick = [&](auto sw_tag) -> int {
+    constexpr int SWV = decltype(sw_tag)::value;
+    switch (ch) {
+      case 1: return run(k_desc_bwd<SWV, 1>, SWV);
+      case 2: return run(k_desc_bwd<SWV, 2>, SWV);
+      case 3: return run(k_desc_bwd<SWV, 3>, SWV);
+      default: return run(k_desc_bwd<SWV, 0>, SWV);
+    }
+  };
   switch (tune_value("desc_atoms_per_cta", SW)) {
-    case 2: return run(k_desc_bwd<2>, 2);
-    case 8: return run(k_desc_bwd<8>, 8);
-    default: return run(k_desc_bwd<4>, 4);
+    case 2: return pick(std::integral_constant<int, 2>{});
+    case 8: return pick(std::integral_constant<int, 8>{});
+    default: return pick(std::integral_constant<int, 4>{});
   }
 }
 

@@ -18,6 +18,10 @@ struct Knob {
 static Knob g_knobs[] = {
     // warps (one center atom each) per CTA of the fused descriptor kernels
     {"desc_atoms_per_cta", 4, 3, {2, 4, 8, 0}},
+    // L1 policy of the table-coefficient loads in the fused descriptor
+    // kernels: 0 default, 1 no_allocate, 2 evict_first, 3 evict_last (measured
+    // fastest on 12,288-atom water: rows near the switch cutoff are shared)
+    {"desc_coef_l1", 3, 4, {0, 1, 2, 3}},
     // columns per tensor-core tile of the fitting GEMMs (160 only where it
     // divides N)
     {"fit_n_tile", 160, 2, {80, 160, 0, 0}},

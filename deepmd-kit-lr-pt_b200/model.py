@@ -719,7 +719,7 @@ class SeAEvaluator:
         sig = (f"frame:{self.nloc}a:{self.mode}:sel{'-'.join(map(str, cfg.sel))}:"
                f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
         return autotune.tune(self.replay, lambda: self.capture(),
-                             ["desc_atoms_per_cta", "fit_n_tile"], signature=sig, reps=reps,
+                             ["desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile"], signature=sig, reps=reps,
                              device=self.dev, use_cache=use_cache)
 
     def replay(self):
