@@ -95,12 +95,43 @@ struct Coef4 {
   float2 hi[6];  // a_k of channels (2, 3)
 };
 
+// L2 cache policies: evict_first for data read once per step (env rows, x,
+// dE/dD), evict_last for the table coefficients reused by every atom
+__device__ __forceinline__ unsigned long long l2_policy_first() {
+  unsigned long long p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long l2_policy_last() {
+  unsigned long long p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// streaming read: not allocated in L1 (keeps L1 for the table rows), first
+// out of L2
+__device__ __forceinline__ float4 ld_stream4(const float4* p, unsigned long long pol) {
+  float4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p, unsigned long long pol) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 // 16-byte read-only load of table coefficients with the L1 policy CH:
-// 0 default, 1 L1::no_allocate, 2 L1::evict_first, 3 L1::evict_last
+// 0 default, 1 L1::no_allocate, 2 L1::evict_first, 3 L1::evict_last,
+// 4 L1::evict_last with the L2 evict_last policy
 template <int CH>
 __device__ __forceinline__ float4 ld_coef(const float* p) {
   float4 v;
-  if (CH == 1)
+  if (CH == 4)
+    asm("ld.global.nc.L1::evict_last.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(l2_policy_last()));
+  else if (CH == 1)
     asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
         : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
   else if (CH == 2)
@@ -161,10 +192,11 @@ __device__ __forceinline__ void hvalgrad2(const float2 (&c)[6], float2 x, float2
 // slot, lane-parallel, so the channel loops only wait on coefficient loads.
 __device__ __forceinline__ void stage_slots(float4* se, float4* sl, const float4* erow,
                                             const TypeTables& tt, int lane) {
+  const unsigned long long pol = l2_policy_first();
   for (int t = 0; t < tt.ntypes; ++t) {
     const FTab inf = tt.info[t];
     for (int s = tt.sec[t] + lane; s < tt.sec[t + 1]; s += 32) {
-      const float4 e = erow[s];
+      const float4 e = ld_stream4(erow + s, pol);
       int idx;
       float xx, delta;
       flocate(inf, e.x, idx, xx, delta);
@@ -345,16 +377,17 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
   float* s_t = s_x + 4 * M;        // [4][naxis]
   float* s_d = s_t + 4 * MAXAX;    // [M][naxis + 1], later the slot staging
   const float* xi = xyz + (size_t)i * 4 * M;
-  for (int q = lane; q < 4 * M; q += 32) s_x[q] = xi[q];
+  const unsigned long long pol = l2_policy_first();
+  for (int q = lane; q < 4 * M; q += 32) s_x[q] = ld_stream(xi + q, pol);
   const float* dr = dD + (size_t)drow[i] * M * naxis;
   const int ldd = naxis + 1;  // padded row: conflict-free column reads
   if (32 % naxis == 0) {
     const int per = 32 / naxis, a = lane % naxis;
-    for (int m = lane / naxis; m < M; m += per) s_d[m * ldd + a] = dr[m * naxis + a];
+    for (int m = lane / naxis; m < M; m += per) s_d[m * ldd + a] = ld_stream(dr + m * naxis + a, pol);
   } else {
     for (int q = lane; q < M * naxis; q += 32) {
       const int m = q / naxis, a = q - m * naxis;
-      s_d[m * ldd + a] = dr[q];
+      s_d[m * ldd + a] = ld_stream(dr + q, pol);
     }
   }
   __syncwarp();
@@ -735,6 +768,7 @@ int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_r
       case 1: return run(k_desc_fwd<SWV, 1>, SWV);
       case 2: return run(k_desc_fwd<SWV, 2>, SWV);
       case 3: return run(k_desc_fwd<SWV, 3>, SWV);
+      case 4: return run(k_desc_fwd<SWV, 4>, SWV);
       default: return run(k_desc_fwd<SWV, 0>, SWV);
     }
   };
@@ -778,6 +812,7 @@ int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
       case 1: return run(k_desc_bwd<SWV, 1>, SWV);
       case 2: return run(k_desc_bwd<SWV, 2>, SWV);
       case 3: return run(k_desc_bwd<SWV, 3>, SWV);
+      case 4: return run(k_desc_bwd<SWV, 4>, SWV);
       default: return run(k_desc_bwd<SWV, 0>, SWV);
     }
   };

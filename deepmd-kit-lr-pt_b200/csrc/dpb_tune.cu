@@ -12,23 +12,24 @@ struct Knob {
   const char* name;
   int value;
   int nopt;
-  int options[4];
+  int options[6];
 };
 
 static Knob g_knobs[] = {
     // warps (one center atom each) per CTA of the fused descriptor kernels
-    {"desc_atoms_per_cta", 4, 3, {2, 4, 8, 0}},
+    {"desc_atoms_per_cta", 4, 3, {2, 4, 8}},
     // L1 policy of the table-coefficient loads in the fused descriptor
     // kernels: 0 default, 1 no_allocate, 2 evict_first, 3 evict_last (measured
-    // fastest on 12,288-atom water: rows near the switch cutoff are shared)
-    {"desc_coef_l1", 3, 4, {0, 1, 2, 3}},
+    // fastest on 12,288-atom water: rows near the switch cutoff are shared),
+    // 4 evict_last in L1 and L2
+    {"desc_coef_l1", 3, 5, {0, 1, 2, 3, 4}},
     // columns per tensor-core tile of the fitting GEMMs (160 only where it
     // divides N)
-    {"fit_n_tile", 160, 2, {80, 160, 0, 0}},
+    {"fit_n_tile", 160, 2, {80, 160}},
     // warps (one center atom each) per CTA of the batched env / force kernels
-    {"batch_atoms_per_cta", 4, 3, {2, 4, 8, 0}},
+    {"batch_atoms_per_cta", 4, 3, {2, 4, 8}},
     // neighbor rows per group in the FP32 training kernels
-    {"train_rows_per_group", 8, 2, {4, 8, 0, 0}},
+    {"train_rows_per_group", 8, 2, {4, 8}},
     // most warps per CTA of the training kernels (fewer when shared memory
     // does not allow them)
     {"train_warps_per_cta", 8, 4, {1, 2, 4, 8}},

@@ -620,8 +620,9 @@ DPB_API int dpb_adam_f64(double* p, const double* g, double* m, double* v, long 
 /* No counterpart in the reference (its kernels have fixed launch shapes).
  * Process-wide knobs read when a launcher runs (a captured CUDA graph keeps
  * the shapes it was captured with): desc_atoms_per_cta {2, 4, 8} (fused
- * descriptor kernels), desc_coef_l1 {0, 1, 2, 3} (L1 policy of their table
- * loads: default, no_allocate, evict_first, evict_last), fit_n_tile {80, 160} (fitting GEMM N tile, 160 only
+ * descriptor kernels), desc_coef_l1 {0, 1, 2, 3, 4} (cache policy of their
+ * table loads: default, L1 no_allocate, L1 evict_first, L1 evict_last, L1 and L2
+ * evict_last), fit_n_tile {80, 160} (fitting GEMM N tile, 160 only
  * where it divides N), batch_atoms_per_cta {2, 4, 8} (batched env / force),
  * train_rows_per_group {4, 8} (FP32 training kernels, standard net),
  * train_warps_per_cta {1, 2, 4, 8}. The autotuner (autotune.py) times the
