@@ -4,7 +4,8 @@
 //
 //   C[m, n] = sum_k A[m, k] B[n, k]      A: [M, K] FP32 row-major (activations)
 //                                        B: [N, K] FP32 row-major (weights),
-//                                           given pre-split into TF32 hi / lo
+//                                           given pre-split into TF32 hi / lo,
+//                                           or in FP32 and split in the kernel
 // 3xTF32: A = Ah + Al and B = Bh + Bl with Ah, Bh the TF32 roundings; the
 // product is Ah Bh + Al Bh + Ah Bl (the Al Bl term, ~2^-22 relative, is
 // dropped), accumulated in FP32 in tensor memory.
@@ -18,7 +19,8 @@
 //   warps 2-5   split each A tile row by row (one row per thread) into TF32
 //               hi / lo and store both straight into one of ASLOTS tensor-
 //               memory slots, so the MMAs read A from TMEM and only B from
-//               shared memory;
+//               shared memory; with FP32 weights they also split the B tile
+//               in shared memory (half the weight bytes from L2);
 //   warp 1      one elected lane issues tcgen05.mma (M=128, N=BN, K=8) into
 //               one of ACCBUF TMEM accumulators and commits to the ring's,
 //               the A slots' and the accumulator's mbarriers;
@@ -104,6 +106,7 @@ struct GemmShape {
   int tile_start[GT_MAXT + 1];
   int n_tiles;  // column tiles per row tile
   int N, K;
+  int split_b;  // 1: B given in FP32 and split into hi / lo in shared memory
 };
 
 struct GemmMaps {
@@ -306,10 +309,12 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
             break;
           }
           unsigned char* st = smem + s * STAGE_BYTES;
-          mbar_expect_tx(&full_bar[s], A_BYTES + 2 * B_BYTES);
+          mbar_expect_tx(&full_bar[s], A_BYTES + (shp.split_b ? 1 : 2) * B_BYTES);
           tma_load_2d(st, &maps.a, &full_bar[s], kb * GT_BK, tc.row0);
           tma_load_2d(st + A_BYTES, &maps.bh[tc.ty], &full_bar[s], kb * GT_BK, tc.n0);
-          tma_load_2d(st + A_BYTES + B_BYTES, &maps.bl[tc.ty], &full_bar[s], kb * GT_BK, tc.n0);
+          if (!shp.split_b)
+            tma_load_2d(st + A_BYTES + B_BYTES, &maps.bl[tc.ty], &full_bar[s], kb * GT_BK,
+                        tc.n0);
         }
       }
       if (!ok) {
@@ -409,6 +414,30 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
         tmem_st16(ta + 16u, hi + 16);
         tmem_st16(ta + 32u, lo);
         tmem_st16(ta + 48u, lo + 16);
+        if (shp.split_b) {
+          // B arrived in FP32 in the hi buffer: TF32 hi in place, lo into the
+          // lo buffer at the same (swizzled) offset; rows r and r + 128
+          unsigned char* bh = smem + s * STAGE_BYTES + A_BYTES;
+          unsigned char* bl = bh + B_BYTES;
+#pragma unroll
+          for (int rr = 0; rr < (BN + 127) / 128; ++rr) {
+            const int n = r + 128 * rr;
+            if (n < BN) {
+#pragma unroll
+              for (int c = 0; c < 8; ++c) {
+                const int off = n * 128 + ((c ^ (n & 7)) << 4);
+                const float4 x = *reinterpret_cast<const float4*>(bh + off);
+                const float4 h = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z),
+                                             tf32_hi(x.w));
+                *reinterpret_cast<float4*>(bh + off) = h;
+                *reinterpret_cast<float4*>(bl + off) =
+                    make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+              }
+            }
+          }
+          // generic-proxy writes, read next by the tensor cores (async proxy)
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive(&conv_bar[s]);
@@ -624,9 +653,11 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
   if (M == 0) return DPB_OK;
   rc = make_map(&maps.a, A, M, K, GT_BM);
   if (rc) return rc;
+  // b_lo == NULL: b_hi holds the FP32 weights, split in the kernel
+  shp.split_b = b_lo == nullptr ? 1 : 0;
   for (int t = 0; t < ntypes; ++t) {
     if ((rc = make_map(&maps.bh[t], b_hi[t], N, K, BN))) return rc;
-    if ((rc = make_map(&maps.bl[t], b_lo[t], N, K, BN))) return rc;
+    if ((rc = make_map(&maps.bl[t], shp.split_b ? b_hi[t] : b_lo[t], N, K, BN))) return rc;
   }
   auto misaligned = [](const void* q) { return ((uintptr_t)q & 15) != 0; };
   bool bad = misaligned(out0) || misaligned(out1) || misaligned(aux0) || misaligned(aux1);

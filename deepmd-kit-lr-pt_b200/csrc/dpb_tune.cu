@@ -26,6 +26,11 @@ static Knob g_knobs[] = {
     // columns per tensor-core tile of the fitting GEMMs (160 only where it
     // divides N)
     {"fit_n_tile", 160, 2, {80, 160}},
+    // fitting GEMM weights: 0 pre-split TF32 hi / lo read from L2, 1 FP32
+    // read and split in shared memory by the kernel (half the weight bytes,
+    // but the split sits on the converter warps' path: 30% slower on the
+    // 12,288-atom water step)
+    {"fit_split_b", 0, 2, {0, 1}},
     // warps (one center atom each) per CTA of the batched env / force kernels
     {"batch_atoms_per_cta", 4, 3, {2, 4, 8}},
     // neighbor rows per group in the FP32 training kernels

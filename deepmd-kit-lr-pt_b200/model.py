@@ -296,14 +296,17 @@ class _FittingTC:
         keep = []
 
         def split(mats):
-            hs, ls = [], []
+            # (hi, lo, fp32): pre-split TF32 parts, and the FP32 weights for
+            # the kernel's own split (fit_split_b knob)
+            hs, ls, fs = [], [], []
             for m in mats:
                 h, l = tf32_split(m)
                 hs.append(f32(h))
                 ls.append(f32(l))
-            keep.extend(hs + ls)
-            return ((ctypes.c_void_p * len(hs))(*[t.data_ptr() for t in hs]),
-                    (ctypes.c_void_p * len(ls))(*[t.data_ptr() for t in ls]))
+                fs.append(f32(np.ascontiguousarray(m)))
+            keep.extend(hs + ls + fs)
+            arr = lambda ts: (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])  # noqa: E731
+            return arr(hs), arr(ls), arr(fs)
 
         def vecs(vs):
             ts = [f32(v) for v in vs]
@@ -338,7 +341,9 @@ class _FittingTC:
 
     def _gemm(self, A, K, B, N, mode, out0, out1=None, aux0=None, aux1=None, bias=None,
               idt=None, w=None, s=None):
-        call("dpb_gemm_tf32x3_f32", ptr(A), self.n, K, B[0], B[1], N, self.type_rows.ctypes.data,
+        split_in_kernel = _capi.lib().dpb_tune_get(b"fit_split_b") == 1
+        bh, bl = (B[2], None) if split_in_kernel else (B[0], B[1])
+        call("dpb_gemm_tf32x3_f32", ptr(A), self.n, K, bh, bl, N, self.type_rows.ctypes.data,
              self.ntypes, mode, ptr(out0), ptr(out1), ptr(aux0), ptr(aux1), bias, idt, w,
              ptr(self.e), ptr(self.status), s)
 
@@ -719,7 +724,8 @@ class SeAEvaluator:
         sig = (f"frame:{self.nloc}a:{self.mode}:sel{'-'.join(map(str, cfg.sel))}:"
                f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
         return autotune.tune(self.replay, lambda: self.capture(),
-                             ["desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile"], signature=sig, reps=reps,
+                             ["desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b"],
+                             signature=sig, reps=reps,
                              device=self.dev, use_cache=use_cache)
 
     def replay(self):

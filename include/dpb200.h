@@ -453,11 +453,12 @@ DPB_API int dpb_force_virial_a_env_f64(double* force, double* virial,
  * deepmd/dpmodel/utils/network.py:282-330): C = A B^T with A [M, K] FP32
  * row-major (rows grouped by type, type_rows[t] rows of type t) and, per
  * type, B [N, K] given pre-split into TF32 hi/lo parts (b_hi/b_lo: HOST
- * arrays of device pointers). mode selects the fused epilogue (0 store,
+ * arrays of device pointers) or, with b_lo = NULL, in FP32 in b_hi and split
+ * in the kernel (half the weight bytes read). mode selects the fused epilogue (0 store,
  * 1 tanh(acc+bias), 2 tanh+timestep residual, 3 last layer + energy and its
  * first gradient, 4/5 backward of the residual layers); bias/idt/w are HOST
- * arrays of per-type device vectors [N]. N must be a multiple of 80
- *; K*4 and the row pitch must be multiples of 16 bytes. */
+ * arrays of per-type device vectors [N]. N must be a multiple of 80; K*4
+ * and the row pitch must be multiples of 16 bytes. */
 DPB_API int dpb_gemm_tf32x3_f32(const float* A, int M, int K,
                                 const float* const* b_hi,
                                 const float* const* b_lo, int N,
@@ -623,7 +624,8 @@ DPB_API int dpb_adam_f64(double* p, const double* g, double* m, double* v, long 
  * descriptor kernels), desc_coef_l1 {0, 1, 2, 3, 4} (cache policy of their
  * table loads: default, L1 no_allocate, L1 evict_first, L1 evict_last, L1 and L2
  * evict_last), fit_n_tile {80, 160} (fitting GEMM N tile, 160 only
- * where it divides N), batch_atoms_per_cta {2, 4, 8} (batched env / force),
+ * where it divides N), fit_split_b {0, 1} (weights pre-split or split in the
+ * GEMM), batch_atoms_per_cta {2, 4, 8} (batched env / force),
  * train_rows_per_group {4, 8} (FP32 training kernels, standard net),
  * train_warps_per_cta {1, 2, 4, 8}. The autotuner (autotune.py) times the
  * options on the caller's own step and sets the fastest. */

@@ -45,7 +45,8 @@ def test_batched_step_same_under_every_shape(mods, restore_knobs):
     params = mdl.prepare_frames(mdl.init_params(cfg, seed=3), frames)
     ev = bt.BatchEvaluator(params, frames)
     E0, F0, V0 = ev.compute()
-    for knob in ("batch_atoms_per_cta", "desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile"):
+    for knob in ("batch_atoms_per_cta", "desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile",
+                 "fit_split_b"):
         for v, (E, F, V) in _sweep(at, knob, ev.compute).items():
             ev.check()
             np.testing.assert_allclose(E, E0, rtol=0, atol=1e-5, err_msg=f"{knob}={v}")
@@ -59,7 +60,7 @@ def test_frame_step_same_under_every_shape(mods, restore_knobs):
     params = mdl.prepare(mdl.init_params(mdl.SeAConfig(), seed=1), coord, atype, box)
     ev = mdl.SeAEvaluator(params, atype, box, mode="compressed")
     E0, F0, V0 = ev.compute(coord)
-    for knob in ("desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile"):
+    for knob in ("desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b"):
         for v, (E, F, V) in _sweep(at, knob, lambda: ev.compute(coord)).items():
             assert abs(E - E0) < 1e-4, (knob, v)
             np.testing.assert_allclose(F, F0, rtol=0, atol=1e-6, err_msg=f"{knob}={v}")

@@ -92,7 +92,8 @@ def test_tile_knob_registry(dpb):
     from deepmd_kit_lr_pt_b200 import autotune
 
     names = autotune.names()
-    assert {"desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "batch_atoms_per_cta",
+    assert {"desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b",
+            "batch_atoms_per_cta",
             "train_rows_per_group", "train_warps_per_cta"} <= set(names)
     for n in names:
         opts = autotune.options(n)

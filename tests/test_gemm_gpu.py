@@ -23,12 +23,17 @@ def _ptrs(ts):
     return (ctypes.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
 
 
-def _run(dpb, mdl, A, Bs, type_rows, mode, aux0=None, aux1=None, bias=None, idt=None, w=None):
+def _run(dpb, mdl, A, Bs, type_rows, mode, aux0=None, aux1=None, bias=None, idt=None, w=None,
+         split_in_kernel=False):
     M, K = A.shape
     N = Bs[0].shape[0]
-    hi, lo = zip(*[mdl.tf32_split(b) for b in Bs])
-    th = [torch.tensor(h, device=DEV) for h in hi]
-    tl = [torch.tensor(l, device=DEV) for l in lo]
+    if split_in_kernel:  # FP32 weights, b_lo = NULL: the kernel splits them
+        th = [torch.tensor(np.ascontiguousarray(b, np.float32), device=DEV) for b in Bs]
+        tl = None
+    else:
+        hi, lo = zip(*[mdl.tf32_split(b) for b in Bs])
+        th = [torch.tensor(h, device=DEV) for h in hi]
+        tl = [torch.tensor(l, device=DEV) for l in lo]
     out0 = torch.zeros((M, N), dtype=torch.float32, device=DEV)
     out1 = torch.zeros((M, N), dtype=torch.float32, device=DEV)
     e = torch.zeros(M, dtype=torch.float32, device=DEV)
@@ -47,7 +52,8 @@ def _run(dpb, mdl, A, Bs, type_rows, mode, aux0=None, aux1=None, bias=None, idt=
     ta = torch.tensor(A, device=DEV)
     x0 = None if aux0 is None else torch.tensor(aux0, device=DEV)
     x1 = None if aux1 is None else torch.tensor(aux1, device=DEV)
-    cap.call("dpb_gemm_tf32x3_f32", cap.ptr(ta), M, K, _ptrs(th), _ptrs(tl), N, tr.ctypes.data,
+    cap.call("dpb_gemm_tf32x3_f32", cap.ptr(ta), M, K, _ptrs(th), None if tl is None else _ptrs(tl),
+             N, tr.ctypes.data,
              len(Bs), mode, cap.ptr(out0), cap.ptr(out1), cap.ptr(x0), cap.ptr(x1), vec(bias),
              vec(idt), vec(w), cap.ptr(e), cap.ptr(st), torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
@@ -78,6 +84,25 @@ def test_gemm_store(dpb, mdl, M, K, N, rows):
     err = _rel(out0, ref)
     print(f"M={M} K={K} N={N}: rel err {err:.2e}")
     assert err < 2e-5
+
+
+@pytest.mark.parametrize("M,K,N,rows,mode", [(256, 64, 80, [128, 128], 0),
+                                             (300, 240, 240, [100, 200], 1),
+                                             (777, 1600, 240, [259, 518], 0),
+                                             (640, 240, 1600, [640], 5)])
+def test_gemm_weight_split_in_kernel_is_exact(dpb, mdl, M, K, N, rows, mode):
+    """FP32 weights split into TF32 hi / lo in shared memory give bit-for-bit
+    the result of the pre-split weights (same rounding, exact remainder)."""
+    rng = np.random.default_rng(7 + M)
+    A = rng.normal(size=(M, K)).astype(np.float32) * 0.5
+    Bs = [rng.normal(size=(N, K)).astype(np.float32) / np.sqrt(K) for _ in rows]
+    kw = dict(bias=[rng.normal(size=N) for _ in rows]) if mode == 1 else dict(
+        aux0=rng.normal(size=(M, N)).astype(np.float32), aux1=rng.normal(size=(M, N)).astype(
+            np.float32)) if mode == 5 else {}
+    pre = _run(dpb, mdl, A, Bs, rows, mode, **kw)
+    ker = _run(dpb, mdl, A, Bs, rows, mode, split_in_kernel=True, **kw)
+    for a, b in zip(pre, ker):
+        assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("N", [240, 320, 400])  # tiles of 80, 160 and 80 columns
