@@ -11,8 +11,8 @@
 // dropped), accumulated in FP32 in tensor memory.
 //
 // Persistent, warp-specialised CTA (one per SM) walking output tiles of 128
-// rows x BN columns (BN = 160 when it divides N and the fit_n_tile knob allows it,
-// else 80):
+// rows x BN columns (the widest of 240 (K <= 512), 160, 80 that divides N and the
+// fit_n_tile knob allows):
 //   warp 0      TMA producer: A tile 128 x 32 and B hi/lo tiles BN x 32 per
 //               k-block into a STAGES-deep shared-memory ring (128-byte
 //               swizzle);
@@ -72,6 +72,9 @@ struct GemmCfg {
 // A re-reads).
 using CfgN80 = GemmCfg<80, 4, 4, 2, 4>;
 using CfgN160 = GemmCfg<160, 4, 2, 2, 8>;
+// one 240-column tile per 128 rows (one accumulator, two stages): for the
+// short-K 240 x 240 layers, one wave instead of two over the row tiles
+using CfgN240 = GemmCfg<240, 2, 4, 1, 8>;
 
 enum : int {
   ST_MMA_TIMEOUT = 1 << 8,
@@ -631,9 +634,12 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
     set_error("gemm_tf32x3: N=%d must be a multiple of 80", N);
     return DPB_ERR_INVALID;
   }
-  const int BN = (N % CfgN160::BN == 0 && tune_value("fit_n_tile", CfgN160::BN) == CfgN160::BN)
-                     ? CfgN160::BN
-                     : CfgN80::BN;
+  // widest tile allowed by the fit_n_tile knob that divides N (240 only for
+  // K <= 512, where two pipeline stages keep the tensor cores fed)
+  const int knob = tune_value("fit_n_tile", CfgN160::BN);
+  const int BN = (knob >= CfgN240::BN && N % CfgN240::BN == 0 && K <= 512) ? CfgN240::BN
+                 : (knob >= CfgN160::BN && N % CfgN160::BN == 0)            ? CfgN160::BN
+                                                                            : CfgN80::BN;
   GemmMaps maps;
   GemmShape shp;
   shp.ntypes = ntypes;
@@ -682,6 +688,7 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
     ep.w[t] = w ? w[t] : nullptr;
   }
   cudaStream_t st = as_stream(stream);
+  if (BN == CfgN240::BN) return launch<CfgN240>(maps, shp, ep, status, st);
   if (BN == CfgN160::BN) return launch<CfgN160>(maps, shp, ep, status, st);
   return launch<CfgN80>(maps, shp, ep, status, st);
 }

@@ -23,9 +23,9 @@ static Knob g_knobs[] = {
     // fastest on 12,288-atom water: rows near the switch cutoff are shared),
     // 4 evict_last in L1 and L2
     {"desc_coef_l1", 3, 5, {0, 1, 2, 3, 4}},
-    // columns per tensor-core tile of the fitting GEMMs (160 only where it
-    // divides N)
-    {"fit_n_tile", 160, 2, {80, 160}},
+    // widest tensor-core tile of the fitting GEMMs (a width is used where it
+    // divides N; 240 only for K <= 512)
+    {"fit_n_tile", 160, 3, {80, 160, 240}},
     // fitting GEMM weights: 0 pre-split TF32 hi / lo read from L2, 1 FP32
     // read and split in shared memory by the kernel (half the weight bytes,
     // but the split sits on the converter warps' path: 30% slower on the

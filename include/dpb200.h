@@ -623,8 +623,8 @@ DPB_API int dpb_adam_f64(double* p, const double* g, double* m, double* v, long 
  * the shapes it was captured with): desc_atoms_per_cta {2, 4, 8} (fused
  * descriptor kernels), desc_coef_l1 {0, 1, 2, 3, 4} (cache policy of their
  * table loads: default, L1 no_allocate, L1 evict_first, L1 evict_last, L1 and L2
- * evict_last), fit_n_tile {80, 160} (fitting GEMM N tile, 160 only
- * where it divides N), fit_split_b {0, 1} (weights pre-split or split in the
+ * evict_last), fit_n_tile {80, 160, 240} (widest fitting GEMM N tile; a
+ * width is used where it divides N, 240 only for K <= 512), fit_split_b {0, 1} (weights pre-split or split in the
  * GEMM), batch_atoms_per_cta {2, 4, 8} (batched env / force),
  * train_rows_per_group {4, 8} (FP32 training kernels, standard net),
  * train_warps_per_cta {1, 2, 4, 8}. The autotuner (autotune.py) times the

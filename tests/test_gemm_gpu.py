@@ -157,3 +157,34 @@ def test_fitting_tc_matches_fp64(dpb, mdl):
     print(f"E {float(E):.8f} ref {Eref:.8f}; dD rel {_rel(dD.cpu().numpy(), gref):.2e}")
     assert abs(float(E) - Eref) / n < 1e-6
     assert _rel(dD.cpu().numpy(), gref) < 2e-5
+
+
+@pytest.mark.parametrize("M,K,N,rows", [(300, 240, 240, [100, 200]), (386, 480, 240, [96, 290])])
+def test_gemm_240_tile(dpb, mdl, M, K, N, rows):
+    """The one-tile-per-128-rows configuration (fit_n_tile = 240, K <= 512):
+    the plain product and every fused epilogue, as with the narrower tiles."""
+    from deepmd_kit_lr_pt_b200 import autotune
+
+    old = autotune.get("fit_n_tile")
+    autotune.set_knob("fit_n_tile", 240)
+    try:
+        rng = np.random.default_rng(M + K)
+        A = rng.normal(size=(M, K)).astype(np.float32) * 0.5
+        Bs = [rng.normal(size=(N, K)).astype(np.float32) / np.sqrt(K) for _ in rows]
+        acc = _ref(A, Bs, rows)
+        o0, _, _ = _run(dpb, mdl, A, Bs, rows, 0)
+        assert _rel(o0, acc) < 2e-5
+        tid = np.repeat(np.arange(len(rows)), rows)
+        bias = [rng.normal(size=N) for _ in rows]
+        idt = [rng.normal(0.1, 0.01, size=N) for _ in rows]
+        w = [rng.normal(size=N) for _ in rows]
+        b, d, wv = np.stack(bias)[tid], np.stack(idt)[tid], np.stack(w)[tid]
+        x0 = rng.normal(size=(M, N)).astype(np.float32) * 0.5
+        o0, o1, _ = _run(dpb, mdl, A, Bs, rows, 2, aux0=x0, bias=bias, idt=idt)
+        y = np.tanh(acc + b)
+        assert _rel(o0, y) < 2e-5 and _rel(o1, x0 + d * y) < 2e-5
+        o0, _, e = _run(dpb, mdl, A, Bs, rows, 3, aux0=x0, bias=bias, idt=idt, w=w)
+        h = x0 + d * y
+        assert _rel(e, (h * wv).sum(1)) < 2e-5 and _rel(o0, wv * d * (1 - y * y)) < 2e-5
+    finally:
+        autotune.set_knob("fit_n_tile", old)
