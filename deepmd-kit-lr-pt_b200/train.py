@@ -285,6 +285,7 @@ class SeATrainer:
             bufs = [{k: z((n, ly["w_out"])) for k in ("Y", "H", "G", "Zb", "Zd", "Hd", "A",
                                                        "Ad", "Zbd")} for ly in layers]
             self.fbuf.append(bufs)
+        self._streams = [torch.cuda.Stream(device=dev) for _ in range(nt)]
         self.loss = loss
         self._natoms_inv = torch.tensor(1.0 / np.maximum(ft.counts, 1), dtype=f64, device=dev)
         self._pref = torch.zeros(3, dtype=f64, device=dev)
@@ -350,28 +351,7 @@ class SeATrainer:
              ptr(self.nlist), ptr(ft.type), ptr(ft.drow), self.Wp, self.bp,
              self.widths.ctypes.data, sec.ctypes.data, sec.size, N, self.ax,
              self.fold.ctypes.data, s)
-        for t, ((layers, out), bufs) in enumerate(zip(self.fit_layers, self.fbuf)):
-            o, n = self.fit_rows[t]
-            if n == 0:
-                continue
-            H = self.D[o:o + n]
-            for ly, bf in zip(layers, bufs):
-                torch.addmm(ly["b"], H, ly["W"], out=bf["Y"])
-                call(f"dpb_fit_act_{suf}", ptr(bf["Y"]), ptr(bf["H"]), ptr(H), ptr(ly["d"]), n,
-                     ly["w_out"], ly["w_in"], s)
-                H = bf["H"]
-            call(f"dpb_fit_out_{suf}", ptr(self.e_rows[o:o + n]), ptr(H), ptr(out["W"]),
-                 ptr(out["b"]), ctypes.c_double(out["ebias"]), n, out["w"], s)
-            # dE/dD through the fitting
-            G = bufs[-1]["G"]
-            call(f"dpb_fit_out_adj_{suf}", ptr(G), None, None, None, ptr(H), None, ptr(out["W"]),
-                 None, n, out["w"], s)
-            for l in range(len(layers) - 1, -1, -1):
-                ly, bf = layers[l], bufs[l]
-                call(f"dpb_fit_bwd_{suf}", ptr(bf["Zb"]), ptr(bf["G"]), ptr(bf["Y"]),
-                     ptr(ly["d"]), n, ly["w_out"], s)
-                dst = self.Dbar[o:o + n] if l == 0 else bufs[l - 1]["G"]
-                self._adj_in(dst, bf["Zb"], ly["W"], bf["G"], ly["w_out"], ly["w_in"], s)
+        self._each_type(self._fit_forward_type)
         e_fn = "dpb_batch_energy" if suf == "f32" else "dpb_batch_energy_f64"
         call(e_fn, ptr(self.energy), ptr(self.e_rows), ptr(ft.drow), ptr(self.e_const),
              ptr(ft.atom_off), F, s)
@@ -384,6 +364,77 @@ class SeATrainer:
              ptr(ft.type), ptr(self.std), ptr(self.nlist), ptr(ft.atom_off), ptr(ft.cell_off),
              ptr(ft.box), ptr(ft.ncell), ptr(ft.row_frame), F, N, cfg.nnei, cfg.ntypes, rc, rs, s)
         return self.energy, self.force, self.virial
+
+    def _each_type(self, fn):
+        """fn(t, stream handle) for every center type with rows; the types'
+        fitting chains are independent and run on side streams forked from
+        (and joined back into) the current stream."""
+        cur = torch.cuda.current_stream(self.dev)
+        active = [t for t in range(self.cfg.ntypes) if self.fit_rows[t][1] > 0]
+        if len(active) <= 1:
+            for t in active:
+                fn(t, cur.cuda_stream)
+            return
+        for t in active:
+            st = self._streams[t]
+            st.wait_stream(cur)
+            with torch.cuda.stream(st):
+                fn(t, st.cuda_stream)
+        for t in active:
+            cur.wait_stream(self._streams[t])
+
+    def _fit_forward_type(self, t, s):
+        """Fitting net of center type t: atomic energies and dE/dD."""
+        suf = self.suf
+        (layers, out), bufs = self.fit_layers[t], self.fbuf[t]
+        o, n = self.fit_rows[t]
+        H = self.D[o:o + n]
+        for ly, bf in zip(layers, bufs):
+            torch.addmm(ly["b"], H, ly["W"], out=bf["Y"])
+            call(f"dpb_fit_act_{suf}", ptr(bf["Y"]), ptr(bf["H"]), ptr(H), ptr(ly["d"]), n,
+                 ly["w_out"], ly["w_in"], s)
+            H = bf["H"]
+        call(f"dpb_fit_out_{suf}", ptr(self.e_rows[o:o + n]), ptr(H), ptr(out["W"]),
+             ptr(out["b"]), ctypes.c_double(out["ebias"]), n, out["w"], s)
+        # dE/dD through the fitting
+        G = bufs[-1]["G"]
+        call(f"dpb_fit_out_adj_{suf}", ptr(G), None, None, None, ptr(H), None, ptr(out["W"]),
+             None, n, out["w"], s)
+        for l in range(len(layers) - 1, -1, -1):
+            ly, bf = layers[l], bufs[l]
+            call(f"dpb_fit_bwd_{suf}", ptr(bf["Zb"]), ptr(bf["G"]), ptr(bf["Y"]),
+                 ptr(ly["d"]), n, ly["w_out"], s)
+            dst = self.Dbar[o:o + n] if l == 0 else bufs[l - 1]["G"]
+            self._adj_in(dst, bf["Zb"], ly["W"], bf["G"], ly["w_out"], ly["w_in"], s)
+
+    def _fit_backward_type(self, t, s):
+        """Tangent and reverse-over-tangent of the fitting net of center type
+        t: its weight gradients and the adjoints of D and D'."""
+        suf = self.suf
+        (layers, out), bufs = self.fit_layers[t], self.fbuf[t]
+        o, n = self.fit_rows[t]
+        Hd = self.Dt[o:o + n]
+        for ly, bf in zip(layers, bufs):
+            torch.mm(Hd, ly["W"], out=bf["Zd"])
+            call(f"dpb_fit_tan_{suf}", ptr(bf["Hd"]), ptr(bf["Zd"]), ptr(Hd), ptr(bf["Y"]),
+                 ptr(ly["d"]), n, ly["w_out"], ly["w_in"], s)
+            Hd = bf["Hd"]
+        call(f"dpb_fit_out_adj_{suf}", ptr(bufs[-1]["A"]), ptr(bufs[-1]["Ad"]),
+             ptr(out["gW"]), ptr(out["gb"]), ptr(bufs[-1]["H"]), ptr(Hd), ptr(out["W"]),
+             ptr(self.lam[o:o + n]), n, out["w"], s)
+        for l in range(len(layers) - 1, -1, -1):
+            ly, bf = layers[l], bufs[l]
+            call(f"dpb_fit_rev_{suf}", ptr(bf["Zb"]), ptr(bf["Zbd"]), ptr(ly["gb"]),
+                 ptr(ly["gd"]), ptr(bf["A"]), ptr(bf["Ad"]), ptr(bf["Y"]), ptr(bf["Zd"]),
+                 ptr(ly["d"]), n, ly["w_out"], s)
+            Hin = self.D[o:o + n] if l == 0 else bufs[l - 1]["H"]
+            Hdin = self.Dt[o:o + n] if l == 0 else bufs[l - 1]["Hd"]
+            ly["gW"].addmm_(Hin.t(), bf["Zb"])
+            ly["gW"].addmm_(Hdin.t(), bf["Zbd"])
+            dA = self.DbarJ[o:o + n] if l == 0 else bufs[l - 1]["A"]
+            dAd = self.Ddbar[o:o + n] if l == 0 else bufs[l - 1]["Ad"]
+            self._adj_in(dA, bf["Zb"], ly["W"], bf["A"], ly["w_out"], ly["w_in"], s)
+            self._adj_in(dAd, bf["Zbd"], ly["W"], bf["Ad"], ly["w_out"], ly["w_in"], s)
 
     # ----------------------------------------------------------- backward
     def _backward(self, gE, gF, gV):
@@ -406,32 +457,7 @@ class SeATrainer:
              ptr(ft.type), ptr(ft.drow), ptr(ft.atom_off), ptr(ft.box), ptr(ft.row_frame), F,
              self.Wp, self.bp, self.widths.ctypes.data, sec.ctypes.data, sec.size, N, self.ax,
              rc, rs, s)
-        for t, ((layers, out), bufs) in enumerate(zip(self.fit_layers, self.fbuf)):
-            o, n = self.fit_rows[t]
-            if n == 0:
-                continue
-            Hd = self.Dt[o:o + n]
-            for ly, bf in zip(layers, bufs):
-                torch.mm(Hd, ly["W"], out=bf["Zd"])
-                call(f"dpb_fit_tan_{suf}", ptr(bf["Hd"]), ptr(bf["Zd"]), ptr(Hd), ptr(bf["Y"]),
-                     ptr(ly["d"]), n, ly["w_out"], ly["w_in"], s)
-                Hd = bf["Hd"]
-            call(f"dpb_fit_out_adj_{suf}", ptr(bufs[-1]["A"]), ptr(bufs[-1]["Ad"]),
-                 ptr(out["gW"]), ptr(out["gb"]), ptr(bufs[-1]["H"]), ptr(Hd), ptr(out["W"]),
-                 ptr(self.lam[o:o + n]), n, out["w"], s)
-            for l in range(len(layers) - 1, -1, -1):
-                ly, bf = layers[l], bufs[l]
-                call(f"dpb_fit_rev_{suf}", ptr(bf["Zb"]), ptr(bf["Zbd"]), ptr(ly["gb"]),
-                     ptr(ly["gd"]), ptr(bf["A"]), ptr(bf["Ad"]), ptr(bf["Y"]), ptr(bf["Zd"]),
-                     ptr(ly["d"]), n, ly["w_out"], s)
-                Hin = self.D[o:o + n] if l == 0 else bufs[l - 1]["H"]
-                Hdin = self.Dt[o:o + n] if l == 0 else bufs[l - 1]["Hd"]
-                ly["gW"].addmm_(Hin.t(), bf["Zb"])
-                ly["gW"].addmm_(Hdin.t(), bf["Zbd"])
-                dA = self.DbarJ[o:o + n] if l == 0 else bufs[l - 1]["A"]
-                dAd = self.Ddbar[o:o + n] if l == 0 else bufs[l - 1]["Ad"]
-                self._adj_in(dA, bf["Zb"], ly["W"], bf["A"], ly["w_out"], ly["w_in"], s)
-                self._adj_in(dAd, bf["Zbd"], ly["W"], bf["Ad"], ly["w_out"], ly["w_in"], s)
+        self._each_type(self._fit_backward_type)
         call(f"dpb_se_a_train_rev_{suf}", self.gWp, self.gbp, ptr(self.xbar), ptr(self.xyz),
              ptr(self.xyz_t),
              ptr(self.DbarJ), ptr(self.Ddbar), ptr(self.avg), ptr(self.std), ptr(gF), ptr(gV),
