@@ -225,3 +225,36 @@ def test_water_batch_of_16_trains(mods):
     t.check()
     assert np.all(np.isfinite(losses))
     assert losses[-1] < losses[0] and min(losses) < 0.9 * losses[0], losses
+
+
+def test_fp64_uneven_three_species_batch_matches_oracle(mods):
+    """Frames of different sizes and species (water 96 and 150 atoms, FCC Cu
+    64 atoms; model O/H/Cu, sel [46, 92, 60]): the per-frame atom counts enter
+    the loss and the ragged batch the kernels; every gradient entry against
+    the oracle's FP64 autograd restatement."""
+    from oracle import model_ref, oracle
+
+    mdl, wl, tr = mods
+    rng = np.random.default_rng(17)
+    frames = [wl.water_frame_density(96, rng), wl.cu_frame(64, rng),
+              wl.water_frame_density(150, rng)]
+    cfg = mdl.SeAConfig(sel=(46, 92, 60))
+    params = mdl.init_params(cfg, seed=5)
+    params.davg, params.dstd, _ = mdl.env_stats_frames(params, frames)
+    nat = np.array([a.size for _, a, _ in frames])
+    labels = (rng.normal(0, 2.0, len(frames)), rng.normal(0, 0.5, (int(nat.sum()), 3)),
+              rng.normal(0, 5.0, (len(frames), 9)))
+    prefs = (0.02, 1000.0, 0.02)
+    loss = tr.EnergyStdLoss(start_pref_e=prefs[0], limit_pref_e=prefs[0],
+                            start_pref_f=prefs[1], limit_pref_f=prefs[1],
+                            start_pref_v=prefs[2], limit_pref_v=prefs[2])
+    t = tr.SeATrainer(params, frames, dtype=torch.float64, loss=loss)
+    t.set_labels(*labels)
+    lv, g = _autograd_grads(t, loss)
+    ref_loss, E, F, V, ref = model_ref.train_loss_grads(oracle.port(), params, frames, labels,
+                                                        prefs)
+    assert abs(lv - ref_loss) <= 1e-10 * abs(ref_loss)
+    for name, v in t.named_grads(g).items():
+        r = ref[name].reshape(v.shape)
+        err = np.abs(v.cpu().numpy() - r).max()
+        assert err <= 1e-9 * np.abs(r).max() + 1e-9, (name, err)
