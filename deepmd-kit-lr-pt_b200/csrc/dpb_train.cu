@@ -188,14 +188,61 @@ __device__ __forceinline__ void tr_entries(int* ent, int* secn, const int* nl, c
   __syncwarp();
 }
 
-// Staged per-row vectors are [channel][row] with the odd row stride R + 1:
-// a lane-owned channel touches its R rows without bank conflicts and the
-// next layer reads one channel of all rows as a broadcast.
+// Staged per-row vectors: the R rows of channel c are contiguous, and with
+// two 16-byte chunks per channel the chunks are swapped when bit 2 of c is
+// set. A lane-owned channel then moves as whole 16-byte chunks without bank
+// conflicts (the 8 lanes of a quarter-warp hit 8 different bank groups) and
+// the next layer reads one channel as one or two broadcast 16-byte loads.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
 
 template <typename T, int R>
-__device__ __forceinline__ void tr_load_col(T (&a)[R], const T* p) {
+__device__ __forceinline__ int stg_chunk(int c, int h) {
+  constexpr int Q = R / Vec16<T>::n;
+  static_assert(Q == 1 || Q == 2, "one or two 16-byte chunks per staged channel");
+  return Q == 2 ? (h ^ ((c >> 2) & 1)) : h;
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void stg_load(T (&a)[R], const T* base, int c) {
+  using V = typename Vec16<T>::type;
+  constexpr int E = Vec16<T>::n, Q = R / E;
 #pragma unroll
-  for (int r = 0; r < R; ++r) a[r] = p[r];
+  for (int h = 0; h < Q; ++h) {
+    const V v = *reinterpret_cast<const V*>(base + c * R + stg_chunk<T, R>(c, h) * E);
+    const T* p = reinterpret_cast<const T*>(&v);
+#pragma unroll
+    for (int k = 0; k < E; ++k) a[h * E + k] = p[k];
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void stg_store(T* base, int c, const T (&a)[R]) {
+  using V = typename Vec16<T>::type;
+  constexpr int E = Vec16<T>::n, Q = R / E;
+#pragma unroll
+  for (int h = 0; h < Q; ++h) {
+    V v;
+    T* p = reinterpret_cast<T*>(&v);
+#pragma unroll
+    for (int k = 0; k < E; ++k) p[k] = a[h * E + k];
+    *reinterpret_cast<V*>(base + c * R + stg_chunk<T, R>(c, h) * E) = v;
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void tr_load_col(T (&a)[R], const T* base, int c) {
+  stg_load<T, R>(a, base, c);
 }
 
 // acc[j][r] = sum_i in[i][r] W[i * sw + c_j], c_j = lane + 32 j (< n_out)
@@ -209,7 +256,7 @@ __device__ __forceinline__ void tr_gemv(T (&acc)[CP][R], const T* in, int n_in, 
 #pragma unroll 5
   for (int i = 0; i < n_in; ++i) {
     T a[R];
-    tr_load_col<T, R>(a, in + i * (R + 1));
+    tr_load_col<T, R>(a, in, i);
 #pragma unroll
     for (int j = 0; j < CP; ++j) {
       const int c = lane + 32 * j;
@@ -232,8 +279,8 @@ __device__ __forceinline__ void tr_gemv2(T (&acc)[CP][R], T (&acd)[CP][R], const
 #pragma unroll 5
   for (int i = 0; i < n_in; ++i) {
     T a[R], ad[R];
-    tr_load_col<T, R>(a, in + i * (R + 1));
-    tr_load_col<T, R>(ad, ind + i * (R + 1));
+    tr_load_col<T, R>(a, in, i);
+    tr_load_col<T, R>(ad, ind, i);
 #pragma unroll
     for (int j = 0; j < CP; ++j) {
       const int c = lane + 32 * j;
@@ -259,7 +306,7 @@ __device__ __forceinline__ void tr_gemvT(T (&acc)[CP][R], const T* zb, int n_out
 #pragma unroll 5
   for (int c = 0; c < n_out; ++c) {
     T z[R];
-    tr_load_col<T, R>(z, zb + c * (R + 1));
+    tr_load_col<T, R>(z, zb, c);
 #pragma unroll
     for (int j = 0; j < CP; ++j) {
       const int i = lane + 32 * j;
@@ -281,8 +328,8 @@ __device__ __forceinline__ void tr_gemvT2(T (&acc)[CP][R], T (&acd)[CP][R], cons
 #pragma unroll 5
   for (int c = 0; c < n_out; ++c) {
     T z[R], zd[R];
-    tr_load_col<T, R>(z, zb + c * (R + 1));
-    tr_load_col<T, R>(zd, zbd + c * (R + 1));
+    tr_load_col<T, R>(z, zb, c);
+    tr_load_col<T, R>(zd, zbd, c);
 #pragma unroll
     for (int j = 0; j < CP; ++j) {
       const int i = lane + 32 * j;
@@ -296,21 +343,36 @@ __device__ __forceinline__ void tr_gemvT2(T (&acc)[CP][R], T (&acd)[CP][R], cons
   }
 }
 
-// residual term of output channel c (< n_out) from the staged input
+// residual term of output channel c (< n_out), all R rows, from the staged
+// input
 template <typename T, int R>
-__device__ __forceinline__ T tr_res(const T* in, int res, int c, int n_in, int r) {
-  if (res == TR_RES_IDENT) return in[c * (R + 1) + r];
-  if (res == TR_RES_DUP) return in[(c < n_in ? c : c - n_in) * (R + 1) + r];
-  return (T)0;
+__device__ __forceinline__ void tr_res_v(T (&o)[R], const T* in, int res, int c, int n_in) {
+  if (res == TR_RES_IDENT) {
+    stg_load<T, R>(o, in, c);
+  } else if (res == TR_RES_DUP) {
+    stg_load<T, R>(o, in, c < n_in ? c : c - n_in);
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[r] = (T)0;
+  }
 }
 
-// adjoint of the residual for input channel i (< n_in) from the staged
-// output adjoint
+// adjoint of the residual for input channel i (< n_in), all R rows, from the
+// staged output adjoint
 template <typename T, int R>
-__device__ __forceinline__ T tr_res_adj(const T* gb, int res, int i, int n_in, int r) {
-  if (res == TR_RES_IDENT) return gb[i * (R + 1) + r];
-  if (res == TR_RES_DUP) return gb[i * (R + 1) + r] + gb[(i + n_in) * (R + 1) + r];
-  return (T)0;
+__device__ __forceinline__ void tr_res_adj_v(T (&o)[R], const T* gb, int res, int i, int n_in) {
+  if (res == TR_RES_IDENT) {
+    stg_load<T, R>(o, gb, i);
+  } else if (res == TR_RES_DUP) {
+    T u[R];
+    stg_load<T, R>(o, gb, i);
+    stg_load<T, R>(u, gb, i + n_in);
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[r] += u[r];
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[r] = (T)0;
+  }
 }
 
 // sum over lanes of v[lane & (NV - 1)] (NV a power of two <= 32), NV - 1
@@ -504,7 +566,6 @@ template <typename T, int R, int N1, int N2, int N3>
 __global__ void __launch_bounds__(256, 1)
 k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ em,
          TrNet<T> net, TrGeom g, TrLayout lay) {
-  constexpr int RS = R + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -555,8 +616,10 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
         __syncwarp();
         if (lane < n1) {
           const T w1 = W.W1[lane], b1 = W.b1[lane];
+          T v1[R];
 #pragma unroll
-          for (int r = 0; r < R; ++r) A1[lane * RS + r] = tr_tanh(fma(ss[r], w1, b1));
+          for (int r = 0; r < R; ++r) v1[r] = tr_tanh(fma(ss[r], w1, b1));
+          stg_store<T, R>(A1, lane, v1);
         }
         __syncwarp();
         {
@@ -567,9 +630,11 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
             const int c = lane + 32 * j;
             if (c < n2) {
               const T bb = W.b2[c];
+              T rs[R], v[R];
+              tr_res_v<T, R>(rs, A1, res2, c, n1);
 #pragma unroll
-              for (int r = 0; r < R; ++r)
-                A2[c * RS + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, res2, c, n1, r);
+              for (int r = 0; r < R; ++r) v[r] = tr_tanh(acc[j][r] + bb) + rs[r];
+              stg_store<T, R>(A2, c, v);
             }
           }
         }
@@ -582,9 +647,11 @@ k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ e
             const int c = lane + 32 * j;
             if (c < n3) {
               const T bb = W.b3[c];
+              T rs[R];
+              tr_res_v<T, R>(rs, A2, res3, c, n2);
 #pragma unroll
               for (int r = 0; r < R; ++r) {
-                const T G = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A2, res3, c, n2, r);
+                const T G = tr_tanh(acc[j][r] + bb) + rs[r];
                 const T mg = mus[r] * G;
 #pragma unroll
                 for (int a = 0; a < 4; ++a) xyz[a][j] = fma(rr[r * 4 + a], mg, xyz[a][j]);
@@ -632,7 +699,6 @@ template <typename T, int R, int N1, int N2, int N3>
 __global__ void __launch_bounds__(256, 1)
 k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xbar,
          TrNet<T> net, TrGeom g, TrLayout lay) {
-  constexpr int RS = R + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -658,7 +724,7 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
     tr_read_x4(xb, xbar + (size_t)row * 4 * n3, n3, lane);
     tr_entries(ent, secn, nl, g, ti, false, lane, 0, g.ntypes);
     T* Zb3 = big;
-    T* Gb = big + n3 * RS;
+    T* Gb = big + n3 * R;
     for (int t = 0; t < g.ntypes; ++t) {
       const WV<T> W = tr_wview<T, WS>(net, sw, t, lay.pw, n1, n2, sw2, sw3);
       for (int e0 = secn[t]; e0 < secn[t + 1]; e0 += R) {
@@ -679,8 +745,10 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
         __syncwarp();
         if (lane < n1) {
           const T w1 = W.W1[lane], b1 = W.b1[lane];
+          T v1[R];
 #pragma unroll
-          for (int r = 0; r < R; ++r) A1[lane * RS + r] = tr_tanh(fma(ss[r], w1, b1));
+          for (int r = 0; r < R; ++r) v1[r] = tr_tanh(fma(ss[r], w1, b1));
+          stg_store<T, R>(A1, lane, v1);
         }
         __syncwarp();
         {
@@ -691,9 +759,11 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
             const int c = lane + 32 * j;
             if (c < n2) {
               const T bb = W.b2[c];
+              T rs[R], v[R];
+              tr_res_v<T, R>(rs, A1, res2, c, n1);
 #pragma unroll
-              for (int r = 0; r < R; ++r)
-                A2[c * RS + r] = tr_tanh(acc[j][r] + bb) + tr_res<T, R>(A1, res2, c, n1, r);
+              for (int r = 0; r < R; ++r) v[r] = tr_tanh(acc[j][r] + bb) + rs[r];
+              stg_store<T, R>(A2, c, v);
             }
           }
         }
@@ -709,19 +779,23 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
             const int c = lane + 32 * j;
             if (c < n3) {
               const T bb = W.b3[c];
+              T rs[R], zv[R], gv[R];
+              tr_res_v<T, R>(rs, A2, res3, c, n2);
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                const T G = y + tr_res<T, R>(A2, res3, c, n2, r);
+                const T G = y + rs[r];
                 T gbar = (T)0;
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
                   part[r * 4 + a] = fma(G, xb[a][j], part[r * 4 + a]);
                   gbar = fma(rr[r * 4 + a], xb[a][j], gbar);
                 }
-                Zb3[c * RS + r] = gbar * ((T)1 - y * y);
-                Gb[c * RS + r] = gbar;
+                zv[r] = gbar * ((T)1 - y * y);
+                gv[r] = gbar;
               }
+              stg_store<T, R>(Zb3, c, zv);
+              stg_store<T, R>(Gb, c, gv);
             }
           }
         }
@@ -733,30 +807,33 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
 #pragma unroll
           for (int j = 0; j < TR_C2; ++j) {
             const int i = lane + 32 * j;
+            if (i < n2) {
+              T ga[R], a2[R], rs[R];
+              tr_res_adj_v<T, R>(ga, Gb, res3, i, n2);
+              stg_load<T, R>(a2, A2, i);
+              tr_res_v<T, R>(rs, A1, res2, i, n1);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-              if (i < n2) {
-                hb2[j][r] += tr_res_adj<T, R>(Gb, res3, i, n2, r);
-                const T y2 = A2[i * RS + r] - tr_res<T, R>(A1, res2, i, n1, r);
+              for (int r = 0; r < R; ++r) {
+                hb2[j][r] += ga[r];
+                const T y2 = a2[r] - rs[r];
                 zb2[j][r] = hb2[j][r] * ((T)1 - y2 * y2);
-              } else {
-                zb2[j][r] = hb2[j][r] = (T)0;
               }
+            } else {
+#pragma unroll
+              for (int r = 0; r < R; ++r) zb2[j][r] = hb2[j][r] = (T)0;
             }
           }
         }
         __syncwarp();
         T* Zb2 = big;
-        T* Hb2 = big + n2 * RS;
+        T* Hb2 = big + n2 * R;
 #pragma unroll
         for (int j = 0; j < TR_C2; ++j) {
           const int i = lane + 32 * j;
-          if (i < n2)
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              Zb2[i * RS + r] = zb2[j][r];
-              Hb2[i * RS + r] = hb2[j][r];
-            }
+          if (i < n2) {
+            stg_store<T, R>(Zb2, i, zb2[j]);
+            stg_store<T, R>(Hb2, i, hb2[j]);
+          }
         }
         __syncwarp();
         {
@@ -764,10 +841,13 @@ k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xb
           tr_gemvT<T, R, TR_C1>(hb1, Zb2, n2, W.W2, sw2, n1, lane);
           if (lane < n1) {
             const T w1 = W.W1[lane];
+            T ha[R], a1[R];
+            tr_res_adj_v<T, R>(ha, Hb2, res2, lane, n1);
+            stg_load<T, R>(a1, A1, lane);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-              const T h = hb1[0][r] + tr_res_adj<T, R>(Hb2, res2, lane, n1, r);
-              const T y1 = A1[lane * RS + r];
+              const T h = hb1[0][r] + ha[r];
+              const T y1 = a1[r];
               part[r * 4] = fma(h * ((T)1 - y1 * y1), w1, part[r * 4]);
             }
           }
@@ -791,7 +871,6 @@ __global__ void __launch_bounds__(256, 1)
 k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__ xyz,
          const T* __restrict__ avg, const T* __restrict__ std_, const double* __restrict__ fbar,
          const double* __restrict__ vbar, TrNet<T> net, TrGeom g, TrLayout lay) {
-  constexpr int RS = R + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -840,12 +919,15 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
         __syncwarp();
         if (lane < n1) {
           const T w1 = W.W1[lane], b1 = W.b1[lane];
+          T v1[R], vt1[R];
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const T y = tr_tanh(fma(ss[r], w1, b1));
-            A1[lane * RS + r] = y;
-            At1[lane * RS + r] = ((T)1 - y * y) * (sd[r] * w1);
+            v1[r] = y;
+            vt1[r] = ((T)1 - y * y) * (sd[r] * w1);
           }
+          stg_store<T, R>(A1, lane, v1);
+          stg_store<T, R>(At1, lane, vt1);
         }
         __syncwarp();
         {
@@ -856,13 +938,17 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
             const int c = lane + 32 * j;
             if (c < n2) {
               const T bb = W.b2[c];
+              T rs[R], rt[R], v[R], vt[R];
+              tr_res_v<T, R>(rs, A1, res2, c, n1);
+              tr_res_v<T, R>(rt, At1, res2, c, n1);
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                A2[c * RS + r] = y + tr_res<T, R>(A1, res2, c, n1, r);
-                At2[c * RS + r] =
-                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, res2, c, n1, r);
+                v[r] = y + rs[r];
+                vt[r] = ((T)1 - y * y) * acd[j][r] + rt[r];
               }
+              stg_store<T, R>(A2, c, v);
+              stg_store<T, R>(At2, c, vt);
             }
           }
         }
@@ -875,12 +961,14 @@ k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__
             const int c = lane + 32 * j;
             if (c < n3) {
               const T bb = W.b3[c];
+              T rs[R], rt[R];
+              tr_res_v<T, R>(rs, A2, res3, c, n2);
+              tr_res_v<T, R>(rt, At2, res3, c, n2);
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                const T G = y + tr_res<T, R>(A2, res3, c, n2, r);
-                const T Gd =
-                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At2, res3, c, n2, r);
+                const T G = y + rs[r];
+                const T Gd = ((T)1 - y * y) * acd[j][r] + rt[r];
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
                   xd[a][j] = fma(rd[r * 4 + a], G, fma(rr[r * 4 + a], Gd, xd[a][j]));
@@ -940,7 +1028,6 @@ __global__ void __launch_bounds__(256, 1)
 k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard,
          const T* __restrict__ avg, const T* __restrict__ std_, const double* __restrict__ fbar,
          const double* __restrict__ vbar, TrNet<T> net, TrGeom g, TrLayout lay) {
-  constexpr int RS = R + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* tb = tr_tbase<T>(smem_raw, lay);
@@ -1015,12 +1102,15 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
         // forward and tangent of layers 1, 2
         if (lane < n1) {
           const T w1 = W.W1[lane], b1 = W.b1[lane];
+          T v1[R], vt1[R];
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const T y = tr_tanh(fma(ss[r], w1, b1));
-            A1[lane * RS + r] = y;
-            At1[lane * RS + r] = ((T)1 - y * y) * (sd[r] * w1);
+            v1[r] = y;
+            vt1[r] = ((T)1 - y * y) * (sd[r] * w1);
           }
+          stg_store<T, R>(A1, lane, v1);
+          stg_store<T, R>(At1, lane, vt1);
         }
         __syncwarp();
         {
@@ -1031,23 +1121,27 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
             const int c = lane + 32 * j;
             if (c < n2) {
               const T bb = W.b2[c];
+              T rs[R], rt[R], v[R], vt[R];
+              tr_res_v<T, R>(rs, A1, res2, c, n1);
+              tr_res_v<T, R>(rt, At1, res2, c, n1);
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
-                A2[c * RS + r] = y + tr_res<T, R>(A1, res2, c, n1, r);
-                At2[c * RS + r] =
-                    ((T)1 - y * y) * acd[j][r] + tr_res<T, R>(At1, res2, c, n1, r);
-                Zt2[c * RS + r] = acd[j][r];
+                v[r] = y + rs[r];
+                vt[r] = ((T)1 - y * y) * acd[j][r] + rt[r];
               }
+              stg_store<T, R>(A2, c, v);
+              stg_store<T, R>(At2, c, vt);
+              stg_store<T, R>(Zt2, c, acd[j]);
             }
           }
         }
         __syncwarp();
         // layer 3: forward, tangent and its adjoints
         T* Zb3 = big;
-        T* Zbt3 = big + n3 * RS;
-        T* Gb = big + 2 * n3 * RS;
-        T* Gbt = big + 3 * n3 * RS;
+        T* Zbt3 = big + n3 * R;
+        T* Gb = big + 2 * n3 * R;
+        T* Gbt = big + 3 * n3 * R;
         {
           T acc[TR_C3][R], acd[TR_C3][R];
           tr_gemv2<T, R, TR_C3>(acc, acd, A2, At2, n2, W.W3, sw3, n3, lane);
@@ -1057,6 +1151,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
             if (c < n3) {
               const T bb = W.b3[c];
               T zsum = (T)0;
+              T gv[R], gvt[R];
 #pragma unroll
               for (int r = 0; r < R; ++r) {
                 const T y = tr_tanh(acc[j][r] + bb);
@@ -1071,22 +1166,24 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
                 gbard *= mus[r];
                 const T zbd = gbard * q;
                 const T zb = (gbar - (T)2 * y * acd[j][r] * gbard) * q;
-                Zb3[c * RS + r] = zb;
-                Zbt3[c * RS + r] = zbd;
-                Gb[c * RS + r] = gbar;
-                Gbt[c * RS + r] = gbard;
+                gv[r] = gbar;
+                gvt[r] = gbard;
                 zsum += zb;
                 acc[j][r] = zb;   // reuse as z-bar
                 acd[j][r] = zbd;  // and z-bar of the tangent
               }
+              stg_store<T, R>(Zb3, c, acc[j]);
+              stg_store<T, R>(Zbt3, c, acd[j]);
+              stg_store<T, R>(Gb, c, gv);
+              stg_store<T, R>(Gbt, c, gvt);
               gb3[c] += zsum;
             }
           }
           // W3 gradient: sum_r A2[i][r] zb[c][r] + At2[i][r] zbd[c][r]
           for (int i = 0; i < n2; ++i) {
             T a[R], ad[R];
-            tr_load_col<T, R>(a, A2 + i * RS);
-            tr_load_col<T, R>(ad, At2 + i * RS);
+            tr_load_col<T, R>(a, A2, i);
+            tr_load_col<T, R>(ad, At2, i);
 #pragma unroll
             for (int j = 0; j < TR_C3; ++j) {
               const int c = lane + 32 * j;
@@ -1106,27 +1203,34 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
 #pragma unroll
         for (int j = 0; j < TR_C2; ++j) {
           const int i = lane + 32 * j;
-          T zsum = (T)0;
+          if (i < n2) {
+            T ga[R], gad[R], a2[R], rs[R], zt[R];
+            tr_res_adj_v<T, R>(ga, Gb, res3, i, n2);
+            tr_res_adj_v<T, R>(gad, Gbt, res3, i, n2);
+            stg_load<T, R>(a2, A2, i);
+            tr_res_v<T, R>(rs, A1, res2, i, n1);
+            stg_load<T, R>(zt, Zt2, i);
+            T zsum = (T)0;
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
-            if (i < n2) {
-              hb2[j][r] += tr_res_adj<T, R>(Gb, res3, i, n2, r);
-              hbd2[j][r] += tr_res_adj<T, R>(Gbt, res3, i, n2, r);
-              const T y = A2[i * RS + r] - tr_res<T, R>(A1, res2, i, n1, r);
+            for (int r = 0; r < R; ++r) {
+              hb2[j][r] += ga[r];
+              hbd2[j][r] += gad[r];
+              const T y = a2[r] - rs[r];
               const T q = (T)1 - y * y;
               zbd2[j][r] = hbd2[j][r] * q;
-              zb2[j][r] = (hb2[j][r] - (T)2 * y * Zt2[i * RS + r] * hbd2[j][r]) * q;
+              zb2[j][r] = (hb2[j][r] - (T)2 * y * zt[r] * hbd2[j][r]) * q;
               zsum += zb2[j][r];
-            } else {
-              zb2[j][r] = zbd2[j][r] = hb2[j][r] = hbd2[j][r] = (T)0;
             }
+            gb2[i] += zsum;
+          } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) zb2[j][r] = zbd2[j][r] = hb2[j][r] = hbd2[j][r] = (T)0;
           }
-          if (i < n2) gb2[i] += zsum;
         }
         for (int k = 0; k < n1; ++k) {
           T a[R], ad[R];
-          tr_load_col<T, R>(a, A1 + k * RS);
-          tr_load_col<T, R>(ad, At1 + k * RS);
+          tr_load_col<T, R>(a, A1, k);
+          tr_load_col<T, R>(ad, At1, k);
 #pragma unroll
           for (int j = 0; j < TR_C2; ++j) {
             const int i = lane + 32 * j;
@@ -1140,20 +1244,18 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
         }
         __syncwarp();
         T* Zb2 = big;
-        T* Zbd2 = big + n2 * RS;
-        T* Hb2 = big + 2 * n2 * RS;
-        T* Hbd2 = big + 3 * n2 * RS;
+        T* Zbd2 = big + n2 * R;
+        T* Hb2 = big + 2 * n2 * R;
+        T* Hbd2 = big + 3 * n2 * R;
 #pragma unroll
         for (int j = 0; j < TR_C2; ++j) {
           const int i = lane + 32 * j;
-          if (i < n2)
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              Zb2[i * RS + r] = zb2[j][r];
-              Zbd2[i * RS + r] = zbd2[j][r];
-              Hb2[i * RS + r] = hb2[j][r];
-              Hbd2[i * RS + r] = hbd2[j][r];
-            }
+          if (i < n2) {
+            stg_store<T, R>(Zb2, i, zb2[j]);
+            stg_store<T, R>(Zbd2, i, zbd2[j]);
+            stg_store<T, R>(Hb2, i, hb2[j]);
+            stg_store<T, R>(Hbd2, i, hbd2[j]);
+          }
         }
         __syncwarp();
         // layer 1, lanes over its channels
@@ -1163,11 +1265,15 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
           if (lane < n1) {
             const T w1 = W.W1[lane];
             T gws = (T)0, gbs = (T)0;
+            T ha[R], had[R], a1[R];
+            tr_res_adj_v<T, R>(ha, Hb2, res2, lane, n1);
+            tr_res_adj_v<T, R>(had, Hbd2, res2, lane, n1);
+            stg_load<T, R>(a1, A1, lane);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-              const T h = hb1[0][r] + tr_res_adj<T, R>(Hb2, res2, lane, n1, r);
-              const T hd = hbd1[0][r] + tr_res_adj<T, R>(Hbd2, res2, lane, n1, r);
-              const T y = A1[lane * RS + r];
+              const T h = hb1[0][r] + ha[r];
+              const T hd = hbd1[0][r] + had[r];
+              const T y = a1[r];
               const T q = (T)1 - y * y;
               const T zd = sd[r] * w1;
               const T zbd = hd * q;
@@ -1407,7 +1513,6 @@ enum TrKind { TR_FWD, TR_BWD, TR_TAN, TR_REV };
 
 template <typename T>
 static TrLayout tr_layout(TrKind kind, int R, const TrDims& d, bool wsmem, int nw) {
-  const int RS = R + 1;
   TrLayout L{};
   L.nw = nw;
   L.ints_warp = (d.nnei + TR_MAXT + 1 + 3) & ~3;
@@ -1438,21 +1543,21 @@ static TrLayout tr_layout(TrKind kind, int R, const TrDims& d, bool wsmem, int n
   o += R;
   o = (o + 3) & ~3;
   L.o_A1 = o;
-  o += d.n1 * RS;
+  o += d.n1 * R;
   L.o_At1 = o;
-  if (tan) o += d.n1 * RS;
+  if (tan) o += d.n1 * R;
   L.o_A2 = o;
-  o += d.n2 * RS;
+  o += d.n2 * R;
   L.o_At2 = o;
-  if (tan) o += d.n2 * RS;
+  if (tan) o += d.n2 * R;
   L.o_Zt2 = o;
-  if (kind == TR_REV) o += d.n2 * RS;
+  if (kind == TR_REV) o += d.n2 * R;
   o = (o + 3) & ~3;
   L.o_big = o;
   int big = 4 * d.n3;
-  if (kind == TR_BWD) big = std::max(2 * d.n3 * RS, 2 * d.n2 * RS);
+  if (kind == TR_BWD) big = std::max(2 * d.n3 * R, 2 * d.n2 * R);
   else if (kind == TR_TAN) big = 8 * d.n3;
-  else if (kind == TR_REV) big = std::max(4 * d.n3 * RS, 4 * d.n2 * RS);
+  else if (kind == TR_REV) big = std::max(4 * d.n3 * R, 4 * d.n2 * R);
   o += big;
   L.warp_sz = (o + 3) & ~3;
   return L;
