@@ -212,10 +212,18 @@ def run_repeated(args) -> None:
     torch.cuda.set_device(device)
     mdl, wl, tab = _load()
     rep = importlib.import_module("deepmd_kit_lr_pt_b200.repeated")
-    cfg = mdl.SeAConfig()
     coord, atype, box = wl.water_frame(args.n_side, seed=100)
-    params = mdl.init_params(cfg, seed=PARAM_SEED)
-    mdl.prepare(params, coord, atype, box, device=device)
+    if args.model == "c2":
+        # the compressed 3-species model of the batched workload (O, H, Cu;
+        # statistics and tables from every 16th of its 512 frames); its Cu
+        # net is not reached on water
+        cfg = mdl.SeAConfig(sel=(46, 92, 60))
+        params = mdl.init_params(cfg, seed=PARAM_SEED)
+        mdl.prepare_frames(params, wl.batched_frames(512, seed=0)[::16], device=device)
+    else:
+        cfg = mdl.SeAConfig()
+        params = mdl.init_params(cfg, seed=PARAM_SEED)
+        mdl.prepare(params, coord, atype, box, device=device)
     nloc = atype.size
     ev = mdl.SeAEvaluator(params, atype, box, mode="compressed", device=device, skin=args.skin)
     plain = mdl.SeAEvaluator(params, atype, box, mode="plain", device=device)
@@ -236,7 +244,9 @@ def run_repeated(args) -> None:
                                    f"rcut + {args.skin} A rebuilt every "
                                    f"{args.rebuild_every} steps",
                        "nloc": nloc, "sel": list(cfg.sel), "embedding": list(cfg.neuron),
-                       "fitting": list(cfg.fitting)},
+                       "fitting": list(cfg.fitting),
+                       "model": "3-species O/H/Cu model of the batched workload" if
+                       args.model == "c2" else "2-species water model, statistics from the frame"},
             "rebuilds": out["rebuilds"],
             "step_device_ms": {"mean": out["step_device_ms_mean"],
                                "max": out["step_device_ms_max"]},
@@ -806,6 +816,9 @@ def main() -> None:
                     help="frame count (batched: 512, train: 16)")
     ap.add_argument("--n-side", type=int, default=48,
                     help="repeated workload: oxygen grid per box side (48: 331,776 atoms)")
+    ap.add_argument("--model", choices=["water", "c2"], default="water",
+                    help="repeated workload: the 2-species water model or the 3-species "
+                         "model of the batched workload")
     ap.add_argument("--skin", type=float, default=2.0)
     ap.add_argument("--rebuild-every", type=int, default=10)
     ap.add_argument("--sigma", type=float, default=0.002)
