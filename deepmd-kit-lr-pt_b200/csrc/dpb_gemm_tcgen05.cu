@@ -19,12 +19,13 @@
 //   warps 2-5   split each A tile row by row (one row per thread) into TF32
 //               hi / lo and store both straight into one of ASLOTS tensor-
 //               memory slots, so the MMAs read A from TMEM and only B from
-//               shared memory; with FP32 weights they also split the B tile
-//               in shared memory (half the weight bytes from L2);
+//               shared memory;
+//   warps 6-9   with FP32 weights, split each B tile into TF32 hi / lo in
+//               shared memory (half the weight bytes from L2), else idle;
 //   warp 1      one elected lane issues tcgen05.mma (M=128, N=BN, K=8) into
 //               one of ACCBUF TMEM accumulators and commits to the ring's,
 //               the A slots' and the accumulator's mbarriers;
-//   warps 6..   EPIW epilogue warps (two per TMEM lane quadrant when EPIW = 8,
+//   warps 10..  EPIW epilogue warps (two per TMEM lane quadrant when EPIW = 8,
 //               splitting the columns): one row per thread, 16-byte loads /
 //               stores; with two accumulators the epilogue of one tile
 //               overlaps the next tile's MMAs.
@@ -53,7 +54,7 @@ template <int BN_, int STAGES_, int ASLOTS_, int ACCBUF_, int EPIW_>
 struct GemmCfg {
   static constexpr int BN = BN_, STAGES = STAGES_, ASLOTS = ASLOTS_, ACCBUF = ACCBUF_,
                        EPIW = EPIW_;
-  static constexpr int THREADS = 64 + 128 + 32 * EPIW;
+  static constexpr int THREADS = 64 + 128 + 128 + 32 * EPIW;
   static constexpr uint32_t ACC_STRIDE = BN <= 128 ? 128u : (uint32_t)((BN + 31) / 32 * 32);
   static constexpr uint32_t A0 = ACCBUF * ACC_STRIDE;
   static constexpr int A_BYTES = GT_BM * GT_BK * 4;  // 16 KB
@@ -274,7 +275,7 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
     abort_flag = 0;
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full_bar[s], 1);
-      mbar_init(&conv_bar[s], 128);
+      mbar_init(&conv_bar[s], shp.split_b ? 256 : 128);
       mbar_init(&empty_bar[s], 1);
     }
     for (int a = 0; a < ASLOTS; ++a) mbar_init(&afree_bar[a], 1);
@@ -417,9 +418,27 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
         tmem_st16(ta + 16u, hi + 16);
         tmem_st16(ta + 32u, lo);
         tmem_st16(ta + 48u, lo + 16);
-        if (shp.split_b) {
-          // B arrived in FP32 in the hi buffer: TF32 hi in place, lo into the
-          // lo buffer at the same (swizzled) offset; rows r and r + 128
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive(&conv_bar[s]);
+      }
+    }
+  } else if (warp < 10) {
+    // ------------------------------------- split FP32 B tiles into hi / lo
+    // (only with FP32 weights): TF32 hi in place, lo into the lo buffer at the
+    // same swizzled offset; rows r and r + 128 of the BN-row tile
+    if (shp.split_b) {
+      const int r = 32 * (warp - 6) + lane;
+      int g = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x) {
+        for (int kb = 0; kb < nk; ++kb, ++g) {
+          const int s = g % STAGES;
+          const uint32_t ph = (g / STAGES) & 1;
+          if (!mbar_wait(&full_bar[s], ph, abort)) {
+            ok = false;
+            break;
+          }
           unsigned char* bh = smem + s * STAGE_BYTES + A_BYTES;
           unsigned char* bl = bh + B_BYTES;
 #pragma unroll
@@ -440,10 +459,8 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
           }
           // generic-proxy writes, read next by the tensor cores (async proxy)
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive(&conv_bar[s]);
         }
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        mbar_arrive(&conv_bar[s]);
       }
     }
   } else {
@@ -452,7 +469,7 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
     // thread; each 16-column chunk moves as 4 x 16-byte loads / stores per
     // operand (64 contiguous bytes per thread and row)
     const int lane_base = 32 * (warp & 3);
-    const int ehalf = EPIW == 8 ? (warp - 6) >> 2 : 0;  // column share of this warp
+    const int ehalf = EPIW == 8 ? (warp - 10) >> 2 : 0;  // column share of this warp
     int lt = 0;
     for (int t = blockIdx.x; t < n_total; t += gridDim.x, ++lt) {
       const int b = lt % ACCBUF;

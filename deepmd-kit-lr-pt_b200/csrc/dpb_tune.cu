@@ -27,9 +27,9 @@ static Knob g_knobs[] = {
     // divides N; 240 only for K <= 512)
     {"fit_n_tile", 160, 3, {80, 160, 240}},
     // fitting GEMM weights: 0 pre-split TF32 hi / lo read from L2, 1 FP32
-    // read and split in shared memory by the kernel (half the weight bytes,
-    // but the split sits on the converter warps' path: 30% slower on the
-    // 12,288-atom water step)
+    // read and split in shared memory by four dedicated warps (half the
+    // weight bytes; 14% slower on the 12,288-atom water step: the GEMMs are
+    // not limited by the weight bytes)
     {"fit_split_b", 0, 2, {0, 1}},
     // warps (one center atom each) per CTA of the batched env / force kernels
     {"batch_atoms_per_cta", 4, 3, {2, 4, 8}},
