@@ -693,14 +693,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     achieved = per_atom_bytes[dom] * nloc / (ours[dom] * 1e-3) / 1e9
     # DRAM bytes per launch of the stage's kernel from the committed ncu capture
     # of this workload (profiles/ncu_dram_water12288.json)
-    kernel_of = {"env_mat": "dpb::k_env<double, float, 256, 4, 1>",
-                 "descriptor_fwd": "dpb::k_desc_fwd", "descriptor_bwd": "dpb::k_desc_bwd",
-                 "force_virial": "dpb::k_force_virial_rc<double, float>"}
+    # (matched on the name before its template arguments, which follow the
+    # tile shape the autotuner picked)
+    kernel_of = {"env_mat": "dpb::k_env", "descriptor_fwd": "dpb::k_desc_fwd",
+                 "descriptor_bwd": "dpb::k_desc_bwd", "force_virial": "dpb::k_force_virial_rc"}
     traffic = None
     dram_path = os.path.join(ROOT, "profiles", "ncu_dram_water12288.json")
     if nloc == 12288 and os.path.exists(dram_path):
         with open(dram_path) as f:
-            kd = json.load(f)["kernels"].get(kernel_of[dom])
+            kernels = json.load(f)["kernels"]
+        kd = next((v for k, v in kernels.items() if k.split("<")[0] == kernel_of[dom]), None)
         if kd:
             traffic = kd["dram_read_bytes"] + kd["dram_write_bytes"]
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
