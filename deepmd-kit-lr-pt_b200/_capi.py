@@ -92,6 +92,7 @@ _FUNCS = {
     "dpb_prod_virial_a_f32": "pppppp" "iiip",
     "dpb_copy_coord_async_f64": "ppppp" "L" "ppiifpp",
     "dpb_cell_grid_build_async_f64": "pLpipfp",
+    "dpb_geometry_cells_f64": "ppppp" "L" "p" "L" "ppiifppp",
     "dpb_se_a_pack_table_f32": "ppiip",
     "dpb_se_a_build_table_f64": "pppiipppipLp",
     "dpb_batch_env_mat_a_f32": "pppppppppp" "ppppp" "iiff" "pipp",
@@ -132,6 +133,7 @@ _FUNCS.update({"dpb_tune_count": "", "dpb_tune_get": "p", "dpb_tune_options": "p
 _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),
     "dpb_cell_grid_bytes": ("i", LL),
+    "dpb_geometry_scratch_bytes": ("ifp", LL),
     "dpb_build_nlist_scratch_bytes": ("ii", LL),
     "dpb_build_nlist_noalloc_max_bytes": ("", LL),
     "dpb_se_a_build_table_scratch_bytes": ("ii", LL),

@@ -22,6 +22,7 @@ enum : int {
   ST_ROW_CAPACITY = 1 << 3,    // build_nlist row longer than mem_size
   ST_CELL_RANGE = 1 << 4,      // ghost/cell index outside the cell grid
   ST_TYPE_RANGE = 1 << 5,      // center type >= ntypes (no avg/std row)
+  ST_SYNC_TIMEOUT = 1 << 6,    // a grid-wide barrier of a cooperative kernel timed out
 };
 
 void set_error(const char* fmt, ...);

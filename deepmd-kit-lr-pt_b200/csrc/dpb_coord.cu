@@ -77,13 +77,10 @@ __device__ __forceinline__ void dev_tt_dot_v(double* o, const double* t,
 
 // ------------------------------------------------------------ normalize ----
 
+// source/lib/src/coord.cc:14-27: inter = rec.p, fmod(.,1), +1 if < 0, back
+// to physical. Region arithmetic runs in T like the reference.
 template <typename T>
-__global__ void k_normalize(T* coord, int natom, HostRegion r) {
-  // source/lib/src/coord.cc:14-27: inter = rec.p, fmod(.,1), +1 if < 0,
-  // back to physical. Region arithmetic runs in T like the reference.
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= natom) return;
-  T p[3] = {coord[3 * i], coord[3 * i + 1], coord[3 * i + 2]};
+__device__ __forceinline__ void normalize_point(T* q, const T* p, const HostRegion& r) {
   T ri[3];
   for (int d = 0; d < 3; ++d) {
     ri[d] = add_rn(add_rn(mul_rn(p[0], (T)r.rec[3 * d]), mul_rn(p[1], (T)r.rec[3 * d + 1])),
@@ -92,9 +89,19 @@ __global__ void k_normalize(T* coord, int natom, HostRegion r) {
     if (ri[d] < (T)0.) ri[d] = add_rn(ri[d], (T)1.);
   }
   for (int d = 0; d < 3; ++d) {
-    coord[3 * i + d] = add_rn(add_rn(mul_rn(ri[0], (T)r.box[d]), mul_rn(ri[1], (T)r.box[3 + d])),
-                              mul_rn(ri[2], (T)r.box[6 + d]));
+    q[d] = add_rn(add_rn(mul_rn(ri[0], (T)r.box[d]), mul_rn(ri[1], (T)r.box[3 + d])),
+                  mul_rn(ri[2], (T)r.box[6 + d]));
   }
+}
+
+template <typename T>
+__global__ void k_normalize(T* coord, int natom, HostRegion r) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natom) return;
+  T p[3] = {coord[3 * i], coord[3 * i + 1], coord[3 * i + 2]};
+  T q[3];
+  normalize_point(q, p, r);
+  for (int d = 0; d < 3; ++d) coord[3 * i + d] = q[d];
 }
 
 // ------------------------------------------------------------ copy_coord ---
@@ -125,15 +132,9 @@ static CopyScratch carve_copy(void* p, int nloc, const HostRegion& r) {
   return s;
 }
 
-template <typename T>
-__global__ void k_cc_cell(CopyScratch s, T* out_c, int* out_t, int* mapping,
-                          const T* in_c, const int* in_t, int nloc,
-                          int mem_nall, HostRegion r) {
-  // cell of each local atom as build_clist computes it
-  // (source/lib/src/neighbor_list.cc:84-111, nat_stt = 0, nat_end = ncell)
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nloc) return;
-  double p[3] = {(double)in_c[3 * i], (double)in_c[3 * i + 1], (double)in_c[3 * i + 2]};
+// Cell of a local atom as build_clist computes it
+// (source/lib/src/neighbor_list.cc:84-111, nat_stt = 0, nat_end = ncell).
+__device__ __forceinline__ int copy_cell_of(const double* p, const HostRegion& r) {
   double inter[3];
   dev_t_dot_v(inter, r.rec, p);
   int idx[3];
@@ -144,7 +145,17 @@ __global__ void k_cc_cell(CopyScratch s, T* out_c, int* out_t, int* mapping,
     if (idx[d] < 0) idx[d] = 0;
     else if (idx[d] >= r.nc[d]) idx[d] = r.nc[d] - 1;
   }
-  int c = (idx[0] * r.nc[1] + idx[1]) * r.nc[2] + idx[2];
+  return (idx[0] * r.nc[1] + idx[1]) * r.nc[2] + idx[2];
+}
+
+template <typename T>
+__global__ void k_cc_cell(CopyScratch s, T* out_c, int* out_t, int* mapping,
+                          const T* in_c, const int* in_t, int nloc,
+                          int mem_nall, HostRegion r) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nloc) return;
+  double p[3] = {(double)in_c[3 * i], (double)in_c[3 * i + 1], (double)in_c[3 * i + 2]};
+  int c = copy_cell_of(p, r);
   s.cell_of[i] = c;
   atomicAdd(&s.cnt[c], 1);
   if (i < mem_nall) {
@@ -451,17 +462,19 @@ __global__ void k_grid_bbox(GridHeader* h, const T* coord, int nall,
   }
 }
 
-__global__ void k_grid_setup(GridHeader* h, float rcut, int max_cells,
-                             int nall, const int* nall_dev) {
-  // cells of edge >= rcut * (1 + 1e-4) over the bounding box, so that every
-  // pair closer than rcut lies in adjacent cells whatever the rounding
-  int n = nall_dev ? min(*nall_dev, nall) : nall;
+// Cells of edge >= rcut * (1 + 1e-4) over the bounding box [kmin, kmax] of n
+// points, so that every pair closer than rcut lies in adjacent cells whatever
+// the rounding; the dimensions are halved until at most max_cells remain.
+__device__ __forceinline__ void grid_setup_from_keys(GridHeader& h,
+                                                     const unsigned long long* kmin,
+                                                     const unsigned long long* kmax, int n,
+                                                     float rcut, int max_cells) {
   double edge = (double)rcut * 1.0001;
   int dims[3];
   double lo[3], ext[3];
   for (int d = 0; d < 3; ++d) {
-    lo[d] = n > 0 ? ord_val(h->kmin[d]) : 0.;
-    double hi = n > 0 ? ord_val(h->kmax[d]) : 0.;
+    lo[d] = n > 0 ? ord_val(kmin[d]) : 0.;
+    double hi = n > 0 ? ord_val(kmax[d]) : 0.;
     ext[d] = hi - lo[d];
     dims[d] = (int)(ext[d] / edge);
     if (dims[d] < 1) dims[d] = 1;
@@ -470,13 +483,27 @@ __global__ void k_grid_setup(GridHeader* h, float rcut, int max_cells,
     for (int d = 0; d < 3; ++d) dims[d] = dims[d] > 1 ? (dims[d] + 1) / 2 : 1;
   }
   for (int d = 0; d < 3; ++d) {
-    h->dims[d] = dims[d];
-    h->origin[d] = lo[d];
+    h.dims[d] = dims[d];
+    h.origin[d] = lo[d];
     double cs = ext[d] / dims[d];
-    h->inv_cs[d] = cs > 0. ? 1. / cs : 0.;
+    h.inv_cs[d] = cs > 0. ? 1. / cs : 0.;
   }
-  h->ncells = dims[0] * dims[1] * dims[2];
-  h->natoms = n;
+  h.ncells = dims[0] * dims[1] * dims[2];
+  h.natoms = n;
+}
+
+__global__ void k_grid_setup(GridHeader* h, float rcut, int max_cells,
+                             int nall, const int* nall_dev) {
+  int n = nall_dev ? min(*nall_dev, nall) : nall;
+  GridHeader v;
+  grid_setup_from_keys(v, h->kmin, h->kmax, n, rcut, max_cells);
+  for (int d = 0; d < 3; ++d) {
+    h->dims[d] = v.dims[d];
+    h->origin[d] = v.origin[d];
+    h->inv_cs[d] = v.inv_cs[d];
+  }
+  h->ncells = v.ncells;
+  h->natoms = v.natoms;
 }
 
 template <typename T>
@@ -563,6 +590,451 @@ int grid_build(void* grid, long long bytes, const T* coord, int nall,
   k_grid_fill<<<na, 256, 0, st>>>(g);
   DPB_CHECK_LAUNCH("cell grid/fill");
   return DPB_OK;
+}
+
+// ------------------------------------------------- fused geometry pass ----
+// normalize_coord + copy_coord + cell grid of one frame as ONE cooperative
+// launch (one 512-thread block per SM). The separate path above takes twelve
+// small launches and three memsets, each a few microseconds of latency for a
+// few hundred kilobytes of work; here the phases are separated by four
+// grid-wide barriers instead:
+//   P0 local atoms: wrap into the box, copy-grid cell and a slot in it
+//      (atomic count), local part of the extended arrays, bounding box keys
+//   P1 every block scans the copy-cell counts in its own shared memory (no
+//      single-block scan to wait for); atoms placed by cell; ghost offsets in
+//      the reference's ghost loop order scanned the same way
+//   P2 one warp per ghost cell: the source cell's atoms ranked by index in
+//      registers or shared memory (copy_coord_cpu's ascending order), ghost
+//      coordinates / types / mapping, bounding box keys
+//   P3 every block derives the cell grid from the bounding box; atoms counted
+//      per grid cell (atomic slot)
+//   P4 every block scans the grid-cell counts; block 0 publishes the cell
+//      starts and the grid header; atoms written in cell order.
+// The results equal the separate path's bit for bit (extended coordinates,
+// types, mapping, nall, grid header, cell starts, cell of every atom); only
+// the order of atoms inside a grid cell may differ, which the neighbor
+// search does not depend on (its keys are sorted).
+//
+// Barriers wait at most GEO_WAIT_NS; a block that gives up sets
+// ST_SYNC_TIMEOUT in the status word and returns. Block 0 writes an empty
+// grid header in P0 and the real one only in P4, so a pass that gave up
+// leaves a grid in which the neighbor search finds nothing, never one that
+// points outside its arrays.
+
+constexpr int GEO_THREADS = 512;
+constexpr int GEO_SCAN_CAP = 32768;  // ints of the block-local scans
+constexpr int GEO_SORT_CAP = 256;    // per-warp buffer of one cell's atoms
+constexpr unsigned long long GEO_WAIT_NS = 200000000ull;  // per barrier
+
+struct GeoHeader {
+  unsigned int arrive;  // barrier arrivals, zeroed before the launch
+  unsigned int pad;
+  unsigned long long kmin_inv[3];  // max of ~key, i.e. ~(min key)
+  unsigned long long kmax[3];
+};
+
+struct GeoArgs {
+  double* cext;
+  int* text;
+  int* mapping;
+  int* nall_dev;
+  GeoHeader* hdr;
+  int* cnt;      // [nloc_cells] copy-cell counts, zeroed before the launch
+  int* cell_of;  // [nloc] copy cell of each local atom
+  int* slot;     // [nloc] slot inside it
+  int* order;    // [nloc] local atoms by copy cell
+  GridView g;
+  int gcap;       // grid cells at most (<= g.max_cells, <= GEO_SCAN_CAP)
+  int scan_ints;  // shared ints of the scans
+  const double* coord;
+  const int* atype;
+  int nloc, mem_nall;
+  float rcut;
+  int* status;
+  HostRegion r;
+};
+
+static long long geo_scratch_bytes(int nloc, const HostRegion& r) {
+  const long long fused = 256 + 4LL * ((r.nloc_cells + 1) + 3LL * nloc) + 256;
+  const long long sep = copy_scratch_ints(nloc, r) * (long long)sizeof(int);
+  return fused > sep ? fused : sep;
+}
+
+__device__ __forceinline__ unsigned long long geo_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier number k (targets k * gridDim.x arrivals). Returns false
+// in every thread of a block that gave up waiting.
+__device__ bool geo_sync(const GeoArgs& a, unsigned k, int* s_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned target = k * gridDim.x;
+    __threadfence();
+    atomicAdd(&a.hdr->arrive, 1u);
+    int ok = 1;
+    if (ld_acquire_u32(&a.hdr->arrive) < target) {
+      const unsigned long long t0 = geo_clock();
+      unsigned it = 0;
+      while (ld_acquire_u32(&a.hdr->arrive) < target) {
+        if (++it > (1u << 24) || geo_clock() - t0 > GEO_WAIT_NS) {
+          atomicOr(a.status, ST_SYNC_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+// Exclusive prefix sum of s[0, n) in shared memory, in place, by the whole
+// block (each thread a contiguous run); returns the total.
+__device__ int geo_scan(int* s, int n, int* s_warp) {
+  __syncthreads();
+  const int T = blockDim.x, t = threadIdx.x, lane = t & 31, wid = t >> 5, nw = T >> 5;
+  const int k = (n + T - 1) / T;
+  const int lo = min(n, t * k), hi = min(n, lo + k);
+  int sum = 0;
+  for (int j = lo; j < hi; ++j) sum += s[j];
+  int x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = lane < nw ? s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    s_warp[lane] = w;
+  }
+  __syncthreads();
+  int run = (wid > 0 ? s_warp[wid - 1] : 0) + x - sum;
+  for (int j = lo; j < hi; ++j) {
+    const int v = s[j];
+    s[j] = run;
+    run += v;
+  }
+  const int total = s_warp[nw - 1];
+  __syncthreads();
+  return total;
+}
+
+__global__ void __launch_bounds__(GEO_THREADS, 1) k_geometry(GeoArgs a) {
+  extern __shared__ int geo_smem[];
+  __shared__ int s_warp[32];
+  __shared__ int s_ok;
+  __shared__ unsigned long long s_red[GEO_THREADS / 32][6];
+  int* s_scan = geo_smem;
+  int* s_sort = geo_smem + a.scan_ints;
+  const HostRegion& r = a.r;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  unsigned long long kmn[3] = {0ull, 0ull, 0ull}, kmx[3] = {0ull, 0ull, 0ull};
+  auto bbox = [&](const double* q) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const unsigned long long k = ord_key(q[d]);
+      kmn[d] = max(kmn[d], ~k);
+      kmx[d] = max(kmx[d], k);
+    }
+  };
+
+  // ---- P0: local atoms
+  for (int i = tid; i < a.nloc; i += nthr) {
+    const double p[3] = {a.coord[3 * i], a.coord[3 * i + 1], a.coord[3 * i + 2]};
+    double q[3];
+    normalize_point(q, p, r);
+    const int c = copy_cell_of(q, r);
+    a.cell_of[i] = c;
+    a.slot[i] = atomicAdd(&a.cnt[c], 1);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) a.cext[3 * i + d] = q[d];
+    a.text[i] = a.atype[i];
+    a.mapping[i] = i;
+    bbox(q);
+  }
+  for (int c = tid; c < a.gcap; c += nthr) a.g.fill[c] = 0;
+  if (tid == 0) {
+    GridHeader* h = a.g.h;
+    for (int d = 0; d < 3; ++d) {
+      h->dims[d] = 1;
+      h->origin[d] = 0.;
+      h->inv_cs[d] = 0.;
+    }
+    h->ncells = 1;
+    h->natoms = 0;
+    a.g.cell_start[0] = 0;
+    a.g.cell_start[1] = 0;
+  }
+  if (!geo_sync(a, 1, &s_ok)) return;
+
+  // ---- P1: copy-cell starts, local atoms by cell, ghost offsets
+  const int ncl = r.nloc_cells, nce = r.next_cells;
+  int* s_cs = s_scan;             // [ncl + 1]
+  int* s_ext = s_scan + ncl + 1;  // [nce + 1]
+  for (int j = threadIdx.x; j < ncl; j += blockDim.x) s_cs[j] = __ldcg(a.cnt + j);
+  if (threadIdx.x == 0) s_cs[ncl] = 0;
+  geo_scan(s_cs, ncl + 1, s_warp);
+  for (int i = tid; i < a.nloc; i += nthr) a.order[s_cs[a.cell_of[i]] + a.slot[i]] = i;
+  for (int e = threadIdx.x; e < nce; e += blockDim.x) {
+    int ii[3];
+    ext_cell_coords(e, r, ii);
+    int v = 0;
+    if (!(ii[0] >= 0 && ii[0] < r.nc[0] && ii[1] >= 0 && ii[1] < r.nc[1] && ii[2] >= 0 &&
+          ii[2] < r.nc[2])) {
+      int jj[3];
+      for (int d = 0; d < 3; ++d) jj[d] = ii[d] + pbc_shift(ii[d], r.nc[d]) * r.nc[d];
+      const int c = (jj[0] * r.nc[1] + jj[1]) * r.nc[2] + jj[2];
+      v = s_cs[c + 1] - s_cs[c];
+    }
+    s_ext[e] = v;
+  }
+  if (threadIdx.x == 0) s_ext[nce] = 0;
+  const int nall = a.nloc + geo_scan(s_ext, nce + 1, s_warp);
+  if (tid == 0) *a.nall_dev = nall;
+  if (!geo_sync(a, 2, &s_ok)) return;
+
+  // ---- P2: ghosts, one warp per extended cell
+  for (int e = blockIdx.x * nwb + wid; e < nce; e += gridDim.x * nwb) {
+    int ii[3];
+    ext_cell_coords(e, r, ii);
+    if (ii[0] >= 0 && ii[0] < r.nc[0] && ii[1] >= 0 && ii[1] < r.nc[1] && ii[2] >= 0 &&
+        ii[2] < r.nc[2])
+      continue;
+    int jj[3];
+    double ps[3];
+    for (int d = 0; d < 3; ++d) {
+      const int sh = pbc_shift(ii[d], r.nc[d]);
+      ps[d] = (double)sh;
+      jj[d] = ii[d] + sh * r.nc[d];
+    }
+    double sv[3];
+    dev_tt_dot_v(sv, r.box, ps);
+    const int c = (jj[0] * r.nc[1] + jj[1]) * r.nc[2] + jj[2];
+    const int b = s_cs[c], n = s_cs[c + 1] - b, w0 = a.nloc + s_ext[e];
+    auto emit = [&](int w, int p) {
+      if (w < a.mem_nall) {
+        double q[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          q[d] = sub_rn(__ldcg(a.cext + 3 * p + d), sv[d]);
+          a.cext[3 * w + d] = q[d];
+        }
+        a.text[w] = a.atype[p];
+        a.mapping[w] = p;
+        bbox(q);
+      }
+    };
+    if (n <= 32) {
+      const int v = lane < n ? __ldcg(a.order + b + lane) : 0x7fffffff;
+      int rank = 0;
+      for (int q = 0; q < n; ++q) rank += __shfl_sync(0xffffffffu, v, q) < v ? 1 : 0;
+      if (lane < n) emit(w0 + rank, v);
+    } else if (n <= GEO_SORT_CAP) {
+      int* buf = s_sort + wid * GEO_SORT_CAP;
+      for (int k = lane; k < n; k += 32) buf[k] = __ldcg(a.order + b + k);
+      __syncwarp();
+      for (int k = lane; k < n; k += 32) {
+        const int x = buf[k];
+        int rank = 0;
+        for (int q = 0; q < n; ++q) rank += buf[q] < x ? 1 : 0;
+        emit(w0 + rank, x);
+      }
+      __syncwarp();
+    } else {
+      for (int k = lane; k < n; k += 32) {
+        const int x = __ldcg(a.order + b + k);
+        int rank = 0;
+        for (int q = 0; q < n; ++q) rank += __ldcg(a.order + b + q) < x ? 1 : 0;
+        emit(w0 + rank, x);
+      }
+    }
+  }
+  // bounding box of this block's atoms: warp, then block, one atomic per key
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      kmn[d] = max(kmn[d], __shfl_xor_sync(0xffffffffu, kmn[d], o));
+      kmx[d] = max(kmx[d], __shfl_xor_sync(0xffffffffu, kmx[d], o));
+    }
+    if (lane == 0) {
+      s_red[wid][d] = kmn[d];
+      s_red[wid][3 + d] = kmx[d];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    unsigned long long m = 0ull;
+    for (int w = 0; w < nwb; ++w) m = max(m, s_red[w][threadIdx.x]);
+    if (m) {
+      unsigned long long* dst = threadIdx.x < 3 ? &a.hdr->kmin_inv[threadIdx.x]
+                                                : &a.hdr->kmax[threadIdx.x - 3];
+      atomicMax(dst, m);
+    }
+  }
+  if (!geo_sync(a, 3, &s_ok)) return;
+
+  // ---- P3: cell grid over the extended atoms; counts per grid cell
+  const int n = min(nall, a.mem_nall);
+  unsigned long long kmin[3], kmax[3];
+  for (int d = 0; d < 3; ++d) {
+    kmin[d] = ~__ldcg(&a.hdr->kmin_inv[d]);
+    kmax[d] = __ldcg(&a.hdr->kmax[d]);
+  }
+  GridHeader gh;
+  grid_setup_from_keys(gh, kmin, kmax, n, a.rcut, a.gcap);
+  int* gslot = a.g.redo + 1;  // the neighbor search zeroes redo[0] before use
+  for (int i = tid; i < n; i += nthr) {
+    const double q[3] = {__ldcg(a.cext + 3 * i), __ldcg(a.cext + 3 * i + 1),
+                         __ldcg(a.cext + 3 * i + 2)};
+    const int c = grid_cell_of(gh, q);
+    a.g.cell_of[i] = c;
+    gslot[i] = atomicAdd(&a.g.fill[c], 1);
+  }
+  if (!geo_sync(a, 4, &s_ok)) return;
+
+  // ---- P4: grid cell starts; atoms in cell order
+  const int ncg = gh.ncells;
+  for (int j = threadIdx.x; j < ncg; j += blockDim.x) s_scan[j] = __ldcg(a.g.fill + j);
+  if (threadIdx.x == 0) s_scan[ncg] = 0;
+  geo_scan(s_scan, ncg + 1, s_warp);
+  if (blockIdx.x == 0) {
+    for (int j = threadIdx.x; j <= ncg; j += blockDim.x) a.g.cell_start[j] = s_scan[j];
+    if (threadIdx.x == 0) {
+      GridHeader* h = a.g.h;
+      for (int d = 0; d < 3; ++d) {
+        h->kmin[d] = kmin[d];
+        h->kmax[d] = kmax[d];
+        h->dims[d] = gh.dims[d];
+        h->origin[d] = gh.origin[d];
+        h->inv_cs[d] = gh.inv_cs[d];
+      }
+      h->ncells = gh.ncells;
+      h->natoms = gh.natoms;
+    }
+  }
+  for (int i = tid; i < n; i += nthr) a.g.cell_atoms[s_scan[a.g.cell_of[i]] + gslot[i]] = i;
+}
+
+// normalize_coord + copy_coord + cell grid of one frame. The fused pass runs
+// when the copy grid's cells fit its block-local scans and the device can
+// hold one block per SM; otherwise the separate kernels run (normalized
+// coordinates written straight into the extended array).
+int geometry_cells(double* cext, int* text, int* mapping, int* nall_dev, void* grid,
+                   long long gbytes, void* scratch, long long sbytes, const double* coord,
+                   const int* atype, int nloc, int mem_nall, float rcut, const double* boxt,
+                   int* status, cudaStream_t st) {
+  if (nloc < 0 || mem_nall < nloc || !(rcut > 0.f) || nall_dev == nullptr ||
+      status == nullptr || (nloc > 0 && (!cext || !text || !mapping || !coord || !atype))) {
+    set_error("geometry_cells: invalid arguments (nloc=%d mem_nall=%d rcut=%g; mem_nall "
+              ">= nloc, nall_dev and status required)", nloc, mem_nall, (double)rcut);
+    return DPB_ERR_INVALID;
+  }
+  HostRegion r;
+  host_region(r, boxt, rcut);
+  if (!(r.volume > 0.)) {
+    set_error("geometry_cells: the box has zero volume");
+    return DPB_ERR_INVALID;
+  }
+  const long long need = geo_scratch_bytes(nloc, r);
+  if (scratch == nullptr || sbytes < need) {
+    set_error("geometry_cells: scratch too small (%lld < %lld bytes)", sbytes, need);
+    return DPB_ERR_INVALID;
+  }
+  if (grid == nullptr || gbytes < grid_bytes(mem_nall)) {
+    set_error("geometry_cells: grid buffer too small (%lld < %lld bytes)", gbytes,
+              grid_bytes(mem_nall));
+    return DPB_ERR_INVALID;
+  }
+  GridView g = carve_grid(grid, mem_nall);
+  const int gcap = g.max_cells < GEO_SCAN_CAP ? g.max_cells : GEO_SCAN_CAP;
+  const long long copy_ints = (long long)r.nloc_cells + r.next_cells + 2;
+  bool fused = nloc > 0 && copy_ints <= GEO_SCAN_CAP && tune_value("geometry_fused", 1) != 0;
+  if (fused) {
+    const int scan_ints = (int)(copy_ints > gcap + 1 ? copy_ints : gcap + 1);
+    const size_t smem = (size_t)scan_ints * 4 + (size_t)(GEO_THREADS / 32) * GEO_SORT_CAP * 4;
+    static unsigned long long attr_devs = 0;  // devices whose limit is raised
+    int dev = 0;
+    DPB_CUDA(cudaGetDevice(&dev), "geometry_cells");
+    if (dev < 64 && !(attr_devs >> dev & 1ull)) {
+      const int most = GEO_SCAN_CAP * 4 + (GEO_THREADS / 32) * GEO_SORT_CAP * 4;
+      DPB_CUDA(cudaFuncSetAttribute(k_geometry, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    most),
+               "geometry_cells");
+      attr_devs |= 1ull << dev;
+    }
+    int occ = 0;
+    DPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_geometry, GEO_THREADS,
+                                                           smem),
+             "geometry_cells");
+    if (occ >= 1) {
+      char* p = (char*)scratch;
+      GeoArgs a;
+      a.cext = cext;
+      a.text = text;
+      a.mapping = mapping;
+      a.nall_dev = nall_dev;
+      a.hdr = (GeoHeader*)p;
+      a.cnt = (int*)(p + 256);
+      a.cell_of = a.cnt + r.nloc_cells + 1;
+      a.slot = a.cell_of + nloc;
+      a.order = a.slot + nloc;
+      a.g = g;
+      a.gcap = gcap;
+      a.scan_ints = scan_ints;
+      a.coord = coord;
+      a.atype = atype;
+      a.nloc = nloc;
+      a.mem_nall = mem_nall;
+      a.rcut = rcut;
+      a.status = status;
+      a.r = r;
+      DPB_CUDA(cudaMemsetAsync(scratch, 0, 256 + sizeof(int) * (size_t)r.nloc_cells, st),
+               "geometry_cells");
+      void* args[] = {&a};
+      DPB_CUDA(cudaLaunchCooperativeKernel((const void*)k_geometry, dim3(sm_count()),
+                                           dim3(GEO_THREADS), args, smem, st),
+               "geometry_cells");
+      return DPB_OK;
+    }
+  }
+  if (nloc > 0) {
+    DPB_CUDA(cudaMemcpyAsync(cext, coord, sizeof(double) * 3 * (size_t)nloc,
+                             cudaMemcpyDeviceToDevice, st),
+             "geometry_cells");
+    k_normalize<double><<<ceil_div(nloc, 256), 256, 0, st>>>(cext, nloc, r);
+    DPB_CHECK_LAUNCH("geometry_cells/normalize");
+  }
+  int rc = copy_coord_async<double>(cext, text, mapping, nall_dev, scratch, sbytes, cext,
+                                    atype, nloc, mem_nall, rcut, boxt, st);
+  if (rc != DPB_OK) return rc;
+  return grid_build<double>(grid, gbytes, cext, mem_nall, nall_dev, rcut, st);
+}
+
+long long geometry_scratch_bytes(int nloc, float rcut, const double* boxt) {
+  HostRegion r;
+  host_region(r, boxt, rcut);
+  return geo_scratch_bytes(nloc, r);
 }
 
 template int grid_build<double>(void*, long long, const double*, int, const int*, float, cudaStream_t);
@@ -703,6 +1175,20 @@ int dpb_copy_coord_f32(float* out_c, int* out_t, int* mapping, int* nall,
 }
 
 long long dpb_cell_grid_bytes(int nall) { return grid_bytes(nall); }
+
+long long dpb_geometry_scratch_bytes(int nloc, float rcut, const double* boxt) {
+  return geometry_scratch_bytes(nloc, rcut, boxt);
+}
+
+int dpb_geometry_cells_f64(double* cext, int* text, int* mapping, int* nall_dev, void* grid,
+                           long long grid_bytes_, void* scratch, long long scratch_bytes,
+                           const double* coord, const int* atype, int nloc, int mem_nall,
+                           float rcut, const double* boxt, int* status,
+                           dpb_stream_t stream) {
+  return geometry_cells(cext, text, mapping, nall_dev, grid, grid_bytes_, scratch,
+                        scratch_bytes, coord, atype, nloc, mem_nall, rcut, boxt, status,
+                        as_stream(stream));
+}
 
 int dpb_cell_grid_build_f64(void* grid, long long grid_bytes_, const double* coord,
                             int nall, float rcut, dpb_stream_t stream) {

@@ -48,6 +48,10 @@ int dpb_status_check(const int* status, dpb_stream_t stream) {
         "row buffer holds (status 0x%x)", h);
     return DPB_ERR_NLIST_CAPACITY;
   }
+  if (h & dpb::ST_SYNC_TIMEOUT) {
+    dpb::set_error("a grid-wide barrier of the geometry pass timed out (status 0x%x)", h);
+    return DPB_ERR_CUDA;
+  }
   if (h & (1 << 8)) {
     dpb::set_error("a tensor-core GEMM timed out waiting on its pipeline (status 0x%x)", h);
     return DPB_ERR_CUDA;

@@ -38,6 +38,9 @@ static Knob g_knobs[] = {
     // most warps per CTA of the training kernels (fewer when shared memory
     // does not allow them)
     {"train_warps_per_cta", 8, 4, {1, 2, 4, 8}},
+    // one frame's wrap / ghost copy / cell grid: 1 one cooperative launch,
+    // 0 the separate kernels
+    {"geometry_fused", 1, 2, {0, 1}},
 };
 
 static Knob* find_knob(const char* name) {

@@ -449,6 +449,9 @@ class SeAEvaluator:
         self.mapping = torch.zeros(self.mem_nall, dtype=torch.int32, device=dev)
         self.nall_dev = torch.zeros(1, dtype=torch.int32, device=dev)
         self.copy_scratch = torch.empty(self.copy_bytes, dtype=torch.uint8, device=dev)
+        self.geo_bytes = int(lib.dpb_geometry_scratch_bytes(
+            nloc, ctypes.c_float(cfg.rcut), self.box.ctypes.data))
+        self.geo_scratch = torch.empty(self.geo_bytes, dtype=torch.uint8, device=dev)
         self.grid = torch.empty(self.grid_bytes, dtype=torch.uint8, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.avg = torch.tensor(params.davg, dtype=fdt, device=dev)
@@ -603,18 +606,13 @@ class SeAEvaluator:
                      self.mem_nall, 1, ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth),
                      self.sec.ctypes.data, self.sec.size, ptr(self.status), s)
         else:
-            with tm("coord"):
-                self.coord_n.copy_(self.coord)
-                call("dpb_normalize_coord_f64", ptr(self.coord_n), nloc, self.box.ctypes.data,
-                     s)
-                call("dpb_copy_coord_async_f64", ptr(self.cext), ptr(self.text),
-                     ptr(self.mapping), ptr(self.nall_dev), ptr(self.copy_scratch),
-                     self.copy_bytes, ptr(self.coord_n), ptr(self.atype), nloc, self.mem_nall,
-                     ctypes.c_float(cfg.rcut), self.box.ctypes.data, s)
-            with tm("cell_grid"):
-                call("dpb_cell_grid_build_async_f64", ptr(self.grid), self.grid_bytes,
-                     ptr(self.cext), self.mem_nall, ptr(self.nall_dev),
-                     ctypes.c_float(cfg.rcut), s)
+            with tm("geometry"):
+                # wrap into the box, ghosts, cell grid: one cooperative launch
+                call("dpb_geometry_cells_f64", ptr(self.cext), ptr(self.text),
+                     ptr(self.mapping), ptr(self.nall_dev), ptr(self.grid), self.grid_bytes,
+                     ptr(self.geo_scratch), self.geo_bytes, ptr(self.coord), ptr(self.atype),
+                     nloc, self.mem_nall, ctypes.c_float(cfg.rcut), self.box.ctypes.data,
+                     ptr(self.status), s)
             env = "dpb_env_mat_a_cells_mixed" if self.mode == "compressed" else \
                 "dpb_env_mat_a_cells_f64"
             with tm("env_mat"):

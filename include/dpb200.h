@@ -310,6 +310,23 @@ DPB_API int dpb_cell_grid_build_async_f64(void* grid, long long grid_bytes,
                                           const double* coord, int mem_nall,
                                           const int* nall_dev, float rcut,
                                           dpb_stream_t stream);
+/* One frame's normalize_coord (coord.cc:14-27) + copy_coord (coord.cc:29-64)
+ * + cell grid in one call, replacing dpb_normalize_coord_f64 on a copy of
+ * `coord`, dpb_copy_coord_async_f64 and dpb_cell_grid_build_async_f64 (the
+ * same cext / atype_ext / mapping / *nall_dev, bit for bit, and the same grid;
+ * `coord` is read only). Runs as one cooperative launch with grid-wide
+ * barriers when the copy grid's cells fit (nloc_cells + next_cells <= 32766),
+ * else as the separate kernels. mem_nall >= nloc; scratch of
+ * dpb_geometry_scratch_bytes(nloc, rcut, box); grid of
+ * dpb_cell_grid_bytes(mem_nall); status: device int (a barrier that timed
+ * out sets a bit there and leaves an empty grid). Knob geometry_fused = 0
+ * forces the separate kernels. */
+DPB_API long long dpb_geometry_scratch_bytes(int nloc, float rcut, const double* boxt);
+DPB_API int dpb_geometry_cells_f64(double* cext, int* atype_ext, int* mapping, int* nall_dev,
+                                   void* grid, long long grid_bytes, void* scratch,
+                                   long long scratch_bytes, const double* coord,
+                                   const int* atype, int nloc, int mem_nall, float rcut,
+                                   const double* boxt, int* status, dpb_stream_t stream);
 
 /* Batched frames (no counterpart in the reference, which evaluates frames of
  * different sizes one call at a time): many frames of uneven atom counts in
@@ -627,7 +644,8 @@ DPB_API int dpb_adam_f64(double* p, const double* g, double* m, double* v, long 
  * width is used where it divides N, 240 only for K <= 512), fit_split_b {0, 1} (weights pre-split or split in the
  * GEMM), batch_atoms_per_cta {2, 4, 8} (batched env / force),
  * train_rows_per_group {4, 8} (FP32 training kernels, standard net),
- * train_warps_per_cta {1, 2, 4, 8}. The autotuner (autotune.py) times the
+ * train_warps_per_cta {1, 2, 4, 8}, geometry_fused {0, 1} (one cooperative
+ * geometry launch or the separate kernels). The autotuner (autotune.py) times the
  * options on the caller's own step and sets the fastest. */
 DPB_API int dpb_tune_count(void);
 DPB_API const char* dpb_tune_name(int index);
