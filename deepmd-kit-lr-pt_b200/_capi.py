@@ -93,6 +93,7 @@ _FUNCS = {
     "dpb_copy_coord_async_f64": "ppppp" "L" "ppiifpp",
     "dpb_cell_grid_build_async_f64": "pLpipfp",
     "dpb_geometry_cells_f64": "ppppp" "L" "p" "L" "ppiifppp",
+    "dpb_fit_energy_sum_f32": "ppidp",
     "dpb_se_a_pack_table_f32": "ppiip",
     "dpb_se_a_build_table_f64": "pppiipppipLp",
     "dpb_batch_env_mat_a_f32": "pppppppppp" "ppppp" "iiff" "pipp",

@@ -120,4 +120,35 @@ inline int grid_stride_blocks(long long items, int per_block) {
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// ---- programmatic dependent launch -----------------------------------------
+// Kernels launched by launch_pdl may be scheduled while the previous kernel of
+// the stream drains (its CTAs have all started and triggered): their launch
+// latency and set-up overlap that kernel's tail. Such a kernel calls
+// pdl_wait() before it touches global memory: the wait returns once the
+// previous kernel has completed and its writes are visible (immediately when
+// the kernel was launched without the attribute). pdl_trigger() lets the next
+// kernel be scheduled once every CTA of this one has called it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launch of a kernel that starts with pdl_wait(); the attribute is dropped
+// when the pdl knob is 0.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = tune_value("pdl", 1) != 0 ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 }  // namespace dpb

@@ -297,6 +297,10 @@ k_gemm_tf32x3(const __grid_constant__ GemmMaps maps, GemmShape shp, GemmEpi epi,
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
   volatile int* abort = &abort_flag;
+  // barriers and tensor memory are set up: wait for the previous kernel of
+  // the stream before the first global access
+  pdl_wait();
+  pdl_trigger();
 
   if (warp == 0) {
     // ---------------------------------------------------------------- TMA
@@ -575,8 +579,9 @@ static int launch_mode(const GemmMaps& maps, const GemmShape& shp, const GemmEpi
   if (tiles == 0) return DPB_OK;
   const int sms = sm_count();
   const int grid = tiles < sms ? tiles : sms;
-  k_gemm_tf32x3<CFG, MODE><<<grid, CFG::THREADS, CFG::SMEM, st>>>(maps, shp, epi, status);
-  DPB_CHECK_LAUNCH("gemm_tf32x3");
+  DPB_CUDA(launch_pdl(k_gemm_tf32x3<CFG, MODE>, dim3(grid), dim3(CFG::THREADS),
+                      (size_t)CFG::SMEM, st, maps, shp, epi, status),
+           "gemm_tf32x3");
   return DPB_OK;
 }
 
@@ -627,6 +632,30 @@ static int make_map(CUtensorMap* m, const float* base, int rows, int cols, int b
     return DPB_ERR_INVALID;
   }
   return DPB_OK;
+}
+
+// Total energy of the fitting rows: energy[0] = e_const + sum_r e[r] in FP64
+// (one block, fixed order: the same bits on every call), then e[r] = 0, so
+// the next step's output-layer epilogue can accumulate into it again.
+__global__ void __launch_bounds__(1024) k_energy_sum(double* energy, float* e, int n,
+                                                     double e_const) {
+  __shared__ double s_w[32];
+  pdl_wait();
+  pdl_trigger();
+  double acc = 0.;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    acc += (double)e[r];
+    e[r] = 0.f;
+  }
+  acc = warp_sum(acc);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) s_w[w] = acc;
+  __syncthreads();
+  if (w == 0) {
+    double v = lane < (int)(blockDim.x >> 5) ? s_w[lane] : 0.;
+    v = warp_sum(v);
+    if (lane == 0) energy[0] = e_const + v;
+  }
 }
 
 }  // namespace dpb
@@ -708,6 +737,18 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
   if (BN == CfgN240::BN) return launch<CfgN240>(maps, shp, ep, status, st);
   if (BN == CfgN160::BN) return launch<CfgN160>(maps, shp, ep, status, st);
   return launch<CfgN80>(maps, shp, ep, status, st);
+}
+
+int dpb_fit_energy_sum_f32(double* energy, float* e, int n, double e_const,
+                           dpb_stream_t stream) {
+  if (n < 0 || energy == nullptr || (n > 0 && e == nullptr)) {
+    set_error("fit_energy_sum: invalid arguments (n=%d)", n);
+    return DPB_ERR_INVALID;
+  }
+  DPB_CUDA(launch_pdl(k_energy_sum, dim3(1), dim3(1024), 0, as_stream(stream), energy, e, n,
+                      e_const),
+           "fit_energy_sum");
+  return DPB_OK;
 }
 
 }  // extern "C"

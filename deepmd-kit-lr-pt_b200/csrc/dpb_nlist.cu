@@ -283,6 +283,8 @@ template <typename CT, typename OT, int CAP, int WARPS, bool FROM_CELLS>
 __global__ void __launch_bounds__(WARPS * 32)
 k_env(EnvIO<CT, OT> io, SecInfo sec, int nrows, int* redo) {
   __shared__ EnvSmem<CAP> sm[WARPS];
+  pdl_wait();
+  pdl_trigger();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * WARPS + w;
   if (row >= nrows) return;
@@ -299,6 +301,8 @@ template <typename CT, typename OT, int CAP>
 __global__ void __launch_bounds__(32) k_env_redo(EnvIO<CT, OT> io, SecInfo sec,
                                                  const int* redo) {
   __shared__ EnvSmem<CAP> sm;
+  pdl_wait();
+  pdl_trigger();
   const int n = redo[0];
   for (int r = blockIdx.x; r < n; r += gridDim.x) {
     env_one<CT, OT, CAP, true>(io, sec, redo[1 + r], sm, false);
@@ -333,11 +337,12 @@ static int env_cells(OT* em, OT* em_deriv, OT* rij, int* nlist, const CT* coord,
   cudaStream_t st = as_stream(stream);
   DPB_CUDA(cudaMemsetAsync(g.redo, 0, sizeof(int), st), "env_mat_a_cells");
   constexpr int W = 4;
-  k_env<CT, OT, ENV_SMALL_CAP, W, true><<<ceil_div(nloc, W), W * 32, 0, st>>>(io, s, nloc,
-                                                                             g.redo);
-  DPB_CHECK_LAUNCH("env_mat_a_cells");
-  k_env_redo<CT, OT, ENV_LARGE_CAP><<<64, 32, 0, st>>>(io, s, g.redo);
-  DPB_CHECK_LAUNCH("env_mat_a_cells/large");
+  DPB_CUDA(launch_pdl(k_env<CT, OT, ENV_SMALL_CAP, W, true>, dim3(ceil_div(nloc, W)),
+                      dim3(W * 32), 0, st, io, s, nloc, g.redo),
+           "env_mat_a_cells");
+  DPB_CUDA(launch_pdl(k_env_redo<CT, OT, ENV_LARGE_CAP>, dim3(64), dim3(32), 0, st, io, s,
+                      (const int*)g.redo),
+           "env_mat_a_cells/large");
   return DPB_OK;
 }
 

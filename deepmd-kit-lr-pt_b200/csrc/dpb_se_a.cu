@@ -270,6 +270,8 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
            const int* __restrict__ drow, const float* __restrict__ em,
            TypeTables tt, int nloc, int M, int naxis, float inv_nnei, int warp_floats) {
   extern __shared__ float4 dsm4[];
+  pdl_wait();
+  pdl_trigger();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * SWT + w;
   if (i >= nloc) return;
@@ -328,10 +330,11 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
 
 constexpr int GRP = 4;  // neighbors reduced together in the backward (even)
 
-// one neighbor slot of the backward: P[0] = sum_c G'_c (e . dyr_c), P[1 + d] =
-// sum_c G_c dyr_c[d] over this lane's 4 channels (times the fold multiplier);
-// dyr01[d] / dyr23[d] hold dyr of channel pairs (0, 1) / (2, 3)
-__device__ __forceinline__ void bwd_slot(float (&P)[5], const Coef4& c, const float4 e,
+// one neighbor slot of the backward over this lane's 4 channels (times the
+// fold multiplier): P[0] = sum_c G'_c (e . dyr_c) + G_c dyr_c[0] (the two
+// terms of the slot's first output component), P[d] = sum_c G_c dyr_c[d] for
+// d = 1..3; dyr01[d] / dyr23[d] hold dyr of channel pairs (0, 1) / (2, 3)
+__device__ __forceinline__ void bwd_slot(float (&P)[4], const Coef4& c, const float4 e,
                                          const float4 L, float rep, const float2 (&dyr01)[4],
                                          const float2 (&dyr23)[4]) {
   const float2 x = f2(L.y), dl = f2(L.z);
@@ -348,16 +351,18 @@ __device__ __forceinline__ void bwd_slot(float (&P)[5], const Coef4& c, const fl
   d23 = __ffma2_rn(dyr23[2], f2(e.z), d23);
   d01 = __ffma2_rn(dyr01[3], f2(e.w), d01);
   d23 = __ffma2_rn(dyr23[3], f2(e.w), d23);
-  const float2 p0 = __ffma2_rn(g23, d23, __fmul2_rn(g01, d01));
+  float2 p0 = __ffma2_rn(g23, d23, __fmul2_rn(g01, d01));
+  p0 = __ffma2_rn(v01, dyr01[0], p0);
+  p0 = __ffma2_rn(v23, dyr23[0], p0);
   P[0] = p0.x + p0.y;
 #pragma unroll
-  for (int d = 0; d < 4; ++d) {
+  for (int d = 1; d < 4; ++d) {
     const float2 pd = __ffma2_rn(v23, dyr23[d], __fmul2_rn(v01, dyr01[d]));
-    P[1 + d] = pd.x + pd.y;
+    P[d] = pd.x + pd.y;
   }
   if (rep != 1.f) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) P[k] *= rep;
+    for (int k = 0; k < 4; ++k) P[k] *= rep;
   }
 }
 
@@ -368,6 +373,8 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
            const float* __restrict__ em, TypeTables tt, int nloc, int M, int naxis,
            float inv_nnei, int warp_floats) {
   extern __shared__ float4 dsm4[];
+  pdl_wait();
+  pdl_trigger();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * SWT + w;
   if (i >= nloc) return;
@@ -464,11 +471,11 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
           nrow[s0 + qq] = make_float4(0.f, 0.f, 0.f, 0.f);
         continue;
       }
-      float P[GRP][5];
+      float P[GRP][4];
 #pragma unroll
       for (int q = 0; q < GRP; ++q) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) P[q][k] = 0.f;
+        for (int k = 0; k < 4; ++k) P[q][k] = 0.f;
         const int qq = g0 + q;
         if (qq <= last && act) {  // warp-uniform apart from the idle lanes
           if ((q & 1) == 0) {
@@ -480,21 +487,21 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
           }
         }
       }
-      // reduce-scatter of the 4 x 5 partials over the warp: after the xor-16
+      // reduce-scatter of the 4 x 4 partials over the warp: after the xor-16
       // and -8 steps lane L holds neighbor q = 2*b4 + b3 summed over 8 lanes;
       // xor-4, -2 and -1 finish the sum in every lane of the group of 8.
-      float R1[2][5];
+      float R1[2][4];
 #pragma unroll
       for (int q = 0; q < 2; ++q)
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
+        for (int k = 0; k < 4; ++k) {
           const float mine = b4 ? P[2 + q][k] : P[q][k];
           const float other = b4 ? P[q][k] : P[2 + q][k];
           R1[q][k] = mine + __shfl_xor_sync(0xffffffffu, other, 16);
         }
-      float R2[5];
+      float R2[4];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) {
+      for (int k = 0; k < 4; ++k) {
         const float mine = b3 ? R1[1][k] : R1[0][k];
         const float other = b3 ? R1[0][k] : R1[1][k];
         R2[k] = mine + __shfl_xor_sync(0xffffffffu, other, 8);
@@ -504,7 +511,7 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
       }
       const int qq = g0 + 2 * b4 + b3;
       if ((lane & 7) == 0 && qq < nt)  // zero beyond the fold point
-        nrow[s0 + qq] = make_float4(R2[1] + R2[0], R2[2], R2[3], R2[4]);
+        nrow[s0 + qq] = make_float4(R2[0], R2[1], R2[2], R2[3]);
     }
   }
 }
@@ -578,6 +585,8 @@ k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
                   const int* __restrict__ type, const OT* __restrict__ std_,
                   const int* __restrict__ nlist, const int* __restrict__ mapping, int nloc,
                   int nnei, int ntypes, float rcut, float rcut_smth) {
+  pdl_wait();
+  pdl_trigger();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // grid-stride over center atoms (one warp each); the virial stays in
   // registers across atoms and is reduced once per block, so the nine
@@ -645,9 +654,10 @@ static int force_virial_rc(double* force, double* virial, const OT* nd, const CT
   DPB_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * 3 * (size_t)nforce, st), "force_virial");
   DPB_CUDA(cudaMemsetAsync(virial, 0, sizeof(double) * 9, st), "force_virial");
   if (nloc == 0 || nnei == 0) return DPB_OK;
-  k_force_virial_rc<CT, OT><<<grid_stride_blocks(nloc, SW), SW * 32, 0, st>>>(
-      force, virial, nd, coord, type, std_, nlist, mapping, nloc, nnei, ntypes, rcut, rcut_smth);
-  DPB_CHECK_LAUNCH("force_virial_env");
+  DPB_CUDA(launch_pdl(k_force_virial_rc<CT, OT>, dim3(grid_stride_blocks(nloc, SW)),
+                      dim3(SW * 32), 0, st, force, virial, nd, coord, type, std_, nlist, mapping,
+                      nloc, nnei, ntypes, rcut, rcut_smth),
+           "force_virial_env");
   return DPB_OK;
 }
 
@@ -756,9 +766,9 @@ int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_r
     const size_t smem = sizeof(float) * sw * (size_t)wf;
     DPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "se_a_descriptor_fwd");
-    kern<<<ceil_div(nloc, sw), sw * 32, smem, st>>>(xyz, descrpt, descrpt_row, em, tt, nloc, M,
-                                                   axis_neuron, inv, wf);
-    DPB_CHECK_LAUNCH("se_a_descriptor_fwd");
+    DPB_CUDA(launch_pdl(kern, dim3(ceil_div(nloc, sw)), dim3(sw * 32), smem, st, xyz, descrpt,
+                        descrpt_row, em, tt, nloc, M, axis_neuron, inv, wf),
+             "se_a_descriptor_fwd");
     return DPB_OK;
   };
   const int ch = tune_value("desc_coef_l1", 3);
@@ -800,9 +810,9 @@ int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
     const size_t smem = sizeof(float) * sw * (size_t)wf;
     DPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "se_a_descriptor_bwd");
-    kern<<<ceil_div(nloc, sw), sw * 32, smem, st>>>(net_deriv, d_descrpt, descrpt_row, xyz, em,
-                                                   tt, nloc, M, axis_neuron, inv, wf);
-    DPB_CHECK_LAUNCH("se_a_descriptor_bwd");
+    DPB_CUDA(launch_pdl(kern, dim3(ceil_div(nloc, sw)), dim3(sw * 32), smem, st, net_deriv,
+                        d_descrpt, descrpt_row, xyz, em, tt, nloc, M, axis_neuron, inv, wf),
+             "se_a_descriptor_bwd");
     return DPB_OK;
   };
   const int ch = tune_value("desc_coef_l1", 3);

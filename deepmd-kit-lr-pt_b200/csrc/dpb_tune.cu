@@ -41,6 +41,9 @@ static Knob g_knobs[] = {
     // one frame's wrap / ghost copy / cell grid: 1 one cooperative launch,
     // 0 the separate kernels
     {"geometry_fused", 1, 2, {0, 1}},
+    // programmatic dependent launch between the kernels of a step: 1 on
+    // (each kernel's launch overlaps the previous kernel's tail), 0 off
+    {"pdl", 1, 2, {0, 1}},
 };
 
 static Knob* find_knob(const char* name) {

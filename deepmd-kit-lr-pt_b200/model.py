@@ -349,15 +349,20 @@ class _FittingTC:
 
     def forward_backward(self, D: torch.Tensor, dD: torch.Tensor, energy: torch.Tensor):
         """energy[0] = sum of atomic energies (FP64); dD = dE/dD (FP32)."""
-        self.layers(D, dD)
-        energy.copy_((self.e.to(torch.float64).sum() + self.e_const).view(1))
+        self.layers(D, dD, zero_e=False)
+        # FP64 total, and self.e left zeroed for the next step's accumulation
+        call("dpb_fit_energy_sum_f32", ptr(energy), ptr(self.e), self.n, self.e_const,
+             torch.cuda.current_stream().cuda_stream)
 
-    def layers(self, D: torch.Tensor, dD: torch.Tensor):
+    def layers(self, D: torch.Tensor, dD: torch.Tensor, zero_e: bool = True):
         """The six GEMMs: self.e[r] = atomic energy of fitting row r without
-        its constant (output bias + atomic energy bias); dD = dE/dD."""
+        its constant (output bias + atomic energy bias); dD = dE/dD. With
+        ``zero_e`` False, self.e must hold zeros already (forward_backward's
+        energy sum leaves it so)."""
         s = torch.cuda.current_stream().cuda_stream
         w, din = self.width, self.din
-        self.e.zero_()
+        if zero_e:
+            self.e.zero_()
         self._gemm(D, din, self.B1f, w, self.EPI_TANH, self.H1, bias=self.b1, s=s)
         self._gemm(self.H1, w, self.B2f, w, self.EPI_RES_DT, self.Y2, self.H2, aux0=self.H1,
                    bias=self.b2, idt=self.d2, s=s)

@@ -484,6 +484,11 @@ DPB_API int dpb_gemm_tf32x3_f32(const float* A, int M, int K,
                                 const float* aux1, const float* const* bias,
                                 const float* const* idt, const float* const* w,
                                 float* e, int* status, dpb_stream_t stream);
+/* energy[0] = e_const + sum of e[0, n) in FP64 (fixed summation order), then
+ * e[0, n) = 0: the per-row energies the mode-3 epilogue accumulates, reduced
+ * and cleared for the next step's accumulation. */
+DPB_API int dpb_fit_energy_sum_f32(double* energy, float* e, int n, double e_const,
+                                   dpb_stream_t stream);
 
 /* ------------------------------------------------- training step ----- */
 /* Energy, force and virial of the uncompressed se_e2_a model together with
