@@ -93,7 +93,7 @@ _FUNCS = {
     "dpb_copy_coord_async_f64": "ppppp" "L" "ppiifpp",
     "dpb_cell_grid_build_async_f64": "pLpipfp",
     "dpb_geometry_cells_f64": "ppppp" "L" "p" "L" "ppiifppp",
-    "dpb_fit_energy_sum_f32": "ppidp",
+    "dpb_fit_energy_sum_f32": "ppidpp",
     "dpb_se_a_pack_table_f32": "ppiip",
     "dpb_se_a_build_table_f64": "pppiipppipLp",
     "dpb_batch_env_mat_a_f32": "pppppppppp" "ppppp" "iiff" "pipp",
@@ -108,6 +108,7 @@ _FUNCS = {
     "dpb_force_virial_a_f64": "pppppp" "pp" "iiiip",
     "dpb_build_nlist_noalloc_f64": "ppppp" "iiif" "i" "pp",
     "dpb_force_virial_a_env_mixed": "pppppppp" "iiii" "ff" "p",
+    "dpb_force_virial_a_env_mixed_acc": "pppppppp" "iiii" "ff" "p",
     "dpb_gemm_tf32x3_f32": "pii" "pp" "i" "pi" "i" "pppp" "ppp" "pp" "p",
     "dpb_force_virial_a_env_f64": "pppppppp" "iiii" "ff" "p",
 }
@@ -135,6 +136,7 @@ _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),
     "dpb_cell_grid_bytes": ("i", LL),
     "dpb_geometry_scratch_bytes": ("ifp", LL),
+    "dpb_fit_energy_sum_work_bytes": ("", LL),
     "dpb_build_nlist_scratch_bytes": ("ii", LL),
     "dpb_build_nlist_noalloc_max_bytes": ("", LL),
     "dpb_se_a_build_table_scratch_bytes": ("ii", LL),

@@ -31,6 +31,8 @@ __global__ void __launch_bounds__(256)
 k_bt_cells(double* __restrict__ cw, int* __restrict__ cell_of, int* __restrict__ cell_start,
            int* __restrict__ cell_atoms, const double* __restrict__ coord, BtFrames fr) {
   __shared__ int cnt[BT_MAXCELLS + 1];
+  pdl_wait();
+  pdl_trigger();
   const int f = blockIdx.x;
   const int a0 = fr.atom_off[f], na = fr.atom_off[f + 1] - a0;
   const int nx = fr.ncell[3 * f], ny = fr.ncell[3 * f + 1], nz = fr.ncell[3 * f + 2];
@@ -80,6 +82,8 @@ k_bt_env(ET* __restrict__ em, int* __restrict__ nlist, const double* __restrict_
          const ET* __restrict__ avg, const ET* __restrict__ std_, BtFrames fr, BtSec sec,
          int nrows, float rcut, float rcut_smth, int* status) {
   __shared__ BtEnvSmem smem[WP];
+  pdl_wait();
+  pdl_trigger();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * WP + w;
   if (row >= nrows) return;
@@ -213,6 +217,8 @@ k_bt_force(double* __restrict__ force, double* __restrict__ virial,
            const int* __restrict__ type, const ET* __restrict__ std_,
            const int* __restrict__ nlist, BtFrames fr, int ntypes, int nnei, int nrows,
            float rcut, float rcut_smth) {
+  pdl_wait();
+  pdl_trigger();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * WP + w;
   if (row >= nrows) return;
@@ -278,6 +284,8 @@ __global__ void __launch_bounds__(256)
 k_bt_energy(double* __restrict__ energy, const ET* __restrict__ e_rows,
             const int* __restrict__ drow, const double* __restrict__ e_const, BtFrames fr) {
   __shared__ double part[8];
+  pdl_wait();
+  pdl_trigger();
   const int f = blockIdx.x;
   double s = 0.;
   for (int r = fr.atom_off[f] + threadIdx.x; r < fr.atom_off[f + 1]; r += blockDim.x)
@@ -317,13 +325,15 @@ static int batch_env(ET* em, int* nlist, double* cw, int* cell_of, int* cell_sta
   for (int k = 0; k < nsec; ++k) s.sec[k] = sec[k];
   if (nrows <= 0) return DPB_OK;
   cudaStream_t st = as_stream(stream);
-  k_bt_cells<<<nframes, 256, 0, st>>>(cw, cell_of, cell_start, cell_atoms, coord, fr);
-  DPB_CHECK_LAUNCH("batch_env_mat_a/cells");
+  DPB_CUDA(launch_pdl(k_bt_cells, dim3(nframes), dim3(256), 0, st, cw, cell_of, cell_start,
+                      cell_atoms, coord, fr),
+           "batch_env_mat_a/cells");
   auto run = [&](auto kern, int wp) -> int {
-    kern<<<ceil_div(nrows, wp), wp * 32, 0, st>>>(em, nlist, cw, type, cell_of, cell_start,
-                                                 cell_atoms, avg, std_, fr, s, nrows, rcut,
-                                                 rcut_smth, status);
-    DPB_CHECK_LAUNCH("batch_env_mat_a/env");
+    DPB_CUDA(launch_pdl(kern, dim3(ceil_div(nrows, wp)), dim3(wp * 32), 0, st, em, nlist, cw,
+                        type, (const int*)cell_of, (const int*)cell_start,
+                        (const int*)cell_atoms, avg, std_, fr, s, nrows, rcut, rcut_smth,
+                        status),
+             "batch_env_mat_a/env");
     return DPB_OK;
   };
   switch (tune_value("batch_atoms_per_cta", BT_WARPS)) {
@@ -348,10 +358,10 @@ static int batch_force(double* force, double* virial, const ET* net_deriv, const
            "batch_force");
   if (nrows <= 0 || nnei <= 0) return DPB_OK;
   auto run = [&](auto kern, int wp) -> int {
-    kern<<<ceil_div(nrows, wp), wp * 32, 0, st>>>(force, virial, net_deriv, cw, type, std_,
-                                                 nlist, fr, ntypes, nnei, nrows, rcut,
-                                                 rcut_smth);
-    DPB_CHECK_LAUNCH("batch_force_virial_a");
+    DPB_CUDA(launch_pdl(kern, dim3(ceil_div(nrows, wp)), dim3(wp * 32), 0, st, force, virial,
+                        net_deriv, cw, type, std_, nlist, fr, ntypes, nnei, nrows, rcut,
+                        rcut_smth),
+             "batch_force_virial_a");
     return DPB_OK;
   };
   switch (tune_value("batch_atoms_per_cta", BT_WARPS)) {
@@ -369,8 +379,9 @@ static int batch_energy(double* energy, const ET* e_rows, const int* drow, const
     return DPB_ERR_INVALID;
   }
   BtFrames fr{atom_off, nullptr, nullptr, nullptr, nullptr, nframes};
-  k_bt_energy<ET><<<nframes, 256, 0, as_stream(stream)>>>(energy, e_rows, drow, e_const, fr);
-  DPB_CHECK_LAUNCH("batch_energy");
+  DPB_CUDA(launch_pdl(k_bt_energy<ET>, dim3(nframes), dim3(256), 0, as_stream(stream), energy,
+                      e_rows, drow, e_const, fr),
+           "batch_energy");
   return DPB_OK;
 }
 

@@ -38,6 +38,8 @@
 #include <cudaTypedefs.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "dpb_common.cuh"
 
 namespace dpb {
@@ -634,16 +636,25 @@ static int make_map(CUtensorMap* m, const float* base, int rows, int cols, int b
   return DPB_OK;
 }
 
-// Total energy of the fitting rows: energy[0] = e_const + sum_r e[r] in FP64
-// (one block, fixed order: the same bits on every call), then e[r] = 0, so
-// the next step's output-layer epilogue can accumulate into it again.
-__global__ void __launch_bounds__(1024) k_energy_sum(double* energy, float* e, int n,
-                                                     double e_const) {
-  __shared__ double s_w[32];
+// Total energy of the fitting rows: energy[0] = e_const + sum_r e[r] in FP64,
+// then e[r] = 0, so the next step's output-layer epilogue can accumulate into
+// it again. Block b sums the fixed row range [b * chunk, (b + 1) * chunk) into
+// part[b]; the last block to finish (ticket) adds the partials in block order,
+// so the bits do not depend on scheduling, and resets the ticket.
+constexpr int ES_MAXB = 148;
+constexpr int ES_ROWS = 4096;  // rows per block at least
+
+__global__ void __launch_bounds__(512) k_energy_sum(double* energy, float* e, int n,
+                                                    double e_const, double* part,
+                                                    unsigned* ticket) {
+  __shared__ double s_w[16];
+  __shared__ int s_last;
   pdl_wait();
   pdl_trigger();
+  const int chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * chunk, r1 = min(n, r0 + chunk);
   double acc = 0.;
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+  for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
     acc += (double)e[r];
     e[r] = 0.f;
   }
@@ -651,10 +662,20 @@ __global__ void __launch_bounds__(1024) k_energy_sum(double* energy, float* e, i
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) s_w[w] = acc;
   __syncthreads();
-  if (w == 0) {
-    double v = lane < (int)(blockDim.x >> 5) ? s_w[lane] : 0.;
-    v = warp_sum(v);
-    if (lane == 0) energy[0] = e_const + v;
+  if (threadIdx.x == 0) {
+    double v = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v += s_w[k];
+    part[blockIdx.x] = v;
+    __threadfence();
+    s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    double t = e_const;
+    for (int k = 0; k < (int)gridDim.x; ++k) t += __ldcg(part + k);
+    energy[0] = t;
+    *ticket = 0u;
   }
 }
 
@@ -739,14 +760,21 @@ int dpb_gemm_tf32x3_f32(const float* A, int M, int K, const float* const* b_hi,
   return launch<CfgN80>(maps, shp, ep, status, st);
 }
 
-int dpb_fit_energy_sum_f32(double* energy, float* e, int n, double e_const,
+long long dpb_fit_energy_sum_work_bytes(void) {
+  return (long long)sizeof(double) * (ES_MAXB + 2);
+}
+
+int dpb_fit_energy_sum_f32(double* energy, float* e, int n, double e_const, void* work,
                            dpb_stream_t stream) {
-  if (n < 0 || energy == nullptr || (n > 0 && e == nullptr)) {
-    set_error("fit_energy_sum: invalid arguments (n=%d)", n);
+  if (n < 0 || energy == nullptr || work == nullptr || (n > 0 && e == nullptr)) {
+    set_error("fit_energy_sum: invalid arguments (n=%d; energy and work required)", n);
     return DPB_ERR_INVALID;
   }
-  DPB_CUDA(launch_pdl(k_energy_sum, dim3(1), dim3(1024), 0, as_stream(stream), energy, e, n,
-                      e_const),
+  const int blocks = std::max(1, std::min(ES_MAXB, ceil_div(n, ES_ROWS)));
+  double* part = static_cast<double*>(work);
+  unsigned* ticket = reinterpret_cast<unsigned*>(part + ES_MAXB);
+  DPB_CUDA(launch_pdl(k_energy_sum, dim3(blocks), dim3(512), 0, as_stream(stream), energy, e,
+                      n, e_const, part, ticket),
            "fit_energy_sum");
   return DPB_OK;
 }

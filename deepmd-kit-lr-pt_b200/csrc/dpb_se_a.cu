@@ -646,13 +646,16 @@ template <typename CT, typename OT>
 static int force_virial_rc(double* force, double* virial, const OT* nd, const CT* coord,
                            const int* type, const OT* std_, const int* nlist,
                            const int* mapping, int nloc, int nforce, int nnei, int ntypes,
-                           float rcut, float rcut_smth, cudaStream_t st) {
+                           float rcut, float rcut_smth, cudaStream_t st, bool zero = true) {
   if (nloc < 0 || nforce < 0 || nnei < 0 || ntypes <= 0) {
     set_error("force_virial_env: invalid sizes");
     return DPB_ERR_INVALID;
   }
-  DPB_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * 3 * (size_t)nforce, st), "force_virial");
-  DPB_CUDA(cudaMemsetAsync(virial, 0, sizeof(double) * 9, st), "force_virial");
+  if (zero) {
+    DPB_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * 3 * (size_t)nforce, st),
+             "force_virial");
+    DPB_CUDA(cudaMemsetAsync(virial, 0, sizeof(double) * 9, st), "force_virial");
+  }
   if (nloc == 0 || nnei == 0) return DPB_OK;
   DPB_CUDA(launch_pdl(k_force_virial_rc<CT, OT>, dim3(grid_stride_blocks(nloc, SW)),
                       dim3(SW * 32), 0, st, force, virial, nd, coord, type, std_, nlist, mapping,
@@ -841,6 +844,16 @@ int dpb_force_virial_a_env_mixed(double* force, double* virial, const float* net
   return force_virial_rc<double, float>(force, virial, net_deriv, coord, type, std_, nlist,
                                         mapping, nloc, nforce, nnei, ntypes, rcut, rcut_smth,
                                         as_stream(stream));
+}
+
+int dpb_force_virial_a_env_mixed_acc(double* force, double* virial, const float* net_deriv,
+                                     const double* coord, const int* type, const float* std_,
+                                     const int* nlist, const int* mapping, int nloc,
+                                     int nforce, int nnei, int ntypes, float rcut,
+                                     float rcut_smth, dpb_stream_t stream) {
+  return force_virial_rc<double, float>(force, virial, net_deriv, coord, type, std_, nlist,
+                                        mapping, nloc, nforce, nnei, ntypes, rcut, rcut_smth,
+                                        as_stream(stream), false);
 }
 
 int dpb_force_virial_a_env_f64(double* force, double* virial, const double* net_deriv,

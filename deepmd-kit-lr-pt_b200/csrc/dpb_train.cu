@@ -519,6 +519,8 @@ __global__ void __launch_bounds__(64)
 k_tr_xbar(T* __restrict__ xb_out, T* __restrict__ xbd_out, const T* __restrict__ xyz,
           const T* __restrict__ xyzd, const T* __restrict__ Dj, const T* __restrict__ Dd,
           const int* __restrict__ drow, int nrows, int n3, int ax, int nnei, int sax) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* base = reinterpret_cast<T*>(smem_raw) + (size_t)w * (8 * n3 + 2 * n3 * sax);
@@ -566,6 +568,8 @@ template <typename T, int R, int N1, int N2, int N3>
 __global__ void __launch_bounds__(256, 1)
 k_tr_fwd(T* __restrict__ xyz_out, T* __restrict__ D_out, const T* __restrict__ em,
          TrNet<T> net, TrGeom g, TrLayout lay) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -699,6 +703,8 @@ template <typename T, int R, int N1, int N2, int N3>
 __global__ void __launch_bounds__(256, 1)
 k_tr_bwd(T* __restrict__ gem, const T* __restrict__ em, const T* __restrict__ xbar,
          TrNet<T> net, TrGeom g, TrLayout lay) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -871,6 +877,8 @@ __global__ void __launch_bounds__(256, 1)
 k_tr_tan(T* __restrict__ xyzd_out, T* __restrict__ Dd_out, const T* __restrict__ xyz,
          const T* __restrict__ avg, const T* __restrict__ std_, const double* __restrict__ fbar,
          const double* __restrict__ vbar, TrNet<T> net, TrGeom g, TrLayout lay) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* sw = tr_tbase<T>(smem_raw, lay) + lay.w_off;
@@ -1028,6 +1036,8 @@ __global__ void __launch_bounds__(256, 1)
 k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard,
          const T* __restrict__ avg, const T* __restrict__ std_, const double* __restrict__ fbar,
          const double* __restrict__ vbar, TrNet<T> net, TrGeom g, TrLayout lay) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* tb = tr_tbase<T>(smem_raw, lay);
@@ -1318,6 +1328,8 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
 template <typename T>
 __global__ void k_fit_act(T* __restrict__ Y, T* __restrict__ H, const T* __restrict__ Hin,
                           const T* __restrict__ d, int n, int w_out, int w_in, int res) {
+  pdl_wait();
+  pdl_trigger();
   const long long tot = (long long)n * w_out;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
@@ -1337,6 +1349,8 @@ template <typename T>
 __global__ void k_fit_tan(T* __restrict__ Hd, const T* __restrict__ Zd, const T* __restrict__ Hdin,
                           const T* __restrict__ Y, const T* __restrict__ d, int n, int w_out,
                           int w_in, int res) {
+  pdl_wait();
+  pdl_trigger();
   const long long tot = (long long)n * w_out;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
@@ -1355,6 +1369,8 @@ __global__ void k_fit_tan(T* __restrict__ Hd, const T* __restrict__ Zd, const T*
 template <typename T>
 __global__ void k_fit_bwd(T* __restrict__ Zb, const T* __restrict__ G, const T* __restrict__ Y,
                           const T* __restrict__ d, int n, int w) {
+  pdl_wait();
+  pdl_trigger();
   const long long tot = (long long)n * w;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
@@ -1375,6 +1391,8 @@ __global__ void k_fit_rev(T* __restrict__ Zb, T* __restrict__ Zbd, T* __restrict
                           T* __restrict__ gd, const T* __restrict__ A, const T* __restrict__ Ad,
                           const T* __restrict__ Y, const T* __restrict__ Zd,
                           const T* __restrict__ d, int n, int w) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ T red[2][8][33];
   const int c = blockIdx.x * 32 + threadIdx.x;
   T sb = (T)0, sd = (T)0;
@@ -1410,6 +1428,8 @@ __global__ void k_fit_rev(T* __restrict__ Zb, T* __restrict__ Zbd, T* __restrict
 template <typename T>
 __global__ void k_fit_res_adj(T* __restrict__ out, const T* __restrict__ G, int n, int w_out,
                               int w_in, int res) {
+  pdl_wait();
+  pdl_trigger();
   const long long tot = (long long)n * w_in;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
@@ -1425,6 +1445,8 @@ __global__ void k_fit_res_adj(T* __restrict__ out, const T* __restrict__ G, int 
 template <typename T>
 __global__ void k_fit_out(T* __restrict__ e, const T* __restrict__ H, const T* __restrict__ Wo,
                           const T* __restrict__ bo, T ebias, int n, int w) {
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & 31;
   for (long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; i < n;
        i += ((long long)gridDim.x * blockDim.x) >> 5) {
@@ -1443,6 +1465,8 @@ __global__ void k_fit_out_adj(T* __restrict__ A, T* __restrict__ Ad, T* __restri
                               T* __restrict__ gbo, const T* __restrict__ H,
                               const T* __restrict__ Hd, const T* __restrict__ Wo,
                               const T* __restrict__ lam, int n, int w) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ T red[8][33];
   __shared__ T redb[8];
   const int c = blockIdx.x * 32 + threadIdx.x;
@@ -1477,6 +1501,8 @@ __global__ void k_fit_out_adj(T* __restrict__ A, T* __restrict__ Ad, T* __restri
 template <typename T>
 __global__ void k_tr_lam(T* __restrict__ lam, const double* __restrict__ gE,
                          const int* __restrict__ drow, const int* __restrict__ row_frame, int n) {
+  pdl_wait();
+  pdl_trigger();
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
     lam[drow[r]] = (T)gE[row_frame[r]];
 }
@@ -1490,6 +1516,8 @@ template <typename T>
 __global__ void k_adam(T* __restrict__ p, const T* __restrict__ g, T* __restrict__ m,
                        T* __restrict__ v, long long n, const double* __restrict__ hp, double b1,
                        double b2, double eps) {
+  pdl_wait();
+  pdl_trigger();
   const T step = (T)(hp[0] / hp[1]);
   const T bc2s = (T)hp[2];
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
@@ -1717,9 +1745,8 @@ static int tr_xbar(T* xb, T* xbd, const T* xyz, const T* xyzd, const T* Dj, cons
     return DPB_ERR_CUDA;
   }
   const int grid = std::max(1, std::min(ceil_div(nrows, 2), sm_count() * 8));
-  k_tr_xbar<T><<<grid, 64, smem, st>>>(xb, xbd, xyz, xyzd, Dj, Dd, drow, nrows, n3, ax, nnei,
-                                       sax);
-  DPB_CHECK_LAUNCH("se_a_train/xbar");
+  DPB_CUDA(launch_pdl(k_tr_xbar<T>, dim3(grid), dim3(64), smem, st, xb, xbd, xyz, xyzd, Dj,
+        Dd, drow, nrows, n3, ax, nnei, sax), "se_a_train/xbar");
   return DPB_OK;
 }
 
@@ -1751,8 +1778,8 @@ using namespace dpb;
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
     if (rc) return rc;                                                                          \
-    kern<<<grid, L.nw * 32, smem, as_stream(stream)>>>(xyz, descrpt, em, net, g, L);           \
-    DPB_CHECK_LAUNCH("se_a_train_fwd");                                                         \
+    DPB_CUDA(launch_pdl(kern, dim3(grid), dim3(L.nw * 32), smem, as_stream(stream), xyz,         \
+          descrpt, em, net, g, L), "se_a_train_fwd");                                            \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_se_a_train_bwd_##SUF(T* net_deriv, T* scratch, const T* em, const T* xyz,          \
@@ -1785,8 +1812,8 @@ using namespace dpb;
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
     if (rc) return rc;                                                                          \
-    kern<<<grid, L.nw * 32, smem, st>>>(net_deriv, em, scratch, net, g, L);                     \
-    DPB_CHECK_LAUNCH("se_a_train_bwd");                                                         \
+    DPB_CUDA(launch_pdl(kern, dim3(grid), dim3(L.nw * 32), smem, st, net_deriv, em, scratch,     \
+          net, g, L), "se_a_train_bwd");                                                         \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_se_a_train_tan_##SUF(T* xyz_t, T* descrpt_t, const T* xyz, const T* avg,             \
@@ -1817,9 +1844,8 @@ using namespace dpb;
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
     if (rc) return rc;                                                                          \
-    kern<<<grid, L.nw * 32, smem, as_stream(stream)>>>(xyz_t, descrpt_t, xyz, avg, std_,       \
-                                                       force_bar, virial_bar, net, g, L);       \
-    DPB_CHECK_LAUNCH("se_a_train_tan");                                                         \
+    DPB_CUDA(launch_pdl(kern, dim3(grid), dim3(L.nw * 32), smem, as_stream(stream), xyz_t,       \
+          descrpt_t, xyz, avg, std_, force_bar, virial_bar, net, g, L), "se_a_train_tan");       \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_se_a_train_rev_##SUF(T* const* gW, T* const* gb, T* scratch, const T* xyz,         \
@@ -1868,43 +1894,39 @@ using namespace dpb;
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
     if (rc) return rc;                                                                          \
-    kern<<<grid, L.nw * 32, smem, st>>>(gr, xb, xbd, avg, std_, force_bar, virial_bar, net, g,  \
-                                        L);                                                     \
-    DPB_CHECK_LAUNCH("se_a_train_rev");                                                         \
+    DPB_CUDA(launch_pdl(kern, dim3(grid), dim3(L.nw * 32), smem, st, gr, xb, xbd, avg, std_,     \
+          force_bar, virial_bar, net, g, L), "se_a_train_rev");                                  \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_fit_act_##SUF(T* Y, T* H, const T* Hin, const T* d, int n, int w_out, int w_in,      \
                         dpb_stream_t stream) {                                                  \
     if (n <= 0) return DPB_OK;                                                                  \
     const int res = w_out == w_in ? TR_RES_IDENT : (w_out == 2 * w_in ? TR_RES_DUP : TR_RES_NONE); \
-    k_fit_act<T><<<fit_grid((long long)n * w_out), 256, 0, as_stream(stream)>>>(               \
-        Y, H, Hin, d, n, w_out, w_in, res);                                                     \
-    DPB_CHECK_LAUNCH("fit_act");                                                                \
+    DPB_CUDA(launch_pdl(k_fit_act<T>, dim3(fit_grid((long long)n * w_out)), dim3(256), 0,        \
+          as_stream(stream), Y, H, Hin, d, n, w_out, w_in, res), "fit_act");                     \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_fit_tan_##SUF(T* Hd, const T* Zd, const T* Hdin, const T* Y, const T* d, int n,      \
                         int w_out, int w_in, dpb_stream_t stream) {                             \
     if (n <= 0) return DPB_OK;                                                                  \
     const int res = w_out == w_in ? TR_RES_IDENT : (w_out == 2 * w_in ? TR_RES_DUP : TR_RES_NONE); \
-    k_fit_tan<T><<<fit_grid((long long)n * w_out), 256, 0, as_stream(stream)>>>(               \
-        Hd, Zd, Hdin, Y, d, n, w_out, w_in, res);                                               \
-    DPB_CHECK_LAUNCH("fit_tan");                                                                \
+    DPB_CUDA(launch_pdl(k_fit_tan<T>, dim3(fit_grid((long long)n * w_out)), dim3(256), 0,        \
+          as_stream(stream), Hd, Zd, Hdin, Y, d, n, w_out, w_in, res), "fit_tan");               \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_fit_bwd_##SUF(T* Zb, const T* G, const T* Y, const T* d, int n, int w,               \
                         dpb_stream_t stream) {                                                  \
     if (n <= 0) return DPB_OK;                                                                  \
-    k_fit_bwd<T><<<fit_grid((long long)n * w), 256, 0, as_stream(stream)>>>(Zb, G, Y, d, n, w); \
-    DPB_CHECK_LAUNCH("fit_bwd");                                                                \
+    DPB_CUDA(launch_pdl(k_fit_bwd<T>, dim3(fit_grid((long long)n * w)), dim3(256), 0,            \
+          as_stream(stream), Zb, G, Y, d, n, w), "fit_bwd");                                     \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_fit_rev_##SUF(T* Zb, T* Zbd, T* gb, T* gd, const T* A, const T* Ad, const T* Y,      \
                         const T* Zd, const T* d, int n, int w, dpb_stream_t stream) {           \
     if (n <= 0) return DPB_OK;                                                                  \
     dim3 grid(ceil_div(w, 32), std::max(1, std::min(ceil_div(n, 8), 64)));                      \
-    k_fit_rev<T><<<grid, dim3(32, 8), 0, as_stream(stream)>>>(Zb, Zbd, gb, gd, A, Ad, Y, Zd, d,  \
-                                                             n, w);                             \
-    DPB_CHECK_LAUNCH("fit_rev");                                                                \
+    DPB_CUDA(launch_pdl(k_fit_rev<T>, dim3(grid), dim3(dim3(32, 8)), 0, as_stream(stream), Zb,   \
+          Zbd, gb, gd, A, Ad, Y, Zd, d, n, w), "fit_rev");                                       \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_fit_res_adj_##SUF(T* out, const T* G, int n, int w_out, int w_in,                    \
@@ -1912,17 +1934,15 @@ using namespace dpb;
     if (n <= 0) return DPB_OK;                                                                  \
     const int res = w_out == w_in ? TR_RES_IDENT : (w_out == 2 * w_in ? TR_RES_DUP : TR_RES_NONE); \
     if (res == TR_RES_NONE) return DPB_OK;                                                      \
-    k_fit_res_adj<T><<<fit_grid((long long)n * w_in), 256, 0, as_stream(stream)>>>(            \
-        out, G, n, w_out, w_in, res);                                                           \
-    DPB_CHECK_LAUNCH("fit_res_adj");                                                            \
+    DPB_CUDA(launch_pdl(k_fit_res_adj<T>, dim3(fit_grid((long long)n * w_in)), dim3(256), 0,     \
+          as_stream(stream), out, G, n, w_out, w_in, res), "fit_res_adj");                       \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_fit_out_##SUF(T* e, const T* H, const T* Wo, const T* bo, double ebias, int n, int w, \
                         dpb_stream_t stream) {                                                  \
     if (n <= 0) return DPB_OK;                                                                  \
-    k_fit_out<T><<<fit_grid((long long)n * 32), 256, 0, as_stream(stream)>>>(e, H, Wo, bo,     \
-                                                                             (T)ebias, n, w);   \
-    DPB_CHECK_LAUNCH("fit_out");                                                                \
+    DPB_CUDA(launch_pdl(k_fit_out<T>, dim3(fit_grid((long long)n * 32)), dim3(256), 0,           \
+          as_stream(stream), e, H, Wo, bo, (T)ebias, n, w), "fit_out");                          \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_fit_out_adj_##SUF(T* A, T* Ad, T* gWo, T* gbo, const T* H, const T* Hd, const T* Wo, \
@@ -1933,16 +1953,15 @@ using namespace dpb;
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
     dim3 grid(ceil_div(w, 32), std::max(1, std::min(ceil_div(n, 8), 64)));                      \
-    k_fit_out_adj<T><<<grid, dim3(32, 8), 0, as_stream(stream)>>>(A, Ad, gWo, gbo, H, Hd, Wo,   \
-                                                                 lam, n, w);                    \
-    DPB_CHECK_LAUNCH("fit_out_adj");                                                            \
+    DPB_CUDA(launch_pdl(k_fit_out_adj<T>, dim3(grid), dim3(dim3(32, 8)), 0, as_stream(stream),   \
+          A, Ad, gWo, gbo, H, Hd, Wo, lam, n, w), "fit_out_adj");                                \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_train_lam_##SUF(T* lam, const double* gE, const int* drow, const int* row_frame,     \
                           int n, dpb_stream_t stream) {                                         \
     if (n <= 0) return DPB_OK;                                                                  \
-    k_tr_lam<T><<<fit_grid(n), 256, 0, as_stream(stream)>>>(lam, gE, drow, row_frame, n);      \
-    DPB_CHECK_LAUNCH("train_lam");                                                              \
+    DPB_CUDA(launch_pdl(k_tr_lam<T>, dim3(fit_grid(n)), dim3(256), 0, as_stream(stream), lam,    \
+          gE, drow, row_frame, n), "train_lam");                                                 \
     return DPB_OK;                                                                              \
   }                                                                                             \
   int dpb_adam_##SUF(T* p, const T* g, T* m, T* v, long long n, const double* hp, double beta1, \
@@ -1952,8 +1971,8 @@ using namespace dpb;
       set_error("adam: null buffer");                                                           \
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
-    k_adam<T><<<fit_grid(n), 256, 0, as_stream(stream)>>>(p, g, m, v, n, hp, beta1, beta2, eps); \
-    DPB_CHECK_LAUNCH("adam");                                                                   \
+    DPB_CUDA(launch_pdl(k_adam<T>, dim3(fit_grid(n)), dim3(256), 0, as_stream(stream), p, g,     \
+          m, v, n, hp, beta1, beta2, eps), "adam");                                              \
     return DPB_OK;                                                                              \
   }
 

@@ -337,6 +337,8 @@ class _FittingTC:
         self.H1, self.Y2, self.H2, self.G3 = z(n, w), z(n, w), z(n, w), z(n, w)
         self.g2, self.G2, self.G1 = z(n, w), z(n, w), z(n, w)
         self.e = z(n)
+        self.esum_work = torch.zeros(int(_capi.lib().dpb_fit_energy_sum_work_bytes()),
+                                     dtype=torch.uint8, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
     def _gemm(self, A, K, B, N, mode, out0, out1=None, aux0=None, aux1=None, bias=None,
@@ -352,7 +354,7 @@ class _FittingTC:
         self.layers(D, dD, zero_e=False)
         # FP64 total, and self.e left zeroed for the next step's accumulation
         call("dpb_fit_energy_sum_f32", ptr(energy), ptr(self.e), self.n, self.e_const,
-             torch.cuda.current_stream().cuda_stream)
+             ptr(self.esum_work), torch.cuda.current_stream().cuda_stream)
 
     def layers(self, D: torch.Tensor, dD: torch.Tensor, zero_e: bool = True):
         """The six GEMMs: self.e[r] = atomic energy of fitting row r without
@@ -464,9 +466,11 @@ class SeAEvaluator:
         self.em = torch.empty((nloc, nnei * 4), dtype=fdt, device=dev)
         self.nlist = torch.empty((nloc, nnei), dtype=torch.int32, device=dev)
         self.net_deriv = torch.empty((nloc, nnei * 4), dtype=fdt, device=dev)
-        self.force = torch.zeros((nloc, 3), dtype=torch.float64, device=dev)
-        self.virial = torch.zeros(9, dtype=torch.float64, device=dev)
-        self.energy = torch.zeros(1, dtype=torch.float64, device=dev)
+        # energy, force and virial side by side: one device-to-host copy
+        self.results = torch.zeros(1 + 3 * nloc + 9, dtype=torch.float64, device=dev)
+        self.energy = self.results[0:1]
+        self.force = self.results[1:1 + 3 * nloc].view(nloc, 3)
+        self.virial = self.results[1 + 3 * nloc:]
         M, ax = cfg.neuron[-1], cfg.axis_neuron
         # atoms grouped by type for the per-type fitting networks
         order = np.argsort(atype, kind="stable")
@@ -596,6 +600,10 @@ class SeAEvaluator:
         cfg, s = self.cfg, torch.cuda.current_stream().cuda_stream
         nloc, nnei = self.nloc, cfg.nnei
         tm = _Stages(timers)
+        if self.mode == "compressed":
+            # force / virial accumulators, zeroed here where no kernel boundary
+            # of the step is delayed by it
+            self.results[1:].zero_()
         if self.skin > 0:
             if not self.built:
                 raise _capi.DPBInvalidArgument("call rebuild() before the first step")
@@ -633,7 +641,8 @@ class SeAEvaluator:
         else:
             with tm("descriptor_fitting_fp64"):
                 self._descriptor_plain()
-        fv = "dpb_force_virial_a_env_mixed" if self.mode == "compressed" else \
+        # the compressed path zeroed force / virial at the start of the step
+        fv = "dpb_force_virial_a_env_mixed_acc" if self.mode == "compressed" else \
             "dpb_force_virial_a_env_f64"
         with tm("force_virial"):
             call(fv, ptr(self.force), ptr(self.virial), ptr(self.net_deriv), ptr(self.cext),
@@ -770,9 +779,7 @@ class SeAEvaluator:
         n = self.nloc
         if out is None:
             out = torch.empty(1 + 3 * n + 9, dtype=torch.float64, pin_memory=True)
-        out[0:1].copy_(self.energy, non_blocking=True)
-        out[1:1 + 3 * n].copy_(self.force.view(-1), non_blocking=True)
-        out[1 + 3 * n:].copy_(self.virial, non_blocking=True)
+        out.copy_(self.results, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         o = out.numpy()
         return float(o[0]), o[1:1 + 3 * n].reshape(-1, 3).copy(), o[1 + 3 * n:].copy()

@@ -457,6 +457,15 @@ DPB_API int dpb_force_virial_a_env_mixed(double* force, double* virial,
                                          const int* mapping, int nloc, int nforce,
                                          int nnei, int ntypes, float rcut,
                                          float rcut_smth, dpb_stream_t stream);
+/* As dpb_force_virial_a_env_mixed, adding into force / virial instead of
+ * overwriting them (the caller zeroes them, e.g. earlier in the step, so no
+ * memset sits between this kernel and the one before it). */
+DPB_API int dpb_force_virial_a_env_mixed_acc(double* force, double* virial,
+                                             const float* net_deriv, const double* coord,
+                                             const int* type, const float* std_,
+                                             const int* nlist, const int* mapping, int nloc,
+                                             int nforce, int nnei, int ntypes, float rcut,
+                                             float rcut_smth, dpb_stream_t stream);
 DPB_API int dpb_force_virial_a_env_f64(double* force, double* virial,
                                        const double* net_deriv,
                                        const double* coord, const int* type,
@@ -486,8 +495,11 @@ DPB_API int dpb_gemm_tf32x3_f32(const float* A, int M, int K,
                                 float* e, int* status, dpb_stream_t stream);
 /* energy[0] = e_const + sum of e[0, n) in FP64 (fixed summation order), then
  * e[0, n) = 0: the per-row energies the mode-3 epilogue accumulates, reduced
- * and cleared for the next step's accumulation. */
-DPB_API int dpb_fit_energy_sum_f32(double* energy, float* e, int n, double e_const,
+ * and cleared for the next step's accumulation. work: device buffer of
+ * dpb_fit_energy_sum_work_bytes(), zeroed once by the caller (the call leaves
+ * it ready for the next one); calls sharing a work buffer must not overlap. */
+DPB_API long long dpb_fit_energy_sum_work_bytes(void);
+DPB_API int dpb_fit_energy_sum_f32(double* energy, float* e, int n, double e_const, void* work,
                                    dpb_stream_t stream);
 
 /* ------------------------------------------------- training step ----- */
