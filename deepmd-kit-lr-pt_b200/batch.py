@@ -217,5 +217,5 @@ class BatchEvaluator:
                f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
         return autotune.tune(self.replay, lambda: self.capture(),
                              ["batch_atoms_per_cta", "desc_atoms_per_cta", "desc_coef_l1",
-                              "fit_n_tile", "fit_split_b"],
+                              "fit_n_tile", "fit_split_b", "pdl"],
                              signature=sig, reps=reps, device=self.dev, use_cache=use_cache)

@@ -727,16 +727,19 @@ class SeAEvaluator:
         return self
 
     def tune(self, reps: int = 10, use_cache: bool = True) -> dict:
-        """Autotune the tile shapes of this step (atoms per CTA of the fused
-        descriptor kernels, fitting GEMM N tile); leaves it captured with the
-        fastest shapes."""
+        """Autotune the launch shapes of this step (atoms per CTA of the fused
+        descriptor kernels, table-load cache policy, fitting GEMM N tile and
+        weight split, programmatic dependent launch on or off); leaves it
+        captured with the fastest."""
         from . import autotune
 
         cfg = self.cfg
-        sig = (f"frame:{self.nloc}a:{self.mode}:sel{'-'.join(map(str, cfg.sel))}:"
+        sig = (f"frame:{self.nloc}a:{self.mode}:skin{self.skin:g}:"
+               f"sel{'-'.join(map(str, cfg.sel))}:"
                f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
         return autotune.tune(self.replay, lambda: self.capture(),
-                             ["desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b"],
+                             ["desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b",
+                              "pdl"],
                              signature=sig, reps=reps,
                              device=self.dev, use_cache=use_cache)
 

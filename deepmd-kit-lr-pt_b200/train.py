@@ -571,7 +571,7 @@ class SeATrainer:
                f"sel{'-'.join(map(str, cfg.sel))}:emb{'-'.join(map(str, cfg.neuron))}")
         res = autotune.tune(step, lambda: self.capture(),
                             ["train_rows_per_group", "train_warps_per_cta",
-                             "batch_atoms_per_cta"],
+                             "batch_atoms_per_cta", "pdl"],
                             signature=sig, reps=reps, device=self.dev, use_cache=use_cache)
         self.flat.detach().copy_(saved[0])
         self.adam_m.copy_(saved[1])
