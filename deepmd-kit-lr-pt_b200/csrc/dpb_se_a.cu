@@ -400,11 +400,36 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
   __syncwarp();
   // second term of dxyz for the first naxis channels, spread over the warp:
   // T[k, a] = sum_m' dD[m', a] x[k, m']
-  for (int o = lane; o < 4 * naxis; o += 32) {
-    const int k = o / naxis, a = o - k * naxis;
-    float acc = 0.f;
-    for (int mp = 0; mp < M; ++mp) acc += s_d[mp * ldd + a] * s_x[k * M + mp];
-    s_t[o] = acc;
+  if (naxis == 16 && (M & 3) == 0) {
+    // lane = (k, a) and (k + 2, a): one dD column read serves both rows of x,
+    // x read four channels at a time
+    const int a = lane & 15, k = lane >> 4;
+    const float* xa = s_x + k * M;
+    const float* xb = s_x + (k + 2) * M;
+    float acc0 = 0.f, acc1 = 0.f;
+    for (int mp = 0; mp < M; mp += 4) {
+      const float4 u = *reinterpret_cast<const float4*>(xa + mp);
+      const float4 v = *reinterpret_cast<const float4*>(xb + mp);
+      const float d0 = s_d[mp * ldd + a], d1 = s_d[(mp + 1) * ldd + a];
+      const float d2 = s_d[(mp + 2) * ldd + a], d3 = s_d[(mp + 3) * ldd + a];
+      acc0 += d0 * u.x;
+      acc1 += d0 * v.x;
+      acc0 += d1 * u.y;
+      acc1 += d1 * v.y;
+      acc0 += d2 * u.z;
+      acc1 += d2 * v.z;
+      acc0 += d3 * u.w;
+      acc1 += d3 * v.w;
+    }
+    s_t[lane] = acc0;
+    s_t[lane + 32] = acc1;
+  } else {
+    for (int o = lane; o < 4 * naxis; o += 32) {
+      const int k = o / naxis, a = o - k * naxis;
+      float acc = 0.f;
+      for (int mp = 0; mp < M; ++mp) acc += s_d[mp * ldd + a] * s_x[k * M + mp];
+      s_t[o] = acc;
+    }
   }
   __syncwarp();
   // dxyz[k, m] = sum_a dD[m, a] x[k, a] + [m < naxis] T[k, m]
