@@ -385,13 +385,30 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
   float* s_d = s_t + 4 * MAXAX;    // [M][naxis + 1], later the slot staging
   const float* xi = xyz + (size_t)i * 4 * M;
   const unsigned long long pol = l2_policy_first();
-  for (int q = lane; q < 4 * M; q += 32) s_x[q] = ld_stream(xi + q, pol);
   const float* dr = dD + (size_t)drow[i] * M * naxis;
   const int ldd = naxis + 1;  // padded row: conflict-free column reads
-  if (32 % naxis == 0) {
+  if ((M & 3) == 0 && (naxis & 3) == 0) {
+    // 16-byte loads: x rows and dD rows are 16-byte aligned when M and naxis
+    // are multiples of 4 (more loads in flight per lane)
+    const float4* x4 = reinterpret_cast<const float4*>(xi);
+    for (int q = lane; q < M; q += 32) reinterpret_cast<float4*>(s_x)[q] = ld_stream4(x4 + q, pol);
+    const float4* d4 = reinterpret_cast<const float4*>(dr);
+    const int per_row = naxis >> 2;
+    for (int q = lane; q < (M * naxis) >> 2; q += 32) {
+      const float4 v = ld_stream4(d4 + q, pol);
+      const int m = q / per_row, a = (q - m * per_row) << 2;
+      float* dst = s_d + m * ldd + a;
+      dst[0] = v.x;
+      dst[1] = v.y;
+      dst[2] = v.z;
+      dst[3] = v.w;
+    }
+  } else if (32 % naxis == 0) {
+    for (int q = lane; q < 4 * M; q += 32) s_x[q] = ld_stream(xi + q, pol);
     const int per = 32 / naxis, a = lane % naxis;
     for (int m = lane / naxis; m < M; m += per) s_d[m * ldd + a] = ld_stream(dr + m * naxis + a, pol);
   } else {
+    for (int q = lane; q < 4 * M; q += 32) s_x[q] = ld_stream(xi + q, pol);
     for (int q = lane; q < M * naxis; q += 32) {
       const int m = q / naxis, a = q - m * naxis;
       s_d[m * ldd + a] = ld_stream(dr + q, pol);
