@@ -190,18 +190,32 @@ __device__ __forceinline__ void hvalgrad2(const float2 (&c)[6], float2 x, float2
 // se[s] = em row s, sl[s] = (table row as int bits, offset in the row,
 // extrapolation distance, 0). The table coordinates are computed once per
 // slot, lane-parallel, so the channel loops only wait on coefficient loads.
+constexpr int STAGE_J = 4;  // env rows per lane requested together
+
 __device__ __forceinline__ void stage_slots(float4* se, float4* sl, const float4* erow,
                                             const TypeTables& tt, int lane) {
   const unsigned long long pol = l2_policy_first();
-  for (int t = 0; t < tt.ntypes; ++t) {
-    const FTab inf = tt.info[t];
-    for (int s = tt.sec[t] + lane; s < tt.sec[t + 1]; s += 32) {
-      const float4 e = ld_stream4(erow + s, pol);
-      int idx;
-      float xx, delta;
-      flocate(inf, e.x, idx, xx, delta);
-      se[s] = e;
-      sl[s] = make_float4(__int_as_float(idx), xx, delta, 0.f);
+  const int nnei = tt.nnei;
+  // STAGE_J rows of this lane requested before the first is used
+  for (int q0 = lane; q0 < nnei; q0 += 32 * STAGE_J) {
+    float4 ev[STAGE_J];
+#pragma unroll
+    for (int j = 0; j < STAGE_J; ++j) {
+      const int q = q0 + 32 * j;
+      if (q < nnei) ev[j] = ld_stream4(erow + q, pol);
+    }
+#pragma unroll
+    for (int j = 0; j < STAGE_J; ++j) {
+      const int q = q0 + 32 * j;
+      if (q < nnei) {
+        int t = 0;
+        while (t + 1 < tt.ntypes && q >= tt.sec[t + 1]) ++t;
+        int idx;
+        float xx, delta;
+        flocate(tt.info[t], ev[j].x, idx, xx, delta);
+        se[q] = ev[j];
+        sl[q] = make_float4(__int_as_float(idx), xx, delta, 0.f);
+      }
     }
   }
 }
