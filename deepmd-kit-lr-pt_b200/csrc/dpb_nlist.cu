@@ -163,32 +163,53 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
     count += __popc(b);
   };
   if (FROM_CELLS) {
+    // the 27 neighbor cells' atom ranges loaded at once (lane L < 27: cell
+    // (dx, dy, dz) = (L / 9, L / 3 % 3, L % 3) - 1), then one flat candidate
+    // list walked in full batches of 32; the next batch's atom indices are
+    // requested before the current batch is tested
     const GridHeader& h = *io.g.h;
     const int ci = io.g.cell_of[i];
     const int cz = ci % h.dims[2], cy = (ci / h.dims[2]) % h.dims[1],
               cx = ci / (h.dims[2] * h.dims[1]);
-    for (int dx = -1; dx <= 1; ++dx) {
-      int x = cx + dx;
-      if (x < 0 || x >= h.dims[0]) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        int y = cy + dy;
-        if (y < 0 || y >= h.dims[1]) continue;
-        for (int dz = -1; dz <= 1; ++dz) {
-          int z = cz + dz;
-          if (z < 0 || z >= h.dims[2]) continue;
-          int c = (x * h.dims[1] + y) * h.dims[2] + z;
-          int b = io.g.cell_start[c], e = io.g.cell_start[c + 1];
-          for (int base = b; base < e; base += 32) {
-            int k = base + lane;
-            unsigned long long key = 0;
-            bool ok = false;
-            if (k < e)
-              ok = accept<CT, true>(key, io.g.cell_atoms[k], i, ti, fc, ft, xi, fxi, rc2,
-                                    rc2f, ntypes, io.status);
-            push(ok, key);
-          }
-        }
+    int cb = 0, cn = 0;
+    if (lane < 27) {
+      const int x = cx + lane / 9 - 1, y = cy + (lane / 3) % 3 - 1, z = cz + lane % 3 - 1;
+      if (x >= 0 && x < h.dims[0] && y >= 0 && y < h.dims[1] && z >= 0 && z < h.dims[2]) {
+        const int c = (x * h.dims[1] + y) * h.dims[2] + z;
+        cb = io.g.cell_start[c];
+        cn = io.g.cell_start[c + 1] - cb;
       }
+    }
+    int incl = cn;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - cn;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    // atom index of flat candidate fl (-1 past the end): the cell is the last
+    // lane whose range starts at or before fl (binary search over the lanes)
+    auto cand_of = [&](int fl) -> int {
+      int lo = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1) {
+        const int ev = __shfl_sync(0xffffffffu, excl, lo + st);
+        if (ev <= fl) lo += st;
+      }
+      const int base_c = __shfl_sync(0xffffffffu, cb, lo);
+      const int start_c = __shfl_sync(0xffffffffu, excl, lo);
+      return fl < total ? io.g.cell_atoms[base_c + (fl - start_c)] : -1;
+    };
+    int jn = cand_of(lane);
+    for (int base = 0; base < total; base += 32) {
+      const int j = jn;
+      jn = cand_of(base + 32 + lane);
+      unsigned long long key = 0;
+      bool ok = false;
+      if (j >= 0)
+        ok = accept<CT, true>(key, j, i, ti, fc, ft, xi, fxi, rc2, rc2f, ntypes, io.status);
+      push(ok, key);
     }
   } else {
     const int nn = io.numneigh[row];
@@ -257,7 +278,17 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
       env_row<OT>(r, rmin, rmax, v, want_d ? gd : nullptr);
     }
     OT* e = io.em + (orow * nnei + jj) * 4;
-    if (ti >= 0) {
+    if constexpr (sizeof(OT) == 4) {
+      // 16-byte rows: one load of avg and std, one store of the env row
+      float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (ti >= 0) {
+        const float4 a4 = *reinterpret_cast<const float4*>(av + jj * 4);
+        const float4 s4 = *reinterpret_cast<const float4*>(sd + jj * 4);
+        o = make_float4((v[0] - a4.x) / s4.x, (v[1] - a4.y) / s4.y, (v[2] - a4.z) / s4.z,
+                        (v[3] - a4.w) / s4.w);
+      }
+      *reinterpret_cast<float4*>(e) = o;
+    } else if (ti >= 0) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) e[k] = (v[k] - av[jj * 4 + k]) / sd[jj * 4 + k];
     } else {
