@@ -88,6 +88,34 @@ __device__ __forceinline__ bool accept(unsigned long long& key, int j, int i,
   return true;
 }
 
+// em row = (v - avg) / std, or zeros for a center without a type row.
+template <typename OT>
+__device__ __forceinline__ void store_env_row(OT* e, const OT* a, const OT* s, const OT (&v)[4],
+                                              bool valid) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) e[k] = valid ? (v[k] - a[k]) / s[k] : (OT)0.;
+}
+// FP32 rows: one 16-byte load of avg and of std and one 16-byte store when
+// the three rows are 16-byte aligned (the same arithmetic either way)
+template <>
+__device__ __forceinline__ void store_env_row<float>(float* e, const float* a, const float* s,
+                                                     const float (&v)[4], bool valid) {
+  if (((reinterpret_cast<uintptr_t>(e) | reinterpret_cast<uintptr_t>(a) |
+        reinterpret_cast<uintptr_t>(s)) & 15) != 0) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) e[k] = valid ? (v[k] - a[k]) / s[k] : 0.f;
+    return;
+  }
+  float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (valid) {
+    const float4 a4 = *reinterpret_cast<const float4*>(a);
+    const float4 s4 = *reinterpret_cast<const float4*>(s);
+    o = make_float4((v[0] - a4.x) / s4.x, (v[1] - a4.y) / s4.y, (v[2] - a4.z) / s4.z,
+                    (v[3] - a4.w) / s4.w);
+  }
+  *reinterpret_cast<float4*>(e) = o;
+}
+
 // Shared-memory workspace of one warp (one center atom).
 template <int CAP>
 struct EnvSmem {
@@ -214,13 +242,15 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
   } else {
     const int nn = io.numneigh[row];
     const int* cand = io.firstneigh[row];
+    int jn = lane < nn ? cand[lane] : -1;  // the next batch's candidate, requested early
     for (int base = 0; base < nn; base += 32) {
-      int k = base + lane;
+      const int k = base + lane;
+      const int j = jn;
+      jn = k + 32 < nn ? cand[k + 32] : -1;
       unsigned long long key = 0;
       bool ok = false;
       if (k < nn)
-        ok = accept<CT, false>(key, cand[k], i, ti, fc, ft, xi, fxi, rc2, rc2f, ntypes,
-                               io.status);
+        ok = accept<CT, false>(key, j, i, ti, fc, ft, xi, fxi, rc2, rc2f, ntypes, io.status);
       push(ok, key);
     }
   }
@@ -278,23 +308,7 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
       env_row<OT>(r, rmin, rmax, v, want_d ? gd : nullptr);
     }
     OT* e = io.em + (orow * nnei + jj) * 4;
-    if constexpr (sizeof(OT) == 4) {
-      // 16-byte rows: one load of avg and std, one store of the env row
-      float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (ti >= 0) {
-        const float4 a4 = *reinterpret_cast<const float4*>(av + jj * 4);
-        const float4 s4 = *reinterpret_cast<const float4*>(sd + jj * 4);
-        o = make_float4((v[0] - a4.x) / s4.x, (v[1] - a4.y) / s4.y, (v[2] - a4.z) / s4.z,
-                        (v[3] - a4.w) / s4.w);
-      }
-      *reinterpret_cast<float4*>(e) = o;
-    } else if (ti >= 0) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) e[k] = (v[k] - av[jj * 4 + k]) / sd[jj * 4 + k];
-    } else {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) e[k] = (OT)0.;
-    }
+    store_env_row(e, av + jj * 4, sd + jj * 4, v, ti >= 0);
     if (want_d) {
       OT* ed = io.em_deriv + (orow * nnei + jj) * 12;
 #pragma unroll
@@ -311,7 +325,7 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
 }
 
 template <typename CT, typename OT, int CAP, int WARPS, bool FROM_CELLS>
-__global__ void __launch_bounds__(WARPS * 32)
+__global__ void __launch_bounds__(WARPS * 32, (CAP <= 256 && sizeof(OT) == 4) ? 32 / WARPS : 1)
 k_env(EnvIO<CT, OT> io, SecInfo sec, int nrows, int* redo) {
   __shared__ EnvSmem<CAP> sm[WARPS];
   pdl_wait();

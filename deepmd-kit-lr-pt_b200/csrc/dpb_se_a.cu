@@ -401,9 +401,9 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
   const unsigned long long pol = l2_policy_first();
   const float* dr = dD + (size_t)drow[i] * M * naxis;
   const int ldd = naxis + 1;  // padded row: conflict-free column reads
-  if ((M & 3) == 0 && (naxis & 3) == 0) {
-    // 16-byte loads: x rows and dD rows are 16-byte aligned when M and naxis
-    // are multiples of 4 (more loads in flight per lane)
+  if ((M & 3) == 0 && (naxis & 3) == 0 &&
+      ((reinterpret_cast<uintptr_t>(xi) | reinterpret_cast<uintptr_t>(dr)) & 15) == 0) {
+    // 16-byte loads (more loads in flight per lane) where the rows allow
     const float4* x4 = reinterpret_cast<const float4*>(xi);
     for (int q = lane; q < M; q += 32) reinterpret_cast<float4*>(s_x)[q] = ld_stream4(x4 + q, pol);
     const float4* d4 = reinterpret_cast<const float4*>(dr);
@@ -635,7 +635,7 @@ k_force_virial(double* __restrict__ force, double* __restrict__ virial,
 // the neighbor list instead of being read back (same formulas and precision
 // as the env kernels, dpb_envmath.cuh): the forward pass then stores only em.
 template <typename CT, typename OT>
-__global__ void __launch_bounds__(SW * 32)
+__global__ void __launch_bounds__(SW * 32, sizeof(OT) == 4 ? 24 / SW : 1)
 k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
                   const OT* __restrict__ nd, const CT* __restrict__ coord,
                   const int* __restrict__ type, const OT* __restrict__ std_,
@@ -657,21 +657,37 @@ k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
   const OT* sd = std_ + (size_t)ti * nnei * 4;
   const OT* ndr = nd + (size_t)i * nnei * 4;
   double c0 = 0., c1 = 0., c2 = 0.;
+  // 16-byte rows of net_deriv and std when both arrays are 16-byte aligned
+  const bool vec16 = ((reinterpret_cast<uintptr_t>(ndr) | reinterpret_cast<uintptr_t>(sd)) & 15) == 0;
+  const int* nl = nlist + (size_t)i * nnei;
+  int jn = lane < nnei ? nl[lane] : -1;  // the next slot's neighbor, requested early
   for (int jj = lane; jj < nnei; jj += 32) {
-    const int j = nlist[(size_t)i * nnei + jj];
+    const int j = jn;
+    jn = jj + 32 < nnei ? nl[jj + 32] : -1;
     if (j < 0) continue;  // padding: em_deriv = 0
     OT r[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) r[d] = (OT)(coord[3 * j + d] - xi[d]);
+    OT nv[4], sv[4];
+    if (sizeof(OT) == 4 && vec16) {
+      const float4 n4 = *reinterpret_cast<const float4*>(ndr + jj * 4);
+      const float4 s4 = *reinterpret_cast<const float4*>(sd + jj * 4);
+      nv[0] = n4.x, nv[1] = n4.y, nv[2] = n4.z, nv[3] = n4.w;
+      sv[0] = s4.x, sv[1] = s4.y, sv[2] = s4.z, sv[3] = s4.w;
+    } else {
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        nv[a] = ndr[jj * 4 + a];
+        sv[a] = sd[jj * 4 + a];
+      }
+    }
     OT v[4], gd[12];
     env_row<OT>(r, rcut_smth, rcut, v, gd);
     OT p[3] = {(OT)0., (OT)0., (OT)0.};
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-      const OT n = ndr[jj * 4 + a];
-      const OT s = sd[jj * 4 + a];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) p[d] += n * (gd[a * 3 + d] / s);
+      for (int d = 0; d < 3; ++d) p[d] += nv[a] * (gd[a * 3 + d] / sv[a]);
     }
     const double q[3] = {(double)p[0], (double)p[1], (double)p[2]};
     c0 += q[0];
