@@ -113,58 +113,84 @@ k_bt_env(ET* __restrict__ em, int* __restrict__ nlist, const double* __restrict_
   int count = 0;
   const int ci = cell_of[row];
   const int cz = ci % nz, cy = (ci / nz) % ny, cx = ci / (nz * ny);
-  for (int dx = -1; dx <= 1; ++dx)
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dz = -1; dz <= 1; ++dz) {
-        // lattice cell (cx+dx, cy+dy, cz+dz) = stored cell (wrapped) + image
-        int X = cx + dx, Y = cy + dy, Z = cz + dz;
-        const int sx = X < 0 ? -1 : (X >= nx ? 1 : 0);
-        const int sy = Y < 0 ? -1 : (Y >= ny ? 1 : 0);
-        const int sz = Z < 0 ? -1 : (Z >= nz ? 1 : 0);
-        X -= sx * nx;
-        Y -= sy * ny;
-        Z -= sz * nz;
-        const int code = (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1);
+  // lane L < 27 owns lattice cell (cx, cy, cz) + (L / 9, L / 3 % 3, L % 3) - 1:
+  // its stored (wrapped) cell's atom range and its image code; the 27 ranges
+  // are then walked as one flat list in full batches of 32, the next batch's
+  // atom indices requested before the current batch is tested
+  int cb = 0, cn = 0, ccode = 13;
+  if (lane < 27) {
+    int X = cx + lane / 9 - 1, Y = cy + (lane / 3) % 3 - 1, Z = cz + lane % 3 - 1;
+    const int sx = X < 0 ? -1 : (X >= nx ? 1 : 0);
+    const int sy = Y < 0 ? -1 : (Y >= ny ? 1 : 0);
+    const int sz = Z < 0 ? -1 : (Z >= nz ? 1 : 0);
+    X -= sx * nx;
+    Y -= sy * ny;
+    Z -= sz * nz;
+    ccode = (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1);
+    const int c = (X * ny + Y) * nz + Z;
+    cb = cs[c];
+    cn = cs[c + 1] - cb;
+  }
+  int incl = cn;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int excl = incl - cn;
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  // atom (-1 past the end) and image code of flat candidate fl
+  auto cand_of = [&](int fl, int& code) -> int {
+    int lo = 0;
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1) {
+      const int ev = __shfl_sync(0xffffffffu, excl, lo + st);
+      if (ev <= fl) lo += st;
+    }
+    const int base_c = __shfl_sync(0xffffffffu, cb, lo);
+    const int start_c = __shfl_sync(0xffffffffu, excl, lo);
+    code = __shfl_sync(0xffffffffu, ccode, lo);
+    return fl < total ? ca[base_c + (fl - start_c)] : -1;
+  };
+  int coden = 13;
+  int jn = cand_of(lane, coden);
+  for (int base = 0; base < total; base += 32) {
+    const int j = jn, code = coden;
+    jn = cand_of(base + 32 + lane, coden);
+    bool ok = false;
+    unsigned long long key = 0;
+    if (j >= 0) {
+      const int tj = ft[j];
+      if (tj >= 0 && tj < ntypes && ti >= 0 && !(j == i && code == 13)) {
+        const int sx = code / 9 - 1, sy = (code / 3) % 3 - 1, sz = code % 3 - 1;
         const double sh[3] = {sx * L[0], sy * L[1], sz * L[2]};
-        const int c = (X * ny + Y) * nz + Z;
-        const int b = cs[c], e = cs[c + 1];
-        for (int base = b; base < e; base += 32) {
-          const int k = base + lane;
-          bool ok = false;
-          unsigned long long key = 0;
-          if (k < e) {
-            const int j = ca[k];
-            const int tj = ft[j];
-            if (tj >= 0 && tj < ntypes && ti >= 0 && !(j == i && code == 13)) {
-              // the image's position, then the single-frame path's two tests
-              const double g0 = fc[3 * j] + sh[0], g1 = fc[3 * j + 1] + sh[1],
-                           g2 = fc[3 * j + 2] + sh[2];
-              const double d0 = sub_rn(xi[0], g0), d1 = sub_rn(xi[1], g1),
-                           d2 = sub_rn(xi[2], g2);
-              if (dot3_rn(d0, d1, d2) < rc2) {
-                const float e0 = sub_rn((float)g0, fxi[0]), e1 = sub_rn((float)g1, fxi[1]),
-                            e2 = sub_rn((float)g2, fxi[2]);
-                const float r2 = dot3_rn(e0, e1, e2);
-                if (r2 <= rc2f) {
-                  ok = true;
-                  key = ((unsigned long long)tj << 56) |
-                        ((unsigned long long)__float_as_uint(r2) << 24) |
-                        (unsigned long long)(j * 27 + code);
-                }
-              }
-            }
+        // the image's position, then the single-frame path's two tests
+        const double g0 = fc[3 * j] + sh[0], g1 = fc[3 * j + 1] + sh[1],
+                     g2 = fc[3 * j + 2] + sh[2];
+        const double d0 = sub_rn(xi[0], g0), d1 = sub_rn(xi[1], g1), d2 = sub_rn(xi[2], g2);
+        if (dot3_rn(d0, d1, d2) < rc2) {
+          const float e0 = sub_rn((float)g0, fxi[0]), e1 = sub_rn((float)g1, fxi[1]),
+                      e2 = sub_rn((float)g2, fxi[2]);
+          const float r2 = dot3_rn(e0, e1, e2);
+          if (r2 <= rc2f) {
+            ok = true;
+            key = ((unsigned long long)tj << 56) |
+                  ((unsigned long long)__float_as_uint(r2) << 24) |
+                  (unsigned long long)(j * 27 + code);
           }
-          const unsigned bal = __ballot_sync(0xffffffffu, ok);
-          if (ok) {
-            const int pos = count + __popc(bal & bt_lanemask_lt());
-            if (pos < BT_CAP) {
-              sm.keys[pos] = key;
-              atomicAdd(&sm.tcnt[key >> 56], 1);
-            }
-          }
-          count += __popc(bal);
         }
       }
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+    if (ok) {
+      const int pos = count + __popc(bal & bt_lanemask_lt());
+      if (pos < BT_CAP) {
+        sm.keys[pos] = key;
+        atomicAdd(&sm.tcnt[key >> 56], 1);
+      }
+    }
+    count += __popc(bal);
+  }
   __syncwarp();
   if (count > BT_CAP && lane == 0) atomicOr(status, ST_NLIST_CAPACITY);
   const int n = count < BT_CAP ? count : BT_CAP;
