@@ -747,8 +747,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             "bytes_per_launch": gather, "slots_evaluated": slots,
             "achieved_tbs": gather / (ours[dom] * 1e-3) / 1e12, "nominal_l1_tbs": l1_peak,
             "frac": gather / (ours[dom] * 1e-3) / 1e12 / l1_peak,
-            "note": "table-row gathers through L1/TEX (ncu: L1/TEX 69% busy in k_desc_bwd, "
-                    "88% in k_desc_fwd, DRAM 5%); the HBM fraction above is low by "
+            "note": "table-row gathers through L1/TEX (ncu: L1/TEX 73% busy in k_desc_bwd, "
+                    "89% in k_desc_fwd, DRAM 5-6%); the HBM fraction above is low by "
                     "construction"}
     # every stage against its own roof: HBM bytes for the memory stages, the
     # tensor pipe for the fitting GEMMs (3xTF32: three TF32 products per FP32
