@@ -193,9 +193,35 @@ class CpuReference:
         return time.perf_counter() - t0
 
 
+# ------------------------------------------------------------ ranks (N > 1) --
+# Frames are independent: each rank evaluates its own frame (seeded by its
+# rank, same size), no data-path collective; the only cross-rank operations
+# are the barriers around the timed region and the max of the step times.
+def frame_seed(rank: int) -> int:
+    """Seed of the water frame evaluated by `rank`."""
+    return 100 + rank
+
+
+def max_over_ranks(v: float, world: int, device) -> float:
+    """The largest of every rank's `v` (all ranks call it in the same order)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_us_per_atom(ms_step: float, nloc: int, world: int) -> float:
+    """Whole-job throughput: world frames of nloc atoms per step of ms_step."""
+    return ms_step * 1e3 / (nloc * world)
+
+
 def _setup_frame(mdl, wl, tab, rank: int, device):
     cfg = mdl.SeAConfig()
-    coord, atype, box = wl.water_frame(N_SIDE, seed=100 + rank)
+    coord, atype, box = wl.water_frame(N_SIDE, seed=frame_seed(rank))
     params = mdl.init_params(cfg, seed=PARAM_SEED)
     mdl.prepare(params, coord, atype, box, device=device)
     return cfg, params, coord, atype, box
@@ -594,12 +620,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         torch.cuda.synchronize()
         return [x.elapsed_time(y) for x, y in ts]
 
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     # ---- device-resident timed region (CUDA graph replay, L2 flushed between).
     # The clock sampler (200 ms period) runs from the warm-up through the e2e
@@ -620,8 +640,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier()
-    ms_step = max_over_ranks(float(np.sum(ms)) / args.steps)
-    value = ms_step * 1e3 / (nloc * world)
+    ms_step = max_over_ranks(float(np.sum(ms)) / args.steps, world, device)
+    value = whole_job_us_per_atom(ms_step, nloc, world)
 
     # ---- end to end through the public call: pinned host in, pinned host out
     host_c = torch.tensor(coord, dtype=torch.float64).pin_memory()
@@ -636,7 +656,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         t0 = time.perf_counter()
         ev.compute(host_c, out=host_out)
         e2e.append(time.perf_counter() - t0)
-    e2e_ms = max_over_ranks(float(np.mean(e2e)) * 1e3)
+    e2e_ms = max_over_ranks(float(np.mean(e2e)) * 1e3, world, device)
     clk = clocks.stop()
     ev.check()
 
@@ -673,7 +693,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         for _ in range(2):
             plain.replay()
         kp = max(3, min(args.steps, 10))
-        ms_plain = max_over_ranks(float(np.mean(timed_steps(plain, kp))))
+        ms_plain = max_over_ranks(float(np.mean(timed_steps(plain, kp))), world, device)
         Ec, Fc, Vc = ev.compute(coord)
         acc = {"vs": "FP64 plain GPU path (matches the reference PyTorch model to 1e-10 in tests)",
                "energy_err_ev_per_atom": abs(Ec - Ep) / nloc,
@@ -792,7 +812,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                                     "differences and energy/force/virial sums",
                        "l2": "256 MiB buffer written between timed steps",
                        "graph": "one CUDA graph per step"},
-            "e2e": {"value": e2e_ms * 1e3 / (nloc * world), "unit": UNIT,
+            "e2e": {"value": whole_job_us_per_atom(e2e_ms, nloc, world), "unit": UNIT,
                     "h2d_bytes_per_step": nloc * 3 * 8,
                     "d2h_bytes_per_step": (1 + 3 * nloc + 9) * 8},
             "gpu_launches": None if launches_per_step is None else launches_per_step * args.steps,
