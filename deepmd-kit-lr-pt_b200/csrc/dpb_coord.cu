@@ -594,10 +594,10 @@ int grid_build(void* grid, long long bytes, const T* coord, int nall,
 
 // ------------------------------------------------- fused geometry pass ----
 // normalize_coord + copy_coord + cell grid of one frame as ONE cooperative
-// launch (one 512-thread block per SM). The separate path above takes twelve
-// small launches and three memsets, each a few microseconds of latency for a
-// few hundred kilobytes of work; here the phases are separated by four
-// grid-wide barriers instead:
+// launch (64 blocks of 512 threads, at most one per SM). The separate path
+// above takes twelve small launches and three memsets, each a few
+// microseconds of latency for a few hundred kilobytes of work; here the
+// phases are separated by four grid-wide barriers instead:
 //   P0 local atoms: wrap into the box, copy-grid cell and a slot in it
 //      (atomic count), local part of the extended arrays, bounding box keys
 //   P1 every block scans the copy-cell counts in its own shared memory (no
@@ -624,6 +624,7 @@ int grid_build(void* grid, long long bytes, const T* coord, int nall,
 constexpr int GEO_THREADS = 512;
 constexpr int GEO_SCAN_CAP = 32768;  // ints of the block-local scans
 constexpr int GEO_SORT_CAP = 256;    // per-warp buffer of one cell's atoms
+constexpr int GEO_BLOCKS = 64;       // CTAs of the cooperative launch (at most the SMs)
 constexpr unsigned long long GEO_WAIT_NS = 200000000ull;  // per barrier
 
 struct GeoHeader {
@@ -1012,7 +1013,10 @@ int geometry_cells(double* cext, int* text, int* mapping, int* nall_dev, void* g
       DPB_CUDA(cudaMemsetAsync(scratch, 0, 256 + sizeof(int) * (size_t)r.nloc_cells, st),
                "geometry_cells");
       void* args[] = {&a};
-      DPB_CUDA(cudaLaunchCooperativeKernel((const void*)k_geometry, dim3(sm_count()),
+      // 64 CTAs: every phase is grid-stride and small, and each barrier costs
+      // one arrival per CTA
+      const int blocks = sm_count() < GEO_BLOCKS ? sm_count() : GEO_BLOCKS;
+      DPB_CUDA(cudaLaunchCooperativeKernel((const void*)k_geometry, dim3(blocks),
                                            dim3(GEO_THREADS), args, smem, st),
                "geometry_cells");
       return DPB_OK;

@@ -642,7 +642,7 @@ static int make_map(CUtensorMap* m, const float* base, int rows, int cols, int b
 // part[b]; the last block to finish (ticket) adds the partials in block order,
 // so the bits do not depend on scheduling, and resets the ticket.
 constexpr int ES_MAXB = 148;
-constexpr int ES_ROWS = 4096;  // rows per block at least
+constexpr int ES_ROWS = 1024;  // rows per block at least
 
 __global__ void __launch_bounds__(512) k_energy_sum(double* energy, float* e, int n,
                                                     double e_const, double* part,
