@@ -94,7 +94,9 @@ def test_tile_knob_registry(dpb):
     names = autotune.names()
     assert {"desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b",
             "batch_atoms_per_cta",
-            "train_rows_per_group", "train_warps_per_cta"} <= set(names)
+            "train_rows_per_group", "train_warps_per_cta", "geometry_fused",
+            "pdl"} <= set(names)
+    assert autotune.options("pdl") == [0, 1] and autotune.options("geometry_fused") == [0, 1]
     for n in names:
         opts = autotune.options(n)
         old = autotune.get(n)
@@ -106,3 +108,22 @@ def test_tile_knob_registry(dpb):
         autotune.set_knob("desc_atoms_per_cta", 3)
     with pytest.raises(dpb._capi.DPBInvalidArgument):
         autotune.get("no_such_knob")
+
+
+def test_step_scratch_sizes(dpb):
+    """Host-side sizes of the single-frame step's buffers (no device needed):
+    the geometry pass's scratch also covers its separate-kernel fallback, and
+    the energy-sum work buffer holds one partial per block plus the ticket."""
+    import ctypes
+
+    import numpy as np
+
+    lib = dpb._capi.lib()
+    box = np.diag([49.67, 49.67, 49.67]).reshape(9).astype(np.float64)
+    rc = ctypes.c_float(6.0)
+    geo = int(lib.dpb_geometry_scratch_bytes(12288, rc, box.ctypes.data))
+    sep = int(lib.dpb_copy_coord_scratch_bytes(12288, rc, box.ctypes.data))
+    assert geo >= sep > 0
+    # three ints per local atom at least (cell, slot, order)
+    assert geo >= 3 * 4 * 12288
+    assert int(lib.dpb_fit_energy_sum_work_bytes()) >= 8 * 149
