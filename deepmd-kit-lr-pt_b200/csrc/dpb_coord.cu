@@ -9,6 +9,7 @@
 // (source/lib/src/gpu/coord.cu:352-414) emits a different ghost order; this
 // one matches the CPU path so that neighbor indices compare bit for bit.
 #include <math.h>
+#include <atomic>
 
 #include "dpb_common.cuh"
 #include "dpb_internal.cuh"
@@ -974,15 +975,18 @@ int geometry_cells(double* cext, int* text, int* mapping, int* nall_dev, void* g
   if (fused) {
     const int scan_ints = (int)(copy_ints > gcap + 1 ? copy_ints : gcap + 1);
     const size_t smem = (size_t)scan_ints * 4 + (size_t)(GEO_THREADS / 32) * GEO_SORT_CAP * 4;
-    static unsigned long long attr_devs = 0;  // devices whose limit is raised
+    // devices whose shared-memory limit is raised; atomic so that host
+    // threads calling this concurrently do not race on the mask (setting the
+    // attribute twice is harmless)
+    static std::atomic<unsigned long long> attr_devs{0};
     int dev = 0;
     DPB_CUDA(cudaGetDevice(&dev), "geometry_cells");
-    if (dev < 64 && !(attr_devs >> dev & 1ull)) {
+    if (dev < 64 && !(attr_devs.load(std::memory_order_acquire) >> dev & 1ull)) {
       const int most = GEO_SCAN_CAP * 4 + (GEO_THREADS / 32) * GEO_SORT_CAP * 4;
       DPB_CUDA(cudaFuncSetAttribute(k_geometry, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     most),
                "geometry_cells");
-      attr_devs |= 1ull << dev;
+      attr_devs.fetch_or(1ull << dev, std::memory_order_acq_rel);
     }
     int occ = 0;
     DPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_geometry, GEO_THREADS,

@@ -9,13 +9,20 @@
 // the file-scope device array below (DPB_NOALLOC_SCRATCH_BYTES, 4 MiB). Every
 // GPU that loads the library holds that array until the process exits.
 //
+// The array holds the cell grid of nall extended atoms plus two status words:
+// dpb_cell_grid_bytes(nall) + 256 <= 4 MiB, i.e. nall <= 209,670 (about 20
+// bytes per extended atom); larger calls are rejected before any GPU work.
+//
 // The device address of the array is looked up with cudaGetSymbolAddress the
 // first time the entry point runs on a device (with that device current) and
-// cached per device. Every call shares the one array per device and leaves
-// its contents behind; the parts that must start at zero (status words, cell
-// counters, bounding box) are reset by each call. Two calls whose work
-// overlaps on the same GPU (e.g. from two host threads on different streams)
-// race on the array and must not be issued.
+// cached per device for the life of the process; make that first call before
+// any stream capture. The cached address belongs to the device's current
+// context: a process that destroys it (cudaDeviceReset) must not call this
+// entry point on that device again. Every call shares the one array per
+// device and leaves its contents behind; the parts that must start at zero
+// (status words, cell counters, bounding box) are reset by each call. Two
+// calls whose work overlaps on the same GPU (e.g. from two host threads on
+// different streams) race on the array and must not be issued.
 #include <mutex>
 
 #include "dpb_common.cuh"

@@ -677,10 +677,12 @@ DPB_API int dpb_tune_set(const char* name, int value);
  * list as dpb_build_nlist_f64 (same arguments and results) without the
  * caller scratch. Its working memory is a 4 MiB file-scope device array in
  * the library (held by every GPU that loads it until exit), which limits nall
- * to what fits (dpb_cell_grid_bytes(nall) + 256 <= 4 MiB, about 260k atoms);
- * larger sizes are rejected with DPB_ERR_INVALID. The first call on a device
- * looks up the array's device address (call it before any stream capture).
- * All calls share the array: calls that overlap on the same GPU race. */
+ * to what fits (dpb_cell_grid_bytes(nall) + 256 <= 4 MiB, i.e. nall <= 209,670
+ * extended atoms); larger sizes are rejected with DPB_ERR_INVALID. The first
+ * call on a device looks up the array's device address and caches it for the
+ * life of the device's context (call it before any stream capture; after a
+ * cudaDeviceReset do not call it on that device again). All calls share the
+ * array: calls that overlap on the same GPU race. */
 DPB_API long long dpb_build_nlist_noalloc_max_bytes(void);
 DPB_API int dpb_build_nlist_noalloc_f64(int* ilist, int* numneigh,
                                         int** firstneigh, int* max_list_size,

@@ -101,20 +101,12 @@ def _fit(f, x):
     return (h @ torch.from_numpy(Wo) + torch.from_numpy(bo)).view(-1)
 
 
-def evaluate(lib, params, coord, atype, box, mode="plain"):
-    """(energy, force [nloc, 3], virial [9]) in FP64; mode plain|compressed."""
+def _network_rows(lib, params, em_rows, atype_rows, mode):
+    """Energy of a block of centers and its gradient w.r.t. their env rows."""
     cfg = params.cfg
-    nloc = atype.size
-    cn = lib.normalize_coord(np.asarray(coord, np.float64).reshape(-1), box).reshape(-1, 3)
-    c, t, mapping = lib.copy_coord(cn, atype, cfg.rcut, box)
-    nall = c.shape[0]
-    ret, il, nn, rb, _ = lib.build_nlist(c, nloc, cfg.rcut, atype=t, mem_size=nall)
-    assert ret == 0
-    em, emd, rij, nlist = lib.prod_env_mat_a(c, t, il, nn, rb, params.davg, params.dstd, nloc,
-                                             cfg.rcut, cfg.rcut_smth, cfg.sec)
-    nnei = cfg.nnei
-    emt = torch.from_numpy(em.reshape(nloc, nnei, 4).copy()).requires_grad_(True)
-    xyz = torch.zeros((nloc, 4, cfg.neuron[-1]), dtype=torch.float64)
+    n, nnei = atype_rows.size, cfg.nnei
+    emt = torch.from_numpy(em_rows.reshape(n, nnei, 4).copy()).requires_grad_(True)
+    xyz = torch.zeros((n, 4, cfg.neuron[-1]), dtype=torch.float64)
     sec = cfg.sec
     for ty in range(cfg.ntypes):
         a, b = int(sec[ty]), int(sec[ty + 1])
@@ -128,19 +120,46 @@ def evaluate(lib, params, coord, atype, box, mode="plain"):
             table, info = params.tables[ty]
             xyz = xyz + _Tab.apply(rr, lib, np.ascontiguousarray(table), info, cfg.neuron[-1])
     xyz = xyz / nnei
-    D = (xyz.transpose(1, 2) @ xyz[:, :, :cfg.axis_neuron]).reshape(nloc, -1)
+    D = (xyz.transpose(1, 2) @ xyz[:, :, :cfg.axis_neuron]).reshape(n, -1)
     E = torch.zeros((), dtype=torch.float64)
     for ty in range(cfg.ntypes):
-        sel = np.nonzero(atype == ty)[0]
+        sel = np.nonzero(atype_rows == ty)[0]
         if sel.size:
             E = E + (_fit(params.fit[ty], D[torch.from_numpy(sel)]) + params.bias_atom_e[ty]).sum()
     (g,) = torch.autograd.grad(E, emt)
-    nd = g.reshape(nloc, nnei * 4).numpy()
+    return float(E.detach()), g.reshape(n, nnei * 4).numpy()
+
+
+def evaluate(lib, params, coord, atype, box, mode="plain", chunk=None):
+    """(energy, force [nloc, 3], virial [9]) in FP64; mode plain|compressed.
+
+    ``chunk`` evaluates the network over blocks of that many centers (the
+    atomic energies are independent, so the result is the same; only the
+    host memory of the autograd graph is bounded)."""
+    cfg = params.cfg
+    nloc = atype.size
+    cn = lib.normalize_coord(np.asarray(coord, np.float64).reshape(-1), box).reshape(-1, 3)
+    c, t, mapping = lib.copy_coord(cn, atype, cfg.rcut, box)
+    nall = c.shape[0]
+    ret, il, nn, rb, _ = lib.build_nlist(c, nloc, cfg.rcut, atype=t, mem_size=nall)
+    assert ret == 0
+    em, emd, rij, nlist = lib.prod_env_mat_a(c, t, il, nn, rb, params.davg, params.dstd, nloc,
+                                             cfg.rcut, cfg.rcut_smth, cfg.sec)
+    nnei = cfg.nnei
+    em = em.reshape(nloc, nnei * 4)
+    step = nloc if not chunk else int(chunk)
+    E = 0.0
+    nd = np.zeros((nloc, nnei * 4))
+    for a in range(0, nloc, step):
+        b = min(nloc, a + step)
+        e, g = _network_rows(lib, params, em[a:b], np.asarray(atype)[a:b], mode)
+        E += e
+        nd[a:b] = g
     fext = lib.prod_force_a(nd, emd, nlist, nloc, nall)[0]
     force = np.zeros((nloc, 3))
     np.add.at(force, mapping, fext)
     virial, _ = lib.prod_virial_a(nd, emd, rij, nlist, nloc, nall)
-    return float(E.detach()), force, virial
+    return E, force, virial
 
 
 # ----------------------------------------------------------------- training --

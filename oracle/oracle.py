@@ -30,18 +30,27 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "libdporacle.so")
 REF_SO = os.path.join(HERE, "_ref", "libdpref.so")
 REF_GPU_SO = os.path.join(HERE, "_ref", "libdpref_gpu.so")
-REF_TREE = "/root/reference"
+# the reference source tree, given by the environment (no built-in location)
+REF_TREE = os.environ.get("DEEPMD_REFERENCE_TREE", "")
 
 _i = ctypes.c_int
 _f = ctypes.c_float
 _p = ctypes.c_void_p
 
 
-def build(ref: bool | None = None, ref_gpu: bool | None = None) -> None:
+def _have_tree(tree: str) -> bool:
+    return bool(tree) and os.path.isdir(os.path.join(tree, "source", "lib"))
+
+
+def build(ref: bool | None = None, ref_gpu: bool | None = None,
+          ref_tree: str | None = None) -> None:
     """Compile the checkers with ``make -C oracle`` (the reference libraries
-    only when its sources exist; the GPU one also needs nvcc)."""
+    only when its source tree is given -- ``ref_tree`` or the environment
+    variable DEEPMD_REFERENCE_TREE -- and exists; the GPU one also needs
+    nvcc)."""
+    tree = ref_tree if ref_tree is not None else REF_TREE
     targets = ["port"]
-    have_tree = os.path.isdir(os.path.join(REF_TREE, "source", "lib"))
+    have_tree = _have_tree(tree)
     if ref is None:
         ref = have_tree
     if ref_gpu is None:
@@ -50,7 +59,8 @@ def build(ref: bool | None = None, ref_gpu: bool | None = None) -> None:
         targets.append("ref")
     if ref_gpu:
         targets.append("refgpu")
-    subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
+    extra = [f"REF={tree}"] if have_tree else []
+    subprocess.run(["make", "-s", "-C", HERE, *targets, *extra], check=True)
 
 
 def _ptr(a):
@@ -257,7 +267,7 @@ def ref() -> _Lib | None:
     """The compiled reference CPU library, or None where it was not built."""
     if "ref" not in _cache:
         if not os.path.exists(REF_SO):
-            if os.path.isdir(os.path.join(REF_TREE, "source", "lib")):
+            if _have_tree(REF_TREE):
                 build(ref=True)
             else:
                 return None

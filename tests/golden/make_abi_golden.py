@@ -6,7 +6,7 @@ A translation unit that takes the address of every float/double
 instantiation is compiled against the reference headers; its undefined
 symbols are the names a binary linked against the reference expects.
 
-    python tests/golden/make_abi_golden.py [/root/reference]
+    python tests/golden/make_abi_golden.py [REFERENCE_TREE]  (or DEEPMD_REFERENCE_TREE in the environment)
 """
 
 import os
@@ -14,7 +14,10 @@ import subprocess
 import sys
 import tempfile
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("give the reference source tree as the first argument or in "
+                     "DEEPMD_REFERENCE_TREE")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_abi_symbols.txt")
 
 FUNCS = ["build_nlist_gpu", "prod_env_mat_a_gpu", "tabulate_fusion_se_a_gpu",

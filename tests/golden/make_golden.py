@@ -14,7 +14,7 @@ hold for the se_e2_a path and stores them as numpy arrays, keyed
 
 Run in a container that holds the reference tree:
 
-    python tests/golden/make_golden.py [/root/reference]
+    python tests/golden/make_golden.py [REFERENCE_TREE]  (or DEEPMD_REFERENCE_TREE in the environment)
 
 The output is committed; nothing at test time reads the reference tree.
 """
@@ -28,7 +28,10 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("give the reference source tree as the first argument or in "
+                     "DEEPMD_REFERENCE_TREE")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_fixtures.npz")
 
 CC_FILES = [

@@ -8,7 +8,7 @@ reference tree through ref_import_shim) is loaded with those weights and run
 in FP64 on the CPU. Stored: the frame, the statistics, a weight checksum and
 the reference E/F/V, plus the FP64 oracle's compressed-model E/F/V.
 
-    python tests/golden/make_model_golden.py [/root/reference]
+    python tests/golden/make_model_golden.py [REFERENCE_TREE]  (or DEEPMD_REFERENCE_TREE in the environment)
 """
 
 from __future__ import annotations
@@ -21,7 +21,10 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("give the reference source tree as the first argument or in "
+                     "DEEPMD_REFERENCE_TREE")
 OUT = os.path.join(HERE, "model_golden.npz")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)

@@ -10,7 +10,7 @@ deepmd/utils/tabulate.py) makes the tables. Stored per embedding net: the
 table_info, the table shape and every 32nd row (plus the last) of the
 [nspline, 6M] FP64 table.
 
-    python tests/golden/make_table_golden.py [/root/reference]
+    python tests/golden/make_table_golden.py [REFERENCE_TREE]  (or DEEPMD_REFERENCE_TREE in the environment)
 """
 
 from __future__ import annotations

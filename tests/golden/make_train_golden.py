@@ -12,7 +12,7 @@ gradient. Stored per weight tensor: its full gradient when it has at most
 projections on seeded Gaussian directions (numpy default_rng(1000 + k) for
 the k-th tensor in name order).
 
-    python tests/golden/make_train_golden.py [/root/reference]
+    python tests/golden/make_train_golden.py [REFERENCE_TREE]  (or DEEPMD_REFERENCE_TREE in the environment)
 """
 
 from __future__ import annotations
@@ -25,7 +25,10 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
+if not REF or not os.path.isdir(REF):
+    raise SystemExit("give the reference source tree as the first argument or in "
+                     "DEEPMD_REFERENCE_TREE")
 OUT = os.path.join(HERE, "train_golden.npz")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)

@@ -27,7 +27,19 @@ class _Stub(types.ModuleType):
         return _Stub(self.__name__ + "()")
 
 
-def install(ref_root: str = "/root/reference") -> None:
+def reference_tree(argv_index: int = 1) -> str:
+    """The reference source tree: the script's argument, else the
+    environment variable DEEPMD_REFERENCE_TREE."""
+    tree = sys.argv[argv_index] if len(sys.argv) > argv_index else \
+        os.environ.get("DEEPMD_REFERENCE_TREE", "")
+    if not tree or not os.path.isdir(tree):
+        raise SystemExit("give the reference source tree as the first argument or in "
+                         "DEEPMD_REFERENCE_TREE")
+    return tree
+
+
+def install(ref_root: str | None = None) -> None:
+    ref_root = ref_root or reference_tree()
     if ref_root not in sys.path:
         sys.path.insert(0, ref_root)
     import torch

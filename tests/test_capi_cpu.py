@@ -127,3 +127,22 @@ def test_step_scratch_sizes(dpb):
     # three ints per local atom at least (cell, slot, order)
     assert geo >= 3 * 4 * 12288
     assert int(lib.dpb_fit_energy_sum_work_bytes()) >= 8 * 149
+
+
+def test_noalloc_size_limit_host_side(dpb):
+    """The allocation-free neighbor list accepts nall up to the figure its
+    documentation gives (dpb_cell_grid_bytes(nall) + 256 <= its 4 MiB array:
+    209,670 extended atoms) and rejects one more before touching a device."""
+    import ctypes
+
+    cap = dpb._capi
+    lib = cap.lib()
+    limit = int(lib.dpb_build_nlist_noalloc_max_bytes())
+    assert limit == 4 << 20
+    nmax = 209_670
+    assert lib.dpb_cell_grid_bytes(nmax) + 256 <= limit
+    assert lib.dpb_cell_grid_bytes(nmax + 1) + 256 > limit
+    # the rejection happens on the host, before any CUDA call
+    code = lib.dpb_build_nlist_noalloc_f64(None, None, None, None, None, 16, nmax + 1, 64,
+                                           ctypes.c_float(6.0), 1, None, None)
+    assert code == 2 and "built-in array" in cap.last_error()
