@@ -22,8 +22,8 @@ ours:      the compressed FP32 path (FP64 coordinate differences and sums),
 reference: the reference's own CPU implementation (deepmd:: *_cpu functions
            compiled from the reference sources, FP64, OpenMP where the
            reference has it, the fitting net in FP64 torch on all host cores)
-           on bounded samples of the same workload (a subset of center atoms
-           per step; per-atom cost does not depend on which atoms).
+           on the same frame, every atom a center in every step; this arm
+           does not load the project's GPU library.
 """
 
 from __future__ import annotations
@@ -46,7 +46,7 @@ METRIC = "us/step/atom, se_e2_a water: mixed-precision vs FP64 plain on same B20
 UNIT = "us/step/atom"
 N_SIDE = 16          # 16^3 molecules = 12,288 atoms
 PARAM_SEED = 1
-CPU_SAMPLE_ATOMS = 1024
+CPU_STEPS = 20      # steps of the CPU baseline leg (whole frame each)
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -117,9 +117,29 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------- CPU reference --
+def _workload_module():
+    """The seeded input generator (numpy only) loaded on its own, without the
+    package: the reference arm must not load this project's GPU library."""
+    import importlib.util
+
+    name = "dpb_workload_standalone"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(ROOT, "deepmd-kit-lr-pt_b200", "workload.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 class CpuReference:
     """The reference CPU path (oracle/_ref: deepmd:: *_cpu compiled from the
-    reference sources; the restatement where that library is absent)."""
+    reference sources; the restatement where that library is absent), FP64:
+    normalize_coord_cpu, copy_coord_cpu, build_nlist_cpu, prod_env_mat_a_cpu,
+    tabulate_fusion_se_a_cpu per neighbor type, the descriptor and fitting
+    net in FP64 torch on the host cores with autograd for dE/dD,
+    tabulate_fusion_se_a_grad_cpu, prod_force_a_cpu and prod_virial_a_cpu."""
 
     def __init__(self, params, coord, atype, box):
         import torch
@@ -139,9 +159,9 @@ class CpuReference:
                                None if d is None else torch.tensor(d)) for W, b, d in f["layers"]],
                              (torch.tensor(f["out"][0]), torch.tensor(f["out"][1]))))
 
-    def step(self, sample: int):
-        """One FP64 evaluation of the first `sample` atoms as centers (all
-        geometry of the full frame); returns the wall time in seconds."""
+    def step(self):
+        """One FP64 energy/force/virial evaluation of the whole frame (every
+        atom a center); returns (wall seconds, energy)."""
         import torch
 
         p, lib, cfg = self.p, self.lib, self.p.cfg
@@ -150,7 +170,7 @@ class CpuReference:
         cn = lib.normalize_coord(self.coord.reshape(-1), self.box).reshape(-1, 3)
         c, t, mapping = lib.copy_coord(cn, self.atype, cfg.rcut, self.box)
         nall = c.shape[0]
-        S = sample
+        S = self.atype.size
         ret, il, nn, rb, _ = lib.build_nlist(c, S, cfg.rcut, atype=t, mem_size=512)
         em, emd, rij, nlist = lib.prod_env_mat_a(c, t, il, nn, rb, p.davg, p.dstd, S,
                                                  cfg.rcut, cfg.rcut_smth, cfg.sec)
@@ -167,10 +187,9 @@ class CpuReference:
             blocks.append((a, b, e, ex, table, info))
         xt = torch.from_numpy(xyz / nnei).requires_grad_(True)
         D = (xt.transpose(1, 2) @ xt[:, :, :cfg.axis_neuron]).reshape(S, -1)
-        at = self.atype[:S]
         E = torch.zeros((), dtype=torch.float64)
         for ty in range(cfg.ntypes):
-            idx = torch.from_numpy(np.nonzero(at == ty)[0])
+            idx = torch.from_numpy(np.nonzero(self.atype == ty)[0])
             if idx.numel() == 0:
                 continue
             layers, (Wo, bo) = self.fit[ty]
@@ -178,7 +197,7 @@ class CpuReference:
             for W, b, d in layers:
                 y = torch.tanh(torch.addmm(b, h, W))
                 h = h + d * y if d is not None else y
-            E = E + torch.addmm(bo, h, Wo).sum()
+            E = E + torch.addmm(bo, h, Wo).sum() + float(p.bias_atom_e[ty]) * idx.numel()
         (dxyz,) = torch.autograd.grad(E, xt)
         dy = np.ascontiguousarray(dxyz.numpy() / nnei)
         nd = np.zeros((S, nnei, 4))
@@ -187,10 +206,12 @@ class CpuReference:
             nd[:, a:b, :] = de
             nd[:, a:b, 0] += dx
         nd = nd.reshape(S, nnei * 4)
-        force = lib.prod_force_a(nd, emd, nlist, S, nall)
+        fext = lib.prod_force_a(nd, emd, nlist, S, nall)[0]
+        force = np.zeros((S, 3))
+        np.add.at(force, mapping, fext)
         virial, _ = lib.prod_virial_a(nd, emd, rij, nlist, S, nall)
         del force, virial
-        return time.perf_counter() - t0
+        return time.perf_counter() - t0, float(E.detach())
 
 
 # ------------------------------------------------------------ ranks (N > 1) --
@@ -552,37 +573,43 @@ def run_train(args) -> None:
 
 # ---------------------------------------------------------------- arms -------
 def run_reference(args, rank: int, world: int) -> None:
+    """The reference's own CPU implementation of the path on this host's
+    cores, on the same 12,288-atom frame and model: every atom a center in
+    every step. Nothing of this project's GPU library is loaded: the inputs
+    come from the numpy generator, the statistics from the reference library
+    and the tables from the oracle's restatement of the reference compressor
+    (pinned to the compressor's own output by the tests)."""
     if rank != 0:
         return
-    mdl, wl, tab = _load()
-    cfg = mdl.SeAConfig()
-    coord, atype, box = wl.water_frame(N_SIDE, seed=100)
-    params = mdl.init_params(cfg, seed=PARAM_SEED)
-    # statistics and tables on the CPU with the reference library
-    from oracle import model_ref, oracle
+    wl = _workload_module()
+    cfg = wl.SeAConfig()
+    coord, atype, box = wl.water_frame(N_SIDE, seed=frame_seed(0))
+    params = wl.init_params(cfg, seed=PARAM_SEED)
+    from oracle import model_ref, oracle, table_ref
 
     lib = oracle.ref() or oracle.port()
     params.davg, params.dstd, mind = model_ref.env_stats(lib, cfg, coord, atype, box)
-    params.tables = tab.build_tables(params.emb, params.davg, params.dstd, cfg.sel, mind,
-                                     cfg.rcut_smth, cfg.rcut)
+    params.tables = table_ref.build_tables(params.emb, params.davg, params.dstd, cfg.sel, mind,
+                                           cfg.rcut_smth, cfg.rcut)
     ref = CpuReference(params, coord, atype, box)
-    S = CPU_SAMPLE_ATOMS
     for _ in range(args.warmup):
-        ref.step(S)
-    ts = [ref.step(S) for _ in range(args.steps)]
-    us = float(np.mean(ts)) * 1e6 / S
+        ref.step()
+    ts = [ref.step()[0] for _ in range(args.steps)]
+    ms = float(np.mean(ts)) * 1e3
+    us = ms * 1e3 / atype.size
     line = {
         "impl": "reference", "metric": METRIC, "value": us, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": us * atype.size / 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": f"water {atype.size} atoms ({atype.size // 3} H2O, "
                                f"{box[0]:.2f} A box), se_e2_a compressed E/F/V, reference CPU path",
                    "nloc": int(atype.size), "sel": list(cfg.sel)},
         "cpu_baseline": {"value": us, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
-                         "sample": f"{S} of {atype.size} center atoms per step, full-frame "
-                                   "geometry; deepmd:: CPU lib compiled from the reference "
-                                   "sources + FP64 torch fitting"},
+                         "sample": f"the whole frame ({atype.size} centers) every step, "
+                                   f"{args.steps} steps after {args.warmup} warm-up; deepmd:: "
+                                   "CPU library compiled from the reference sources + FP64 "
+                                   "torch fitting"},
         "e2e": {"value": us, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -791,12 +818,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref = CpuReference(params, coord, atype, box)
-        ref.step(CPU_SAMPLE_ATOMS)
-        ts = [ref.step(CPU_SAMPLE_ATOMS) for _ in range(3)]
-        us_cpu = float(np.mean(ts)) * 1e6 / CPU_SAMPLE_ATOMS
+        ref.step()
+        ts = [ref.step()[0] for _ in range(CPU_STEPS)]
+        us_cpu = float(np.mean(ts)) * 1e6 / nloc
         cpu = {"value": us_cpu, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
-               "sample": f"{CPU_SAMPLE_ATOMS} of {nloc} center atoms, 3 steps, full-frame "
-                         "geometry; FP64"}
+               "sample": f"the whole frame ({nloc} centers) every step, {CPU_STEPS} steps after "
+                         "1 warm-up; FP64"}
 
     if rank == 0:
         line = {

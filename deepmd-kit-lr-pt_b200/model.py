@@ -22,75 +22,13 @@ is captured once into a CUDA graph and replayed.
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, field
 
 import numpy as np
 import torch
 
 from . import _capi, ops, table as table_mod
 from ._capi import call, ptr
-
-
-@dataclass
-class SeAConfig:
-    rcut: float = 6.0
-    rcut_smth: float = 0.5
-    sel: tuple = (46, 92)
-    neuron: tuple = (25, 50, 100)
-    axis_neuron: int = 16
-    fitting: tuple = (240, 240, 240)
-
-    @property
-    def ntypes(self) -> int:
-        return len(self.sel)
-
-    @property
-    def nnei(self) -> int:
-        return int(sum(self.sel))
-
-    @property
-    def sec(self) -> np.ndarray:
-        return np.concatenate([[0], np.cumsum(self.sel)]).astype(np.int32)
-
-
-@dataclass
-class SeAParams:
-    cfg: SeAConfig
-    emb: list                 # per neighbor type: [(W, b), ...]
-    fit: list                 # per center type: [(W, b, idt|None), ...] + out (W, b)
-    bias_atom_e: np.ndarray
-    davg: np.ndarray = None   # [ntypes, nnei * 4]
-    dstd: np.ndarray = None
-    tables: list = field(default_factory=list)  # [(table f64, info f64)] per neighbor type
-
-
-def init_params(cfg: SeAConfig, seed: int = 0) -> SeAParams:
-    """Seeded random weights: W ~ N(0, 1/fan_in), b ~ N(0, 1); timestep
-    vectors ~ N(0.1, 0.001) as the reference initialises them
-    (deepmd/dpmodel/utils/network.py:135-146)."""
-    rng = np.random.default_rng(seed)
-
-    def layer(n_in, n_out, idt=False):
-        W = rng.normal(0.0, np.sqrt(1.0 / n_in), size=(n_in, n_out))
-        b = rng.normal(0.0, 1.0, size=n_out)
-        d = rng.normal(0.1, 0.001, size=n_out) if idt else None
-        return W, b, d
-
-    emb = []
-    for _ in range(cfg.ntypes):
-        widths = [1, *cfg.neuron]
-        emb.append([layer(widths[k], widths[k + 1])[:2] for k in range(len(cfg.neuron))])
-    fit = []
-    din = cfg.neuron[-1] * cfg.axis_neuron
-    for _ in range(cfg.ntypes):
-        widths = [din, *cfg.fitting]
-        layers = []
-        for k in range(len(cfg.fitting)):
-            W, b, d = layer(widths[k], widths[k + 1], idt=True)
-            layers.append((W, b, d if widths[k] == widths[k + 1] else None))
-        Wo, bo, _ = layer(cfg.fitting[-1], 1)
-        fit.append({"layers": layers, "out": (Wo, bo)})
-    return SeAParams(cfg=cfg, emb=emb, fit=fit, bias_atom_e=np.zeros(cfg.ntypes))
+from .workload import SeAConfig, SeAParams, init_params  # noqa: F401  (model definition)
 
 
 # ------------------------------------------------------------ statistics --

@@ -14,10 +14,18 @@ import subprocess
 import sys
 import tempfile
 
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
-if not REF or not os.path.isdir(REF):
-    raise SystemExit("give the reference source tree as the first argument or in "
-                     "DEEPMD_REFERENCE_TREE")
+
+
+def _ref_tree() -> str:
+    """The reference source tree: the first argument, else the environment
+    variable DEEPMD_REFERENCE_TREE (checked when a fixture is made)."""
+    tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
+    if not tree or not os.path.isdir(tree):
+        raise SystemExit("give the reference source tree as the first argument or in "
+                         "DEEPMD_REFERENCE_TREE")
+    return tree
+
+
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_abi_symbols.txt")
 
 FUNCS = ["build_nlist_gpu", "prod_env_mat_a_gpu", "tabulate_fusion_se_a_gpu",
@@ -51,7 +59,7 @@ def main():
         obj = os.path.join(d, "abi.o")
         open(src, "w").write(SRC)
         subprocess.run(["g++", "-std=c++17", "-DGOOGLE_CUDA=1", "-c", src, "-o", obj,
-                        "-I" + os.path.join(REF, "source", "lib", "include"),
+                        "-I" + os.path.join(_ref_tree(), "source", "lib", "include"),
                         "-I/usr/local/cuda/include"], check=True)
         out = subprocess.run(["nm", "-u", obj], capture_output=True, text=True, check=True).stdout
     syms = sorted({ln.split()[-1] for ln in out.splitlines() if "6deepmd" in ln})

@@ -28,10 +28,18 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
-if not REF or not os.path.isdir(REF):
-    raise SystemExit("give the reference source tree as the first argument or in "
-                     "DEEPMD_REFERENCE_TREE")
+
+
+def _ref_tree() -> str:
+    """The reference source tree: the first argument, else the environment
+    variable DEEPMD_REFERENCE_TREE (checked when a fixture is made)."""
+    tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
+    if not tree or not os.path.isdir(tree):
+        raise SystemExit("give the reference source tree as the first argument or in "
+                         "DEEPMD_REFERENCE_TREE")
+    return tree
+
+
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_fixtures.npz")
 
 CC_FILES = [
@@ -110,8 +118,8 @@ def parse_py(path: str, tag: str, out: dict) -> None:
 def main() -> None:
     out: dict[str, np.ndarray] = {}
     for rel in CC_FILES:
-        parse_cc(os.path.join(REF, rel), os.path.basename(rel), out)
-    parse_py(os.path.join(REF, PY_FILE), os.path.basename(PY_FILE), out)
+        parse_cc(os.path.join(_ref_tree(), rel), os.path.basename(rel), out)
+    parse_py(os.path.join(_ref_tree(), PY_FILE), os.path.basename(PY_FILE), out)
     np.savez_compressed(OUT, **out)
     for k in sorted(out):
         print(f"{k:70s} {out[k].shape}")

@@ -21,10 +21,18 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
-if not REF or not os.path.isdir(REF):
-    raise SystemExit("give the reference source tree as the first argument or in "
-                     "DEEPMD_REFERENCE_TREE")
+
+
+def _ref_tree() -> str:
+    """The reference source tree: the first argument, else the environment
+    variable DEEPMD_REFERENCE_TREE (checked when a fixture is made)."""
+    tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
+    if not tree or not os.path.isdir(tree):
+        raise SystemExit("give the reference source tree as the first argument or in "
+                         "DEEPMD_REFERENCE_TREE")
+    return tree
+
+
 OUT = os.path.join(HERE, "model_golden.npz")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
@@ -45,7 +53,7 @@ def weight_checksum(params) -> float:
 def reference_model(params):
     import ref_import_shim
 
-    ref_import_shim.install(REF)
+    ref_import_shim.install(_ref_tree())
     from deepmd.pt.model.model import get_model
 
     cfg = params.cfg

@@ -25,10 +25,18 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
-if not REF or not os.path.isdir(REF):
-    raise SystemExit("give the reference source tree as the first argument or in "
-                     "DEEPMD_REFERENCE_TREE")
+
+
+def _ref_tree() -> str:
+    """The reference source tree: the first argument, else the environment
+    variable DEEPMD_REFERENCE_TREE (checked when a fixture is made)."""
+    tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DEEPMD_REFERENCE_TREE", "")
+    if not tree or not os.path.isdir(tree):
+        raise SystemExit("give the reference source tree as the first argument or in "
+                         "DEEPMD_REFERENCE_TREE")
+    return tree
+
+
 OUT = os.path.join(HERE, "train_golden.npz")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)

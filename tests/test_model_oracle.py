@@ -136,3 +136,37 @@ def test_tables_match_reference_compressor(mdl, tab):
             x = h * frac
             pw = np.stack([x ** k for k in range(6)], -1)
             assert np.abs(((mine - ref) * pw).sum(-1)).max() <= 1e-12, (t, frac)
+
+
+def test_oracle_table_builder_matches_reference_compressor(mdl):
+    """The oracle's restatement of the reference compressor (used by the
+    benchmark's reference arm instead of the product's builder) against the
+    compressor's own output, with the bars of the product builder's test."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_model_golden import weight_checksum
+
+    from oracle import table_ref
+
+    with np.load(os.path.join(os.path.dirname(GOLD), "table_golden.npz")) as z:
+        g = {k: z[k] for k in z.files}
+    cfg = mdl.SeAConfig()
+    p = mdl.init_params(cfg, seed=1)
+    assert abs(weight_checksum(p) - float(g["weight_checksum"])) < 1e-9
+    tables = table_ref.build_tables(p.emb, g["davg"], g["dstd"], cfg.sel,
+                                    float(g["min_nbor_dist"]), cfg.rcut_smth, cfg.rcut)
+    M = cfg.neuron[-1]
+    tol = [1e-12, 1e-12, 1e-12, 1e-6, 1e-4, 2e-3]
+    for t, (table, info) in enumerate(tables):
+        np.testing.assert_array_equal(info, g[f"net{t}:info"])
+        assert tuple(table.shape) == tuple(g[f"net{t}:shape"])
+        rows = g[f"net{t}:rows"]
+        mine, ref = table[rows].reshape(-1, M, 6), g[f"net{t}:table_rows"].reshape(-1, M, 6)
+        for k in range(6):
+            assert np.abs(mine[:, :, k] - ref[:, :, k]).max() <= tol[k], (t, k)
+        first = int((info[1] - info[0]) / info[3])
+        h = np.where(rows < first, info[3], info[4])[:, None]
+        for frac in (0.0, 0.37, 0.999):
+            pw = np.stack([(h * frac) ** k for k in range(6)], -1)
+            assert np.abs(((mine - ref) * pw).sum(-1)).max() <= 1e-12, (t, frac)
