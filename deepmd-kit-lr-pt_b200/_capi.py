@@ -111,6 +111,11 @@ _FUNCS = {
     "dpb_force_virial_a_env_mixed_acc": "pppppppp" "iiii" "ff" "p",
     "dpb_gemm_tf32x3_f32": "pii" "pp" "i" "pi" "i" "pppp" "ppp" "pp" "p",
     "dpb_force_virial_a_env_f64": "pppppppp" "iiii" "ff" "p",
+    "dpb_copy_coord_cells_f64": "ppppp" "L" "pp" "ii" "pp" "p",
+    "dpb_copy_coord_cells_f32": "ppppp" "L" "pp" "ii" "pp" "p",
+    "dpb_use_nlist_map": "pp" "ii" "p",
+    "dpb_nlist_rows_to_device": "pppp" "i" "ppp" "i" "p" "L" "p",
+    "dpb_gemm_f64": "pppp" "iiiiii" "iii" "p",
 }
 _TRAIN = {
     "dpb_se_a_train_fwd": "pppppppppp" "iii" "pp",
@@ -140,6 +145,8 @@ _SIZE_QUERIES = {
     "dpb_build_nlist_scratch_bytes": ("ii", LL),
     "dpb_build_nlist_noalloc_max_bytes": ("", LL),
     "dpb_se_a_build_table_scratch_bytes": ("ii", LL),
+    "dpb_copy_coord_cells_scratch_bytes": ("ip", LL),
+    "dpb_nlist_rows_scratch_bytes": ("pi", LL),
 }
 
 _lib = None

@@ -116,9 +116,124 @@ int c_nlist(int* il, int* nn, int** fn, int* mx, void* s, long long sb, const do
   return dpb_build_nlist_f64(il, nn, fn, mx, s, sb, c, nloc, nall, mem, rc, nf, t, nullptr);
 }
 
+int c_normalize(float* c, int n, const float* b) {
+  return dpb_normalize_coord_f32(c, n, b, nullptr);
+}
+int c_normalize(double* c, int n, const double* b) {
+  return dpb_normalize_coord_f64(c, n, b, nullptr);
+}
+int c_copy_cells(float* oc, int* ot, int* m, int* nall, void* s, long long sb, const float* ic,
+                 const int* it, int nloc, int mem, const int* ci, const float* b) {
+  return dpb_copy_coord_cells_f32(oc, ot, m, nall, s, sb, ic, it, nloc, mem, ci, b, nullptr);
+}
+int c_copy_cells(double* oc, int* ot, int* m, int* nall, void* s, long long sb, const double* ic,
+                 const int* it, int nloc, int mem, const int* ci, const double* b) {
+  return dpb_copy_coord_cells_f64(oc, ot, m, nall, s, sb, ic, it, nloc, mem, ci, b, nullptr);
+}
+
+template <typename T>
+void d2h(T* dst, const T* src, size_t n, const char* what) {
+  cudaError_t e = cudaMemcpy(dst, src, sizeof(T) * n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess)
+    throw deepmd::deepmd_exception(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+void dev_alloc(T*& p, size_t n, const char* what) {
+  p = nullptr;
+  cudaError_t e = cudaMalloc((void**)&p, sizeof(T) * (n > 0 ? n : 1));
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    throw deepmd::deepmd_exception_oom(std::string(what) + ": cudaMalloc failed");
+  }
+  if (e != cudaSuccess)
+    throw deepmd::deepmd_exception(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
 }  // namespace
 
 namespace deepmd {
+
+template <typename FPTYPE>
+void normalize_coord_gpu(FPTYPE* coord, const int natom, const Region<FPTYPE>& region) {
+  sync("normalize_coord_gpu");
+  FPTYPE box[9];
+  d2h(box, region.boxt, 9, "normalize_coord_gpu");
+  raise(c_normalize(coord, natom, box), "normalize_coord_gpu");
+  sync("normalize_coord_gpu");
+}
+
+template <typename FPTYPE>
+int copy_coord_gpu(FPTYPE* out_c, int* out_t, int* mapping, int* nall, int* int_data,
+                   const FPTYPE* in_c, const int* in_t, const int& nloc, const int& mem_nall,
+                   const int& loc_cellnum, const int& total_cellnum, const int* cell_info,
+                   const Region<FPTYPE>& region) {
+  sync("copy_coord_gpu");
+  int ci[23];
+  FPTYPE box[9];
+  d2h(ci, cell_info, 23, "copy_coord_gpu");
+  d2h(box, region.boxt, 9, "copy_coord_gpu");
+  if (ci[21] != loc_cellnum || ci[22] != total_cellnum)
+    throw deepmd_exception("copy_coord_gpu: loc_cellnum / total_cellnum disagree with cell_info");
+  // the int_data the reference's callers allocate
+  // (op/tf/prod_env_mat_multi_device.cc:2428-2430, less the 23 cell_info ints)
+  const long long have =
+      (4LL * nloc + 2LL * loc_cellnum + 7LL * total_cellnum + 2) * (long long)sizeof(int);
+  int code = c_copy_cells(out_c, out_t, mapping, nall, int_data, have, in_c, in_t, nloc,
+                          mem_nall, ci, box);
+  if (code == DPB_ERR_CAPACITY) return 1;
+  raise(code, "copy_coord_gpu");
+  sync("copy_coord_gpu");
+  return 0;
+}
+
+void convert_nlist_gpu_device(InputNlist& gpu_nlist, InputNlist& cpu_nlist, int*& gpu_memory,
+                              const int& max_nbor_size) {
+  // every row is checked before gpu_nlist is touched (neighbor_list.cc:993-1016)
+  for (int ii = 0; ii < cpu_nlist.inum; ++ii) {
+    if (cpu_nlist.numneigh[ii] > max_nbor_size)
+      throw deepmd_exception_nlist_capacity(
+          "Neighbor list row " + std::to_string(ii) + " contains " +
+          std::to_string(cpu_nlist.numneigh[ii]) +
+          " neighbors, exceeding the allocated GPU row capacity " +
+          std::to_string(max_nbor_size));
+  }
+  const int inum = cpu_nlist.inum;
+  gpu_nlist.inum = inum;
+  dev_alloc(gpu_nlist.ilist, inum, "convert_nlist_gpu_device");
+  dev_alloc(gpu_nlist.numneigh, inum, "convert_nlist_gpu_device");
+  dev_alloc(gpu_nlist.firstneigh, inum, "convert_nlist_gpu_device");
+  const long long sb = dpb_nlist_rows_scratch_bytes(cpu_nlist.numneigh, inum);
+  unsigned char* scratch = nullptr;
+  dev_alloc(scratch, (size_t)sb, "convert_nlist_gpu_device");
+  int code = dpb_nlist_rows_to_device(gpu_nlist.ilist, gpu_nlist.numneigh, gpu_nlist.firstneigh,
+                                      gpu_memory, max_nbor_size, cpu_nlist.ilist,
+                                      cpu_nlist.numneigh, cpu_nlist.firstneigh, inum, scratch,
+                                      sb, nullptr);
+  cudaFree(scratch);
+  raise(code, "convert_nlist_gpu_device");
+  sync("convert_nlist_gpu_device");
+}
+
+void free_nlist_gpu_device(InputNlist& gpu_nlist) {
+  for (void* p : {(void*)gpu_nlist.ilist, (void*)gpu_nlist.numneigh,
+                  (void*)gpu_nlist.firstneigh}) {
+    if (p != nullptr) {
+      cudaError_t e = cudaFree(p);
+      if (e != cudaSuccess)
+        throw deepmd_exception(std::string("free_nlist_gpu_device: ") + cudaGetErrorString(e));
+    }
+  }
+  gpu_nlist.ilist = nullptr;
+  gpu_nlist.numneigh = nullptr;
+  gpu_nlist.firstneigh = nullptr;
+}
+
+void use_nlist_map(int* nlist, const int* nlist_map, const int nloc, const int nnei) {
+  sync("use_nlist_map");
+  raise(dpb_use_nlist_map(nlist, nlist_map, nloc, nnei, nullptr), "use_nlist_map");
+  sync("use_nlist_map");
+}
 
 template <typename FPTYPE>
 int build_nlist_gpu(InputNlist& nlist, int* max_list_size, int* nlist_data,
@@ -242,6 +357,10 @@ void prod_virial_grad_a_gpu(FPTYPE* grad_net, const FPTYPE* grad, const FPTYPE* 
 }
 
 #define DPB_INSTANTIATE(T)                                                                   \
+  template void normalize_coord_gpu<T>(T*, const int, const Region<T>&);                     \
+  template int copy_coord_gpu<T>(T*, int*, int*, int*, int*, const T*, const int*,           \
+                                 const int&, const int&, const int&, const int&, const int*, \
+                                 const Region<T>&);                                          \
   template int build_nlist_gpu<T>(InputNlist&, int*, int*, const T*, const int&, const int&, \
                                   const int&, const float&, const int&, const int*);         \
   template void prod_env_mat_a_gpu<T>(T*, T*, T*, int*, const T*, const int*,                \

@@ -342,18 +342,13 @@ __global__ void k_cc_copy(CopyScratch s, T* out_c, int* out_t, int* mapping,
   }
 }
 
+// The copy on a given cell decomposition (nc local cells and ng ghost layers
+// per dimension): the steps of copy_coord_cpu (coord.cc:29-64) as kernels.
 template <typename T>
-int copy_coord_async(T* out_c, int* out_t, int* mapping, int* nall_dev,
-                     void* scratch, long long scratch_bytes, const T* in_c,
-                     const int* in_t, int nloc, int mem_nall, float rcut,
-                     const double* boxt, cudaStream_t st) {
-  if (nloc < 0 || mem_nall < 0 || !(rcut > 0.f)) {
-    set_error("copy_coord: invalid sizes (nloc=%d mem_nall=%d rcut=%g)", nloc,
-              mem_nall, (double)rcut);
-    return DPB_ERR_INVALID;
-  }
-  HostRegion r;
-  host_region(r, boxt, rcut);
+static int copy_coord_region_async(T* out_c, int* out_t, int* mapping, int* nall_dev,
+                                   void* scratch, long long scratch_bytes, const T* in_c,
+                                   const int* in_t, int nloc, int mem_nall,
+                                   const HostRegion& r, cudaStream_t st) {
   if (!(r.volume > 0.)) {
     set_error("copy_coord: the box has zero volume");
     return DPB_ERR_INVALID;
@@ -392,18 +387,30 @@ int copy_coord_async(T* out_c, int* out_t, int* mapping, int* nall_dev,
 }
 
 template <typename T>
-int copy_coord_sync(T* out_c, int* out_t, int* mapping, int* nall,
-                    void* scratch, long long scratch_bytes, const T* in_c,
-                    const int* in_t, int nloc, int mem_nall, float rcut,
-                    const T* boxt, cudaStream_t st) {
-  double b[9];
-  for (int k = 0; k < 9; ++k) b[k] = (double)boxt[k];
-  int rc = copy_coord_async<T>(out_c, out_t, mapping, nullptr, scratch,
-                               scratch_bytes, in_c, in_t, nloc, mem_nall, rcut,
-                               b, st);
-  if (rc != DPB_OK) return rc;
+int copy_coord_async(T* out_c, int* out_t, int* mapping, int* nall_dev,
+                     void* scratch, long long scratch_bytes, const T* in_c,
+                     const int* in_t, int nloc, int mem_nall, float rcut,
+                     const double* boxt, cudaStream_t st) {
+  if (nloc < 0 || mem_nall < 0 || !(rcut > 0.f)) {
+    set_error("copy_coord: invalid sizes (nloc=%d mem_nall=%d rcut=%g)", nloc,
+              mem_nall, (double)rcut);
+    return DPB_ERR_INVALID;
+  }
   HostRegion r;
-  host_region(r, b, rcut);
+  host_region(r, boxt, rcut);
+  return copy_coord_region_async<T>(out_c, out_t, mapping, nall_dev, scratch, scratch_bytes,
+                                    in_c, in_t, nloc, mem_nall, r, st);
+}
+
+// the copy, then nall read back (DPB_ERR_CAPACITY when it exceeds mem_nall)
+template <typename T>
+static int copy_coord_region_sync(T* out_c, int* out_t, int* mapping, int* nall,
+                                  void* scratch, long long scratch_bytes, const T* in_c,
+                                  const int* in_t, int nloc, int mem_nall,
+                                  const HostRegion& r, cudaStream_t st) {
+  int rc = copy_coord_region_async<T>(out_c, out_t, mapping, nullptr, scratch, scratch_bytes,
+                                      in_c, in_t, nloc, mem_nall, r, st);
+  if (rc != DPB_OK) return rc;
   CopyScratch s = carve_copy(scratch, nloc, r);
   int h = 0;
   DPB_CUDA(cudaMemcpyAsync(&h, s.nall, sizeof(int), cudaMemcpyDeviceToHost, st),
@@ -415,6 +422,77 @@ int copy_coord_sync(T* out_c, int* out_t, int* mapping, int* nall,
     return DPB_ERR_CAPACITY;
   }
   return DPB_OK;
+}
+
+template <typename T>
+int copy_coord_sync(T* out_c, int* out_t, int* mapping, int* nall,
+                    void* scratch, long long scratch_bytes, const T* in_c,
+                    const int* in_t, int nloc, int mem_nall, float rcut,
+                    const T* boxt, cudaStream_t st) {
+  if (nloc < 0 || mem_nall < 0 || !(rcut > 0.f)) {
+    set_error("copy_coord: invalid sizes (nloc=%d mem_nall=%d rcut=%g)", nloc,
+              mem_nall, (double)rcut);
+    return DPB_ERR_INVALID;
+  }
+  double b[9];
+  for (int k = 0; k < 9; ++k) b[k] = (double)boxt[k];
+  HostRegion r;
+  host_region(r, b, rcut);
+  return copy_coord_region_sync<T>(out_c, out_t, mapping, nall, scratch, scratch_bytes, in_c,
+                                   in_t, nloc, mem_nall, r, st);
+}
+
+// A region whose cell decomposition is given in the layout of
+// compute_cell_info (coord.cc:69-108: ncell at [3..5], ngcell at [12..14],
+// loc_cellnum at [21], total_cellnum at [22]) instead of derived from rcut.
+static int host_region_cells(HostRegion& r, const double* boxt, const int* cell_info) {
+  host_region(r, boxt, 1.f);
+  long long nl = 1, ne = 1;
+  for (int d = 0; d < 3; ++d) {
+    const int n = cell_info[3 + d], g = cell_info[12 + d];
+    if (n < 1 || g < 1 || n > (1 << 20) || g > (1 << 20)) {
+      set_error("copy_coord: invalid cell_info (ncell %d, ngcell %d in dimension %d)", n, g, d);
+      return DPB_ERR_INVALID;
+    }
+    r.nc[d] = n;
+    r.ng[d] = g;
+    r.inv_nc[d] = 1. / n;
+    nl *= n;
+    ne *= n + 2LL * g;
+  }
+  if (nl != cell_info[21] || ne != cell_info[22] || ne > (1LL << 30)) {
+    set_error("copy_coord: cell_info counts (%d local, %d total cells) disagree with its "
+              "ncell / ngcell", cell_info[21], cell_info[22]);
+    return DPB_ERR_INVALID;
+  }
+  r.nloc_cells = (int)nl;
+  r.next_cells = (int)ne;
+  return DPB_OK;
+}
+
+template <typename T>
+static int copy_coord_cells(T* out_c, int* out_t, int* mapping, int* nall, void* scratch,
+                            long long scratch_bytes, const T* in_c, const int* in_t, int nloc,
+                            int mem_nall, const int* cell_info, const T* boxt,
+                            cudaStream_t st) {
+  if (nloc < 0 || mem_nall < 0 || cell_info == nullptr || boxt == nullptr || nall == nullptr) {
+    set_error("copy_coord: invalid arguments (nloc=%d mem_nall=%d)", nloc, mem_nall);
+    return DPB_ERR_INVALID;
+  }
+  double b[9];
+  for (int k = 0; k < 9; ++k) b[k] = (double)boxt[k];
+  HostRegion r;
+  int rc = host_region_cells(r, b, cell_info);
+  if (rc != DPB_OK) return rc;
+  return copy_coord_region_sync<T>(out_c, out_t, mapping, nall, scratch, scratch_bytes, in_c,
+                                   in_t, nloc, mem_nall, r, st);
+}
+
+long long copy_coord_cells_scratch_bytes(int nloc, const int* cell_info) {
+  double b[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  HostRegion r;
+  if (cell_info == nullptr || nloc < 0 || host_region_cells(r, b, cell_info) != DPB_OK) return -1;
+  return copy_scratch_ints(nloc, r) * (long long)sizeof(int);
 }
 
 // ------------------------------------------------------------ cell grid ----
@@ -1180,6 +1258,26 @@ int dpb_copy_coord_f32(float* out_c, int* out_t, int* mapping, int* nall,
   return copy_coord_sync<float>(out_c, out_t, mapping, nall, scratch,
                                 scratch_bytes, in_c, in_t, nloc, mem_nall,
                                 rcut, boxt, as_stream(stream));
+}
+
+long long dpb_copy_coord_cells_scratch_bytes(int nloc, const int* cell_info) {
+  return copy_coord_cells_scratch_bytes(nloc, cell_info);
+}
+
+int dpb_copy_coord_cells_f64(double* out_c, int* out_t, int* mapping, int* nall, void* scratch,
+                             long long scratch_bytes, const double* in_c, const int* in_t,
+                             int nloc, int mem_nall, const int* cell_info, const double* boxt,
+                             dpb_stream_t stream) {
+  return copy_coord_cells<double>(out_c, out_t, mapping, nall, scratch, scratch_bytes, in_c,
+                                  in_t, nloc, mem_nall, cell_info, boxt, as_stream(stream));
+}
+
+int dpb_copy_coord_cells_f32(float* out_c, int* out_t, int* mapping, int* nall, void* scratch,
+                             long long scratch_bytes, const float* in_c, const int* in_t,
+                             int nloc, int mem_nall, const int* cell_info, const float* boxt,
+                             dpb_stream_t stream) {
+  return copy_coord_cells<float>(out_c, out_t, mapping, nall, scratch, scratch_bytes, in_c,
+                                 in_t, nloc, mem_nall, cell_info, boxt, as_stream(stream));
 }
 
 long long dpb_cell_grid_bytes(int nall) { return grid_bytes(nall); }

@@ -201,6 +201,75 @@ class _Fitting:
         return torch.addmm(bo, h, Wo).view(-1) + self.bias[t]
 
 
+class _FittingF64:
+    """Per-type fitting networks of the FP64 plain path: the layers' GEMMs on
+    the project's FP64 GEMM (dpb_gemm_f64), the activations, residuals, the
+    atomic energies and the input gradient dE/dD on the fitting-layer kernels
+    (dpb_fit_*_f64). Rows of D are grouped by center type; ``type_rows`` gives
+    the group sizes (deepmd/pt/model/task/ener.py, layers as
+    deepmd/dpmodel/utils/network.py:282-330)."""
+
+    def __init__(self, params: SeAParams, type_rows, device):
+        dev = torch.device(device)
+        f64 = lambda a: torch.tensor(np.asarray(a, np.float64), device=dev).contiguous()  # noqa: E731
+        self.groups = []
+        o = 0
+        widths_in = params.cfg.neuron[-1] * params.cfg.axis_neuron
+        for t, f in enumerate(params.fit):
+            n = int(type_rows[t])
+            layers, w_in = [], widths_in
+            for W, b, d in f["layers"]:
+                w_out = int(np.asarray(W).shape[1])
+                layers.append(dict(W=f64(W), b=f64(b), d=None if d is None else f64(d),
+                                   w_in=w_in, w_out=w_out,
+                                   Y=torch.empty((n, w_out), dtype=torch.float64, device=dev),
+                                   H=torch.empty((n, w_out), dtype=torch.float64, device=dev),
+                                   G=torch.empty((n, w_out), dtype=torch.float64, device=dev)))
+                w_in = w_out
+            Wo, bo = f["out"]
+            out = dict(W=f64(np.asarray(Wo).reshape(-1)), b=f64(np.asarray(bo).reshape(1)),
+                       ebias=float(params.bias_atom_e[t]), w=w_in)
+            zb = torch.empty((n, max([ly["w_out"] for ly in layers] + [1])),
+                             dtype=torch.float64, device=dev)
+            self.groups.append((o, n, layers, out, zb))
+            o += n
+        self.n = o
+
+    @staticmethod
+    def _gemm(C, A, B, bias, M, N, K, lda, ldb, ldc, trans_b, acc, s):
+        call("dpb_gemm_f64", ptr(C), ptr(A), ptr(B), ptr(bias), M, N, K, lda, ldb, ldc, 0,
+             trans_b, acc, s)
+
+    def forward_backward(self, D: torch.Tensor, dD: torch.Tensor, e_rows: torch.Tensor, s):
+        """e_rows[r] = atomic energy of fitting row r (with the output and
+        atomic energy biases); dD = dE/dD."""
+        for o, n, layers, out, zb in self.groups:
+            if n == 0:
+                continue
+            H, w_in = D[o:o + n], D.shape[1]
+            for ly in layers:
+                self._gemm(ly["Y"], H, ly["W"], ly["b"], n, ly["w_out"], w_in, w_in, ly["w_out"],
+                           ly["w_out"], 0, 0, s)
+                call("dpb_fit_act_f64", ptr(ly["Y"]), ptr(ly["H"]), ptr(H), ptr(ly["d"]), n,
+                     ly["w_out"], w_in, s)
+                H, w_in = ly["H"], ly["w_out"]
+            call("dpb_fit_out_f64", ptr(e_rows[o:o + n]), ptr(H), ptr(out["W"]), ptr(out["b"]),
+                 ctypes.c_double(out["ebias"]), n, out["w"], s)
+            # dE/dH of the last hidden layer = Wo on every row, then back
+            call("dpb_fit_out_adj_f64", ptr(layers[-1]["G"]), None, None, None, ptr(H), None,
+                 ptr(out["W"]), None, n, out["w"], s)
+            for k in range(len(layers) - 1, -1, -1):
+                ly = layers[k]
+                call("dpb_fit_bwd_f64", ptr(zb), ptr(ly["G"]), ptr(ly["Y"]), ptr(ly["d"]), n,
+                     ly["w_out"], s)
+                dst = dD[o:o + n] if k == 0 else layers[k - 1]["G"]
+                # dst = Zb W^T, plus the residual's share of G
+                self._gemm(dst, zb, ly["W"], None, n, ly["w_in"], ly["w_out"], ly["w_out"],
+                           ly["w_out"], ly["w_in"], 1, 0, s)
+                call("dpb_fit_res_adj_f64", ptr(dst), ptr(ly["G"]), n, ly["w_out"], ly["w_in"],
+                     s)
+
+
 def tf32_split(w: np.ndarray):
     """(hi, lo) FP32 arrays with hi the round-to-nearest (ties away) TF32 value
     of w, as cvt.rna.tf32.f32 computes it, and lo = w - hi."""
@@ -348,8 +417,9 @@ class SeAEvaluator:
     """Energy/force/virial of one frame of fixed size, types and box.
 
     mode "compressed": FP32 table path (needs params.tables);
-    mode "plain": FP64 embedding-MLP path (centers in chunks of
-    ``plain_chunk`` atoms, so large frames fit).
+    mode "plain": FP64 embedding-MLP path (the embedding net, descriptor and
+    its backward on the se_a training kernels in FP64, the fitting on the
+    FP64 GEMM; 3-layer embedding nets of widths <= 32 / 64 / 128).
     Device buffers are allocated once; ``step()`` runs one evaluation on the
     current coordinates in ``self.coord``; ``capture()`` records the step into
     a CUDA graph that ``replay()`` re-runs.
@@ -363,13 +433,13 @@ class SeAEvaluator:
 
     def __init__(self, params: SeAParams, atype: np.ndarray, box: np.ndarray,
                  mode: str = "compressed", device="cuda:0", nall_capacity: int | None = None,
-                 tensor_core_fitting: bool = True, skin: float = 0.0,
-                 plain_chunk: int = 16384):
+                 tensor_core_fitting: bool = True, skin: float = 0.0):
         cfg = params.cfg
+        if mode not in ("compressed", "plain"):
+            raise _capi.DPBInvalidArgument(f"mode must be 'compressed' or 'plain', not {mode!r}")
         self.cfg, self.params, self.mode = cfg, params, mode
         self.skin = float(skin)
         self.rc_list = float(cfg.rcut) + self.skin
-        self.plain_chunk = int(plain_chunk)
         self.dev = torch.device(device)
         self.nloc = int(atype.size)
         self.box = np.ascontiguousarray(np.asarray(box, np.float64).reshape(9))
@@ -421,8 +491,8 @@ class SeAEvaluator:
                             zip(np.concatenate([[0], np.cumsum(counts)[:-1]]), counts)]
         # the FP32 fitting must not silently drop to TF32 tensor-core math
         torch.backends.cuda.matmul.allow_tf32 = False
-        self.fitting = _Fitting(params, fdt, dev)
         if mode == "compressed":
+            self.fitting = _Fitting(params, fdt, dev)
             self.xyz = torch.empty((nloc, 4, M), dtype=torch.float32, device=dev)
             self.D = torch.empty((nloc, M * ax), dtype=torch.float32, device=dev)
             self.dD = torch.empty_like(self.D)
@@ -443,11 +513,7 @@ class SeAEvaluator:
                 if dt.numel() < need:
                     raise _capi.DPBInvalidArgument("table smaller than its table_info addresses")
         else:
-            self.emb = [[(torch.tensor(W, dtype=torch.float64, device=dev),
-                          torch.tensor(b, dtype=torch.float64, device=dev)) for W, b in net]
-                        for net in params.emb]
-        if mode != "compressed":
-            self._plain_index(atype)
+            self._plain_setup(params, counts)
         if self.skin > 0:
             self.shift = torch.zeros_like(self.cext)
             self.ilist = torch.arange(nloc, dtype=torch.int32, device=dev)
@@ -470,19 +536,33 @@ class SeAEvaluator:
         ng = np.floor(rc / (L / nc)) + 1
         return int(np.prod(nc + 2 * ng) / np.prod(nc) * self.nloc)
 
-    def _plain_index(self, atype: np.ndarray):
-        """Per chunk of centers and per type: the rows of that type (device
-        index tensors built once, so the plain step stays capturable)."""
-        n, ch = self.nloc, self.plain_chunk
-        self.plain_chunks = []
-        for a in range(0, n, ch):
-            b = min(n, a + ch)
-            per_type = []
-            for t in range(self.cfg.ntypes):
-                idx = np.nonzero(atype[a:b] == t)[0]
-                per_type.append(None if idx.size == 0 else
-                                torch.tensor(idx, dtype=torch.int64, device=self.dev))
-            self.plain_chunks.append((a, b, per_type))
+    def _plain_setup(self, params: SeAParams, counts):
+        """Device buffers and weights of the FP64 plain path."""
+        from .train import fold_flags
+
+        cfg, dev, n = self.cfg, self.dev, self.nloc
+        if len(cfg.neuron) != 3 or not (3 <= cfg.neuron[0] <= 32 and cfg.neuron[1] <= 64 and
+                                        cfg.neuron[2] <= 128) or cfg.axis_neuron > 32:
+            raise _capi.DPBInvalidArgument(
+                "the FP64 plain path takes 3-layer embedding nets of widths <= 32 / 64 / 128 "
+                "and axis_neuron <= 32")
+        M, ax = cfg.neuron[-1], cfg.axis_neuron
+        f64 = lambda a: torch.tensor(np.asarray(a, np.float64), device=dev).contiguous()  # noqa: E731
+        self.emb_W = [f64(W) for net in params.emb for W, _ in net]
+        self.emb_b = [f64(b) for net in params.emb for _, b in net]
+        vp = lambda xs: (ctypes.c_void_p * len(xs))(*[x.data_ptr() for x in xs])  # noqa: E731
+        self.Wp, self.bp = vp(self.emb_W), vp(self.emb_b)
+        self.widths = np.array([1, *cfg.neuron], np.int32)
+        self.fold = fold_flags(params)
+        z = lambda *shape: torch.zeros(shape, dtype=torch.float64, device=dev)  # noqa: E731
+        self.xyz = z(n, 4, M)
+        self.D = z(n, M * ax)
+        self.dD = z(n, M * ax)
+        self.xbar = z(n, 4, M)
+        self.e_rows = z(n)
+        self.fit64 = _FittingF64(params, counts, dev)
+        self.one_frame = torch.tensor([0, n], dtype=torch.int32, device=dev)
+        self.zero_const = z(1)
 
     # ---- neighbor list with a skin, rebuilt on request (host syncs allowed)
     def rebuild(self):
@@ -577,8 +657,7 @@ class SeAEvaluator:
         if self.mode == "compressed":
             self._descriptor_compressed(s, tm)
         else:
-            with tm("descriptor_fitting_fp64"):
-                self._descriptor_plain()
+            self._descriptor_plain(s, tm)
         # the compressed path zeroed force / virial at the start of the step
         fv = "dpb_force_virial_a_env_mixed_acc" if self.mode == "compressed" else \
             "dpb_force_virial_a_env_f64"
@@ -612,40 +691,26 @@ class SeAEvaluator:
                  self.tab_info.ctypes.data, self.sec.ctypes.data, self.sec.size, self.nloc, M,
                  ax, s)
 
-    def _descriptor_plain(self):
-        cfg = self.cfg
-        nnei = cfg.nnei
-        etot = torch.zeros((), dtype=torch.float64, device=self.dev)
-        for a, b, per_type in self.plain_chunks:
-            with torch.enable_grad():
-                n = b - a
-                em = self.em[a:b].view(n, nnei, 4).detach().requires_grad_(True)
-                xyz = None
-                for t in range(cfg.ntypes):
-                    s0, s1 = int(self.sec[t]), int(self.sec[t + 1])
-                    if s1 == s0:
-                        continue
-                    rr = em[:, s0:s1, :]
-                    h = rr[:, :, :1]
-                    for W, bb in self.emb[t]:
-                        y = torch.tanh(h @ W + bb)
-                        if W.shape[1] == W.shape[0]:
-                            y = y + h
-                        elif W.shape[1] == 2 * W.shape[0]:
-                            y = y + torch.cat([h, h], -1)
-                        h = y
-                    gr = rr.transpose(1, 2) @ h
-                    xyz = gr if xyz is None else xyz + gr
-                xyz = xyz / nnei
-                D = (xyz.transpose(1, 2) @ xyz[:, :, :cfg.axis_neuron]).reshape(n, -1)
-                e = torch.zeros((), dtype=torch.float64, device=self.dev)
-                for t, idx in enumerate(per_type):
-                    if idx is not None:
-                        e = e + self.fitting.forward(t, D.index_select(0, idx)).sum()
-                (g,) = torch.autograd.grad(e, em)
-            etot = etot + e.detach()
-            self.net_deriv[a:b].copy_(g.reshape(n, nnei * 4))
-        self.energy.copy_(etot.view(1))
+    def _descriptor_plain(self, s, tm):
+        """Embedding net, descriptor, fitting and their backward in FP64:
+        net_deriv = dE/d(em) and the energy, all in kernels of this package
+        (deepmd/pt/model/descriptor/se_a.py:826-851 and the fitting net)."""
+        cfg, n = self.cfg, self.nloc
+        sec = self.sec
+        with tm("embedding_fwd_fp64"):
+            call("dpb_se_a_train_fwd_f64", ptr(self.xyz), ptr(self.D), ptr(self.em),
+                 ptr(self.nlist), ptr(self.atype), ptr(self.drow), self.Wp, self.bp,
+                 self.widths.ctypes.data, sec.ctypes.data, sec.size, n, cfg.axis_neuron,
+                 self.fold.ctypes.data, s)
+        with tm("fitting_fp64"):
+            self.fit64.forward_backward(self.D, self.dD, self.e_rows, s)
+            call("dpb_batch_energy_f64", ptr(self.energy), ptr(self.e_rows), ptr(self.drow),
+                 ptr(self.zero_const), ptr(self.one_frame), 1, s)
+        with tm("embedding_bwd_fp64"):
+            call("dpb_se_a_train_bwd_f64", ptr(self.net_deriv), ptr(self.xbar), ptr(self.em),
+                 ptr(self.xyz), ptr(self.dD), ptr(self.nlist), ptr(self.atype),
+                 ptr(self.drow), self.Wp, self.bp, self.widths.ctypes.data, sec.ctypes.data,
+                 sec.size, n, cfg.axis_neuron, s)
 
     # ---- graph capture / replay
     def capture(self, warmup: int = 2):

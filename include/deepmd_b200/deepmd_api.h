@@ -68,6 +68,48 @@ struct InputNlist {
         recvproc(nullptr), world(nullptr) {}
 };
 
+// source/lib/include/region.h:6-16 (member layout). Its constructors and
+// destructor are the reference's own (source/lib/src/region.cc); the
+// functions below only read boxt and rec_boxt, which point to device memory
+// as the reference's GPU callers set them up
+// (op/tf/prod_env_mat_multi_device.cc:2417-2442).
+template <typename FPTYPE>
+struct Region {
+  FPTYPE* boxt;
+  FPTYPE* rec_boxt;
+  Region();
+  Region(FPTYPE* extern_boxt, FPTYPE* extern_rec_boxt);
+  ~Region();
+
+ private:
+  bool self_allocated;
+};
+
+// source/lib/include/coord.h:56-59: wrap natom device coordinates into the
+// box (the box is read from region.boxt on the device).
+template <typename FPTYPE>
+DPB_CXX_API void normalize_coord_gpu(FPTYPE* coord, const int natom,
+                                     const Region<FPTYPE>& region);
+
+// source/lib/include/coord.h:72-85: ghost copy on the caller's cell
+// decomposition (cell_info, 23 device ints from compute_cell_info); int_data
+// is the caller's scratch of 4 nloc + 2 loc_cellnum + 7 total_cellnum + 2
+// ints (what the reference's callers allocate). Returns 1 when nall exceeds
+// mem_nall. Ghost order: that of copy_coord_cpu.
+template <typename FPTYPE>
+DPB_CXX_API int copy_coord_gpu(FPTYPE* out_c, int* out_t, int* mapping, int* nall,
+                               int* int_data, const FPTYPE* in_c, const int* in_t,
+                               const int& nloc, const int& mem_nall, const int& loc_cellnum,
+                               const int& total_cellnum, const int* cell_info,
+                               const Region<FPTYPE>& region);
+
+// source/lib/include/neighbor_list.h:201-228
+DPB_CXX_API void convert_nlist_gpu_device(InputNlist& gpu_nlist, InputNlist& cpu_nlist,
+                                          int*& gpu_memory, const int& max_nbor_size);
+DPB_CXX_API void free_nlist_gpu_device(InputNlist& gpu_nlist);
+DPB_CXX_API void use_nlist_map(int* nlist, const int* nlist_map, const int nloc,
+                               const int nnei);
+
 // source/lib/include/neighbor_list.h:260-270
 template <typename FPTYPE>
 DPB_CXX_API int build_nlist_gpu(InputNlist& nlist, int* max_list_size,

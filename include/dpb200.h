@@ -670,6 +670,52 @@ DPB_API int dpb_tune_get(const char* name);
 DPB_API int dpb_tune_options(const char* name, int* out, int capacity);
 DPB_API int dpb_tune_set(const char* name, int value);
 
+/* FP64 GEMM of the fitting network (FP64 plain path, FP64 training):
+ * C[M, N] = op(A) op(B) (+ bias[N]) (+ C when accumulate), row-major, op(X)
+ * = X^T when trans_* is set; lda / ldb / ldc are the row strides of the
+ * stored A, B, C. The layer algebra of deepmd/dpmodel/utils/network.py:
+ * 282-330 (y = x W + b, g_in = g W^T, gW += x^T g). */
+DPB_API int dpb_gemm_f64(double* C, const double* A, const double* B, const double* bias,
+                         int M, int N, int K, int lda, int ldb, int ldc, int trans_a,
+                         int trans_b, int accumulate, dpb_stream_t stream);
+
+/* ----------------------------------------- engine-facing list helpers ---- */
+/* copy_coord_gpu (source/lib/include/coord.h:72-85) takes the cell
+ * decomposition its caller computed with compute_cell_info
+ * (source/lib/src/coord.cc:69-108) instead of rcut: `cell_info` is that
+ * 23-int host array (ncell at [3..5], ngcell at [12..14], loc_cellnum at
+ * [21], total_cellnum at [22]); `boxt` the host box. Ghosts come out in the
+ * order of copy_coord_cpu. Returns DPB_ERR_CAPACITY with *nall set when nall
+ * exceeds mem_nall. Synchronises `stream` (nall is read back). */
+DPB_API long long dpb_copy_coord_cells_scratch_bytes(int nloc, const int* cell_info);
+DPB_API int dpb_copy_coord_cells_f64(double* out_c, int* out_t, int* mapping, int* nall,
+                                     void* scratch, long long scratch_bytes,
+                                     const double* in_c, const int* in_t, int nloc,
+                                     int mem_nall, const int* cell_info, const double* boxt,
+                                     dpb_stream_t stream);
+DPB_API int dpb_copy_coord_cells_f32(float* out_c, int* out_t, int* mapping, int* nall,
+                                     void* scratch, long long scratch_bytes,
+                                     const float* in_c, const int* in_t, int nloc,
+                                     int mem_nall, const int* cell_info, const float* boxt,
+                                     dpb_stream_t stream);
+/* use_nlist_map (source/lib/include/neighbor_list.h:225-228): every entry of
+ * nlist [nloc, nnei] that is not -1 replaced by nlist_map[entry]. */
+DPB_API int dpb_use_nlist_map(int* nlist, const int* nlist_map, int nloc, int nnei,
+                              dpb_stream_t stream);
+/* convert_nlist_gpu_device (source/lib/include/neighbor_list.h:201-218): a
+ * host neighbor list (ilist, numneigh, firstneigh rows) into caller device
+ * arrays: d_ilist / d_numneigh [inum], d_firstneigh [inum] pointers into
+ * d_rows [inum, width] (only the first numneigh[ii] entries of each row are
+ * written). One packed host-to-device copy plus one scatter kernel, using
+ * d_scratch (dpb_nlist_rows_scratch_bytes); a row longer than width gives
+ * DPB_ERR_NLIST_CAPACITY before any device work. Synchronises `stream`. */
+DPB_API long long dpb_nlist_rows_scratch_bytes(const int* numneigh, int inum);
+DPB_API int dpb_nlist_rows_to_device(int* d_ilist, int* d_numneigh, int** d_firstneigh,
+                                     int* d_rows, int width, const int* ilist,
+                                     const int* numneigh, const int* const* firstneigh,
+                                     int inum, void* d_scratch, long long scratch_bytes,
+                                     dpb_stream_t stream);
+
 /* ------------------------------------------- allocation-free variant ---- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc,
  * e.g. an MD engine's force callback that runs inside the engine's own

@@ -31,9 +31,11 @@ OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_abi_symbols.
 FUNCS = ["build_nlist_gpu", "prod_env_mat_a_gpu", "tabulate_fusion_se_a_gpu",
          "tabulate_fusion_se_a_grad_gpu", "tabulate_fusion_se_a_grad_grad_gpu",
          "prod_force_a_gpu", "prod_virial_a_gpu", "prod_force_grad_a_gpu",
-         "prod_virial_grad_a_gpu"]
+         "prod_virial_grad_a_gpu", "normalize_coord_gpu", "copy_coord_gpu"]
+PLAIN = ["convert_nlist_gpu_device", "free_nlist_gpu_device", "use_nlist_map"]
 
-SRC = """#include "neighbor_list.h"
+SRC = """#include "coord.h"
+#include "neighbor_list.h"
 #include "prod_env_mat.h"
 #include "tabulate.h"
 #include "prod_force.h"
@@ -50,7 +52,8 @@ SRC = """#include "neighbor_list.h"
     f"const deepmd::InputNlist&, int*, unsigned long long*, const int, const {t}*, "
     f"const {t}*, const int, const int, const int, const float, const float, "
     f"const std::vector<int>, const int*) = &deepmd::prod_env_mat_a_gpu<{t}>;\n"
-    for t in ("float", "double"))
+    for t in ("float", "double")) + "".join(
+    f"void* p_{f} = (void*)&deepmd::{f};\n" for f in PLAIN)
 
 
 def main():

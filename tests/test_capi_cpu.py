@@ -83,7 +83,7 @@ def test_cxx_dropin_exports_reference_symbols(dpb):
                          text=True, check=True).stdout
     have = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
     missing = [s for s in want if s not in have]
-    assert len(want) == 18 and not missing, missing
+    assert len(want) == 25 and not missing, missing
 
 
 def test_tile_knob_registry(dpb):

@@ -188,3 +188,55 @@ def test_gemm_240_tile(dpb, mdl, M, K, N, rows):
         assert _rel(e, (h * wv).sum(1)) < 2e-5 and _rel(o0, wv * d * (1 - y * y)) < 2e-5
     finally:
         autotune.set_knob("fit_n_tile", old)
+
+
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (77, 240, 1600), (300, 1600, 240), (129, 65, 33),
+                                   (64, 64, 16), (5000, 240, 240)])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_gemm_f64_matches_fp64_reference(dpb, M, N, K, ta, tb):
+    """dpb_gemm_f64 (FP64 plain path, FP64 training) against an FP64 matmul:
+    every transpose combination, ragged edges, the bias and accumulate
+    epilogues; the FP64 bar 1e-12 relative to the output scale."""
+    rng = np.random.default_rng(M * 7 + N * 3 + K + 11 * ta + 5 * tb)
+    A = rng.normal(size=(K, M) if ta else (M, K))
+    B = rng.normal(size=(N, K) if tb else (K, N))
+    bias = rng.normal(size=N)
+    C0 = rng.normal(size=(M, N))
+    At, Bt = torch.tensor(A, device=DEV), torch.tensor(B, device=DEV)
+    C = torch.tensor(C0, device=DEV)
+    cap = dpb._capi
+    s = torch.cuda.current_stream().cuda_stream
+    cap.call("dpb_gemm_f64", cap.ptr(C), cap.ptr(At), cap.ptr(Bt), cap.ptr(torch.tensor(bias, device=DEV)),
+             M, N, K, A.shape[1], B.shape[1], N, ta, tb, 1, s)
+    ref = (A.T if ta else A) @ (B.T if tb else B) + bias + C0
+    got = C.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()) * max(1, K) ** 0.5
+    # no bias, no accumulate: C is overwritten
+    C.fill_(7.0)
+    cap.call("dpb_gemm_f64", cap.ptr(C), cap.ptr(At), cap.ptr(Bt), None, M, N, K, A.shape[1],
+             B.shape[1], N, ta, tb, 0, s)
+    ref = (A.T if ta else A) @ (B.T if tb else B)
+    assert np.abs(C.cpu().numpy() - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()) * max(1, K) ** 0.5
+
+
+def test_fitting_f64_matches_torch_autograd(dpb, mdl):
+    """The FP64 plain path's fitting networks (FP64 GEMM + fitting-layer
+    kernels): atomic energies and dE/dD against FP64 torch autograd."""
+    cfg = mdl.SeAConfig()
+    p = mdl.init_params(cfg, seed=4)
+    rows = [70, 190]
+    n = sum(rows)
+    rng = np.random.default_rng(1)
+    D = rng.normal(size=(n, 1600)) * 0.05
+    fit = mdl._FittingF64(p, rows, DEV)
+    Dt = torch.tensor(D, device=DEV)
+    dD = torch.zeros_like(Dt)
+    e = torch.zeros(n, dtype=torch.float64, device=DEV)
+    fit.forward_backward(Dt, dD, e, torch.cuda.current_stream().cuda_stream)
+    ref = mdl._Fitting(p, torch.float64, DEV)
+    e0, g0 = ref.forward_backward(0, Dt[:rows[0]])
+    e1, g1 = ref.forward_backward(1, Dt[rows[0]:])
+    np.testing.assert_allclose(e.cpu().numpy(), torch.cat([e0, e1]).cpu().numpy(), atol=1e-11,
+                               rtol=0)
+    np.testing.assert_allclose(dD.cpu().numpy(), torch.cat([g0, g1]).cpu().numpy(), atol=1e-12,
+                               rtol=0)
