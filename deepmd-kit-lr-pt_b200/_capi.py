@@ -104,6 +104,8 @@ _FUNCS = {
     "dpb_batch_energy_f64": "pppppip",
     "dpb_se_a_descriptor_fwd_f32": "pppp" "pp" "pi" "iiip",
     "dpb_se_a_descriptor_bwd_f32": "ppppp" "pp" "pi" "iiip",
+    "dpb_se_a_descriptor_fwd_cubic_f32": "pppp" "pp" "pi" "iiip",
+    "dpb_se_a_descriptor_bwd_cubic_f32": "ppppp" "pp" "pi" "iiip",
     "dpb_force_virial_a_f32": "pppppp" "pp" "iiiip",
     "dpb_force_virial_a_f64": "pppppp" "pp" "iiiip",
     "dpb_build_nlist_noalloc_f64": "ppppp" "iiif" "i" "pp",

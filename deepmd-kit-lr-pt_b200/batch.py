@@ -16,7 +16,7 @@ import torch
 
 from . import _capi
 from ._capi import call, ptr
-from .model import SeAParams, _FittingTC
+from .model import PipelineTables, SeAParams, _FittingTC
 
 CELL_MARGIN = 1.0001  # cell edge >= rcut * margin, as the single-frame grid
 
@@ -89,7 +89,7 @@ class BatchEvaluator:
     """Energy [F], force [N, 3] and virial [F, 9] of F frames whose atoms are
     concatenated in frame order (compressed FP32 path, FP64 sums)."""
 
-    def __init__(self, params: SeAParams, frames, device="cuda:0"):
+    def __init__(self, params: SeAParams, frames, device="cuda:0", table_degree: int = 5):
         cfg = params.cfg
         self.cfg, self.params = cfg, params
         self.dev = dev = torch.device(device)
@@ -123,17 +123,7 @@ class BatchEvaluator:
                             for t in range(cfg.ntypes)])
         per_frame = np.array([np.bincount(t, minlength=cfg.ntypes) @ const_t for t in ft.types])
         self.e_const = torch.tensor(per_frame, dtype=f64, device=dev)
-        self.tab = []
-        s = torch.cuda.current_stream(dev).cuda_stream
-        for t, _ in params.tables:
-            ref_layout = torch.tensor(t, dtype=f32, device=dev)
-            packed = torch.empty_like(ref_layout)
-            call("dpb_se_a_pack_table_f32", ptr(packed), ptr(ref_layout), t.shape[0], M, s)
-            self.tab.append(packed)
-        torch.cuda.synchronize(dev)
-        self.tab_ptrs = (ctypes.c_void_p * len(self.tab))(*[t.data_ptr() for t in self.tab])
-        self.tab_info = np.ascontiguousarray(
-            np.concatenate([i for _, i in params.tables]).astype(np.float32))
+        self.ptab = PipelineTables(params, dev, table_degree)
         self.graph = None
         self.set_coords([fr[0] for fr in frames])
 
@@ -153,13 +143,13 @@ class BatchEvaluator:
              ptr(self.cell_off), ptr(self.box), ptr(self.ncell), ptr(self.row_frame), F, N,
              ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth), cfg.sec.ctypes.data,
              cfg.sec.size, ptr(self.status), s)
-        call("dpb_se_a_descriptor_fwd_f32", ptr(self.xyz), ptr(self.D), ptr(self.drow),
-             ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data, cfg.sec.ctypes.data,
-             cfg.sec.size, N, M, ax, s)
+        pt = self.ptab
+        call(pt.fwd, ptr(self.xyz), ptr(self.D), ptr(self.drow), ptr(self.em), pt.ptrs,
+             pt.info.ctypes.data, cfg.sec.ctypes.data, cfg.sec.size, N, M, ax, s)
         self.fit.layers(self.D, self.dD)
-        call("dpb_se_a_descriptor_bwd_f32", ptr(self.net_deriv), ptr(self.dD), ptr(self.drow),
-             ptr(self.xyz), ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data,
-             cfg.sec.ctypes.data, cfg.sec.size, N, M, ax, s)
+        call(pt.bwd, ptr(self.net_deriv), ptr(self.dD), ptr(self.drow), ptr(self.xyz),
+             ptr(self.em), pt.ptrs, pt.info.ctypes.data, cfg.sec.ctypes.data, cfg.sec.size, N,
+             M, ax, s)
         call("dpb_batch_force_virial_a", ptr(self.force), ptr(self.virial),
              ptr(self.net_deriv), ptr(self.cw), ptr(self.type), ptr(self.std),
              ptr(self.nlist), ptr(self.atom_off), ptr(self.cell_off), ptr(self.box),
@@ -213,7 +203,8 @@ class BatchEvaluator:
         from . import autotune
 
         cfg = self.cfg
-        sig = (f"batch:{self.nframes}f:{self.N}a:sel{'-'.join(map(str, cfg.sel))}:"
+        sig = (f"batch:{self.nframes}f:{self.N}a:deg{self.ptab.degree}:"
+               f"sel{'-'.join(map(str, cfg.sel))}:"
                f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
         return autotune.tune(self.replay, lambda: self.capture(),
                              ["batch_atoms_per_cta", "desc_atoms_per_cta", "desc_coef_l1",

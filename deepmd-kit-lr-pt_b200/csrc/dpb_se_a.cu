@@ -90,9 +90,12 @@ __device__ __forceinline__ int block_fold(const float4* e4, int n, int lane) {
 // q[k] holds a_k of the 4 channels, so each of the 6 loads of a warp reads one
 // contiguous 4M-byte segment of the row (M % 4 == 0 keeps them 16-byte
 // aligned).
+// NC = 6: the reference's quintic table; NC = 4: its cubic re-interpolation
+// on the fine grid (dpb_se_a_descriptor_*_cubic_f32).
+template <int NC>
 struct Coef4 {
-  float2 lo[6];  // a_k of channels (0, 1)
-  float2 hi[6];  // a_k of channels (2, 3)
+  float2 lo[NC];  // a_k of channels (0, 1)
+  float2 hi[NC];  // a_k of channels (2, 3)
 };
 
 // L2 cache policies: evict_first for data read once per step (env rows, x,
@@ -145,11 +148,11 @@ __device__ __forceinline__ float4 ld_coef(const float* p) {
   return v;
 }
 
-template <int CH = 0>
-__device__ __forceinline__ Coef4 load_coef4(const float* row, int M) {
-  Coef4 c;
+template <int CH, int NC>
+__device__ __forceinline__ Coef4<NC> load_coef4(const float* row, int M) {
+  Coef4<NC> c;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
+  for (int k = 0; k < NC; ++k) {
     const float4 v = ld_coef<CH>(row + k * M);
     c.lo[k] = make_float2(v.x, v.y);
     c.hi[k] = make_float2(v.z, v.w);
@@ -162,26 +165,25 @@ __device__ __forceinline__ Coef4 load_coef4(const float* row, int M) {
 // __fadd_rn).
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-// value only: a0 + (a1 + (a2 + (a3 + (a4 + a5 x) x) x) x) x  (tabulate.cc:123-130)
-__device__ __forceinline__ float2 hval2(const float2 (&c)[6], float2 x) {
-  float2 p = __ffma2_rn(c[5], x, c[4]);
-  p = __ffma2_rn(p, x, c[3]);
-  p = __ffma2_rn(p, x, c[2]);
-  p = __ffma2_rn(p, x, c[1]);
-  return __ffma2_rn(p, x, c[0]);
+// value only: a0 + (a1 + (a2 + (a3 + (a4 + a5 x) x) x) x) x  (tabulate.cc:123-130;
+// degree NC - 1)
+template <int NC>
+__device__ __forceinline__ float2 hval2(const float2 (&c)[NC], float2 x) {
+  float2 p = __ffma2_rn(c[NC - 1], x, c[NC - 2]);
+#pragma unroll
+  for (int k = NC - 3; k >= 0; --k) p = __ffma2_rn(p, x, c[k]);
+  return p;
 }
 
-// value and derivative by the joint Horner recurrence (9 FMA)
-__device__ __forceinline__ void hvalgrad2(const float2 (&c)[6], float2 x, float2& v, float2& g) {
-  float2 p = c[5], d = c[5];
-  p = __ffma2_rn(p, x, c[4]);
-  d = __ffma2_rn(d, x, p);
-  p = __ffma2_rn(p, x, c[3]);
-  d = __ffma2_rn(d, x, p);
-  p = __ffma2_rn(p, x, c[2]);
-  d = __ffma2_rn(d, x, p);
-  p = __ffma2_rn(p, x, c[1]);
-  d = __ffma2_rn(d, x, p);
+// value and derivative by the joint Horner recurrence (2 NC - 3 FMA)
+template <int NC>
+__device__ __forceinline__ void hvalgrad2(const float2 (&c)[NC], float2 x, float2& v, float2& g) {
+  float2 p = c[NC - 1], d = c[NC - 1];
+#pragma unroll
+  for (int k = NC - 2; k >= 1; --k) {
+    p = __ffma2_rn(p, x, c[k]);
+    d = __ffma2_rn(d, x, p);
+  }
   v = __ffma2_rn(p, x, c[0]);
   g = d;
 }
@@ -234,17 +236,18 @@ static size_t bwd_smem_floats(int M, int nnei, int naxis) {
 // one neighbor slot of the forward: G row of 4 channels (fold multiplier at
 // the fold slot) times the env row, accumulated into acc01[k] / acc23[k]
 // (channel pairs (0, 1) and (2, 3) of env column k)
-__device__ __forceinline__ void fwd_slot(float2 (&acc01)[4], float2 (&acc23)[4], const Coef4& c,
+template <int NC>
+__device__ __forceinline__ void fwd_slot(float2 (&acc01)[4], float2 (&acc23)[4], const Coef4<NC>& c,
                                          const float4 e, const float4 L, float rep) {
   const float2 x = f2(L.y);
   float2 v01, v23;
   if (L.z == 0.f) {
-    v01 = hval2(c.lo, x);
-    v23 = hval2(c.hi, x);
+    v01 = hval2<NC>(c.lo, x);
+    v23 = hval2<NC>(c.hi, x);
   } else {  // linear extrapolation outside the table (tabulate.cc:133-144)
     float2 g01, g23;
-    hvalgrad2(c.lo, x, v01, g01);
-    hvalgrad2(c.hi, x, v23, g23);
+    hvalgrad2<NC>(c.lo, x, v01, g01);
+    hvalgrad2<NC>(c.hi, x, v23, g23);
     v01 = __ffma2_rn(g01, f2(L.z), v01);
     v23 = __ffma2_rn(g23, f2(L.z), v23);
   }
@@ -278,7 +281,7 @@ __device__ __forceinline__ void write_descriptor(float* __restrict__ Dr, const f
 }
 
 // SWT warps (one center atom each) per CTA, about 20 warps per SM
-template <int SWT, int CH>
+template <int SWT, int CH, int NC>
 __global__ void __launch_bounds__(SWT * 32, 20 / SWT)
 k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
            const int* __restrict__ drow, const float* __restrict__ em,
@@ -307,7 +310,7 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
     const int last = brk < nt ? brk : nt - 1;
     if (!act) continue;
     const float* tab = tt.table[t] + m0;
-    const size_t rs = (size_t)M * 6;
+    const size_t rs = (size_t)M * NC;
     const float4* E = se + s0;
     const float4* Ls = sl + s0;
     auto rep = [&](int q) { return q == brk ? (float)(nt - q) : 1.f; };
@@ -316,15 +319,15 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
     // the current one is evaluated (reusing a row shared by consecutive slots
     // saves L1 traffic but costs the prefetch distance, a net loss measured
     // on 12k-atom water)
-    Coef4 ca = load_coef4<CH>(row(0), M), cb;
+    Coef4<NC> ca = load_coef4<CH, NC>(row(0), M), cb;
     int q = 0;
     for (; q + 1 <= last; q += 2) {
-      cb = load_coef4<CH>(row(q + 1), M);
-      fwd_slot(acc01, acc23, ca, E[q], Ls[q], rep(q));
-      if (q + 2 <= last) ca = load_coef4<CH>(row(q + 2), M);
-      fwd_slot(acc01, acc23, cb, E[q + 1], Ls[q + 1], rep(q + 1));
+      cb = load_coef4<CH, NC>(row(q + 1), M);
+      fwd_slot<NC>(acc01, acc23, ca, E[q], Ls[q], rep(q));
+      if (q + 2 <= last) ca = load_coef4<CH, NC>(row(q + 2), M);
+      fwd_slot<NC>(acc01, acc23, cb, E[q + 1], Ls[q + 1], rep(q + 1));
     }
-    if (q <= last) fwd_slot(acc01, acc23, ca, E[q], Ls[q], rep(q));
+    if (q <= last) fwd_slot<NC>(acc01, acc23, ca, E[q], Ls[q], rep(q));
   }
   __syncwarp();  // the slot staging is reused for x below
   float* sx = wsm;  // [4][M]
@@ -348,13 +351,14 @@ constexpr int GRP = 4;  // neighbors reduced together in the backward (even)
 // fold multiplier): P[0] = sum_c G'_c (e . dyr_c) + G_c dyr_c[0] (the two
 // terms of the slot's first output component), P[d] = sum_c G_c dyr_c[d] for
 // d = 1..3; dyr01[d] / dyr23[d] hold dyr of channel pairs (0, 1) / (2, 3)
-__device__ __forceinline__ void bwd_slot(float (&P)[4], const Coef4& c, const float4 e,
+template <int NC>
+__device__ __forceinline__ void bwd_slot(float (&P)[4], const Coef4<NC>& c, const float4 e,
                                          const float4 L, float rep, const float2 (&dyr01)[4],
                                          const float2 (&dyr23)[4]) {
   const float2 x = f2(L.y), dl = f2(L.z);
   float2 v01, g01, v23, g23;
-  hvalgrad2(c.lo, x, v01, g01);
-  hvalgrad2(c.hi, x, v23, g23);
+  hvalgrad2<NC>(c.lo, x, v01, g01);
+  hvalgrad2<NC>(c.hi, x, v23, g23);
   v01 = __ffma2_rn(g01, dl, v01);
   v23 = __ffma2_rn(g23, dl, v23);
   float2 d01 = __fmul2_rn(dyr01[0], f2(e.x));
@@ -380,7 +384,7 @@ __device__ __forceinline__ void bwd_slot(float (&P)[4], const Coef4& c, const fl
   }
 }
 
-template <int SWT, int CH>
+template <int SWT, int CH, int NC>
 __global__ void __launch_bounds__(SWT * 32, 20 / SWT)
 k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
            const int* __restrict__ drow, const float* __restrict__ xyz,
@@ -512,15 +516,15 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
     const int brk = block_fold(se + s0, nt, lane);
     const int last = brk < nt ? brk : nt - 1;
     const float* tab = tt.table[t] + m0;
-    const size_t rs = (size_t)M * 6;
+    const size_t rs = (size_t)M * NC;
     const float4* E = se + s0;
     const float4* Ls = sl + s0;
     auto rep = [&](int q) { return q == brk ? (float)(nt - q) : 1.f; };
     auto row = [&](int q) { return tab + (size_t)__float_as_int(Ls[q].x) * rs; };
     // two coefficient buffers in turn (GRP is even, so slot parity fixes the
     // buffer): the next slot's row is in flight while the current one is used
-    Coef4 ca, cb;
-    if (act) ca = load_coef4<CH>(row(0), M);
+    Coef4<NC> ca, cb;
+    if (act) ca = load_coef4<CH, NC>(row(0), M);
     for (int g0 = 0; g0 < nt; g0 += GRP) {
       if (g0 > last) {  // beyond the fold point: zero rows
         for (int qq = g0 + lane; qq < nt && qq < g0 + GRP; qq += 32)
@@ -535,11 +539,11 @@ k_desc_bwd(float* __restrict__ net_deriv, const float* __restrict__ dD,
         const int qq = g0 + q;
         if (qq <= last && act) {  // warp-uniform apart from the idle lanes
           if ((q & 1) == 0) {
-            if (qq + 1 <= last) cb = load_coef4<CH>(row(qq + 1), M);
-            bwd_slot(P[q], ca, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
+            if (qq + 1 <= last) cb = load_coef4<CH, NC>(row(qq + 1), M);
+            bwd_slot<NC>(P[q], ca, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
           } else {
-            if (qq + 1 <= last) ca = load_coef4<CH>(row(qq + 1), M);
-            bwd_slot(P[q], cb, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
+            if (qq + 1 <= last) ca = load_coef4<CH, NC>(row(qq + 1), M);
+            bwd_slot<NC>(P[q], cb, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
           }
         }
       }
@@ -748,8 +752,11 @@ __global__ void k_pack_table(float* __restrict__ out, const float* __restrict__ 
   }
 }
 
+// cubic: the tables are the uniform-stride cubic re-interpolation
+// (info = [lower, max, max, stride, stride, K] with K intervals and a
+// guard row K holding the value and slope at max)
 static int make_tables(TypeTables& tt, const float* const* tables, const float* info,
-                       const int* sec, int nsec, int M) {
+                       const int* sec, int nsec, int M, bool cubic = false) {
   if (nsec < 2 || nsec - 1 > PMAXT || tables == nullptr || info == nullptr || sec == nullptr) {
     set_error("se_a pipeline: need 1..%d neighbor types with tables, info and sec", PMAXT);
     return DPB_ERR_INVALID;
@@ -779,8 +786,17 @@ static int make_tables(TypeTables& tt, const float* const* tables, const float* 
     x.max = f[2];
     x.s0 = f[3];
     x.s1 = f[4];
-    x.first = (int)((x.upper - x.lower) / x.s0);
-    x.high_idx = x.first + (int)((nextafterf(x.max, x.lower) - x.upper) / x.s1);
+    if (cubic) {
+      if (!(f[5] >= 1.f) || f[1] != f[2] || f[3] != f[4] || !(f[3] > 0.f)) {
+        set_error("se_a pipeline: invalid cubic table info for neighbor type %d", t);
+        return DPB_ERR_INVALID;
+      }
+      x.first = (int)f[5];
+      x.high_idx = x.first;  // the guard row at max
+    } else {
+      x.first = (int)((x.upper - x.lower) / x.s0);
+      x.high_idx = x.first + (int)((nextafterf(x.max, x.lower) - x.upper) / x.s1);
+    }
   }
   return DPB_OK;
 }
@@ -820,13 +836,17 @@ int dpb_se_a_pack_table_f32(float* out, const float* table, int nrow, int M,
   return DPB_OK;
 }
 
-int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_row,
-                                const float* em, const float* const* tables,
-                                const float* table_info, const int* sec, int nsec,
-                                int nloc, int last_layer_size, int axis_neuron,
-                                dpb_stream_t stream) {
+}  // extern "C"
+
+namespace dpb {
+
+template <int NC>
+static int desc_fwd(float* xyz, float* descrpt, const int* descrpt_row, const float* em,
+                    const float* const* tables, const float* table_info, const int* sec,
+                    int nsec, int nloc, int last_layer_size, int axis_neuron,
+                    dpb_stream_t stream) {
   TypeTables tt;
-  int rc = make_tables(tt, tables, table_info, sec, nsec, last_layer_size);
+  int rc = make_tables(tt, tables, table_info, sec, nsec, last_layer_size, NC == 4);
   if (rc) return rc;
   if (axis_neuron <= 0 || axis_neuron > MAXAX || axis_neuron > last_layer_size) {
     set_error("se_a descriptor: axis_neuron must be in [1, min(%d, M)]", MAXAX);
@@ -850,11 +870,11 @@ int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_r
   auto pick = [&](auto sw_tag) -> int {
     constexpr int SWV = decltype(sw_tag)::value;
     switch (ch) {
-      case 1: return run(k_desc_fwd<SWV, 1>, SWV);
-      case 2: return run(k_desc_fwd<SWV, 2>, SWV);
-      case 3: return run(k_desc_fwd<SWV, 3>, SWV);
-      case 4: return run(k_desc_fwd<SWV, 4>, SWV);
-      default: return run(k_desc_fwd<SWV, 0>, SWV);
+      case 1: return run(k_desc_fwd<SWV, 1, NC>, SWV);
+      case 2: return run(k_desc_fwd<SWV, 2, NC>, SWV);
+      case 3: return run(k_desc_fwd<SWV, 3, NC>, SWV);
+      case 4: return run(k_desc_fwd<SWV, 4, NC>, SWV);
+      default: return run(k_desc_fwd<SWV, 0, NC>, SWV);
     }
   };
   switch (tune_value("desc_atoms_per_cta", SW)) {
@@ -864,13 +884,13 @@ int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_r
   }
 }
 
-int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
-                                const int* descrpt_row, const float* xyz, const float* em,
-                                const float* const* tables, const float* table_info,
-                                const int* sec, int nsec, int nloc, int last_layer_size,
-                                int axis_neuron, dpb_stream_t stream) {
+template <int NC>
+static int desc_bwd(float* net_deriv, const float* d_descrpt, const int* descrpt_row,
+                    const float* xyz, const float* em, const float* const* tables,
+                    const float* table_info, const int* sec, int nsec, int nloc,
+                    int last_layer_size, int axis_neuron, dpb_stream_t stream) {
   TypeTables tt;
-  int rc = make_tables(tt, tables, table_info, sec, nsec, last_layer_size);
+  int rc = make_tables(tt, tables, table_info, sec, nsec, last_layer_size, NC == 4);
   if (rc) return rc;
   if (axis_neuron <= 0 || axis_neuron > MAXAX || axis_neuron > last_layer_size) {
     set_error("se_a descriptor: axis_neuron must be in [1, min(%d, M)]", MAXAX);
@@ -894,11 +914,11 @@ int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
   auto pick = [&](auto sw_tag) -> int {
     constexpr int SWV = decltype(sw_tag)::value;
     switch (ch) {
-      case 1: return run(k_desc_bwd<SWV, 1>, SWV);
-      case 2: return run(k_desc_bwd<SWV, 2>, SWV);
-      case 3: return run(k_desc_bwd<SWV, 3>, SWV);
-      case 4: return run(k_desc_bwd<SWV, 4>, SWV);
-      default: return run(k_desc_bwd<SWV, 0>, SWV);
+      case 1: return run(k_desc_bwd<SWV, 1, NC>, SWV);
+      case 2: return run(k_desc_bwd<SWV, 2, NC>, SWV);
+      case 3: return run(k_desc_bwd<SWV, 3, NC>, SWV);
+      case 4: return run(k_desc_bwd<SWV, 4, NC>, SWV);
+      default: return run(k_desc_bwd<SWV, 0, NC>, SWV);
     }
   };
   switch (tune_value("desc_atoms_per_cta", SW)) {
@@ -906,6 +926,46 @@ int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
     case 8: return pick(std::integral_constant<int, 8>{});
     default: return pick(std::integral_constant<int, 4>{});
   }
+}
+
+}  // namespace dpb
+
+extern "C" {
+
+int dpb_se_a_descriptor_fwd_f32(float* xyz, float* descrpt, const int* descrpt_row,
+                                const float* em, const float* const* tables,
+                                const float* table_info, const int* sec, int nsec,
+                                int nloc, int last_layer_size, int axis_neuron,
+                                dpb_stream_t stream) {
+  return desc_fwd<6>(xyz, descrpt, descrpt_row, em, tables, table_info, sec, nsec, nloc,
+                     last_layer_size, axis_neuron, stream);
+}
+
+int dpb_se_a_descriptor_fwd_cubic_f32(float* xyz, float* descrpt, const int* descrpt_row,
+                                      const float* em, const float* const* tables,
+                                      const float* table_info, const int* sec, int nsec,
+                                      int nloc, int last_layer_size, int axis_neuron,
+                                      dpb_stream_t stream) {
+  return desc_fwd<4>(xyz, descrpt, descrpt_row, em, tables, table_info, sec, nsec, nloc,
+                     last_layer_size, axis_neuron, stream);
+}
+
+int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt,
+                                const int* descrpt_row, const float* xyz, const float* em,
+                                const float* const* tables, const float* table_info,
+                                const int* sec, int nsec, int nloc, int last_layer_size,
+                                int axis_neuron, dpb_stream_t stream) {
+  return desc_bwd<6>(net_deriv, d_descrpt, descrpt_row, xyz, em, tables, table_info, sec, nsec,
+                     nloc, last_layer_size, axis_neuron, stream);
+}
+
+int dpb_se_a_descriptor_bwd_cubic_f32(float* net_deriv, const float* d_descrpt,
+                                      const int* descrpt_row, const float* xyz, const float* em,
+                                      const float* const* tables, const float* table_info,
+                                      const int* sec, int nsec, int nloc, int last_layer_size,
+                                      int axis_neuron, dpb_stream_t stream) {
+  return desc_bwd<4>(net_deriv, d_descrpt, descrpt_row, xyz, em, tables, table_info, sec, nsec,
+                     nloc, last_layer_size, axis_neuron, stream);
 }
 
 int dpb_force_virial_a_env_mixed(double* force, double* virial, const float* net_deriv,

@@ -30,7 +30,7 @@ import torch
 
 from . import _capi, ops
 from ._capi import call, ptr
-from .model import SeAParams, _FittingTC
+from .model import PipelineTables, SeAParams, _FittingTC
 
 
 class ForwardLower:
@@ -39,7 +39,7 @@ class ForwardLower:
     rows hold at most ``max_nbor`` entries."""
 
     def __init__(self, params: SeAParams, nloc_max: int, nall_max: int, max_nbor: int = 512,
-                 device="cuda:0"):
+                 device="cuda:0", table_degree: int = 5):
         cfg = params.cfg
         if not params.tables:
             raise _capi.DPBInvalidArgument("forward_lower needs the compressed model's tables")
@@ -62,20 +62,7 @@ class ForwardLower:
         self.status = z(1, torch.int32)
         self.avg = torch.tensor(params.davg, dtype=f32, device=dev)
         self.std = torch.tensor(params.dstd, dtype=f32, device=dev)
-        s = torch.cuda.current_stream(dev).cuda_stream
-        self.tab = []
-        for t, _ in params.tables:
-            ref_layout = torch.tensor(t, dtype=f32, device=dev)
-            packed = torch.empty_like(ref_layout)
-            call("dpb_se_a_pack_table_f32", ptr(packed), ptr(ref_layout), t.shape[0], M, s)
-            self.tab.append(packed)
-        torch.cuda.synchronize(dev)
-        self.tab_ptrs = (ctypes.c_void_p * len(self.tab))(*[t.data_ptr() for t in self.tab])
-        self.tab_info = np.ascontiguousarray(
-            np.concatenate([i for _, i in params.tables]).astype(np.float32))
-        for (t, info), dt in zip(params.tables, self.tab):
-            if dt.numel() < ops.table_rows_needed(info.astype(np.float32)) * 6 * M:
-                raise _capi.DPBInvalidArgument("table smaller than its table_info addresses")
+        self.ptab = PipelineTables(params, dev, table_degree)
         self.fit = None
         self.nloc = -1
 
@@ -124,13 +111,13 @@ class ForwardLower:
              ptr(firstneigh), self.max_nbor, ptr(self.avg), ptr(self.std), nloc, nall, 1,
              ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth), sec.ctypes.data, sec.size,
              ptr(self.status), s)
-        call("dpb_se_a_descriptor_fwd_f32", ptr(self.xyz), ptr(self.D), ptr(self.drow),
-             ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data, sec.ctypes.data, sec.size,
-             nloc, M, ax, s)
+        pt = self.ptab
+        call(pt.fwd, ptr(self.xyz), ptr(self.D), ptr(self.drow), ptr(self.em), pt.ptrs,
+             pt.info.ctypes.data, sec.ctypes.data, sec.size, nloc, M, ax, s)
         self.fit.forward_backward(self.D[:nloc], self.dD[:nloc], energy)
-        call("dpb_se_a_descriptor_bwd_f32", ptr(self.net_deriv), ptr(self.dD), ptr(self.drow),
-             ptr(self.xyz), ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data,
-             sec.ctypes.data, sec.size, nloc, M, ax, s)
+        call(pt.bwd, ptr(self.net_deriv), ptr(self.dD), ptr(self.drow), ptr(self.xyz),
+             ptr(self.em), pt.ptrs, pt.info.ctypes.data, sec.ctypes.data, sec.size, nloc, M,
+             ax, s)
         call("dpb_force_virial_a_env_mixed_acc", ptr(force), ptr(virial), ptr(self.net_deriv),
              ptr(c), ptr(t), ptr(self.std), ptr(self.nlist), ptr(self.identity), nloc, nall,
              cfg.nnei, cfg.ntypes, ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth), s)

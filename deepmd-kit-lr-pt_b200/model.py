@@ -201,6 +201,46 @@ class _Fitting:
         return torch.addmm(bo, h, Wo).view(-1) + self.bias[t]
 
 
+class PipelineTables:
+    """The compression tables in the layout of the fused descriptor kernels:
+    the reference's quintic rows, coefficient-major per row
+    (dpb_se_a_pack_table_f32; degree 5), or their cubic re-interpolation on
+    the fine stride (table.cubic_table; degree 3), in FP32 on the device."""
+
+    def __init__(self, params: SeAParams, device, degree: int = 5):
+        if degree not in (3, 5):
+            raise _capi.DPBInvalidArgument("table_degree must be 5 (the reference's quintic "
+                                           "table) or 3 (its cubic re-interpolation)")
+        dev = torch.device(device)
+        M = params.cfg.neuron[-1]
+        self.degree = degree
+        self.tabs, infos = [], []
+        s = torch.cuda.current_stream(dev).cuda_stream
+        for t, info in params.tables:
+            if degree == 3:
+                cub = table_mod.cubic_table(t, info)
+                if cub is None:
+                    raise _capi.DPBInvalidArgument(
+                        "table_degree 3 needs stride1 to be a whole multiple of stride0")
+                coef, ic = cub
+                self.tabs.append(torch.tensor(coef.astype(np.float32).reshape(-1), device=dev))
+                infos.append(ic)
+            else:
+                ref_layout = torch.tensor(t, dtype=torch.float32, device=dev)
+                packed = torch.empty_like(ref_layout)
+                call("dpb_se_a_pack_table_f32", ptr(packed), ptr(ref_layout), t.shape[0], M, s)
+                self.tabs.append(packed)
+                if packed.numel() < ops.table_rows_needed(info.astype(np.float32)) * 6 * M:
+                    raise _capi.DPBInvalidArgument("table smaller than its table_info addresses")
+                infos.append(info)
+        torch.cuda.synchronize(dev)
+        self.ptrs = (ctypes.c_void_p * len(self.tabs))(*[x.data_ptr() for x in self.tabs])
+        self.info = np.ascontiguousarray(np.concatenate(infos).astype(np.float32))
+        sfx = "_cubic_f32" if degree == 3 else "_f32"
+        self.fwd = "dpb_se_a_descriptor_fwd" + sfx
+        self.bwd = "dpb_se_a_descriptor_bwd" + sfx
+
+
 class _FittingF64:
     """Per-type fitting networks of the FP64 plain path: the layers' GEMMs on
     the project's FP64 GEMM (dpb_gemm_f64), the activations, residuals, the
@@ -433,7 +473,8 @@ class SeAEvaluator:
 
     def __init__(self, params: SeAParams, atype: np.ndarray, box: np.ndarray,
                  mode: str = "compressed", device="cuda:0", nall_capacity: int | None = None,
-                 tensor_core_fitting: bool = True, skin: float = 0.0):
+                 tensor_core_fitting: bool = True, skin: float = 0.0,
+                 table_degree: int = 5):
         cfg = params.cfg
         if mode not in ("compressed", "plain"):
             raise _capi.DPBInvalidArgument(f"mode must be 'compressed' or 'plain', not {mode!r}")
@@ -497,21 +538,7 @@ class SeAEvaluator:
             self.D = torch.empty((nloc, M * ax), dtype=torch.float32, device=dev)
             self.dD = torch.empty_like(self.D)
             self.fit_tc = _FittingTC(params, counts, dev) if tensor_core_fitting else None
-            self.tab = []
-            for t, _ in params.tables:
-                ref_layout = torch.tensor(t, dtype=torch.float32, device=dev)
-                packed = torch.empty_like(ref_layout)
-                call("dpb_se_a_pack_table_f32", ptr(packed), ptr(ref_layout), t.shape[0], M,
-                     torch.cuda.current_stream(dev).cuda_stream)
-                self.tab.append(packed)
-            torch.cuda.synchronize(dev)
-            self.tab_ptrs = (ctypes.c_void_p * len(self.tab))(*[t.data_ptr() for t in self.tab])
-            self.tab_info = np.ascontiguousarray(
-                np.concatenate([i for _, i in params.tables]).astype(np.float32))
-            for (t, info), dt in zip(params.tables, self.tab):
-                need = ops.table_rows_needed(info.astype(np.float32)) * 6 * M
-                if dt.numel() < need:
-                    raise _capi.DPBInvalidArgument("table smaller than its table_info addresses")
+            self.ptab = PipelineTables(params, dev, table_degree)
         else:
             self._plain_setup(params, counts)
         if self.skin > 0:
@@ -669,10 +696,10 @@ class SeAEvaluator:
     def _descriptor_compressed(self, s, tm):
         cfg = self.cfg
         M, ax = cfg.neuron[-1], cfg.axis_neuron
+        pt = self.ptab
         with tm("descriptor_fwd"):
-            call("dpb_se_a_descriptor_fwd_f32", ptr(self.xyz), ptr(self.D), ptr(self.drow),
-                 ptr(self.em), self.tab_ptrs, self.tab_info.ctypes.data, self.sec.ctypes.data,
-                 self.sec.size, self.nloc, M, ax, s)
+            call(pt.fwd, ptr(self.xyz), ptr(self.D), ptr(self.drow), ptr(self.em), pt.ptrs,
+                 pt.info.ctypes.data, self.sec.ctypes.data, self.sec.size, self.nloc, M, ax, s)
         with tm("fitting"):
             if self.fit_tc is not None:
                 self.fit_tc.forward_backward(self.D, self.dD, self.energy)
@@ -686,10 +713,9 @@ class SeAEvaluator:
                     etot = etot + e.to(torch.float64).sum()
                 self.energy.copy_(etot.view(1))
         with tm("descriptor_bwd"):
-            call("dpb_se_a_descriptor_bwd_f32", ptr(self.net_deriv), ptr(self.dD),
-                 ptr(self.drow), ptr(self.xyz), ptr(self.em), self.tab_ptrs,
-                 self.tab_info.ctypes.data, self.sec.ctypes.data, self.sec.size, self.nloc, M,
-                 ax, s)
+            call(pt.bwd, ptr(self.net_deriv), ptr(self.dD), ptr(self.drow), ptr(self.xyz),
+                 ptr(self.em), pt.ptrs, pt.info.ctypes.data, self.sec.ctypes.data,
+                 self.sec.size, self.nloc, M, ax, s)
 
     def _descriptor_plain(self, s, tm):
         """Embedding net, descriptor, fitting and their backward in FP64:
@@ -737,7 +763,7 @@ class SeAEvaluator:
         from . import autotune
 
         cfg = self.cfg
-        sig = (f"frame:{self.nloc}a:{self.mode}:skin{self.skin:g}:"
+        sig = (f"frame:{self.nloc}a:{self.mode}:skin{self.skin:g}:deg{self.ptab.degree}:"
                f"sel{'-'.join(map(str, cfg.sel))}:"
                f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
         return autotune.tune(self.replay, lambda: self.capture(),

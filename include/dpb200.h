@@ -429,6 +429,27 @@ DPB_API int dpb_se_a_descriptor_bwd_f32(float* net_deriv, const float* d_descrpt
                                         const float* table_info, const int* sec,
                                         int nsec, int nloc, int last_layer_size,
                                         int axis_neuron, dpb_stream_t stream);
+/* The same two passes on the cubic re-interpolation of the tables (no
+ * counterpart in the reference): tables [K + 1, 4, M] FP32 per neighbor type,
+ * coefficient-major rows of a cubic Hermite on the fine stride everywhere
+ * (the reference's quintic rows give the value and slope at every knot; row K
+ * is a guard row [y(max), y'(max), 0, 0]); table_info [lower, max, max,
+ * stride, stride, K] per type. Four coefficients per channel instead of six
+ * cut the table bytes each neighbor slot gathers by a third; the cubic
+ * differs from the quintic by its Hermite remainder, h^4 / 384 times the
+ * fourth derivative of the embedding net. */
+DPB_API int dpb_se_a_descriptor_fwd_cubic_f32(float* xyz, float* descrpt,
+                                              const int* descrpt_row, const float* em,
+                                              const float* const* tables,
+                                              const float* table_info, const int* sec,
+                                              int nsec, int nloc, int last_layer_size,
+                                              int axis_neuron, dpb_stream_t stream);
+DPB_API int dpb_se_a_descriptor_bwd_cubic_f32(float* net_deriv, const float* d_descrpt,
+                                              const int* descrpt_row, const float* xyz,
+                                              const float* em, const float* const* tables,
+                                              const float* table_info, const int* sec,
+                                              int nsec, int nloc, int last_layer_size,
+                                              int axis_neuron, dpb_stream_t stream);
 /* prod_force_a + prod_virial_a in one pass with FP64 accumulation; ghost
  * forces are added to their owner mapping[j] (force: [nforce, 3], nforce =
  * nloc with a mapping, nall without). atom_virial [nall, 9] may be NULL. */

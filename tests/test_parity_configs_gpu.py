@@ -223,14 +223,16 @@ def water12288(dpb, mods):
     return coord, atype, box, params
 
 
-def test_water12288_compressed_vs_fp64_oracle(checker, mods, water12288):
-    """The benchmark frame: the mixed-precision compressed path against the
-    FP64 oracle of the same compressed model, every atom."""
+@pytest.mark.parametrize("degree", [5, 3])
+def test_water12288_compressed_vs_fp64_oracle(checker, mods, water12288, degree):
+    """The benchmark frame: the mixed-precision compressed path (the
+    reference's quintic table, or its cubic re-interpolation) against the FP64
+    oracle of the same compressed model, every atom."""
     from oracle import model_ref
 
     mdl = mods[1]
     coord, atype, box, params = water12288
-    ev = mdl.SeAEvaluator(params, atype, box, mode="compressed")
+    ev = mdl.SeAEvaluator(params, atype, box, mode="compressed", table_degree=degree)
     E, F, V = ev.compute(coord)
     ev.check()
     e0, f0, v0 = model_ref.evaluate(checker, params, coord, atype, box, mode="compressed",
@@ -239,7 +241,8 @@ def test_water12288_compressed_vs_fp64_oracle(checker, mods, water12288):
     e_err = abs(E - e0) / n
     f_rmse = float(np.sqrt(np.mean((F - f0) ** 2)))
     v_err = float(np.abs(V - v0).max())
-    print(f"12,288 atoms, compressed FP32 vs FP64 oracle: |dE|/N {e_err:.2e} eV/atom, "
+    print(f"12,288 atoms, compressed FP32 (table degree {degree}) vs FP64 oracle: "
+          f"|dE|/N {e_err:.2e} eV/atom, "
           f"force RMSE {f_rmse:.2e} eV/A, max |dF| {np.abs(F - f0).max():.2e}, |dV| {v_err:.2e}")
     assert e_err <= 1e-6
     assert f_rmse <= 1e-5
