@@ -345,6 +345,147 @@ k_desc_fwd(float* __restrict__ xyz_out, float* __restrict__ D,
   write_descriptor(D + (size_t)drow[i] * M * naxis, sx, M, naxis, lane);
 }
 
+// ---- tensor-core variant of the forward contraction (knob desc_tc = 1) ----
+// The contraction xyz[k, m] = sum_s e_s[k] G_s[m] as warp-level MMAs
+// (mma.sync m16n8k8, TF32 operands, 3xTF32 split for FP32-level products):
+// per group of 8 slots and 16 channels, A[m][s] = G_s[m] (each lane evaluates
+// the 4 table polynomials of its A-fragment positions: channels g, g + 8 of
+// slots t, t + 4, g = lane / 4, t = lane % 4) and B[s][k] = e_s[k] (k < 4,
+// columns 4..7 zero). Kept as a measured option next to the CUDA-core
+// contraction of k_desc_fwd.
+__device__ __forceinline__ unsigned tf32_rna(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const unsigned (&a)[4],
+                                         const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, "
+      "{%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// G of channel c (< M) at one staged slot L (row, offset, extrapolation
+// distance), times the fold multiplier
+template <int NC>
+__device__ __forceinline__ float g_scalar(const float* tab, size_t rs, int M, int c,
+                                          const float4 L, float rep) {
+  const float* r = tab + (size_t)__float_as_int(L.x) * rs + c;
+  float a[NC];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) a[k] = __ldg(r + k * M);
+  const float x = L.y;
+  float p = a[NC - 1], d = a[NC - 1];
+#pragma unroll
+  for (int k = NC - 2; k >= 1; --k) {
+    p = fmaf(p, x, a[k]);
+    d = fmaf(d, x, p);
+  }
+  const float v = fmaf(p, x, a[0]);
+  return (L.z == 0.f ? v : fmaf(d, L.z, v)) * rep;
+}
+
+constexpr int TC_MT = MAXM / 16;  // channel tiles of 16
+
+template <int SWT, int NC>
+__global__ void __launch_bounds__(SWT * 32, 20 / SWT)
+k_desc_fwd_tc(float* __restrict__ xyz_out, float* __restrict__ D,
+              const int* __restrict__ drow, const float* __restrict__ em,
+              TypeTables tt, int nloc, int M, int naxis, float inv_nnei, int warp_floats) {
+  extern __shared__ float4 dsm4[];
+  pdl_wait();
+  pdl_trigger();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * SWT + w;
+  if (i >= nloc) return;
+  const int nnei = tt.nnei;
+  float* wsm = reinterpret_cast<float*>(dsm4) + (size_t)w * warp_floats;
+  float4* se = reinterpret_cast<float4*>(wsm);
+  float4* sl = se + nnei;
+  stage_slots(se, sl, reinterpret_cast<const float4*>(em + (size_t)i * nnei * 4), tt, lane);
+  __syncwarp();
+  const int g = lane >> 2, t4 = lane & 3;
+  const int ntile = (M + 15) / 16;
+  float acc[TC_MT][4];
+#pragma unroll
+  for (int mt = 0; mt < TC_MT; ++mt)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[mt][k] = 0.f;
+  for (int t = 0; t < tt.ntypes; ++t) {
+    const int s0 = tt.sec[t], nt = tt.sec[t + 1] - s0;
+    if (nt <= 0) continue;
+    const int brk = block_fold(se + s0, nt, lane);
+    const int last = brk < nt ? brk : nt - 1;
+    const float* tab = tt.table[t];
+    const size_t rs = (size_t)M * NC;
+    for (int q0 = 0; q0 <= last; q0 += 8) {
+      const int qa = q0 + t4, qb = q0 + t4 + 4;
+      const bool va = qa <= last, vb = qb <= last;
+      // B: e_s[k] of slots qa (row t4) and qb (row t4 + 4), column g
+      float eb0 = 0.f, eb1 = 0.f;
+      if (g < 4) {
+        if (va) eb0 = reinterpret_cast<const float*>(se + s0 + qa)[g];
+        if (vb) eb1 = reinterpret_cast<const float*>(se + s0 + qb)[g];
+      }
+      unsigned bh[2], bl[2];
+      split_tf32(eb0, bh[0], bl[0]);
+      split_tf32(eb1, bh[1], bl[1]);
+      const float4 La = va ? sl[s0 + qa] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 Lb = vb ? sl[s0 + qb] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float ra = qa == brk ? (float)(nt - qa) : 1.f;
+      const float rb = qb == brk ? (float)(nt - qb) : 1.f;
+#pragma unroll
+      for (int mt = 0; mt < TC_MT; ++mt) {
+        if (mt >= ntile) break;
+        const int c0 = mt * 16 + g, c1 = c0 + 8;
+        const float a0 = (va && c0 < M) ? g_scalar<NC>(tab, rs, M, c0, La, ra) : 0.f;
+        const float a1 = (va && c1 < M) ? g_scalar<NC>(tab, rs, M, c1, La, ra) : 0.f;
+        const float a2 = (vb && c0 < M) ? g_scalar<NC>(tab, rs, M, c0, Lb, rb) : 0.f;
+        const float a3 = (vb && c1 < M) ? g_scalar<NC>(tab, rs, M, c1, Lb, rb) : 0.f;
+        unsigned ah[4], al[4];
+        split_tf32(a0, ah[0], al[0]);
+        split_tf32(a1, ah[1], al[1]);
+        split_tf32(a2, ah[2], al[2]);
+        split_tf32(a3, ah[3], al[3]);
+        mma_tf32(acc[mt], ah, bh);
+        mma_tf32(acc[mt], al, bh);
+        mma_tf32(acc[mt], ah, bl);
+      }
+    }
+  }
+  __syncwarp();  // the slot staging is reused for x below
+  float* sx = wsm;  // [4][M]
+  float* xo = xyz_out + (size_t)i * 4 * M;
+  // C fragment: rows (channels) g, g + 8; columns (env components) 2 t4, 2 t4 + 1
+  if (t4 < 2) {
+#pragma unroll
+    for (int mt = 0; mt < TC_MT; ++mt) {
+      if (mt >= ntile) break;
+      const int c0 = mt * 16 + g, c1 = c0 + 8;
+      const int k0 = 2 * t4, k1 = 2 * t4 + 1;
+      if (c0 < M) {
+        sx[k0 * M + c0] = acc[mt][0] * inv_nnei;
+        sx[k1 * M + c0] = acc[mt][1] * inv_nnei;
+      }
+      if (c1 < M) {
+        sx[k0 * M + c1] = acc[mt][2] * inv_nnei;
+        sx[k1 * M + c1] = acc[mt][3] * inv_nnei;
+      }
+    }
+  }
+  __syncwarp();
+  for (int q = lane; q < 4 * M; q += 32) xo[q] = sx[q];
+  write_descriptor(D + (size_t)drow[i] * M * naxis, sx, M, naxis, lane);
+}
+
 constexpr int GRP = 4;  // neighbors reduced together in the backward (even)
 
 // one neighbor slot of the backward over this lane's 4 channels (times the
@@ -867,8 +1008,10 @@ static int desc_fwd(float* xyz, float* descrpt, const int* descrpt_row, const fl
     return DPB_OK;
   };
   const int ch = tune_value("desc_coef_l1", 3);
+  const bool tc = tune_value("desc_tc", 0) != 0;
   auto pick = [&](auto sw_tag) -> int {
     constexpr int SWV = decltype(sw_tag)::value;
+    if (tc) return run(k_desc_fwd_tc<SWV, NC>, SWV);
     switch (ch) {
       case 1: return run(k_desc_fwd<SWV, 1, NC>, SWV);
       case 2: return run(k_desc_fwd<SWV, 2, NC>, SWV);

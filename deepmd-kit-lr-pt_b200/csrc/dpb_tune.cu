@@ -41,6 +41,11 @@ static Knob g_knobs[] = {
     // one frame's wrap / ghost copy / cell grid: 1 one cooperative launch,
     // 0 the separate kernels
     {"geometry_fused", 1, 2, {0, 1}},
+    // contraction of the fused descriptor forward: 0 FP32 CUDA cores (packed
+    // FMA on the table values in registers), 1 tensor cores (mma.sync
+    // m16n8k8, 3xTF32; the table values are evaluated in the MMA fragment
+    // layout)
+    {"desc_tc", 0, 2, {0, 1}},
     // programmatic dependent launch between the kernels of a step: 1 on
     // (each kernel's launch overlaps the previous kernel's tail), 0 off
     {"pdl", 1, 2, {0, 1}},

@@ -767,8 +767,8 @@ class SeAEvaluator:
                f"sel{'-'.join(map(str, cfg.sel))}:"
                f"M{cfg.neuron[-1]}:fit{'-'.join(map(str, cfg.fitting))}")
         return autotune.tune(self.replay, lambda: self.capture(),
-                             ["desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b",
-                              "pdl"],
+                             ["desc_atoms_per_cta", "desc_coef_l1", "desc_tc", "fit_n_tile",
+                              "fit_split_b", "pdl"],
                              signature=sig, reps=reps,
                              device=self.dev, use_cache=use_cache)
 

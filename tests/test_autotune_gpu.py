@@ -46,7 +46,7 @@ def test_batched_step_same_under_every_shape(mods, restore_knobs):
     ev = bt.BatchEvaluator(params, frames)
     E0, F0, V0 = ev.compute()
     for knob in ("batch_atoms_per_cta", "desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile",
-                 "fit_split_b"):
+                 "fit_split_b", "desc_tc"):
         for v, (E, F, V) in _sweep(at, knob, ev.compute).items():
             ev.check()
             np.testing.assert_allclose(E, E0, rtol=0, atol=1e-5, err_msg=f"{knob}={v}")
@@ -60,7 +60,7 @@ def test_frame_step_same_under_every_shape(mods, restore_knobs):
     params = mdl.prepare(mdl.init_params(mdl.SeAConfig(), seed=1), coord, atype, box)
     ev = mdl.SeAEvaluator(params, atype, box, mode="compressed")
     E0, F0, V0 = ev.compute(coord)
-    for knob in ("desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b"):
+    for knob in ("desc_atoms_per_cta", "desc_coef_l1", "fit_n_tile", "fit_split_b", "desc_tc"):
         for v, (E, F, V) in _sweep(at, knob, lambda: ev.compute(coord)).items():
             assert abs(E - E0) < 1e-4, (knob, v)
             np.testing.assert_allclose(F, F0, rtol=0, atol=1e-6, err_msg=f"{knob}={v}")
@@ -111,3 +111,20 @@ def test_autotuner_leaves_a_working_step(mods, restore_knobs, tmp_path, monkeypa
     np.testing.assert_allclose(F1, F0, rtol=0, atol=1e-6)
     again = ev.tune(reps=3)
     assert again["cached"] and again["knobs"] == res["knobs"]
+
+
+@pytest.mark.parametrize("degree", [5, 3])
+def test_tensor_core_contraction_matches(mods, restore_knobs, degree):
+    """desc_tc = 1 (the forward contraction on the tensor cores, 3xTF32)
+    against the CUDA-core contraction: xyz and D to FP32 resolution."""
+    mdl, wl, at = mods["model"], mods["workload"], mods["autotune"]
+    coord, atype, box = wl.water_frame(5, seed=6)
+    params = mdl.prepare(mdl.init_params(mdl.SeAConfig(), seed=1), coord, atype, box)
+    ev = mdl.SeAEvaluator(params, atype, box, mode="compressed", table_degree=degree)
+    out = {}
+    for v in (0, 1):
+        at.set_knob("desc_tc", v)
+        ev.compute(coord)
+        out[v] = (ev.xyz.double().cpu().numpy(), ev.D.double().cpu().numpy())
+    for a, b in zip(out[1], out[0]):
+        assert np.abs(a - b).max() <= 2e-6 * np.abs(b).max()
