@@ -118,6 +118,8 @@ _FUNCS = {
     "dpb_use_nlist_map": "pp" "ii" "p",
     "dpb_nlist_rows_to_device": "pppp" "i" "ppp" "i" "p" "L" "p",
     "dpb_gemm_f64": "pppp" "iiiiii" "iii" "p",
+    "dpb_gemm_f32": "pppp" "iiiiii" "iii" "p",
+    "dpb_transpose_f32": "pp" "iiiii" "p",
 }
 _TRAIN = {
     "dpb_se_a_train_fwd": "pppppppppp" "iii" "pp",

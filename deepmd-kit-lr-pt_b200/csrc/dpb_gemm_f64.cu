@@ -1,5 +1,7 @@
 // FP64 GEMM for the fitting network of the FP64 plain path (and the FP64
-// training step): C[M, N] = op(A) op(B) (+ bias[N]) (+ C), row-major, with
+// training step), and its FP32 instance for the shapes the tensor-core GEMM
+// does not take (N not a multiple of 80): C[M, N] = op(A) op(B) (+ bias[N])
+// (+ C), row-major, with
 // op(X) = X or X^T. The fitting layers are y = x W + b (forward, W [in, out]
 // as stored), g_in = g W^T (input gradient) and gW += x^T g (weight
 // gradient), the layer algebra of deepmd/dpmodel/utils/network.py:282-330.
@@ -19,20 +21,25 @@ namespace {
 constexpr int GB_M = 64, GB_N = 64, GB_K = 16, GB_T = 256;
 
 // element (r, c) of op(X) for an [rows, cols] operand with leading dim ld
-template <bool TRANS>
-__device__ __forceinline__ double ld_op(const double* __restrict__ X, int r, int c, int rows,
-                                        int cols, int ld) {
-  if (r >= rows || c >= cols) return 0.0;
+template <bool TRANS, typename T>
+__device__ __forceinline__ T ld_op(const T* __restrict__ X, int r, int c, int rows, int cols,
+                                   int ld) {
+  if (r >= rows || c >= cols) return (T)0;
   return TRANS ? X[(size_t)c * ld + r] : X[(size_t)r * ld + c];
 }
 
-template <bool TA, bool TB>
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+template <bool TA, bool TB, typename T>
 __global__ void __launch_bounds__(GB_T)
-k_gemm_f64(double* __restrict__ C, const double* __restrict__ A, const double* __restrict__ B,
-           const double* __restrict__ bias, int M, int N, int K, int lda, int ldb, int ldc,
+k_gemm_f64(T* __restrict__ C, const T* __restrict__ A, const T* __restrict__ B,
+           const T* __restrict__ bias, int M, int N, int K, int lda, int ldb, int ldc,
            int accumulate) {
-  __shared__ __align__(16) double As[2][GB_K][GB_M + 2];
-  __shared__ __align__(16) double Bs[2][GB_K][GB_N + 2];
+  using T2 = typename Vec2<T>::type;
+  __shared__ __align__(16) T As[2][GB_K][GB_M + 2];
+  __shared__ __align__(16) T Bs[2][GB_K][GB_N + 2];
   pdl_wait();
   const int tid = threadIdx.x;
   const int m0 = blockIdx.y * GB_M, n0 = blockIdx.x * GB_N;
@@ -40,19 +47,19 @@ k_gemm_f64(double* __restrict__ C, const double* __restrict__ A, const double* _
   // staging assignment: 64 x 16 = 1024 elements per operand, 4 per thread.
   // A (op(A) is M x K): element q = tid + 256 j -> (row, k); for a plain A
   // consecutive threads walk k (contiguous in memory), for A^T they walk m.
-  double ra[4], rb[4];
+  T ra[4], rb[4];
   auto fetch = [&](int k0) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int q = tid + GB_T * j;
       int r, k;
       if (TA) { r = q & 63; k = q >> 6; } else { k = q & 15; r = q >> 4; }
-      ra[j] = TA ? ld_op<true>(A, m0 + r, k0 + k, M, K, lda)
-                 : ld_op<false>(A, m0 + r, k0 + k, M, K, lda);
+      ra[j] = TA ? ld_op<true, T>(A, m0 + r, k0 + k, M, K, lda)
+                 : ld_op<false, T>(A, m0 + r, k0 + k, M, K, lda);
       int c, kk;
       if (TB) { kk = q & 15; c = q >> 4; } else { c = q & 63; kk = q >> 6; }
-      rb[j] = TB ? ld_op<true>(B, k0 + kk, n0 + c, K, N, ldb)
-                 : ld_op<false>(B, k0 + kk, n0 + c, K, N, ldb);
+      rb[j] = TB ? ld_op<true, T>(B, k0 + kk, n0 + c, K, N, ldb)
+                 : ld_op<false, T>(B, k0 + kk, n0 + c, K, N, ldb);
     }
   };
   auto stash = [&](int buf) {
@@ -67,11 +74,11 @@ k_gemm_f64(double* __restrict__ C, const double* __restrict__ A, const double* _
       Bs[buf][kk][c] = rb[j];
     }
   };
-  double acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j] = (T)0;
   const int nk = (K + GB_K - 1) / GB_K;
   fetch(0);
   stash(0);
@@ -81,12 +88,12 @@ k_gemm_f64(double* __restrict__ C, const double* __restrict__ A, const double* _
     if (t + 1 < nk) fetch((t + 1) * GB_K);
 #pragma unroll
     for (int k = 0; k < GB_K; ++k) {
-      const double2 a01 = *reinterpret_cast<const double2*>(&As[buf][k][ty * 4]);
-      const double2 a23 = *reinterpret_cast<const double2*>(&As[buf][k][ty * 4 + 2]);
-      const double2 b01 = *reinterpret_cast<const double2*>(&Bs[buf][k][tx * 4]);
-      const double2 b23 = *reinterpret_cast<const double2*>(&Bs[buf][k][tx * 4 + 2]);
-      const double a[4] = {a01.x, a01.y, a23.x, a23.y};
-      const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+      const T2 a01 = *reinterpret_cast<const T2*>(&As[buf][k][ty * 4]);
+      const T2 a23 = *reinterpret_cast<const T2*>(&As[buf][k][ty * 4 + 2]);
+      const T2 b01 = *reinterpret_cast<const T2*>(&Bs[buf][k][tx * 4]);
+      const T2 b23 = *reinterpret_cast<const T2*>(&Bs[buf][k][tx * 4 + 2]);
+      const T a[4] = {a01.x, a01.y, a23.x, a23.y};
+      const T b[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -106,9 +113,9 @@ k_gemm_f64(double* __restrict__ C, const double* __restrict__ A, const double* _
     for (int j = 0; j < 4; ++j) {
       const int c = n0 + tx * 4 + j;
       if (c >= N) continue;
-      double v = acc[i][j];
+      T v = acc[i][j];
       if (bias) v += bias[c];
-      double* p = C + (size_t)r * ldc + c;
+      T* p = C + (size_t)r * ldc + c;
       if (accumulate) v += *p;
       *p = v;
     }
@@ -120,38 +127,89 @@ k_gemm_f64(double* __restrict__ C, const double* __restrict__ A, const double* _
 
 using namespace dpb;
 
-extern "C" int dpb_gemm_f64(double* C, const double* A, const double* B, const double* bias,
-                            int M, int N, int K, int lda, int ldb, int ldc, int trans_a,
-                            int trans_b, int accumulate, dpb_stream_t stream) {
+template <typename T>
+static int gemm(const char* what, T* C, const T* A, const T* B, const T* bias, int M, int N,
+                int K, int lda, int ldb, int ldc, int trans_a, int trans_b, int accumulate,
+                dpb_stream_t stream) {
   if (M < 0 || N < 0 || K < 0 || (M > 0 && N > 0 && (!C || (K > 0 && (!A || !B))))) {
-    set_error("gemm_f64: invalid arguments (M=%d N=%d K=%d)", M, N, K);
+    set_error("%s: invalid arguments (M=%d N=%d K=%d)", what, M, N, K);
     return DPB_ERR_INVALID;
   }
   const int a_cols = trans_a ? M : K, b_cols = trans_b ? K : N;
   if (ldc < N || lda < a_cols || ldb < b_cols) {
-    set_error("gemm_f64: leading dimensions too small (lda=%d ldb=%d ldc=%d)", lda, ldb, ldc);
+    set_error("%s: leading dimensions too small (lda=%d ldb=%d ldc=%d)", what, lda, ldb, ldc);
     return DPB_ERR_INVALID;
   }
   if (M == 0 || N == 0) return DPB_OK;
   const dim3 grid((N + GB_N - 1) / GB_N, (M + GB_M - 1) / GB_M);
   if (grid.y > 65535) {
-    set_error("gemm_f64: M=%d needs more than 65535 row tiles", M);
+    set_error("%s: M=%d needs more than 65535 row tiles", what, M);
     return DPB_ERR_INVALID;
   }
   cudaStream_t st = as_stream(stream);
   const int ta = trans_a != 0, tb = trans_b != 0;
   if (!ta && !tb)
-    launch_pdl(k_gemm_f64<false, false>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K, lda,
-               ldb, ldc, accumulate);
+    launch_pdl(k_gemm_f64<false, false, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
+               lda, ldb, ldc, accumulate);
   else if (!ta && tb)
-    launch_pdl(k_gemm_f64<false, true>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K, lda,
-               ldb, ldc, accumulate);
+    launch_pdl(k_gemm_f64<false, true, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
+               lda, ldb, ldc, accumulate);
   else if (ta && !tb)
-    launch_pdl(k_gemm_f64<true, false>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K, lda,
-               ldb, ldc, accumulate);
+    launch_pdl(k_gemm_f64<true, false, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
+               lda, ldb, ldc, accumulate);
   else
-    launch_pdl(k_gemm_f64<true, true>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K, lda,
-               ldb, ldc, accumulate);
-  DPB_CHECK_LAUNCH("gemm_f64");
+    launch_pdl(k_gemm_f64<true, true, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
+               lda, ldb, ldc, accumulate);
+  DPB_CHECK_LAUNCH(what);
+  return DPB_OK;
+}
+
+extern "C" int dpb_gemm_f64(double* C, const double* A, const double* B, const double* bias,
+                            int M, int N, int K, int lda, int ldb, int ldc, int trans_a,
+                            int trans_b, int accumulate, dpb_stream_t stream) {
+  return gemm<double>("gemm_f64", C, A, B, bias, M, N, K, lda, ldb, ldc, trans_a, trans_b,
+                      accumulate, stream);
+}
+
+extern "C" int dpb_gemm_f32(float* C, const float* A, const float* B, const float* bias, int M,
+                            int N, int K, int lda, int ldb, int ldc, int trans_a, int trans_b,
+                            int accumulate, dpb_stream_t stream) {
+  return gemm<float>("gemm_f32", C, A, B, bias, M, N, K, lda, ldb, ldc, trans_a, trans_b,
+                     accumulate, stream);
+}
+
+// out[c * ld_out + r] = in[r * ld_in + c] for r < rows, c < cols, and zero for
+// rows <= r < out_rows (a K padded to a multiple of 4 for the tensor-core
+// GEMM's 16-byte rows, or one block of a concatenation along K)
+__global__ void k_transpose_f32(float* __restrict__ out, const float* __restrict__ in, int rows,
+                                int cols, int ld_in, int ld_out, int out_rows) {
+  __shared__ float tile[32][33];
+  pdl_wait();
+  pdl_trigger();
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int r = r0 + k, c = c0 + threadIdx.x;
+    tile[k][threadIdx.x] = (r < rows && c < cols) ? in[(size_t)r * ld_in + c] : 0.f;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int c = c0 + k, r = r0 + threadIdx.x;
+    if (c < cols && r < out_rows) out[(size_t)c * ld_out + r] = tile[threadIdx.x][k];
+  }
+}
+
+extern "C" int dpb_transpose_f32(float* out, const float* in, int rows, int cols, int ld_in,
+                                 int ld_out, int out_rows, dpb_stream_t stream) {
+  if (rows < 0 || cols < 0 || out_rows < rows || ld_out < out_rows || ld_in < cols ||
+      (out_rows > 0 && cols > 0 && (!out || (rows > 0 && !in)))) {
+    set_error("transpose_f32: invalid arguments (rows=%d cols=%d ld_in=%d ld_out=%d "
+              "out_rows=%d)", rows, cols, ld_in, ld_out, out_rows);
+    return DPB_ERR_INVALID;
+  }
+  if (cols == 0 || out_rows == 0) return DPB_OK;
+  const dim3 grid((cols + 31) / 32, (out_rows + 31) / 32);
+  DPB_CUDA(launch_pdl(k_transpose_f32, grid, dim3(32, 8), 0, as_stream(stream), out, in, rows,
+                      cols, ld_in, ld_out, out_rows),
+           "transpose_f32");
   return DPB_OK;
 }

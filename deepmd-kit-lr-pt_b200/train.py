@@ -8,8 +8,9 @@ The reference trains this model with PyTorch autograd: the force is
 (deepmd/pt/loss/ener.py:219-340) is differentiated through it. Here:
 
 * forward  (SeATrainer._forward): geometry (dpb_batch_env_mat_a_*), the
-  embedding and descriptor (dpb_se_a_train_fwd_*), the fitting net (library
-  GEMM + dpb_fit_act_*), E per frame; the force backward through the
+  embedding and descriptor (dpb_se_a_train_fwd_*), the fitting net (the
+  project's GEMMs: 3xTF32 tensor cores in FP32, dpb_gemm_f64 in FP64; layer
+  kernels dpb_fit_*), E per frame; the force backward through the
   fitting (dpb_fit_bwd_*) and the embedding (dpb_se_a_train_bwd_*) to
   g = dE/d(em); force and virial (dpb_batch_force_virial_a*);
 * backward (SeATrainer._backward), given dL/dE, dL/dF, dL/dV: the force
@@ -38,6 +39,9 @@ from . import _capi
 from ._capi import call, ptr
 from .batch import FrameTable
 from .model import SeAParams
+
+# epilogues of dpb_gemm_tf32x3_f32 (include/dpb200.h)
+EPI_STORE, EPI_TANH, EPI_RES_DT = 0, 1, 2
 
 EMB_PREFIX = "atomic_model.descriptor.sea.filter_layers.networks"
 FIT_PREFIX = "atomic_model.fitting_net.filter_layers.networks"
@@ -206,9 +210,15 @@ class SeATrainer:
         specs = param_specs(params)
         self.names = [n for n, _ in specs]
         self.shapes = [a.shape for _, a in specs]
-        sizes = [int(a.size) for _, a in specs]
-        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
-        flat = np.concatenate([a.ravel() for _, a in specs]) if specs else np.zeros(0)
+        # every tensor starts on a 16-byte boundary of the flat vector (the
+        # tensor-core GEMM reads biases and writes weight gradients in place);
+        # the gaps stay zero and get zero gradients
+        self.sizes = [int(a.size) for _, a in specs]
+        padded = [(n + 3) // 4 * 4 for n in self.sizes]
+        self.offsets = np.concatenate([[0], np.cumsum(padded)]).astype(np.int64)
+        flat = np.zeros(int(self.offsets[-1]))
+        for k, (_, a) in enumerate(specs):
+            flat[int(self.offsets[k]):int(self.offsets[k]) + self.sizes[k]] = np.ravel(a)
         self.flat = torch.tensor(flat, dtype=dtype, device=dev).requires_grad_(True)
         self.grad = torch.zeros(self.flat.numel(), dtype=dtype, device=dev)
         self.adam_m = torch.zeros_like(self.grad)
@@ -284,7 +294,11 @@ class SeATrainer:
             n = self.fit_rows[t][1]
             bufs = [{k: z((n, ly["w_out"])) for k in ("Y", "H", "G", "Zb", "Zd", "Hd", "A",
                                                        "Ad", "Zbd")} for ly in layers]
+            for ly, bf in zip(layers, bufs):
+                self._tc_setup(ly, bf, n, z)
             self.fbuf.append(bufs)
+        self._e_dummy = z(1)
+        self._rows_cache = {}
         self._streams = [torch.cuda.Stream(device=dev) for _ in range(nt)]
         self.loss = loss
         self._natoms_inv = torch.tensor(1.0 / np.maximum(ft.counts, 1), dtype=f64, device=dev)
@@ -294,10 +308,29 @@ class SeATrainer:
         self.graph = None
         self.set_coords([fr[0] for fr in frames])
 
+    def _tc_setup(self, ly, bf, n, z):
+        """Tensor-core buffers of one FP32 fitting layer: W^T for x W (and
+        the tangent), and the transposed operands of the weight gradient."""
+        w_in, w_out = ly["w_in"], ly["w_out"]
+        res = _res(w_out, w_in)
+        ly["WT"] = None
+        ly["d_or_one"] = ly["d"]
+        if self._tc_ok(w_out, w_in) and (res == 1 or (res == 0 and ly["d"] is None)):
+            ly["WT"] = z((w_out, w_in))
+            if res == 1 and ly["d"] is None:
+                ly["d_or_one"] = torch.ones(w_out, dtype=self.dtype, device=self.dev)
+            if res == 0:
+                bf["H"] = bf["Y"]  # tanh(x W + b) is the layer's output
+        bf["At"] = bf["Bt"] = None
+        kp = (2 * n + 3) // 4 * 4
+        if self._tc_ok(w_out, kp) and n > 0:
+            bf["At"] = z((w_in, kp))
+            bf["Bt"] = z((w_out, kp))
+
     # ---------------------------------------------------------- parameters
     def _views(self, base: torch.Tensor) -> dict:
-        return {n: base[int(self.offsets[k]):int(self.offsets[k + 1])].view(self.shapes[k])
-                for k, n in enumerate(self.names)}
+        return {n: base[int(self.offsets[k]):int(self.offsets[k]) + self.sizes[k]]
+                .view(self.shapes[k]) for k, n in enumerate(self.names)}
 
     def named_parameters(self) -> dict:
         """{reference state_dict name: view of the flat parameters}."""
@@ -325,15 +358,51 @@ class SeATrainer:
                 dst.copy_(src)
 
     # ------------------------------------------------------------ forward
+    # ------------------------------------------------------------- GEMMs
+    # The fitting layers' products on this package's GEMMs: in FP32 the
+    # 3xTF32 tensor-core GEMM (dpb_gemm_tf32x3_f32, weights split into TF32
+    # hi / lo in the kernel) wherever its output width is a multiple of 80,
+    # else the FP32 SIMT GEMM; in FP64 dpb_gemm_f64.
+    def _mm(self, C, A, B, bias, M, N, K, ta, tb, acc, s):
+        """C = op(A) op(B) (+ bias) (+ C), row-major operands."""
+        call(f"dpb_gemm_{self.suf}", ptr(C), ptr(A), ptr(B), ptr(bias), M, N, K,
+             int(A.shape[-1]), int(B.shape[-1]), int(C.shape[-1]), ta, tb, acc, s)
+
+    def _tc_ok(self, N: int, K: int) -> bool:
+        return self.suf == "f32" and N % 80 == 0 and K % 4 == 0
+
+    def _tc(self, A, M, K, B, N, mode, out0, s, out1=None, aux0=None, bias=None, idt=None):
+        """out0 (, out1) = epilogue(A [M, K] B^T) with B [N, K] FP32 (split in
+        the kernel), one row group."""
+        vp = lambda t: None if t is None else (ctypes.c_void_p * 1)(t.data_ptr())  # noqa: E731
+        call("dpb_gemm_tf32x3_f32", ptr(A), M, K, vp(B), None, N, self._rows1(M), 1, mode,
+             ptr(out0), ptr(out1), ptr(aux0), None, vp(bias), vp(idt), None, ptr(self._e_dummy),
+             ptr(self.status), s)
+
+    def _rows1(self, M):
+        a = self._rows_cache.get(M)
+        if a is None:
+            a = self._rows_cache[M] = np.array([M], np.int32)
+        return a.ctypes.data
+
     def _adj_in(self, out, Zb, W, G, w_out, w_in, s):
         """out = Zb W^T + (adjoint of the layer's residual, from G)."""
-        r = _res(w_out, w_in)
-        if r == 1:
-            torch.addmm(G, Zb, W.t(), out=out)
+        n = out.shape[0]
+        if self._tc_ok(w_in, w_out):
+            self._tc(Zb, n, w_out, W, w_in, EPI_STORE, out, s)
         else:
-            torch.mm(Zb, W.t(), out=out)
-            if r == 2:
-                call(f"dpb_fit_res_adj_{self.suf}", ptr(out), ptr(G), out.shape[0], w_out, w_in, s)
+            self._mm(out, Zb, W, None, n, w_in, w_out, 0, 1, 0, s)
+        if _res(w_out, w_in):
+            call(f"dpb_fit_res_adj_{self.suf}", ptr(out), ptr(G), n, w_out, w_in, s)
+
+    def _weights_t(self, s):
+        """W^T of every fitting layer whose forward runs on the tensor cores
+        (the weights change every step)."""
+        for layers, _ in self.fit_layers:
+            for ly in layers:
+                if ly.get("WT") is not None:
+                    call("dpb_transpose_f32", ptr(ly["WT"]), ptr(ly["W"]), ly["w_in"],
+                         ly["w_out"], ly["w_out"], ly["w_in"], ly["w_in"], s)
 
     def _forward(self):
         cfg, ft, suf = self.cfg, self.ft, self.suf
@@ -342,6 +411,7 @@ class SeATrainer:
         sec = self.sec
         rc, rs = ctypes.c_float(cfg.rcut), ctypes.c_float(cfg.rcut_smth)
         self._version += 1
+        self._weights_t(s)
         call(f"dpb_batch_env_mat_a_{suf}", ptr(self.em), ptr(self.nlist), ptr(ft.cw),
              ptr(ft.cell_of), ptr(ft.cell_start), ptr(ft.cell_atoms), ptr(self.coord),
              ptr(ft.type), ptr(self.avg), ptr(self.std), ptr(ft.atom_off), ptr(ft.cell_off),
@@ -390,9 +460,17 @@ class SeATrainer:
         o, n = self.fit_rows[t]
         H = self.D[o:o + n]
         for ly, bf in zip(layers, bufs):
-            torch.addmm(ly["b"], H, ly["W"], out=bf["Y"])
-            call(f"dpb_fit_act_{suf}", ptr(bf["Y"]), ptr(bf["H"]), ptr(H), ptr(ly["d"]), n,
-                 ly["w_out"], ly["w_in"], s)
+            if ly.get("WT") is not None:  # bias, tanh and residual in the epilogue
+                if _res(ly["w_out"], ly["w_in"]):
+                    self._tc(H, n, ly["w_in"], ly["WT"], ly["w_out"], EPI_RES_DT, bf["Y"], s,
+                             out1=bf["H"], aux0=H, bias=ly["b"], idt=ly["d_or_one"])
+                else:  # H aliases Y
+                    self._tc(H, n, ly["w_in"], ly["WT"], ly["w_out"], EPI_TANH, bf["Y"], s,
+                             bias=ly["b"])
+            else:
+                self._mm(bf["Y"], H, ly["W"], ly["b"], n, ly["w_out"], ly["w_in"], 0, 0, 0, s)
+                call(f"dpb_fit_act_{suf}", ptr(bf["Y"]), ptr(bf["H"]), ptr(H), ptr(ly["d"]), n,
+                     ly["w_out"], ly["w_in"], s)
             H = bf["H"]
         call(f"dpb_fit_out_{suf}", ptr(self.e_rows[o:o + n]), ptr(H), ptr(out["W"]),
              ptr(out["b"]), ctypes.c_double(out["ebias"]), n, out["w"], s)
@@ -415,7 +493,10 @@ class SeATrainer:
         o, n = self.fit_rows[t]
         Hd = self.Dt[o:o + n]
         for ly, bf in zip(layers, bufs):
-            torch.mm(Hd, ly["W"], out=bf["Zd"])
+            if ly.get("WT") is not None:
+                self._tc(Hd, n, ly["w_in"], ly["WT"], ly["w_out"], EPI_STORE, bf["Zd"], s)
+            else:
+                self._mm(bf["Zd"], Hd, ly["W"], None, n, ly["w_out"], ly["w_in"], 0, 0, 0, s)
             call(f"dpb_fit_tan_{suf}", ptr(bf["Hd"]), ptr(bf["Zd"]), ptr(Hd), ptr(bf["Y"]),
                  ptr(ly["d"]), n, ly["w_out"], ly["w_in"], s)
             Hd = bf["Hd"]
@@ -429,12 +510,29 @@ class SeATrainer:
                  ptr(ly["d"]), n, ly["w_out"], s)
             Hin = self.D[o:o + n] if l == 0 else bufs[l - 1]["H"]
             Hdin = self.Dt[o:o + n] if l == 0 else bufs[l - 1]["Hd"]
-            ly["gW"].addmm_(Hin.t(), bf["Zb"])
-            ly["gW"].addmm_(Hdin.t(), bf["Zbd"])
+            self._weight_grad(ly, bf, Hin, Hdin, n, s)
             dA = self.DbarJ[o:o + n] if l == 0 else bufs[l - 1]["A"]
             dAd = self.Ddbar[o:o + n] if l == 0 else bufs[l - 1]["Ad"]
             self._adj_in(dA, bf["Zb"], ly["W"], bf["A"], ly["w_out"], ly["w_in"], s)
             self._adj_in(dAd, bf["Zbd"], ly["W"], bf["Ad"], ly["w_out"], ly["w_in"], s)
+
+    def _weight_grad(self, ly, bf, Hin, Hdin, n, s):
+        """gW = Hin^T Zb + Hdin^T Zbd (the gradient buffer was zeroed): on the
+        tensor cores as one product along K = 2 n of the transposed operands
+        [Hin | Hdin]^T and [Zb | Zbd]^T, else two SIMT products."""
+        w_in, w_out = ly["w_in"], ly["w_out"]
+        At, Bt = bf.get("At"), bf.get("Bt")
+        if At is not None:
+            kp = At.shape[1]
+            call("dpb_transpose_f32", ptr(At), ptr(Hin), n, w_in, w_in, kp, n, s)
+            call("dpb_transpose_f32", ptr(At[:, n:]), ptr(Hdin), n, w_in, w_in, kp, kp - n, s)
+            call("dpb_transpose_f32", ptr(Bt), ptr(bf["Zb"]), n, w_out, w_out, kp, n, s)
+            call("dpb_transpose_f32", ptr(Bt[:, n:]), ptr(bf["Zbd"]), n, w_out, w_out, kp,
+                 kp - n, s)
+            self._tc(At, w_in, kp, Bt, w_out, EPI_STORE, ly["gW"], s)
+        else:
+            self._mm(ly["gW"], Hin, bf["Zb"], None, w_in, w_out, n, 1, 0, 1, s)
+            self._mm(ly["gW"], Hdin, bf["Zbd"], None, w_in, w_out, n, 1, 0, 1, s)
 
     # ----------------------------------------------------------- backward
     def _backward(self, gE, gF, gV):

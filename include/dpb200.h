@@ -700,6 +700,18 @@ DPB_API int dpb_gemm_f64(double* C, const double* A, const double* B, const doub
                          int M, int N, int K, int lda, int ldb, int ldc, int trans_a,
                          int trans_b, int accumulate, dpb_stream_t stream);
 
+/* The same in FP32 (the FP32 training step's layers whose widths the
+ * tensor-core GEMM does not take). */
+DPB_API int dpb_gemm_f32(float* C, const float* A, const float* B, const float* bias, int M,
+                         int N, int K, int lda, int ldb, int ldc, int trans_a, int trans_b,
+                         int accumulate, dpb_stream_t stream);
+/* out[c * ld_out + r] = in[r * ld_in + c] (r < rows, c < cols) and zero for
+ * rows <= r < out_rows: the transposed operands of the tensor-core GEMM in
+ * the training step (weights W^T for x W; activations and adjoints for the
+ * weight gradient x^T g, concatenated along K). */
+DPB_API int dpb_transpose_f32(float* out, const float* in, int rows, int cols, int ld_in,
+                              int ld_out, int out_rows, dpb_stream_t stream);
+
 /* ----------------------------------------- engine-facing list helpers ---- */
 /* copy_coord_gpu (source/lib/include/coord.h:72-85) takes the cell
  * decomposition its caller computed with compute_cell_info
