@@ -16,7 +16,7 @@ import torch
 
 from . import _capi
 from ._capi import call, ptr
-from .model import PipelineTables, SeAParams, _FittingTC
+from .model import DEFAULT_TABLE_DEGREE, PipelineTables, SeAParams, _FittingTC
 
 CELL_MARGIN = 1.0001  # cell edge >= rcut * margin, as the single-frame grid
 
@@ -89,7 +89,8 @@ class BatchEvaluator:
     """Energy [F], force [N, 3] and virial [F, 9] of F frames whose atoms are
     concatenated in frame order (compressed FP32 path, FP64 sums)."""
 
-    def __init__(self, params: SeAParams, frames, device="cuda:0", table_degree: int = 5):
+    def __init__(self, params: SeAParams, frames, device="cuda:0",
+                 table_degree: int = DEFAULT_TABLE_DEGREE):
         cfg = params.cfg
         self.cfg, self.params = cfg, params
         self.dev = dev = torch.device(device)

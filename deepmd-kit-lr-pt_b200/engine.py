@@ -30,7 +30,7 @@ import torch
 
 from . import _capi, ops
 from ._capi import call, ptr
-from .model import PipelineTables, SeAParams, _FittingTC
+from .model import DEFAULT_TABLE_DEGREE, PipelineTables, SeAParams, _FittingTC
 
 
 class ForwardLower:
@@ -39,7 +39,7 @@ class ForwardLower:
     rows hold at most ``max_nbor`` entries."""
 
     def __init__(self, params: SeAParams, nloc_max: int, nall_max: int, max_nbor: int = 512,
-                 device="cuda:0", table_degree: int = 5):
+                 device="cuda:0", table_degree: int = DEFAULT_TABLE_DEGREE):
         cfg = params.cfg
         if not params.tables:
             raise _capi.DPBInvalidArgument("forward_lower needs the compressed model's tables")

@@ -49,7 +49,8 @@ def test_batched_step_same_under_every_shape(mods, restore_knobs):
                  "fit_split_b", "desc_tc"):
         for v, (E, F, V) in _sweep(at, knob, ev.compute).items():
             ev.check()
-            np.testing.assert_allclose(E, E0, rtol=0, atol=1e-5, err_msg=f"{knob}={v}")
+            # FP32 sums in another order: a few 1e-8 of the frame energies
+            np.testing.assert_allclose(E, E0, rtol=3e-7, atol=1e-5, err_msg=f"{knob}={v}")
             np.testing.assert_allclose(F, F0, rtol=0, atol=1e-6, err_msg=f"{knob}={v}")
             np.testing.assert_allclose(V, V0, rtol=0, atol=1e-4, err_msg=f"{knob}={v}")
 
@@ -116,7 +117,8 @@ def test_autotuner_leaves_a_working_step(mods, restore_knobs, tmp_path, monkeypa
 @pytest.mark.parametrize("degree", [5, 3])
 def test_tensor_core_contraction_matches(mods, restore_knobs, degree):
     """desc_tc = 1 (the forward contraction on the tensor cores, 3xTF32)
-    against the CUDA-core contraction: xyz and D to FP32 resolution."""
+    against the CUDA-core contraction: xyz and D to FP32 resolution (3xTF32
+    drops the lo x lo product, 2^-22 relative per product)."""
     mdl, wl, at = mods["model"], mods["workload"], mods["autotune"]
     coord, atype, box = wl.water_frame(5, seed=6)
     params = mdl.prepare(mdl.init_params(mdl.SeAConfig(), seed=1), coord, atype, box)
@@ -127,4 +129,4 @@ def test_tensor_core_contraction_matches(mods, restore_knobs, degree):
         ev.compute(coord)
         out[v] = (ev.xyz.double().cpu().numpy(), ev.D.double().cpu().numpy())
     for a, b in zip(out[1], out[0]):
-        assert np.abs(a - b).max() <= 2e-6 * np.abs(b).max()
+        assert np.abs(a - b).max() <= 5e-6 * np.abs(b).max()
