@@ -777,11 +777,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                 "algorithmic_bytes_per_atom": per_atom_bytes[dom],
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
     # The descriptor kernels are bound by L1/TEX serving the gathers of table
-    # rows (ncu: L1/TEX 69-88% busy, DRAM 5%), not by HBM: a second roof for
+    # rows (ncu: L1/TEX 76-85% busy, DRAM 6-7%), not by HBM: a second roof for
     # the dominant descriptor stage counts the algorithmic gather bytes (one
-    # 6 x M FP32 coefficient row per evaluated slot: the real neighbors plus
-    # one folded padding slot per type section) against the nominal L1 data
-    # rate (128 B/clk/SM at the sampled SM clock).
+    # (degree + 1) x M FP32 coefficient row per evaluated slot: the real
+    # neighbors plus one folded padding slot per type section) against the
+    # nominal L1 data rate (128 B/clk/SM at the sampled SM clock).
     if dom.startswith("descriptor"):
         nl = ev.nlist.view(nloc, cfg.nnei).cpu().numpy()
         sec = cfg.sec
@@ -789,7 +789,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         for t in range(cfg.ntypes):
             real = (nl[:, sec[t]:sec[t + 1]] >= 0).sum(1)
             slots += int(real.sum() + (real < (sec[t + 1] - sec[t])).sum())
-        gather = slots * 6 * cfg.neuron[-1] * 4
+        ncoef = ev.ptab.degree + 1
+        gather = slots * ncoef * cfg.neuron[-1] * 4
         sm_mhz = None
         try:
             sm_mhz = float(subprocess.run(
@@ -799,15 +800,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             pass
         l1_peak = 128 * 148 * (sm_mhz or 1965.0) * 1e6 / 1e12
         roofline["l1_gather"] = {
-            "bytes_per_launch": gather, "slots_evaluated": slots,
+            "bytes_per_launch": gather, "slots_evaluated": slots, "coefficients_per_channel": ncoef,
             "achieved_tbs": gather / (ours[dom] * 1e-3) / 1e12, "nominal_l1_tbs": l1_peak,
             "frac": gather / (ours[dom] * 1e-3) / 1e12 / l1_peak,
-            "note": "table-row gathers through L1/TEX (ncu: L1/TEX 73% busy in k_desc_bwd, "
-                    "89% in k_desc_fwd, DRAM 5-6%); the HBM fraction above is low by "
+            "note": "table-row gathers through L1/TEX (ncu: L1/TEX 76% busy in k_desc_bwd, "
+                    "85% in k_desc_fwd, DRAM 6-7%); the HBM fraction above is low by "
                     "construction"}
     # every stage against its own roof: HBM bytes for the memory stages, the
-    # tensor pipe for the fitting GEMMs (3xTF32: three TF32 products per FP32
-    # multiply-add; TF32 dense peak taken as half the measured BF16 GEMM rate)
+    # tensor pipe for the fitting GEMMs (split TF32: three or four TF32
+    # products per FP32 multiply-add, the fit_terms knob; TF32 dense peak
+    # taken as half the measured BF16 GEMM rate)
     fit = cfg.fitting
     din = cfg.neuron[-1] * cfg.axis_neuron
     mac_fit = 2 * (din * fit[0] + sum(fit[k] * fit[k + 1] for k in range(len(fit) - 1)))
@@ -818,8 +820,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             gbs = per_atom_bytes[k] * nloc / (v * 1e-3) / 1e9
             stage_roofs[k] = {"bound": "hbm", "achieved_gbs": gbs, "frac": gbs / hbm_peak}
         elif k == "fitting":
-            tf = 3 * 2 * mac_fit * nloc / (v * 1e-3) / 1e12
-            stage_roofs[k] = {"bound": "tensor", "achieved_tflops_tf32": tf,
+            capi = importlib.import_module("deepmd_kit_lr_pt_b200._capi")
+            terms = int(capi.lib().dpb_tune_get(b"fit_terms"))
+            tf = terms * 2 * mac_fit * nloc / (v * 1e-3) / 1e12
+            stage_roofs[k] = {"bound": "tensor", "achieved_tflops_tf32": tf, "tf32_terms": terms,
                               "peak_tflops_tf32": tf32_peak, "frac": tf / tf32_peak}
 
     # ---- CPU baseline: the reference CPU path on a bounded sample (rank 0, N=1)

@@ -58,6 +58,7 @@ _SPEC = {"p": P, "i": I, "f": F, "L": LL, "d": D}
 # name -> argument kinds (p pointer, i int, f float, L long long, d double)
 _FUNCS = {
     "dpb_status_check": "pp",
+    "dpb_zero_async": "pLp",
     "dpb_normalize_coord_f64": "pipp",
     "dpb_normalize_coord_f32": "pipp",
     # out_c, out_t, mapping, nall(host), scratch, scratch_bytes, in_c, in_t,
@@ -141,6 +142,9 @@ for _name, _spec in _TRAIN.items():
         _FUNCS[f"{_name}_{_suf}"] = _spec
 _FUNCS.update({"dpb_tune_count": "", "dpb_tune_get": "p", "dpb_tune_options": "ppi",
                "dpb_tune_set": "pi"})
+# the batched step as one launch (description struct: batch.BtStepDesc)
+_FUNCS.update({"dpb_bt_step_create": "pp", "dpb_bt_step_launch": "pp",
+               "dpb_bt_step_destroy": "p"})
 _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),
     "dpb_cell_grid_bytes": ("i", LL),
@@ -151,6 +155,7 @@ _SIZE_QUERIES = {
     "dpb_se_a_build_table_scratch_bytes": ("ii", LL),
     "dpb_copy_coord_cells_scratch_bytes": ("ip", LL),
     "dpb_nlist_rows_scratch_bytes": ("pi", LL),
+    "dpb_bt_step_desc_layout": ("i", LL),
 }
 
 _lib = None

@@ -1,8 +1,14 @@
-"""Many frames of uneven size and species mix evaluated together: every stage
-is one launch over all frames (geometry through per-frame cell lists with
-periodic images, dpb_batch_env_mat_a_f32; the descriptor and the tensor-core
-fitting over the concatenated rows; dpb_batch_force_virial_a and
-dpb_batch_energy per frame), captured as one CUDA graph.
+"""Many frames of uneven size and species mix evaluated together, captured as
+one CUDA graph. Two forms of the step:
+
+* fused (default, knob batch_fused = 1): ONE persistent cooperative launch
+  per step (dpb_bt_step_launch): cells, env rows + descriptor forward, the six
+  fitting GEMMs on the tensor cores, descriptor backward + forces, energies,
+  separated by grid barriers inside the kernel;
+* staged: one launch per stage over all frames (geometry through per-frame
+  cell lists with periodic images, dpb_batch_env_mat_a_f32; the descriptor
+  and the tensor-core fitting over the concatenated rows;
+  dpb_batch_force_virial_a and dpb_batch_energy per frame).
 
 Frames must have orthorhombic boxes whose edges are all at least rcut.
 """
@@ -19,6 +25,28 @@ from ._capi import call, ptr
 from .model import DEFAULT_TABLE_DEGREE, PipelineTables, SeAParams, _FittingTC
 
 CELL_MARGIN = 1.0001  # cell edge >= rcut * margin, as the single-frame grid
+
+_P, _I, _F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+
+
+class GemmLayer(ctypes.Structure):
+    """dpb_gemm_layer of include/dpb200.h."""
+    _fields_ = [("A", _P), ("K", _I), ("b_hi", _P), ("b_lo", _P), ("N", _I), ("mode", _I),
+                ("out0", _P), ("out1", _P), ("aux0", _P), ("aux1", _P), ("bias", _P),
+                ("idt", _P), ("w", _P)]
+
+
+class BtStepDesc(ctypes.Structure):
+    """dpb_bt_step_desc of include/dpb200.h."""
+    _fields_ = [("nframes", _I), ("nrows", _I), ("atom_off", _P), ("cell_off", _P),
+                ("box", _P), ("ncell", _P), ("row_frame", _P), ("coord", _P), ("type", _P),
+                ("cw", _P), ("cell_of", _P), ("cell_start", _P), ("cell_atoms", _P),
+                ("avg", _P), ("std_", _P), ("rcut", _F), ("rcut_smth", _F), ("sec", _P),
+                ("nsec", _I), ("em", _P), ("nlist", _P), ("tables", _P), ("table_info", _P),
+                ("table_degree", _I), ("M", _I), ("naxis", _I), ("drow", _P), ("xyz", _P),
+                ("descrpt", _P), ("d_descrpt", _P), ("net_deriv", _P), ("type_rows", _P),
+                ("ntypes", _I), ("fit", GemmLayer * 6), ("e_rows", _P), ("e_const", _P),
+                ("energy", _P), ("force", _P), ("virial", _P), ("sync", _P), ("status", _P)]
 
 
 class FrameTable:
@@ -90,7 +118,7 @@ class BatchEvaluator:
     concatenated in frame order (compressed FP32 path, FP64 sums)."""
 
     def __init__(self, params: SeAParams, frames, device="cuda:0",
-                 table_degree: int = DEFAULT_TABLE_DEGREE):
+                 table_degree: int = DEFAULT_TABLE_DEGREE, fused: bool | None = None):
         cfg = params.cfg
         self.cfg, self.params = cfg, params
         self.dev = dev = torch.device(device)
@@ -126,7 +154,76 @@ class BatchEvaluator:
         self.e_const = torch.tensor(per_frame, dtype=f64, device=dev)
         self.ptab = PipelineTables(params, dev, table_degree)
         self.graph = None
+        self.plan = None
+        if fused is None:
+            fused = _capi.lib().dpb_tune_get(b"batch_fused") != 0
+        if fused:
+            self._make_plan()
         self.set_coords([fr[0] for fr in frames])
+
+    def _make_plan(self):
+        """The description of the one-launch step (dpb_bt_step_create)."""
+        cfg, ft, fit = self.cfg, self.ft, self.fit
+        M, ax = cfg.neuron[-1], cfg.axis_neuron
+        w, din = fit.width, fit.din
+        self.sync = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        d = BtStepDesc()
+        d.nframes, d.nrows = self.nframes, self.N
+        for name, t in (("atom_off", self.atom_off), ("cell_off", self.cell_off),
+                        ("box", self.box), ("ncell", self.ncell), ("row_frame", self.row_frame),
+                        ("coord", self.coord), ("type", self.type), ("cw", self.cw),
+                        ("cell_of", self.cell_of), ("cell_start", self.cell_start),
+                        ("cell_atoms", self.cell_atoms), ("avg", self.avg), ("std_", self.std),
+                        ("em", self.em), ("nlist", self.nlist), ("drow", self.drow),
+                        ("xyz", self.xyz), ("descrpt", self.D), ("d_descrpt", self.dD),
+                        ("net_deriv", self.net_deriv), ("e_rows", fit.e),
+                        ("e_const", self.e_const), ("energy", self.energy),
+                        ("force", self.force), ("virial", self.virial), ("sync", self.sync),
+                        ("status", self.status)):
+            setattr(d, name, t.data_ptr())
+        d.rcut, d.rcut_smth = cfg.rcut, cfg.rcut_smth
+        self._sec = np.ascontiguousarray(cfg.sec, dtype=np.int32)
+        d.sec, d.nsec = self._sec.ctypes.data, self._sec.size
+        pt = self.ptab
+        d.tables = ctypes.cast(pt.ptrs, _P)
+        d.table_info = pt.info.ctypes.data
+        d.table_degree, d.M, d.naxis = pt.degree, M, ax
+        d.type_rows, d.ntypes = fit.type_rows.ctypes.data, fit.ntypes
+        E = fit
+
+        def layer(A, K, B, N, mode, out0, out1=None, aux0=None, aux1=None, bias=None,
+                  idt=None, wv=None):
+            g = GemmLayer()
+            g.A, g.K, g.N, g.mode = A.data_ptr(), K, N, mode
+            g.b_hi, g.b_lo = ctypes.cast(B[0], _P), ctypes.cast(B[1], _P)
+            for name, t in (("out0", out0), ("out1", out1), ("aux0", aux0), ("aux1", aux1)):
+                setattr(g, name, None if t is None else t.data_ptr())
+            for name, v in (("bias", bias), ("idt", idt), ("w", wv)):
+                setattr(g, name, None if v is None else ctypes.cast(v, _P))
+            return g
+
+        layers = [
+            layer(self.D, din, E.B1f, w, E.EPI_TANH, E.H1, bias=E.b1),
+            layer(E.H1, w, E.B2f, w, E.EPI_RES_DT, E.Y2, E.H2, aux0=E.H1, bias=E.b2, idt=E.d2),
+            layer(E.H2, w, E.B3f, w, E.EPI_LAST, E.G3, aux0=E.H2, bias=E.b3, idt=E.d3,
+                  wv=E.w4),
+            layer(E.G3, w, E.B3b, w, E.EPI_BWD_DT, E.G2, E.g2, aux0=E.Y2, idt=E.d2, wv=E.w4),
+            layer(E.G2, w, E.B2b, w, E.EPI_BWD_RES, E.G1, aux0=E.H1, aux1=E.g2),
+            layer(E.G1, w, E.B1b, din, E.EPI_STORE, self.dD)]
+        for k, g in enumerate(layers):
+            d.fit[k] = g
+        self._desc = d
+        handle = ctypes.c_void_p()
+        call("dpb_bt_step_create", ctypes.byref(handle), ctypes.byref(d))
+        self.plan = handle
+
+    def __del__(self):
+        if getattr(self, "plan", None) is not None and _capi is not None:
+            try:
+                _capi.lib().dpb_bt_step_destroy(self.plan)
+            except Exception:  # noqa: BLE001 - interpreter shutdown
+                pass
+            self.plan = None
 
     def set_coords(self, coords):
         """Host coordinates of every frame (a list, or one [N, 3] array)."""
@@ -137,6 +234,9 @@ class BatchEvaluator:
     # ---- one step over all frames, no host synchronisation
     def step(self):
         cfg, s = self.cfg, torch.cuda.current_stream().cuda_stream
+        if self.plan is not None:
+            call("dpb_bt_step_launch", self.plan, s)
+            return
         M, ax, F, N = cfg.neuron[-1], cfg.axis_neuron, self.nframes, self.N
         call("dpb_batch_env_mat_a_f32", ptr(self.em), ptr(self.nlist), ptr(self.cw),
              ptr(self.cell_of), ptr(self.cell_start), ptr(self.cell_atoms), ptr(self.coord),
@@ -203,6 +303,9 @@ class BatchEvaluator:
         leaves the step captured with the fastest shapes."""
         from . import autotune
 
+        if self.plan is not None:  # the one-launch step has its shapes fixed
+            self.capture()
+            return {}
         cfg = self.cfg
         sig = (f"batch:{self.nframes}f:{self.N}a:deg{self.ptab.degree}:"
                f"sel{'-'.join(map(str, cfg.sel))}:"

@@ -22,8 +22,7 @@
 // Requirements checked on the host: orthorhombic boxes whose edges are all
 // at least rcut (every neighbor then lies in the 27 lattice cells), at most
 // 4096 cells and 600,000 atoms per frame.
-#include "dpb_batch.cuh"
-#include "dpb_envmath.cuh"
+#include "dpb_batch_dev.cuh"
 
 namespace dpb {
 
@@ -33,46 +32,8 @@ k_bt_cells(double* __restrict__ cw, int* __restrict__ cell_of, int* __restrict__
   __shared__ int cnt[BT_MAXCELLS + 1];
   pdl_wait();
   pdl_trigger();
-  const int f = blockIdx.x;
-  const int a0 = fr.atom_off[f], na = fr.atom_off[f + 1] - a0;
-  const int nx = fr.ncell[3 * f], ny = fr.ncell[3 * f + 1], nz = fr.ncell[3 * f + 2];
-  const int nc = nx * ny * nz;
-  const double L[3] = {fr.box[3 * f], fr.box[3 * f + 1], fr.box[3 * f + 2]};
-  for (int c = threadIdx.x; c <= nc; c += blockDim.x) cnt[c] = 0;
-  __syncthreads();
-  for (int k = threadIdx.x; k < na; k += blockDim.x) {
-    double w[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const double x = coord[3 * (size_t)(a0 + k) + d];
-      w[d] = x - floor(x / L[d]) * L[d];
-      if (w[d] >= L[d]) w[d] -= L[d];  // rounding at the upper edge
-      if (w[d] < 0.0) w[d] += L[d];    // and at the lower one
-      cw[3 * (size_t)(a0 + k) + d] = w[d];
-    }
-    const int c = (bt_wrap_cell(w[0], L[0], nx) * ny + bt_wrap_cell(w[1], L[1], ny)) * nz +
-                  bt_wrap_cell(w[2], L[2], nz);
-    cell_of[a0 + k] = c;
-    atomicAdd(&cnt[c + 1], 1);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0)  // exclusive offsets over at most 4096 cells
-    for (int c = 0; c < nc; ++c) cnt[c + 1] += cnt[c];
-  __syncthreads();
-  int* cs = cell_start + fr.cell_off[f];
-  for (int c = threadIdx.x; c <= nc; c += blockDim.x) cs[c] = cnt[c];
-  __syncthreads();
-  for (int k = threadIdx.x; k < na; k += blockDim.x) {
-    const int pos = atomicAdd(&cnt[cell_of[a0 + k]], 1);
-    cell_atoms[a0 + pos] = k;
-  }
+  bt_cells_frame(blockIdx.x, cw, cell_of, cell_start, cell_atoms, coord, fr, cnt);
 }
-
-struct BtEnvSmem {
-  unsigned long long keys[BT_CAP];
-  int row[BT_NMAX];
-  int tcnt[32];
-};
 
 template <typename ET, int WP>
 __global__ void __launch_bounds__(WP * 32)
@@ -87,153 +48,8 @@ k_bt_env(ET* __restrict__ em, int* __restrict__ nlist, const double* __restrict_
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * WP + w;
   if (row >= nrows) return;
-  BtEnvSmem& sm = smem[w];
-  const int f = fr.row_frame[row];
-  const int a0 = fr.atom_off[f];
-  const int i = row - a0;
-  const int nx = fr.ncell[3 * f], ny = fr.ncell[3 * f + 1], nz = fr.ncell[3 * f + 2];
-  const double L[3] = {fr.box[3 * f], fr.box[3 * f + 1], fr.box[3 * f + 2]};
-  const double* fc = cw + 3 * (size_t)a0;
-  const int* ft = type + a0;
-  const int* cs = cell_start + fr.cell_off[f];
-  const int* ca = cell_atoms + a0;
-  const int nnei = sec.nnei, ntypes = sec.ntypes;
-  int ti = ft[i];
-  if (ti < 0 || ti >= ntypes) {
-    if (lane == 0) atomicOr(status, ST_TYPE_RANGE);
-    ti = -1;
-  }
-  const double xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
-  const float fxi[3] = {(float)xi[0], (float)xi[1], (float)xi[2]};
-  const float rc2f = rcut * rcut;
-  const double rc2 = (double)rc2f;
-  for (int t = lane; t < 32; t += 32) sm.tcnt[t] = 0;
-  for (int jj = lane; jj < nnei; jj += 32) sm.row[jj] = -1;
-  __syncwarp();
-  int count = 0;
-  const int ci = cell_of[row];
-  const int cz = ci % nz, cy = (ci / nz) % ny, cx = ci / (nz * ny);
-  // lane L < 27 owns lattice cell (cx, cy, cz) + (L / 9, L / 3 % 3, L % 3) - 1:
-  // its stored (wrapped) cell's atom range and its image code; the 27 ranges
-  // are then walked as one flat list in full batches of 32, the next batch's
-  // atom indices requested before the current batch is tested
-  int cb = 0, cn = 0, ccode = 13;
-  if (lane < 27) {
-    int X = cx + lane / 9 - 1, Y = cy + (lane / 3) % 3 - 1, Z = cz + lane % 3 - 1;
-    const int sx = X < 0 ? -1 : (X >= nx ? 1 : 0);
-    const int sy = Y < 0 ? -1 : (Y >= ny ? 1 : 0);
-    const int sz = Z < 0 ? -1 : (Z >= nz ? 1 : 0);
-    X -= sx * nx;
-    Y -= sy * ny;
-    Z -= sz * nz;
-    ccode = (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1);
-    const int c = (X * ny + Y) * nz + Z;
-    cb = cs[c];
-    cn = cs[c + 1] - cb;
-  }
-  int incl = cn;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const int excl = incl - cn;
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
-  // atom (-1 past the end) and image code of flat candidate fl
-  auto cand_of = [&](int fl, int& code) -> int {
-    int lo = 0;
-#pragma unroll
-    for (int st = 16; st > 0; st >>= 1) {
-      const int ev = __shfl_sync(0xffffffffu, excl, lo + st);
-      if (ev <= fl) lo += st;
-    }
-    const int base_c = __shfl_sync(0xffffffffu, cb, lo);
-    const int start_c = __shfl_sync(0xffffffffu, excl, lo);
-    code = __shfl_sync(0xffffffffu, ccode, lo);
-    return fl < total ? ca[base_c + (fl - start_c)] : -1;
-  };
-  int coden = 13;
-  int jn = cand_of(lane, coden);
-  for (int base = 0; base < total; base += 32) {
-    const int j = jn, code = coden;
-    jn = cand_of(base + 32 + lane, coden);
-    bool ok = false;
-    unsigned long long key = 0;
-    if (j >= 0) {
-      const int tj = ft[j];
-      if (tj >= 0 && tj < ntypes && ti >= 0 && !(j == i && code == 13)) {
-        const int sx = code / 9 - 1, sy = (code / 3) % 3 - 1, sz = code % 3 - 1;
-        const double sh[3] = {sx * L[0], sy * L[1], sz * L[2]};
-        // the image's position, then the single-frame path's two tests
-        const double g0 = fc[3 * j] + sh[0], g1 = fc[3 * j + 1] + sh[1],
-                     g2 = fc[3 * j + 2] + sh[2];
-        const double d0 = sub_rn(xi[0], g0), d1 = sub_rn(xi[1], g1), d2 = sub_rn(xi[2], g2);
-        if (dot3_rn(d0, d1, d2) < rc2) {
-          const float e0 = sub_rn((float)g0, fxi[0]), e1 = sub_rn((float)g1, fxi[1]),
-                      e2 = sub_rn((float)g2, fxi[2]);
-          const float r2 = dot3_rn(e0, e1, e2);
-          if (r2 <= rc2f) {
-            ok = true;
-            key = ((unsigned long long)tj << 56) |
-                  ((unsigned long long)__float_as_uint(r2) << 24) |
-                  (unsigned long long)(j * 27 + code);
-          }
-        }
-      }
-    }
-    const unsigned bal = __ballot_sync(0xffffffffu, ok);
-    if (ok) {
-      const int pos = count + __popc(bal & bt_lanemask_lt());
-      if (pos < BT_CAP) {
-        sm.keys[pos] = key;
-        atomicAdd(&sm.tcnt[key >> 56], 1);
-      }
-    }
-    count += __popc(bal);
-  }
-  __syncwarp();
-  if (count > BT_CAP && lane == 0) atomicOr(status, ST_NLIST_CAPACITY);
-  const int n = count < BT_CAP ? count : BT_CAP;
-  int tstart = lane < ntypes ? sm.tcnt[lane] : 0;
-  {
-    int x = tstart;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    tstart = x - tstart;
-  }
-  for (int q = 0; q * 32 < n; ++q) {
-    const int kk = q * 32 + lane;
-    const unsigned long long own = kk < n ? sm.keys[kk] : ~0ull;
-    int r = 0;
-    for (int p = 0; p < n; ++p) r += sm.keys[p] < own ? 1 : 0;
-    const int t = (int)(own >> 56) & 31;
-    const int ts = __shfl_sync(0xffffffffu, tstart, t);
-    if (kk < n) {
-      const int rr = r - ts;
-      if (rr < sec.sec[t + 1] - sec.sec[t]) sm.row[sec.sec[t] + rr] = (int)(own & 0xFFFFFFull);
-      else atomicOr(status, ST_SEL_OVERFLOW);
-    }
-  }
-  __syncwarp();
-  const ET* av = avg + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
-  const ET* sd = std_ + (size_t)(ti < 0 ? 0 : ti) * nnei * 4;
-  for (int jj = lane; jj < nnei; jj += 32) {
-    const int packed = sm.row[jj];
-    nlist[(size_t)row * nnei + jj] = packed;
-    ET v[4] = {(ET)0, (ET)0, (ET)0, (ET)0};
-    if (packed >= 0) {
-      ET r[3];
-      bt_rij<ET>(r, fc, packed, xi, L);
-      env_row<ET>(r, rcut_smth, rcut, v, nullptr);
-    }
-    ET* e = em + ((size_t)row * nnei + jj) * 4;
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      e[k] = ti >= 0 ? (v[k] - av[jj * 4 + k]) / sd[jj * 4 + k] : (ET)0;
-  }
+  bt_env_row<ET>(row, lane, smem[w], em, nlist, cw, type, cell_of, cell_start, cell_atoms, avg,
+                 std_, fr, sec, rcut, rcut_smth, status);
 }
 
 template <typename ET, int WP>
@@ -248,61 +64,8 @@ k_bt_force(double* __restrict__ force, double* __restrict__ virial,
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * WP + w;
   if (row >= nrows) return;
-  const int f = fr.row_frame[row];
-  const int a0 = fr.atom_off[f];
-  const int i = row - a0;
-  const int ti = type[row];
-  if (ti < 0 || ti >= ntypes) return;  // env derivative rows are zero
-  const double L[3] = {fr.box[3 * f], fr.box[3 * f + 1], fr.box[3 * f + 2]};
-  const double* fc = cw + 3 * (size_t)a0;
-  const double xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
-  const ET* sd = std_ + (size_t)ti * nnei * 4;
-  const ET* ndr = nd + (size_t)row * nnei * 4;
-  double c0 = 0., c1 = 0., c2 = 0.;
-  double vs[9];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) vs[k] = 0.;
-  for (int jj = lane; jj < nnei; jj += 32) {
-    const int packed = nlist[(size_t)row * nnei + jj];
-    if (packed < 0) continue;
-    const int j = packed / 27;
-    ET r[3];
-    bt_rij<ET>(r, fc, packed, xi, L);
-    ET v[4], gd[12];
-    env_row<ET>(r, rcut_smth, rcut, v, gd);
-    ET p[3] = {(ET)0, (ET)0, (ET)0};
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const ET n = ndr[jj * 4 + a];
-      const ET sa = sd[jj * 4 + a];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) p[d] += n * (gd[a * 3 + d] / sa);
-    }
-    const double q[3] = {(double)p[0], (double)p[1], (double)p[2]};
-    c0 += q[0];
-    c1 += q[1];
-    c2 += q[2];
-    atomicAdd(&force[3 * (size_t)(a0 + j) + 0], q[0]);
-    atomicAdd(&force[3 * (size_t)(a0 + j) + 1], q[1]);
-    atomicAdd(&force[3 * (size_t)(a0 + j) + 2], q[2]);
-#pragma unroll
-    for (int d0 = 0; d0 < 3; ++d0)
-#pragma unroll
-      for (int d1 = 0; d1 < 3; ++d1) vs[d0 * 3 + d1] += q[d0] * (double)r[d1];
-  }
-  c0 = warp_sum(c0);
-  c1 = warp_sum(c1);
-  c2 = warp_sum(c2);
-  if (lane == 0) {
-    atomicAdd(&force[3 * (size_t)row + 0], -c0);
-    atomicAdd(&force[3 * (size_t)row + 1], -c1);
-    atomicAdd(&force[3 * (size_t)row + 2], -c2);
-  }
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    const double t = warp_sum(vs[k]);
-    if (lane == 0) atomicAdd(&virial[9 * (size_t)f + k], t);
-  }
+  bt_force_row<ET>(row, lane, force, virial, nd, cw, type, std_, nlist, fr, ntypes, nnei, rcut,
+                   rcut_smth);
 }
 
 template <typename ET>
@@ -312,18 +75,7 @@ k_bt_energy(double* __restrict__ energy, const ET* __restrict__ e_rows,
   __shared__ double part[8];
   pdl_wait();
   pdl_trigger();
-  const int f = blockIdx.x;
-  double s = 0.;
-  for (int r = fr.atom_off[f] + threadIdx.x; r < fr.atom_off[f + 1]; r += blockDim.x)
-    s += (double)e_rows[drow[r]];
-  s = warp_sum(s);
-  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = e_const[f];
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
-    energy[f] = t;
-  }
+  bt_energy_frame<ET>(blockIdx.x, energy, e_rows, drow, e_const, fr, part);
 }
 
 }  // namespace dpb

@@ -28,6 +28,16 @@ const char* dpb_last_error(void) { return dpb::g_msg; }
 
 int dpb_abi_version(void) { return 1; }
 
+int dpb_zero_async(void* dst, long long bytes, dpb_stream_t stream) {
+  if (bytes == 0) return DPB_OK;
+  if (dst == nullptr || bytes < 0) {
+    dpb::set_error("dpb_zero_async: null destination or negative size (%lld bytes)", bytes);
+    return DPB_ERR_INVALID;
+  }
+  DPB_CUDA(cudaMemsetAsync(dst, 0, (size_t)bytes, dpb::as_stream(stream)), "dpb_zero_async");
+  return DPB_OK;
+}
+
 int dpb_status_check(const int* status, dpb_stream_t stream) {
   if (status == nullptr) return DPB_OK;
   int h = 0;

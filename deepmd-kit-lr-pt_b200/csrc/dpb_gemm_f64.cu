@@ -122,6 +122,109 @@ k_gemm_f64(T* __restrict__ C, const T* __restrict__ A, const T* __restrict__ B,
   }
 }
 
+// The large-M form: 128 x 64 tiles, K in steps of 8, each thread a block of
+// 8 rows (ty * 4 + i and 64 + ty * 4 + i) by 4 columns, so every k step
+// reads 6 shared-memory vectors for 32 FMAs (the 64 x 64 form above: 4 for
+// 16).
+constexpr int GL_M = 128, GL_N = 64, GL_K = 8;
+
+template <bool TA, bool TB, typename T>
+__global__ void __launch_bounds__(GB_T)
+k_gemm_big(T* __restrict__ C, const T* __restrict__ A, const T* __restrict__ B,
+           const T* __restrict__ bias, int M, int N, int K, int lda, int ldb, int ldc,
+           int accumulate) {
+  using T2 = typename Vec2<T>::type;
+  __shared__ __align__(16) T As[2][GL_K][GL_M + 2];
+  __shared__ __align__(16) T Bs[2][GL_K][GL_N + 2];
+  pdl_wait();
+  const int tid = threadIdx.x;
+  const int m0 = blockIdx.y * GL_M, n0 = blockIdx.x * GL_N;
+  const int tx = tid & 15, ty = tid >> 4;
+  T ra[4], rb[2];
+  auto a_at = [&](int q, int& r, int& k) {
+    if (TA) { r = q & 127; k = q >> 7; } else { k = q & 7; r = q >> 3; }
+  };
+  auto b_at = [&](int q, int& c, int& k) {
+    if (TB) { k = q & 7; c = q >> 3; } else { c = q & 63; k = q >> 6; }
+  };
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int r, k;
+      a_at(tid + GB_T * j, r, k);
+      ra[j] = ld_op<TA, T>(A, m0 + r, k0 + k, M, K, lda);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      int c, k;
+      b_at(tid + GB_T * j, c, k);
+      rb[j] = ld_op<TB, T>(B, k0 + k, n0 + c, K, N, ldb);
+    }
+  };
+  auto stash = [&](int buf) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int r, k;
+      a_at(tid + GB_T * j, r, k);
+      As[buf][k][r] = ra[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      int c, k;
+      b_at(tid + GB_T * j, c, k);
+      Bs[buf][k][c] = rb[j];
+    }
+  };
+  T acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = (T)0;
+  const int nk = (K + GL_K - 1) / GL_K;
+  fetch(0);
+  stash(0);
+  __syncthreads();
+  for (int t = 0; t < nk; ++t) {
+    const int buf = t & 1;
+    if (t + 1 < nk) fetch((t + 1) * GL_K);
+#pragma unroll
+    for (int k = 0; k < GL_K; ++k) {
+      const T2 a0 = *reinterpret_cast<const T2*>(&As[buf][k][ty * 4]);
+      const T2 a1 = *reinterpret_cast<const T2*>(&As[buf][k][ty * 4 + 2]);
+      const T2 a2 = *reinterpret_cast<const T2*>(&As[buf][k][64 + ty * 4]);
+      const T2 a3 = *reinterpret_cast<const T2*>(&As[buf][k][64 + ty * 4 + 2]);
+      const T2 b0 = *reinterpret_cast<const T2*>(&Bs[buf][k][tx * 4]);
+      const T2 b1 = *reinterpret_cast<const T2*>(&Bs[buf][k][tx * 4 + 2]);
+      const T a[8] = {a0.x, a0.y, a1.x, a1.y, a2.x, a2.y, a3.x, a3.y};
+      const T b[4] = {b0.x, b0.y, b1.x, b1.y};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    if (t + 1 < nk) {
+      stash(buf ^ 1);
+      __syncthreads();
+    }
+  }
+  pdl_trigger();
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = n0 + tx * 4 + j;
+      if (c >= N) continue;
+      T v = acc[i][j];
+      if (bias) v += bias[c];
+      T* p = C + (size_t)r * ldc + c;
+      if (accumulate) v += *p;
+      *p = v;
+    }
+  }
+}
+
 }  // namespace
 }  // namespace dpb
 
@@ -141,13 +244,34 @@ static int gemm(const char* what, T* C, const T* A, const T* B, const T* bias, i
     return DPB_ERR_INVALID;
   }
   if (M == 0 || N == 0) return DPB_OK;
+  cudaStream_t st = as_stream(stream);
+  const int ta = trans_a != 0, tb = trans_b != 0;
+  if (M >= GL_M && tune_value("gemm_simt_big", 1)) {
+    const dim3 grid((N + GL_N - 1) / GL_N, (M + GL_M - 1) / GL_M);
+    if (grid.y > 65535) {
+      set_error("%s: M=%d needs more than 65535 row tiles", what, M);
+      return DPB_ERR_INVALID;
+    }
+    if (!ta && !tb)
+      launch_pdl(k_gemm_big<false, false, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
+                 lda, ldb, ldc, accumulate);
+    else if (!ta && tb)
+      launch_pdl(k_gemm_big<false, true, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
+                 lda, ldb, ldc, accumulate);
+    else if (ta && !tb)
+      launch_pdl(k_gemm_big<true, false, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
+                 lda, ldb, ldc, accumulate);
+    else
+      launch_pdl(k_gemm_big<true, true, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
+                 lda, ldb, ldc, accumulate);
+    DPB_CHECK_LAUNCH(what);
+    return DPB_OK;
+  }
   const dim3 grid((N + GB_N - 1) / GB_N, (M + GB_M - 1) / GB_M);
   if (grid.y > 65535) {
     set_error("%s: M=%d needs more than 65535 row tiles", what, M);
     return DPB_ERR_INVALID;
   }
-  cudaStream_t st = as_stream(stream);
-  const int ta = trans_a != 0, tb = trans_b != 0;
   if (!ta && !tb)
     launch_pdl(k_gemm_f64<false, false, T>, grid, dim3(GB_T), 0, st, C, A, B, bias, M, N, K,
                lda, ldb, ldc, accumulate);

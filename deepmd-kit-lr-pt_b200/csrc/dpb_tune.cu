@@ -31,8 +31,26 @@ static Knob g_knobs[] = {
     // weight bytes; 14% slower on the 12,288-atom water step: the GEMMs are
     // not limited by the weight bytes)
     {"fit_split_b", 0, 2, {0, 1}},
+    // TF32 products per k step of the fitting GEMM: 3 (Ah Bh + Al Bh + Ah Bl)
+    // or 4 (with Al Bl, 2^-22 of a product: measured to change no output
+    // beyond FP32 accumulation noise, at 4% more fitting time)
+    {"fit_terms", 3, 2, {3, 4}},
+    // k-blocks (32 wide) per accumulator chunk of the fitting GEMM, 0 for one
+    // accumulator per output tile: the tensor cores' FP32 accumulation loses
+    // up to an ulp of the running sum per instruction, always in the same
+    // direction, so long sums over rows that are alike drift
+    {"fit_kchunk", 4, 5, {0, 1, 2, 4, 8}},
+    // order inside a chunk: 1 the cross products of all its k-blocks first
+    // (the chunk's stages stay resident until its Ah Bh products are issued),
+    // 0 k-block by k-block
+    {"fit_kchunk_cross_first", 1, 2, {0, 1}},
+    // chunked accumulation only for K at least this (shorter sums drift less)
+    {"fit_kchunk_min_k", 0, 2, {0, 512}},
     // warps (one center atom each) per CTA of the batched env / force kernels
     {"batch_atoms_per_cta", 4, 3, {2, 4, 8}},
+    // batched-frames step: 1 one persistent cooperative launch
+    // (dpb_bt_step_launch), 0 one launch per stage
+    {"batch_fused", 0, 2, {0, 1}},
     // neighbor rows per group in the FP32 training kernels
     {"train_rows_per_group", 8, 2, {4, 8}},
     // most warps per CTA of the training kernels (fewer when shared memory
@@ -48,6 +66,10 @@ static Knob g_knobs[] = {
     // so 1 is a tested option the autotuner does not try
     // (the kernel is bound by the table gathers, which 1 makes scalar)
     {"desc_tc", 0, 2, {0, 1}},
+    // SIMT GEMMs (FP64 plain path and training, FP32 odd widths): 1 the
+    // 128 x 64 tile with 8 x 4 outputs per thread where M >= 128, 0 the
+    // 64 x 64 tile with 4 x 4 outputs
+    {"gemm_simt_big", 1, 2, {0, 1}},
     // programmatic dependent launch between the kernels of a step: 1 on
     // (each kernel's launch overlaps the previous kernel's tail), 0 off
     {"pdl", 1, 2, {0, 1}},

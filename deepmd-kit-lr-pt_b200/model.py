@@ -316,20 +316,27 @@ class _FittingF64:
                      s)
 
 
+def _tf32_rna(w: np.ndarray) -> np.ndarray:
+    """Round-to-nearest (ties away) TF32 value of FP32 w, as
+    cvt.rna.tf32.f32 computes it (finite inputs)."""
+    u = np.ascontiguousarray(w, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return ((u + 0x1000) & 0xFFFFE000).astype(np.uint32).view(np.float32)
+
+
 def tf32_split(w: np.ndarray):
-    """(hi, lo) FP32 arrays with hi the round-to-nearest (ties away) TF32 value
-    of w, as cvt.rna.tf32.f32 computes it, and lo = w - hi."""
+    """(hi, lo) FP32 arrays holding TF32 values: hi the TF32 rounding of w,
+    lo the TF32 rounding of w - hi (hi + lo = w to 2^-24 relative)."""
     w = np.ascontiguousarray(w, dtype=np.float32)
-    u = w.view(np.uint32).astype(np.uint64)
-    hi = ((u + 0x1000) & 0xFFFFE000).astype(np.uint32).view(np.float32)
-    lo = (w - hi).astype(np.float32)
+    hi = _tf32_rna(w)
+    lo = _tf32_rna((w - hi).astype(np.float32))
     return hi, lo
 
 
 class _FittingTC:
     """Per-type fitting networks, forward and input-gradient, as six fused
-    3xTF32 tensor-core GEMMs (dpb_gemm_tf32x3_f32). Rows of the descriptor are
-    grouped by center type; ``type_rows`` gives the group sizes."""
+    split-TF32 tensor-core GEMMs (dpb_gemm_tf32x3_f32, FP32 accumulation in
+    chunks). Rows of the descriptor are grouped by center type;
+    ``type_rows`` gives the group sizes."""
 
     EPI_STORE, EPI_TANH, EPI_RES_DT, EPI_LAST, EPI_BWD_DT, EPI_BWD_RES = range(6)
 
@@ -654,7 +661,7 @@ class SeAEvaluator:
         if self.mode == "compressed":
             # force / virial accumulators, zeroed here where no kernel boundary
             # of the step is delayed by it
-            self.results[1:].zero_()
+            call("dpb_zero_async", ptr(self.results) + 8, 8 * (self.results.numel() - 1), s)
         if self.skin > 0:
             if not self.built:
                 raise _capi.DPBInvalidArgument("call rebuild() before the first step")

@@ -45,6 +45,11 @@ DPB_API int dpb_abi_version(void);
  * `stream` (synchronises the stream) and maps it to a dpb_status. */
 DPB_API int dpb_status_check(const int* status, dpb_stream_t stream);
 
+/* Sets `bytes` bytes at device address `dst` to zero, ordered on `stream`
+ * (a memset node when the stream is being captured into a CUDA graph). Used
+ * for the force / virial accumulators at the start of a step. */
+DPB_API int dpb_zero_async(void* dst, long long bytes, dpb_stream_t stream);
+
 /* ---------------------------------------------------------- coordinates -- */
 
 /* normalize_coord_gpu (source/lib/include/coord.h:56-59; coord.cu:263-282).
@@ -384,6 +389,93 @@ DPB_API int dpb_batch_energy(double* energy, const float* e_rows, const int* dro
 DPB_API int dpb_batch_energy_f64(double* energy, const double* e_rows, const int* drow,
                                  const double* e_const, const int* atom_off, int nframes,
                                  dpb_stream_t stream);
+
+/* ------------------------------------- batched step as one persistent launch -- */
+
+/* One fitting GEMM of the step (the arguments of dpb_gemm_tf32x3_f32 that
+ * differ per layer). b_hi / b_lo / bias / idt / w are host arrays of ntypes
+ * device pointers (bias / idt / w may be NULL); b_lo is required. */
+typedef struct {
+  const float* A;
+  int K;
+  const float* const* b_hi;
+  const float* const* b_lo;
+  int N;
+  int mode;
+  float* out0;
+  float* out1;
+  const float* aux0;
+  const float* aux1;
+  const float* const* bias;
+  const float* const* idt;
+  const float* const* w;
+} dpb_gemm_layer;
+
+/* Everything one batched-frames step touches (device buffers unless noted):
+ * the frame table and geometry scratch of dpb_batch_env_mat_a_f32, the
+ * descriptor tables and buffers of dpb_se_a_descriptor_{fwd,bwd}[_cubic]_f32
+ * (tables: host array of device pointers, table_info: host, 6 per type,
+ * table_degree 5 or 3), the six fitting GEMMs in the order layer 1..3
+ * forward (epilogues 1, 2, 3) and layer 3..1 backward (4, 5, 0), the
+ * per-frame energy constants and the outputs. sync: one device word for the
+ * grid barriers (zeroed by each launch); status: the device status word. */
+typedef struct {
+  int nframes;
+  int nrows;
+  const int* atom_off;
+  const int* cell_off;
+  const double* box;
+  const int* ncell;
+  const int* row_frame;
+  const double* coord;
+  const int* type;
+  double* cw;
+  int* cell_of;
+  int* cell_start;
+  int* cell_atoms;
+  const float* avg;
+  const float* std_;
+  float rcut;
+  float rcut_smth;
+  const int* sec;
+  int nsec;
+  float* em;
+  int* nlist;
+  const float* const* tables;
+  const float* table_info;
+  int table_degree;
+  int M;
+  int naxis;
+  const int* drow;
+  float* xyz;
+  float* descrpt;
+  float* d_descrpt;
+  float* net_deriv;
+  const int* type_rows;
+  int ntypes;
+  dpb_gemm_layer fit[6];
+  float* e_rows;
+  const double* e_const;
+  double* energy;
+  double* force;
+  double* virial;
+  unsigned* sync;
+  int* status;
+} dpb_bt_step_desc;
+
+/* Checks the description and prepares the launch (tensor maps of the six
+ * GEMMs, table descriptors); *plan is freed by dpb_bt_step_destroy. The
+ * buffers must stay allocated while the plan is used. */
+DPB_API int dpb_bt_step_create(void** plan, const dpb_bt_step_desc* desc);
+/* One step: env, descriptor, fitting, descriptor backward, forces, virials
+ * and energies of every frame in ONE cooperative launch (one CTA per SM),
+ * preceded by a 4-byte memset of the barrier word. */
+DPB_API int dpb_bt_step_launch(const void* plan, dpb_stream_t stream);
+DPB_API void dpb_bt_step_destroy(void* plan);
+/* Layout of the description structs as this library was compiled: which = 0
+ * sizeof(dpb_bt_step_desc), 1 offsetof(fit), 2 offsetof(status),
+ * 3 sizeof(dpb_gemm_layer), 4 offsetof(dpb_gemm_layer, w); -1 otherwise. */
+DPB_API long long dpb_bt_step_desc_layout(int which);
 
 /* FP64 compression table of one se_a embedding net, built on the device
  * (the reference builds it on the host: deepmd/utils/tabulate.py:275-371).

@@ -1,7 +1,9 @@
 """Batched uneven frames (water at 1.0 g/cm^3 and FCC Cu with vacancies,
 3-species model O/H/Cu, sel [46, 92, 60]) evaluated together against the
 single-frame evaluator frame by frame (ghost copies, its own cell grid): the
-same energy, force and virial to FP32 precision."""
+same energy, force and virial to FP32 precision; in both forms of the step
+(one persistent launch, one launch per stage), and the two forms against
+each other."""
 
 import importlib
 
@@ -25,9 +27,11 @@ def setup(dpb):
     return mdl, bt, frames, params
 
 
-def test_batch_matches_single_frames(setup):
+@pytest.mark.parametrize("fused", [True, False])
+def test_batch_matches_single_frames(setup, fused):
     mdl, bt, frames, params = setup
-    ev = bt.BatchEvaluator(params, frames)
+    ev = bt.BatchEvaluator(params, frames, fused=fused)
+    assert (ev.plan is not None) == fused
     E, F, V = ev.compute()
     ev.check()
     for f, (coord, atype, box) in enumerate(frames):
@@ -39,9 +43,10 @@ def test_batch_matches_single_frames(setup):
         assert np.abs(V[f] - v0).max() < 1e-4 * max(1.0, np.abs(v0).max()), f
 
 
-def test_batch_graph_replay_repeats(setup):
+@pytest.mark.parametrize("fused", [True, False])
+def test_batch_graph_replay_repeats(setup, fused):
     mdl, bt, frames, params = setup
-    ev = bt.BatchEvaluator(params, frames)
+    ev = bt.BatchEvaluator(params, frames, fused=fused)
     E0, F0, V0 = ev.compute()
     ev.capture()
     for _ in range(2):
@@ -51,6 +56,29 @@ def test_batch_graph_replay_repeats(setup):
         np.testing.assert_allclose(E1, E0, rtol=0, atol=1e-5)
         np.testing.assert_allclose(F1, F0, rtol=0, atol=1e-9)
         np.testing.assert_allclose(V1, V0, rtol=0, atol=1e-7)
+
+
+def test_fused_step_equals_staged_step(setup):
+    """The one-launch step and the per-stage launches run the same device
+    bodies: neighbor lists, env rows and descriptors identical; energies,
+    forces and virials equal up to the order of the atomic sums."""
+    mdl, bt, frames, params = setup
+    a = bt.BatchEvaluator(params, frames, fused=True)
+    b = bt.BatchEvaluator(params, frames, fused=False)
+    Ea, Fa, Va = a.compute()
+    Eb, Fb, Vb = b.compute()
+    a.check()
+    b.check()
+    assert np.array_equal(a.nlist.cpu().numpy(), b.nlist.cpu().numpy())
+    assert np.array_equal(a.em.cpu().numpy(), b.em.cpu().numpy())
+    assert np.array_equal(a.D.cpu().numpy(), b.D.cpu().numpy())
+    np.testing.assert_allclose(Ea, Eb, rtol=0, atol=1e-5)
+    np.testing.assert_allclose(Fa, Fb, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(Va, Vb, rtol=0, atol=1e-7)
+    # a second step of the fused form (accumulators re-zeroed in the launch)
+    Ea2, Fa2, _ = a.compute()
+    np.testing.assert_allclose(Ea2, Ea, rtol=0, atol=1e-5)
+    np.testing.assert_allclose(Fa2, Fa, rtol=0, atol=1e-9)
 
 
 def test_batch_rejects_small_or_skewed_boxes(setup, dpb):

@@ -146,3 +146,18 @@ def test_noalloc_size_limit_host_side(dpb):
     code = lib.dpb_build_nlist_noalloc_f64(None, None, None, None, None, 16, nmax + 1, 64,
                                            ctypes.c_float(6.0), 1, None, None)
     assert code == 2 and "built-in array" in cap.last_error()
+
+
+def test_step_description_layout_matches_ctypes(dpb):
+    """The ctypes mirrors of dpb_bt_step_desc / dpb_gemm_layer have the
+    layout the library was compiled with."""
+    import ctypes
+
+    from deepmd_kit_lr_pt_b200 import batch
+
+    lib = dpb._capi.lib()
+    assert lib.dpb_bt_step_desc_layout(0) == ctypes.sizeof(batch.BtStepDesc)
+    assert lib.dpb_bt_step_desc_layout(1) == batch.BtStepDesc.fit.offset
+    assert lib.dpb_bt_step_desc_layout(2) == batch.BtStepDesc.status.offset
+    assert lib.dpb_bt_step_desc_layout(3) == ctypes.sizeof(batch.GemmLayer)
+    assert lib.dpb_bt_step_desc_layout(4) == batch.GemmLayer.w.offset

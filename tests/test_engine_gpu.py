@@ -71,7 +71,10 @@ def test_forward_lower_matches_evaluator_and_oracle(dpb, mods, case):
     np.add.at(F, mx.cpu().numpy(), Fext.cpu().numpy())
     V = V.cpu().numpy()
     e1, f1, v1 = mdl.SeAEvaluator(params, atype, box, mode="compressed").compute(coord)
-    assert abs(E - e1) <= 1e-9 * max(1.0, abs(e1))
+    # the same kernels; each row's FP32 energy gets one partial sum per
+    # column tile of the output layer, added atomically in whatever order the
+    # tiles finish, so the totals agree to FP32 rounding per row
+    assert abs(E - e1) <= 1e-8 * nloc
     np.testing.assert_allclose(F, f1, atol=1e-9, rtol=0)
     np.testing.assert_allclose(V, v1, atol=1e-8 * max(1.0, np.abs(v1).max()), rtol=0)
     e0, f0, v0 = model_ref.evaluate(oracle.ref() or oracle.port(), params, coord, atype, box,

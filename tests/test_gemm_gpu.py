@@ -1,5 +1,6 @@
-"""3xTF32 tensor-core GEMM (dpb_gemm_tf32x3_f32) and the fitting networks built
-on it, against FP64 references. 3xTF32 keeps FP32-level accuracy: relative
+"""Split-TF32 tensor-core GEMM (dpb_gemm_tf32x3_f32: 3 TF32 products per k
+step by default, 4 with the fit_terms knob) and the fitting networks built
+on it, against FP64 references. The split keeps FP32-level accuracy: relative
 errors of a few 1e-6 on these sizes; the bar is 2e-5 relative to the output
 scale (the FP32 bar of the reference tests is 1e-5 absolute on O(1) values)."""
 
@@ -197,6 +198,17 @@ def test_gemm_f64_matches_fp64_reference(dpb, M, N, K, ta, tb):
     """dpb_gemm_f64 (FP64 plain path, FP64 training) against an FP64 matmul:
     every transpose combination, ragged edges, the bias and accumulate
     epilogues; the FP64 bar 1e-12 relative to the output scale."""
+    from deepmd_kit_lr_pt_b200 import autotune
+
+    for big in (1, 0):  # the 128 x 64 and the 64 x 64 tile forms
+        autotune.set_knob("gemm_simt_big", big)
+        try:
+            _check_gemm_f64(dpb, M, N, K, ta, tb)
+        finally:
+            autotune.set_knob("gemm_simt_big", 1)
+
+
+def _check_gemm_f64(dpb, M, N, K, ta, tb):
     rng = np.random.default_rng(M * 7 + N * 3 + K + 11 * ta + 5 * tb)
     A = rng.normal(size=(K, M) if ta else (M, K))
     B = rng.normal(size=(N, K) if tb else (K, N))
@@ -240,3 +252,78 @@ def test_fitting_f64_matches_torch_autograd(dpb, mdl):
                                rtol=0)
     np.testing.assert_allclose(dD.cpu().numpy(), torch.cat([g0, g1]).cpu().numpy(), atol=1e-12,
                                rtol=0)
+
+
+@pytest.mark.parametrize("split_in_kernel", [False, True])
+def test_gemm_alike_rows_fp32_resolution(dpb, mdl, split_in_kernel):
+    """Rows that are all alike (the atoms of a crystal see nearly the same
+    descriptor). The tensor cores' FP32 accumulation loses up to an ulp of
+    the running sum per instruction, always in the same direction, so over
+    K = 1600 the outputs drift (about 1.5e-5 of the output scale with one
+    accumulator per tile). With chunked accumulation (fresh accumulator every
+    kchunk k-blocks, cross products first, chunk sums added on the CUDA
+    cores; the default) the error is at FP32-GEMM level: below 2e-6, at
+    least 5x smaller than with one accumulator."""
+    from deepmd_kit_lr_pt_b200 import autotune
+
+    rng = np.random.default_rng(41)
+    K, N = 1600, 240
+    row = (rng.normal(size=K) * 0.05 + 0.3).astype(np.float32)
+    A = np.tile(row, (256, 1)) + (rng.normal(size=(256, K)) * 1e-4).astype(np.float32)
+    A = A.astype(np.float32)
+    Bs = [(rng.normal(size=(N, K)) / np.sqrt(K)).astype(np.float32)]
+    ref = _ref(A, Bs, [256])
+    errs = {}
+    old = autotune.get("fit_terms"), autotune.get("fit_kchunk")
+    try:
+        for terms in (3, 4):
+            for kc in (0, 1, 2, 4):
+                autotune.set_knob("fit_terms", terms)
+                autotune.set_knob("fit_kchunk", kc)
+                o0, _, _ = _run(dpb, mdl, A, Bs, [256], 0, split_in_kernel=split_in_kernel)
+                errs[terms, kc] = _rel(o0, ref)
+    finally:
+        autotune.set_knob("fit_terms", old[0])
+        autotune.set_knob("fit_kchunk", old[1])
+    print("alike rows, K=1600, max relative error by (products, kchunk):",
+          {k: f"{v:.2e}" for k, v in errs.items()})
+    d = (old[0], old[1])
+    assert d[1] > 0
+    assert errs[d] < 2e-6
+    assert errs[d] * 5 < errs[d[0], 0]
+
+
+@pytest.mark.parametrize("kchunk", [0, 1, 2, 4])
+@pytest.mark.parametrize("M,K,N,rows,mode", [(300, 240, 240, [100, 200], 1),
+                                             (777, 1600, 240, [259, 518], 0),
+                                             (257, 96, 240, [257], 3)])
+def test_gemm_chunked_accumulation_modes(dpb, mdl, kchunk, M, K, N, rows, mode):
+    """Every chunk size gives the GEMM to FP32 accuracy, including a K that
+    is not a whole number of chunks and the energy-accumulating last layer."""
+    from deepmd_kit_lr_pt_b200 import autotune
+
+    rng = np.random.default_rng(M + kchunk)
+    A = (rng.normal(size=(M, K)) * 0.5).astype(np.float32)
+    Bs = [(rng.normal(size=(N, K)) / np.sqrt(K)).astype(np.float32) for _ in rows]
+    bias = [rng.normal(size=N).astype(np.float32) for _ in rows]
+    idt = [(rng.normal(size=N) * 0.1).astype(np.float32) for _ in rows]
+    w = [(rng.normal(size=N) / np.sqrt(N)).astype(np.float32) for _ in rows]
+    aux0 = rng.normal(size=(M, N)).astype(np.float32) * 0.5
+    old = autotune.get("fit_kchunk")
+    try:
+        autotune.set_knob("fit_kchunk", kchunk)
+        o0, o1, e = _run(dpb, mdl, A, Bs, rows, mode, aux0=aux0, bias=bias, idt=idt, w=w)
+    finally:
+        autotune.set_knob("fit_kchunk", old)
+    acc = _ref(A, Bs, rows)
+    tb = np.concatenate([np.tile(b, (n, 1)) for b, n in zip(bias, rows)])
+    if mode == 0:
+        assert _rel(o0, acc) < 2e-5
+    elif mode == 1:
+        np.testing.assert_allclose(o0, np.tanh(acc + tb), atol=1e-5, rtol=0)
+    else:  # EPI_LAST: y = tanh(acc + b); h = aux0 + idt y; e += h . w
+        td = np.concatenate([np.tile(d, (n, 1)) for d, n in zip(idt, rows)])
+        tw = np.concatenate([np.tile(x, (n, 1)) for x, n in zip(w, rows)])
+        y = np.tanh(acc + tb)
+        np.testing.assert_allclose(e, ((aux0 + td * y) * tw).sum(1), atol=5e-5, rtol=0)
+        np.testing.assert_allclose(o0, tw * td * (1 - y * y), atol=1e-5, rtol=0)

@@ -185,9 +185,11 @@ def test_batched_nlist_bit_exact(dpb, checker, mods):
 
 
 # --------------------------------------------- batched frames: E / F / V ---
-def test_batched_frames_vs_fp64_oracle(dpb, checker, mods):
-    """One water and one Cu frame of the batched path against the FP64
-    oracle of the same compressed model (and the plain model)."""
+@pytest.mark.parametrize("fused", [True, False])
+def test_batched_frames_vs_fp64_oracle(dpb, checker, mods, fused):
+    """Water and Cu frames of the batched path (one persistent launch, or one
+    launch per stage) against the FP64 oracle of the same compressed model
+    (and the plain model)."""
     from oracle import model_ref
 
     wl, mdl, bt = mods
@@ -196,7 +198,7 @@ def test_batched_frames_vs_fp64_oracle(dpb, checker, mods):
               wl.water_frame_density(90, rng), wl.cu_frame(64, rng)]
     cfg = mdl.SeAConfig(sel=SEL3)
     params = mdl.prepare_frames(mdl.init_params(cfg, seed=3), frames)
-    ev = bt.BatchEvaluator(params, frames)
+    ev = bt.BatchEvaluator(params, frames, fused=fused)
     E, F, V = ev.compute()
     ev.check()
     for f, (coord, atype, box) in enumerate(frames):
