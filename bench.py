@@ -374,6 +374,36 @@ def run_batched(args) -> None:
                            (F[ev.frame_slice(f)] - f0) ** 2))),
                        "virial_max_abs_err": float(np.abs(V[f] - v0).max())})
         del plain
+    # the same step as ONE persistent cooperative launch (dpb_bt_step_launch),
+    # timed the same way, with its pass times
+    one = None
+    if not args.no_one_launch:
+        del ev
+        torch.cuda.synchronize()
+        ev1 = bt.BatchEvaluator(params, frames, device=device, fused=True)
+        E1, F1, V1 = ev1.compute()
+        ev1.check()
+        ev1.capture()
+        for _ in range(max(3, args.warmup)):
+            ev1.replay()
+        ts1 = []
+        for _ in range(args.steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            ev1.replay()
+            b.record()
+            ts1.append((a, b))
+        torch.cuda.synchronize()
+        ms1 = float(np.mean([a.elapsed_time(b) for a, b in ts1]))
+        ev1.check()
+        one = {"ms_per_step": ms1, "us_per_step_atom": ms1 * 1e3 / N, "launches_per_step": 1,
+               "pass_us": ev1.pass_times_us(),
+               "max_abs_diff_vs_staged": {"energy": float(np.abs(E1 - E).max()),
+                                          "force": float(np.abs(F1 - F).max()),
+                                          "virial": float(np.abs(V1 - V).max())}}
+        del ev1
     line = {"metric": "us/step/atom, se_e2_a batched uneven frames (compressed, mixed "
                       "precision)",
             "value": ms * 1e3 / N, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -385,7 +415,7 @@ def run_batched(args) -> None:
                        "sel": list(cfg.sel), "embedding": list(cfg.neuron),
                        "fitting": list(cfg.fitting), "graph": "one CUDA graph per step",
                        "l2": "256 MiB buffer written between timed steps"},
-            "clocks": clk, "checks_vs_fp64_plain": checks,
+            "clocks": clk, "checks_vs_fp64_plain": checks, "one_launch": one,
             "autotune": None if tuned is None else {
                 "knobs": tuned["knobs"], "tuned_ms": tuned["ms"],
                 "default_shapes_ms": tuned["baseline_ms"], "trials": len(tuned["history"])}}
@@ -876,6 +906,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the tile-shape autotuner (batched and train workloads)")
+    ap.add_argument("--no-one-launch", action="store_true",
+                    help="batched workload: skip the one-launch form of the step")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the FP64 plain path (smaller device footprint for profiling)")
     ap.add_argument("--workload", choices=["step", "repeated", "batched", "train"],

@@ -46,7 +46,8 @@ class BtStepDesc(ctypes.Structure):
                 ("table_degree", _I), ("M", _I), ("naxis", _I), ("drow", _P), ("xyz", _P),
                 ("descrpt", _P), ("d_descrpt", _P), ("net_deriv", _P), ("type_rows", _P),
                 ("ntypes", _I), ("fit", GemmLayer * 6), ("e_rows", _P), ("e_const", _P),
-                ("energy", _P), ("force", _P), ("virial", _P), ("sync", _P), ("status", _P)]
+                ("energy", _P), ("force", _P), ("virial", _P), ("sync", _P), ("status", _P),
+                ("pass_ns", _P)]
 
 
 class FrameTable:
@@ -166,7 +167,9 @@ class BatchEvaluator:
         cfg, ft, fit = self.cfg, self.ft, self.fit
         M, ax = cfg.neuron[-1], cfg.axis_neuron
         w, din = fit.width, fit.din
-        self.sync = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.sync = torch.zeros(8, dtype=torch.int32, device=self.dev)
+        # global timer at the start and after each pass of the launch (ns)
+        self.pass_ns = torch.zeros(12, dtype=torch.int64, device=self.dev)
         d = BtStepDesc()
         d.nframes, d.nrows = self.nframes, self.N
         for name, t in (("atom_off", self.atom_off), ("cell_off", self.cell_off),
@@ -179,7 +182,7 @@ class BatchEvaluator:
                         ("net_deriv", self.net_deriv), ("e_rows", fit.e),
                         ("e_const", self.e_const), ("energy", self.energy),
                         ("force", self.force), ("virial", self.virial), ("sync", self.sync),
-                        ("status", self.status)):
+                        ("status", self.status), ("pass_ns", self.pass_ns)):
             setattr(d, name, t.data_ptr())
         d.rcut, d.rcut_smth = cfg.rcut, cfg.rcut_smth
         self._sec = np.ascontiguousarray(cfg.sec, dtype=np.int32)
@@ -215,7 +218,23 @@ class BatchEvaluator:
         self._desc = d
         handle = ctypes.c_void_p()
         call("dpb_bt_step_create", ctypes.byref(handle), ctypes.byref(d))
+        self._split = _capi.lib().dpb_tune_get(b"batch_fused_split") != 0
         self.plan = handle
+
+    def pass_times_us(self) -> dict | None:
+        """Durations (us) of the passes of the last one-launch step, from the
+        global timer read by the first CTA after each grid barrier."""
+        if self.plan is None:
+            return None
+        t = self.pass_ns.cpu().numpy().astype(np.float64)
+        fit = ["fit_layer1", "fit_layer2", "fit_layer3", "fit_layer3_bwd", "fit_layer2_bwd",
+               "fit_layer1_bwd"]
+        if self._split:
+            names = ["cells", "env", "descriptor_fwd"] + fit + ["energy_descriptor_bwd",
+                                                                 "force_virial"]
+        else:
+            names = ["cells", "env_descriptor_fwd"] + fit + ["energy_descriptor_bwd_force"]
+        return {n: (t[k + 1] - t[k]) / 1e3 for k, n in enumerate(names)}
 
     def __del__(self):
         if getattr(self, "plan", None) is not None and _capi is not None:

@@ -41,13 +41,26 @@
 
 namespace dpb {
 
-constexpr int BS_WARPS = 18;
+constexpr int BS_WARPS = 16;
 constexpr int BS_THREADS = 32 * BS_WARPS;
 constexpr int BS_CH = 3;  // table-coefficient loads: L1::evict_last
 constexpr int BS_PASSES = 6;
 constexpr unsigned long long BS_WAIT_NS = 500000000ull;  // per barrier
-static_assert(CfgN80C::THREADS == BS_THREADS && CfgN160::THREADS == BS_THREADS,
-              "the GEMM passes use every warp of the step kernel");
+
+// The GEMM passes of the step kernel: 80-column tiles (N = 240 and the
+// N = 1600 input gradient), chunk-draining epilogue, a THREE-stage ring. The
+// L1 cache and shared memory share 256 KB per SM and the split is fixed per
+// launch: the descriptor passes gather table rows through L1, so the step
+// kernel keeps its shared memory small (the ring, or the per-warp descriptor
+// staging, whichever is larger) and leaves the rest to L1.
+//
+// 16 warps per CTA (512 threads): registers are allocated to warps in
+// groups of four, so 16 warps can have 128 registers a thread where 18 have
+// 96 (at 96 the descriptor passes spilled). The GEMM passes use 14 of them:
+// the weights are pre-split, so no weight-splitting warps, and 8 epilogue
+// warps (40 or 48 chunk sums a thread).
+using CfgBS = GemmCfg<80, 3, 4, 2, 8, false>;
+static_assert(CfgBS::THREADS <= BS_THREADS, "the GEMM passes fit in the step kernel's warps");
 
 struct BtStepArgs {
   GemmMaps maps[BS_PASSES];
@@ -76,9 +89,12 @@ struct BtStepArgs {
   double* energy;
   double* force;
   double* virial;
-  unsigned* sync;
+  unsigned* sync;  // [0] barrier arrivals, [1]-[4] row counters, [5] frame counter
   int* status;
+  unsigned long long* pass_ns;
   int nrows, M, naxis, wsm_floats;
+  int split_rows;  // 1: env / descriptor forward (descriptor backward / forces)
+                   // as separate passes, rows through memory; 0: one pass each
   float inv_nnei, rcut, rcut_smth;
 };
 
@@ -122,10 +138,59 @@ __device__ bool bs_sync(const BtStepArgs& a, unsigned k, int* s_ok) {
   return *s_ok != 0;
 }
 
+// next work item of a pass for this warp (rows are taken dynamically: rows
+// of Cu and water frames differ in cost)
+__device__ __forceinline__ int bs_next_row(unsigned* counter, int lane) {
+  int r = 0;
+  if (lane == 0) r = (int)atomicAdd(counter, 1u);
+  return __shfl_sync(0xffffffffu, r, 0);
+}
+// next frame for the whole CTA
+__device__ __forceinline__ int bs_next_frame(unsigned* counter, int* s_item) {
+  __syncthreads();
+  if (threadIdx.x == 0) *s_item = (int)atomicAdd(counter, 1u);
+  __syncthreads();
+  return *s_item;
+}
+__device__ __forceinline__ void bs_stamp(const BtStepArgs& a, int k) {
+  if (a.pass_ns != nullptr && blockIdx.x == 0 && threadIdx.x == 0) a.pass_ns[k] = bs_clock();
+}
+
 // shared memory leaves generic use for TMA use (or back)
 __device__ __forceinline__ void bs_smem_switch() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();
+}
+
+// The per-row work of the row passes.
+__device__ __forceinline__ void bs_row_env(const BtStepArgs& a, int row, int lane, float* wsm) {
+  bt_env_row<float>(row, lane, *reinterpret_cast<BtEnvSmem*>(wsm), a.em, a.nlist, a.cw, a.type,
+                    a.cell_of, a.cell_start, a.cell_atoms, a.avg, a.std_, a.fr, a.sec, a.rcut,
+                    a.rcut_smth, a.status);
+}
+
+template <int NC, bool COH>
+__device__ __forceinline__ void bs_row_fwd(const BtStepArgs& a, int row, int lane, float* wsm) {
+  desc_fwd_atom<BS_CH, NC, COH>(row, lane, wsm, a.xyz, a.D, a.drow, a.em, a.tt, a.M, a.naxis,
+                                a.inv_nnei);
+}
+
+template <int NC>
+__device__ __forceinline__ void bs_row_bwd(const BtStepArgs& a, int row, int lane, float* wsm) {
+  desc_bwd_atom<BS_CH, NC>(row, lane, wsm, a.net_deriv, a.dD, a.drow, a.xyz, a.em, a.tt, a.M,
+                           a.naxis, a.inv_nnei);
+}
+
+template <bool COH>
+__device__ __forceinline__ void bs_row_force(const BtStepArgs& a, int row, int lane) {
+  bt_force_row<float, COH>(row, lane, a.force, a.virial, a.net_deriv, a.cw, a.type, a.std_,
+                           a.nlist, a.fr, a.sec.ntypes, a.sec.nnei, a.rcut, a.rcut_smth);
+}
+
+template <int MODE>
+__device__ __forceinline__ void bs_gemm(const BtStepArgs& a, int l, unsigned char* smem,
+                                     GemmBars& bars, uint32_t tmem) {
+  gemm_run<CfgBS, MODE, true>(a.maps[l], a.shp[l], a.epi[l], a.status, smem, bars, tmem);
 }
 
 template <int NC>
@@ -134,7 +199,7 @@ __global__ void __launch_bounds__(BS_THREADS, 1) k_bt_step(const __grid_constant
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ GemmBars bars[BS_PASSES];
   __shared__ uint32_t tmem_slot;
-  __shared__ int s_ok;
+  __shared__ int s_ok, s_item;
   __shared__ double s_part[BS_WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp == 1) tmem_alloc_all(&tmem_slot);
@@ -144,67 +209,77 @@ __global__ void __launch_bounds__(BS_THREADS, 1) k_bt_step(const __grid_constant
   const uint32_t tmem = tmem_slot;
   const int nrows = a.nrows, F = a.fr.nframes;
   const int gthreads = gridDim.x * BS_THREADS, gtid = blockIdx.x * BS_THREADS + threadIdx.x;
-  const int gwarps = gridDim.x * BS_WARPS, gwarp = blockIdx.x * BS_WARPS + warp;
   float* wsm = reinterpret_cast<float*>(smem) + (size_t)warp * a.wsm_floats;
   unsigned k = 0;
+  bs_stamp(a, 0);
 
   // ---- P0: accumulators, cells
   for (int q = gtid; q < 3 * nrows; q += gthreads) a.force[q] = 0.;
   for (int q = gtid; q < 9 * F; q += gthreads) a.virial[q] = 0.;
   for (int q = gtid; q < nrows; q += gthreads) a.e_rows[q] = 0.f;
-  for (int f = blockIdx.x; f < F; f += gridDim.x) {
+  for (int f = bs_next_frame(a.sync + 5, &s_item); f < F; f = bs_next_frame(a.sync + 5, &s_item))
     bt_cells_frame(f, a.cw, a.cell_of, a.cell_start, a.cell_atoms, a.coord, a.fr,
                    reinterpret_cast<int*>(smem));
-    __syncthreads();  // the counts are reused by the next frame
-  }
   bool ok = bs_sync(a, ++k, &s_ok);
+  bs_stamp(a, k);
 
   // ---- P1: env rows + descriptor forward
   if (ok) {
-    for (int row = gwarp; row < nrows; row += gwarps) {
-      bt_env_row<float>(row, lane, *reinterpret_cast<BtEnvSmem*>(wsm), a.em, a.nlist, a.cw,
-                        a.type, a.cell_of, a.cell_start, a.cell_atoms, a.avg, a.std_, a.fr,
-                        a.sec, a.rcut, a.rcut_smth, a.status);
+    for (int row = bs_next_row(a.sync + 1, lane); row < nrows;
+         row = bs_next_row(a.sync + 1, lane)) {
+      bs_row_env(a, row, lane, wsm);
       __syncwarp();
-      desc_fwd_atom<BS_CH, NC, true>(row, lane, wsm, a.xyz, a.D, a.drow, a.em, a.tt, a.M,
-                                     a.naxis, a.inv_nnei);
-      __syncwarp();
+      if (!a.split_rows) {
+        bs_row_fwd<NC, true>(a, row, lane, wsm);
+        __syncwarp();
+      }
+    }
+    if (a.split_rows) {
+      ok = bs_sync(a, ++k, &s_ok);
+      bs_stamp(a, k);
+      if (ok)
+        for (int row = bs_next_row(a.sync + 2, lane); row < nrows;
+             row = bs_next_row(a.sync + 2, lane)) {
+          bs_row_fwd<NC, false>(a, row, lane, wsm);
+          __syncwarp();
+        }
     }
     bs_smem_switch();
     ok = bs_sync(a, ++k, &s_ok);
+    bs_stamp(a, k);
   }
 
   // ---- P2-P7: the fitting GEMMs
   if (ok) {
-    gemm_run<CfgN80C, EPI_TANH, true>(a.maps[0], a.shp[0], a.epi[0], a.status, smem, bars[0],
-                                       tmem);
+    bs_gemm<EPI_TANH>(a, 0, smem, bars[0], tmem);
     ok = bs_sync(a, ++k, &s_ok);
+    bs_stamp(a, k);
   }
   if (ok) {
-    gemm_run<CfgN80C, EPI_RES_DT, true>(a.maps[1], a.shp[1], a.epi[1], a.status, smem,
-                                         bars[1], tmem);
+    bs_gemm<EPI_RES_DT>(a, 1, smem, bars[1], tmem);
     ok = bs_sync(a, ++k, &s_ok);
+    bs_stamp(a, k);
   }
   if (ok) {
-    gemm_run<CfgN80C, EPI_LAST, true>(a.maps[2], a.shp[2], a.epi[2], a.status, smem, bars[2],
-                                       tmem);
+    bs_gemm<EPI_LAST>(a, 2, smem, bars[2], tmem);
     ok = bs_sync(a, ++k, &s_ok);
+    bs_stamp(a, k);
   }
   if (ok) {
-    gemm_run<CfgN80C, EPI_BWD_DT, true>(a.maps[3], a.shp[3], a.epi[3], a.status, smem,
-                                         bars[3], tmem);
+    bs_gemm<EPI_BWD_DT>(a, 3, smem, bars[3], tmem);
     ok = bs_sync(a, ++k, &s_ok);
+    bs_stamp(a, k);
   }
   if (ok) {
-    gemm_run<CfgN80C, EPI_BWD_RES, true>(a.maps[4], a.shp[4], a.epi[4], a.status, smem,
-                                          bars[4], tmem);
+    bs_gemm<EPI_BWD_RES>(a, 4, smem, bars[4], tmem);
     ok = bs_sync(a, ++k, &s_ok);
+    bs_stamp(a, k);
   }
   if (ok) {
-    gemm_run<CfgN160, EPI_STORE, false>(a.maps[5], a.shp[5], a.epi[5], a.status, smem,
-                                         bars[5], tmem);
+    bs_gemm<EPI_STORE>(a, 5, smem, bars[5], tmem);
     bs_smem_switch();
     ok = bs_sync(a, ++k, &s_ok);
+    bs_stamp(a, k);
   }
 
   // ---- P8: energies, descriptor backward + forces
@@ -213,19 +288,34 @@ __global__ void __launch_bounds__(BS_THREADS, 1) k_bt_step(const __grid_constant
       bt_energy_frame<float>(f, a.energy, a.e_rows, a.drow, a.e_const, a.fr, s_part);
       __syncthreads();
     }
-    for (int row = gwarp; row < nrows; row += gwarps) {
-      desc_bwd_atom<BS_CH, NC>(row, lane, wsm, a.net_deriv, a.dD, a.drow, a.xyz, a.em, a.tt,
-                               a.M, a.naxis, a.inv_nnei);
+    for (int row = bs_next_row(a.sync + 3, lane); row < nrows;
+         row = bs_next_row(a.sync + 3, lane)) {
+      bs_row_bwd<NC>(a, row, lane, wsm);
       __syncwarp();
-      bt_force_row<float, true>(row, lane, a.force, a.virial, a.net_deriv, a.cw, a.type,
-                                a.std_, a.nlist, a.fr, a.sec.ntypes, a.sec.nnei, a.rcut,
-                                a.rcut_smth);
-      __syncwarp();
+      if (!a.split_rows) {
+        bs_row_force<true>(a, row, lane);
+        __syncwarp();
+      }
+    }
+    if (a.split_rows) {
+      ok = bs_sync(a, ++k, &s_ok);
+      bs_stamp(a, k);
+      if (ok)
+        for (int row = bs_next_row(a.sync + 4, lane); row < nrows;
+             row = bs_next_row(a.sync + 4, lane)) {
+          bs_row_force<false>(a, row, lane);
+          __syncwarp();
+        }
     }
   }
 
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  if (ok && a.pass_ns != nullptr && threadIdx.x == 0) {
+    // the end of the last pass: when the last CTA finishes it
+    __threadfence();
+    if (atomicAdd(a.sync, 1u) == (k + 1) * gridDim.x - 1) a.pass_ns[k + 1] = bs_clock();
+  }
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     tmem_free_all(tmem);
@@ -239,9 +329,6 @@ struct BtStepPlan {
   size_t smem;
 };
 
-static size_t bs_dyn_smem() {
-  return (size_t)std::max(CfgN80C::SMEM, CfgN160::SMEM);
-}
 
 }  // namespace dpb
 
@@ -283,16 +370,21 @@ int dpb_bt_step_create(void** plan, const dpb_bt_step_desc* d) {
   size_t wf = std::max(fwd_smem_floats(d->M, nnei), bwd_smem_floats(d->M, nnei, d->naxis));
   wf = std::max(wf, (sizeof(BtEnvSmem) + 3) / 4);
   wf = (wf + 3) / 4 * 4;
-  const size_t smem = bs_dyn_smem();
-  if (wf * 4 * BS_WARPS + 1024 > smem || 4 * (BT_MAXCELLS + 1) + 1024 > (int)smem) {
+  const size_t smem = std::max({(size_t)CfgBS::SMEM, wf * 4 * BS_WARPS + 1024,
+                                (size_t)4 * (BT_MAXCELLS + 1) + 1024});
+  if (smem + 4096 > 232448) {
     set_error("bt_step: the per-warp descriptor staging (%zu B) does not fit", wf * 4);
     return DPB_ERR_INVALID;
   }
   // the six fitting GEMMs, in the order and with the epilogues of the step
   static const int modes[BS_PASSES] = {EPI_TANH, EPI_RES_DT, EPI_LAST,
                                        EPI_BWD_DT, EPI_BWD_RES, EPI_STORE};
-  const int P = std::max(1, std::min(tune_value("fit_kchunk", 4),
-                                     std::min(CfgN80C::STAGES, CfgN80C::ASLOTS)));
+  // chunked accumulation as the fit_kchunk* knobs ask (at least one chunk
+  // per tile: the 80-column passes always drain through the chunk sums)
+  const int cross_first = tune_value("fit_kchunk_cross_first", 0) != 0;
+  int P = tune_value("fit_kchunk", 8);
+  if (cross_first) P = std::min(P, std::min(CfgBS::STAGES, CfgBS::ASLOTS));
+  if (P <= 0) P = 1 << 20;  // one chunk per tile
   for (int l = 0; l < BS_PASSES; ++l) {
     const dpb_gemm_layer& g = d->fit[l];
     if (g.mode != modes[l] || g.b_lo == nullptr) {
@@ -303,12 +395,10 @@ int dpb_bt_step_create(void** plan, const dpb_bt_step_desc* d) {
     int bn = 0;
     rc = gemm_prepare(g.A, d->nrows, g.K, g.b_hi, g.b_lo, g.N, d->type_rows, d->ntypes,
                       g.mode, g.out0, g.out1, g.aux0, g.aux1, g.bias, g.idt, g.w, d->e_rows,
-                      l < 5 ? CfgN80C::BN : CfgN160::BN, a.maps[l], a.shp[l], a.epi[l], bn);
+                      CfgBS::BN, a.maps[l], a.shp[l], a.epi[l], bn);
     if (rc) return rc;
-    if (l < 5) {
-      a.shp[l].kchunk = P;
-      a.shp[l].cross_first = 1;
-    }
+    a.shp[l].kchunk = P;
+    a.shp[l].cross_first = cross_first && P <= CfgBS::STAGES;
   }
   a.cw = d->cw;
   a.cell_of = d->cell_of;
@@ -332,6 +422,8 @@ int dpb_bt_step_create(void** plan, const dpb_bt_step_desc* d) {
   a.virial = d->virial;
   a.sync = d->sync;
   a.status = d->status;
+  a.pass_ns = d->pass_ns;
+  a.split_rows = tune_value("batch_fused_split", 0) != 0;
   a.nrows = d->nrows;
   a.M = d->M;
   a.naxis = d->naxis;
@@ -348,6 +440,10 @@ int dpb_bt_step_create(void** plan, const dpb_bt_step_desc* d) {
   const int nc = d->table_degree + 1;
   const void* fn = nc == 4 ? (const void*)k_bt_step<4> : (const void*)k_bt_step<6>;
   DPB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+           "bt_step");
+  // the smallest shared-memory carve-out that holds it: the rest is L1
+  const int pct = (int)std::min<size_t>(100, ((smem + 4096) * 100 + 233471) / 233472);
+  DPB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct),
            "bt_step");
   int per_sm = 0;
   DPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, BS_THREADS, smem),
@@ -372,7 +468,7 @@ int dpb_bt_step_launch(const void* plan, dpb_stream_t stream) {
   }
   const BtStepPlan* p = static_cast<const BtStepPlan*>(plan);
   cudaStream_t st = as_stream(stream);
-  DPB_CUDA(cudaMemsetAsync(p->a.sync, 0, sizeof(unsigned), st), "bt_step");
+  DPB_CUDA(cudaMemsetAsync(p->a.sync, 0, 8 * sizeof(unsigned), st), "bt_step");
   void* args[] = {(void*)&p->a};
   const void* fn = p->nc == 4 ? (const void*)k_bt_step<4> : (const void*)k_bt_step<6>;
   DPB_CUDA(cudaLaunchCooperativeKernel(fn, dim3(p->grid), dim3(BS_THREADS), args, p->smem, st),

@@ -21,11 +21,16 @@ constexpr uint32_t TM_COLS = 512;
 
 // one kernel configuration: tile width, ring depth, TMEM A slots,
 // accumulator buffers and epilogue warps
-template <int BN_, int STAGES_, int ASLOTS_, int ACCBUF_, int EPIW_>
+// BSPLIT: with the four warps that split FP32 weights into TF32 hi / lo in
+// shared memory (false: pre-split weights only, the epilogue warps follow
+// the A-split warps)
+template <int BN_, int STAGES_, int ASLOTS_, int ACCBUF_, int EPIW_, bool BSPLIT_ = true>
 struct GemmCfg {
   static constexpr int BN = BN_, STAGES = STAGES_, ASLOTS = ASLOTS_, ACCBUF = ACCBUF_,
                        EPIW = EPIW_;
-  static constexpr int THREADS = 64 + 128 + 128 + 32 * EPIW;
+  static constexpr bool BSPLIT = BSPLIT_;
+  static constexpr int EPI0 = BSPLIT ? 10 : 6;  // first epilogue warp
+  static constexpr int THREADS = 32 * EPI0 + 32 * EPIW;
   static constexpr uint32_t ACC_STRIDE = BN <= 128 ? 128u : (uint32_t)((BN + 31) / 32 * 32);
   static constexpr uint32_t A0 = ACCBUF * ACC_STRIDE;
   static constexpr int A_BYTES = GT_BM * GT_BK * 4;  // 16 KB
@@ -292,7 +297,7 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
     abort_flag = 0;
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full_bar[s], 1);
-      mbar_init(&conv_bar[s], shp.split_b ? 256 : 128);
+      mbar_init(&conv_bar[s], CFG::BSPLIT && shp.split_b ? 256 : 128);
       mbar_init(&empty_bar[s], 1);
     }
     for (int a = 0; a < ASLOTS; ++a) mbar_init(&afree_bar[a], 1);
@@ -504,7 +509,7 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
         mbar_arrive(&conv_bar[s]);
       }
     }
-  } else if (warp < 10) {
+  } else if (CFG::BSPLIT && warp < 10) {
     // ------------------------------------- split FP32 B tiles into hi / lo
     // (only with FP32 weights): TF32 hi in place, lo into the lo buffer at the
     // same swizzled offset; rows r and r + 128 of the BN-row tile
@@ -545,13 +550,13 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
         }
       }
     }
-  } else if (warp < 10 + EPIW) {
+  } else if (warp >= CFG::EPI0 && warp < CFG::EPI0 + EPIW) {
     // ---------------------------------------------------------------- epilogue
     // warp (warp % 4) owns TMEM lanes 32 * (warp % 4) ..., one row per
     // thread; each 16-column chunk moves as 4 x 16-byte loads / stores per
     // operand (64 contiguous bytes per thread and row)
     const int lane_base = 32 * (warp & 3);
-    const int ehalf = EPIW == 8 ? (warp - 10) >> 2 : 0;  // column share of this warp
+    const int ehalf = EPIW == 8 ? (warp - CFG::EPI0) >> 2 : 0;  // column share of this warp
     constexpr int CSTEP = 16 * (EPIW / 4);               // column stride of this warp's groups
     // chunked kernels: each warp of a lane quadrant owns a contiguous column
     // range, [0, CH0) or [CH0, BN), in 16-column groups

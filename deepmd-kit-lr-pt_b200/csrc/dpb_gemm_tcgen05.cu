@@ -14,11 +14,13 @@
 // loses up to an ulp of the running sum per instruction, always in the same
 // direction: over K = 1600 that is ~1.5e-5 of the output scale, and it does
 // not average out where rows are alike (the atoms of a crystal). So long
-// sums are accumulated in chunks (knob fit_kchunk k-blocks per chunk, on the
-// 80-column tiles): each chunk starts a fresh TMEM accumulator, takes its
-// small cross products first and its Ah Bh products after them, and the
-// epilogue warps add the chunks in FP32 (round to nearest) in registers.
-// That brings the error to FP32-GEMM level (~5e-7 on the same rows).
+// sums are accumulated in chunks (knob fit_kchunk k-blocks per chunk, 8 by
+// default, on the 80-column tiles): each chunk starts a fresh TMEM
+// accumulator and the epilogue warps add the chunks in FP32 (round to
+// nearest) in registers. With knob fit_kchunk_cross_first a chunk (at most 4
+// k-blocks) also takes its small cross products before its Ah Bh products,
+// which brings the error to FP32-GEMM level (~5e-7 on the same rows) at
+// 15% more fitting time.
 //
 // Persistent, warp-specialised CTA (one per SM) walking output tiles of 128
 // rows x BN columns (the widest of 240 (K <= 512), 160, 80 that divides N and the
@@ -120,8 +122,8 @@ static int launch(const GemmMaps& maps, GemmShape shp, const GemmEpi& epi, int* 
   if constexpr (CFG::BN == 80) {
     using C = CfgN80C;
     const int nk = (shp.K + GT_BK - 1) / GT_BK;
-    shp.cross_first = tune_value("fit_kchunk_cross_first", 1) != 0;
-    int P = tune_value("fit_kchunk", 4);
+    shp.cross_first = tune_value("fit_kchunk_cross_first", 0) != 0;
+    int P = tune_value("fit_kchunk", 8);
     if (shp.cross_first) P = std::min(P, std::min(C::STAGES, C::ASLOTS));
     if (P > 0 && nk > P && shp.K >= tune_value("fit_kchunk_min_k", 0)) {
       shp.kchunk = P;

@@ -39,11 +39,14 @@ static Knob g_knobs[] = {
     // accumulator per output tile: the tensor cores' FP32 accumulation loses
     // up to an ulp of the running sum per instruction, always in the same
     // direction, so long sums over rows that are alike drift
-    {"fit_kchunk", 4, 5, {0, 1, 2, 4, 8}},
+    // (measured, 12,288-atom water fitting stage / worst Cu-frame energy
+    // error: 0 298 us / 1.4e-6 eV/atom; 8 k-block order 302 us / 2.3e-7;
+    // 4 k-block order 320 us / 1.1e-7; 4 cross first 345 us / 3.1e-8)
+    {"fit_kchunk", 8, 5, {0, 1, 2, 4, 8}},
     // order inside a chunk: 1 the cross products of all its k-blocks first
-    // (the chunk's stages stay resident until its Ah Bh products are issued),
-    // 0 k-block by k-block
-    {"fit_kchunk_cross_first", 1, 2, {0, 1}},
+    // (the chunk's stages stay resident until its Ah Bh products are issued;
+    // at most 4 k-blocks per chunk), 0 k-block by k-block
+    {"fit_kchunk_cross_first", 0, 2, {0, 1}},
     // chunked accumulation only for K at least this (shorter sums drift less)
     {"fit_kchunk_min_k", 0, 2, {0, 512}},
     // warps (one center atom each) per CTA of the batched env / force kernels
@@ -51,6 +54,10 @@ static Knob g_knobs[] = {
     // batched-frames step: 1 one persistent cooperative launch
     // (dpb_bt_step_launch), 0 one launch per stage
     {"batch_fused", 0, 2, {0, 1}},
+    // one-launch step: 1 the env rows and the descriptor forward (the
+    // descriptor backward and the forces) as separate passes, 0 back to back
+    // per row in one pass
+    {"batch_fused_split", 0, 2, {0, 1}},
     // neighbor rows per group in the FP32 training kernels
     {"train_rows_per_group", 8, 2, {4, 8}},
     // most warps per CTA of the training kernels (fewer when shared memory

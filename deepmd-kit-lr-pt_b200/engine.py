@@ -102,7 +102,7 @@ class ForwardLower:
         il = self._ilist if ilist is None else ilist.to(torch.int32).contiguous()
         M, ax = cfg.neuron[-1], cfg.axis_neuron
         sec = cfg.sec
-        self.results.zero_()
+        call("dpb_zero_async", ptr(self.results), 8 * self.results.numel(), s)
         energy = self.results[0:1]
         force = self.results[1:1 + 3 * nall].view(nall, 3)
         virial = self.results[1 + 3 * self.nall_max:]

@@ -417,8 +417,10 @@ typedef struct {
  * (tables: host array of device pointers, table_info: host, 6 per type,
  * table_degree 5 or 3), the six fitting GEMMs in the order layer 1..3
  * forward (epilogues 1, 2, 3) and layer 3..1 backward (4, 5, 0), the
- * per-frame energy constants and the outputs. sync: one device word for the
- * grid barriers (zeroed by each launch); status: the device status word. */
+ * per-frame energy constants and the outputs. sync: eight device words (grid
+ * barrier and work counters, zeroed by each launch); status: the device
+ * status word; pass_ns: NULL, or 12 device words that receive the global
+ * timer (ns) at the start and after each of the 11 passes. */
 typedef struct {
   int nframes;
   int nrows;
@@ -461,6 +463,7 @@ typedef struct {
   double* virial;
   unsigned* sync;
   int* status;
+  unsigned long long* pass_ns;
 } dpb_bt_step_desc;
 
 /* Checks the description and prepares the launch (tensor maps of the six
@@ -469,7 +472,7 @@ typedef struct {
 DPB_API int dpb_bt_step_create(void** plan, const dpb_bt_step_desc* desc);
 /* One step: env, descriptor, fitting, descriptor backward, forces, virials
  * and energies of every frame in ONE cooperative launch (one CTA per SM),
- * preceded by a 4-byte memset of the barrier word. */
+ * preceded by a 32-byte memset of the barrier and work counters. */
 DPB_API int dpb_bt_step_launch(const void* plan, dpb_stream_t stream);
 DPB_API void dpb_bt_step_destroy(void* plan);
 /* Layout of the description structs as this library was compiled: which = 0

@@ -61,7 +61,9 @@ def test_batch_graph_replay_repeats(setup, fused):
 def test_fused_step_equals_staged_step(setup):
     """The one-launch step and the per-stage launches run the same device
     bodies: neighbor lists, env rows and descriptors identical; energies,
-    forces and virials equal up to the order of the atomic sums."""
+    forces and virials to FP32 accuracy (the one-launch step runs the short
+    K = 240 fitting layers on the chunk-draining tile form, whose products
+    are issued in another order, so the FP32 sums round differently)."""
     mdl, bt, frames, params = setup
     a = bt.BatchEvaluator(params, frames, fused=True)
     b = bt.BatchEvaluator(params, frames, fused=False)
@@ -73,8 +75,8 @@ def test_fused_step_equals_staged_step(setup):
     assert np.array_equal(a.em.cpu().numpy(), b.em.cpu().numpy())
     assert np.array_equal(a.D.cpu().numpy(), b.D.cpu().numpy())
     np.testing.assert_allclose(Ea, Eb, rtol=0, atol=1e-5)
-    np.testing.assert_allclose(Fa, Fb, rtol=0, atol=1e-9)
-    np.testing.assert_allclose(Va, Vb, rtol=0, atol=1e-7)
+    np.testing.assert_allclose(Fa, Fb, rtol=0, atol=1e-6)
+    np.testing.assert_allclose(Va, Vb, rtol=0, atol=1e-5 * max(1.0, float(np.abs(Vb).max())))
     # a second step of the fused form (accumulators re-zeroed in the launch)
     Ea2, Fa2, _ = a.compute()
     np.testing.assert_allclose(Ea2, Ea, rtol=0, atol=1e-5)
