@@ -190,9 +190,10 @@ __device__ __forceinline__ void tr_entries(int* ent, int* secn, const int* nl, c
 
 // Staged per-row vectors: the R rows of channel c are contiguous, and with
 // two 16-byte chunks per channel the chunks are swapped when bit 2 of c is
-// set. A lane-owned channel then moves as whole 16-byte chunks without bank
-// conflicts (the 8 lanes of a quarter-warp hit 8 different bank groups) and
-// the next layer reads one channel as one or two broadcast 16-byte loads.
+// set (with four, chunk h goes to h ^ ((c >> 1) & 3)). A lane-owned channel
+// then moves as whole 16-byte chunks without bank conflicts (the 8 lanes of
+// a quarter-warp hit 8 different bank groups) and the next layer reads one
+// channel as one to four broadcast 16-byte loads.
 template <typename T>
 struct Vec16;
 template <>
@@ -209,8 +210,8 @@ struct Vec16<double> {
 template <typename T, int R>
 __device__ __forceinline__ int stg_chunk(int c, int h) {
   constexpr int Q = R / Vec16<T>::n;
-  static_assert(Q == 1 || Q == 2, "one or two 16-byte chunks per staged channel");
-  return Q == 2 ? (h ^ ((c >> 2) & 1)) : h;
+  static_assert(Q == 1 || Q == 2 || Q == 4, "one, two or four 16-byte chunks per channel");
+  return Q == 4 ? (h ^ ((c >> 1) & 3)) : Q == 2 ? (h ^ ((c >> 2) & 1)) : h;
 }
 
 template <typename T, int R>
@@ -1695,13 +1696,18 @@ static int tr_pick_warps(TrKind kind, const TrDims& d, int maxw, int R) {
   return 0;
 }
 
-// rows per group: the train_rows_per_group knob for the FP32 standard net,
-// else the precision's default
+// rows per group: the train_rows_per_group knob for the FP32 standard net;
+// train_rows_per_group_f64 for the FP64 force-backward kernel of the
+// standard net (measured on the 12,288-atom FP64 plain step: backward 7.30
+// ms with 4 rows, 5.88 ms with 8; the forward is faster with 4, 3.18 against
+// 3.46 ms, and the tangent and reverse kernels spill at 8); else the
+// precision's default
 template <typename T>
-static int tr_rows(const TrNet<T>& net) {
-  if (sizeof(T) == 4 && tr_std_net(net))
-    return tune_value("train_rows_per_group", TrTraits<T>::R) == 4 ? 4 : 8;
-  return TrTraits<T>::R;
+static int tr_rows(const TrNet<T>& net, TrKind kind) {
+  if (!tr_std_net(net)) return TrTraits<T>::R;
+  if (sizeof(T) == 4) return tune_value("train_rows_per_group", TrTraits<T>::R) == 4 ? 4 : 8;
+  if (kind != TR_BWD) return TrTraits<T>::R;
+  return tune_value("train_rows_per_group_f64", 8) == 4 ? 4 : 8;
 }
 
 template <typename T>
@@ -1721,7 +1727,7 @@ static int tr_prepare(TrKind kind, TrNet<T>& net, TrGeom& g, TrLayout& L, int& R
     return DPB_ERR_INVALID;
   }
   const TrDims d{net.n1, net.n2, net.n3, ax, g.nnei, g.ntypes};
-  R = tr_rows(net);
+  R = tr_rows(net, kind);
   const int maxw = std::min(tune_value("train_warps_per_cta", 8), kind == TR_REV ? 4 : 8);
   const int nw = tr_pick_warps<T>(kind, d, maxw, R);
   if (nw < 1) {
@@ -1773,7 +1779,7 @@ using namespace dpb;
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
     auto kern = !tr_std_net(net) ? k_tr_fwd<T, TrTraits<T>::R, 0, 0, 0>                         \
-                : (R == 4 ? k_tr_fwd<T, 4, 25, 50, 100> : k_tr_fwd<T, TrTraits<T>::R, 25, 50, 100>);\
+                : (R == 4 ? k_tr_fwd<T, 4, 25, 50, 100> : k_tr_fwd<T, 8, 25, 50, 100>);\
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1807,7 +1813,7 @@ using namespace dpb;
                     axis, g.nnei, st);                                                          \
     if (rc) return rc;                                                                          \
     auto kern = !tr_std_net(net) ? k_tr_bwd<T, TrTraits<T>::R, 0, 0, 0>                         \
-                : (R == 4 ? k_tr_bwd<T, 4, 25, 50, 100> : k_tr_bwd<T, TrTraits<T>::R, 25, 50, 100>);\
+                : (R == 4 ? k_tr_bwd<T, 4, 25, 50, 100> : k_tr_bwd<T, 8, 25, 50, 100>);\
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1839,7 +1845,7 @@ using namespace dpb;
       return DPB_ERR_INVALID;                                                                   \
     }                                                                                           \
     auto kern = !tr_std_net(net) ? k_tr_tan<T, TrTraits<T>::R, 0, 0, 0>                         \
-                : (R == 4 ? k_tr_tan<T, 4, 25, 50, 100> : k_tr_tan<T, TrTraits<T>::R, 25, 50, 100>);\
+                : (R == 4 ? k_tr_tan<T, 4, 25, 50, 100> : k_tr_tan<T, 8, 25, 50, 100>);\
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \
@@ -1889,7 +1895,7 @@ using namespace dpb;
                     g.nnei, st);                                                                \
     if (rc) return rc;                                                                          \
     auto kern = !tr_std_net(net) ? k_tr_rev<T, TrTraits<T>::R, 0, 0, 0>                         \
-                : (R == 4 ? k_tr_rev<T, 4, 25, 50, 100> : k_tr_rev<T, TrTraits<T>::R, 25, 50, 100>);\
+                : (R == 4 ? k_tr_rev<T, 4, 25, 50, 100> : k_tr_rev<T, 8, 25, 50, 100>);\
     int grid;                                                                                   \
     size_t smem;                                                                                \
     rc = tr_launch_cfg(kern, L, sizeof(T), nrows, grid, smem);                                  \

@@ -49,6 +49,8 @@ static Knob g_knobs[] = {
     {"fit_kchunk_cross_first", 0, 2, {0, 1}},
     // chunked accumulation only for K at least this (shorter sums drift less)
     {"fit_kchunk_min_k", 0, 2, {0, 512}},
+    // epilogue warps of the unchunked 80-column GEMM tiles (short-K layers)
+    {"fit_epi_warps", 4, 2, {4, 8}},
     // warps (one center atom each) per CTA of the batched env / force kernels
     {"batch_atoms_per_cta", 4, 3, {2, 4, 8}},
     // batched-frames step: 1 one persistent cooperative launch
@@ -60,6 +62,9 @@ static Knob g_knobs[] = {
     {"batch_fused_split", 0, 2, {0, 1}},
     // neighbor rows per group in the FP32 training kernels
     {"train_rows_per_group", 8, 2, {4, 8}},
+    // the same for the FP64 force-backward kernel (also the embedding
+    // backward of the FP64 plain evaluation path)
+    {"train_rows_per_group_f64", 8, 2, {4, 8}},
     // most warps per CTA of the training kernels (fewer when shared memory
     // does not allow them)
     {"train_warps_per_cta", 8, 4, {1, 2, 4, 8}},
