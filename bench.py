@@ -15,9 +15,9 @@ fitting net forward and backward, descriptor backward, force and virial.
 
 ours:      the compressed FP32 path (FP64 coordinate differences and sums),
            replayed as a CUDA graph; device time per step with the L2 flushed
-           between steps; e2e through SeAEvaluator.compute() with pinned host
-           buffers (H2D coordinates, D2H energy/force/virial) in the timed
-           region. The FP64 plain path, per-stage times and errors are
+           between steps; e2e through SeAEvaluator.run_pinned() (pinned host
+           buffers; H2D coordinates, the step and D2H energy/force/virial in
+           one graph) in the timed region, compute() beside it. The FP64 plain path, per-stage times and errors are
            reported beside it.
 reference: the reference's own CPU implementation (deepmd:: *_cpu functions
            compiled from the reference sources, FP64, OpenMP where the
@@ -700,20 +700,34 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     ms_step = max_over_ranks(float(np.sum(ms)) / args.steps, world, device)
     value = whole_job_us_per_atom(ms_step, nloc, world)
 
-    # ---- end to end through the public call: pinned host in, pinned host out
+    # ---- end to end through the public calls: pinned host in, pinned host out.
+    # run_pinned(): the host-to-device copy of the coordinates, the step and
+    # the device-to-host copy of energy / forces / virial as one graph;
+    # compute(host_c): the same through separate copies (reported beside it)
     host_c = torch.tensor(coord, dtype=torch.float64).pin_memory()
     host_out = torch.empty(1 + 3 * nloc + 9, dtype=torch.float64).pin_memory()
+    io_c, _ = ev.io_buffers()
+    io_c.copy_(host_c)
     for _ in range(args.warmup):
         ev.compute(host_c, out=host_out)
+        ev.run_pinned()
     barrier()
-    e2e = []
+    e2e, e2e_compute = [], []
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ev.compute(host_c, out=host_out)
+        e_step = float(ev.run_pinned()[0][0])
         e2e.append(time.perf_counter() - t0)
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev.compute(host_c, out=host_out)
+        e2e_compute.append(time.perf_counter() - t0)
+    # the same step (up to the order of the FP32 atomic energy partials)
+    assert abs(e_step - float(host_out[0])) <= 1e-8 * nloc, "run_pinned and compute disagree"
     e2e_ms = max_over_ranks(float(np.mean(e2e)) * 1e3, world, device)
+    e2e_compute_ms = max_over_ranks(float(np.mean(e2e_compute)) * 1e3, world, device)
     clk = clocks.stop()
     ev.check()
 
@@ -883,7 +897,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                        "graph": "one CUDA graph per step"},
             "e2e": {"value": whole_job_us_per_atom(e2e_ms, nloc, world), "unit": UNIT,
                     "h2d_bytes_per_step": nloc * 3 * 8,
-                    "d2h_bytes_per_step": (1 + 3 * nloc + 9) * 8},
+                    "d2h_bytes_per_step": (1 + 3 * nloc + 9) * 8,
+                    "call": "SeAEvaluator.run_pinned() (copies and step in one graph)",
+                    "compute_call_value": whole_job_us_per_atom(e2e_compute_ms, nloc, world)},
             "gpu_launches": None if launches_per_step is None else launches_per_step * args.steps,
             "clocks": clk,
             "roofline": roofline,

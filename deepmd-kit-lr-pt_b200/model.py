@@ -766,7 +766,53 @@ class SeAEvaluator:
         with torch.cuda.graph(self.graph):
             self.step()
         torch.cuda.synchronize()
+        self.io_graph = None  # recaptured by the next run_pinned()
         return self
+
+    # ---- one graph from pinned host input to pinned host output
+    def io_buffers(self):
+        """(coord [nloc, 3], results [1 + 3 nloc + 9]): pinned host buffers
+        of run_pinned(). Write the coordinates into ``coord``; after
+        run_pinned() ``results`` holds the energy, the forces (row-major) and
+        the virial, all FP64."""
+        if getattr(self, "h_coord", None) is None:
+            self.h_coord = torch.zeros((self.nloc, 3), dtype=torch.float64, pin_memory=True)
+            self.h_results = torch.zeros(1 + 3 * self.nloc + 9, dtype=torch.float64,
+                                         pin_memory=True)
+            self.io_graph = None
+        return self.h_coord, self.h_results
+
+    def run_pinned(self):
+        """One evaluation of the coordinates in io_buffers()[0] into
+        io_buffers()[1]: the host-to-device copy, the step and the
+        device-to-host copy of the results replayed as ONE CUDA graph, then
+        one synchronisation. (energy, force [nloc, 3], virial [9]) are
+        returned as views of the result buffer, valid until the next call.
+        For evaluators without a skin list (with one, use compute())."""
+        if self.skin > 0:
+            raise _capi.DPBInvalidArgument("run_pinned: evaluators with a skin list use compute()")
+        hc, hr = self.io_buffers()
+        if self.io_graph is None or getattr(self, "_recapture", False):
+            self._recapture = False
+            s = torch.cuda.Stream(device=self.dev)
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                for _ in range(2):
+                    self.coord.copy_(hc, non_blocking=True)
+                    self.step()
+                    hr.copy_(self.results, non_blocking=True)
+            torch.cuda.current_stream().wait_stream(s)
+            torch.cuda.synchronize()
+            self.io_graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.io_graph):
+                self.coord.copy_(hc, non_blocking=True)
+                self.step()
+                hr.copy_(self.results, non_blocking=True)
+            torch.cuda.synchronize()
+        self.io_graph.replay()
+        torch.cuda.current_stream().synchronize()
+        n = self.nloc
+        return hr[0:1], hr[1:1 + 3 * n].view(n, 3), hr[1 + 3 * n:]
 
     def tune(self, reps: int = 10, use_cache: bool = True) -> dict:
         """Autotune the launch shapes of this step (atoms per CTA of the fused

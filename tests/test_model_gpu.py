@@ -102,6 +102,27 @@ def test_graph_replay_equals_eager(mdl, gold, mode):
     np.testing.assert_allclose(V1, V0, rtol=1e-9 if mode == "plain" else 1e-5, atol=1e-9)
 
 
+@pytest.mark.parametrize("mode", ["compressed", "plain"])
+def test_run_pinned_equals_compute(mdl, gold, mode):
+    """The one-graph evaluation from pinned host input to pinned host output
+    (run_pinned) gives compute()'s results, for new coordinates written into
+    its input buffer between calls."""
+    p = _params(mdl, gold, "w192", tables=(mode == "compressed"))
+    ev = mdl.SeAEvaluator(p, gold["w192:atype"], gold["w192:box"], mode=mode)
+    hc, hr = ev.io_buffers()
+    rng = np.random.default_rng(5)
+    for k in range(3):
+        c = gold["w192:coord"] + rng.normal(scale=0.01, size=gold["w192:coord"].shape) * k
+        hc.copy_(torch.tensor(c))
+        E, F, V = ev.run_pinned()
+        E0, F0, V0 = ev.compute(c)
+        tol = 1e-12 if mode == "plain" else 1e-6
+        assert abs(float(E[0]) - E0) <= tol * abs(E0)
+        np.testing.assert_allclose(F.numpy(), F0, atol=1e-9 if mode == "plain" else 1e-6)
+        np.testing.assert_allclose(V.numpy(), V0, rtol=1e-9 if mode == "plain" else 1e-5,
+                                   atol=1e-9)
+
+
 def _quintic_close(a, b, rows, info, M):
     """a0..a2 to 1e-12 and the quintic to 1e-12 across each interval (a3..a5
     carry the cancellation of their formulas, divided by up to h^5)."""
