@@ -48,10 +48,6 @@ struct GemmCfg {
 // per row block leaves 52 SMs idle), 160-column tiles for N = 1600 (half the
 // A re-reads).
 using CfgN80 = GemmCfg<80, 4, 4, 2, 4>;
-// the same with 8 epilogue warps (two per TMEM lane quadrant): the short-K
-// layers' epilogue (tanh, residual, stores of 80 columns a row) is half
-// their time with 4 (knob fit_epi_warps)
-using CfgN80E8 = GemmCfg<80, 4, 4, 2, 8>;
 using CfgN160 = GemmCfg<160, 4, 2, 2, 8>;
 // one 240-column tile per 128 rows (one accumulator, two stages): for the
 // short-K 240 x 240 layers, one wave instead of two over the row tiles

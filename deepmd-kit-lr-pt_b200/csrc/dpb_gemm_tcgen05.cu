@@ -129,8 +129,6 @@ static int launch(const GemmMaps& maps, GemmShape shp, const GemmEpi& epi, int* 
       shp.kchunk = P;
       return launch_c<C, true>(maps, shp, epi, status, st);
     }
-    if (tune_value("fit_epi_warps", 4) == 8)
-      return launch_c<CfgN80E8, false>(maps, shp, epi, status, st);
   }
   return launch_c<CFG, false>(maps, shp, epi, status, st);
 }

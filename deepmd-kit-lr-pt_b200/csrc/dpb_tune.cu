@@ -49,8 +49,6 @@ static Knob g_knobs[] = {
     {"fit_kchunk_cross_first", 0, 2, {0, 1}},
     // chunked accumulation only for K at least this (shorter sums drift less)
     {"fit_kchunk_min_k", 0, 2, {0, 512}},
-    // epilogue warps of the unchunked 80-column GEMM tiles (short-K layers)
-    {"fit_epi_warps", 4, 2, {4, 8}},
     // warps (one center atom each) per CTA of the batched env / force kernels
     {"batch_atoms_per_cta", 4, 3, {2, 4, 8}},
     // batched-frames step: 1 one persistent cooperative launch

@@ -106,19 +106,9 @@ def test_gemm_weight_split_in_kernel_is_exact(dpb, mdl, M, K, N, rows, mode):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("epi_warps", [4, 8])
 @pytest.mark.parametrize("N", [240, 320, 400])  # tiles of 80, 160 and 80 columns
-def test_gemm_epilogues(dpb, mdl, N, epi_warps):
-    """Every fused epilogue, with 4 or 8 epilogue warps on the 80-column
-    tiles (knob fit_epi_warps)."""
-    from deepmd_kit_lr_pt_b200 import autotune
-
-    old = autotune.get("fit_epi_warps")
-    autotune.set_knob("fit_epi_warps", epi_warps)
-    try:
-        _check_epilogues(dpb, mdl, N)
-    finally:
-        autotune.set_knob("fit_epi_warps", old)
+def test_gemm_epilogues(dpb, mdl, N):
+    _check_epilogues(dpb, mdl, N)
 
 
 def _check_epilogues(dpb, mdl, N):
