@@ -52,7 +52,7 @@ __device__ __forceinline__ void bt_cells_frame(int f, double* __restrict__ cw,
 }
 
 struct BtEnvSmem {
-  unsigned long long keys[BT_CAP];
+  __align__(16) unsigned long long keys[BT_CAP];  // read two at a time by the ranking
   int row[BT_NMAX];
   int tcnt[32];
 };
@@ -191,7 +191,13 @@ __device__ __forceinline__ void bt_env_row(int row, int lane, BtEnvSmem& sm,
     const int kk = q * 32 + lane;
     const unsigned long long own = kk < n ? sm.keys[kk] : ~0ull;
     int r = 0;
-    for (int p = 0; p < n; ++p) r += sm.keys[p] < own ? 1 : 0;
+    const ulonglong2* k2 = reinterpret_cast<const ulonglong2*>(sm.keys);
+    int p = 0;
+    for (; 2 * p + 1 < n; ++p) {  // two keys per 16-byte load (broadcast)
+      const ulonglong2 v = k2[p];
+      r += (v.x < own ? 1 : 0) + (v.y < own ? 1 : 0);
+    }
+    if (2 * p < n) r += sm.keys[2 * p] < own ? 1 : 0;
     const int t = (int)(own >> 56) & 31;
     const int ts = __shfl_sync(0xffffffffu, tstart, t);
     if (kk < n) {

@@ -119,7 +119,7 @@ __device__ __forceinline__ void store_env_row<float>(float* e, const float* a, c
 // Shared-memory workspace of one warp (one center atom).
 template <int CAP>
 struct EnvSmem {
-  unsigned long long keys[CAP];
+  __align__(16) unsigned long long keys[CAP];  // read two at a time by the ranking
   int row[NMAX];
   int tcnt[MAXT];
 };
@@ -277,7 +277,14 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
     int kk = q * 32 + lane;
     unsigned long long own = kk < n ? keys[kk] : ~0ull;
     int r = 0;
-    for (int p = 0; p < n; ++p) r += keys[p] < own ? 1 : 0;
+    // two keys per 16-byte shared-memory load (broadcast to the warp)
+    const ulonglong2* k2 = reinterpret_cast<const ulonglong2*>(keys);
+    int p = 0;
+    for (; 2 * p + 1 < n; ++p) {
+      const ulonglong2 v = k2[p];
+      r += (v.x < own ? 1 : 0) + (v.y < own ? 1 : 0);
+    }
+    if (2 * p < n) r += keys[2 * p] < own ? 1 : 0;
     int t = (int)(own >> 56) & 31;
     int ts = __shfl_sync(0xffffffffu, tstart, t);
     if (kk < n) {
