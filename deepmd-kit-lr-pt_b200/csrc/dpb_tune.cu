@@ -54,6 +54,9 @@ static Knob g_knobs[] = {
     // batched-frames step: 1 one persistent cooperative launch
     // (dpb_bt_step_launch), 0 one launch per stage
     {"batch_fused", 0, 2, {0, 1}},
+    // knots of the cubic re-interpolated tables every this many fine strides
+    // of the reference's table (read by the host when it builds the tables)
+    {"table_cubic_stride", 1, 2, {1, 2}},
     // one-launch step: 1 the env rows and the descriptor forward (the
     // descriptor backward and the forces) as separate passes, 0 back to back
     // per row in one pass

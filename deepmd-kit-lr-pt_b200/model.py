@@ -224,7 +224,12 @@ class PipelineTables:
         s = torch.cuda.current_stream(dev).cuda_stream
         for t, info in params.tables:
             if degree == 3:
-                cub = table_mod.cubic_table(t, info)
+                # knots every table_cubic_stride fine strides (knob; 1: the
+                # reference's fine stride)
+                m = int(_capi.lib().dpb_tune_get(b"table_cubic_stride"))
+                cub = table_mod.cubic_table(t, info, m)
+                if cub is None and m > 1:
+                    cub = table_mod.cubic_table(t, info)
                 if cub is None:
                     raise _capi.DPBInvalidArgument(
                         "table_degree 3 needs stride1 to be a whole multiple of stride0")

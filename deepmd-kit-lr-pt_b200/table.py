@@ -174,7 +174,7 @@ def build_tables_device(emb_layers, davg, dstd, sel, min_nbor_dist: float, rcut_
 
 
 
-def cubic_table(table: np.ndarray, info: np.ndarray):
+def cubic_table(table: np.ndarray, info: np.ndarray, stride_mult: int = 1):
     """The compressed embedding of one table re-interpolated by a cubic
     Hermite polynomial on the fine stride everywhere, for the fused
     descriptor kernels (dpb_se_a_descriptor_*_cubic_f32): the quintic rows
@@ -188,17 +188,24 @@ def cubic_table(table: np.ndarray, info: np.ndarray):
     FP32 resolution); loading 4 coefficients per channel instead of 6 cuts
     the table bytes every neighbor slot gathers by a third.
 
+    With stride_mult m > 1 the knots are every m fine strides (h = m
+    stride0; m must divide both the fine-region knot count and stride1 /
+    stride0): half or fewer table rows, at an interpolation error m^4 times
+    larger.
+
     Returns (coefficients [K + 1, 4, M] float64, coefficient-major rows with
     a last guard row [y(max), y'(max), 0, 0] for the linear extrapolation
-    beyond max; info [lower, max, max, stride0, stride0, K]), or None when
-    the strides do not nest (stride1 not a whole multiple of stride0)."""
+    beyond max; info [lower, max, max, h, h, K]), or None when the strides do
+    not nest (stride1 not a whole multiple of stride0, or not of h)."""
     lower, upper, mx, s0, s1 = (float(v) for v in info[:5])
     first = int(round((upper - lower) / s0))
     ratio = int(round(s1 / s0))
     n1 = int(round((mx - upper) / s1))
     M = table.shape[1] // 6
+    m = int(stride_mult)
     if (ratio < 1 or abs(ratio * s0 - s1) > 1e-9 * s1 or abs(first * s0 - (upper - lower)) >
-            1e-9 * max(1.0, abs(upper - lower)) or first + n1 != table.shape[0]):
+            1e-9 * max(1.0, abs(upper - lower)) or first + n1 != table.shape[0] or m < 1 or
+            first % m or ratio % m):
         return None
     T = np.asarray(table, np.float64).reshape(-1, M, 6)
     K = first + n1 * ratio
@@ -221,7 +228,9 @@ def cubic_table(table: np.ndarray, info: np.ndarray):
         y[first + j:K:ratio] = v
         d[first + j:K:ratio] = g
     y[K], d[K] = poly(T[-1], s1)
-    h = s0
+    if m > 1:  # every m-th knot
+        y, d, K = y[::m], d[::m], K // m
+    h = s0 * m
     C = np.zeros((K + 1, 4, M))
     C[:K, 0] = y[:K]
     C[:K, 1] = d[:K]
@@ -229,4 +238,4 @@ def cubic_table(table: np.ndarray, info: np.ndarray):
     C[:K, 3] = (2.0 * (y[:K] - y[1:]) / h + d[:K] + d[1:]) / (h * h)
     C[K, 0] = y[K]
     C[K, 1] = d[K]
-    return C, np.array([lower, mx, mx, s0, s0, float(K)])
+    return C, np.array([lower, mx, mx, h, h, float(K)])

@@ -26,30 +26,33 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / max(1e-30, np.abs(b).max()))
 
 
-def test_cubic_table_matches_quintic_on_host(mods):
+@pytest.mark.parametrize("m,tol", [(1, 1e-7), (2, 2e-6)])
+def test_cubic_table_matches_quintic_on_host(mods, m, tol):
     """table.cubic_table reproduces the quintic's value and slope at every
-    knot exactly and stays within 1e-7 of |G| between knots (FP64, host)."""
+    knot exactly and stays within 1e-7 of |G| between knots on the fine
+    stride (2e-6 with knots every two fine strides) (FP64, host)."""
     wl, mdl, tab, _ = mods
     coord, atype, box = wl.water_frame(4, seed=0)
     p = mdl.prepare(mdl.init_params(mdl.SeAConfig(), seed=1), coord, atype, box)
     rng = np.random.default_rng(0)
     for table, info in p.tables:
-        C, ic = tab.cubic_table(table, info)
+        C, ic = tab.cubic_table(table, info, m)
         lower, upper, mx, s0, s1 = info[:5]
         M = table.shape[1] // 6
         T = table.reshape(-1, M, 6)
         first = int(round((upper - lower) / s0))
         K = int(ic[5])
-        assert C.shape == (K + 1, 4, M) and ic[1] == mx and ic[3] == s0
+        h = s0 * m
+        assert C.shape == (K + 1, 4, M) and ic[1] == mx and abs(ic[3] - h) < 1e-15
         x = np.concatenate([rng.uniform(lower, upper, 300), rng.uniform(upper, mx, 300)])
         for xv in x:
             r = first + int((xv - upper) / s1) if xv >= upper else int((xv - lower) / s0)
             t = xv - (upper + (r - first) * s1 if xv >= upper else lower + r * s0)
             q = sum(T[r, :, k] * t ** k for k in range(6))
-            rc = min(int((xv - lower) / s0), K)
-            tc = xv - (lower + rc * s0)
+            rc = min(int((xv - lower) / h), K)
+            tc = xv - (lower + rc * h)
             c = C[rc, 0] + tc * (C[rc, 1] + tc * (C[rc, 2] + tc * C[rc, 3]))
-            assert np.abs(c - q).max() <= 1e-7 * max(1.0, np.abs(q).max()), xv
+            assert np.abs(c - q).max() <= tol * max(1.0, np.abs(q).max()), xv
 
 
 def test_cubic_descriptor_matches_quintic(mods):
