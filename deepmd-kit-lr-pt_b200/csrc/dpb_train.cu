@@ -82,6 +82,8 @@ struct TrLayout {
   int w_off, acc_off, warp_off, warp_sz;
   int o_rr, o_rd, o_mu, o_s, o_sd, o_A1, o_At1, o_A2, o_At2, o_Zt2, o_big;
   int wsmem;         // weights staged in shared memory
+  int sacc;          // reverse pass: one gradient copy per block (shared-memory
+                     // atomics) instead of one per warp
 };
 
 struct TrGeom {
@@ -1058,7 +1060,12 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
   const int res3 = N1 > 0 ? tr_res_kind(N3, N2) : net.res3;
   const int sw2 = WS ? (n2 | 1) : n2, sw3 = WS ? (n3 | 1) : n3;
   const int s2 = n2 | 1, s3 = n3 | 1;  // gradient copies: the staged layout
-  T* gacc = tb + lay.acc_off + (size_t)w * lay.pw;  // this warp's gradient copy
+  // this warp's gradient copy, or the block's (lay.sacc: updated atomically)
+  T* gacc = tb + lay.acc_off + (lay.sacc ? (size_t)0 : (size_t)w * lay.pw);
+  auto gadd = [&](T* p, T v) {
+    if (lay.sacc) atomicAdd(p, v);
+    else *p += v;
+  };
   T* gW1 = gacc;
   T* gb1 = gW1 + n1;
   T* gW2 = gb1 + n1;
@@ -1078,7 +1085,10 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
       one.b[0][2] = net.b[t][2];
       tr_stage_weights(sw, one, lay, 1);
     }
-    for (int e = lane; e < lay.pw; e += 32) gacc[e] = (T)0;
+    if (lay.sacc)
+      for (int e = threadIdx.x; e < lay.pw; e += blockDim.x) gacc[e] = (T)0;
+    else
+      for (int e = lane; e < lay.pw; e += 32) gacc[e] = (T)0;
     __syncthreads();
     const WV<T> W = tr_wview<T, WS>(net, sw, WS ? 0 : t, lay.pw, n1, n2, sw2, sw3);
     for (int row = blockIdx.x * lay.nw + w; row < g.nrows; row += gw) {
@@ -1187,7 +1197,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
               stg_store<T, R>(Zbt3, c, acd[j]);
               stg_store<T, R>(Gb, c, gv);
               stg_store<T, R>(Gbt, c, gvt);
-              gb3[c] += zsum;
+              gadd(&gb3[c], zsum);
             }
           }
           // W3 gradient: sum_r A2[i][r] zb[c][r] + At2[i][r] zbd[c][r]
@@ -1202,7 +1212,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
                 T s = (T)0;
 #pragma unroll
                 for (int r = 0; r < R; ++r) s = fma(a[r], acc[j][r], fma(ad[r], acd[j][r], s));
-                gW3[i * s3 + c] += s;
+                gadd(&gW3[i * s3 + c], s);
               }
             }
           }
@@ -1232,7 +1242,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
               zb2[j][r] = (hb2[j][r] - (T)2 * y * zt[r] * hbd2[j][r]) * q;
               zsum += zb2[j][r];
             }
-            gb2[i] += zsum;
+            gadd(&gb2[i], zsum);
           } else {
 #pragma unroll
             for (int r = 0; r < R; ++r) zb2[j][r] = zbd2[j][r] = hb2[j][r] = hbd2[j][r] = (T)0;
@@ -1249,7 +1259,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
               T s = (T)0;
 #pragma unroll
               for (int r = 0; r < R; ++r) s = fma(a[r], zb2[j][r], fma(ad[r], zbd2[j][r], s));
-              gW2[k * s2 + i] += s;
+              gadd(&gW2[k * s2 + i], s);
             }
           }
         }
@@ -1292,8 +1302,8 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
               gws = fma(ss[r], zb, fma(sd[r], zbd, gws));
               gbs += zb;
             }
-            gW1[lane] += gws;
-            gb1[lane] += gbs;
+            gadd(&gW1[lane], gws);
+            gadd(&gb1[lane], gbs);
           }
         }
         __syncwarp();
@@ -1304,7 +1314,7 @@ k_tr_rev(TrGrad<T> grad, const T* __restrict__ xbar, const T* __restrict__ xbard
     const T* accb = tb + lay.acc_off;
     auto sumw = [&](int e) {
       T s = (T)0;
-      for (int k = 0; k < lay.nw; ++k) s += accb[(size_t)k * lay.pw + e];
+      for (int k = 0; k < (lay.sacc ? 1 : lay.nw); ++k) s += accb[(size_t)k * lay.pw + e];
       return s;
     };
     for (int k = threadIdx.x; k < n1; k += blockDim.x) {
@@ -1541,9 +1551,11 @@ struct TrDims {
 enum TrKind { TR_FWD, TR_BWD, TR_TAN, TR_REV };
 
 template <typename T>
-static TrLayout tr_layout(TrKind kind, int R, const TrDims& d, bool wsmem, int nw) {
+static TrLayout tr_layout(TrKind kind, int R, const TrDims& d, bool wsmem, int nw,
+                          bool sacc = false) {
   TrLayout L{};
   L.nw = nw;
+  L.sacc = kind == TR_REV && sacc ? 1 : 0;
   L.ints_warp = (d.nnei + TR_MAXT + 1 + 3) & ~3;
   L.s2 = d.n2 | 1;
   L.s3 = d.n3 | 1;
@@ -1551,9 +1563,9 @@ static TrLayout tr_layout(TrKind kind, int R, const TrDims& d, bool wsmem, int n
   L.pw = (2 * d.n1 + d.n1 * L.s2 + d.n2 + d.n2 * L.s3 + d.n3 + 3) & ~3;
   L.wsmem = wsmem ? 1 : 0;
   L.w_off = 0;
-  if (kind == TR_REV) {  // one type's weights, then a gradient copy per warp
+  if (kind == TR_REV) {  // one type's weights, then a gradient copy per warp (or block)
     L.acc_off = wsmem ? L.pw : 0;
-    L.warp_off = L.acc_off + nw * L.pw;
+    L.warp_off = L.acc_off + (L.sacc ? 1 : nw) * L.pw;
   } else {
     L.acc_off = wsmem ? d.ntypes * L.pw : 0;
     L.warp_off = L.acc_off;
@@ -1688,9 +1700,9 @@ static int tr_launch_cfg(K kernel, const TrLayout& L, size_t tsize, int nrows, i
 }
 
 template <typename T>
-static int tr_pick_warps(TrKind kind, const TrDims& d, int maxw, int R) {
+static int tr_pick_warps(TrKind kind, const TrDims& d, int maxw, int R, bool sacc) {
   for (int nw = maxw; nw >= 1; --nw) {
-    const TrLayout L = tr_layout<T>(kind, R, d, TrTraits<T>::WSMEM, nw);
+    const TrLayout L = tr_layout<T>(kind, R, d, TrTraits<T>::WSMEM, nw, sacc);
     if (tr_smem_bytes(L, sizeof(T)) <= 227 * 1024) return nw;
   }
   return 0;
@@ -1728,13 +1740,17 @@ static int tr_prepare(TrKind kind, TrNet<T>& net, TrGeom& g, TrLayout& L, int& R
   }
   const TrDims d{net.n1, net.n2, net.n3, ax, g.nnei, g.ntypes};
   R = tr_rows(net, kind);
-  const int maxw = std::min(tune_value("train_warps_per_cta", 8), kind == TR_REV ? 4 : 8);
-  const int nw = tr_pick_warps<T>(kind, d, maxw, R);
+  // the reverse pass: a gradient copy per warp (at most 4 warps fit), or one
+  // per block updated with shared-memory atomics (up to 8 warps)
+  const bool sacc = kind == TR_REV && tune_value("train_rev_shared_acc", 1) != 0;
+  const int maxw =
+      std::min(tune_value("train_warps_per_cta", 8), kind == TR_REV && !sacc ? 4 : 8);
+  const int nw = tr_pick_warps<T>(kind, d, maxw, R, sacc);
   if (nw < 1) {
     set_error("se_a_train: the network does not fit in shared memory");
     return DPB_ERR_INVALID;
   }
-  L = tr_layout<T>(kind, R, d, TrTraits<T>::WSMEM, nw);
+  L = tr_layout<T>(kind, R, d, TrTraits<T>::WSMEM, nw, sacc);
   return DPB_OK;
 }
 

@@ -96,12 +96,23 @@ def test_fp64_gradient_matches_reference_autograd(mods, case, golden):
     check_against_golden(golden, grads, rtol=1e-8, atol=1e-9)
 
 
-def test_fp64_gradient_matches_oracle_every_entry(mods, case, golden):
+@pytest.mark.parametrize("shared_acc", [0, 1])
+def test_fp64_gradient_matches_oracle_every_entry(mods, case, golden, shared_acc):
+    """Every gradient entry against the oracle, with the reverse kernel's
+    weight gradients in one copy per warp or one per block (shared-memory
+    atomics, knob train_rev_shared_acc)."""
     from oracle import model_ref, oracle
 
+    from deepmd_kit_lr_pt_b200 import autotune
+
     params, frames, labels, _ = case
-    t = _trainer(mods, case, torch.float64)
-    _, g = _autograd_grads(t, case[3])
+    old = autotune.get("train_rev_shared_acc")
+    autotune.set_knob("train_rev_shared_acc", shared_acc)
+    try:
+        t = _trainer(mods, case, torch.float64)
+        _, g = _autograd_grads(t, case[3])
+    finally:
+        autotune.set_knob("train_rev_shared_acc", old)
     _, _, _, _, ref = model_ref.train_loss_grads(oracle.port(), params, frames, labels,
                                                  tuple(golden["prefs"]))
     for name, v in t.named_grads(g).items():
