@@ -81,6 +81,12 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
     os.replace(LIB + ".tmp", LIB)
+    # drop the objects of earlier source versions: the cache holds one object
+    # per source file
+    keep = set(objs)
+    for old in glob.glob(os.path.join(BUILD, "*.o")):
+        if old not in keep:
+            os.remove(old)
     return LIB
 
 

@@ -187,6 +187,18 @@ __device__ __forceinline__ void mma_tf32_ta(uint32_t tmem_d, uint32_t tmem_a, ui
       "r"(0u), "r"(0u));
 }
 
+// one lane of a converged warp (elect.sync): the lane that issues the
+// warp's tcgen05 / TMA instructions
+__device__ __forceinline__ bool elect_one() {
+  uint32_t p;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\t"
+      "elect.sync _|P, 0xffffffff;\n\t"
+      "selp.b32 %0, 1, 0, P;\n\t}"
+      : "=r"(p));
+  return p != 0;
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -313,20 +325,26 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   volatile int* abort = &abort_flag;
 
+  // The producer and MMA warps run their loops with all 32 lanes, so every
+  // stage index, barrier phase, descriptor and TMEM address is warp-uniform
+  // and stays in uniform registers; one elected lane issues the TMA copies,
+  // MMAs and commits. Measured on the K = 1600 layer: a loop run by lane 0
+  // alone spent ~80 cycles per tcgen05.mma (its operands moved into uniform
+  // registers instruction by instruction), the warp-uniform loop ~10.
   if (warp == 0) {
     // ---------------------------------------------------------------- TMA
-    if (lane == 0) {
-      int g = 0;  // k-blocks issued over all tiles
-      bool ok = true;
-      for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x) {
-        const TileCoord tc = tile_coord(shp, t, BN);
-        for (int kb = 0; kb < nk; ++kb, ++g) {
-          const int s = g % STAGES;
-          const uint32_t ph = (g / STAGES) & 1;
-          if (!mbar_wait(&empty_bar[s], ph ^ 1, abort)) {
-            ok = false;
-            break;
-          }
+    int g = 0;  // k-blocks issued over all tiles
+    bool ok = true;
+    for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x) {
+      const TileCoord tc = tile_coord(shp, t, BN);
+      for (int kb = 0; kb < nk; ++kb, ++g) {
+        const int s = g % STAGES;
+        const uint32_t ph = (g / STAGES) & 1;
+        if (!__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], ph ^ 1, abort))) {
+          ok = false;
+          break;
+        }
+        if (elect_one()) {
           unsigned char* st = smem + s * STAGE_BYTES;
           mbar_expect_tx(&full_bar[s], A_BYTES + (shp.split_b ? 1 : 2) * B_BYTES);
           tma_load_2d(st, &maps.a, &full_bar[s], kb * GT_BK, tc.row0);
@@ -335,21 +353,23 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
             tma_load_2d(st + A_BYTES + B_BYTES, &maps.bl[tc.ty], &full_bar[s], kb * GT_BK,
                         tc.n0);
         }
+        __syncwarp();
       }
-      if (!ok) {
-        // let the copies already in flight land before the CTA's shared
-        // memory is released (bounded, like every other wait here)
-        for (int q = g - STAGES < 0 ? 0 : g - STAGES; q < g; ++q) {
-          const int s = q % STAGES;
-          for (unsigned it = 0; it < GT_WAIT_LIMIT; ++it)
-            if (mbar_try(&full_bar[s], (q / STAGES) & 1)) break;
-        }
+    }
+    if (!ok) {
+      // let the copies already in flight land before the CTA's shared
+      // memory is released (bounded, like every other wait here)
+      for (int q = g - STAGES < 0 ? 0 : g - STAGES; q < g; ++q) {
+        const int s = q % STAGES;
+        for (unsigned it = 0; it < GT_WAIT_LIMIT; ++it)
+          if (mbar_try(&full_bar[s], (q / STAGES) & 1)) break;
       }
     }
     __syncwarp();
   } else if (warp == 1) {
     // ---------------------------------------------------------------- MMA
-    if (lane == 0 && CHUNK) {
+    bool ok = true, issued = false;
+    if constexpr (CHUNK) {
       // Chunked accumulation: every kchunk k-blocks start a fresh accumulator
       // (the epilogue adds the chunks in FP32 on the CUDA cores), and within
       // a chunk the small cross products (Al Bh, Ah Bl, Al Bl) go in first,
@@ -359,11 +379,11 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
       // alike (the atoms of a crystal) that loss would not average out.
       const int P = shp.kchunk;
       int g = 0, cc = 0;
-      bool ok = true;
       for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x) {
         for (int kb0 = 0; kb0 < nk && ok; kb0 += P, ++cc) {
           const int b = cc % ACCBUF;
-          if (!mbar_wait(&tempty_bar[b], ((cc / ACCBUF) & 1) ^ 1, abort)) {
+          if (!__all_sync(0xffffffffu,
+                          mbar_wait(&tempty_bar[b], ((cc / ACCBUF) & 1) ^ 1, abort))) {
             ok = false;
             break;
           }
@@ -372,7 +392,7 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
           const int nkc = nk - kb0 < P ? nk - kb0 : P;
           for (int i = 0; i < nkc; ++i) {  // pass 1: cross products
             const int gi = g + i, s = gi % STAGES, as = gi % ASLOTS;
-            if (!mbar_wait(&conv_bar[s], (gi / STAGES) & 1, abort)) {
+            if (!__all_sync(0xffffffffu, mbar_wait(&conv_bar[s], (gi / STAGES) & 1, abort))) {
               ok = false;
               break;
             }
@@ -381,48 +401,50 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
             const uint32_t ah = tmem + TM_A0 + 64u * (uint32_t)as, al = ah + 32u;
             const uint64_t bh = smem_desc(st + A_BYTES);
             const uint64_t bl = smem_desc(st + A_BYTES + B_BYTES);
+            if (elect_one()) {
 #pragma unroll
-            for (int j = 0; j < GT_BK / 8; ++j) {
-              const uint32_t ca = 8u * (uint32_t)j;
-              const uint64_t ob = (uint64_t)(j * 32) >> 4;
-              mma_tf32_ta(d, al + ca, bh + ob, IDESC, (i > 0 || j > 0) ? 1u : 0u);
-              mma_tf32_ta(d, ah + ca, bl + ob, IDESC, 1u);
-              if (shp.terms == 4) mma_tf32_ta(d, al + ca, bl + ob, IDESC, 1u);
-              if (!shp.cross_first) mma_tf32_ta(d, ah + ca, bh + ob, IDESC, 1u);
+              for (int j = 0; j < GT_BK / 8; ++j) {
+                const uint32_t ca = 8u * (uint32_t)j;
+                const uint64_t ob = (uint64_t)(j * 32) >> 4;
+                mma_tf32_ta(d, al + ca, bh + ob, IDESC, (i > 0 || j > 0) ? 1u : 0u);
+                mma_tf32_ta(d, ah + ca, bl + ob, IDESC, 1u);
+                if (shp.terms == 4) mma_tf32_ta(d, al + ca, bl + ob, IDESC, 1u);
+                if (!shp.cross_first) mma_tf32_ta(d, ah + ca, bh + ob, IDESC, 1u);
+              }
+              if (!shp.cross_first) {  // k-block order: its stage is free once read
+                mma_commit(&empty_bar[s]);
+                mma_commit(&afree_bar[as]);
+              }
             }
-            if (!shp.cross_first) {  // k-block order: its stage is free once read
+            __syncwarp();
+            issued = true;
+          }
+          if (!ok) break;
+          if (elect_one()) {
+            for (int i = 0; i < nkc && shp.cross_first; ++i) {  // pass 2: Ah Bh
+              const int gi = g + i, s = gi % STAGES, as = gi % ASLOTS;
+              unsigned char* st = smem + s * STAGE_BYTES;
+              const uint32_t ah = tmem + TM_A0 + 64u * (uint32_t)as;
+              const uint64_t bh = smem_desc(st + A_BYTES);
+#pragma unroll
+              for (int j = 0; j < GT_BK / 8; ++j)
+                mma_tf32_ta(d, ah + 8u * (uint32_t)j, bh + ((uint64_t)(j * 32) >> 4), IDESC,
+                            1u);
               mma_commit(&empty_bar[s]);
               mma_commit(&afree_bar[as]);
             }
+            mma_commit(&tfull_bar[b]);  // chunk accumulator b complete
           }
-          if (!ok) break;
-          for (int i = 0; i < nkc && shp.cross_first; ++i) {  // pass 2: Ah Bh
-            const int gi = g + i, s = gi % STAGES, as = gi % ASLOTS;
-            unsigned char* st = smem + s * STAGE_BYTES;
-            const uint32_t ah = tmem + TM_A0 + 64u * (uint32_t)as;
-            const uint64_t bh = smem_desc(st + A_BYTES);
-#pragma unroll
-            for (int j = 0; j < GT_BK / 8; ++j)
-              mma_tf32_ta(d, ah + 8u * (uint32_t)j, bh + ((uint64_t)(j * 32) >> 4), IDESC, 1u);
-            mma_commit(&empty_bar[s]);
-            mma_commit(&afree_bar[as]);
-          }
+          __syncwarp();
           g += nkc;
-          mma_commit(&tfull_bar[b]);  // chunk accumulator b complete
         }
       }
-      if (!ok) *abort = 1;
-      if (g > 0) {  // a CTA without tiles (grid wider than the tiles) issued nothing
-        mma_commit(drain);
-        for (unsigned it = 0; it < GT_WAIT_LIMIT; ++it)
-          if (mbar_try(drain, 0)) break;
-      }
-    } else if (lane == 0) {
+    } else {
       int g = 0, lt = 0;
-      bool ok = true;
       for (int t = blockIdx.x; t < n_total && ok; t += gridDim.x, ++lt) {
         const int b = lt % ACCBUF;
-        if (!mbar_wait(&tempty_bar[b], ((lt / ACCBUF) & 1) ^ 1, abort)) {
+        if (!__all_sync(0xffffffffu,
+                        mbar_wait(&tempty_bar[b], ((lt / ACCBUF) & 1) ^ 1, abort))) {
           ok = false;
           break;
         }
@@ -431,7 +453,7 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
         for (int kb = 0; kb < nk; ++kb, ++g) {
           const int s = g % STAGES;
           const uint32_t ph = (g / STAGES) & 1;
-          if (!mbar_wait(&conv_bar[s], ph, abort)) {
+          if (!__all_sync(0xffffffffu, mbar_wait(&conv_bar[s], ph, abort))) {
             ok = false;
             break;
           }
@@ -441,29 +463,36 @@ __device__ __forceinline__ void gemm_run(const GemmMaps& maps, const GemmShape& 
           const uint32_t ah = tmem + TM_A0 + 64u * (uint32_t)as, al = ah + 32u;
           const uint64_t bh = smem_desc(st + A_BYTES);
           const uint64_t bl = smem_desc(st + A_BYTES + B_BYTES);
+          if (elect_one()) {
 #pragma unroll
-          for (int j = 0; j < GT_BK / 8; ++j) {  // K = 8 per instruction
-            const uint32_t ca = 8u * (uint32_t)j;           // TMEM columns
-            const uint64_t ob = (uint64_t)(j * 32) >> 4;    // +32 B in the swizzled row
-            const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
-            mma_tf32_ta(d, ah + ca, bh + ob, IDESC, acc);
-            mma_tf32_ta(d, al + ca, bh + ob, IDESC, 1u);
-            mma_tf32_ta(d, ah + ca, bl + ob, IDESC, 1u);
-            if (shp.terms == 4) mma_tf32_ta(d, al + ca, bl + ob, IDESC, 1u);
+            for (int j = 0; j < GT_BK / 8; ++j) {  // K = 8 per instruction
+              const uint32_t ca = 8u * (uint32_t)j;           // TMEM columns
+              const uint64_t ob = (uint64_t)(j * 32) >> 4;    // +32 B in the swizzled row
+              const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
+              mma_tf32_ta(d, ah + ca, bh + ob, IDESC, acc);
+              mma_tf32_ta(d, al + ca, bh + ob, IDESC, 1u);
+              mma_tf32_ta(d, ah + ca, bl + ob, IDESC, 1u);
+              if (shp.terms == 4) mma_tf32_ta(d, al + ca, bl + ob, IDESC, 1u);
+            }
+            mma_commit(&empty_bar[s]);    // frees the shared-memory stage once read
+            mma_commit(&afree_bar[as]);   // and the TMEM A slot
           }
-          mma_commit(&empty_bar[s]);    // frees the shared-memory stage once read
-          mma_commit(&afree_bar[as]);   // and the TMEM A slot
+          __syncwarp();
+          issued = true;
         }
         if (!ok) break;
-        mma_commit(&tfull_bar[b]);  // accumulator b complete
+        if (elect_one()) mma_commit(&tfull_bar[b]);  // accumulator b complete
+        __syncwarp();
       }
-      if (!ok) *abort = 1;
-      // every MMA issued by this thread has completed before teardown
-      if (g > 0) {
-        mma_commit(drain);
-        for (unsigned it = 0; it < GT_WAIT_LIMIT; ++it)
-          if (mbar_try(drain, 0)) break;
-      }
+    }
+    if (!ok && lane == 0) *abort = 1;
+    // every MMA issued by this warp has completed before teardown (a CTA
+    // without tiles, when the grid is wider than the tiles, issued nothing)
+    if (issued) {
+      if (elect_one()) mma_commit(drain);
+      __syncwarp();
+      for (unsigned it = 0; it < GT_WAIT_LIMIT; ++it)
+        if (mbar_try(drain, 0)) break;
     }
     __syncwarp();
   } else if (warp < 6) {
