@@ -301,20 +301,26 @@ __device__ __forceinline__ void desc_fwd_atom(int i, int lane, float* wsm, float
     const float4* E = se + s0;
     const float4* Ls = sl + s0;
     auto rep = [&](int q) { return q == brk ? (float)(nt - q) : 1.f; };
-    auto row = [&](int q) { return tab + (size_t)__float_as_int(Ls[q].x) * rs; };
+    auto row = [&](const float4& L) { return tab + (size_t)__float_as_int(L.x) * rs; };
     // two coefficient buffers in turn: the next slot's row is in flight while
     // the current one is evaluated (reusing a row shared by consecutive slots
     // saves L1 traffic but costs the prefetch distance, a net loss measured
-    // on 12k-atom water)
-    Coef4<NC> ca = load_coef4<CH, NC>(row(0), M), cb;
+    // on 12k-atom water); each buffer keeps the staged table coordinates of
+    // its slot, read from shared memory once
+    float4 La = Ls[0], Lb;
+    Coef4<NC> ca = load_coef4<CH, NC>(row(La), M), cb;
     int q = 0;
     for (; q + 1 <= last; q += 2) {
-      cb = load_coef4<CH, NC>(row(q + 1), M);
-      fwd_slot<NC>(acc01, acc23, ca, E[q], Ls[q], rep(q));
-      if (q + 2 <= last) ca = load_coef4<CH, NC>(row(q + 2), M);
-      fwd_slot<NC>(acc01, acc23, cb, E[q + 1], Ls[q + 1], rep(q + 1));
+      Lb = Ls[q + 1];
+      cb = load_coef4<CH, NC>(row(Lb), M);
+      fwd_slot<NC>(acc01, acc23, ca, E[q], La, rep(q));
+      if (q + 2 <= last) {
+        La = Ls[q + 2];
+        ca = load_coef4<CH, NC>(row(La), M);
+      }
+      fwd_slot<NC>(acc01, acc23, cb, E[q + 1], Lb, rep(q + 1));
     }
-    if (q <= last) fwd_slot<NC>(acc01, acc23, ca, E[q], Ls[q], rep(q));
+    if (q <= last) fwd_slot<NC>(acc01, acc23, ca, E[q], La, rep(q));
   }
   __syncwarp();  // the slot staging is reused for x below
   float* sx = wsm;  // [4][M]
@@ -379,11 +385,13 @@ __device__ __forceinline__ void desc_bwd_atom(int i, int lane, float* wsm, float
   const int nnei = tt.nnei;
   float* s_x = wsm;                // [4][M]
   float* s_t = s_x + 4 * M;        // [4][naxis]
-  float* s_d = s_t + 4 * MAXAX;    // [M][naxis + 1], later the slot staging
+  // the atom's dD tile transposed, [naxis][M]: a lane's four channels of one
+  // column a are one 16-byte read (M % 4 == 0), conflict-free across lanes;
+  // later the slot staging
+  float* s_d = s_t + 4 * MAXAX;
   const float* xi = xyz + (size_t)i * 4 * M;
   const unsigned long long pol = l2_policy_first();
   const float* dr = dD + (size_t)drow[i] * M * naxis;
-  const int ldd = naxis + 1;  // padded row: conflict-free column reads
   if ((M & 3) == 0 && (naxis & 3) == 0 &&
       ((reinterpret_cast<uintptr_t>(xi) | reinterpret_cast<uintptr_t>(dr)) & 15) == 0) {
     // 16-byte loads (more loads in flight per lane) where the rows allow
@@ -394,21 +402,21 @@ __device__ __forceinline__ void desc_bwd_atom(int i, int lane, float* wsm, float
     for (int q = lane; q < (M * naxis) >> 2; q += 32) {
       const float4 v = ld_stream4(d4 + q, pol);
       const int m = q / per_row, a = (q - m * per_row) << 2;
-      float* dst = s_d + m * ldd + a;
+      float* dst = s_d + a * M + m;
       dst[0] = v.x;
-      dst[1] = v.y;
-      dst[2] = v.z;
-      dst[3] = v.w;
+      dst[M] = v.y;
+      dst[2 * M] = v.z;
+      dst[3 * M] = v.w;
     }
   } else if (32 % naxis == 0) {
     for (int q = lane; q < 4 * M; q += 32) s_x[q] = ld_stream(xi + q, pol);
     const int per = 32 / naxis, a = lane % naxis;
-    for (int m = lane / naxis; m < M; m += per) s_d[m * ldd + a] = ld_stream(dr + m * naxis + a, pol);
+    for (int m = lane / naxis; m < M; m += per) s_d[a * M + m] = ld_stream(dr + m * naxis + a, pol);
   } else {
     for (int q = lane; q < 4 * M; q += 32) s_x[q] = ld_stream(xi + q, pol);
     for (int q = lane; q < M * naxis; q += 32) {
       const int m = q / naxis, a = q - m * naxis;
-      s_d[m * ldd + a] = ld_stream(dr + q, pol);
+      s_d[a * M + m] = ld_stream(dr + q, pol);
     }
   }
   __syncwarp();
@@ -416,16 +424,17 @@ __device__ __forceinline__ void desc_bwd_atom(int i, int lane, float* wsm, float
   // T[k, a] = sum_m' dD[m', a] x[k, m']
   if (naxis == 16 && (M & 3) == 0) {
     // lane = (k, a) and (k + 2, a): one dD column read serves both rows of x,
-    // x read four channels at a time
+    // x and the column read four channels at a time
     const int a = lane & 15, k = lane >> 4;
     const float* xa = s_x + k * M;
     const float* xb = s_x + (k + 2) * M;
+    const float* da = s_d + a * M;
     float acc0 = 0.f, acc1 = 0.f;
     for (int mp = 0; mp < M; mp += 4) {
       const float4 u = *reinterpret_cast<const float4*>(xa + mp);
       const float4 v = *reinterpret_cast<const float4*>(xb + mp);
-      const float d0 = s_d[mp * ldd + a], d1 = s_d[(mp + 1) * ldd + a];
-      const float d2 = s_d[(mp + 2) * ldd + a], d3 = s_d[(mp + 3) * ldd + a];
+      const float4 dv = *reinterpret_cast<const float4*>(da + mp);
+      const float d0 = dv.x, d1 = dv.y, d2 = dv.z, d3 = dv.w;
       acc0 += d0 * u.x;
       acc1 += d0 * v.x;
       acc0 += d1 * u.y;
@@ -441,7 +450,7 @@ __device__ __forceinline__ void desc_bwd_atom(int i, int lane, float* wsm, float
     for (int o = lane; o < 4 * naxis; o += 32) {
       const int k = o / naxis, a = o - k * naxis;
       float acc = 0.f;
-      for (int mp = 0; mp < M; ++mp) acc += s_d[mp * ldd + a] * s_x[k * M + mp];
+      for (int mp = 0; mp < M; ++mp) acc += s_d[a * M + mp] * s_x[k * M + mp];
       s_t[o] = acc;
     }
   }
@@ -457,9 +466,11 @@ __device__ __forceinline__ void desc_bwd_atom(int i, int lane, float* wsm, float
   if (act) {
     for (int a = 0; a < naxis; ++a) {
       const float x0 = s_x[a], x1 = s_x[M + a], x2 = s_x[2 * M + a], x3 = s_x[3 * M + a];
+      const float4 g4 = *reinterpret_cast<const float4*>(s_d + a * M + m0);
+      const float gch[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
       for (int ch = 0; ch < 4; ++ch) {
-        const float g = s_d[(m0 + ch) * ldd + a];
+        const float g = gch[ch];
         dyr[ch][0] += g * x0;
         dyr[ch][1] += g * x1;
         dyr[ch][2] += g * x2;
@@ -499,11 +510,16 @@ __device__ __forceinline__ void desc_bwd_atom(int i, int lane, float* wsm, float
     const float4* E = se + s0;
     const float4* Ls = sl + s0;
     auto rep = [&](int q) { return q == brk ? (float)(nt - q) : 1.f; };
-    auto row = [&](int q) { return tab + (size_t)__float_as_int(Ls[q].x) * rs; };
+    auto row = [&](const float4& L) { return tab + (size_t)__float_as_int(L.x) * rs; };
     // two coefficient buffers in turn (GRP is even, so slot parity fixes the
-    // buffer): the next slot's row is in flight while the current one is used
+    // buffer): the next slot's row is in flight while the current one is
+    // used; each buffer keeps its slot's staged table coordinates
     Coef4<NC> ca, cb;
-    if (act) ca = load_coef4<CH, NC>(row(0), M);
+    float4 La = make_float4(0.f, 0.f, 0.f, 0.f), Lb = La;
+    if (act) {
+      La = Ls[0];
+      ca = load_coef4<CH, NC>(row(La), M);
+    }
     for (int g0 = 0; g0 < nt; g0 += GRP) {
       if (g0 > last) {  // beyond the fold point: zero rows
         for (int qq = g0 + lane; qq < nt && qq < g0 + GRP; qq += 32)
@@ -518,11 +534,17 @@ __device__ __forceinline__ void desc_bwd_atom(int i, int lane, float* wsm, float
         const int qq = g0 + q;
         if (qq <= last && act) {  // warp-uniform apart from the idle lanes
           if ((q & 1) == 0) {
-            if (qq + 1 <= last) cb = load_coef4<CH, NC>(row(qq + 1), M);
-            bwd_slot<NC>(P[q], ca, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
+            if (qq + 1 <= last) {
+              Lb = Ls[qq + 1];
+              cb = load_coef4<CH, NC>(row(Lb), M);
+            }
+            bwd_slot<NC>(P[q], ca, E[qq], La, rep(qq), dyr01, dyr23);
           } else {
-            if (qq + 1 <= last) ca = load_coef4<CH, NC>(row(qq + 1), M);
-            bwd_slot<NC>(P[q], cb, E[qq], Ls[qq], rep(qq), dyr01, dyr23);
+            if (qq + 1 <= last) {
+              La = Ls[qq + 1];
+              ca = load_coef4<CH, NC>(row(La), M);
+            }
+            bwd_slot<NC>(P[q], cb, E[qq], Lb, rep(qq), dyr01, dyr23);
           }
         }
       }
