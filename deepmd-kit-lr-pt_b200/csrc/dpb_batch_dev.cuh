@@ -265,9 +265,9 @@ __device__ __forceinline__ void bt_force_row(int row, int lane, double* __restri
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
       const ET n = COH ? __ldcg(ndr + jj * 4 + a) : ndr[jj * 4 + a];
-      const ET sa = sd[jj * 4 + a];
+      const ET ns = n / sd[jj * 4 + a];  // dE/d(env): one division per env column
 #pragma unroll
-      for (int d = 0; d < 3; ++d) p[d] += n * (gd[a * 3 + d] / sa);
+      for (int d = 0; d < 3; ++d) p[d] += ns * gd[a * 3 + d];
     }
     const double q[3] = {(double)p[0], (double)p[1], (double)p[2]};
     c0 += q[0];

@@ -312,11 +312,13 @@ k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
     }
     OT v[4], gd[12];
     env_row<OT>(r, rcut_smth, rcut, v, gd);
+    // dE/d(env) = net_deriv / std, one division per env column
     OT p[3] = {(OT)0., (OT)0., (OT)0.};
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
+      const OT ns = nv[a] / sv[a];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) p[d] += nv[a] * (gd[a * 3 + d] / sv[a]);
+      for (int d = 0; d < 3; ++d) p[d] += ns * gd[a * 3 + d];
     }
     const double q[3] = {(double)p[0], (double)p[1], (double)p[2]};
     c0 += q[0];
