@@ -249,6 +249,7 @@ __device__ __forceinline__ void bt_force_row(int row, int lane, double* __restri
   const double xi[3] = {fc[3 * i], fc[3 * i + 1], fc[3 * i + 2]};
   const ET* sd = std_ + (size_t)ti * nnei * 4;
   const ET* ndr = nd + (size_t)row * nnei * 4;
+  const ET inv_span = (ET)1. / (ET)(rcut - rcut_smth);
   double c0 = 0., c1 = 0., c2 = 0.;
   double vs[9];
 #pragma unroll
@@ -259,8 +260,8 @@ __device__ __forceinline__ void bt_force_row(int row, int lane, double* __restri
     const int j = packed / 27;
     ET r[3];
     bt_rij<ET>(r, fc, packed, xi, L);
-    ET v[4], gd[12];
-    env_row<ET>(r, rcut_smth, rcut, v, gd);
+    ET gd[12];
+    env_deriv<ET>(r, rcut_smth, rcut, inv_span, gd);
     ET p[3] = {(ET)0, (ET)0, (ET)0};
 #pragma unroll
     for (int a = 0; a < 4; ++a) {

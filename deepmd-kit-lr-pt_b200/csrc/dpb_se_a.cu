@@ -273,6 +273,7 @@ k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
   pdl_wait();
   pdl_trigger();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const OT inv_span = (OT)1. / (OT)(rcut - rcut_smth);
   // grid-stride over center atoms (one warp each); the virial stays in
   // registers across atoms and is reduced once per block, so the nine
   // accumulators see one atomic per block instead of one per atom
@@ -310,8 +311,8 @@ k_force_virial_rc(double* __restrict__ force, double* __restrict__ virial,
         sv[a] = sd[jj * 4 + a];
       }
     }
-    OT v[4], gd[12];
-    env_row<OT>(r, rcut_smth, rcut, v, gd);
+    OT gd[12];
+    env_deriv<OT>(r, rcut_smth, rcut, inv_span, gd);
     // dE/d(env) = net_deriv / std, one division per env column
     OT p[3] = {(OT)0., (OT)0., (OT)0.};
 #pragma unroll
