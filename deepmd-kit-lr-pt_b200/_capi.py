@@ -148,6 +148,7 @@ _FUNCS.update({"dpb_bt_step_create": "pp", "dpb_bt_step_launch": "pp",
 _SIZE_QUERIES = {
     "dpb_copy_coord_scratch_bytes": ("ifp", LL),
     "dpb_cell_grid_bytes": ("i", LL),
+    "dpb_cell_grid_bytes_packed": ("i", LL),
     "dpb_geometry_scratch_bytes": ("ifp", LL),
     "dpb_fit_energy_sum_work_bytes": ("", LL),
     "dpb_build_nlist_scratch_bytes": ("ii", LL),

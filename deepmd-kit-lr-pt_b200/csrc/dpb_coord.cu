@@ -511,6 +511,7 @@ __global__ void k_grid_init(GridHeader* h) {
     h->kmin[d] = ~0ull;
     h->kmax[d] = 0ull;
   }
+  h->packed = 0;  // these builders do not write cell_pos
 }
 
 template <typename T>
@@ -624,9 +625,16 @@ long long grid_bytes(int nall) {
   return (long long)sizeof(GridHeader) + 256 + ints * (long long)sizeof(int);
 }
 
+static long long packed_offset(int nall) { return (grid_bytes(nall) + 255) / 256 * 256; }
+
+long long grid_bytes_packed(int nall) { return packed_offset(nall) + 32LL * nall; }
+
 GridView carve_grid(void* p, int nall) {
   int max_cells = nall > 64 ? nall : 64;
   GridView g;
+  // address only: dereferenced while h->packed == 1, which the fused
+  // geometry pass sets only when the buffer has grid_bytes_packed(nall) bytes
+  g.cell_pos = (double4*)((char*)p + packed_offset(nall));
   g.h = (GridHeader*)p;
   int* q = (int*)((char*)p + ((sizeof(GridHeader) + 255) / 256) * 256);
   g.cell_start = q; q += max_cells + 1;
@@ -1011,9 +1019,23 @@ __global__ void __launch_bounds__(GEO_THREADS, 1) k_geometry(GeoArgs a) {
       }
       h->ncells = gh.ncells;
       h->natoms = gh.natoms;
+      h->packed = a.g.cell_pos != nullptr ? 1 : 0;
     }
   }
-  for (int i = tid; i < n; i += nthr) a.g.cell_atoms[s_scan[a.g.cell_of[i]] + gslot[i]] = i;
+  if (a.g.cell_pos != nullptr) {
+    // the atoms' positions, types and indices in cell order as well, so
+    // that the env kernel's candidate walk reads them contiguously (written
+    // in this launch before the last barrier: L2-coherent loads)
+    for (int i = tid; i < n; i += nthr) {
+      const int pos = s_scan[a.g.cell_of[i]] + gslot[i];
+      a.g.cell_atoms[pos] = i;
+      const long long w = ((long long)__ldcg(a.text + i) << 32) | (long long)(unsigned)i;
+      a.g.cell_pos[pos] = make_double4(__ldcg(a.cext + 3 * i), __ldcg(a.cext + 3 * i + 1),
+                                       __ldcg(a.cext + 3 * i + 2), __longlong_as_double(w));
+    }
+  } else {
+    for (int i = tid; i < n; i += nthr) a.g.cell_atoms[s_scan[a.g.cell_of[i]] + gslot[i]] = i;
+  }
 }
 
 // normalize_coord + copy_coord + cell grid of one frame. The fused pass runs
@@ -1047,6 +1069,7 @@ int geometry_cells(double* cext, int* text, int* mapping, int* nall_dev, void* g
     return DPB_ERR_INVALID;
   }
   GridView g = carve_grid(grid, mem_nall);
+  if (gbytes < grid_bytes_packed(mem_nall)) g.cell_pos = nullptr;  // no room: not written
   const int gcap = g.max_cells < GEO_SCAN_CAP ? g.max_cells : GEO_SCAN_CAP;
   const long long copy_ints = (long long)r.nloc_cells + r.next_cells + 2;
   bool fused = nloc > 0 && copy_ints <= GEO_SCAN_CAP && tune_value("geometry_fused", 1) != 0;
@@ -1060,7 +1083,8 @@ int geometry_cells(double* cext, int* text, int* mapping, int* nall_dev, void* g
     int dev = 0;
     DPB_CUDA(cudaGetDevice(&dev), "geometry_cells");
     if (dev < 64 && !(attr_devs.load(std::memory_order_acquire) >> dev & 1ull)) {
-      const int most = GEO_SCAN_CAP * 4 + (GEO_THREADS / 32) * GEO_SORT_CAP * 4;
+      // scan_ints is at most GEO_SCAN_CAP + 1 (gcap + 1 cell starts)
+      const int most = (GEO_SCAN_CAP + 1) * 4 + (GEO_THREADS / 32) * GEO_SORT_CAP * 4;
       DPB_CUDA(cudaFuncSetAttribute(k_geometry, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     most),
                "geometry_cells");
@@ -1281,6 +1305,8 @@ int dpb_copy_coord_cells_f32(float* out_c, int* out_t, int* mapping, int* nall, 
 }
 
 long long dpb_cell_grid_bytes(int nall) { return grid_bytes(nall); }
+
+long long dpb_cell_grid_bytes_packed(int nall) { return grid_bytes_packed(nall); }
 
 long long dpb_geometry_scratch_bytes(int nloc, float rcut, const double* boxt) {
   return geometry_scratch_bytes(nloc, rcut, boxt);

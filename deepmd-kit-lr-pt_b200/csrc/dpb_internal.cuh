@@ -27,7 +27,8 @@ struct GridHeader {
   int dims[3];
   int ncells;
   int natoms;
-  int pad[3];
+  int packed;  // 1: cell_pos holds this grid's atoms in cell order (fused builder)
+  int pad[2];
 };
 
 struct GridView {
@@ -37,11 +38,17 @@ struct GridView {
   int* cell_of;     // [natoms]
   int* cell_atoms;  // [natoms], atoms sorted by cell
   int* redo;        // [natoms + 1]: count, then atoms deferred to a larger buffer
+  // [natoms] in cell order: x, y, z and (type << 32 | atom index) as the
+  // bits of the fourth double. Its storage follows the grid in buffers of
+  // grid_bytes_packed(nall) bytes; valid only while h->packed == 1
+  double4* cell_pos;
   int max_cells;
   int cap_atoms;
 };
 
 long long grid_bytes(int nall);
+// a grid buffer with room for the cell-ordered positions after the grid
+long long grid_bytes_packed(int nall);
 GridView carve_grid(void* p, int nall);
 template <typename T>
 int grid_build(void* grid, long long bytes, const T* coord, int nall,

@@ -88,6 +88,39 @@ __device__ __forceinline__ bool accept(unsigned long long& key, int j, int i,
   return true;
 }
 
+// accept<double, true> on one cell-ordered record of the grid (x, y, z and
+// type << 32 | index as the fourth double's bits): the same tests on the
+// same values, the record read as two 16-byte loads instead of the index,
+// the type and three coordinates gathered
+__device__ __forceinline__ bool accept_packed(unsigned long long& key, const double4* rec, int i,
+                                              int ti, const double xi[3], const float fxi[3],
+                                              double rc2, float rc2f, int ntypes, int* status) {
+  const double2 xy = __ldg(reinterpret_cast<const double2*>(rec));
+  const double2 zw = __ldg(reinterpret_cast<const double2*>(rec) + 1);
+  const long long w = __double_as_longlong(zw.y);
+  const int j = (int)(unsigned)(w & 0xffffffffll);
+  const int tj = (int)(w >> 32);
+  if (tj < 0) return false;
+  if (j == i || ti < 0) return false;
+  double d0 = sub_rn(xi[0], xy.x);
+  double d1 = sub_rn(xi[1], xy.y);
+  double d2 = sub_rn(xi[2], zw.x);
+  if (!(dot3_rn(d0, d1, d2) < rc2)) return false;
+  float e0 = sub_rn((float)xy.x, fxi[0]);
+  float e1 = sub_rn((float)xy.y, fxi[1]);
+  float e2 = sub_rn((float)zw.x, fxi[2]);
+  float r2 = dot3_rn(e0, e1, e2);
+  if (!(r2 <= rc2f)) return false;
+  if (tj >= 128 || j >= (1 << 24)) {
+    atomicOr(status, ST_KEY_OVERFLOW);
+    return false;
+  }
+  if (tj >= ntypes) return false;  // no sel slot exists for this type
+  key = ((unsigned long long)tj << 56) |
+        ((unsigned long long)__float_as_uint(r2) << 24) | (unsigned long long)j;
+  return true;
+}
+
 // em row = (v - avg) / std, or zeros for a center without a type row.
 template <typename OT>
 __device__ __forceinline__ void store_env_row(OT* e, const OT* a, const OT* s, const OT (&v)[4],
@@ -193,8 +226,10 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
   if (FROM_CELLS) {
     // the 27 neighbor cells' atom ranges loaded at once (lane L < 27: cell
     // (dx, dy, dz) = (L / 9, L / 3 % 3, L % 3) - 1), then one flat candidate
-    // list walked in full batches of 32; the next batch's atom indices are
-    // requested before the current batch is tested
+    // list walked in full batches of 32: with the grid's cell-ordered
+    // records when the fused geometry pass wrote them, else through the
+    // atom indices (the next batch's requested before the current batch is
+    // tested)
     const GridHeader& h = *io.g.h;
     const int ci = io.g.cell_of[i];
     const int cz = ci % h.dims[2], cy = (ci / h.dims[2]) % h.dims[1],
@@ -216,9 +251,10 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
     }
     const int excl = incl - cn;
     const int total = __shfl_sync(0xffffffffu, incl, 31);
-    // atom index of flat candidate fl (-1 past the end): the cell is the last
-    // lane whose range starts at or before fl (binary search over the lanes)
-    auto cand_of = [&](int fl) -> int {
+    // position in the cell-ordered arrays of flat candidate fl (-1 past
+    // the end): the cell is the last lane whose range starts at or before fl
+    // (binary search over the lanes)
+    auto slot_of = [&](int fl) -> int {
       int lo = 0;
 #pragma unroll
       for (int st = 16; st > 0; st >>= 1) {
@@ -227,17 +263,40 @@ __device__ bool env_one(const EnvIO<CT, OT>& io, const SecInfo& sec, int row,
       }
       const int base_c = __shfl_sync(0xffffffffu, cb, lo);
       const int start_c = __shfl_sync(0xffffffffu, excl, lo);
-      return fl < total ? io.g.cell_atoms[base_c + (fl - start_c)] : -1;
+      return fl < total ? base_c + (fl - start_c) : -1;
     };
-    int jn = cand_of(lane);
-    for (int base = 0; base < total; base += 32) {
-      const int j = jn;
-      jn = cand_of(base + 32 + lane);
-      unsigned long long key = 0;
-      bool ok = false;
-      if (j >= 0)
-        ok = accept<CT, true>(key, j, i, ti, fc, ft, xi, fxi, rc2, rc2f, ntypes, io.status);
-      push(ok, key);
+    bool walked = false;
+    if constexpr (sizeof(CT) == 8) {
+      if (h.packed != 0) {
+        // the grid's cell-ordered records (fused geometry pass): contiguous
+        // 32-byte reads per batch
+        for (int base = 0; base < total; base += 32) {
+          const int k = slot_of(base + lane);
+          unsigned long long key = 0;
+          bool ok = false;
+          if (k >= 0)
+            ok = accept_packed(key, io.g.cell_pos + k, i, ti, xi, fxi, rc2, rc2f, ntypes,
+                               io.status);
+          push(ok, key);
+        }
+        walked = true;
+      }
+    }
+    if (!walked) {
+      auto cand_of = [&](int fl) -> int {
+        const int k = slot_of(fl);
+        return k >= 0 ? io.g.cell_atoms[k] : -1;
+      };
+      int jn = cand_of(lane);
+      for (int base = 0; base < total; base += 32) {
+        const int j = jn;
+        jn = cand_of(base + 32 + lane);
+        unsigned long long key = 0;
+        bool ok = false;
+        if (j >= 0)
+          ok = accept<CT, true>(key, j, i, ti, fc, ft, xi, fxi, rc2, rc2f, ntypes, io.status);
+        push(ok, key);
+      }
     }
   } else {
     const int nn = io.numneigh[row];

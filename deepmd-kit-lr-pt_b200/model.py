@@ -512,7 +512,8 @@ class SeAEvaluator:
             # ghosts are at most the ghost cells' share of the atoms; +25% slack
             nall_capacity = int(self._estimate_nall() * 1.25) + 64
         self.mem_nall = nall_capacity
-        self.grid_bytes = int(lib.dpb_cell_grid_bytes(self.mem_nall))
+        # with room for the cell-ordered candidate records of the env kernel
+        self.grid_bytes = int(lib.dpb_cell_grid_bytes_packed(self.mem_nall))
         dev = self.dev
         fdt = torch.float32 if mode == "compressed" else torch.float64
         self.fdt = fdt

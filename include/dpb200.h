@@ -86,6 +86,12 @@ DPB_API int dpb_copy_coord_f32(float* out_c, int* out_t, int* mapping,
  * below; it replaces the O(nloc*nall) pair test of build_nlist_gpu
  * (source/lib/src/gpu/neighbor_list.cu:77-113). */
 DPB_API long long dpb_cell_grid_bytes(int nall);
+/* A grid buffer with room, after the grid, for the atoms' positions, types
+ * and indices in cell order (32 bytes per atom). dpb_geometry_cells_f64 given
+ * a buffer of this size writes them, and the cell-list env kernels then read
+ * the candidates contiguously from them (same results); every other builder
+ * marks them absent. */
+DPB_API long long dpb_cell_grid_bytes_packed(int nall);
 DPB_API int dpb_cell_grid_build_f64(void* grid, long long grid_bytes,
                                     const double* coord, int nall, float rcut,
                                     dpb_stream_t stream);

@@ -7,7 +7,11 @@ mapping, nall); the cell grid must equal the separate grid build's (header,
 cell starts, cell of every atom; atoms inside a cell as a set, since their
 order there is not defined). Cases cover cells of <= 32, 33..256 and > 256
 atoms (the three ranking paths of the ghost copy), triclinic boxes, coordinates
-outside the box, and a ghost capacity smaller than nall.
+outside the box, and a ghost capacity smaller than nall. Given a buffer of
+dpb_cell_grid_bytes_packed bytes the fused pass also writes the atoms' cell-
+ordered records (position, type, index), which the cell-list env kernels
+read instead of gathering: the records must equal the extended arrays, and
+the env kernels' outputs must not depend on them (bit for bit).
 """
 
 import ctypes
@@ -22,12 +26,12 @@ pytestmark = pytest.mark.gpu
 HDR_BYTES = 256  # grid header, rounded up to 256 bytes in the grid buffer
 
 
-def _run(dpb, coord, atype, box, rcut, mem_nall, fused):
+def _run(dpb, coord, atype, box, rcut, mem_nall, fused, packed=False):
     cap, dev = dpb._capi, torch.device("cuda:0")
     lib = cap.lib()
     nloc = atype.size
     boxc = np.ascontiguousarray(box, np.float64).reshape(9)
-    gb = int(lib.dpb_cell_grid_bytes(mem_nall))
+    gb = int(lib.dpb_cell_grid_bytes_packed(mem_nall) if packed else lib.dpb_cell_grid_bytes(mem_nall))
     sb = int(lib.dpb_geometry_scratch_bytes(nloc, ctypes.c_float(rcut), boxc.ctypes.data))
     c = torch.tensor(coord, dtype=torch.float64, device=dev).reshape(-1, 3).contiguous()
     c0 = c.clone()
@@ -54,7 +58,8 @@ def _run(dpb, coord, atype, box, rcut, mem_nall, fused):
     n_all = int(nall.item())
     return dict(nall=n_all, cext=cext.cpu().numpy(), text=text.cpu().numpy(),
                 mapping=mapping.cpu().numpy(), grid=_grid(grid.cpu().numpy(), mem_nall,
-                                                          min(n_all, mem_nall)))
+                                                          min(n_all, mem_nall)),
+                dev=dict(grid=grid, cext=cext, text=text))
 
 
 def _grid(buf, mem_nall, n):
@@ -65,15 +70,23 @@ def _grid(buf, mem_nall, n):
     inv_cs = hdr[72:96].view(np.float64)
     ints = hdr[96:116].view(np.int32)
     dims, ncells, natoms = ints[:3].copy(), int(ints[3]), int(ints[4])
+    packed = int(hdr[116:120].view(np.int32)[0])
     max_cells = max(mem_nall, 64)
     body = buf[HDR_BYTES:].view(np.int32)
     cell_start = body[:ncells + 1].copy()
     off = (max_cells + 1) + max_cells
     cell_of = body[off:off + n].copy()
     cell_atoms = body[off + mem_nall:off + mem_nall + n].copy()
+    # cell-ordered records after the grid, at grid_bytes rounded up to 256
+    ints_total = (max_cells + 1) + max_cells + 3 * mem_nall + 1 + 64
+    off_rec = (128 + 256 + 4 * ints_total + 255) // 256 * 256
+    rec = None
+    if packed == 1:
+        rec = buf[off_rec:off_rec + 32 * n].view(np.float64).reshape(-1, 4).copy()
     return dict(kmin=kmin.copy(), kmax=kmax.copy(), origin=origin.copy(),
                 inv_cs=inv_cs.copy(), dims=dims, ncells=ncells, natoms=natoms,
-                cell_start=cell_start, cell_of=cell_of, cell_atoms=cell_atoms)
+                cell_start=cell_start, cell_of=cell_of, cell_atoms=cell_atoms,
+                packed=packed, rec=rec)
 
 
 def _same(a, b):
@@ -162,3 +175,76 @@ def test_water_12288(dpb):
     a = _run(dpb, coord, atype, box, 6.0, mem, fused=True)
     b = _run(dpb, coord, atype, box, 6.0, mem, fused=False)
     _same(a, b)
+
+
+def _check_records(r):
+    g = r["grid"]
+    assert g["packed"] == 1
+    n = g["natoms"]
+    rec = g["rec"][:n]
+    j = g["cell_atoms"][:n]
+    assert np.array_equal(rec[:, :3].view(np.uint64), r["cext"][j].view(np.uint64))
+    w = rec[:, 3].copy().view(np.int64)
+    assert np.array_equal((w & 0xFFFFFFFF).astype(np.int64), j.astype(np.int64))
+    assert np.array_equal((w >> 32).astype(np.int64), r["text"][j].astype(np.int64))
+
+
+@pytest.mark.parametrize("name", ["water_192", "water_1536", "dense_one_cell"])
+def test_packed_records(dpb, name):
+    """The fused pass with a packed-size buffer writes one record per atom in
+    cell order and flags the header; without the room, or from the separate
+    kernels, the flag stays 0 and the rest of the grid is unchanged."""
+    build, rcut = CASES[name]
+    coord, atype, box = build(dpb)
+    mem = int(atype.size * 30) + 64
+    a = _run(dpb, coord, atype, box, rcut, mem, fused=True, packed=True)
+    _check_records(a)
+    b = _run(dpb, coord, atype, box, rcut, mem, fused=True)
+    c = _run(dpb, coord, atype, box, rcut, mem, fused=False, packed=True)
+    assert b["grid"]["packed"] == 0 and c["grid"]["packed"] == 0
+    _same(a, b)
+    _same(a, c)
+
+
+def _env(dpb, r, nloc, mem_nall, rcut, sel, kind):
+    cap, dev = dpb._capi, torch.device("cuda:0")
+    ft = torch.float64 if kind == "f64" else torch.float32
+    nnei = int(sum(sel))
+    sec = np.concatenate([[0], np.cumsum(sel)]).astype(np.int32)
+    ntypes = len(sel)
+    g = torch.Generator().manual_seed(5)
+    avg = (0.1 * torch.randn(ntypes, nnei * 4, generator=g, dtype=torch.float64)).to(dev, ft)
+    std = (1.0 + 0.2 * torch.rand(ntypes, nnei * 4, generator=g, dtype=torch.float64)).to(dev, ft)
+    em = torch.zeros(nloc, nnei * 4, dtype=ft, device=dev)
+    ed = torch.zeros(nloc, nnei * 12, dtype=ft, device=dev)
+    rij = torch.zeros(nloc, nnei * 3, dtype=ft, device=dev)
+    nl = torch.zeros(nloc, nnei, dtype=torch.int32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    d = r["dev"]
+    s = torch.cuda.current_stream().cuda_stream
+    fn = "dpb_env_mat_a_cells_f64" if kind == "f64" else "dpb_env_mat_a_cells_mixed"
+    cap.call(fn, cap.ptr(em), cap.ptr(ed), cap.ptr(rij), cap.ptr(nl), cap.ptr(d["cext"]),
+             cap.ptr(d["text"]), cap.ptr(d["grid"]), cap.ptr(avg), cap.ptr(std), nloc, mem_nall,
+             ctypes.c_float(rcut), ctypes.c_float(0.5), sec.ctypes.data, sec.size,
+             cap.ptr(status), s)
+    cap.call("dpb_status_check", cap.ptr(status), s)
+    return [t.cpu().numpy() for t in (em, ed, rij, nl)]
+
+
+@pytest.mark.parametrize("kind", ["f64", "mixed"])
+def test_env_packed_equals_gathered(dpb, kind):
+    """The cell-list env kernel walking the packed records gives the same
+    neighbor list, env matrix, derivative and rij as walking the atom indices
+    (12,288-atom water and a dense one-cell frame with a small sel)."""
+    for build, rcut, sel in ((lambda d: _water(d, 16), 6.0, [46, 92]),
+                             (lambda d: _water(d, 4, 2), 9.0, [20, 40])):
+        coord, atype, box = build(dpb)
+        mem = int(atype.size * 30) + 64 if atype.size < 1000 else int(atype.size * 3)
+        a = _run(dpb, coord, atype, box, rcut, mem, fused=True, packed=True)
+        b = _run(dpb, coord, atype, box, rcut, mem, fused=True)
+        assert a["grid"]["packed"] == 1 and b["grid"]["packed"] == 0
+        oa = _env(dpb, a, atype.size, mem, rcut, sel, kind)
+        ob = _env(dpb, b, atype.size, mem, rcut, sel, kind)
+        for x, y in zip(oa, ob):
+            assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+        assert (oa[3] >= 0).any()
