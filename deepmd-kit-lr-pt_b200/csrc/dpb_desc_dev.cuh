@@ -260,7 +260,26 @@ __device__ __forceinline__ void fwd_slot(float2 (&acc01)[4], float2 (&acc23)[4],
 // D[m, a] = sum_k x[k, m] x[k, a] of one atom from x [4][M] in shared memory
 __device__ __forceinline__ void write_descriptor(float* __restrict__ Dr, const float* sx, int M,
                                                  int naxis, int lane) {
-  if (32 % naxis == 0) {  // fixed column a per lane, 32 / naxis rows per pass
+  if ((naxis & 3) == 0 && 32 % (naxis >> 2) == 0 && (M & 3) == 0 &&
+      (reinterpret_cast<uintptr_t>(Dr) & 15) == 0) {
+    // four columns a..a+3 per lane, kept in registers; naxis / 4 lanes per
+    // row, so each pass stores 32 / (naxis / 4) whole rows as one contiguous
+    // run of 16-byte stores, and reads x[k, m] once per row and lane
+    const int lpr = naxis >> 2, rpi = 32 / lpr;
+    const int a = (lane % lpr) * 4, mr = lane / lpr;
+    float4 xa[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) xa[k] = *reinterpret_cast<const float4*>(sx + k * M + a);
+    for (int m = mr; m < M; m += rpi) {
+      const float x0 = sx[m], x1 = sx[M + m], x2 = sx[2 * M + m], x3 = sx[3 * M + m];
+      float4 o;
+      o.x = x0 * xa[0].x + x1 * xa[1].x + x2 * xa[2].x + x3 * xa[3].x;
+      o.y = x0 * xa[0].y + x1 * xa[1].y + x2 * xa[2].y + x3 * xa[3].y;
+      o.z = x0 * xa[0].z + x1 * xa[1].z + x2 * xa[2].z + x3 * xa[3].z;
+      o.w = x0 * xa[0].w + x1 * xa[1].w + x2 * xa[2].w + x3 * xa[3].w;
+      *reinterpret_cast<float4*>(Dr + m * naxis + a) = o;
+    }
+  } else if (32 % naxis == 0) {  // fixed column a per lane, 32 / naxis rows per pass
     const int per = 32 / naxis, a = lane % naxis;
     const float x0 = sx[a], x1 = sx[M + a], x2 = sx[2 * M + a], x3 = sx[3 * M + a];
     for (int m = lane / naxis; m < M; m += per)
