@@ -847,9 +847,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             "bytes_per_launch": gather, "slots_evaluated": slots, "coefficients_per_channel": ncoef,
             "achieved_tbs": gather / (ours[dom] * 1e-3) / 1e12, "nominal_l1_tbs": l1_peak,
             "frac": gather / (ours[dom] * 1e-3) / 1e12 / l1_peak,
-            "note": "table-row gathers through L1/TEX (ncu: L1/TEX 76% busy in k_desc_bwd, "
-                    "85% in k_desc_fwd, DRAM 6-7%); the HBM fraction above is low by "
-                    "construction"}
+            "note": "table-row gathers through L1/TEX (ncu: L1 data-pipe wavefronts 73% of "
+                    "peak and issue 62% in k_desc_bwd, L1/TEX 85% busy in k_desc_fwd, DRAM "
+                    "6-7%); the HBM fraction above is low by construction"}
     # every stage against its own roof: HBM bytes for the memory stages, the
     # tensor pipe for the fitting GEMMs (split TF32: three or four TF32
     # products per FP32 multiply-add, the fit_terms knob; TF32 dense peak
