@@ -50,12 +50,17 @@ def _strip(state: dict) -> dict:
 
 
 def load(path_or_state, sel=None, rcut: float | None = None,
-         rcut_smth: float | None = None) -> SeAParams:
+         rcut_smth: float | None = None, trusted: bool = False) -> SeAParams:
     """SeAParams of a reference model: a state dict, a training checkpoint
     ({"model": state dict}) or the path of a checkpoint / TorchScript file.
     sel, rcut and rcut_smth are not part of the state dict (they are in the
     model's input script): a TorchScript model reports sel and rcut itself
-    (get_sel / get_rcut of the reference model); otherwise give them."""
+    (get_sel / get_rcut of the reference model); otherwise give them (rcut
+    and rcut_smth default to the reference's se_e2_a input defaults, 6.0 and
+    0.5). A checkpoint file is read with torch.load(weights_only=True):
+    tensors and plain containers only, which is all a reference checkpoint
+    holds; trusted=True unpickles arbitrary objects, for files of a trusted
+    origin only."""
     state = path_or_state
     if isinstance(state, str):
         import torch
@@ -66,7 +71,7 @@ def load(path_or_state, sel=None, rcut: float | None = None,
             rcut = rcut if rcut is not None else float(mod.get_rcut())
             state = mod.state_dict()
         except RuntimeError:
-            state = torch.load(state, map_location="cpu", weights_only=False)
+            state = torch.load(state, map_location="cpu", weights_only=not trusted)
     if isinstance(state, dict) and "model" in state and isinstance(state["model"], dict):
         state = state["model"]
     return params_from_state_dict(state, sel=sel, rcut=6.0 if rcut is None else rcut,

@@ -95,6 +95,53 @@ def test_reader_round_trip_and_prefixes(dpb, layout, model):
             np.testing.assert_array_equal(i0, i1)
 
 
+def test_reader_from_checkpoint_file(dpb, layout, model, tmp_path):
+    """A training checkpoint file as the reference writes it (the wrapper's
+    state dict under "model", optimizer state and training info beside it)
+    read back by path, with the default weights-only unpickling."""
+    import torch
+
+    ck = importlib.import_module("deepmd_kit_lr_pt_b200.checkpoint")
+    g = layout[0]
+    sd = ck.params_to_state_dict(model)
+    wrapped = {"model.Default." + k.replace(".networks.", "._networks."): v
+               for k, v in sd.items()}
+    wrapped["_extra_state"] = {"model_params": {"type_map": ["O", "H"]},
+                               "train_infos": {"lr": 1e-3, "step": 10}}
+    path = str(tmp_path / "model.ckpt.pt")
+    torch.save({"model": wrapped, "optimizer": {"state": {}, "param_groups": [{"lr": 1e-3}]}},
+               path)
+    p = ck.load(path, sel=tuple(int(x) for x in g["sel"]), rcut=float(g["rcut"]))
+    np.testing.assert_array_equal(p.davg, model.davg)
+    for (t0, i0), (t1, i1) in zip(p.tables, model.tables):
+        np.testing.assert_array_equal(t0, t1)
+        np.testing.assert_array_equal(i0, i1)
+    for (a, b), (c, d) in zip([x for net in p.emb for x in net],
+                              [x for net in model.emb for x in net]):
+        np.testing.assert_array_equal(a, c)
+        np.testing.assert_array_equal(b, d)
+
+
+class _Opaque:
+    """An object only a full unpickler can rebuild."""
+
+
+def test_reader_refuses_pickled_objects_unless_trusted(dpb, model, tmp_path):
+    """A file that needs arbitrary unpickling is refused by default."""
+    import pickle
+
+    import torch
+
+    ck = importlib.import_module("deepmd_kit_lr_pt_b200.checkpoint")
+    sd = ck.params_to_state_dict(model)
+    path = str(tmp_path / "odd.pt")
+    torch.save({"model": sd, "extra": _Opaque()}, path)
+    with pytest.raises(pickle.UnpicklingError):
+        ck.load(path, sel=model.cfg.sel, rcut=model.cfg.rcut)
+    p = ck.load(path, sel=model.cfg.sel, rcut=model.cfg.rcut, trusted=True)
+    np.testing.assert_array_equal(p.dstd, model.dstd)
+
+
 def test_reader_rejects_wrong_sel(dpb, model):
     ck = importlib.import_module("deepmd_kit_lr_pt_b200.checkpoint")
     sd = ck.params_to_state_dict(model)
