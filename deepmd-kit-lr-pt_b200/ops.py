@@ -104,7 +104,8 @@ def copy_coord(coord: torch.Tensor, atype: torch.Tensor, rcut: float, box,
             ptr(out_c), ptr(out_t), ptr(mapping), ctypes.addressof(nall), ptr(scratch),
             sbytes, ptr(c), ptr(t), nloc, mem, ctypes.c_float(rcut), bx.ctypes.data, _stream())
         if code == 1 and mem_nall is None:
-            mem = nall.value
+            # the capacity code reports the ghost count needed; always grow
+            mem = max(nall.value, mem + 1)
             continue
         _capi.check(code, "copy_coord")
         n = nall.value
