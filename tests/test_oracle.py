@@ -307,3 +307,205 @@ def test_format_nlist_overflow_reports_type(port):
                                    np.array([0, 1, 3], np.int32))
     assert r == 1  # three type-1 neighbors into two slots: farthest dropped
     np.testing.assert_array_equal(fmt, [-1, 1, 2])
+
+
+# --------------------------------------------- neighbor-list golden vectors
+def _pbc_shift(idx: int, n: int) -> int:
+    """compute_pbc_shift (source/lib/src/neighbor_list.cc:731-745)."""
+    s = 0
+    if idx < 0:
+        s = 1
+        while idx + s * n < 0:
+            s += 1
+    elif idx >= n:
+        s = -1
+        while idx + s * n >= n:
+            s -= 1
+    return s
+
+
+def _legacy_copy_coord(posi, atype, rc, box):
+    """Ghosts in the order of the reference's older std::vector copy_coord
+    (source/lib/src/neighbor_list.cc:747-830 with the cell list of build_clist,
+    :43-113), the order behind the ghost indices of the golden lists in
+    test_fmt_nlist.cc and test_neighbor_list.cc. Orthorhombic boxes only (the
+    fixtures use a 13 A cube): internal coordinates are x / L, a ghost is
+    its owner minus the cell-image shift times L, and ghost cells are walked
+    x-major over [-ngcell, ncell + ngcell) with the local cells skipped."""
+    L = np.diag(np.asarray(box, np.float64).reshape(3, 3))
+    ncell = [max(int(L[d] / rc), 1) for d in range(3)]
+    ngcell = [int(rc / (L[d] / ncell[d])) + 1 for d in range(3)]
+    p = np.asarray(posi, np.float64).reshape(-1, 3)
+    nloc = p.shape[0]
+    clist: dict[tuple, list] = {}
+    for i in range(nloc):
+        idx = []
+        for d in range(3):
+            u = p[i, d] / L[d]
+            k = int(u / (1.0 / ncell[d]))
+            if u < 0.0:
+                k -= 1
+            idx.append(min(max(k, 0), ncell[d] - 1))
+        clist.setdefault(tuple(idx), []).append(i)
+    out_c, out_t, mapping = [x for x in p], list(atype), list(range(nloc))
+    rng = [range(-ngcell[d], ncell[d] + ngcell[d]) for d in range(3)]
+    for i0 in rng[0]:
+        for i1 in rng[1]:
+            for i2 in rng[2]:
+                ii = (i0, i1, i2)
+                if all(0 <= ii[d] < ncell[d] for d in range(3)):
+                    continue
+                sh = [_pbc_shift(ii[d], ncell[d]) for d in range(3)]
+                jj = tuple(ii[d] + sh[d] * ncell[d] for d in range(3))
+                shift_v = np.array(sh, np.float64) * L
+                for q in clist.get(jj, []):
+                    out_c.append(p[q] - shift_v)
+                    out_t.append(atype[q])
+                    mapping.append(q)
+    return (np.array(out_c, np.float64), np.array(out_t, np.int32),
+            np.array(mapping, np.int32))
+
+
+def test_legacy_ghosts_equal_copy_coord_cpu(port, ref_fixtures):
+    """On the golden lists' fixture the older ghost order and the oracle's
+    copy_coord_cpu order are the same array (owners, types, coordinates), so
+    the golden indices below refer to the oracle's own ghosts."""
+    fx, key = ref_fixtures, "test_fmt_nlist.cc:TestFormatNlist:"
+    posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+    box = np.diag([13.0] * 3).reshape(9)
+    c0, t0, m0 = _legacy_copy_coord(posi, atype, float(fx[key + "rc"]), box)
+    c1, t1, m1 = port.copy_coord(posi, atype, float(fx[key + "rc"]), box)
+    np.testing.assert_array_equal(m0, m1)
+    np.testing.assert_array_equal(t0, t1)
+    np.testing.assert_array_equal(c0, c1.reshape(-1, 3))
+
+
+@pytest.mark.parametrize("which", ["port", "ref_lib"])
+@pytest.mark.parametrize("cls", ["TestFormatNlist", "TestFormatNlistShortSel"])
+def test_format_nlist_golden(request, ref_fixtures, cls, which):
+    """test_fmt_nlist.cc (cpu): ghost copy, raw list and the list formatted
+    into the sel slots (type, float r^2, index order) give expect_nlist_cpy
+    index for index (the oracle, and the reference library as the harness's
+    own check)."""
+    port = request.getfixturevalue(which)
+    fx, key = ref_fixtures, f"test_fmt_nlist.cc:{cls}:"
+    posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+    rc, sec = float(fx[key + "rc"]), fx[key + "sec_a"].astype(np.int32)
+    c, t, _ = port.copy_coord(posi, atype, rc, np.diag([13.0] * 3).reshape(9))
+    c = c.reshape(-1, 3)
+    nloc, nnei = atype.size, int(sec[-1])
+    ret, il, nn, rb, _ = port.build_nlist(c, nloc, rc, atype=t)
+    assert ret == 0
+    avg = np.zeros((2, nnei * 4))
+    std = np.ones((2, nnei * 4))
+    nlist = port.prod_env_mat_a(c, t, il, nn, rb, avg, std, nloc, rc, 0.5, sec)[3]
+    np.testing.assert_array_equal(nlist.reshape(-1), fx[key + "expect_nlist_cpy"])
+
+
+@pytest.mark.parametrize("which", ["port", "ref_lib"])
+def test_build_nlist_golden(request, ref_fixtures, which):
+    """test_neighbor_list.cc (cpu): every extended atom within rc of each
+    local atom (strict r^2 < rc^2), compared as sorted rows, and the longest
+    row (max_list_size 5)."""
+    port = request.getfixturevalue(which)
+    fx, key = ref_fixtures, "test_neighbor_list.cc:TestNeighborList:"
+    posi, atype = fx[key + "posi"], fx[key + "atype"].astype(np.int32)
+    rc = float(fx[key + "rc"])
+    c, t, _ = port.copy_coord(posi, atype, rc, fx[key + "boxt"])
+    nloc = atype.size
+    ret, il, nn, rb, mx = port.build_nlist(c.reshape(-1, 3), nloc, rc, mem_size=10)
+    assert ret == 0 and mx == 5
+    np.testing.assert_array_equal(il, np.arange(nloc))
+    flat, lens = fx[key + "expect_nlist_cpy"], fx[key + "expect_nlist_cpy_len"]
+    np.testing.assert_array_equal(nn, lens)
+    o = 0
+    for i in range(nloc):
+        np.testing.assert_array_equal(np.sort(rb[i, :nn[i]]), np.sort(flat[o:o + lens[i]]))
+        o += lens[i]
+
+
+# ------------------------------------- tabulate extrapolation known answers
+def _kat_locate(xx, info):
+    """Interval, offset and extrapolation distance of x on a two-stride
+    table, as test_tabulate_extrapolate.cc's se_a lookup states it: below
+    lower the first interval at offset 0 with distance x - lower; at or above
+    max the interval holding nextafter(max, lower) at the offset of max with
+    distance x - max."""
+    lower, upper, mx, s0, s1 = info[:5]
+    if xx < lower:
+        return 0, 0.0, xx - lower
+    if xx < upper:
+        k = int((xx - lower) / s0)
+        return k, xx - (k * s0 + lower), 0.0
+    first = int((upper - lower) / s0)
+    if xx < mx:
+        k = first + int((xx - upper) / s1)
+        return k, xx - ((k - first) * s1 + upper), 0.0
+    k = first + int((np.nextafter(mx, lower) - upper) / s1)
+    return k, mx - ((k - first) * s1 + upper), xx - mx
+
+
+def _poly(c, x):
+    return c[0] + (c[1] + (c[2] + (c[3] + (c[4] + c[5] * x) * x) * x) * x) * x
+
+
+def _dpoly(c, x):
+    return c[1] + (2 * c[2] + (3 * c[3] + (4 * c[4] + 5 * c[5] * x) * x) * x) * x
+
+
+@pytest.mark.parametrize("which", ["port", "ref_lib"])
+@pytest.mark.parametrize("info_key,points", [
+    ("kTableInfo", ("below", "max", "above")),
+    ("kOffGridTableInfo", ("max", "above")),
+])
+def test_tabulate_extrapolation_known_answers(request, ref_fixtures, info_key, points, which):
+    """test_tabulate_extrapolate.cc (SeAUsesC1LinearTails and the off-grid
+    max case of the shared lookup): outside [lower, max) the value is the
+    boundary polynomial continued linearly with its slope (C1 tails) and
+    dy/dx is that slope; one neighbor, em = (1, 0, 0, 0), M = 1."""
+    port = request.getfixturevalue(which)
+    fx, k = ref_fixtures, "test_tabulate_extrapolate.cc:"
+    table, info = fx[k + "kTable"], fx[k + info_key]
+    tol = float(fx[k + "kTolerance"])
+    lower, mx = float(fx[k + "kLower"]), float(info[2])
+    xs = {"below": lower - 0.25, "max": mx, "above": mx + 0.25}
+    em = np.array([[[1.0, 0.0, 0.0, 0.0]]])
+    for name in points:
+        xx = xs[name]
+        idx, off, delta = _kat_locate(xx, info)
+        c = table[6 * idx:6 * idx + 6]
+        want_v = _poly(c, off) + _dpoly(c, off) * delta
+        want_g = _dpoly(c, off)
+        ex = np.array([[xx]])
+        out = port.tabulate(table, info, ex, em, 1)
+        assert abs(out.reshape(-1)[0] - want_v) <= tol, (name, out.reshape(-1)[0], want_v)
+        dy = np.zeros((1, 4, 1))
+        dy[0, 0, 0] = 1.0
+        dx, de = port.tabulate_grad(table, info, ex, em, dy, 1)
+        assert abs(dx.reshape(-1)[0] - want_g) <= tol, (name, dx.reshape(-1)[0], want_g)
+        assert abs(de.reshape(-1)[0] - want_v) <= tol
+
+
+def test_tabulate_grad_grad_in_tails(port, ref_fixtures):
+    """test_tabulate_extrapolate.cc (GradGradKernelsMatchDyFiniteDifferenceInTails,
+    se_a): in both tails, the second-derivative op applied to the fixed
+    (dz_dem_x, dz_dem) equals the central difference, over dy, of the
+    projection <dz_dem_x, dy_dem_x(dy)> + <dz_dem, dy_dem(dy)>."""
+    fx, k = ref_fixtures, "test_tabulate_extrapolate.cc:"
+    table, info = fx[k + "kTable"], fx[k + "kTableInfo"]
+    h = float(fx[k + "kFiniteDiffStep"])
+    em = np.array([[[0.7, -0.3, 0.2, 0.5]]])
+    zx, ze = np.array([[0.4]]), np.array([[[0.1, -0.2, 0.3, -0.4]]])
+    for xx in (float(fx[k + "kLower"]) - 0.25, float(fx[k + "kMax"]) + 0.25):
+        ex = np.array([[xx]])
+        dz = port.tabulate_grad_grad(table, info, ex, em, zx, ze, 1).reshape(-1)
+
+        def proj(dy):
+            dx, de = port.tabulate_grad(table, info, ex, em, dy.reshape(1, 4, 1), 1)
+            return float((zx * dx).sum() + (ze * de).sum())
+
+        for i in range(4):
+            e = np.zeros(4)
+            e[i] = h
+            fd = (proj(np.full(4, 0.3) + e) - proj(np.full(4, 0.3) - e)) / (2 * h)
+            assert abs(dz[i] - fd) <= 1e-8, (xx, i, dz[i], fd)
