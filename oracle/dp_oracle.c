@@ -129,6 +129,7 @@ int orc_copy_coord(double* out_c, int* out_t, int* mapping, int* nall,
   /* cell list of the local atoms (build_clist, neighbor_list.cc:43-112), with
    * nat_stt = ext_stt = 0, nat_end = ext_end = global_grid = ncell */
   int ncl = nc[0] * nc[1] * nc[2];
+  if (ncl <= 0 || nloc < 0) return 2; /* cell count out of int range: not a box */
   int* cell_of = (int*)malloc(sizeof(int) * (nloc > 0 ? nloc : 1));
   int* cnt = (int*)calloc(ncl + 1, sizeof(int));
   for (int ii = 0; ii < nloc; ++ii) {
