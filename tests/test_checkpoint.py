@@ -122,6 +122,69 @@ def test_reader_from_checkpoint_file(dpb, layout, model, tmp_path):
         np.testing.assert_array_equal(b, d)
 
 
+def _scripted_model(sd, sel, rcut):
+    """A TorchScript module with the reference model's state-dict layout and
+    its get_sel / get_rcut (the two facts the reader takes from a frozen or
+    compressed model file besides the state dict)."""
+    from typing import List
+
+    import torch
+
+    class Node(torch.nn.Module):
+        pass
+
+    class Frozen(torch.nn.Module):
+        def __init__(self):
+            super().__init__()
+            for k, v in sd.items():
+                parts = k.split(".")
+                m = self
+                for part in parts[:-1]:
+                    if part not in m._modules:
+                        m.add_module(part, Node())
+                    m = m._modules[part]
+                m.register_buffer(parts[-1], v)
+            self.sel = [int(x) for x in sel]
+            self.rcut = float(rcut)
+
+        @torch.jit.export
+        def get_sel(self) -> List[int]:
+            return self.sel
+
+        @torch.jit.export
+        def get_rcut(self) -> float:
+            return self.rcut
+
+        def forward(self, x: torch.Tensor) -> torch.Tensor:
+            return x
+
+    return torch.jit.script(Frozen())
+
+
+def test_reader_from_torchscript_file(dpb, layout, model, tmp_path):
+    """A frozen / compressed TorchScript file: sel and rcut come from the
+    model's own get_sel / get_rcut, the entries (tables included) from its
+    state dict."""
+    import torch
+
+    ck = importlib.import_module("deepmd_kit_lr_pt_b200.checkpoint")
+    g = layout[0]
+    sd = ck.params_to_state_dict(model)
+    path = str(tmp_path / "frozen_compressed.pth")
+    torch.jit.save(_scripted_model(sd, g["sel"], g["rcut"]), path)
+    p = ck.load(path)
+    assert p.cfg.sel == tuple(int(x) for x in g["sel"]) and p.cfg.rcut == float(g["rcut"])
+    np.testing.assert_array_equal(p.dstd, model.dstd)
+    assert len(p.tables) == len(model.tables)
+    for (t0, i0), (t1, i1) in zip(p.tables, model.tables):
+        np.testing.assert_array_equal(t0, t1)
+        np.testing.assert_array_equal(i0, i1)
+    for f0, f1 in zip(p.fit, model.fit):
+        for (W, b, _), (W1, b1, _) in zip(f0["layers"], f1["layers"]):
+            np.testing.assert_array_equal(W, W1)
+            np.testing.assert_array_equal(b, b1)
+
+
 class _Opaque:
     """An object only a full unpickler can rebuild."""
 
