@@ -212,3 +212,20 @@ def test_reader_rejects_wrong_sel(dpb, model):
         ck.params_from_state_dict(sd, sel=(46, 90))
     with pytest.raises(ValueError):
         ck.params_from_state_dict({"x": 1}, sel=(46, 92))
+
+
+def test_trainable_names_are_the_reference_parameters(dpb, layout, model):
+    """Every trainable tensor of the training step (train.param_specs, the
+    flat layout's order) is a reference state-dict entry of the same shape,
+    and together they are all of the reference's network weights, so trained
+    weights go back into the reference's checkpoint by name."""
+    tr = importlib.import_module("deepmd_kit_lr_pt_b200.train")
+    _, shapes, _ = layout
+    specs = tr.param_specs(model)
+    names = [n for n, _ in specs]
+    assert len(names) == len(set(names))
+    for n, a in specs:
+        assert n in shapes, n
+        assert tuple(a.shape) == shapes[n], (n, a.shape, shapes[n])
+    nets = {k for k in shapes if ".networks." in k}
+    assert set(names) == nets, sorted(nets ^ set(names))
